@@ -1,0 +1,304 @@
+"""Reader / writer for omegagene's binary ".cls" launch-set input (format v.0.52).
+
+The layout follows ``Read::load_launch_set`` and its section loaders
+(src/celeste/core/Read.cpp:50-600): a magic number (66261), a version string, thirteen
+section sizes in bytes, then the sections in header order.  Atom indices in the bond,
+angle, torsion, 1-4, 1-5-exclusion and constraint sections are 0-based; atom types,
+LJ type pairs and atom-group members are 1-based (Read.cpp:279, 306, 568).
+
+Sections the MD hot path does not use (torsions, impropers, 1-4 pairs, restraints, VcMD,
+group coordinates, potential tables) are kept as raw bytes so that a file read and
+written back is byte-identical.
+"""
+import struct
+
+import numpy as np
+
+MAGIC = 66261
+VERSION = "v.0.52"
+SECTIONS = ("box", "crd", "vel", "topol", "constraint", "settle", "extended", "groups",
+            "dist_restraint", "pos_restraint", "extended_vcmd", "group_coord", "pote")
+
+
+class ClsFormatError(ValueError):
+    pass
+
+
+class _Reader:
+    def __init__(self, buf):
+        self.b = buf
+        self.o = 0
+
+    def i(self, n=None):
+        if n is None:
+            v = struct.unpack_from("<i", self.b, self.o)[0]
+            self.o += 4
+            return v
+        v = np.frombuffer(self.b, dtype="<i4", count=n, offset=self.o).astype(np.int32)
+        self.o += 4 * n
+        return v
+
+    def d(self, n=None):
+        if n is None:
+            v = struct.unpack_from("<d", self.b, self.o)[0]
+            self.o += 8
+            return v
+        v = np.frombuffer(self.b, dtype="<f8", count=n, offset=self.o).astype(np.float64)
+        self.o += 8 * n
+        return v
+
+    def rec(self, dtype, n):
+        v = np.frombuffer(self.b, dtype=dtype, count=n, offset=self.o).copy()
+        self.o += np.dtype(dtype).itemsize * n
+        return v
+
+    def raw(self, n):
+        v = bytes(self.b[self.o:self.o + n])
+        self.o += n
+        return v
+
+
+BOND = np.dtype([("a1", "<i4"), ("a2", "<i4"), ("k", "<f8"), ("r0", "<f8")])
+ANGLE = np.dtype([("a1", "<i4"), ("a2", "<i4"), ("a3", "<i4"), ("k", "<f8"), ("t0", "<f8")])
+LJ = np.dtype([("t1", "<i4"), ("t2", "<i4"), ("p6", "<f8"), ("p12", "<f8")])
+
+
+def _parse_topol(b, n_atoms):
+    r = _Reader(b)
+    t = {}
+    n = r.i()
+    if n != n_atoms:
+        raise ClsFormatError("topology atom count %d != %d" % (n, n_atoms))
+    t["charge"] = r.d(n)
+    t["mass"] = r.d(n)
+    t["atom_type"] = r.i(n) - 1
+    size_lj = r.i()
+    t["n_lj_types"] = r.i()
+    n_pairs = r.i()
+    t["lj_pairs"] = r.rec(LJ, n_pairs)
+    if size_lj != 8 + LJ.itemsize * n_pairs:
+        raise ClsFormatError("inconsistent LJ section")
+    size_hps = r.i()
+    t["lj_hps_raw"] = r.raw(size_hps)
+    size_bond = r.i()
+    nb = r.i()
+    t["bonds"] = r.rec(BOND, nb)
+    size_angle = r.i()
+    na = r.i()
+    t["angles"] = r.rec(ANGLE, na)
+    for key in ("torsions_raw", "impros_raw", "nb14_raw"):
+        size = r.i()
+        t[key] = r.raw(size)
+    size_15 = r.i()
+    n15 = r.i()
+    t["nb15off_pairs"] = r.i(2 * n15).reshape(n15, 2)
+    if r.o != len(b):
+        raise ClsFormatError("trailing bytes in topology section")
+    return t
+
+
+def _parse_constraint(b):
+    r = _Reader(b)
+    n2, n3, n4 = r.i(), r.i(), r.i()
+    c = {}
+    p = r.rec(np.dtype([("a", "<i4", 2), ("d", "<f8")]), n2)
+    c["pair_atoms"], c["pair_dist"] = p["a"].copy(), p["d"].copy()
+    t = r.rec(np.dtype([("a", "<i4", 3), ("d", "<f8", 3)]), n3)
+    c["trio_atoms"], c["trio_dist"] = t["a"].copy(), t["d"].copy()
+    q = r.rec(np.dtype([("a", "<i4", 4), ("d", "<f8", 6)]), n4)
+    c["quad_atoms"], c["quad_dist"] = q["a"].copy(), q["d"].copy()
+    return c
+
+
+def _parse_vmcmd(b):
+    r = _Reader(b)
+    v = {"n_vs": r.i(), "interval": r.i(), "temperature": r.d(), "states": []}
+    for _ in range(v["n_vs"]):
+        order = r.i()
+        lam_lo, lam_hi, p_lo, p_hi = r.d(), r.d(), r.d(), r.d()
+        coef = r.d(order + 1)
+        a_lo, a_hi = r.d(), r.d()
+        v["states"].append(dict(order=order, lambda_low=lam_lo, lambda_high=lam_hi, prob_low=p_lo,
+                                prob_high=p_hi, coef=coef, alpha_low=a_lo, alpha_high=a_hi))
+    v["init_vs"] = r.i()
+    v["seed"] = r.i()
+    return v
+
+
+def _parse_groups(b):
+    r = _Reader(b)
+    n = r.i()
+    names, counts = [], []
+    for _ in range(n):
+        ln = r.i()
+        names.append(r.raw(ln).split(b"\0")[0].decode())
+        counts.append(r.i())
+    groups = [r.i(c) - 1 for c in counts]
+    return {"names": names, "atoms": groups}
+
+
+def read_cls(path):
+    """Returns a dict with numpy arrays; raises ClsFormatError on a malformed file."""
+    with open(path, "rb") as f:
+        buf = f.read()
+    r = _Reader(buf)
+    if len(buf) < 8 or r.i() != MAGIC:
+        raise ClsFormatError("%s: bad magic number" % path)
+    ln = r.i()
+    version = r.raw(ln).split(b"\0")[0].decode()
+    if version != VERSION:
+        raise ClsFormatError("%s: version %s, %s required" % (path, version, VERSION))
+    sizes = dict(zip(SECTIONS, [r.i() for _ in SECTIONS]))
+    raw = {}
+    for s in SECTIONS:
+        if sizes[s] < 0 or r.o + sizes[s] > len(buf):
+            raise ClsFormatError("%s: section %s runs past the end of the file" % (path, s))
+        raw[s] = r.raw(sizes[s])
+    if r.o != len(buf):
+        raise ClsFormatError("%s: trailing bytes" % path)
+    out = {"version_len": ln, "raw": raw}
+    if raw["box"]:
+        out["pbc_val"] = np.frombuffer(raw["box"], dtype="<f8").copy()
+    if raw["crd"]:
+        rr = _Reader(raw["crd"])
+        n = rr.i()
+        out["n_atoms"] = n
+        out["crd"] = rr.d(3 * n).reshape(n, 3)
+    if raw["vel"]:
+        rr = _Reader(raw["vel"])
+        n = rr.i()
+        out["vel"] = rr.d(3 * n).reshape(n, 3)
+    if raw["topol"]:
+        out["topol"] = _parse_topol(raw["topol"], out["n_atoms"])
+    if raw["constraint"]:
+        out["constraint"] = _parse_constraint(raw["constraint"])
+    if raw["settle"]:
+        out["settle"] = _parse_constraint(raw["settle"])
+    if raw["extended"]:
+        out["vmcmd"] = _parse_vmcmd(raw["extended"])
+    if raw["groups"]:
+        out["groups"] = _parse_groups(raw["groups"])
+    return out
+
+
+# ------------------------------------------------------------------ writer
+
+def _pack_topol(t, n_atoms):
+    parts = [struct.pack("<i", n_atoms),
+             np.asarray(t["charge"], "<f8").tobytes(),
+             np.asarray(t["mass"], "<f8").tobytes(),
+             (np.asarray(t["atom_type"], np.int64) + 1).astype("<i4").tobytes()]
+    lj = np.asarray(t["lj_pairs"], LJ)
+    body = struct.pack("<ii", int(t["n_lj_types"]), len(lj)) + lj.tobytes()
+    parts += [struct.pack("<i", len(body)), body]
+    hps = t.get("lj_hps_raw", b"")
+    parts += [struct.pack("<i", len(hps)), hps]
+    for key, dt in (("bonds", BOND), ("angles", ANGLE)):
+        arr = np.asarray(t.get(key, np.zeros(0, dt)), dt)
+        body = struct.pack("<i", len(arr)) + arr.tobytes()
+        parts += [struct.pack("<i", len(body)), body]
+    for key in ("torsions_raw", "impros_raw", "nb14_raw"):
+        body = t.get(key, struct.pack("<i", 0))
+        parts += [struct.pack("<i", len(body)), body]
+    p15 = np.asarray(t["nb15off_pairs"], "<i4").reshape(-1, 2)
+    body = struct.pack("<i", len(p15)) + p15.tobytes()
+    parts += [struct.pack("<i", len(body)), body]
+    return b"".join(parts)
+
+
+def _pack_constraint(c):
+    pa = np.asarray(c.get("pair_atoms", np.zeros((0, 2))), "<i4").reshape(-1, 2)
+    ta = np.asarray(c.get("trio_atoms", np.zeros((0, 3))), "<i4").reshape(-1, 3)
+    qa = np.asarray(c.get("quad_atoms", np.zeros((0, 4))), "<i4").reshape(-1, 4)
+    pd = np.asarray(c.get("pair_dist", np.zeros(0)), "<f8").reshape(-1)
+    td = np.asarray(c.get("trio_dist", np.zeros((0, 3))), "<f8").reshape(-1, 3)
+    qd = np.asarray(c.get("quad_dist", np.zeros((0, 6))), "<f8").reshape(-1, 6)
+    out = [struct.pack("<iii", len(pa), len(ta), len(qa))]
+    rp = np.zeros(len(pa), np.dtype([("a", "<i4", 2), ("d", "<f8")]))
+    rp["a"], rp["d"] = pa, pd
+    rt = np.zeros(len(ta), np.dtype([("a", "<i4", 3), ("d", "<f8", 3)]))
+    rt["a"], rt["d"] = ta, td
+    rq = np.zeros(len(qa), np.dtype([("a", "<i4", 4), ("d", "<f8", 6)]))
+    rq["a"], rq["d"] = qa, qd
+    return b"".join(out + [rp.tobytes(), rt.tobytes(), rq.tobytes()])
+
+
+def _pack_vmcmd(v):
+    out = [struct.pack("<iid", len(v["states"]), int(v["interval"]), float(v["temperature"]))]
+    for s in v["states"]:
+        coef = np.asarray(s["coef"], "<f8")
+        out.append(struct.pack("<idddd", len(coef) - 1, s["lambda_low"], s["lambda_high"],
+                               s["prob_low"], s["prob_high"]))
+        out.append(coef.tobytes())
+        out.append(struct.pack("<dd", s.get("alpha_low", 0.0), s.get("alpha_high", 0.0)))
+    out.append(struct.pack("<ii", int(v["init_vs"]), int(v["seed"])))
+    return b"".join(out)
+
+
+def _pack_groups(g):
+    out = [struct.pack("<i", len(g["names"]))]
+    for name, atoms in zip(g["names"], g["atoms"]):
+        nb = name.encode() + b"\0"
+        out += [struct.pack("<i", len(nb)), nb, struct.pack("<i", len(atoms))]
+    for atoms in g["atoms"]:
+        out.append((np.asarray(atoms, np.int64) + 1).astype("<i4").tobytes())
+    return b"".join(out)
+
+
+def write_cls(path, s):
+    """Writes a launch set.  ``s`` uses the keys produced by read_cls (parsed sections win
+    over their raw bytes)."""
+    raw = dict(s.get("raw", {}))
+    n = int(s["n_atoms"])
+    if "pbc_val" in s:
+        raw["box"] = np.asarray(s["pbc_val"], "<f8").tobytes()
+    raw["crd"] = struct.pack("<i", n) + np.asarray(s["crd"], "<f8").reshape(-1).tobytes()
+    if "vel" in s:
+        raw["vel"] = struct.pack("<i", n) + np.asarray(s["vel"], "<f8").reshape(-1).tobytes()
+    if "topol" in s:
+        raw["topol"] = _pack_topol(s["topol"], n)
+    if "constraint" in s:
+        raw["constraint"] = _pack_constraint(s["constraint"])
+    if "settle" in s:
+        raw["settle"] = _pack_constraint(s["settle"])
+    if "vmcmd" in s:
+        raw["extended"] = _pack_vmcmd(s["vmcmd"])
+    if "groups" in s:
+        raw["groups"] = _pack_groups(s["groups"])
+    ver = VERSION.encode() + b"\0"
+    hdr = [struct.pack("<i", MAGIC), struct.pack("<i", len(ver)), ver]
+    hdr += [struct.pack("<i", len(raw.get(k, b""))) for k in SECTIONS]
+    with open(path, "wb") as f:
+        f.write(b"".join(hdr))
+        for k in SECTIONS:
+            f.write(raw.get(k, b""))
+
+
+def lj_tables(topol):
+    """Dense n_types x n_types C6/C12 tables from the LJ type-pair records
+    (MmSystem::set_lj_pair_param, MmSystem.cpp:313-319)."""
+    nt = int(topol["n_lj_types"])
+    c6 = np.zeros((nt, nt), np.float64)
+    c12 = np.zeros((nt, nt), np.float64)
+    for rec in topol["lj_pairs"]:
+        i, j = int(rec["t1"]) - 1, int(rec["t2"]) - 1
+        c6[i, j] = c6[j, i] = rec["p6"]
+        c12[i, j] = c12[j, i] = rec["p12"]
+    return c6, c12
+
+
+def nb15off_table(n_atoms, pairs, max_nb15off=32):
+    """Padded exclusion table as MmSystem::set_nb15off builds it (MmSystem.cpp:478-525):
+    each listed pair is entered in both rows unless already present; -1 pads."""
+    tab = np.full((n_atoms, max_nb15off), -1, np.int32)
+    cnt = np.zeros(n_atoms, np.int64)
+    for a1, a2 in np.asarray(pairs).reshape(-1, 2):
+        for x, y in ((a1, a2), (a2, a1)):
+            row = tab[x, :cnt[x]]
+            if (row == y).any():
+                continue
+            if cnt[x] >= max_nb15off:
+                raise ClsFormatError("more than %d exclusions for atom %d" % (max_nb15off, x))
+            tab[x, cnt[x]] = y
+            cnt[x] += 1
+    return tab

@@ -1,0 +1,274 @@
+"""Seeded synthetic systems for the benchmark workloads (no public dataset is used by the
+reference or named for these workloads; these generators stand in for them).
+
+All systems are returned as launch-set dicts with the keys of :mod:`cls_io` (so they can
+be written as .cls files for the reference CPU programs) plus a few convenience arrays.
+
+Water model: rigid TIP3P, O-H 0.9572 A, H-O-H 104.52 deg, q_O -0.834 e, q_H +0.417 e,
+LJ on O only (sigma 3.15061 A, epsilon 0.1521 kcal/mol) written in the .cls convention
+E = C12/r^12 - C6/r^6 with C12 = 4 eps sigma^12, C6 = 4 eps sigma^6.
+"""
+import math
+
+import numpy as np
+
+WATER_NUMBER_DENSITY = 0.997 * 6.02214076e23 / 18.01528 / 1e24  # molecules / A^3 at 0.997 g/cm^3
+R_OH = 0.9572
+THETA_HOH = math.radians(104.52)
+R_HH = 2.0 * R_OH * math.sin(THETA_HOH / 2.0)
+Q_O, Q_H = -0.834, 0.417
+M_O, M_H = 15.9994, 1.008
+SIGMA_O, EPS_O = 3.15061, 0.1521
+KB_KCAL = 8.31451 / 4.184 * 1e-3  # GAS_CONST / JOULE_CAL * 1e-3 (kcal/mol/K)
+
+
+def water_box_side(n_waters):
+    return (n_waters / WATER_NUMBER_DENSITY) ** (1.0 / 3.0)
+
+
+def _random_rotations(rng, n):
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    return np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1),
+    ], 1)
+
+
+def _maxwell(rng, mass, temperature):
+    """Velocities in A/fs drawn at the temperature (KINETIC_COEFF convention, kcal/mol)."""
+    # KE[kcal/mol] = 0.5 m v^2 * 1e7/4184 with v in A/fs and m in amu (CelesteObject.cpp:39)
+    sd = np.sqrt(KB_KCAL * temperature / (mass * (1e7 / 4184.0)))
+    return rng.normal(size=(len(mass), 3)) * sd[:, None]
+
+
+def water_positions(rng, n_waters, box, lattice_m=None, jitter=0.3, origin=0.0):
+    """O on seeded-random sites of an m^3 lattice with uniform jitter, random orientations."""
+    m = lattice_m or int(math.ceil(n_waters ** (1.0 / 3.0) - 1e-9))
+    spacing = box / m
+    sites = rng.choice(m ** 3, size=n_waters, replace=False)
+    ijk = np.stack([sites // (m * m), (sites // m) % m, sites % m], 1).astype(np.float64)
+    o = origin + (ijk + 0.5) * spacing + rng.uniform(-jitter, jitter, size=(n_waters, 3))
+    half = THETA_HOH / 2.0
+    h_local = np.array([[R_OH * math.sin(half), 0.0, R_OH * math.cos(half)],
+                        [-R_OH * math.sin(half), 0.0, R_OH * math.cos(half)]])
+    rot = _random_rotations(rng, n_waters)
+    h = np.einsum("nij,kj->nki", rot, h_local) + o[:, None, :]
+    xyz = np.empty((n_waters, 3, 3))
+    xyz[:, 0] = o
+    xyz[:, 1:] = h
+    return xyz.reshape(-1, 3)
+
+
+def _wrap(crd, lo, box):
+    return lo + np.mod(crd - lo, box)
+
+
+def water_system(n_waters, box=None, seed=0, temperature=300.0, lattice_m=None, jitter=0.3):
+    """Rigid TIP3P box: one SHAKE trio per molecule, exclusions within molecules."""
+    rng = np.random.default_rng(seed)
+    box = float(box if box is not None else water_box_side(n_waters))
+    crd = water_positions(rng, n_waters, box, lattice_m=lattice_m, jitter=jitter)
+    n = 3 * n_waters
+    mass = np.tile([M_O, M_H, M_H], n_waters)
+    vel = _maxwell(rng, mass, temperature)
+    vel -= (mass[:, None] * vel).sum(0) / mass.sum()
+    sys_ = _assemble(crd, vel, box,
+                     charge=np.tile([Q_O, Q_H, Q_H], n_waters),
+                     mass=mass,
+                     atom_type=np.tile([0, 1, 1], n_waters),
+                     lj_types=[(SIGMA_O, EPS_O), (0.0, 0.0)],
+                     bonds=None, angles=None,
+                     excl=_water_exclusions(0, n_waters),
+                     pairs=None,
+                     trios=_water_trios(0, n_waters))
+    sys_["meta"] = {"kind": "water", "n_waters": n_waters, "seed": seed, "box": box}
+    return sys_
+
+
+def _water_exclusions(first_atom, n_waters):
+    o = first_atom + 3 * np.arange(n_waters)
+    return np.concatenate([np.stack([o, o + 1], 1), np.stack([o, o + 2], 1), np.stack([o + 1, o + 2], 1)])
+
+
+def _water_trios(first_atom, n_waters):
+    o = first_atom + 3 * np.arange(n_waters)
+    atoms = np.stack([o, o + 1, o + 2], 1)
+    dist = np.tile([R_OH, R_HH, R_OH], (n_waters, 1))
+    return atoms, dist
+
+
+def _lj_records(lj_types, mix="lb"):
+    """LJ pair records with Lorentz-Berthelot mixing; types with eps 0 get zero terms."""
+    recs = []
+    nt = len(lj_types)
+    for i in range(nt):
+        for j in range(i, nt):
+            si, ei = lj_types[i]
+            sj, ej = lj_types[j]
+            s = 0.5 * (si + sj)
+            e = math.sqrt(ei * ej)
+            recs.append((i + 1, j + 1, 4.0 * e * s ** 6, 4.0 * e * s ** 12))
+    return np.array(recs, dtype=[("t1", "<i4"), ("t2", "<i4"), ("p6", "<f8"), ("p12", "<f8")])
+
+
+def _assemble(crd, vel, box, charge, mass, atom_type, lj_types, bonds, angles, excl, pairs, trios,
+              groups=None):
+    n = len(crd)
+    lo = -0.5 * box
+    # box centred on the origin (pbc_val[9..11] is the box centre, PBC.cpp:36)
+    crd = _wrap(crd - 0.5 * box, lo, box)
+    topol = {
+        "charge": np.asarray(charge, np.float64),
+        "mass": np.asarray(mass, np.float64),
+        "atom_type": np.asarray(atom_type, np.int32),
+        "n_lj_types": len(lj_types),
+        "lj_pairs": _lj_records(lj_types),
+        "lj_hps_raw": b"",
+        "bonds": bonds if bonds is not None else np.zeros(0, [("a1", "<i4"), ("a2", "<i4"), ("k", "<f8"), ("r0", "<f8")]),
+        "angles": angles if angles is not None else np.zeros(0, [("a1", "<i4"), ("a2", "<i4"), ("a3", "<i4"), ("k", "<f8"), ("t0", "<f8")]),
+        "torsions_raw": b"\0\0\0\0", "impros_raw": b"\0\0\0\0", "nb14_raw": b"\0\0\0\0",
+        "nb15off_pairs": np.concatenate([excl, excl[:, ::-1]], 1).reshape(-1, 2).astype(np.int32),
+    }
+    cons = {"pair_atoms": np.zeros((0, 2), np.int32), "pair_dist": np.zeros(0),
+            "trio_atoms": np.zeros((0, 3), np.int32), "trio_dist": np.zeros((0, 3)),
+            "quad_atoms": np.zeros((0, 4), np.int32), "quad_dist": np.zeros((0, 6))}
+    if pairs is not None:
+        cons["pair_atoms"], cons["pair_dist"] = pairs
+    if trios is not None:
+        cons["trio_atoms"], cons["trio_dist"] = trios
+    pbc_val = np.array([box, 0, 0, 0, box, 0, 0, 0, box, 0.0, 0.0, 0.0])
+    out = {"n_atoms": n, "pbc_val": pbc_val, "crd": crd, "vel": vel, "topol": topol, "constraint": cons,
+           "groups": groups or {"names": ["all"], "atoms": [np.arange(n, dtype=np.int32)]}}
+    return out
+
+
+def _saw_chain(rng, n_backbone, radius, bond=1.53, angle_deg=111.0, min_dist=2.4, max_tries=200):
+    """Self-avoiding random walk with fixed bond length and bond angle, confined to a sphere."""
+    theta = math.radians(angle_deg)
+    pts = [np.zeros(3)]
+    d0 = rng.normal(size=3)
+    d0 /= np.linalg.norm(d0)
+    pts.append(pts[0] + bond * d0)
+    while len(pts) < n_backbone:
+        ok = False
+        for _ in range(max_tries):
+            prev = pts[-1] - pts[-2]
+            prev /= np.linalg.norm(prev)
+            perp = np.cross(prev, rng.normal(size=3))
+            perp /= np.linalg.norm(perp)
+            phi = rng.uniform(0, 2 * math.pi)
+            perp = perp * math.cos(phi) + np.cross(prev, perp) * math.sin(phi)
+            d = math.cos(math.pi - theta) * prev + math.sin(math.pi - theta) * perp
+            cand = pts[-1] + bond * d
+            if np.linalg.norm(cand) > radius:
+                continue
+            arr = np.asarray(pts[:-2])
+            if len(arr) and np.min(np.linalg.norm(arr - cand, axis=1)) < min_dist:
+                continue
+            pts.append(cand)
+            ok = True
+            break
+        if not ok:  # restart the walk from a shorter prefix
+            del pts[max(2, len(pts) - 20):]
+    return np.asarray(pts)
+
+
+def chain_water_system(n_chain=2000, n_waters=30000, seed=1, radius=30.0, box=None, temperature=300.0,
+                       n_sigma_bins=8, n_eps_bins=8):
+    """Solvated synthetic chain: every third atom is a hydrogen bonded (SHAKE pair, 1.09 A) to
+    the preceding backbone atom; backbone bonds 1.53 A / 310, angles 111 deg / 63 (E = k(x-x0)^2,
+    ForceField.cpp:108-177).  Charges ~ N(0, 0.25) shifted to zero net; sigma ~ U(2.5, 3.8),
+    epsilon ~ U(0.02, 0.2) binned into n_sigma_bins x n_eps_bins LJ types with Lorentz-Berthelot
+    mixing.  Waters within 2.4 A of the solute are removed.  Exclusions: 1-2 and 1-3 pairs."""
+    rng = np.random.default_rng(seed)
+    n_h = n_chain // 3
+    n_bb = n_chain - n_h
+    bb = _saw_chain(rng, n_bb, radius)
+    # atom order: for k-th H, insert after its parent backbone atom
+    order = []
+    parent_of_h = {}
+    bb_index = []
+    idx = 0
+    for b in range(n_bb):
+        bb_index.append(idx)
+        idx += 1
+        if len(parent_of_h) < n_h and (b % 2 == 1):
+            parent_of_h[idx] = idx - 1
+            idx += 1
+    while len(parent_of_h) < n_h:  # if the chain is short, attach remaining H at the end
+        parent_of_h[idx] = bb_index[len(parent_of_h) % n_bb]
+        idx += 1
+    n_c = idx
+    crd_c = np.zeros((n_c, 3))
+    crd_c[bb_index] = bb
+    for h, p in parent_of_h.items():
+        v = rng.normal(size=3)
+        v /= np.linalg.norm(v)
+        crd_c[h] = crd_c[p] + 1.09 * v
+    sig = rng.uniform(2.5, 3.8, n_c)
+    eps = rng.uniform(0.02, 0.2, n_c)
+    sb = np.minimum((sig - 2.5) / 1.3 * n_sigma_bins, n_sigma_bins - 1).astype(int)
+    eb = np.minimum((eps - 0.02) / 0.18 * n_eps_bins, n_eps_bins - 1).astype(int)
+    lj_types = [(SIGMA_O, EPS_O), (0.0, 0.0)]
+    for i in range(n_sigma_bins):
+        for j in range(n_eps_bins):
+            lj_types.append((2.5 + (i + 0.5) * 1.3 / n_sigma_bins, 0.02 + (j + 0.5) * 0.18 / n_eps_bins))
+    type_c = 2 + sb * n_eps_bins + eb
+    q = rng.normal(0.0, 0.25, n_c)
+    q -= q.mean()
+    mass_c = np.where(np.isin(np.arange(n_c), list(parent_of_h.keys())), M_H, 12.011)
+    box = float(box if box is not None else water_box_side(n_waters + n_chain / 3.0))
+    # waters on a lattice filling the box, solute at the centre, then overlap removal
+    w = water_positions(rng, n_waters, box, jitter=0.3).reshape(n_waters, 3, 3) - 0.5 * box
+    dmin = np.full(n_waters, np.inf)
+    for start in range(0, n_c, 256):
+        blk = crd_c[start:start + 256]
+        d = np.linalg.norm(w[:, None, :, :] - blk[None, :, None, :], axis=-1).min(axis=(1, 2))
+        dmin = np.minimum(dmin, d)
+    w = w[dmin >= 2.4]
+    nw = len(w)
+    crd = np.concatenate([crd_c, w.reshape(-1, 3)]) + 0.5 * box
+    n = len(crd)
+    charge = np.concatenate([q, np.tile([Q_O, Q_H, Q_H], nw)])
+    mass = np.concatenate([mass_c, np.tile([M_O, M_H, M_H], nw)])
+    atom_type = np.concatenate([type_c, np.tile([0, 1, 1], nw)])
+    bonds = [(bb_index[i], bb_index[i + 1], 310.0, 1.53) for i in range(n_bb - 1)]
+    angles = [(bb_index[i], bb_index[i + 1], bb_index[i + 2], 63.0, math.radians(111.0)) for i in range(n_bb - 2)]
+    bonds = np.array(bonds, dtype=[("a1", "<i4"), ("a2", "<i4"), ("k", "<f8"), ("r0", "<f8")])
+    angles = np.array(angles, dtype=[("a1", "<i4"), ("a2", "<i4"), ("a3", "<i4"), ("k", "<f8"), ("t0", "<f8")])
+    excl = set()
+    for b in bonds:
+        excl.add((int(b["a1"]), int(b["a2"])))
+    for a in angles:
+        excl.add((int(a["a1"]), int(a["a3"])))
+    for h, p in parent_of_h.items():
+        excl.add((p, h))
+        # the H and the backbone neighbours of its parent are 1-3
+        k = bb_index.index(p)
+        for kk in (k - 1, k + 1):
+            if 0 <= kk < n_bb:
+                excl.add((min(h, bb_index[kk]), max(h, bb_index[kk])))
+    excl = np.array(sorted((min(a, b), max(a, b)) for a, b in excl), np.int64)
+    excl = np.concatenate([excl, _water_exclusions(n_c, nw)])
+    pairs = (np.array([(p, h) for h, p in sorted(parent_of_h.items())], np.int32),
+             np.full(len(parent_of_h), 1.09))
+    trios = _water_trios(n_c, nw)
+    vel = _maxwell(rng, mass, temperature)
+    vel -= (mass[:, None] * vel).sum(0) / mass.sum()
+    groups = {"names": ["solute", "solvent"],
+              "atoms": [np.arange(n_c, dtype=np.int32), np.arange(n_c, n, dtype=np.int32)]}
+    s = _assemble(crd, vel, box, charge, mass, atom_type, lj_types, bonds, angles, excl, pairs, trios, groups)
+    s["meta"] = {"kind": "chain_water", "n_chain": n_c, "n_waters": nw, "seed": seed, "box": box}
+    return s
+
+
+def poisson_job_stream(n_jobs=256, seed=3, lo=500, hi=10000, mean_interarrival_s=0.05):
+    """Serving workload: water counts log-uniform in [lo, hi], Poisson arrival times."""
+    rng = np.random.default_rng(seed)
+    counts = np.exp(rng.uniform(math.log(lo), math.log(hi), n_jobs)).astype(int)
+    arrivals = np.cumsum(rng.exponential(mean_interarrival_s, n_jobs))
+    return [{"job": i, "n_waters": int(c), "seed": 1000 + i, "arrival_s": float(t)}
+            for i, (c, t) in enumerate(zip(counts, arrivals))]

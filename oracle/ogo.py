@@ -1,0 +1,284 @@
+"""ctypes bindings for the CPU oracle (TEST INFRASTRUCTURE; imported only by tests/,
+__graft_entry__.smoke() and bench.py's CPU legs).
+
+``OracleSystem`` drives the C restatement (libogo.so) through the reference's per-step
+sequence (DynamicsModePresto::calc_in_each_step, src/celeste/core/DynamicsMode.cpp:468-560).
+``ref_minicell`` runs the reference's own MiniCell.cpp (oracle/_ref/libogref_minicell.so).
+"""
+import ctypes as C
+import math
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+MAX_NB15OFF = 32
+
+i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+
+
+class Pbc(C.Structure):
+    _fields_ = [(k, C.c_float * 3) for k in ("L", "L_half", "L_inv", "L_half_inv", "lower", "upper")]
+
+
+class Geom(C.Structure):
+    _fields_ = [("n_atoms", C.c_int), ("cutoff_pair", C.c_float), ("cutoff_pair_half", C.c_float),
+                ("cutoff_pair2", C.c_float), ("exbox_l", C.c_float * 3), ("box_lower", C.c_float * 3),
+                ("n_cells_xy", C.c_int * 2), ("L_cell", C.c_float * 2), ("n_columns", C.c_int),
+                ("n_neighbors", C.c_int * 2), ("n_uni_z", C.c_int), ("L_z_uni", C.c_float)]
+
+
+class Grid(C.Structure):
+    _fields_ = [("n_cells", C.c_int), ("n_slots", C.c_int), ("slot_atomid", C.POINTER(C.c_int)),
+                ("slot_crd", C.POINTER(C.c_double)), ("atomids_rev", C.POINTER(C.c_int)),
+                ("cell_column", C.POINTER(C.c_int)), ("cell_z", C.POINTER(C.c_int)),
+                ("col_head_cell", C.POINTER(C.c_int)), ("col_n_atoms", C.POINTER(C.c_int))]
+
+
+class CellPairs(C.Structure):
+    _fields_ = [("n_pairs", C.c_int), ("idx_head", C.POINTER(C.c_int)), ("cell1", C.POINTER(C.c_int)),
+                ("cell2", C.POINTER(C.c_int)), ("image", C.POINTER(C.c_int)),
+                ("mask", C.POINTER(C.c_uint64))]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        from . import build
+        path = build.build_oracle()
+        L = C.CDLL(path)
+        L.ogo_pbc_init.argtypes = [C.POINTER(Pbc), f64p]
+        L.ogo_geom_init.argtypes = [C.POINTER(Geom), C.POINTER(Pbc), C.c_int, C.c_double]
+        L.ogo_grid_build.argtypes = [C.POINTER(Geom), C.c_int, f64p, C.POINTER(Grid)]
+        L.ogo_grid_free.argtypes = [C.POINTER(Grid)]
+        L.ogo_enumerate_cell_pairs.argtypes = [C.POINTER(Geom), C.POINTER(Pbc), C.POINTER(Grid), i32p, C.c_int,
+                                               C.POINTER(CellPairs)]
+        L.ogo_cellpairs_free.argtypes = [C.POINTER(CellPairs)]
+        L.ogo_zd_constants.argtypes = [C.c_double, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                       C.POINTER(C.c_float)]
+        L.ogo_pair_cells_f32.argtypes = [C.POINTER(Pbc), C.POINTER(Grid), C.POINTER(CellPairs), f32p, i32p, C.c_int,
+                                         f32p, f32p, C.c_double, C.c_float, C.c_float, C.c_float, f64p, f64p]
+        L.ogo_pair_allpairs_f32.argtypes = [C.POINTER(Pbc), C.c_int, f64p, f32p, i32p, C.c_int, f32p, f32p, i32p,
+                                            C.c_int, C.c_double, C.c_float, C.c_float, C.c_float, f64p, f64p]
+        L.ogo_pair_allpairs_f64.argtypes = [f64p, C.c_int, f64p, f64p, i32p, C.c_int, f64p, f64p, i32p, C.c_int,
+                                            C.c_double, f64p, f64p, f64p]
+        L.ogo_pair_cells_f64.argtypes = [f64p, C.POINTER(Grid), C.POINTER(CellPairs), f64p, f64p, i32p, C.c_int,
+                                         f64p, f64p, C.c_double, f64p, f64p, f64p]
+        L.ogo_excess_f32.argtypes = [C.POINTER(Pbc), C.c_int, i32p, f64p, f32p, C.c_float, C.c_float, f64p]
+        L.ogo_excess_f32.restype = C.c_double
+        L.ogo_excess_f64.argtypes = [f64p, C.c_int, i32p, f64p, f64p, C.c_double, f64p, f64p]
+        L.ogo_excess_f64.restype = C.c_double
+        L.ogo_self_energy.argtypes = [C.c_int, C.c_int, i32p, f32p, C.c_float]
+        L.ogo_self_energy.restype = C.c_double
+        L.ogo_excess_pairs.argtypes = [C.c_int, i32p, C.c_int, i32p, C.c_int]
+        L.ogo_bonds.argtypes = [C.POINTER(Pbc), C.c_int, i32p, f64p, f64p, f64p, f64p]
+        L.ogo_bonds.restype = C.c_double
+        L.ogo_angles.argtypes = [C.POINTER(Pbc), C.c_int, i32p, f64p, f64p, f64p, f64p]
+        L.ogo_angles.restype = C.c_double
+        L.ogo_mcmd_scale.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int, f64p, C.c_double, C.c_int, f64p]
+        L.ogo_mcmd_scale.restype = C.c_double
+        _lib = L
+    return _lib
+
+
+def _arr(ptr, n, dtype):
+    if n <= 0:
+        return np.zeros(0, dtype)
+    return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dtype, copy=True)
+
+
+def make_pbc(pbc_val):
+    p = Pbc()
+    lib().ogo_pbc_init(C.byref(p), np.ascontiguousarray(pbc_val, np.float64))
+    return p
+
+
+def make_geom(pbc, n_atoms, nsgrid_cutoff):
+    g = Geom()
+    rc = lib().ogo_geom_init(C.byref(g), C.byref(pbc), int(n_atoms), float(nsgrid_cutoff))
+    if rc != 0:
+        raise ValueError("grid geometry rejected (%d)" % rc)
+    return g
+
+
+def geom_dict(g):
+    return {"n_cells_x": g.n_cells_xy[0], "n_cells_y": g.n_cells_xy[1], "L_cell_x": g.L_cell[0],
+            "L_cell_y": g.L_cell[1], "n_neighbors_x": g.n_neighbors[0], "n_neighbors_y": g.n_neighbors[1],
+            "n_uni_z": g.n_uni_z, "L_z_uni": g.L_z_uni, "n_columns": g.n_columns}
+
+
+def wrap_inbox(pbc, crd):
+    """MmSystem::revise_crd_inbox (MmSystem.cpp:808-816) in numpy (while loops, float bounds)."""
+    crd = np.array(crd, np.float64).reshape(-1, 3)
+    lo = np.array(pbc.lower, np.float32).astype(np.float64)
+    up = np.array(pbc.upper, np.float32).astype(np.float64)
+    L = np.array(pbc.L, np.float32).astype(np.float64)
+    for d in range(3):
+        x = crd[:, d]
+        while (x < lo[d]).any():
+            x[x < lo[d]] += L[d]
+        while (x >= up[d]).any():
+            x[x >= up[d]] -= L[d]
+    return crd
+
+
+class CellList:
+    """Grid assignment + cell-pair list computed by the oracle (copied to numpy)."""
+
+    def __init__(self, pbc, geom, crd, nb15off):
+        L = lib()
+        grid = Grid()
+        crd = np.ascontiguousarray(crd, np.float64).reshape(-1)
+        n = len(crd) // 3
+        L.ogo_grid_build(C.byref(geom), n, crd, C.byref(grid))
+        cps = CellPairs()
+        L.ogo_enumerate_cell_pairs(C.byref(geom), C.byref(pbc), C.byref(grid),
+                                   np.ascontiguousarray(nb15off, np.int32).reshape(-1), MAX_NB15OFF, C.byref(cps))
+        self._grid, self._cps = grid, cps
+        self.n_cells = grid.n_cells
+        self.n_slots = grid.n_slots
+        self.slot_atomid = _arr(grid.slot_atomid, grid.n_slots, np.int32)
+        self.slot_crd = _arr(grid.slot_crd, 3 * grid.n_slots, np.float64).reshape(-1, 3)
+        self.atomids_rev = _arr(grid.atomids_rev, n, np.int32)
+        self.cell_column = _arr(grid.cell_column, grid.n_cells, np.int32)
+        self.col_head_cell = _arr(grid.col_head_cell, geom.n_columns + 1, np.int32)
+        self.n_pairs = cps.n_pairs
+        self.idx_head = _arr(cps.idx_head, grid.n_cells + 1, np.int32)
+        self.cell1 = _arr(cps.cell1, cps.n_pairs, np.int32)
+        self.cell2 = _arr(cps.cell2, cps.n_pairs, np.int32)
+        self.image = _arr(cps.image, cps.n_pairs, np.int32)
+        self.mask = _arr(cps.mask, cps.n_pairs, np.uint64)
+
+    def __del__(self):
+        try:
+            lib().ogo_grid_free(C.byref(self._grid))
+            lib().ogo_cellpairs_free(C.byref(self._cps))
+        except Exception:
+            pass
+
+
+def unmasked_pair_keys(slot_atomid, cell1, cell2, image, mask):
+    """Order-free content of a cell-pair list: one int64 key per unmasked atom pair,
+    (lo_id, hi_id, image seen from lo_id), sorted.  Two lists whose grids differ only in the
+    order of atoms with equal float z (the reference's quicksort tie order) give equal keys."""
+    slot_atomid = np.asarray(slot_atomid, np.int64)
+    bits = ((np.asarray(mask, np.uint64)[:, None] >> np.arange(64, dtype=np.uint64)[None, :]) & np.uint64(1)) == 0
+    cp, b = np.nonzero(bits)
+    a1 = b % 8
+    a2 = b // 8
+    id1 = slot_atomid[np.asarray(cell1, np.int64)[cp] * 8 + a1]
+    id2 = slot_atomid[np.asarray(cell2, np.int64)[cp] * 8 + a2]
+    img = np.asarray(image, np.int64)[cp]
+    neg = ((img & 1) << 1) | ((img & 2) >> 1) | ((img & 4) << 1) | ((img & 8) >> 1) | ((img & 16) << 1) | ((img & 32) >> 1)
+    swap = id1 > id2
+    lo = np.where(swap, id2, id1)
+    hi = np.where(swap, id1, id2)
+    im = np.where(swap, neg, img)
+    return np.sort((lo << 32) | (hi << 6) | im)
+
+
+def zd_constants(cutoff):
+    z, b, f = C.c_float(), C.c_float(), C.c_float()
+    lib().ogo_zd_constants(float(cutoff), C.byref(z), C.byref(b), C.byref(f))
+    return z.value, b.value, f.value
+
+
+def excess_pairs(n, nb15off):
+    cap = int((np.asarray(nb15off) >= 0).sum()) + 1
+    out = np.zeros(2 * cap, np.int32)
+    ne = lib().ogo_excess_pairs(n, np.ascontiguousarray(nb15off, np.int32).reshape(-1), MAX_NB15OFF, out, cap)
+    return out[:2 * ne].reshape(-1, 2)
+
+
+# ------------------------------------------------------------------ reference MiniCell
+
+_ref = None
+
+
+class RefCapacityError(RuntimeError):
+    pass
+
+
+def ref_lib():
+    """The reference's own MiniCell (None when oracle/_ref was not built)."""
+    global _ref
+    if _ref is None:
+        path = os.path.join(HERE, "_ref", "libogref_minicell.so")
+        if not os.path.exists(path):
+            return None
+        R = C.CDLL(path)
+        R.ogref_minicell.argtypes = [C.c_int, f64p, C.c_double, C.c_double, f64p, i32p, C.c_int, i32p, f32p,
+                                     C.c_int, C.POINTER(C.c_int), i32p, f64p, C.c_int, i32p, C.c_int,
+                                     C.POINTER(C.c_int), i32p, i32p, i32p, i32p, u32p]
+        _ref = R
+    return _ref
+
+
+def ref_pair_capacity(geom, n_atoms, density=1.0):
+    """MiniCell::set_grid_xy's cell-pair capacity (MiniCell.cpp:248-280).  The reference calls
+    exit(0) from add_cell_pair (:1170-1173) when a list exceeds it, so callers check first."""
+    f = np.float32
+    nx, ny = geom.n_cells_xy[0], geom.n_cells_xy[1]
+    mac = int(math.ceil(f(f(f(f(geom.exbox_l[2]) * f(geom.L_cell[0])) * f(geom.L_cell[1])) * f(density)) * 1.3))
+    mac = min(mac, n_atoms)
+    nz = (mac - 8 + 1) // 8
+    max_cells = nx * ny * nz
+    tmp1 = n_atoms // 8 + nx * ny
+    if density > 0 and max_cells > tmp1:
+        max_cells = tmp1
+    nnx, nny = geom.n_neighbors[0], geom.n_neighbors[1]
+    cap = int(((nnx * 2 + 1) * (nny * 2 + 1) * (nnx + nny + 2)) * 0.5 * max_cells * 2.5)
+    return min(cap, (max_cells * max_cells) // 2)
+
+
+def ref_minicell(pbc_val, crd, nb15off, nsgrid_cutoff, density=1.0, expected_pairs=None, geom=None):
+    """Runs the reference MiniCell; returns None when it is not built.  With expected_pairs and
+    geom given, raises RefCapacityError instead of letting the reference exit the process."""
+    R = ref_lib()
+    if R is None:
+        return None
+    if expected_pairs is not None and geom is not None:
+        n_at = len(np.asarray(crd).reshape(-1)) // 3
+        if expected_pairs > ref_pair_capacity(geom, n_at, density):
+            raise RefCapacityError("the reference's cell-pair capacity is too small for this box")
+    crd = np.ascontiguousarray(crd, np.float64).reshape(-1)
+    n = len(crd) // 3
+    cap_slots = n + 8 * 200000
+    cap_cols = 200000
+    cap_pairs = 600 * (n // 8 + 1000)
+    gi = np.zeros(8, np.int32)
+    gf = np.zeros(4, np.float32)
+    slot_atomid = np.zeros(cap_slots, np.int32)
+    slot_crd = np.zeros(3 * cap_slots, np.float64)
+    col_head = np.zeros(cap_cols, np.int32)
+    idx_head = np.zeros(cap_slots // 8 + 2, np.int32)
+    c1 = np.zeros(cap_pairs, np.int32)
+    c2 = np.zeros(cap_pairs, np.int32)
+    img = np.zeros(cap_pairs, np.int32)
+    mask = np.zeros(2 * cap_pairs, np.uint32)
+    n_cells = C.c_int()
+    n_pairs = C.c_int()
+    rc = R.ogref_minicell(n, np.ascontiguousarray(pbc_val, np.float64), float(nsgrid_cutoff), float(density), crd,
+                          np.ascontiguousarray(nb15off, np.int32).reshape(-1), MAX_NB15OFF, gi, gf, cap_slots,
+                          C.byref(n_cells), slot_atomid, slot_crd, cap_cols, col_head, cap_pairs, C.byref(n_pairs),
+                          idx_head, c1, c2, img, mask)
+    if rc != 0:
+        raise RuntimeError("reference MiniCell capacity exceeded")
+    nc, npairs, ncol = n_cells.value, n_pairs.value, int(gi[5])
+    m = mask[:2 * npairs].astype(np.uint64)
+    return {
+        "geom": {"n_cells_x": int(gi[0]), "n_cells_y": int(gi[1]), "n_neighbors_x": int(gi[2]),
+                 "n_neighbors_y": int(gi[3]), "n_uni_z": int(gi[4]), "n_columns": ncol,
+                 "L_cell_x": float(gf[0]), "L_cell_y": float(gf[1]), "L_z_uni": float(gf[2])},
+        "n_cells": nc, "slot_atomid": slot_atomid[:8 * nc].copy(), "slot_crd": slot_crd[:24 * nc].reshape(-1, 3).copy(),
+        "col_head_cell": col_head[:ncol + 1].copy(), "n_pairs": npairs, "idx_head": idx_head[:nc + 1].copy(),
+        "cell1": c1[:npairs].copy(), "cell2": c2[:npairs].copy(), "image": img[:npairs].copy(),
+        "mask": m[0::2] | (m[1::2] << np.uint64(32)),
+    }

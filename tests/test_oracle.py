@@ -1,0 +1,118 @@
+"""The CPU oracle against the reference: its own MiniCell (bit for bit) and the ala3
+known answer printed by the reference all-pairs build."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from omegagene_b200 import cls_io, systems
+from oracle import build as obuild
+from oracle import ogo
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _cell_list_case(s, cutoff=13.0):
+    nb = cls_io.nb15off_table(s["n_atoms"], s["topol"]["nb15off_pairs"])
+    pbc = ogo.make_pbc(s["pbc_val"])
+    crd = ogo.wrap_inbox(pbc, s["crd"])
+    geom = ogo.make_geom(pbc, s["n_atoms"], cutoff)
+    return nb, pbc, crd, geom
+
+
+@pytest.fixture(scope="module")
+def ref_built():
+    if obuild.build_ref() is None or ogo.ref_lib() is None:
+        pytest.skip("reference sources not available to build oracle/_ref")
+    return True
+
+
+@pytest.mark.parametrize("n_waters,box,seed", [(3000, 44.8, 0), (1500, None, 5), (1234, None, 7)])
+def test_cell_list_matches_reference_minicell(ref_built, n_waters, box, seed):
+    s = systems.water_system(n_waters, box=box, seed=seed)
+    nb, pbc, crd, geom = _cell_list_case(s)
+    ours = ogo.CellList(pbc, geom, crd, nb)
+    ref = ogo.ref_minicell(s["pbc_val"], crd, nb, 13.0, expected_pairs=ours.n_pairs, geom=geom)
+    assert ogo.geom_dict(geom) == pytest.approx(ref["geom"])
+    assert ours.n_cells == ref["n_cells"]
+    for k in ("slot_atomid", "col_head_cell", "idx_head", "cell1", "cell2", "image", "mask"):
+        np.testing.assert_array_equal(getattr(ours, k), ref[k], err_msg=k)
+    np.testing.assert_array_equal(ours.slot_crd, ref["slot_crd"])
+
+
+def test_cell_list_matches_reference_on_ala3(ref_built, reference_root):
+    """ala3's coordinates come from a PDB (0.001 A grid), so atoms of one column can share a
+    float z; the reference's quicksort orders such ties arbitrarily.  A seeded 1e-3 A
+    perturbation removes the ties; both implementations get the same coordinates."""
+    s = cls_io.read_cls(os.path.join(reference_root, "samples/ala3/md.inp.cls"))
+    s["crd"] = s["crd"] + np.random.default_rng(11).uniform(-1e-3, 1e-3, s["crd"].shape)
+    nb, pbc, crd, geom = _cell_list_case(s)
+    ours = ogo.CellList(pbc, geom, crd, nb)
+    ref = ogo.ref_minicell(s["pbc_val"], crd, nb, 13.0, expected_pairs=ours.n_pairs, geom=geom)
+    for k in ("slot_atomid", "idx_head", "cell1", "cell2", "image", "mask"):
+        np.testing.assert_array_equal(getattr(ours, k), ref[k], err_msg=k)
+    np.testing.assert_array_equal(ours.slot_crd, ref["slot_crd"])
+
+
+def test_reference_capacity_guard():
+    """Small boxes overflow the reference's max_n_cells^2/2 pair buffer (it exits); the guard
+    reports that instead of running it."""
+    s = systems.water_system(700, seed=5)
+    nb, pbc, crd, geom = _cell_list_case(s)
+    ours = ogo.CellList(pbc, geom, crd, nb)
+    assert ours.n_pairs > ogo.ref_pair_capacity(geom, s["n_atoms"])
+
+
+def _ala3_energies(reference_root):
+    s = cls_io.read_cls(os.path.join(reference_root, "samples/ala3/md.inp.cls"))
+    n, t = s["n_atoms"], s["topol"]
+    nb = cls_io.nb15off_table(n, t["nb15off_pairs"])
+    pbc = ogo.make_pbc(s["pbc_val"])
+    crd = ogo.wrap_inbox(pbc, s["crd"]).reshape(-1)
+    c6, c12 = cls_io.lj_tables(t)
+    q = t["charge"].astype(np.float32)
+    ty = t["atom_type"].astype(np.int32)
+    z, b, f = ogo.zd_constants(12.0)
+    work, ene = np.zeros(3 * n), np.zeros(2)
+    L = ogo.lib()
+    L.ogo_pair_allpairs_f32(pbc, n, crd, q, ty, int(t["n_lj_types"]), c6.astype(np.float32).reshape(-1),
+                            c12.astype(np.float32).reshape(-1), nb.reshape(-1), 32, 12.0, z, b, f, work, ene)
+    ep = ogo.excess_pairs(n, nb).reshape(-1).astype(np.int32)
+    exc = L.ogo_excess_f32(pbc, len(ep) // 2, ep, crd, q, b, f, np.zeros(3 * n))
+    self_e = L.ogo_self_energy(n, len(ep) // 2, ep, q, z)
+    return ene[0], ene[1] + exc + self_e
+
+
+def test_oracle_reproduces_ala3_known_answer(reference_root):
+    gold = json.load(open(os.path.join(HERE, "golden", "ala3_step0.json")))["step0"]
+    vdw, ele = _ala3_energies(reference_root)
+    assert float("%.10e" % vdw) == gold["VDW"]
+    assert float("%.10e" % ele) == gold["Ele"]
+
+
+def test_zd_constants_alpha0():
+    z, b, f = ogo.zd_constants(12.0)
+    assert z == pytest.approx(1.5 / 12.0, rel=1e-7)
+    assert f == pytest.approx(1.0 / 12.0 ** 3, rel=1e-7)
+    assert b == pytest.approx(0.5 / 12.0 ** 3, rel=1e-7)
+
+
+def test_fp32_cell_path_close_to_fp64_oracle():
+    s = systems.water_system(700, seed=2)
+    nb, pbc, crd, geom = _cell_list_case(s)
+    cl = ogo.CellList(pbc, geom, crd, nb)
+    n, t = s["n_atoms"], s["topol"]
+    c6, c12 = cls_io.lj_tables(t)
+    q, ty = t["charge"], t["atom_type"].astype(np.int32)
+    L = np.array(pbc.L, np.float32).astype(np.float64)
+    w64, e64, v64 = np.zeros(3 * n), np.zeros(2), np.zeros(9)
+    ogo.lib().ogo_pair_allpairs_f64(L, n, crd.reshape(-1), q, ty, int(t["n_lj_types"]), c6.reshape(-1),
+                                    c12.reshape(-1), nb.reshape(-1), 32, 12.0, w64, e64, v64)
+    w64c, e64c, v64c = np.zeros(3 * n), np.zeros(2), np.zeros(9)
+    ogo.lib().ogo_pair_cells_f64(L, cl._grid, cl._cps, crd.reshape(-1), q, ty, int(t["n_lj_types"]),
+                                 c6.reshape(-1), c12.reshape(-1), 12.0, w64c, e64c, v64c)
+    # the cell list is complete: FP64 over the list equals FP64 over all pairs
+    np.testing.assert_allclose(w64c, w64, rtol=0, atol=1e-9)
+    np.testing.assert_allclose(e64c, e64, rtol=1e-12)
+    np.testing.assert_allclose(v64c, v64, rtol=1e-10, atol=1e-7)
