@@ -1,0 +1,169 @@
+/*
+ * omegagene_b200.h -- C ABI of the B200 (sm_100a) engine for omegagene's per-step MD hot path:
+ * MiniCell cell assignment + cell-pair list, the Lennard-Jones + zero-dipole pair kernel, and
+ * the leapfrog integrator with SHAKE, velocity scaling and McMD force scaling.
+ *
+ * Plain C types only.  Every call returns an og_status and never exits the process
+ * (the reference's HANDLE_ERROR exits, src/celeste/cuda/cuda_common.h:7-14).  State lives
+ * behind an explicit handle; the reference keeps one system in file-scope device globals
+ * (src/celeste/cuda/cuda_setup.h:32-134).  One engine holds one or more independent systems
+ * ("batch"); every step kernel advances all of them in one launch.
+ *
+ * Units follow the reference: A, fs, amu, kcal/mol, e.  "work" is dE/dx (minus the force),
+ * as in SubBox::work (src/celeste/core/SubBox.cpp:1445-1454).
+ */
+#ifndef OMEGAGENE_B200_H
+#define OMEGAGENE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    OG_OK = 0,
+    OG_ERR_INVALID = 1,   /* bad argument or unsupported input */
+    OG_ERR_CUDA = 2,      /* CUDA runtime error (message in og_last_error) */
+    OG_ERR_CAPACITY = 3,  /* a device buffer is too small (cell pairs, column size) */
+    OG_ERR_STATE = 4,     /* call out of order (e.g. step before finalize) */
+    OG_ERR_NOMEM = 5,     /* device allocation failed */
+    OG_ERR_NOT_CONVERGED = 6 /* SHAKE / thermostat loop hit its iteration limit */
+} og_status;
+
+typedef struct og_engine og_engine;
+
+/* Thermostat kinds (CelesteObject.h THMSTT_*). */
+#define OG_THERMOSTAT_NONE 0
+#define OG_THERMOSTAT_SCALING 1
+
+/* Energies reported per system (og_get_energies). */
+#define OG_E_VDW 0
+#define OG_E_ELE 1        /* pair + excluded-pair ("excess") ZD term + self energy */
+#define OG_E_BOND 2
+#define OG_E_ANGLE 3
+#define OG_E_POTENTIAL 4
+#define OG_E_KINETIC 5
+#define OG_E_TEMPERATURE 6
+#define OG_E_TOTAL 7
+#define OG_E_ELE_EXCESS 8 /* excluded-pair ZD part of OG_E_ELE */
+#define OG_E_ELE_SELF 9   /* constant self energy part of OG_E_ELE */
+#define OG_E_MCMD_FACTOR 10
+#define OG_N_ENERGY 11
+
+/*
+ * One system.  Arrays are host pointers in original atom order, copied by og_add_system.
+ * Replaces the data the reference moves to the device through cuda_alloc_atom_info,
+ * cuda_memcpy_htod_atom_info, cuda_alloc_set_lj_params, cuda_set_pbc,
+ * cuda_zerodipole_constant and cuda_set_constant (src/celeste/cuda/cuda_setup.cu:42-300),
+ * plus the host-side integrator inputs of SubBox / ConstraintShake / ThermostatScaling.
+ */
+typedef struct {
+    int32_t n_atoms;
+    double pbc_val[12];          /* .cls box block: L in [0],[4],[8]; box centre in [9..11] */
+    const double *crd;           /* [3n] */
+    const double *vel;           /* [3n] initial velocities (placed in vel_next as the reference does) */
+    const double *charge;        /* [n] e */
+    const double *mass;          /* [n] amu */
+    const int32_t *atom_type;    /* [n] 0-based LJ types */
+    int32_t n_lj_types;
+    const double *lj6;           /* [n_lj_types^2]  C6 of E = C12/r^12 - C6/r^6 */
+    const double *lj12;          /* [n_lj_types^2] */
+    int32_t n_excl;              /* 1-5-off ("nb15off") pairs, each listed once */
+    const int32_t *excl;         /* [2*n_excl] */
+    int32_t n_shake_pair;        /* ConstraintShake pairs */
+    const int32_t *shake_pair;   /* [2*n] */
+    const double *shake_pair_dist;  /* [n] distance (not squared) */
+    int32_t n_shake_trio;        /* ConstraintShake trios, e.g. (O, H1, H2) */
+    const int32_t *shake_trio;   /* [3*n] */
+    const double *shake_trio_dist;  /* [3*n] d12, d23, d31 (not squared) */
+    int32_t n_bonds;
+    const int32_t *bond;         /* [2*n] */
+    const double *bond_k, *bond_r0;    /* E = k (r - r0)^2 */
+    int32_t n_angles;
+    const int32_t *angle;        /* [3*n] */
+    const double *angle_k, *angle_t0;  /* E = k (theta - t0)^2, t0 in rad */
+    int32_t n_com_groups;        /* COM translation cancelled per group (COMMotion.cpp:30-55) */
+    const int32_t *com_group_start;  /* [n_com_groups+1] */
+    const int32_t *com_group_atoms;
+    /* run parameters (Config keys of the reference) */
+    double cutoff;               /* --cutoff */
+    double nsgrid_cutoff;        /* --nsgrid-cutoff */
+    int32_t nsgrid_update_intvl; /* --nsgrid-update-intvl */
+    double time_step;            /* --time-step (fs) */
+    int32_t thermostat;          /* OG_THERMOSTAT_* (--thermostat) */
+    double temperature;          /* --temperature */
+    double temperature_init;     /* --temperature-init (<0: same as temperature) */
+    int32_t heating_steps;       /* --heating-steps */
+    double berendsen_tau;        /* --berendsen-tau (fs, after the reference's x1000) */
+    int32_t const_max_loops;     /* --const-max-loops */
+    double const_tolerance;      /* --const-tolerance */
+    int32_t thermo_const_max_loops;    /* --thermo-const-max-loops */
+    double thermo_const_tolerance;     /* --thermo-const-tolerance */
+    /* V-McMD force scaling with one virtual state (Extend.cpp:178-203); order < 0 disables */
+    int32_t mcmd_order;
+    double mcmd_lambda_low, mcmd_lambda_high, mcmd_temperature;
+    const double *mcmd_coef;     /* [order+1] */
+} og_system_desc;
+
+/* Creates an engine on a CUDA device (cuda_set_device, cuda_setup.cu:1085-1093). */
+og_status og_create(int device, og_engine **out);
+og_status og_destroy(og_engine *e);
+/* Last error message of this engine ("" if none); valid until the next call. */
+const char *og_last_error(const og_engine *e);
+
+/* Adds a system (before og_finalize).  Its id is returned in sys_id (0, 1, ...). */
+og_status og_add_system(og_engine *e, const og_system_desc *d, int32_t *sys_id);
+/* Allocates device memory for every added system, uploads topology and state, builds the
+ * cell grid and cell-pair list and computes the step-0 forces.  Replaces SubBox::set_nsgrid's
+ * device part: gpu_device_setup, update_device_cell_info, cuda_enumerate_cell_pairs
+ * (SubBox.cpp:487-551, 1683-1723; cuda_setup.cu:1095-1216). */
+og_status og_finalize(og_engine *e);
+
+/* Advances every system by n_steps of DynamicsModePresto::calc_in_each_step
+ * (DynamicsMode.cpp:468-560), rebuilding the cell-pair list every nsgrid_update_intvl steps.
+ * Replaces the per-step cuda_memcpy_htod_crd / cuda_set_crd / cuda_pairwise_ljzd /
+ * cuda_memcpy_dtoh_work sequence (cuda_setup.cu:124-136, 777-823) and the host integrator. */
+og_status og_step(og_engine *e, int32_t n_steps);
+
+/* Rebuilds the cell grid and cell-pair list from the current coordinates and recomputes
+ * forces and energies without advancing time (SubBox::nsgrid_update + SubBox::calc_energy). */
+og_status og_compute_forces(og_engine *e);
+
+og_status og_set_state(og_engine *e, int32_t sys, const double *crd, const double *vel_next);
+og_status og_get_state(og_engine *e, int32_t sys, double *crd, double *vel_next);
+/* work[3n] = dE/dx of the last force evaluation (pair + excess + bonded, before McMD scaling),
+ * energies[OG_N_ENERGY], virial[9] = sum_pairs d_a f_b of the nonbonded (LJ + ZD) terms. */
+og_status og_get_forces(og_engine *e, int32_t sys, double *work, double *energies, double *virial);
+og_status og_get_energies(og_engine *e, int32_t sys, double *energies);
+
+/* Cell grid of the last list build (MiniCell's arrays in canonical order):
+ * n_cells; slot_atomid[8*n_cells] (-1 dummy); col_head_cell[n_columns+1] (-1 empty column). */
+og_status og_get_grid_info(og_engine *e, int32_t sys, int32_t *n_cells, int32_t *n_columns, int32_t *n_pairs);
+og_status og_get_grid(og_engine *e, int32_t sys, int32_t *slot_atomid, double *slot_crd, int32_t *col_head_cell);
+/* Cell-pair list in the reference's CSR order (MiniCell::enumerate_cell_pairs):
+ * idx_head[n_cells+1], cell1/cell2/image[n_pairs], mask[n_pairs] (bit a2*8+a1 = skipped). */
+og_status og_get_cell_pairs(og_engine *e, int32_t sys, int32_t *idx_head, int32_t *cell1, int32_t *cell2,
+                            int32_t *image, uint64_t *mask);
+
+/* Per-step energy trace: enables recording of the last `capacity` steps (0 disables). */
+og_status og_set_trace(og_engine *e, int32_t capacity);
+/* Copies up to max_steps recorded rows [steps][n_sys][OG_N_ENERGY]; returns the count in n_out. */
+og_status og_get_trace(og_engine *e, double *out, int32_t max_steps, int32_t *n_out);
+
+/* Launch statistics: kernels launched by the last og_step and device time of its pair kernel. */
+og_status og_get_stats(og_engine *e, int64_t *kernel_launches, double *pair_kernel_ms, double *step_ms);
+/* Enables CUDA-event timing of the pair kernel and of whole og_step calls (read with
+ * og_get_stats); adds one host synchronisation per step while on. */
+og_status og_set_timing(og_engine *e, int32_t on);
+/* Device flags raised since the last og_step began: bit 8 = a SHAKE trio hit const_max_loops,
+ * bit 16 = the thermostat loop hit thermo_const_max_loops (both non-fatal, as in the reference,
+ * which prints a warning and continues: ConstraintShake.cpp:135-139, Thermostat.cpp:168). */
+og_status og_get_flags(og_engine *e, int32_t *flags);
+/* Number of systems and atoms held. */
+og_status og_get_sizes(og_engine *e, int32_t *n_systems, int64_t *n_atoms_total);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,55 @@
+"""Builds the CUDA engine for sm_100a in-tree: omegagene_b200/libomegagene_b200.so."""
+import concurrent.futures as cf
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "libomegagene_b200.so")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+SOURCES = ["og_grid.cu", "og_pair.cu", "og_integrate.cu", "og_engine.cu"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+
+def _flags(src):
+    f = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE] + ARCH
+    if src == "og_grid.cu":
+        # the cell-membership float arithmetic must not be contracted into FMAs
+        f.append("-fmad=false")
+    return f
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("%s\n%s%s" % (" ".join(cmd), r.stdout, r.stderr))
+    return r.stdout + r.stderr
+
+
+def build(force=False, verbose=False):
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(INCLUDE, "omegagene_b200.h")]
+    newest = max(os.path.getmtime(d) for d in deps)
+    if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= newest:
+        return OUT
+
+    def one(src):
+        obj = os.path.join(objdir, src.replace(".cu", ".o"))
+        out = _run([NVCC, "-c", os.path.join(CSRC, src), "-o", obj] + _flags(src) +
+                   (["-Xptxas", "-v"] if verbose else []))
+        return obj, out
+
+    with cf.ThreadPoolExecutor(len(SOURCES)) as ex:
+        res = list(ex.map(one, SOURCES))
+    if verbose:
+        for _, out in res:
+            print(out)
+    _run([NVCC, "-shared", "-o", OUT] + [o for o, _ in res] + ARCH + ["-lcudart"])
+    return OUT
+
+
+if __name__ == "__main__":
+    import sys
+    print(build(force=True, verbose="-v" in sys.argv))

@@ -1,0 +1,1300 @@
+// og_engine.cu -- host side of the engine and the C ABI declared in include/omegagene_b200.h.
+//
+// Owns every device buffer of a batch of systems, computes the MiniCell geometry on the host
+// with the reference's float arithmetic (MiniCell.cpp:221-290, 1279-1303), and sequences the
+// kernels of one DynamicsModePresto step (DynamicsMode.cpp:468-560) on one CUDA stream.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/omegagene_b200.h"
+#include "og_internal.cuh"
+
+namespace og {
+// og_grid.cu
+__global__ void k_assign_columns(const SysDev *, const int *, const double *, int, int *, unsigned long long *,
+                                 int *, int *);
+__global__ void k_scan_columns(const int *, int, int *, int *, int *, int *, const int *, int, int *);
+__global__ void k_scatter_columns(const int *, const unsigned long long *, int, const int *, int *,
+                                  unsigned long long *);
+__global__ void k_sort_columns(const int *, const int *, const int *, const int *, const unsigned long long *,
+                               const SysDev *, const double *, int *, double *, int *, int *, int *, int *);
+__global__ void k_cell_info(const int *, int, const int *, const int *, const int *, const SysDev *, const double *,
+                            const int *, double *, float2 *, int2 *, unsigned char *, int *, int *);
+__global__ void k_count_pairs(const int *, int, int, const int *, const int *, const SysDev *, const int *,
+                              const int *, const int *, const float2 *, const int2 *, const int *, const int *,
+                              const unsigned char *, int *);
+__global__ void k_fill_pairs(int *, int, int, long long, const int *, const int *, const SysDev *, const int *,
+                             const int *, const int *, const float2 *, const int2 *, const int *, const int *,
+                             const unsigned char *, const int *, const int *, const int *, const int *, const int *,
+                             int2 *, unsigned long long *);
+__global__ void k_pair_heads(int *, int, int, const int *, int *);
+__global__ void k_scan_block(const int *, int *, long long, int *);
+__global__ void k_scan_add(int *, long long, const int *);
+// og_pair.cu
+template <bool VIR>
+__global__ void k_pair_ljzd(const int *, const int *, const SysDev *, const double *, const float4 *, const int *,
+                            const int *, const int2 *, const unsigned long long *, const float2 *,
+                            unsigned long long *, double *, long long);
+// og_integrate.cu
+__global__ void k_excess(int, const int2 *, const int *, const SysDev *, const double *, const double *, const int *,
+                         unsigned long long *, double *, double *);
+__global__ void k_bonds(int, const int2 *, const double2 *, const int *, const SysDev *, const double *, const int *,
+                        unsigned long long *, double *);
+__global__ void k_angles(int, const int4 *, const double2 *, const SysDev *, const double *, const int *,
+                         unsigned long long *, double *);
+__global__ void k_atom_virial(int, const int *, const unsigned long long *, const float4 *, const double *, double *);
+__global__ void k_collect(int, const int *, unsigned long long *, double *);
+__global__ void k_reduce_potential(const SysDev *, const int *, const double *, const double *, const double *,
+                                   const double *, double *, double *);
+__global__ void k_reduce_virial(const SysDev *, const int *, const double *, const double *, const double *,
+                                double *);
+__global__ void k_group_moment(const int *, const int *, const float *, const float *, const double *, const int *,
+                               const int *, double *);
+__global__ void k_reduce_atoms(const SysDev *, const double *, double *, int, int);
+__global__ void k_update_velocities(int, const int *, const SysDev *, const double *, double *, const float *,
+                                    double *, double *);
+__global__ void k_com_apply(int, const int *, const double *, const int *, const int *, double *);
+__global__ void k_thermo_scaling_ke(int, const int *, const SysDev *, const double *, const float *, const float *,
+                                    const double *, double *);
+__global__ void k_thermo_scaling_apply(int, const int *, const SysDev *, const double *, const double *,
+                                       const long long *, const double *, const float *, const double *, double *);
+__global__ void k_update_coordinates(int, const int *, const SysDev *, double *, double *, const double *);
+__global__ void k_shake_pair(int, const int2 *, const double *, const int *, const SysDev *, const int *,
+                             const float *, double *, const double *);
+__global__ void k_shake_trio(int, const int4 *, const double *, const SysDev *, const int *, const float *, double *,
+                             const double *, int, double, int *);
+__global__ void k_ke_mid(int, const float *, const double *, const double *, double *);
+__global__ void k_thermo_check(int, const SysDev *, const double *, const double *, const long long *, int, int,
+                               double, int *, int *, int *);
+__global__ void k_thermo_half(int, const int *, const SysDev *, const int *, const double *, const float *,
+                              const float *, const double *, const double *, const double *, double *, double *);
+__global__ void k_thermo_rescale(int, const int *, const SysDev *, const int *, const double *, const double *,
+                                 const long long *, const double *, const float *, const double *, const double *,
+                                 const double *, double *);
+__global__ void k_thermo_crd(int, const int *, const SysDev *, const int *, double *, const double *,
+                             const double *);
+__global__ void k_finish(int, const int *, const SysDev *, int, double *, const double *, const double *, double *,
+                         const int *, double *, const double *, float4 *, const float *, double *);
+__global__ void k_slot_refresh(const int *, int, const int *, const double *, const double *, const float *,
+                               const int *, float4 *, int *);
+__global__ void k_energies(int, const SysDev *, const double *, const double *, double *, double *, int,
+                           long long *);
+__global__ void k_trace_advance(long long *, long long *);
+
+__global__ void k_fill_int(int *p, long long n, int v) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+__global__ void k_copy_double(double *dst, const double *src, long long n) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[i];
+}
+}  // namespace og
+
+using namespace og;
+
+namespace {
+
+struct HostSystem {
+    og_system_desc d;  // pointers below refer to the owned vectors
+    std::vector<double> crd, vel, charge, mass, lj6, lj12, spd, std_, bk, br0, ak, at0, mcoef;
+    std::vector<int32_t> type, excl, sp, st, bond, angle, gstart, gatoms;
+    SysDev dev;
+    int n_excess = 0;
+    std::vector<int32_t> excess;  // pairs (i<j) in MmSystem::set_excess_pairs order, local ids
+    int d_free = 0;
+};
+
+template <class T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+};
+
+}  // namespace
+
+struct og_engine {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    bool finalized = false;
+    std::vector<HostSystem> sys;
+    // sizes
+    int n_sys = 0, n_atoms = 0, n_cols = 0, n_uni = 0, cells_cap = 0, slots_cap = 0, nnc = 1, intvl = 1;
+    long long pair_cap = 0;
+    int n_excess = 0, n_bonds = 0, n_angles = 0, n_spair = 0, n_strio = 0, n_groups = 0;
+    int shake_max_loops = 1000, thermo_max_loops = 100;
+    double shake_tol = 1e-7, thermo_tol = 1e-5;
+    bool any_groups = false, any_thermo_free = false, any_thermo_cons = false, any_plain_cons = false;
+    bool any_bonds = false, any_angles = false;
+    long long host_step = 0;
+    // device buffers
+    SysDev *d_sys = nullptr;
+    int *d_counters = nullptr;
+    long long *d_step = nullptr, *d_trace_count = nullptr;
+    double *d_crd = nullptr, *d_crd_prev = nullptr, *d_vel = nullptr, *d_vel_next = nullptr, *d_work = nullptr,
+           *d_buf_crd = nullptr, *d_charge = nullptr, *d_ke = nullptr, *d_vir_atom = nullptr;
+    float *d_charge_f = nullptr, *d_mass = nullptr, *d_mass_inv = nullptr;
+    int *d_atom_type = nullptr, *d_atom_sys = nullptr, *d_atom_col = nullptr, *d_atom_slot = nullptr,
+        *d_atom_group = nullptr;
+    unsigned long long *d_atom_key = nullptr, *d_col_keys = nullptr;
+    int *d_col_count = nullptr, *d_col_fill = nullptr, *d_col_atom_start = nullptr, *d_col_cell_start = nullptr,
+        *d_col_head_cell = nullptr, *d_col_sys = nullptr, *d_sys_col_base = nullptr, *d_sys_cell_base = nullptr;
+    int *d_cell_col = nullptr, *d_cell_sys = nullptr, *d_cp_head = nullptr;
+    double *d_cell_origin = nullptr, *d_cell_acc = nullptr;
+    float2 *d_cell_zr = nullptr;
+    int2 *d_cell_uni = nullptr;
+    unsigned char *d_cell_valid = nullptr;
+    int *d_slot_atom = nullptr, *d_slot_type = nullptr;
+    double *d_slot_crd = nullptr;
+    float4 *d_xq = nullptr;
+    unsigned long long *d_frc = nullptr;
+    int *d_uni_lo = nullptr, *d_uni_hi = nullptr;
+    int *d_count = nullptr, *d_offset = nullptr;
+    std::vector<int *> d_scan_tmp;  // per level: sums, scanned sums
+    std::vector<long long> scan_len;
+    int2 *d_cp_c2img = nullptr;
+    unsigned long long *d_cp_mask = nullptr;
+    int *d_excl_start = nullptr, *d_excl_list = nullptr;
+    int2 *d_excess = nullptr;
+    int *d_excess_sys = nullptr;
+    double *d_e_exc = nullptr, *d_vir_exc = nullptr;
+    int2 *d_bond = nullptr;
+    int *d_bond_sys = nullptr;
+    double2 *d_bond_kr = nullptr;
+    double *d_e_bond = nullptr;
+    int4 *d_angle = nullptr;
+    double2 *d_angle_kt = nullptr;
+    double *d_e_angle = nullptr;
+    int2 *d_spair = nullptr;
+    int *d_spair_sys = nullptr;
+    double *d_spair_d2 = nullptr;
+    int4 *d_strio = nullptr;
+    double *d_strio_d2 = nullptr;
+    int *d_grp_start = nullptr, *d_grp_atoms = nullptr, *d_grp_sys = nullptr;
+    float *d_grp_mass_inv = nullptr;
+    double *d_moment = nullptr;
+    float2 *d_lj = nullptr;
+    double *d_sys_acc = nullptr, *d_mcmd = nullptr, *d_energies = nullptr, *d_thermo = nullptr,
+           *d_sum_tmp = nullptr;
+    int *d_mask_plain = nullptr, *d_mask_thermo = nullptr, *d_active = nullptr, *d_any = nullptr;
+    // trace
+    double *d_trace = nullptr;
+    int trace_cap = 0;
+    // snapshot for capacity retries
+    double *d_snap = nullptr;
+    // host pinned
+    int *h_pinned = nullptr;
+    // stats
+    long long launches = 0;
+    cudaEvent_t ev_pair0 = nullptr, ev_pair1 = nullptr, ev_step0 = nullptr, ev_step1 = nullptr;
+    double pair_ms = 0.0, step_ms = 0.0;
+    bool timing = false;
+    std::vector<void *> allocs;
+};
+
+namespace {
+
+og_status fail(og_engine *e, og_status s, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (e) e->err = buf;
+    return s;
+}
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t _e = (call);                                                                   \
+        if (_e != cudaSuccess)                                                                     \
+            return fail(e, _e == cudaErrorMemoryAllocation ? OG_ERR_NOMEM : OG_ERR_CUDA, "%s: %s (%s:%d)", \
+                        #call, cudaGetErrorString(_e), __FILE__, __LINE__);                        \
+    } while (0)
+
+#define LAUNCH_CHECK()                                                                             \
+    do {                                                                                           \
+        e->launches++;                                                                             \
+        cudaError_t _e = cudaGetLastError();                                                       \
+        if (_e != cudaSuccess)                                                                     \
+            return fail(e, OG_ERR_CUDA, "kernel launch: %s (%s:%d)", cudaGetErrorString(_e), __FILE__, __LINE__); \
+    } while (0)
+
+template <class T>
+og_status dalloc(og_engine *e, T **p, size_t n) {
+    if (n == 0) n = 1;
+    void *q = nullptr;
+    cudaError_t r = cudaMalloc(&q, n * sizeof(T));
+    if (r != cudaSuccess) return fail(e, OG_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(r));
+    e->allocs.push_back(q);
+    *p = (T *)q;
+    return OG_OK;
+}
+
+void dfree(og_engine *e, void *p) {
+    if (!p) return;
+    for (size_t i = 0; i < e->allocs.size(); i++)
+        if (e->allocs[i] == p) {
+            e->allocs.erase(e->allocs.begin() + i);
+            break;
+        }
+    cudaFree(p);
+}
+
+template <class T>
+og_status upload(og_engine *e, T **p, const std::vector<T> &v) {
+    og_status s = dalloc(e, p, v.size());
+    if (s) return s;
+    if (!v.empty()) CK(cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, e->stream));
+    return OG_OK;
+}
+
+inline unsigned blocks(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// ---------------------------------------------------------- host geometry
+
+// PBC::set_pbc (PBC.cpp:19-41) + MiniCell geometry (MiniCell.cpp:221-290, 1279-1303).
+og_status setup_geometry(og_engine *e, HostSystem &h) {
+    SysDev &S = h.dev;
+    const og_system_desc &d = h.d;
+    float L[3] = {(float)d.pbc_val[0], (float)d.pbc_val[4], (float)d.pbc_val[8]};
+    for (int i = 0; i < 3; i++) {
+        if (!(L[i] > 0.0f)) return fail(e, OG_ERR_INVALID, "box length %d must be positive", i);
+        float Lh = (float)((double)L[i] * 0.5);
+        S.Lf[i] = L[i];
+        S.L_half_inv_f[i] = (float)(1.0 / (double)Lh);
+        S.lowerf[i] = (float)(d.pbc_val[9 + i] - (double)Lh);
+        S.upperf[i] = S.lowerf[i] + L[i];
+        S.L[i] = (double)L[i];
+        S.lower[i] = (double)S.lowerf[i];
+        S.upper[i] = (double)S.upperf[i];
+    }
+    const float cp = (float)d.nsgrid_cutoff;
+    const float cph = (float)((double)cp * 0.5);
+    S.cutoff_pair2 = cp * cp;
+    S.n_uni_z = (int)(L[2] / cph);
+    if (S.n_uni_z < 1) return fail(e, OG_ERR_INVALID, "box z length below half the pair-list cutoff");
+    S.L_z_uni = L[2] / (float)S.n_uni_z;
+    volatile float vol = L[0] * L[1];
+    vol = vol * L[2];
+    volatile float dens = (float)d.n_atoms / vol;
+    volatile float ratio = (float)8 / dens;
+    float w = powf(ratio, (float)(1.0 / 3.0));
+    if (w > cph) w = cph;
+    int n[2], nn[2];
+    for (int k = 0; k < 2; k++) {
+        n[k] = (int)floorf(L[k] / w);
+        if (n[k] < 1) return fail(e, OG_ERR_INVALID, "box too small for one column");
+        S.L_cell[k] = L[k] / (float)n[k];
+        nn[k] = (int)ceilf(cp / S.L_cell[k]);
+        if (nn[k] > n[k])
+            return fail(e, OG_ERR_INVALID,
+                        "box too small: neighbour reach %d exceeds %d columns (the reference indexes out of range)",
+                        nn[k], n[k]);
+    }
+    S.nx = n[0];
+    S.ny = n[1];
+    S.n_columns = n[0] * n[1];
+    S.n_nb[0] = nn[0];
+    S.n_nb[1] = nn[1];
+    S.n_nb_cols = (2 * nn[0] + 1) * (2 * nn[1] + 1);
+    // ZeroMultipoleSum::set_zms_params, alpha = 0 (float members)
+    float c = (float)d.cutoff;
+    float c2 = c * c, c3 = c2 * c;
+    S.fcoeff = (float)(1.0 / (double)c3);
+    S.bcoeff = (float)(0.5 * (double)S.fcoeff);
+    S.zcore = erfcf(c * 0.0f) / c + S.bcoeff * c2;
+    S.cutoff = (double)c;
+    S.cutoff2 = (float)((double)d.cutoff * (double)d.cutoff);
+    return OG_OK;
+}
+
+// ZeroMultipoleSum::cal_self_energy (ZeroMultipoleSum.cpp:43-106) with its float running sum.
+double self_energy(const HostSystem &h) {
+    const int n = h.d.n_atoms;
+    std::vector<double> dw(n, 0.0);
+    for (int k = 0; k < h.n_excess; k++) {
+        int i = h.excess[2 * k], j = h.excess[2 * k + 1];
+        dw[i] += (double)(float)h.charge[j];
+        dw[j] += (double)(float)h.charge[i];
+    }
+    float mon = 0.0f;
+    const double zm = (double)h.dev.zcore;
+    for (int i = 0; i < n; i++) {
+        double q = (double)(float)h.charge[i];
+        double es = ((double)(-0.0f * (float)q * (float)q) - zm * q * (q + dw[i])) * 0.5 * OG_CHARGE_COEFF;
+        mon = (float)((double)mon + es);
+    }
+    return (double)mon;
+}
+
+// MmSystem::set_nb15off + set_excess_pairs (MmSystem.cpp:478-525, 700-736): rows in insertion
+// order, then pairs i < j walking the rows.
+og_status build_exclusions(og_engine *e, HostSystem &h, std::vector<std::vector<int>> &rows) {
+    const int n = h.d.n_atoms;
+    rows.assign(n, {});
+    for (int k = 0; k < h.d.n_excl; k++) {
+        int a = h.excl[2 * k], b = h.excl[2 * k + 1];
+        if (a < 0 || b < 0 || a >= n || b >= n || a == b) return fail(e, OG_ERR_INVALID, "bad exclusion pair %d", k);
+        bool ab = false, ba = false;
+        for (int x : rows[a]) ab |= x == b;
+        for (int x : rows[b]) ba |= x == a;
+        if (!ab) rows[a].push_back(b);
+        if (!ba) rows[b].push_back(a);
+    }
+    h.excess.clear();
+    for (int i = 0; i < n; i++)
+        for (int j : rows[i])
+            if (i < j) {
+                h.excess.push_back(i);
+                h.excess.push_back(j);
+            }
+    h.n_excess = (int)h.excess.size() / 2;
+    return OG_OK;
+}
+
+// ---------------------------------------------------------- device scan
+
+og_status scan_exclusive(og_engine *e, const int *in, int *out, long long n, int level) {
+    const long long nb = (n + 2047) / 2048;
+    if (level >= (int)e->d_scan_tmp.size() / 2) return fail(e, OG_ERR_CAPACITY, "scan depth");
+    int *sums = e->d_scan_tmp[2 * level], *sums_out = e->d_scan_tmp[2 * level + 1];
+    k_scan_block<<<(unsigned)nb, 1024, 0, e->stream>>>(in, out, n, nb > 1 ? sums : nullptr);
+    LAUNCH_CHECK();
+    if (nb > 1) {
+        og_status s = scan_exclusive(e, sums, sums_out, nb, level + 1);
+        if (s) return s;
+        k_scan_add<<<blocks(n, 256), 256, 0, e->stream>>>(out, n, sums_out);
+        LAUNCH_CHECK();
+    }
+    return OG_OK;
+}
+
+// ---------------------------------------------------------- list build
+
+og_status build_list(og_engine *e) {
+    cudaStream_t st = e->stream;
+    CK(cudaMemsetAsync(e->d_col_count, 0, sizeof(int) * e->n_cols, st));
+    CK(cudaMemsetAsync(e->d_col_fill, 0, sizeof(int) * e->n_cols, st));
+    k_assign_columns<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->d_sys, e->d_atom_sys, e->d_crd, e->n_atoms,
+                                                               e->d_atom_col, e->d_atom_key, e->d_col_count,
+                                                               e->d_counters);
+    LAUNCH_CHECK();
+    k_scan_columns<<<1, 1024, 0, st>>>(e->d_col_count, e->n_cols, e->d_col_atom_start, e->d_col_cell_start,
+                                       e->d_col_head_cell, e->d_counters, e->d_sys_col_base, e->n_sys,
+                                       e->d_sys_cell_base);
+    LAUNCH_CHECK();
+    k_scatter_columns<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->d_atom_col, e->d_atom_key, e->n_atoms,
+                                                                e->d_col_atom_start, e->d_col_fill, e->d_col_keys);
+    LAUNCH_CHECK();
+    k_sort_columns<<<e->n_cols, 512, 0, st>>>(e->d_col_count, e->d_col_atom_start, e->d_col_cell_start, e->d_col_sys,
+                                              e->d_col_keys, e->d_sys, e->d_crd, e->d_slot_atom, e->d_slot_crd,
+                                              e->d_atom_slot, e->d_cell_col, e->d_cell_sys, e->d_counters);
+    LAUNCH_CHECK();
+    k_fill_int<<<blocks(e->n_uni, 256), 256, 0, st>>>(e->d_uni_lo, e->n_uni, 0x7fffffff);
+    LAUNCH_CHECK();
+    k_fill_int<<<blocks(e->n_uni, 256), 256, 0, st>>>(e->d_uni_hi, e->n_uni, -1);
+    LAUNCH_CHECK();
+    k_cell_info<<<blocks(e->cells_cap, 256), 256, 0, st>>>(e->d_counters, e->cells_cap, e->d_cell_col, e->d_cell_sys,
+                                                            e->d_col_cell_start, e->d_sys, e->d_slot_crd,
+                                                            e->d_slot_atom, e->d_cell_origin, e->d_cell_zr,
+                                                            e->d_cell_uni, e->d_cell_valid, e->d_uni_lo, e->d_uni_hi);
+    LAUNCH_CHECK();
+    k_slot_refresh<<<blocks(e->slots_cap, 256), 256, 0, st>>>(e->d_counters, e->slots_cap, e->d_slot_atom,
+                                                               e->d_slot_crd, e->d_cell_origin, e->d_charge_f,
+                                                               e->d_atom_type, e->d_xq, e->d_slot_type);
+    LAUNCH_CHECK();
+    const long long n_items = (long long)e->cells_cap * e->nnc;
+    k_count_pairs<<<blocks(n_items, 256), 256, 0, st>>>(e->d_counters, e->cells_cap, e->nnc, e->d_cell_sys,
+                                                         e->d_sys_cell_base, e->d_sys, e->d_cell_col,
+                                                         e->d_col_cell_start, e->d_col_head_cell, e->d_cell_zr,
+                                                         e->d_cell_uni, e->d_uni_lo, e->d_uni_hi, e->d_cell_valid,
+                                                         e->d_count);
+    LAUNCH_CHECK();
+    og_status s = scan_exclusive(e, e->d_count, e->d_offset, n_items + 1, 0);
+    if (s) return s;
+    k_pair_heads<<<blocks(e->cells_cap + 1, 256), 256, 0, st>>>(e->d_counters, e->cells_cap, e->nnc, e->d_offset,
+                                                                 e->d_cp_head);
+    LAUNCH_CHECK();
+    k_fill_pairs<<<blocks(n_items, 256), 256, 0, st>>>(
+        e->d_counters, e->cells_cap, e->nnc, e->pair_cap, e->d_cell_sys, e->d_sys_cell_base, e->d_sys, e->d_cell_col,
+        e->d_col_cell_start, e->d_col_head_cell, e->d_cell_zr, e->d_cell_uni, e->d_uni_lo, e->d_uni_hi,
+        e->d_cell_valid, e->d_slot_atom, e->d_atom_slot, e->d_excl_start, e->d_excl_list, e->d_offset, e->d_cp_c2img,
+        e->d_cp_mask);
+    LAUNCH_CHECK();
+    return OG_OK;
+}
+
+// ---------------------------------------------------------- forces
+
+og_status compute_forces(og_engine *e, bool vir) {
+    cudaStream_t st = e->stream;
+    const unsigned pair_blocks = blocks((long long)e->cells_cap * 32, 256);
+    if (e->timing) CK(cudaEventRecord(e->ev_pair0, st));
+    if (vir)
+        k_pair_ljzd<true><<<pair_blocks, 256, 0, st>>>(e->d_counters, e->d_cell_sys, e->d_sys, e->d_cell_origin,
+                                                       e->d_xq, e->d_slot_type, e->d_cp_head, e->d_cp_c2img,
+                                                       e->d_cp_mask, e->d_lj, e->d_frc, e->d_cell_acc, e->pair_cap);
+    else
+        k_pair_ljzd<false><<<pair_blocks, 256, 0, st>>>(e->d_counters, e->d_cell_sys, e->d_sys, e->d_cell_origin,
+                                                        e->d_xq, e->d_slot_type, e->d_cp_head, e->d_cp_c2img,
+                                                        e->d_cp_mask, e->d_lj, e->d_frc, e->d_cell_acc, e->pair_cap);
+    LAUNCH_CHECK();
+    if (e->timing) CK(cudaEventRecord(e->ev_pair1, st));
+    if (vir) {
+        if (!e->d_vir_atom) {
+            og_status s = dalloc(e, &e->d_vir_atom, 9 * (size_t)e->n_atoms);
+            if (s) return s;
+            s = dalloc(e, &e->d_vir_exc, 9 * (size_t)(e->n_excess + 1));
+            if (s) return s;
+        }
+        k_atom_virial<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_slot, e->d_frc, e->d_xq,
+                                                                e->d_cell_origin, e->d_vir_atom);
+        LAUNCH_CHECK();
+    }
+    if (e->n_excess) {
+        k_excess<<<blocks(e->n_excess, 256), 256, 0, st>>>(e->n_excess, e->d_excess, e->d_excess_sys, e->d_sys,
+                                                            e->d_crd, e->d_charge, e->d_atom_slot, e->d_frc,
+                                                            e->d_e_exc, vir ? e->d_vir_exc : nullptr);
+        LAUNCH_CHECK();
+    }
+    if (e->n_bonds) {
+        k_bonds<<<blocks(e->n_bonds, 256), 256, 0, st>>>(e->n_bonds, e->d_bond, e->d_bond_kr, e->d_bond_sys, e->d_sys,
+                                                          e->d_crd, e->d_atom_slot, e->d_frc, e->d_e_bond);
+        LAUNCH_CHECK();
+    }
+    if (e->n_angles) {
+        k_angles<<<blocks(e->n_angles, 256), 256, 0, st>>>(e->n_angles, e->d_angle, e->d_angle_kt, e->d_sys,
+                                                            e->d_crd, e->d_atom_slot, e->d_frc, e->d_e_angle);
+        LAUNCH_CHECK();
+    }
+    k_collect<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_slot, e->d_frc, e->d_work);
+    LAUNCH_CHECK();
+    k_reduce_potential<<<e->n_sys, 256, 0, st>>>(e->d_sys, e->d_sys_cell_base, e->d_cell_acc, e->d_e_exc,
+                                                  e->d_e_bond, e->d_e_angle, e->d_sys_acc, e->d_mcmd);
+    LAUNCH_CHECK();
+    if (vir) {
+        k_reduce_virial<<<e->n_sys, 256, 0, st>>>(e->d_sys, e->d_sys_cell_base, e->d_cell_acc, e->d_vir_atom,
+                                                   e->d_vir_exc, e->d_sys_acc);
+        LAUNCH_CHECK();
+    }
+    return OG_OK;
+}
+
+og_status com_cancel(og_engine *e, double *v, const int *active) {
+    if (!e->any_groups) return OG_OK;
+    k_group_moment<<<e->n_groups, 256, 0, e->stream>>>(e->d_grp_start, e->d_grp_atoms, e->d_grp_mass_inv, e->d_mass,
+                                                        v, e->d_grp_sys, active, e->d_moment);
+    LAUNCH_CHECK();
+    k_com_apply<<<blocks(e->n_atoms, 256), 256, 0, e->stream>>>(e->n_atoms, e->d_atom_group, e->d_moment,
+                                                                 e->d_atom_sys, active, v);
+    LAUNCH_CHECK();
+    return OG_OK;
+}
+
+og_status shake(og_engine *e, const int *active) {
+    cudaStream_t st = e->stream;
+    if (e->n_spair) {
+        k_shake_pair<<<blocks(e->n_spair, 128), 128, 0, st>>>(e->n_spair, e->d_spair, e->d_spair_d2, e->d_spair_sys,
+                                                               e->d_sys, active, e->d_mass_inv, e->d_crd,
+                                                               e->d_crd_prev);
+        LAUNCH_CHECK();
+    }
+    if (e->n_strio) {
+        k_shake_trio<<<blocks(e->n_strio, 128), 128, 0, st>>>(e->n_strio, e->d_strio, e->d_strio_d2, e->d_sys,
+                                                               active, e->d_mass_inv, e->d_crd, e->d_crd_prev,
+                                                               e->shake_max_loops, e->shake_tol, e->d_counters);
+        LAUNCH_CHECK();
+    }
+    return OG_OK;
+}
+
+// ThermostatScaling::apply_thermostat_with_shake (Thermostat.cpp:86-170) for every system that
+// has constraints and the scaling thermostat; the loop ends when all have converged.
+og_status thermostat_with_shake(og_engine *e) {
+    cudaStream_t st = e->stream;
+    CK(cudaMemcpyAsync(e->d_active, e->d_mask_thermo, sizeof(int) * e->n_sys, cudaMemcpyDeviceToDevice, st));
+    k_copy_double<<<blocks(3LL * e->n_atoms, 256), 256, 0, st>>>(e->d_buf_crd, e->d_crd, 3LL * e->n_atoms);
+    LAUNCH_CHECK();
+    for (int it = 0; it < e->thermo_max_loops; it++) {
+        og_status s = shake(e, e->d_active);
+        if (s) return s;
+        k_ke_mid<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_mass, e->d_vel, e->d_vel_next, e->d_ke);
+        LAUNCH_CHECK();
+        k_reduce_atoms<<<e->n_sys, 256, 0, st>>>(e->d_sys, e->d_ke, e->d_sum_tmp, 1, 0);
+        LAUNCH_CHECK();
+        CK(cudaMemsetAsync(e->d_any, 0, sizeof(int), st));
+        k_thermo_check<<<blocks(e->n_sys, 128), 128, 0, st>>>(e->n_sys, e->d_sys, e->d_sum_tmp, e->d_thermo, e->d_step,
+                                                               it, e->thermo_max_loops, e->thermo_tol, e->d_active,
+                                                               e->d_any, e->d_counters);
+        LAUNCH_CHECK();
+        CK(cudaMemcpyAsync(e->h_pinned, e->d_any, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (e->h_pinned[0] == 0) break;
+        k_thermo_half<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys, e->d_active,
+                                                                e->d_work, e->d_mass, e->d_mass_inv, e->d_crd,
+                                                                e->d_buf_crd, e->d_vel, e->d_vel_next, e->d_ke);
+        LAUNCH_CHECK();
+        k_reduce_atoms<<<e->n_sys, 256, 0, st>>>(e->d_sys, e->d_ke, e->d_sum_tmp, 1, 0);
+        LAUNCH_CHECK();
+        k_thermo_rescale<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys, e->d_active,
+                                                                   e->d_sum_tmp, e->d_thermo, e->d_step, e->d_work,
+                                                                   e->d_mass_inv, e->d_crd, e->d_buf_crd, e->d_vel,
+                                                                   e->d_vel_next);
+        LAUNCH_CHECK();
+        s = com_cancel(e, e->d_vel_next, e->d_active);
+        if (s) return s;
+        k_thermo_crd<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys, e->d_active,
+                                                               e->d_crd, e->d_crd_prev, e->d_vel_next);
+        LAUNCH_CHECK();
+    }
+    return OG_OK;
+}
+
+og_status run_step(og_engine *e) {
+    cudaStream_t st = e->stream;
+    og_status s;
+    if (e->host_step % e->intvl == 0) {
+        s = build_list(e);
+        if (s) return s;
+    }
+    s = compute_forces(e, false);
+    if (s) return s;
+    k_update_velocities<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys, e->d_mcmd,
+                                                                  e->d_work, e->d_mass_inv, e->d_vel,
+                                                                  e->d_vel_next);
+    LAUNCH_CHECK();
+    s = com_cancel(e, e->d_vel_next, nullptr);
+    if (s) return s;
+    if (e->any_thermo_free) {
+        k_thermo_scaling_ke<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys, e->d_work,
+                                                                      e->d_mass, e->d_mass_inv, e->d_vel, e->d_ke);
+        LAUNCH_CHECK();
+        k_reduce_atoms<<<e->n_sys, 256, 0, st>>>(e->d_sys, e->d_ke, e->d_sum_tmp, 1, 0);
+        LAUNCH_CHECK();
+        k_thermo_scaling_apply<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys,
+                                                                         e->d_sum_tmp, e->d_thermo, e->d_step,
+                                                                         e->d_work, e->d_mass_inv, e->d_vel,
+                                                                         e->d_vel_next);
+        LAUNCH_CHECK();
+    }
+    k_update_coordinates<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys, e->d_crd,
+                                                                   e->d_crd_prev, e->d_vel_next);
+    LAUNCH_CHECK();
+    if (e->any_plain_cons) {
+        s = shake(e, e->d_mask_plain);
+        if (s) return s;
+    }
+    if (e->any_thermo_cons) {
+        s = thermostat_with_shake(e);
+        if (s) return s;
+    }
+    k_finish<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys, 1, e->d_crd,
+                                                       e->d_crd_prev, e->d_vel, e->d_vel_next, e->d_atom_slot,
+                                                       e->d_slot_crd, e->d_cell_origin, e->d_xq, e->d_mass, e->d_ke);
+    LAUNCH_CHECK();
+    k_reduce_atoms<<<e->n_sys, 256, 0, st>>>(e->d_sys, e->d_ke, e->d_sys_acc, OG_ACC_SIZE, OG_ACC_KIN);
+    LAUNCH_CHECK();
+    k_energies<<<blocks(e->n_sys, 128), 128, 0, st>>>(e->n_sys, e->d_sys, e->d_sys_acc, e->d_mcmd, e->d_energies,
+                                                       e->d_trace, e->trace_cap, e->d_trace_count);
+    LAUNCH_CHECK();
+    k_trace_advance<<<1, 32, 0, st>>>(e->d_trace_count, e->d_step);
+    LAUNCH_CHECK();
+    e->host_step++;
+    return OG_OK;
+}
+
+og_status read_counters(og_engine *e, int *out) {
+    CK(cudaMemcpyAsync(e->h_pinned, e->d_counters, sizeof(int) * OG_CNT_SIZE, cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    memcpy(out, e->h_pinned, sizeof(int) * OG_CNT_SIZE);
+    return OG_OK;
+}
+
+og_status check_flags(og_engine *e) {
+    int c[OG_CNT_SIZE];
+    og_status s = read_counters(e, c);
+    if (s) return s;
+    int f = c[OG_CNT_FLAGS];
+    if (f & OG_FLAG_BAD_COORD) return fail(e, OG_ERR_INVALID, "non-finite or far out-of-box coordinate");
+    if (f & OG_FLAG_COLUMN_CAPACITY)
+        return fail(e, OG_ERR_CAPACITY, "a MiniCell column holds more than %d atoms", OG_MAX_COLUMN_ATOMS);
+    if (f & OG_FLAG_PAIR_CAPACITY)
+        return fail(e, OG_ERR_CAPACITY, "cell-pair list needs %d entries, capacity %lld", c[OG_CNT_N_PAIRS], e->pair_cap);
+    return OG_OK;
+}
+
+og_status grow_pairs(og_engine *e, long long need) {
+    long long cap = need + need / 2 + 4096;
+    dfree(e, e->d_cp_c2img);
+    dfree(e, e->d_cp_mask);
+    e->d_cp_c2img = nullptr;
+    e->d_cp_mask = nullptr;
+    og_status s = dalloc(e, &e->d_cp_c2img, (size_t)cap);
+    if (s) return s;
+    s = dalloc(e, &e->d_cp_mask, (size_t)cap);
+    if (s) return s;
+    e->pair_cap = cap;
+    return OG_OK;
+}
+
+og_status clear_flags(og_engine *e) {
+    CK(cudaMemsetAsync(e->d_counters + OG_CNT_FLAGS, 0, sizeof(int), e->stream));
+    return OG_OK;
+}
+
+// Builds the list and grows the pair buffer until it fits (synchronous; used at setup and
+// after a capacity miss).
+og_status build_list_checked(og_engine *e) {
+    for (int attempt = 0; attempt < 4; attempt++) {
+        og_status s = clear_flags(e);
+        if (s) return s;
+        s = build_list(e);
+        if (s) return s;
+        int c[OG_CNT_SIZE];
+        s = read_counters(e, c);
+        if (s) return s;
+        if (c[OG_CNT_FLAGS] & OG_FLAG_PAIR_CAPACITY) {
+            s = grow_pairs(e, c[OG_CNT_N_PAIRS]);
+            if (s) return s;
+            continue;
+        }
+        return check_flags(e);
+    }
+    return fail(e, OG_ERR_CAPACITY, "cell-pair list did not fit after growing");
+}
+
+}  // namespace
+
+// ======================================================================= C ABI
+
+extern "C" {
+
+og_status og_create(int device, og_engine **out) {
+    if (!out) return OG_ERR_INVALID;
+    *out = nullptr;
+    og_engine *e = new og_engine();
+    e->device = device;
+    cudaError_t r = cudaSetDevice(device);
+    if (r != cudaSuccess) {
+        delete e;
+        return OG_ERR_CUDA;
+    }
+    if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&e->ev_pair0) != cudaSuccess || cudaEventCreate(&e->ev_pair1) != cudaSuccess ||
+        cudaEventCreate(&e->ev_step0) != cudaSuccess || cudaEventCreate(&e->ev_step1) != cudaSuccess ||
+        cudaMallocHost((void **)&e->h_pinned, 64 * sizeof(int)) != cudaSuccess) {
+        delete e;
+        return OG_ERR_CUDA;
+    }
+    *out = e;
+    return OG_OK;
+}
+
+og_status og_destroy(og_engine *e) {
+    if (!e) return OG_OK;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    for (void *p : e->allocs) cudaFree(p);
+    e->allocs.clear();
+    if (e->h_pinned) cudaFreeHost(e->h_pinned);
+    if (e->ev_pair0) cudaEventDestroy(e->ev_pair0);
+    if (e->ev_pair1) cudaEventDestroy(e->ev_pair1);
+    if (e->ev_step0) cudaEventDestroy(e->ev_step0);
+    if (e->ev_step1) cudaEventDestroy(e->ev_step1);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+    return OG_OK;
+}
+
+const char *og_last_error(const og_engine *e) { return e ? e->err.c_str() : "null engine"; }
+
+og_status og_add_system(og_engine *e, const og_system_desc *d, int32_t *sys_id) {
+    if (!e || !d) return OG_ERR_INVALID;
+    if (e->finalized) return fail(e, OG_ERR_STATE, "og_add_system after og_finalize");
+    const int n = d->n_atoms;
+    if (n <= 0 || !d->crd || !d->vel || !d->charge || !d->mass || !d->atom_type || d->n_lj_types <= 0 || !d->lj6 ||
+        !d->lj12)
+        return fail(e, OG_ERR_INVALID, "system needs atoms, coordinates, velocities, charges, masses and LJ tables");
+    if (d->cutoff <= 0 || d->nsgrid_cutoff < d->cutoff || d->time_step <= 0 || d->nsgrid_update_intvl <= 0)
+        return fail(e, OG_ERR_INVALID, "need 0 < cutoff <= nsgrid_cutoff, time_step > 0, nsgrid_update_intvl > 0");
+    if (!e->sys.empty() && d->nsgrid_update_intvl != e->intvl)
+        return fail(e, OG_ERR_INVALID, "all systems of one engine share nsgrid_update_intvl");
+    if (d->mcmd_order > 7) return fail(e, OG_ERR_INVALID, "McMD polynomial order above 7");
+    e->sys.emplace_back();
+    HostSystem &h = e->sys.back();
+    h.d = *d;
+    auto cp = [](auto &vec, const auto *src, size_t cnt) {
+        vec.assign(src ? src : nullptr, src ? src + cnt : nullptr);
+    };
+    cp(h.crd, d->crd, 3 * (size_t)n);
+    cp(h.vel, d->vel, 3 * (size_t)n);
+    cp(h.charge, d->charge, n);
+    cp(h.mass, d->mass, n);
+    cp(h.type, d->atom_type, n);
+    cp(h.lj6, d->lj6, (size_t)d->n_lj_types * d->n_lj_types);
+    cp(h.lj12, d->lj12, (size_t)d->n_lj_types * d->n_lj_types);
+    cp(h.excl, d->excl, 2 * (size_t)d->n_excl);
+    cp(h.sp, d->shake_pair, 2 * (size_t)d->n_shake_pair);
+    cp(h.spd, d->shake_pair_dist, d->n_shake_pair);
+    cp(h.st, d->shake_trio, 3 * (size_t)d->n_shake_trio);
+    cp(h.std_, d->shake_trio_dist, 3 * (size_t)d->n_shake_trio);
+    cp(h.bond, d->bond, 2 * (size_t)d->n_bonds);
+    cp(h.bk, d->bond_k, d->n_bonds);
+    cp(h.br0, d->bond_r0, d->n_bonds);
+    cp(h.angle, d->angle, 3 * (size_t)d->n_angles);
+    cp(h.ak, d->angle_k, d->n_angles);
+    cp(h.at0, d->angle_t0, d->n_angles);
+    cp(h.gstart, d->com_group_start, d->n_com_groups > 0 ? d->n_com_groups + 1 : 0);
+    if (d->n_com_groups > 0) cp(h.gatoms, d->com_group_atoms, d->com_group_start[d->n_com_groups]);
+    if (d->mcmd_order >= 0) cp(h.mcoef, d->mcmd_coef, d->mcmd_order + 1);
+    for (int i = 0; i < n; i++)
+        if (h.type[i] < 0 || h.type[i] >= d->n_lj_types || !(h.mass[i] > 0)) {
+            e->sys.pop_back();
+            return fail(e, OG_ERR_INVALID, "atom %d: bad type or mass", i);
+        }
+    og_status s = setup_geometry(e, h);
+    if (s) {
+        e->sys.pop_back();
+        return s;
+    }
+    // MmSystem::revise_crd_inbox (MmSystem.cpp:808-816): wrap into [lower, upper) with the
+    // float box bounds
+    for (int i = 0; i < n; i++)
+        for (int q = 0; q < 3; q++) {
+            double &x = h.crd[3 * i + q];
+            const double lo = (double)h.dev.lowerf[q], up = (double)h.dev.upperf[q], L = (double)h.dev.Lf[q];
+            if (!std::isfinite(x) || std::fabs(x - lo) > 1e4 * L) {
+                e->sys.pop_back();
+                return fail(e, OG_ERR_INVALID, "atom %d: coordinate not finite or far outside the box", i);
+            }
+            while (x < lo) x += L;
+            while (x >= up) x -= L;
+        }
+    std::vector<std::vector<int>> rows;
+    s = build_exclusions(e, h, rows);
+    if (s) {
+        e->sys.pop_back();
+        return s;
+    }
+    e->intvl = d->nsgrid_update_intvl;
+    if (sys_id) *sys_id = (int32_t)e->sys.size() - 1;
+    return OG_OK;
+}
+
+og_status og_finalize(og_engine *e) {
+    if (!e) return OG_ERR_INVALID;
+    if (e->finalized) return fail(e, OG_ERR_STATE, "already finalized");
+    if (e->sys.empty()) return fail(e, OG_ERR_STATE, "no systems");
+    CK(cudaSetDevice(e->device));
+    og_status s;
+    const int S = (int)e->sys.size();
+    e->n_sys = S;
+    // ---- global layout
+    std::vector<SysDev> sd(S);
+    std::vector<int> atom_sys, col_sys, sys_col_base(S + 1), atom_type, atom_group, excl_start(1, 0), excl_list;
+    std::vector<double> crd, vel, charge;
+    std::vector<float> charge_f, mass, mass_inv;
+    std::vector<float2> lj;
+    std::vector<int2> excess, bondv, spair;
+    std::vector<int> excess_sys, bond_sys, spair_sys, grp_start(1, 0), grp_atoms, grp_sys;
+    std::vector<double2> bond_kr, angle_kt;
+    std::vector<int4> anglev, strio;
+    std::vector<double> spair_d2, strio_d2, thermo;
+    std::vector<float> grp_mass_inv;
+    std::vector<int> mask_plain(S), mask_thermo(S);
+    int atom_base = 0, col_base = 0, uni_base = 0, lj_base = 0, cells_cap = 0, nnc = 1;
+    for (int k = 0; k < S; k++) {
+        HostSystem &h = e->sys[k];
+        SysDev &D = h.dev;
+        const og_system_desc &d = h.d;
+        const int n = d.n_atoms;
+        D.atom_base = atom_base;
+        D.n_atoms = n;
+        D.col_base = col_base;
+        D.uni_base = uni_base;
+        D.lj_base = lj_base;
+        D.n_types = d.n_lj_types;
+        D.dt = d.time_step;
+        D.thermostat = d.thermostat;
+        D.has_constraints = (d.n_shake_pair + d.n_shake_trio) > 0;
+        h.d_free = 3 * n - 3 - (d.n_shake_pair + 3 * d.n_shake_trio);
+        if (h.d_free <= 0) return fail(e, OG_ERR_INVALID, "system %d has no degrees of freedom", k);
+        D.temperature_coeff_thermo =
+            (2.0 * OG_JOULE_CAL * 1e+3) / (OG_GAS_CONST * (double)h.d_free) * OG_KINETIC_COEFF;
+        D.temperature_coeff_dyn = 1.0 / (OG_GAS_CONST * (double)h.d_free) * OG_JOULE_CAL * 1e3 * 2.0;
+        double tau = d.berendsen_tau;
+        if (d.time_step < tau) tau = d.time_step;
+        D.tau_inv = 1.0 / tau;
+        D.mcmd_order = d.mcmd_order;
+        D.mcmd_lo = d.mcmd_lambda_low;
+        D.mcmd_hi = d.mcmd_lambda_high;
+        D.mcmd_k = (OG_GAS_CONST / OG_JOULE_CAL) * 1e-3 * d.mcmd_temperature;
+        for (int i = 0; i < 8; i++) D.mcmd_coef[i] = (d.mcmd_order >= 0 && i <= d.mcmd_order) ? h.mcoef[i] : 0.0;
+        D.self_energy = self_energy(h);
+        D.excess_base = (int)excess.size();
+        D.n_excess = h.n_excess;
+        D.bond_base = (int)bondv.size();
+        D.n_bonds = d.n_bonds;
+        D.angle_base = (int)anglev.size();
+        D.n_angles = d.n_angles;
+        D.trio_base = (int)strio.size();
+        D.n_trio = d.n_shake_trio;
+        D.pair_base = (int)spair.size();
+        D.n_pair = d.n_shake_pair;
+        thermo.push_back(d.temperature);
+        thermo.push_back(d.temperature_init < 0 ? d.temperature : d.temperature_init);
+        thermo.push_back((double)d.heating_steps);
+        thermo.push_back(0.0);
+        mask_plain[k] = D.has_constraints && d.thermostat != OG_THERMOSTAT_SCALING;
+        mask_thermo[k] = D.has_constraints && d.thermostat == OG_THERMOSTAT_SCALING;
+        e->any_plain_cons |= mask_plain[k] != 0;
+        e->any_thermo_cons |= mask_thermo[k] != 0;
+        e->any_thermo_free |= (!D.has_constraints && d.thermostat == OG_THERMOSTAT_SCALING);
+        if (d.n_shake_trio || d.n_shake_pair) {
+            e->shake_max_loops = d.const_max_loops > 0 ? d.const_max_loops : 1000;
+            e->shake_tol = d.const_tolerance > 0 ? d.const_tolerance : 1e-7;
+        }
+        if (d.thermostat == OG_THERMOSTAT_SCALING) {
+            e->thermo_max_loops = d.thermo_const_max_loops > 0 ? d.thermo_const_max_loops : 100;
+            e->thermo_tol = d.thermo_const_tolerance > 0 ? d.thermo_const_tolerance : 1e-5;
+        }
+        for (int i = 0; i < n; i++) {
+            atom_sys.push_back(k);
+            for (int q = 0; q < 3; q++) {
+                crd.push_back(h.crd[3 * i + q]);
+                vel.push_back(h.vel[3 * i + q]);
+            }
+            charge.push_back(h.charge[i]);
+            charge_f.push_back((float)h.charge[i]);
+            mass.push_back((float)h.mass[i]);
+            mass_inv.push_back((float)(1.0 / (double)(float)h.mass[i]));
+            atom_type.push_back(h.type[i]);
+        }
+        // exclusion CSR (global ids)
+        std::vector<std::vector<int>> rows;
+        s = build_exclusions(e, h, rows);
+        if (s) return s;
+        for (int i = 0; i < n; i++) {
+            for (int x : rows[i]) excl_list.push_back(atom_base + x);
+            excl_start.push_back((int)excl_list.size());
+        }
+        for (int q = 0; q < h.n_excess; q++) {
+            excess.push_back(make_int2(atom_base + h.excess[2 * q], atom_base + h.excess[2 * q + 1]));
+            excess_sys.push_back(k);
+        }
+        for (int q = 0; q < d.n_bonds; q++) {
+            bondv.push_back(make_int2(atom_base + h.bond[2 * q], atom_base + h.bond[2 * q + 1]));
+            bond_sys.push_back(k);
+            bond_kr.push_back(make_double2(h.bk[q], h.br0[q]));
+        }
+        for (int q = 0; q < d.n_angles; q++) {
+            anglev.push_back(make_int4(atom_base + h.angle[3 * q], atom_base + h.angle[3 * q + 1],
+                                       atom_base + h.angle[3 * q + 2], k));
+            angle_kt.push_back(make_double2(h.ak[q], h.at0[q]));
+        }
+        for (int q = 0; q < d.n_shake_pair; q++) {
+            spair.push_back(make_int2(atom_base + h.sp[2 * q], atom_base + h.sp[2 * q + 1]));
+            spair_sys.push_back(k);
+            spair_d2.push_back(h.spd[q] * h.spd[q]);
+        }
+        for (int q = 0; q < d.n_shake_trio; q++) {
+            strio.push_back(make_int4(atom_base + h.st[3 * q], atom_base + h.st[3 * q + 1], atom_base + h.st[3 * q + 2], k));
+            for (int r = 0; r < 3; r++) strio_d2.push_back(h.std_[3 * q + r] * h.std_[3 * q + r]);
+        }
+        // COM groups: MmSystem::set_atom_group_info mass sums in float (MmSystem.cpp:568-584)
+        std::vector<int> grp_of(n, -1);
+        for (int g = 0; g < d.n_com_groups; g++) {
+            float msum = 0.0f;
+            for (int q = h.gstart[g]; q < h.gstart[g + 1]; q++) {
+                int a = h.gatoms[q];
+                if (a < 0 || a >= n) return fail(e, OG_ERR_INVALID, "COM group atom out of range");
+                if (grp_of[a] >= 0) return fail(e, OG_ERR_INVALID, "COM groups must be disjoint");
+                grp_of[a] = (int)grp_mass_inv.size();
+                grp_atoms.push_back(atom_base + a);
+                msum += (float)h.mass[a];
+            }
+            grp_start.push_back((int)grp_atoms.size());
+            grp_mass_inv.push_back((float)(1.0 / (double)msum));
+            grp_sys.push_back(k);
+        }
+        for (int i = 0; i < n; i++) atom_group.push_back(grp_of[i]);
+        for (int i = 0; i < d.n_lj_types; i++)
+            for (int j = 0; j < d.n_lj_types; j++)
+                lj.push_back(make_float2((float)h.lj6[i * d.n_lj_types + j], (float)h.lj12[i * d.n_lj_types + j]));
+        for (int c = 0; c < D.n_columns; c++) col_sys.push_back(k);
+        sys_col_base[k] = col_base;
+        cells_cap += n / OG_CELL + D.n_columns + 1;
+        nnc = std::max(nnc, D.n_nb_cols);
+        atom_base += n;
+        col_base += D.n_columns;
+        uni_base += D.n_columns * D.n_uni_z;
+        lj_base += d.n_lj_types * d.n_lj_types;
+        sd[k] = D;
+    }
+    sys_col_base[S] = col_base;
+    e->n_atoms = atom_base;
+    e->n_cols = col_base;
+    e->n_uni = uni_base;
+    e->cells_cap = cells_cap;
+    e->slots_cap = cells_cap * OG_CELL;
+    e->nnc = nnc;
+    e->n_excess = (int)excess.size();
+    e->n_bonds = (int)bondv.size();
+    e->n_angles = (int)anglev.size();
+    e->n_spair = (int)spair.size();
+    e->n_strio = (int)strio.size();
+    e->n_groups = (int)grp_mass_inv.size();
+    e->any_groups = e->n_groups > 0;
+    // ---- allocation + upload
+    std::vector<SysDev> sdv(sd);
+    if ((s = upload(e, &e->d_sys, sdv)) || (s = dalloc(e, &e->d_counters, OG_CNT_SIZE)) ||
+        (s = dalloc(e, &e->d_step, 1)) || (s = dalloc(e, &e->d_trace_count, 1)) || (s = upload(e, &e->d_crd, crd)) ||
+        (s = dalloc(e, &e->d_crd_prev, crd.size())) || (s = dalloc(e, &e->d_vel, crd.size())) ||
+        (s = upload(e, &e->d_vel_next, vel)) || (s = dalloc(e, &e->d_work, crd.size())) ||
+        (s = dalloc(e, &e->d_buf_crd, crd.size())) || (s = upload(e, &e->d_charge, charge)) ||
+        (s = dalloc(e, &e->d_ke, e->n_atoms)) || (s = upload(e, &e->d_charge_f, charge_f)) ||
+        (s = upload(e, &e->d_mass, mass)) || (s = upload(e, &e->d_mass_inv, mass_inv)) ||
+        (s = upload(e, &e->d_atom_type, atom_type)) || (s = upload(e, &e->d_atom_sys, atom_sys)) ||
+        (s = dalloc(e, &e->d_atom_col, e->n_atoms)) || (s = dalloc(e, &e->d_atom_slot, e->n_atoms)) ||
+        (s = upload(e, &e->d_atom_group, atom_group)) || (s = dalloc(e, &e->d_atom_key, e->n_atoms)) ||
+        (s = dalloc(e, &e->d_col_keys, e->n_atoms)) || (s = dalloc(e, &e->d_col_count, e->n_cols)) ||
+        (s = dalloc(e, &e->d_col_fill, e->n_cols)) || (s = dalloc(e, &e->d_col_atom_start, e->n_cols + 1)) ||
+        (s = dalloc(e, &e->d_col_cell_start, e->n_cols + 1)) || (s = dalloc(e, &e->d_col_head_cell, e->n_cols + 1)) ||
+        (s = upload(e, &e->d_col_sys, col_sys)) || (s = upload(e, &e->d_sys_col_base, sys_col_base)) ||
+        (s = dalloc(e, &e->d_sys_cell_base, S + 1)) || (s = dalloc(e, &e->d_cell_col, cells_cap)) ||
+        (s = dalloc(e, &e->d_cell_sys, cells_cap)) || (s = dalloc(e, &e->d_cp_head, cells_cap + 1)) ||
+        (s = dalloc(e, &e->d_cell_origin, 3 * (size_t)cells_cap)) ||
+        (s = dalloc(e, &e->d_cell_acc, 11 * (size_t)cells_cap)) || (s = dalloc(e, &e->d_cell_zr, cells_cap)) ||
+        (s = dalloc(e, &e->d_cell_uni, cells_cap)) || (s = dalloc(e, &e->d_cell_valid, cells_cap)) ||
+        (s = dalloc(e, &e->d_slot_atom, e->slots_cap)) || (s = dalloc(e, &e->d_slot_type, e->slots_cap)) ||
+        (s = dalloc(e, &e->d_slot_crd, 3 * (size_t)e->slots_cap)) || (s = dalloc(e, &e->d_xq, e->slots_cap)) ||
+        (s = dalloc(e, &e->d_frc, 3 * (size_t)e->slots_cap)) || (s = dalloc(e, &e->d_uni_lo, e->n_uni)) ||
+        (s = dalloc(e, &e->d_uni_hi, e->n_uni)) || (s = upload(e, &e->d_excl_start, excl_start)) ||
+        (s = upload(e, &e->d_excl_list, excl_list)) || (s = upload(e, &e->d_excess, excess)) ||
+        (s = upload(e, &e->d_excess_sys, excess_sys)) || (s = dalloc(e, &e->d_e_exc, excess.size())) ||
+        (s = upload(e, &e->d_bond, bondv)) || (s = upload(e, &e->d_bond_sys, bond_sys)) ||
+        (s = upload(e, &e->d_bond_kr, bond_kr)) || (s = dalloc(e, &e->d_e_bond, bondv.size())) ||
+        (s = upload(e, &e->d_angle, anglev)) || (s = upload(e, &e->d_angle_kt, angle_kt)) ||
+        (s = dalloc(e, &e->d_e_angle, anglev.size())) || (s = upload(e, &e->d_spair, spair)) ||
+        (s = upload(e, &e->d_spair_sys, spair_sys)) || (s = upload(e, &e->d_spair_d2, spair_d2)) ||
+        (s = upload(e, &e->d_strio, strio)) || (s = upload(e, &e->d_strio_d2, strio_d2)) ||
+        (s = upload(e, &e->d_grp_start, grp_start)) || (s = upload(e, &e->d_grp_atoms, grp_atoms)) ||
+        (s = upload(e, &e->d_grp_sys, grp_sys)) || (s = upload(e, &e->d_grp_mass_inv, grp_mass_inv)) ||
+        (s = dalloc(e, &e->d_moment, 3 * (size_t)(e->n_groups + 1))) || (s = upload(e, &e->d_lj, lj)) ||
+        (s = dalloc(e, &e->d_sys_acc, OG_ACC_SIZE * (size_t)S)) || (s = dalloc(e, &e->d_mcmd, S)) ||
+        (s = dalloc(e, &e->d_energies, 11 * (size_t)S)) || (s = upload(e, &e->d_thermo, thermo)) ||
+        (s = dalloc(e, &e->d_sum_tmp, S)) || (s = upload(e, &e->d_mask_plain, mask_plain)) ||
+        (s = upload(e, &e->d_mask_thermo, mask_thermo)) || (s = dalloc(e, &e->d_active, S)) ||
+        (s = dalloc(e, &e->d_any, 1)))
+        return s;
+    const long long n_items = (long long)cells_cap * nnc + 1;
+    if ((s = dalloc(e, &e->d_count, n_items)) || (s = dalloc(e, &e->d_offset, n_items))) return s;
+    for (long long len = n_items; len > 1;) {
+        long long nb = (len + 2047) / 2048;
+        int *a, *b;
+        if ((s = dalloc(e, &a, nb)) || (s = dalloc(e, &b, nb))) return s;
+        e->d_scan_tmp.push_back(a);
+        e->d_scan_tmp.push_back(b);
+        len = nb;
+    }
+    CK(cudaMemsetAsync(e->d_counters, 0, sizeof(int) * OG_CNT_SIZE, e->stream));
+    CK(cudaMemsetAsync(e->d_step, 0, sizeof(long long), e->stream));
+    CK(cudaMemsetAsync(e->d_trace_count, 0, sizeof(long long), e->stream));
+    CK(cudaMemsetAsync(e->d_count + (n_items - 1), 0, sizeof(int), e->stream));
+    CK(cudaMemsetAsync(e->d_frc, 0, sizeof(unsigned long long) * 3 * (size_t)e->slots_cap, e->stream));
+    CK(cudaMemsetAsync(e->d_cell_acc, 0, sizeof(double) * 11 * (size_t)cells_cap, e->stream));
+    CK(cudaMemsetAsync(e->d_sys_acc, 0, sizeof(double) * OG_ACC_SIZE * S, e->stream));
+    CK(cudaMemsetAsync(e->d_slot_crd, 0, sizeof(double) * 3 * (size_t)e->slots_cap, e->stream));
+    if ((s = grow_pairs(e, (long long)cells_cap * 180))) return s;
+    e->finalized = true;
+    e->host_step = 0;
+    // initial list + forces (DynamicsMode::initial_preprocess -> calc_energy_force)
+    if ((s = build_list_checked(e))) return s;
+    if ((s = compute_forces(e, false))) return s;
+    CK(cudaStreamSynchronize(e->stream));
+    return check_flags(e);
+}
+
+og_status og_step(og_engine *e, int32_t n_steps) {
+    if (!e) return OG_ERR_INVALID;
+    if (!e->finalized) return fail(e, OG_ERR_STATE, "og_step before og_finalize");
+    if (n_steps < 0) return fail(e, OG_ERR_INVALID, "negative step count");
+    CK(cudaSetDevice(e->device));
+    og_status s;
+    e->launches = 0;
+    if (e->timing) {
+        e->pair_ms = 0.0;
+    }
+    // snapshot for a capacity retry: crd, vel_next and the step counters
+    if (!e->d_snap && (s = dalloc(e, &e->d_snap, 6 * (size_t)e->n_atoms))) return s;
+    const long long step0 = e->host_step;
+    for (int attempt = 0; attempt < 3; attempt++) {
+        CK(cudaMemcpyAsync(e->d_snap, e->d_crd, sizeof(double) * 3 * e->n_atoms, cudaMemcpyDeviceToDevice, e->stream));
+        CK(cudaMemcpyAsync(e->d_snap + 3 * (size_t)e->n_atoms, e->d_vel_next, sizeof(double) * 3 * e->n_atoms,
+                           cudaMemcpyDeviceToDevice, e->stream));
+        if ((s = clear_flags(e))) return s;
+        if (e->timing) CK(cudaEventRecord(e->ev_step0, e->stream));
+        for (int i = 0; i < n_steps; i++) {
+            if ((s = run_step(e))) return s;
+            if (e->timing) {
+                CK(cudaEventSynchronize(e->ev_pair1));
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, e->ev_pair0, e->ev_pair1));
+                e->pair_ms += ms;
+            }
+        }
+        if (e->timing) {
+            CK(cudaEventRecord(e->ev_step1, e->stream));
+            CK(cudaEventSynchronize(e->ev_step1));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, e->ev_step0, e->ev_step1));
+            e->step_ms = ms;
+        }
+        int c[OG_CNT_SIZE];
+        if ((s = read_counters(e, c))) return s;
+        if (!(c[OG_CNT_FLAGS] & OG_FLAG_PAIR_CAPACITY)) return check_flags(e);
+        // capacity miss: grow, restore the state of the call's start and redo
+        if ((s = grow_pairs(e, (long long)c[OG_CNT_N_PAIRS] * 5 / 4))) return s;
+        CK(cudaMemcpyAsync(e->d_crd, e->d_snap, sizeof(double) * 3 * e->n_atoms, cudaMemcpyDeviceToDevice, e->stream));
+        CK(cudaMemcpyAsync(e->d_vel_next, e->d_snap + 3 * (size_t)e->n_atoms, sizeof(double) * 3 * e->n_atoms,
+                           cudaMemcpyDeviceToDevice, e->stream));
+        long long st = step0;
+        CK(cudaMemcpyAsync(e->d_step, &st, sizeof(long long), cudaMemcpyHostToDevice, e->stream));
+        CK(cudaStreamSynchronize(e->stream));
+        e->host_step = step0;
+        // the list must be rebuilt from the restored coordinates before the first step
+        if (step0 % e->intvl != 0) {
+            if ((s = build_list_checked(e))) return s;
+        }
+    }
+    return fail(e, OG_ERR_CAPACITY, "cell-pair list kept overflowing");
+}
+
+og_status og_compute_forces(og_engine *e) {
+    if (!e) return OG_ERR_INVALID;
+    if (!e->finalized) return fail(e, OG_ERR_STATE, "og_compute_forces before og_finalize");
+    CK(cudaSetDevice(e->device));
+    og_status s = build_list_checked(e);
+    if (s) return s;
+    // forces of the current list: the accumulators are clear after every collect
+    if ((s = compute_forces(e, true))) return s;
+    CK(cudaStreamSynchronize(e->stream));
+    return check_flags(e);
+}
+
+og_status og_set_state(og_engine *e, int32_t sys, const double *crd, const double *vel_next) {
+    if (!e || !e->finalized) return fail(e, OG_ERR_STATE, "og_set_state before og_finalize");
+    if (sys < 0 || sys >= e->n_sys) return fail(e, OG_ERR_INVALID, "bad system id");
+    const SysDev &D = e->sys[sys].dev;
+    if (crd)
+        CK(cudaMemcpyAsync(e->d_crd + 3 * (size_t)D.atom_base, crd, sizeof(double) * 3 * D.n_atoms,
+                           cudaMemcpyHostToDevice, e->stream));
+    if (vel_next)
+        CK(cudaMemcpyAsync(e->d_vel_next + 3 * (size_t)D.atom_base, vel_next, sizeof(double) * 3 * D.n_atoms,
+                           cudaMemcpyHostToDevice, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    // new coordinates invalidate the grid: rebuild at the next step
+    if (crd) e->host_step = ((e->host_step + e->intvl - 1) / e->intvl) * e->intvl;
+    if (crd && e->host_step % e->intvl != 0) return build_list_checked(e);
+    if (crd) {
+        long long st = e->host_step;
+        CK(cudaMemcpyAsync(e->d_step, &st, sizeof(long long), cudaMemcpyHostToDevice, e->stream));
+        CK(cudaStreamSynchronize(e->stream));
+    }
+    return OG_OK;
+}
+
+og_status og_get_state(og_engine *e, int32_t sys, double *crd, double *vel_next) {
+    if (!e || !e->finalized) return fail(e, OG_ERR_STATE, "og_get_state before og_finalize");
+    if (sys < 0 || sys >= e->n_sys) return fail(e, OG_ERR_INVALID, "bad system id");
+    const SysDev &D = e->sys[sys].dev;
+    if (crd)
+        CK(cudaMemcpyAsync(crd, e->d_crd + 3 * (size_t)D.atom_base, sizeof(double) * 3 * D.n_atoms,
+                           cudaMemcpyDeviceToHost, e->stream));
+    if (vel_next)
+        CK(cudaMemcpyAsync(vel_next, e->d_vel_next + 3 * (size_t)D.atom_base, sizeof(double) * 3 * D.n_atoms,
+                           cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    return OG_OK;
+}
+
+og_status og_get_forces(og_engine *e, int32_t sys, double *work, double *energies, double *virial) {
+    if (!e || !e->finalized) return fail(e, OG_ERR_STATE, "og_get_forces before og_finalize");
+    if (sys < 0 || sys >= e->n_sys) return fail(e, OG_ERR_INVALID, "bad system id");
+    const SysDev &D = e->sys[sys].dev;
+    if (work)
+        CK(cudaMemcpyAsync(work, e->d_work + 3 * (size_t)D.atom_base, sizeof(double) * 3 * D.n_atoms,
+                           cudaMemcpyDeviceToHost, e->stream));
+    double acc[OG_ACC_SIZE];
+    CK(cudaMemcpyAsync(acc, e->d_sys_acc + OG_ACC_SIZE * sys, sizeof(acc), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    if (energies) {
+        for (int q = 0; q < OG_N_ENERGY; q++) energies[q] = 0.0;
+        energies[OG_E_VDW] = acc[OG_ACC_VDW];
+        energies[OG_E_ELE] = acc[OG_ACC_ELE] + acc[OG_ACC_EXCESS] + D.self_energy;
+        energies[OG_E_BOND] = acc[OG_ACC_BOND];
+        energies[OG_E_ANGLE] = acc[OG_ACC_ANGLE];
+        energies[OG_E_POTENTIAL] = energies[0] + energies[1] + energies[2] + energies[3];
+        energies[OG_E_ELE_EXCESS] = acc[OG_ACC_EXCESS];
+        energies[OG_E_ELE_SELF] = D.self_energy;
+    }
+    if (virial)
+        for (int q = 0; q < 9; q++) virial[q] = acc[OG_ACC_VIR + q];
+    return OG_OK;
+}
+
+og_status og_get_energies(og_engine *e, int32_t sys, double *energies) {
+    if (!e || !e->finalized) return fail(e, OG_ERR_STATE, "og_get_energies before og_finalize");
+    if (sys < 0 || sys >= e->n_sys || !energies) return fail(e, OG_ERR_INVALID, "bad arguments");
+    CK(cudaMemcpyAsync(energies, e->d_energies + 11 * (size_t)sys, sizeof(double) * OG_N_ENERGY,
+                       cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    return OG_OK;
+}
+
+og_status og_get_grid_info(og_engine *e, int32_t sys, int32_t *n_cells, int32_t *n_columns, int32_t *n_pairs) {
+    if (!e || !e->finalized) return fail(e, OG_ERR_STATE, "og_get_grid_info before og_finalize");
+    if (sys < 0 || sys >= e->n_sys) return fail(e, OG_ERR_INVALID, "bad system id");
+    std::vector<int> base(e->n_sys + 1);
+    CK(cudaMemcpyAsync(base.data(), e->d_sys_cell_base, sizeof(int) * (e->n_sys + 1), cudaMemcpyDeviceToHost,
+                       e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    int h0 = 0, h1 = 0;
+    CK(cudaMemcpy(&h0, e->d_cp_head + base[sys], sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&h1, e->d_cp_head + base[sys + 1], sizeof(int), cudaMemcpyDeviceToHost));
+    if (n_cells) *n_cells = base[sys + 1] - base[sys];
+    if (n_columns) *n_columns = e->sys[sys].dev.n_columns;
+    if (n_pairs) *n_pairs = h1 - h0;
+    return OG_OK;
+}
+
+og_status og_get_grid(og_engine *e, int32_t sys, int32_t *slot_atomid, double *slot_crd, int32_t *col_head_cell) {
+    int32_t nc = 0, ncol = 0, np = 0;
+    og_status s = og_get_grid_info(e, sys, &nc, &ncol, &np);
+    if (s) return s;
+    std::vector<int> base(e->n_sys + 1);
+    CK(cudaMemcpy(base.data(), e->d_sys_cell_base, sizeof(int) * (e->n_sys + 1), cudaMemcpyDeviceToHost));
+    const SysDev &D = e->sys[sys].dev;
+    const size_t s0 = (size_t)base[sys] * OG_CELL, ns = (size_t)nc * OG_CELL;
+    if (slot_atomid) {
+        CK(cudaMemcpy(slot_atomid, e->d_slot_atom + s0, sizeof(int) * ns, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < ns; i++)
+            if (slot_atomid[i] >= 0) slot_atomid[i] -= D.atom_base;
+    }
+    if (slot_crd) CK(cudaMemcpy(slot_crd, e->d_slot_crd + 3 * s0, sizeof(double) * 3 * ns, cudaMemcpyDeviceToHost));
+    if (col_head_cell) {
+        CK(cudaMemcpy(col_head_cell, e->d_col_head_cell + D.col_base, sizeof(int) * D.n_columns,
+                      cudaMemcpyDeviceToHost));
+        for (int c = 0; c < D.n_columns; c++)
+            if (col_head_cell[c] >= 0) col_head_cell[c] -= base[sys];
+        col_head_cell[D.n_columns] = nc;
+    }
+    return OG_OK;
+}
+
+og_status og_get_cell_pairs(og_engine *e, int32_t sys, int32_t *idx_head, int32_t *cell1, int32_t *cell2,
+                            int32_t *image, uint64_t *mask) {
+    int32_t nc = 0, ncol = 0, np = 0;
+    og_status s = og_get_grid_info(e, sys, &nc, &ncol, &np);
+    if (s) return s;
+    std::vector<int> base(e->n_sys + 1);
+    CK(cudaMemcpy(base.data(), e->d_sys_cell_base, sizeof(int) * (e->n_sys + 1), cudaMemcpyDeviceToHost));
+    std::vector<int> head(nc + 1);
+    CK(cudaMemcpy(head.data(), e->d_cp_head + base[sys], sizeof(int) * (nc + 1), cudaMemcpyDeviceToHost));
+    const int p0 = head[0];
+    std::vector<int2> ci(np);
+    if (np) CK(cudaMemcpy(ci.data(), e->d_cp_c2img + p0, sizeof(int2) * np, cudaMemcpyDeviceToHost));
+    if (mask && np) CK(cudaMemcpy(mask, e->d_cp_mask + p0, sizeof(uint64_t) * np, cudaMemcpyDeviceToHost));
+    for (int c = 0; c <= nc; c++)
+        if (idx_head) idx_head[c] = head[c] - p0;
+    for (int c = 0; c < nc; c++)
+        for (int k = head[c]; k < head[c + 1]; k++) {
+            if (cell1) cell1[k - p0] = c;
+            if (cell2) cell2[k - p0] = ci[k - p0].x - base[sys];
+            if (image) image[k - p0] = ci[k - p0].y;
+        }
+    return OG_OK;
+}
+
+og_status og_set_trace(og_engine *e, int32_t capacity) {
+    if (!e || !e->finalized) return fail(e, OG_ERR_STATE, "og_set_trace before og_finalize");
+    if (capacity < 0) return fail(e, OG_ERR_INVALID, "negative capacity");
+    if (e->d_trace) {
+        dfree(e, e->d_trace);
+        e->d_trace = nullptr;
+    }
+    e->trace_cap = capacity;
+    if (capacity > 0) {
+        og_status s = dalloc(e, &e->d_trace, (size_t)capacity * e->n_sys * OG_N_ENERGY);
+        if (s) return s;
+    }
+    CK(cudaMemsetAsync(e->d_trace_count, 0, sizeof(long long), e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    return OG_OK;
+}
+
+og_status og_get_trace(og_engine *e, double *out, int32_t max_steps, int32_t *n_out) {
+    if (!e || !e->finalized) return fail(e, OG_ERR_STATE, "og_get_trace before og_finalize");
+    long long cnt = 0;
+    CK(cudaMemcpy(&cnt, e->d_trace_count, sizeof(long long), cudaMemcpyDeviceToHost));
+    if (e->trace_cap <= 0) {
+        if (n_out) *n_out = 0;
+        return OG_OK;
+    }
+    long long avail = cnt < e->trace_cap ? cnt : e->trace_cap;
+    long long first = cnt - avail;
+    int n = (int)(avail < max_steps ? avail : max_steps);
+    const size_t row = (size_t)e->n_sys * OG_N_ENERGY;
+    std::vector<double> all((size_t)e->trace_cap * row);
+    CK(cudaMemcpy(all.data(), e->d_trace, sizeof(double) * all.size(), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; i++) {
+        long long r = (first + i) % e->trace_cap;
+        memcpy(out + i * row, all.data() + r * row, sizeof(double) * row);
+    }
+    if (n_out) *n_out = n;
+    return OG_OK;
+}
+
+og_status og_get_stats(og_engine *e, int64_t *kernel_launches, double *pair_kernel_ms, double *step_ms) {
+    if (!e) return OG_ERR_INVALID;
+    if (kernel_launches) *kernel_launches = e->launches;
+    if (pair_kernel_ms) *pair_kernel_ms = e->pair_ms;
+    if (step_ms) *step_ms = e->step_ms;
+    return OG_OK;
+}
+
+og_status og_get_sizes(og_engine *e, int32_t *n_systems, int64_t *n_atoms_total) {
+    if (!e) return OG_ERR_INVALID;
+    if (n_systems) *n_systems = (int32_t)e->sys.size();
+    if (n_atoms_total) {
+        int64_t t = 0;
+        for (auto &h : e->sys) t += h.d.n_atoms;
+        *n_atoms_total = t;
+    }
+    return OG_OK;
+}
+
+// Per-step timing of the pair kernel (CUDA events on the engine's stream).  Not in the public
+// header's main list: enabled by the benchmark.
+og_status og_set_timing(og_engine *e, int32_t on) {
+    if (!e) return OG_ERR_INVALID;
+    e->timing = on != 0;
+    return OG_OK;
+}
+
+}  // extern "C"
+
+extern "C" og_status og_get_flags(og_engine *e, int32_t *flags) {
+    if (!e || !e->finalized || !flags) return OG_ERR_INVALID;
+    int c[OG_CNT_SIZE];
+    og_status s = read_counters(e, c);
+    if (s) return s;
+    *flags = c[OG_CNT_FLAGS];
+    return OG_OK;
+}

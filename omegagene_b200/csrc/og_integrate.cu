@@ -1,0 +1,616 @@
+// og_integrate.cu -- everything of the per-step path except the cell list and the pair kernel:
+// excluded-pair ZD correction, bonds/angles, fixed-point -> FP64 work, V-McMD force scaling,
+// the leapfrog-presto update, COM cancel, SHAKE pair/trio, velocity-scaling thermostat (with
+// and without constraints), grid move, PBC wrap, kinetic energy and the fixed-order
+// per-system reductions.  One thread per atom / constraint / term; every kernel covers all
+// systems of the batch.  All integrator arithmetic is FP64 (the reference's `real`).
+#include "og_internal.cuh"
+
+namespace og {
+
+// ------------------------------------------------------------- helpers
+
+// Minimum image of PBC::diff_crd_minim_image, double overload (PBC.cpp:70-84): the reference
+// truncates d * (1 / (L/2)) to int twice, with float box lengths.
+__device__ __forceinline__ double minim(double d, float L, float lhi) {
+    d = d - (double)(L * (float)(int)(d * (double)lhi));
+    d = d - (double)(L * (float)(int)(d * (double)lhi));
+    return d;
+}
+
+__device__ __forceinline__ void add_fix(unsigned long long *f, double wx, double wy, double wz) {
+    atomicAdd(f + 0, (unsigned long long)og_to_fix(wx));
+    atomicAdd(f + 1, (unsigned long long)og_to_fix(wy));
+    atomicAdd(f + 2, (unsigned long long)og_to_fix(wz));
+}
+
+// ------------------------------------------------------------- forces
+
+// Excluded-pair ("excess") zero-dipole term, E = cc bcoeff r^2, dE/dx = cc fcoeff d
+// (ForceField.cpp:420-437, ZeroMultipoleSum.cpp:191-202, SubBox.cpp:1347-1367), in FP64.
+__global__ void k_excess(int n_pairs, const int2 *__restrict__ pairs, const int *__restrict__ pair_sys,
+                         const SysDev *__restrict__ sys, const double *__restrict__ crd,
+                         const double *__restrict__ charge, const int *__restrict__ atom_slot,
+                         unsigned long long *__restrict__ frc, double *__restrict__ e_out,
+                         double *__restrict__ vir_out) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n_pairs) return;
+    const SysDev &S = sys[pair_sys[k]];
+    const int i = pairs[k].x, j = pairs[k].y;
+    double d[3];
+    for (int q = 0; q < 3; q++) d[q] = minim(crd[3 * i + q] - crd[3 * j + q], S.Lf[q], S.L_half_inv_f[q]);
+    const double cc = charge[i] * charge[j] * OG_CHARGE_COEFF;
+    const double fco = 1.0 / (S.cutoff * S.cutoff * S.cutoff);
+    const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    e_out[k] = cc * 0.5 * fco * r2;
+    const double gc = cc * fco;
+    add_fix(frc + 3 * (size_t)atom_slot[i], gc * d[0], gc * d[1], gc * d[2]);
+    add_fix(frc + 3 * (size_t)atom_slot[j], -gc * d[0], -gc * d[1], -gc * d[2]);
+    if (vir_out)
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) vir_out[9 * (size_t)k + a * 3 + b] = -d[a] * gc * d[b];
+}
+
+// Harmonic bonds E = k (r - r0)^2 (ForceField.cpp:108-128).
+__global__ void k_bonds(int n, const int2 *__restrict__ b, const double2 *__restrict__ kr,
+                        const int *__restrict__ bsys, const SysDev *__restrict__ sys,
+                        const double *__restrict__ crd, const int *__restrict__ atom_slot,
+                        unsigned long long *__restrict__ frc, double *__restrict__ e_out) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const SysDev &S = sys[bsys[k]];
+    const int i = b[k].x, j = b[k].y;
+    double d[3];
+    for (int q = 0; q < 3; q++) d[q] = minim(crd[3 * i + q] - crd[3 * j + q], S.Lf[q], S.L_half_inv_f[q]);
+    const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    const double dif = r - kr[k].y, coef = kr[k].x * dif;
+    e_out[k] = coef * dif;
+    const double gc = 2.0 * coef / r;
+    add_fix(frc + 3 * (size_t)atom_slot[i], d[0] * gc, d[1] * gc, d[2] * gc);
+    add_fix(frc + 3 * (size_t)atom_slot[j], -d[0] * gc, -d[1] * gc, -d[2] * gc);
+}
+
+// Harmonic angles E = k (theta - theta0)^2 (ForceField.cpp:130-177).
+__global__ void k_angles(int n, const int4 *__restrict__ a, const double2 *__restrict__ kt,
+                         const SysDev *__restrict__ sys, const double *__restrict__ crd,
+                         const int *__restrict__ atom_slot, unsigned long long *__restrict__ frc,
+                         double *__restrict__ e_out) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const SysDev &S = sys[a[k].w];
+    const int i = a[k].x, j = a[k].y, l = a[k].z;
+    double d12[3], d32[3];
+    for (int q = 0; q < 3; q++) {
+        d12[q] = minim(crd[3 * i + q] - crd[3 * j + q], S.Lf[q], S.L_half_inv_f[q]);
+        d32[q] = minim(crd[3 * l + q] - crd[3 * j + q], S.Lf[q], S.L_half_inv_f[q]);
+    }
+    const double r12_2 = d12[0] * d12[0] + d12[1] * d12[1] + d12[2] * d12[2];
+    const double r32_2 = d32[0] * d32[0] + d32[1] * d32[1] + d32[2] * d32[2];
+    const double rri = 1.0 / sqrt(r12_2 * r32_2);
+    double cost = (d12[0] * d32[0] + d12[1] * d32[1] + d12[2] * d32[2]) * rri;
+    cost = fmax(fmin(cost, 1.0), -1.0);
+    const double th = acos(cost);
+    const double dif = th - kt[k].y, coef = kt[k].x * dif;
+    e_out[k] = coef * dif;
+    const double st = fmax(1e-10, sin(th));
+    const double gc = -(2.0 * coef) / st;
+    double w1[3], w2[3];
+    for (int q = 0; q < 3; q++) {
+        w1[q] = gc * (d32[q] * rri - d12[q] * cost / r12_2);
+        w2[q] = gc * (d12[q] * rri - d32[q] * cost / r32_2);
+    }
+    add_fix(frc + 3 * (size_t)atom_slot[i], w1[0], w1[1], w1[2]);
+    add_fix(frc + 3 * (size_t)atom_slot[j], -w1[0] - w2[0], -w1[1] - w2[1], -w1[2] - w2[2]);
+    add_fix(frc + 3 * (size_t)atom_slot[l], w2[0], w2[1], w2[2]);
+}
+
+// Per-atom x (x) F of the pair forces alone (virial, single-sum form); positions are the
+// cell-relative coordinates the pair kernel used plus their cell origin.
+__global__ void k_atom_virial(int n_atoms, const int *__restrict__ atom_slot,
+                              const unsigned long long *__restrict__ frc, const float4 *__restrict__ xq,
+                              const double *__restrict__ cell_origin, double *__restrict__ vir_out) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n_atoms) return;
+    const int s = atom_slot[a], c = s >> 3;
+    const float4 p = xq[s];
+    const double x[3] = {cell_origin[3 * c] + p.x, cell_origin[3 * c + 1] + p.y, cell_origin[3 * c + 2] + p.z};
+    double F[3];
+    for (int q = 0; q < 3; q++) F[q] = -(double)(long long)frc[3 * (size_t)s + q] * OG_FIX_INV;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) vir_out[9 * (size_t)a + i * 3 + j] = x[i] * F[j];
+}
+
+// Fixed-point accumulators -> FP64 work in atom order; clears the accumulators.
+__global__ void k_collect(int n_atoms, const int *__restrict__ atom_slot, unsigned long long *__restrict__ frc,
+                          double *__restrict__ work) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n_atoms) return;
+    unsigned long long *f = frc + 3 * (size_t)atom_slot[a];
+    for (int q = 0; q < 3; q++) {
+        work[3 * a + q] = (double)(long long)f[q] * OG_FIX_INV;
+        f[q] = 0ull;
+    }
+}
+
+// ------------------------------------------------------------- reductions
+
+// Block-wide sum of NV doubles per thread in a fixed order (deterministic).
+template <int NV>
+__device__ void block_sum(double (&v)[NV], double *sh) {
+    const int t = threadIdx.x;
+    for (int q = 0; q < NV; q++) sh[q * blockDim.x + t] = v[q];
+    __syncthreads();
+    for (int off = blockDim.x >> 1; off > 0; off >>= 1) {
+        if (t < off)
+            for (int q = 0; q < NV; q++) sh[q * blockDim.x + t] += sh[q * blockDim.x + t + off];
+        __syncthreads();
+    }
+    for (int q = 0; q < NV; q++) v[q] = sh[q * blockDim.x];
+    __syncthreads();
+}
+
+// One block (256 threads) per system: potential-energy terms, then the McMD scaling factor
+// (Extend.cpp:178-203) and the total potential used for it (MmSystem::set_potential_e).
+__global__ void k_reduce_potential(const SysDev *__restrict__ sys, const int *__restrict__ sys_cell_base,
+                                   const double *__restrict__ cell_acc, const double *__restrict__ e_exc,
+                                   const double *__restrict__ e_bond, const double *__restrict__ e_angle,
+                                   double *__restrict__ sys_acc, double *__restrict__ mcmd_factor) {
+    __shared__ double sh[5 * 256];
+    const int s = blockIdx.x;
+    const SysDev &S = sys[s];
+    double v[5] = {0, 0, 0, 0, 0};
+    for (int c = sys_cell_base[s] + threadIdx.x; c < sys_cell_base[s + 1]; c += blockDim.x) {
+        v[0] += cell_acc[11 * (size_t)c];
+        v[1] += cell_acc[11 * (size_t)c + 1];
+    }
+    for (int k = threadIdx.x; k < S.n_excess; k += blockDim.x) v[2] += e_exc[S.excess_base + k];
+    for (int k = threadIdx.x; k < S.n_bonds; k += blockDim.x) v[3] += e_bond[S.bond_base + k];
+    for (int k = threadIdx.x; k < S.n_angles; k += blockDim.x) v[4] += e_angle[S.angle_base + k];
+    block_sum<5>(v, sh);
+    if (threadIdx.x == 0) {
+        double *acc = sys_acc + OG_ACC_SIZE * s;
+        acc[OG_ACC_VDW] = v[0];
+        acc[OG_ACC_ELE] = v[1];
+        acc[OG_ACC_EXCESS] = v[2];
+        acc[OG_ACC_BOND] = v[3];
+        acc[OG_ACC_ANGLE] = v[4];
+        double f = 1.0;
+        if (S.mcmd_order >= 0) {
+            const double lambda = v[0] + v[1] + v[2] + S.self_energy + v[3] + v[4];
+            double param = lambda;
+            if (lambda <= S.mcmd_lo) param = S.mcmd_lo;
+            else if (lambda >= S.mcmd_hi) param = S.mcmd_hi;
+            double dlnp = S.mcmd_coef[0], t = 1.0;
+            for (int i = 1; i < S.mcmd_order + 1; i++) {
+                t *= param;
+                dlnp += S.mcmd_coef[i] * t;
+            }
+            f = S.mcmd_k * dlnp;
+        }
+        mcmd_factor[s] = f;
+    }
+}
+
+// One block per system: virial = sum_atoms x (x) F + sum_cell-pairs shift (x) F_j + excess.
+__global__ void k_reduce_virial(const SysDev *__restrict__ sys, const int *__restrict__ sys_cell_base,
+                                const double *__restrict__ cell_acc, const double *__restrict__ vir_atom,
+                                const double *__restrict__ vir_exc, double *__restrict__ sys_acc) {
+    __shared__ double sh[9 * 256];
+    const int s = blockIdx.x;
+    const SysDev &S = sys[s];
+    double v[9];
+    for (int q = 0; q < 9; q++) v[q] = 0;
+    for (int c = sys_cell_base[s] + threadIdx.x; c < sys_cell_base[s + 1]; c += blockDim.x)
+        for (int q = 0; q < 9; q++) v[q] += cell_acc[11 * (size_t)c + 2 + q];
+    for (int a = S.atom_base + threadIdx.x; a < S.atom_base + S.n_atoms; a += blockDim.x)
+        for (int q = 0; q < 9; q++) v[q] += vir_atom[9 * (size_t)a + q];
+    for (int k = S.excess_base + threadIdx.x; k < S.excess_base + S.n_excess; k += blockDim.x)
+        for (int q = 0; q < 9; q++) v[q] += vir_exc[9 * (size_t)k + q];
+    block_sum<9>(v, sh);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 9; q++) sys_acc[OG_ACC_SIZE * s + OG_ACC_VIR + q] = v[q];
+}
+
+// One block per COM group: moment = (sum m v) / M_group (COMMotion.cpp:30-55).
+__global__ void k_group_moment(const int *__restrict__ grp_start, const int *__restrict__ grp_atoms,
+                               const float *__restrict__ grp_mass_inv, const float *__restrict__ mass,
+                               const double *__restrict__ v, const int *__restrict__ grp_sys,
+                               const int *__restrict__ sys_active, double *__restrict__ moment) {
+    __shared__ double sh[3 * 256];
+    const int g = blockIdx.x;
+    double m[3] = {0, 0, 0};
+    if (sys_active == nullptr || sys_active[grp_sys[g]]) {
+        for (int k = grp_start[g] + threadIdx.x; k < grp_start[g + 1]; k += blockDim.x) {
+            const int a = grp_atoms[k];
+            for (int q = 0; q < 3; q++) m[q] += v[3 * a + q] * (double)mass[a];
+        }
+    }
+    block_sum<3>(m, sh);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 3; q++) moment[3 * g + q] = m[q] * (double)grp_mass_inv[g];
+}
+
+// One block per system: sum over atoms of a per-atom scalar.
+__global__ void k_reduce_atoms(const SysDev *__restrict__ sys, const double *__restrict__ val,
+                               double *__restrict__ out, int out_stride, int out_index) {
+    __shared__ double sh[256];
+    const int s = blockIdx.x;
+    const SysDev &S = sys[s];
+    double v[1] = {0};
+    for (int a = S.atom_base + threadIdx.x; a < S.atom_base + S.n_atoms; a += blockDim.x) v[0] += val[a];
+    block_sum<1>(v, sh);
+    if (threadIdx.x == 0) out[out_stride * s + out_index] = v[0];
+}
+
+// ------------------------------------------------------------- integrator
+
+// SubBox::cpy_vel_prev + update_velocities (SubBox.cpp:1427-1454) with McMD scaling of the
+// work (ExtendedVMcMD::scale_force multiplies work in place).
+__global__ void k_update_velocities(int n_atoms, const int *__restrict__ atom_sys, const SysDev *__restrict__ sys,
+                                    const double *__restrict__ mcmd_factor, double *__restrict__ work,
+                                    const float *__restrict__ mass_inv, double *__restrict__ vel,
+                                    double *__restrict__ vel_next) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n_atoms) return;
+    const int s = atom_sys[a];
+    const SysDev &S = sys[s];
+    const double f = mcmd_factor[s];
+    for (int q = 0; q < 3; q++) {
+        const int k = 3 * a + q;
+        double w = work[k];
+        if (S.mcmd_order >= 0) {
+            w *= f;
+            work[k] = w;
+        }
+        const double v = vel_next[k];
+        vel[k] = v;
+        vel_next[k] = v + (S.dt * -OG_FORCE_VEL * w * (double)mass_inv[a]);
+    }
+}
+
+// vel_next -= moment of the atom's COM group.
+__global__ void k_com_apply(int n_atoms, const int *__restrict__ atom_group, const double *__restrict__ moment,
+                            const int *__restrict__ atom_sys, const int *__restrict__ sys_active,
+                            double *__restrict__ v) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n_atoms) return;
+    const int g = atom_group[a];
+    if (g < 0) return;
+    if (sys_active && !sys_active[atom_sys[a]]) return;
+    for (int q = 0; q < 3; q++) v[3 * a + q] -= moment[3 * g + q];
+}
+
+// Per-atom kinetic term of ThermostatScaling::apply_thermostat (Thermostat.cpp:57-73).
+__global__ void k_thermo_scaling_ke(int n_atoms, const int *__restrict__ atom_sys, const SysDev *__restrict__ sys,
+                                    const double *__restrict__ work, const float *__restrict__ mass,
+                                    const float *__restrict__ mass_inv, const double *__restrict__ vel,
+                                    double *__restrict__ tmp) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n_atoms) return;
+    const SysDev &S = sys[atom_sys[a]];
+    double vn = 0.0;
+    for (int q = 0; q < 3; q++) {
+        const double vt = vel[3 * a + q] - 0.5 * (S.dt * work[3 * a + q] * OG_FORCE_VEL * (double)mass_inv[a]);
+        vn += vt * vt;
+    }
+    tmp[a] = (double)mass[a] * vn;
+}
+
+// SubBox::update_thermostat target (SubBox.cpp:1745-1757).
+__device__ __forceinline__ double target_temperature(const double *thermo, int s, long long step) {
+    const double t0 = thermo[4 * s], tinit = thermo[4 * s + 1], heat = thermo[4 * s + 2];
+    if ((double)step < heat) return tinit + ((t0 - tinit) / heat) * (double)step;
+    return t0;
+}
+
+__global__ void k_thermo_scaling_apply(int n_atoms, const int *__restrict__ atom_sys, const SysDev *__restrict__ sys,
+                                       const double *__restrict__ sum_ke, const double *__restrict__ thermo,
+                                       const long long *__restrict__ step, const double *__restrict__ work,
+                                       const float *__restrict__ mass_inv, const double *__restrict__ vel,
+                                       double *__restrict__ vel_next) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n_atoms) return;
+    const int s = atom_sys[a];
+    const SysDev &S = sys[s];
+    if (S.thermostat != 1 || S.has_constraints) return;
+    const double tcur = sum_ke[s] * S.temperature_coeff_thermo;
+    const double tt = target_temperature(thermo, s, *step);
+    const double scale = sqrt(1 + S.dt * S.tau_inv * (tt / tcur - 1));
+    for (int q = 0; q < 3; q++) {
+        const double vd = S.dt * -OG_FORCE_VEL * work[3 * a + q] * (double)mass_inv[a];
+        vel_next[3 * a + q] = (2.0 * scale - 1.0) * vel[3 * a + q] + scale * vd;
+    }
+}
+
+// SubBox::cpy_crd_prev + update_coordinates_cur (SubBox.cpp:1417-1420, 1567-1580).
+__global__ void k_update_coordinates(int n_atoms, const int *__restrict__ atom_sys, const SysDev *__restrict__ sys,
+                                     double *__restrict__ crd, double *__restrict__ crd_prev,
+                                     const double *__restrict__ vel_next) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n_atoms) return;
+    const double dt = sys[atom_sys[a]].dt;
+    for (int q = 0; q < 3; q++) {
+        const int k = 3 * a + q;
+        const double x = crd[k];
+        crd_prev[k] = x;
+        crd[k] = x + vel_next[k] * dt;
+    }
+}
+
+// ConstraintShake::shake_pair (ConstraintShake.cpp:18-49): one analytic correction.
+__global__ void k_shake_pair(int n, const int2 *__restrict__ p, const double *__restrict__ d2,
+                             const int *__restrict__ psys, const SysDev *__restrict__ sys,
+                             const int *__restrict__ sys_active, const float *__restrict__ mass_inv,
+                             double *__restrict__ crd, const double *__restrict__ crd_prev) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int s = psys[k];
+    if (sys_active && !sys_active[s]) return;
+    const SysDev &S = sys[s];
+    const int i = p[k].x, j = p[k].y;
+    double d[3], dp[3];
+    for (int q = 0; q < 3; q++) {
+        d[q] = minim(crd[3 * j + q] - crd[3 * i + q], S.Lf[q], S.L_half_inv_f[q]);
+        dp[q] = minim(crd_prev[3 * j + q] - crd_prev[3 * i + q], S.Lf[q], S.L_half_inv_f[q]);
+    }
+    const double m1 = (double)mass_inv[i], m2 = (double)mass_inv[j], m12 = m1 + m2;
+    const double dsq = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    const double dsqp = dp[0] * dp[0] + dp[1] * dp[1] + dp[2] * dp[2];
+    const double dip = d[0] * dp[0] + d[1] * dp[1] + d[2] * dp[2];
+    const double va = m12 * m12 * dsqp, vb = m12 * dip, vc = dsq - d2[k];
+    const double g = (vb - sqrt(fmax(vb * vb - vc * va, 0.0))) / va;
+    for (int q = 0; q < 3; q++) {
+        crd[3 * i + q] += m1 * g * dp[q];
+        crd[3 * j + q] -= m2 * g * dp[q];
+    }
+}
+
+// ConstraintShake::shake_trio (ConstraintShake.cpp:51-149): Newton iteration on the three
+// squared distances with the cofactor inverse, until every relative residual < tol.
+__global__ void k_shake_trio(int n, const int4 *__restrict__ t, const double *__restrict__ td,
+                             const SysDev *__restrict__ sys, const int *__restrict__ sys_active,
+                             const float *__restrict__ mass_inv, double *__restrict__ crd,
+                             const double *__restrict__ crd_prev, int max_loops, double tol,
+                             int *__restrict__ counters) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int s = t[k].w;
+    if (sys_active && !sys_active[s]) return;
+    const SysDev &S = sys[s];
+    const int a1 = t[k].x, a2 = t[k].y, a3 = t[k].z;
+    double d12[3], d23[3], d31[3], p12[3], p23[3], p31[3];
+    for (int q = 0; q < 3; q++) {
+        d12[q] = minim(crd[3 * a1 + q] - crd[3 * a2 + q], S.Lf[q], S.L_half_inv_f[q]);
+        p12[q] = minim(crd_prev[3 * a1 + q] - crd_prev[3 * a2 + q], S.Lf[q], S.L_half_inv_f[q]);
+        d23[q] = minim(crd[3 * a2 + q] - crd[3 * a3 + q], S.Lf[q], S.L_half_inv_f[q]);
+        p23[q] = minim(crd_prev[3 * a2 + q] - crd_prev[3 * a3 + q], S.Lf[q], S.L_half_inv_f[q]);
+        d31[q] = minim(crd[3 * a3 + q] - crd[3 * a1 + q], S.Lf[q], S.L_half_inv_f[q]);
+        p31[q] = minim(crd_prev[3 * a3 + q] - crd_prev[3 * a1 + q], S.Lf[q], S.L_half_inv_f[q]);
+    }
+    const double m1 = (double)mass_inv[a1], m2 = (double)mass_inv[a2], m3 = (double)mass_inv[a3];
+    const double c11 = m1 + m2, c12 = -m2, c13 = -m1;
+    const double c21 = -m2, c22 = m2 + m3, c23 = -m3;
+    const double c31 = -m1, c32 = -m3, c33 = m3 + m1;
+    const double t0 = td[3 * k], t1 = td[3 * k + 1], t2 = td[3 * k + 2];
+    double g0 = 0, g1 = 0, g2 = 0, g3 = 0, g4 = 0, g5 = 0;
+    bool conv = false;
+#define DOT(a, b) (a[0] * b[0] + a[1] * b[1] + a[2] * b[2])
+    for (int it = 0; it < max_loops; it++) {
+        for (int q = 0; q < 3; q++) {
+            d12[q] += (c11 * p12[q] * g0 + c12 * p23[q] * g1 + c13 * p31[q] * g2);
+            d23[q] += (c21 * p12[q] * g0 + c22 * p23[q] * g1 + c23 * p31[q] * g2);
+            d31[q] += (c31 * p12[q] * g0 + c32 * p23[q] * g1 + c33 * p31[q] * g2);
+        }
+        const double f11 = 2.0 * c11 * DOT(d12, p12), f12 = 2.0 * c12 * DOT(d12, p23), f13 = 2.0 * c13 * DOT(d12, p31);
+        const double f21 = 2.0 * c21 * DOT(d23, p12), f22 = 2.0 * c22 * DOT(d23, p23), f23 = 2.0 * c23 * DOT(d23, p31);
+        const double f31 = 2.0 * c31 * DOT(d31, p12), f32 = 2.0 * c32 * DOT(d31, p23), f33 = 2.0 * c33 * DOT(d31, p31);
+        const double r0 = t0 - DOT(d12, d12), r1 = t1 - DOT(d23, d23), r2 = t2 - DOT(d31, d31);
+        if (fabs(r0 / t0) < tol && fabs(r1 / t1) < tol && fabs(r2 / t2) < tol) {
+            conv = true;
+            break;
+        }
+        const double det = 1.0 / (f11 * f22 * f33 + f12 * f23 * f31 + f13 * f21 * f32 - f11 * f23 * f32 -
+                                  f12 * f21 * f33 - f13 * f22 * f31);
+        const double b11 = f22 * f33 - f23 * f32, b12 = f32 * f13 - f33 * f12, b13 = f12 * f23 - f13 * f22;
+        const double b21 = f23 * f31 - f21 * f33, b22 = f33 * f11 - f31 * f13, b23 = f13 * f21 - f11 * f23;
+        const double b31 = f21 * f32 - f22 * f31, b32 = f31 * f12 - f32 * f11, b33 = f11 * f22 - f12 * f21;
+        g0 = (b11 * r0 + b12 * r1 + b13 * r2) * det;
+        g1 = (b21 * r0 + b22 * r1 + b23 * r2) * det;
+        g2 = (b31 * r0 + b32 * r1 + b33 * r2) * det;
+        g3 += g0;
+        g4 += g1;
+        g5 += g2;
+    }
+#undef DOT
+    if (!conv) og_set_flag(counters, OG_FLAG_SHAKE);
+    for (int q = 0; q < 3; q++) {
+        crd[3 * a1 + q] += m1 * (g3 * p12[q] - g5 * p31[q]);
+        crd[3 * a2 + q] += m2 * (-g3 * p12[q] + g4 * p23[q]);
+        crd[3 * a3 + q] += m3 * (-g4 * p23[q] + g5 * p31[q]);
+    }
+}
+
+// Per-atom KE of (vel_next + vel)/2 (start of each thermostat iteration, Thermostat.cpp:114-123).
+__global__ void k_ke_mid(int n_atoms, const float *__restrict__ mass, const double *__restrict__ vel,
+                         const double *__restrict__ vel_next, double *__restrict__ tmp) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n_atoms) return;
+    double vn = 0.0;
+    for (int q = 0; q < 3; q++) {
+        const double vt = (vel_next[3 * a + q] + vel[3 * a + q]) * 0.5;
+        vn += vt * vt;
+    }
+    tmp[a] = vn * (double)mass[a];
+}
+
+// Convergence test of the thermostat loop, one thread per system (Thermostat.cpp:124-131).
+// sys_active[s] stays 1 while the system still iterates; *any receives the count.
+__global__ void k_thermo_check(int n_sys, const SysDev *__restrict__ sys, const double *__restrict__ sum_ke,
+                               const double *__restrict__ thermo, const long long *__restrict__ step, int it,
+                               int max_loops, double tol, int *__restrict__ sys_active, int *__restrict__ any,
+                               int *__restrict__ counters) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_sys) return;
+    if (!sys_active[s]) return;
+    const SysDev &S = sys[s];
+    const double tcur = sum_ke[s] * S.temperature_coeff_thermo;
+    const double tt = target_temperature(thermo, s, *step);
+    if (it == max_loops - 1) {
+        sys_active[s] = 0;
+        og_set_flag(counters, OG_FLAG_THERMO);
+        return;
+    }
+    if (fabs(tcur - tt) / tt < tol) {
+        sys_active[s] = 0;
+        return;
+    }
+    atomicAdd(any, 1);
+}
+
+// Half-step velocities with the constraint acceleration (Thermostat.cpp:133-148).
+__global__ void k_thermo_half(int n_atoms, const int *__restrict__ atom_sys, const SysDev *__restrict__ sys,
+                              const int *__restrict__ sys_active, const double *__restrict__ work,
+                              const float *__restrict__ mass, const float *__restrict__ mass_inv,
+                              const double *__restrict__ crd, const double *__restrict__ buf_crd,
+                              const double *__restrict__ vel, double *__restrict__ vel_next,
+                              double *__restrict__ tmp) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n_atoms) return;
+    const int s = atom_sys[a];
+    if (!sys_active[s]) { tmp[a] = 0.0; return; }
+    const double dt = sys[s].dt, dtisq = 1.0 / (dt * dt);
+    double vn = 0.0;
+    for (int q = 0; q < 3; q++) {
+        const int k = 3 * a + q;
+        const double vd = -OG_FORCE_VEL * work[k] * (double)mass_inv[a] + (crd[k] - buf_crd[k]) * dtisq;
+        vel_next[k] = vel[k] + 0.5 * dt * vd;
+        vn += vel_next[k] * vel_next[k];
+    }
+    tmp[a] = (double)mass[a] * vn;
+}
+
+// Rescale to the target temperature (Thermostat.cpp:150-164).
+__global__ void k_thermo_rescale(int n_atoms, const int *__restrict__ atom_sys, const SysDev *__restrict__ sys,
+                                 const int *__restrict__ sys_active, const double *__restrict__ sum_ke,
+                                 const double *__restrict__ thermo, const long long *__restrict__ step,
+                                 const double *__restrict__ work, const float *__restrict__ mass_inv,
+                                 const double *__restrict__ crd, const double *__restrict__ buf_crd,
+                                 const double *__restrict__ vel, double *__restrict__ vel_next) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n_atoms) return;
+    const int s = atom_sys[a];
+    if (!sys_active[s]) return;
+    const SysDev &S = sys[s];
+    const double dt = S.dt, dtisq = 1.0 / (dt * dt);
+    const double tcur = sum_ke[s] * S.temperature_coeff_thermo;
+    const double scale = sqrt(target_temperature(thermo, s, *step) / tcur);
+    for (int q = 0; q < 3; q++) {
+        const int k = 3 * a + q;
+        const double vd = -OG_FORCE_VEL * work[k] * (double)mass_inv[a] + (crd[k] - buf_crd[k]) * dtisq;
+        vel_next[k] = (2.0 * scale - 1.0) * vel[k] + scale * dt * vd;
+    }
+}
+
+// crd = crd_prev + dt vel_next for still-iterating systems (Thermostat.cpp:166-170).
+__global__ void k_thermo_crd(int n_atoms, const int *__restrict__ atom_sys, const SysDev *__restrict__ sys,
+                             const int *__restrict__ sys_active, double *__restrict__ crd,
+                             const double *__restrict__ crd_prev, const double *__restrict__ vel_next) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n_atoms) return;
+    const int s = atom_sys[a];
+    if (!sys_active[s]) return;
+    const double dt = sys[s].dt;
+    for (int q = 0; q < 3; q++) crd[3 * a + q] = crd_prev[3 * a + q] + dt * vel_next[3 * a + q];
+}
+
+// End of step, per atom: velocities from the constrained displacement (SubBox.cpp:1462-1481,
+// only when the plain constraint path ran), MiniCell::move_atom (MiniCell.cpp:1312-1325) and the
+// refreshed cell-relative float coordinate, PBC wrap (SubBox.cpp:1482-1502) and the kinetic
+// term of (vel + vel_next)/2 (SubBox.cpp:1504-1516, DynamicsMode.cpp:358-372).
+__global__ void k_finish(int n_atoms, const int *__restrict__ atom_sys, const SysDev *__restrict__ sys,
+                         int vel_from_crd, double *__restrict__ crd, const double *__restrict__ crd_prev,
+                         const double *__restrict__ vel, double *__restrict__ vel_next,
+                         const int *__restrict__ atom_slot, double *__restrict__ slot_crd,
+                         const double *__restrict__ cell_origin, float4 *__restrict__ xq,
+                         const float *__restrict__ mass, double *__restrict__ ke) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n_atoms) return;
+    const SysDev &S = sys[atom_sys[a]];
+    const int sl = atom_slot[a], c = sl >> 3;
+    double vn = 0.0;
+    float r[3];
+    for (int q = 0; q < 3; q++) {
+        const int k = 3 * a + q;
+        const double x = crd[k], xp = crd_prev[k];
+        if (vel_from_crd && S.has_constraints && S.thermostat != 1) vel_next[k] = (x - xp) * (1.0 / S.dt);
+        const double gcrd = slot_crd[3 * (size_t)sl + q] + (x - xp);
+        slot_crd[3 * (size_t)sl + q] = gcrd;
+        r[q] = (float)(gcrd - cell_origin[3 * c + q]);
+        double xw = x;
+        if (xw >= (double)S.upperf[q]) xw -= (double)S.Lf[q];
+        else if (xw < (double)S.lowerf[q]) xw += (double)S.Lf[q];
+        crd[k] = xw;
+        const double vj = (vel[k] + vel_next[k]) * 0.5;
+        vn += vj * vj;
+    }
+    float4 p = xq[sl];
+    p.x = r[0];
+    p.y = r[1];
+    p.z = r[2];
+    xq[sl] = p;
+    ke[a] = vn * (double)mass[a];
+}
+
+// Slot coordinates/charges/types after a list rebuild (cuda_setup.cu:364-402 roles).
+__global__ void k_slot_refresh(const int *__restrict__ counters, int slots_cap, const int *__restrict__ slot_atom,
+                               const double *__restrict__ slot_crd, const double *__restrict__ cell_origin,
+                               const float *__restrict__ charge_f, const int *__restrict__ atom_type,
+                               float4 *__restrict__ xq, int *__restrict__ slot_type) {
+    int sl = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n_slots = counters[OG_CNT_N_CELLS] * OG_CELL;
+    if (sl >= n_slots || sl >= slots_cap) return;
+    const int c = sl >> 3, a = slot_atom[sl];
+    float4 p;
+    p.x = (float)(slot_crd[3 * (size_t)sl] - cell_origin[3 * c]);
+    p.y = (float)(slot_crd[3 * (size_t)sl + 1] - cell_origin[3 * c + 1]);
+    p.z = (float)(slot_crd[3 * (size_t)sl + 2] - cell_origin[3 * c + 2]);
+    p.w = a >= 0 ? charge_f[a] : 0.0f;
+    xq[sl] = p;
+    slot_type[sl] = a >= 0 ? atom_type[a] : 0;
+}
+
+// Final per-system energies of a step (DynamicsMode::gather_energies + cal_kinetic_energy),
+// appended to the trace ring when enabled.
+__global__ void k_energies(int n_sys, const SysDev *__restrict__ sys, const double *__restrict__ sys_acc,
+                           const double *__restrict__ mcmd_factor, double *__restrict__ energies,
+                           double *__restrict__ trace, int trace_cap, long long *__restrict__ trace_count) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_sys) return;
+    const SysDev &S = sys[s];
+    const double *acc = sys_acc + OG_ACC_SIZE * s;
+    double *e = energies + 11 * s;
+    e[0] = acc[OG_ACC_VDW];
+    e[1] = acc[OG_ACC_ELE] + acc[OG_ACC_EXCESS] + S.self_energy;
+    e[2] = acc[OG_ACC_BOND];
+    e[3] = acc[OG_ACC_ANGLE];
+    e[4] = e[0] + e[1] + e[2] + e[3];
+    e[5] = acc[OG_ACC_KIN] * OG_KINETIC_COEFF;
+    e[6] = e[5] * S.temperature_coeff_dyn;
+    e[7] = e[4] + e[5];
+    e[8] = acc[OG_ACC_EXCESS];
+    e[9] = S.self_energy;
+    e[10] = mcmd_factor[s];
+    if (trace && trace_cap > 0) {
+        const long long row = *trace_count % trace_cap;
+        for (int q = 0; q < 11; q++) trace[(row * n_sys + s) * 11 + q] = e[q];
+    }
+}
+
+__global__ void k_trace_advance(long long *trace_count, long long *step) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        *trace_count += 1;
+        *step += 1;
+    }
+}
+
+}  // namespace og

@@ -1,0 +1,99 @@
+// og_internal.cuh -- device-side data layout shared by the engine's kernels.
+//
+// One engine holds S independent systems laid end to end in every array ("batch").
+// Index spaces (all global across systems):
+//   atom   -- original atom order, system s owns [atom_base, atom_base + n_atoms)
+//   column -- MiniCell xy columns, system s owns [col_base, col_base + n_columns)
+//   cell   -- 8-slot MiniCell cells, rebuilt on device; system s owns
+//             [sys_cell_base[s], sys_cell_base[s+1])
+//   slot   -- 8 * cell + k, grid order (MiniCell::atomids)
+//   pair   -- cell pairs in CSR order over cell1
+// Per-slot data are structure-of-arrays so that one warp reads 8-slot cells with
+// coalesced 16-byte loads.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define OG_CELL 8
+#define OG_MAX_COLUMN_ATOMS 4096     // per-column sort capacity (shared memory)
+#define OG_FIX_SCALE 4294967296.0    // 2^32: work (kcal/mol/A) -> int64 fixed point
+#define OG_FIX_INV (1.0 / 4294967296.0)
+#define OG_CHARGE_COEFF 332.06378    // CelesteObject.cpp:35
+#define OG_FORCE_VEL 4.184e-4        // CelesteObject.cpp:36
+#define OG_GAS_CONST 8.31451         // CelesteObject.cpp:37
+#define OG_JOULE_CAL 4.184           // CelesteObject.cpp:38
+#define OG_KINETIC_COEFF ((1e7 / (OG_JOULE_CAL * 1e3)) * 0.5)  // CelesteObject.cpp:39
+
+// device error flags (bit set in d_counters[OG_CNT_FLAGS])
+#define OG_FLAG_PAIR_CAPACITY 1
+#define OG_FLAG_COLUMN_CAPACITY 2
+#define OG_FLAG_BAD_COORD 4
+#define OG_FLAG_SHAKE 8
+#define OG_FLAG_THERMO 16
+
+// d_counters slots
+#define OG_CNT_N_CELLS 0
+#define OG_CNT_N_PAIRS 1
+#define OG_CNT_FLAGS 2
+#define OG_CNT_ACTIVE 3
+#define OG_CNT_SIZE 8
+
+// Per-system constants (read-only during a step).
+struct SysDev {
+    // box, PBC.h:21-27 (float) with double copies used by the FP64 integrator
+    float Lf[3], lowerf[3], upperf[3], L_half_inv_f[3];
+    double L[3], lower[3], upper[3];
+    // MiniCell geometry (MiniCell.cpp:221-290)
+    int nx, ny, n_columns, col_base;
+    float L_cell[2];
+    int n_nb[2], n_nb_cols;
+    int n_uni_z, uni_base;
+    float L_z_uni;
+    float cutoff_pair2;          // nsgrid cutoff^2, float
+    // atoms
+    int atom_base, n_atoms;
+    // pair interaction
+    float cutoff2;               // interaction cutoff^2
+    float zcore, bcoeff, fcoeff; // zero-dipole alpha=0 (ZeroMultipoleSum.cpp:150-202), float
+    double cutoff;
+    int lj_base, n_types;
+    // integrator
+    double dt;
+    double temperature_coeff_thermo;  // Thermostat.cpp:13-16
+    double temperature_coeff_dyn;     // DynamicsMode.cpp:67
+    double tau_inv;
+    double self_energy;
+    int thermostat;
+    int has_constraints;
+    // McMD
+    int mcmd_order;
+    double mcmd_lo, mcmd_hi, mcmd_k;  // const_k = (GAS_CONST/JOULE_CAL) 1e-3 T
+    double mcmd_coef[8];
+    // constraint / term ranges (global index spaces of their own arrays)
+    int trio_base, n_trio, pair_base, n_pair;
+    int excess_base, n_excess, bond_base, n_bonds, angle_base, n_angles;
+};
+
+// per-system reduction slots in d_sys_acc (double)
+#define OG_ACC_VDW 0
+#define OG_ACC_ELE 1
+#define OG_ACC_EXCESS 2
+#define OG_ACC_BOND 3
+#define OG_ACC_ANGLE 4
+#define OG_ACC_KIN 5
+#define OG_ACC_VIR 6     // 9 entries
+#define OG_ACC_SIZE 16
+
+__device__ __forceinline__ unsigned int og_float_order(float f) {
+    f = f + 0.0f;  // -0 -> +0 so that equal values give equal keys
+    unsigned int u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__device__ __forceinline__ void og_set_flag(int *counters, int flag) {
+    atomicOr(&counters[OG_CNT_FLAGS], flag);
+}
+
+__device__ __forceinline__ long long og_to_fix(double w) {
+    return __double2ll_rn(w * OG_FIX_SCALE);
+}

@@ -1,0 +1,163 @@
+// og_pair.cu -- Lennard-Jones + zero-dipole (alpha = 0) pair forces over the cell-pair list.
+//
+// Physics of ForceField::calc_pairwise + ZeroMultipoleSum::calc_zero02pole_alpha0
+// (src/celeste/core/ForceField.cpp:333-418, ZeroMultipoleSum.cpp:309-332) and the reference
+// GPU kernel kernel_pairwise_ljzd / cal_pair (src/celeste/cuda/cuda_setup.cu:487-675):
+//   E_vdw = C12/r^12 - C6/r^6
+//   E_ele = q_i q_j 332.06378 (1/r - zcore + bcoeff r^2),  r < cutoff
+//   dE/dx_i = [r^-2 (6 C6/r^6 - 12 C12/r^12) - cc (r^-3 - fcoeff)] (x_i - x_j)
+//
+// B200 layout: one warp per cell1; lane = (i-group g = lane>>3, j-slot jj = lane&7); each lane
+// evaluates i = g and i = g+4 against j = jj of every cell2 in cell1's CSR range.
+// Coordinates are float offsets from a per-cell FP64 origin, so the pair distance carries the
+// rounding of a ~10 A quantity instead of the absolute coordinate.  The per-cell-pair shift
+// (origin2 + image - origin1) is formed in FP64.  Work on j is reduced over the 4 i-groups
+// with shuffles and added to an int64 fixed-point accumulator (2^-32 kcal/mol/A), which makes
+// the per-atom sums independent of launch order; i-work is summed in FP64 registers and
+// added once at the end.  Energies and the virial go to per-cell slots that a fixed-order
+// reduction sums later.
+#include "og_internal.cuh"
+
+namespace og {
+
+template <bool VIR>
+__global__ void __launch_bounds__(256)
+k_pair_ljzd(const int *__restrict__ counters, const int *__restrict__ cell_sys, const SysDev *__restrict__ sys,
+            const double *__restrict__ cell_origin, const float4 *__restrict__ xq, const int *__restrict__ slot_type,
+            const int *__restrict__ cp_head, const int2 *__restrict__ cp_c2img,
+            const unsigned long long *__restrict__ cp_mask, const float2 *__restrict__ lj,
+            unsigned long long *__restrict__ frc, double *__restrict__ cell_acc, long long pair_cap) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int n_cells = counters[OG_CNT_N_CELLS];
+    if (warp >= n_cells) return;
+    const int c1 = warp;
+    const int jj = lane & 7, g = lane >> 3;
+    const SysDev &S = sys[cell_sys[c1]];
+    const double o1x = cell_origin[3 * c1], o1y = cell_origin[3 * c1 + 1], o1z = cell_origin[3 * c1 + 2];
+    const float4 xi0 = xq[c1 * OG_CELL + g], xi1 = xq[c1 * OG_CELL + g + 4];
+    const int ti0 = slot_type[c1 * OG_CELL + g] * S.n_types + S.lj_base;
+    const int ti1 = slot_type[c1 * OG_CELL + g + 4] * S.n_types + S.lj_base;
+    const float qc0 = xi0.w * (float)OG_CHARGE_COEFF, qc1 = xi1.w * (float)OG_CHARGE_COEFF;
+    const float rc2 = S.cutoff2, zcore = S.zcore, bco = S.bcoeff, fco = S.fcoeff;
+    double f0x = 0, f0y = 0, f0z = 0, f1x = 0, f1y = 0, f1z = 0;
+    double e_vdw = 0, e_ele = 0;
+    double v[9];
+    if (VIR)
+        for (int q = 0; q < 9; q++) v[q] = 0;
+    // a list that overflowed its buffer is flagged and redone; never read past the buffer
+    const int k_end = (int)min((long long)cp_head[c1 + 1], pair_cap);
+    for (int k = cp_head[c1]; k < k_end; k++) {
+        const int2 ci = cp_c2img[k];
+        const unsigned long long m = cp_mask[k];
+        const int c2 = ci.x, img = ci.y;
+        const double shx = (img & 1) ? -S.L[0] : ((img & 2) ? S.L[0] : 0.0);
+        const double shy = (img & 4) ? -S.L[1] : ((img & 8) ? S.L[1] : 0.0);
+        const double shz = (img & 16) ? -S.L[2] : ((img & 32) ? S.L[2] : 0.0);
+        const float sx = (float)(cell_origin[3 * c2] - o1x + shx);
+        const float sy = (float)(cell_origin[3 * c2 + 1] - o1y + shy);
+        const float sz = (float)(cell_origin[3 * c2 + 2] - o1z + shz);
+        const float4 xj = xq[c2 * OG_CELL + jj];
+        const int tj = slot_type[c2 * OG_CELL + jj];
+        const float rjx = xj.x + sx, rjy = xj.y + sy, rjz = xj.z + sz;
+        float wjx = 0.f, wjy = 0.f, wjz = 0.f, ev = 0.f, ee = 0.f;
+#pragma unroll
+        for (int t = 0; t < 2; t++) {
+            const float4 xi = t ? xi1 : xi0;
+            const float dx = xi.x - rjx, dy = xi.y - rjy, dz = xi.z - rjz;
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            const int bit = jj * OG_CELL + g + 4 * t;
+            const bool act = (((m >> bit) & 1ull) == 0ull) && (r2 < rc2);
+            const float r2s = act ? r2 : 1.0f;
+            const float rinv = rsqrtf(r2s);
+            const float r2inv = rinv * rinv;
+            const float r6inv = r2inv * r2inv * r2inv;
+            const float2 p = __ldg(&lj[(t ? ti1 : ti0) + tj]);
+            const float t6 = p.x * r6inv, t12 = p.y * r6inv * r6inv;
+            const float cc = (t ? qc1 : qc0) * xj.w;
+            float pv = t12 - t6;
+            float pe = cc * (rinv - zcore + bco * r2s);
+            float wc = r2inv * (6.0f * t6 - 12.0f * t12) - cc * (rinv * r2inv - fco);
+            if (!act) { pv = 0.f; pe = 0.f; wc = 0.f; }
+            const float wx = wc * dx, wy = wc * dy, wz = wc * dz;
+            ev += pv;
+            ee += pe;
+            wjx -= wx;
+            wjy -= wy;
+            wjz -= wz;
+            if (t) { f1x += wx; f1y += wy; f1z += wz; }
+            else { f0x += wx; f0y += wy; f0z += wz; }
+        }
+        e_vdw += ev;
+        e_ele += ee;
+        // work on j: sum over the four i-groups (lanes jj, jj+8, jj+16, jj+24)
+        wjx += __shfl_xor_sync(0xffffffffu, wjx, 8);
+        wjy += __shfl_xor_sync(0xffffffffu, wjy, 8);
+        wjz += __shfl_xor_sync(0xffffffffu, wjz, 8);
+        wjx += __shfl_xor_sync(0xffffffffu, wjx, 16);
+        wjy += __shfl_xor_sync(0xffffffffu, wjy, 16);
+        wjz += __shfl_xor_sync(0xffffffffu, wjz, 16);
+        if (g == 0 && (wjx != 0.f || wjy != 0.f || wjz != 0.f)) {
+            unsigned long long *fj = frc + 3 * (size_t)(c2 * OG_CELL + jj);
+            atomicAdd(fj + 0, (unsigned long long)__float2ll_rn(wjx * (float)OG_FIX_SCALE));
+            atomicAdd(fj + 1, (unsigned long long)__float2ll_rn(wjy * (float)OG_FIX_SCALE));
+            atomicAdd(fj + 2, (unsigned long long)__float2ll_rn(wjz * (float)OG_FIX_SCALE));
+            if (VIR && img != 0) {
+                // sum over pairs of d (x) f = sum_atoms x (x) F + sum_cell-pairs shift (x) F_j
+                const double sh[3] = {shx, shy, shz};
+                const double fjv[3] = {-(double)wjx, -(double)wjy, -(double)wjz};
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++) v[a * 3 + b] += sh[a] * fjv[b];
+            }
+        }
+    }
+    // work on i: sum over the 8 j lanes of each i-group
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) {
+        f0x += __shfl_xor_sync(0xffffffffu, f0x, o);
+        f0y += __shfl_xor_sync(0xffffffffu, f0y, o);
+        f0z += __shfl_xor_sync(0xffffffffu, f0z, o);
+        f1x += __shfl_xor_sync(0xffffffffu, f1x, o);
+        f1y += __shfl_xor_sync(0xffffffffu, f1y, o);
+        f1z += __shfl_xor_sync(0xffffffffu, f1z, o);
+    }
+    if (jj == 0) {
+        unsigned long long *fa = frc + 3 * (size_t)(c1 * OG_CELL + g);
+        unsigned long long *fb = frc + 3 * (size_t)(c1 * OG_CELL + g + 4);
+        if (f0x != 0.0 || f0y != 0.0 || f0z != 0.0) {
+            atomicAdd(fa + 0, (unsigned long long)og_to_fix(f0x));
+            atomicAdd(fa + 1, (unsigned long long)og_to_fix(f0y));
+            atomicAdd(fa + 2, (unsigned long long)og_to_fix(f0z));
+        }
+        if (f1x != 0.0 || f1y != 0.0 || f1z != 0.0) {
+            atomicAdd(fb + 0, (unsigned long long)og_to_fix(f1x));
+            atomicAdd(fb + 1, (unsigned long long)og_to_fix(f1y));
+            atomicAdd(fb + 2, (unsigned long long)og_to_fix(f1z));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        e_vdw += __shfl_xor_sync(0xffffffffu, e_vdw, o);
+        e_ele += __shfl_xor_sync(0xffffffffu, e_ele, o);
+    }
+    if (VIR) {
+        for (int q = 0; q < 9; q++)
+            for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    }
+    if (lane == 0) {
+        double *acc = cell_acc + (size_t)c1 * 11;
+        acc[0] = e_vdw;
+        acc[1] = e_ele;
+        if (VIR)
+            for (int q = 0; q < 9; q++) acc[2 + q] = v[q];
+    }
+}
+
+template __global__ void k_pair_ljzd<true>(const int *, const int *, const SysDev *, const double *, const float4 *,
+                                           const int *, const int *, const int2 *, const unsigned long long *,
+                                           const float2 *, unsigned long long *, double *, long long);
+template __global__ void k_pair_ljzd<false>(const int *, const int *, const SysDev *, const double *, const float4 *,
+                                            const int *, const int *, const int2 *, const unsigned long long *,
+                                            const float2 *, unsigned long long *, double *, long long);
+
+}  // namespace og

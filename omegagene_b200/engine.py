@@ -1,0 +1,357 @@
+"""Python host mirror of the engine's C ABI (include/omegagene_b200.h).
+
+The compute path is the CUDA library ``libomegagene_b200.so`` built in-tree for sm_100a; this
+module only marshals arrays.  There is no fallback: loading fails loudly when the library is
+missing or no CUDA device is present.
+
+The run parameters use the reference's config keys (src/celeste/core/Config.cpp:37-367), so a
+``.cls`` launch set plus an ``md.inp.run``-style option list describes a system exactly as it
+does for ``omegagene --cfg md.inp.run --inp md.inp.cls``.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import cls_io
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libomegagene_b200.so")
+
+OG_OK, OG_ERR_INVALID, OG_ERR_CUDA, OG_ERR_CAPACITY, OG_ERR_STATE, OG_ERR_NOMEM, OG_ERR_NOT_CONVERGED = range(7)
+ENERGY_NAMES = ["vdw", "ele", "bond", "angle", "potential", "kinetic", "temperature", "total", "ele_excess",
+                "ele_self", "mcmd_factor"]
+N_ENERGY = len(ENERGY_NAMES)
+
+
+class OgError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("og status %d: %s" % (status, msg))
+        self.status = status
+
+
+_p = C.POINTER
+
+
+class SystemDesc(C.Structure):
+    _fields_ = [
+        ("n_atoms", C.c_int32), ("pbc_val", C.c_double * 12),
+        ("crd", _p(C.c_double)), ("vel", _p(C.c_double)), ("charge", _p(C.c_double)), ("mass", _p(C.c_double)),
+        ("atom_type", _p(C.c_int32)), ("n_lj_types", C.c_int32), ("lj6", _p(C.c_double)), ("lj12", _p(C.c_double)),
+        ("n_excl", C.c_int32), ("excl", _p(C.c_int32)),
+        ("n_shake_pair", C.c_int32), ("shake_pair", _p(C.c_int32)), ("shake_pair_dist", _p(C.c_double)),
+        ("n_shake_trio", C.c_int32), ("shake_trio", _p(C.c_int32)), ("shake_trio_dist", _p(C.c_double)),
+        ("n_bonds", C.c_int32), ("bond", _p(C.c_int32)), ("bond_k", _p(C.c_double)), ("bond_r0", _p(C.c_double)),
+        ("n_angles", C.c_int32), ("angle", _p(C.c_int32)), ("angle_k", _p(C.c_double)), ("angle_t0", _p(C.c_double)),
+        ("n_com_groups", C.c_int32), ("com_group_start", _p(C.c_int32)), ("com_group_atoms", _p(C.c_int32)),
+        ("cutoff", C.c_double), ("nsgrid_cutoff", C.c_double), ("nsgrid_update_intvl", C.c_int32),
+        ("time_step", C.c_double), ("thermostat", C.c_int32), ("temperature", C.c_double),
+        ("temperature_init", C.c_double), ("heating_steps", C.c_int32), ("berendsen_tau", C.c_double),
+        ("const_max_loops", C.c_int32), ("const_tolerance", C.c_double),
+        ("thermo_const_max_loops", C.c_int32), ("thermo_const_tolerance", C.c_double),
+        ("mcmd_order", C.c_int32), ("mcmd_lambda_low", C.c_double), ("mcmd_lambda_high", C.c_double),
+        ("mcmd_temperature", C.c_double), ("mcmd_coef", _p(C.c_double)),
+    ]
+
+
+_lib = None
+
+
+def load_library():
+    """Loads the in-tree CUDA library (raises if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise OgError(OG_ERR_STATE, "%s is missing: run `python -c 'import __graft_entry__ as g; g.build()'`"
+                      % LIB_PATH)
+    L = C.CDLL(LIB_PATH)
+    E = C.c_void_p
+    sig = {
+        "og_create": [C.c_int, _p(E)], "og_destroy": [E], "og_add_system": [E, _p(SystemDesc), _p(C.c_int32)],
+        "og_finalize": [E], "og_step": [E, C.c_int32], "og_compute_forces": [E],
+        "og_set_state": [E, C.c_int32, C.c_void_p, C.c_void_p], "og_get_state": [E, C.c_int32, C.c_void_p, C.c_void_p],
+        "og_get_forces": [E, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p],
+        "og_get_energies": [E, C.c_int32, C.c_void_p],
+        "og_get_grid_info": [E, C.c_int32, _p(C.c_int32), _p(C.c_int32), _p(C.c_int32)],
+        "og_get_grid": [E, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p],
+        "og_get_cell_pairs": [E, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+        "og_set_trace": [E, C.c_int32], "og_get_trace": [E, C.c_void_p, C.c_int32, _p(C.c_int32)],
+        "og_get_stats": [E, _p(C.c_int64), _p(C.c_double), _p(C.c_double)],
+        "og_get_sizes": [E, _p(C.c_int32), _p(C.c_int64)], "og_set_timing": [E, C.c_int32],
+        "og_get_flags": [E, _p(C.c_int32)],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    L.og_last_error.argtypes = [E]
+    L.og_last_error.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def _ptr(a, ctype):
+    return a.ctypes.data_as(_p(ctype)) if a is not None and a.size else None
+
+
+DEFAULT_PARAMS = {
+    "cutoff": 12.0, "nsgrid_cutoff": 13.0, "nsgrid_update_intvl": 1, "time_step": 2.0, "thermostat": "none",
+    "temperature": 300.0, "temperature_init": -1.0, "heating_steps": 0, "berendsen_tau": 0.0,
+    "const_max_loops": 1000, "const_tolerance": 1e-7, "thermo_const_max_loops": 100,
+    "thermo_const_tolerance": 1e-5, "com_motion": "cancel", "com_cancel_groups": None, "constraint": "shake",
+}
+
+
+def parse_run_config(text):
+    """Parses the hot-path keys of an ``md.inp.run`` file (Config.cpp:9-35 tokeniser: whitespace
+    separated `--key value`, `;` and `#` start comments).  Keys this engine does not implement
+    raise ValueError, as unknown keys do in the reference (Config.cpp:359-362)."""
+    toks = []
+    for line in text.splitlines():
+        for c in ";#":
+            line = line.split(c)[0]
+        toks += line.split()
+    p = dict(DEFAULT_PARAMS)
+    groups = []
+    accepted_ignored = {"--processor", "--gpu-device-id", "--mode", "--n-steps", "--print-interval-log",
+                        "--print-interval-coord", "--fn-o-coord", "--format-o-coord", "--group-o-coord",
+                        "--fn-o-log", "--fn-o-energy", "--fn-o-restart", "--integrator", "--electrostatic",
+                        "--ele-alpha", "--expected-num-density", "--random-seed"}
+    i = 0
+    while i < len(toks):
+        k = toks[i]
+        v = toks[i + 1] if i + 1 < len(toks) else None
+        i += 2
+        if k == "--cutoff":
+            p["cutoff"] = float(v)
+        elif k == "--nsgrid-cutoff":
+            p["nsgrid_cutoff"] = float(v)
+        elif k == "--nsgrid-update-intvl":
+            p["nsgrid_update_intvl"] = int(v)
+        elif k == "--time-step":
+            p["time_step"] = float(v)
+        elif k == "--thermostat":
+            p["thermostat"] = v
+        elif k == "--temperature":
+            p["temperature"] = float(v)
+        elif k == "--temperature-init":
+            p["temperature_init"] = float(v)
+        elif k == "--heating-steps":
+            p["heating_steps"] = int(v)
+        elif k == "--berendsen-tau":
+            p["berendsen_tau"] = float(v) * 1000.0  # Config.cpp:162-164
+        elif k == "--const-max-loops":
+            p["const_max_loops"] = int(v)
+        elif k == "--const-tolerance":
+            p["const_tolerance"] = float(v)
+        elif k == "--thermo-const-max-loops":
+            p["thermo_const_max_loops"] = int(v)
+        elif k == "--thermo-const-tolerance":
+            p["thermo_const_tolerance"] = float(v)
+        elif k == "--com-motion":
+            p["com_motion"] = v
+        elif k == "--com-cancel-group-name":
+            groups.append(v)
+        elif k == "--constraint":
+            p["constraint"] = v
+        elif k in accepted_ignored:
+            if k == "--integrator" and v != "leapfrog-presto":
+                raise ValueError("only --integrator leapfrog-presto is on the hot path")
+            if k == "--electrostatic" and v != "zero-dipole":
+                raise ValueError("only --electrostatic zero-dipole is on the hot path")
+            if k == "--ele-alpha" and float(v) != 0.0:
+                raise ValueError("only --ele-alpha 0 is on the hot path")
+        else:
+            raise ValueError("unsupported config key %s" % k)
+    if groups:
+        p["com_cancel_groups"] = groups
+    return p
+
+
+class _Keep:
+    """Holds the numpy arrays a SystemDesc points into."""
+
+
+def make_desc(system, params=None, mcmd=None):
+    """Builds an og_system_desc from a launch-set dict (cls_io.read_cls or systems.*)."""
+    prm = dict(DEFAULT_PARAMS)
+    prm.update(params or {})
+    keep = _Keep()
+    t = system["topol"]
+    n = int(system["n_atoms"])
+    keep.crd = np.ascontiguousarray(system["crd"], np.float64).reshape(-1)
+    keep.vel = np.ascontiguousarray(system.get("vel", np.zeros((n, 3))), np.float64).reshape(-1)
+    keep.charge = np.ascontiguousarray(t["charge"], np.float64)
+    keep.mass = np.ascontiguousarray(t["mass"], np.float64)
+    keep.type = np.ascontiguousarray(t["atom_type"], np.int32)
+    c6, c12 = cls_io.lj_tables(t)
+    keep.lj6 = np.ascontiguousarray(c6.reshape(-1))
+    keep.lj12 = np.ascontiguousarray(c12.reshape(-1))
+    keep.excl = np.ascontiguousarray(np.asarray(t["nb15off_pairs"], np.int32).reshape(-1))
+    d = SystemDesc()
+    d.n_atoms = n
+    for i in range(12):
+        d.pbc_val[i] = float(system["pbc_val"][i])
+    d.crd, d.vel = _ptr(keep.crd, C.c_double), _ptr(keep.vel, C.c_double)
+    d.charge, d.mass = _ptr(keep.charge, C.c_double), _ptr(keep.mass, C.c_double)
+    d.atom_type = _ptr(keep.type, C.c_int32)
+    d.n_lj_types = int(t["n_lj_types"])
+    d.lj6, d.lj12 = _ptr(keep.lj6, C.c_double), _ptr(keep.lj12, C.c_double)
+    d.n_excl = len(keep.excl) // 2
+    d.excl = _ptr(keep.excl, C.c_int32)
+    cons = system.get("constraint") if prm["constraint"] in ("shake", "shake-settle", "settle") else None
+    if cons is not None:
+        keep.sp = np.ascontiguousarray(np.asarray(cons["pair_atoms"], np.int32).reshape(-1))
+        keep.spd = np.ascontiguousarray(np.asarray(cons["pair_dist"], np.float64).reshape(-1))
+        keep.st = np.ascontiguousarray(np.asarray(cons["trio_atoms"], np.int32).reshape(-1))
+        keep.std = np.ascontiguousarray(np.asarray(cons["trio_dist"], np.float64).reshape(-1))
+        if len(np.asarray(cons.get("quad_atoms", np.zeros((0, 4))))):
+            raise ValueError("SHAKE quads are not on the hot path of these workloads")
+        d.n_shake_pair, d.shake_pair, d.shake_pair_dist = len(keep.spd), _ptr(keep.sp, C.c_int32), _ptr(keep.spd, C.c_double)
+        d.n_shake_trio, d.shake_trio, d.shake_trio_dist = len(keep.st) // 3, _ptr(keep.st, C.c_int32), _ptr(keep.std, C.c_double)
+    b = t.get("bonds")
+    if b is not None and len(b):
+        keep.bond = np.ascontiguousarray(np.stack([b["a1"], b["a2"]], 1).astype(np.int32).reshape(-1))
+        keep.bk, keep.br0 = np.ascontiguousarray(b["k"], np.float64), np.ascontiguousarray(b["r0"], np.float64)
+        d.n_bonds, d.bond, d.bond_k, d.bond_r0 = len(b), _ptr(keep.bond, C.c_int32), _ptr(keep.bk, C.c_double), _ptr(keep.br0, C.c_double)
+    a = t.get("angles")
+    if a is not None and len(a):
+        keep.angle = np.ascontiguousarray(np.stack([a["a1"], a["a2"], a["a3"]], 1).astype(np.int32).reshape(-1))
+        keep.ak, keep.at0 = np.ascontiguousarray(a["k"], np.float64), np.ascontiguousarray(a["t0"], np.float64)
+        d.n_angles, d.angle, d.angle_k, d.angle_t0 = len(a), _ptr(keep.angle, C.c_int32), _ptr(keep.ak, C.c_double), _ptr(keep.at0, C.c_double)
+    if prm["com_motion"] == "cancel" and "groups" in system:
+        names = prm["com_cancel_groups"] or system["groups"]["names"]
+        lists = [np.asarray(system["groups"]["atoms"][system["groups"]["names"].index(nm)], np.int32) for nm in names]
+        keep.gstart = np.ascontiguousarray(np.concatenate([[0], np.cumsum([len(x) for x in lists])]).astype(np.int32))
+        keep.gatoms = np.ascontiguousarray(np.concatenate(lists).astype(np.int32))
+        d.n_com_groups, d.com_group_start, d.com_group_atoms = len(lists), _ptr(keep.gstart, C.c_int32), _ptr(keep.gatoms, C.c_int32)
+    d.cutoff, d.nsgrid_cutoff = prm["cutoff"], prm["nsgrid_cutoff"]
+    d.nsgrid_update_intvl, d.time_step = prm["nsgrid_update_intvl"], prm["time_step"]
+    d.thermostat = 1 if prm["thermostat"] == "scaling" else 0
+    d.temperature, d.temperature_init = prm["temperature"], prm["temperature_init"]
+    d.heating_steps, d.berendsen_tau = prm["heating_steps"], prm["berendsen_tau"]
+    d.const_max_loops, d.const_tolerance = prm["const_max_loops"], prm["const_tolerance"]
+    d.thermo_const_max_loops, d.thermo_const_tolerance = prm["thermo_const_max_loops"], prm["thermo_const_tolerance"]
+    d.mcmd_order = -1
+    if mcmd is not None:
+        keep.mcoef = np.ascontiguousarray(mcmd["coef"], np.float64)
+        d.mcmd_order = len(keep.mcoef) - 1
+        d.mcmd_lambda_low, d.mcmd_lambda_high = mcmd["lambda_low"], mcmd["lambda_high"]
+        d.mcmd_temperature = mcmd["temperature"]
+        d.mcmd_coef = _ptr(keep.mcoef, C.c_double)
+    return d, keep
+
+
+class Engine:
+    """One engine = one CUDA context user holding a batch of independent systems."""
+
+    def __init__(self, device=0):
+        self.L = load_library()
+        self.h = C.c_void_p()
+        self._check(self.L.og_create(int(device), C.byref(self.h)), "og_create")
+        self.n_atoms = []
+        self._keep = []
+
+    def _check(self, status, what=""):
+        if status != OG_OK:
+            msg = self.L.og_last_error(self.h).decode() if self.h else ""
+            raise OgError(status, "%s: %s" % (what, msg))
+
+    def close(self):
+        if self.h:
+            self.L.og_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_system(self, system, params=None, mcmd=None):
+        d, keep = make_desc(system, params, mcmd)
+        sid = C.c_int32()
+        self._check(self.L.og_add_system(self.h, C.byref(d), C.byref(sid)), "og_add_system")
+        self._keep.append(keep)
+        self.n_atoms.append(int(system["n_atoms"]))
+        return sid.value
+
+    def finalize(self):
+        self._check(self.L.og_finalize(self.h), "og_finalize")
+        self._keep = []
+
+    def step(self, n=1):
+        self._check(self.L.og_step(self.h, int(n)), "og_step")
+
+    def compute_forces(self):
+        self._check(self.L.og_compute_forces(self.h), "og_compute_forces")
+
+    def set_state(self, sys, crd=None, vel_next=None):
+        c = None if crd is None else np.ascontiguousarray(crd, np.float64).reshape(-1)
+        v = None if vel_next is None else np.ascontiguousarray(vel_next, np.float64).reshape(-1)
+        self._check(self.L.og_set_state(self.h, sys, c.ctypes.data if c is not None else None,
+                                        v.ctypes.data if v is not None else None), "og_set_state")
+
+    def get_state(self, sys):
+        n = self.n_atoms[sys]
+        crd, vel = np.zeros((n, 3)), np.zeros((n, 3))
+        self._check(self.L.og_get_state(self.h, sys, crd.ctypes.data, vel.ctypes.data), "og_get_state")
+        return crd, vel
+
+    def get_forces(self, sys):
+        n = self.n_atoms[sys]
+        work, ene, vir = np.zeros((n, 3)), np.zeros(N_ENERGY), np.zeros(9)
+        self._check(self.L.og_get_forces(self.h, sys, work.ctypes.data, ene.ctypes.data, vir.ctypes.data),
+                    "og_get_forces")
+        return work, dict(zip(ENERGY_NAMES, ene)), vir.reshape(3, 3)
+
+    def get_energies(self, sys):
+        ene = np.zeros(N_ENERGY)
+        self._check(self.L.og_get_energies(self.h, sys, ene.ctypes.data), "og_get_energies")
+        return dict(zip(ENERGY_NAMES, ene))
+
+    def grid_info(self, sys):
+        nc, ncol, npair = C.c_int32(), C.c_int32(), C.c_int32()
+        self._check(self.L.og_get_grid_info(self.h, sys, C.byref(nc), C.byref(ncol), C.byref(npair)), "grid_info")
+        return nc.value, ncol.value, npair.value
+
+    def get_grid(self, sys):
+        nc, ncol, _ = self.grid_info(sys)
+        sa = np.zeros(8 * nc, np.int32)
+        sc = np.zeros((8 * nc, 3))
+        ch = np.zeros(ncol + 1, np.int32)
+        self._check(self.L.og_get_grid(self.h, sys, sa.ctypes.data, sc.ctypes.data, ch.ctypes.data), "og_get_grid")
+        return {"n_cells": nc, "slot_atomid": sa, "slot_crd": sc, "col_head_cell": ch}
+
+    def get_cell_pairs(self, sys):
+        nc, _, npair = self.grid_info(sys)
+        head = np.zeros(nc + 1, np.int32)
+        c1, c2, img = (np.zeros(npair, np.int32) for _ in range(3))
+        mask = np.zeros(npair, np.uint64)
+        self._check(self.L.og_get_cell_pairs(self.h, sys, head.ctypes.data, c1.ctypes.data, c2.ctypes.data,
+                                             img.ctypes.data, mask.ctypes.data), "og_get_cell_pairs")
+        return {"idx_head": head, "cell1": c1, "cell2": c2, "image": img, "mask": mask, "n_pairs": npair}
+
+    def set_trace(self, capacity):
+        self._check(self.L.og_set_trace(self.h, int(capacity)), "og_set_trace")
+
+    def get_trace(self, max_steps):
+        n_sys = len(self.n_atoms)
+        out = np.zeros((max_steps, n_sys, N_ENERGY))
+        n = C.c_int32()
+        self._check(self.L.og_get_trace(self.h, out.ctypes.data, int(max_steps), C.byref(n)), "og_get_trace")
+        return out[:n.value]
+
+    def set_timing(self, on=True):
+        self._check(self.L.og_set_timing(self.h, 1 if on else 0), "og_set_timing")
+
+    def stats(self):
+        k, p, s = C.c_int64(), C.c_double(), C.c_double()
+        self._check(self.L.og_get_stats(self.h, C.byref(k), C.byref(p), C.byref(s)), "og_get_stats")
+        return {"kernel_launches": k.value, "pair_kernel_ms": p.value, "step_ms": s.value}
+
+    def flags(self):
+        f = C.c_int32()
+        self._check(self.L.og_get_flags(self.h, C.byref(f)), "og_get_flags")
+        return f.value

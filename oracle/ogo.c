@@ -314,6 +314,9 @@ int ogo_enumerate_cell_pairs(const ogo_geom *g, const ogo_pbc *p, const ogo_grid
                     int lo = uni_lo[fu], hi = uni_hi[lu];
                     if (lo > hi || head2 < 0) continue;
                     int first_cell = head2 + lo, last_cell = head2 + hi;
+                    /* z indices stay inside column 2, as in the engine */
+                    int ncz2 = (gr->col_n_atoms[col2] + OGO_N_ATOM_CELL - 1) / OGO_N_ATOM_CELL;
+                    if (last_cell > head2 + ncz2 - 1) last_cell = head2 + ncz2 - 1;
                     for (int c2 = first_cell; c2 <= last_cell; c2++) {
                         float z2t = (float)gr->slot_crd[(c2 * OGO_N_ATOM_CELL + OGO_N_ATOM_CELL - 1) * 3 + 2]
                                     + (float)iz * p->L[2];

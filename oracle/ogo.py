@@ -282,3 +282,205 @@ def ref_minicell(pbc_val, crd, nb15off, nsgrid_cutoff, density=1.0, expected_pai
         "cell1": c1[:npairs].copy(), "cell2": c2[:npairs].copy(), "image": img[:npairs].copy(),
         "mask": m[0::2] | (m[1::2] << np.uint64(32)),
     }
+
+
+# ------------------------------------------------------------------ oracle MD driver
+
+class Integ(C.Structure):
+    _fields_ = [("n", C.c_int), ("dt", C.c_double),
+                ("crd", C.POINTER(C.c_double)), ("crd_prev", C.POINTER(C.c_double)), ("vel", C.POINTER(C.c_double)),
+                ("vel_next", C.POINTER(C.c_double)), ("work", C.POINTER(C.c_double)),
+                ("mass", C.POINTER(C.c_float)), ("mass_inv", C.POINTER(C.c_float)),
+                ("n_pair", C.c_int), ("n_trio", C.c_int), ("pair_atoms", C.POINTER(C.c_int)),
+                ("pair_dist2", C.POINTER(C.c_double)), ("trio_atoms", C.POINTER(C.c_int)),
+                ("trio_dist2", C.POINTER(C.c_double)), ("shake_max_loops", C.c_int), ("shake_tol", C.c_double),
+                ("n_com_groups", C.c_int), ("com_group_start", C.POINTER(C.c_int)),
+                ("com_group_atoms", C.POINTER(C.c_int)), ("com_mass_inv", C.POINTER(C.c_float)),
+                ("thermostat", C.c_int), ("temperature", C.c_double), ("temperature_coeff", C.c_double),
+                ("tau_inv", C.c_double), ("thermo_max_loops", C.c_int), ("thermo_tol", C.c_double),
+                ("buf_crd", C.POINTER(C.c_double))]
+
+
+def _bind_integ(L):
+    if getattr(L, "_integ_bound", False):
+        return
+    ip = C.POINTER(Integ)
+    for name in ("ogo_update_velocities", "ogo_thermostat_scaling", "ogo_update_coordinates",
+                 "ogo_set_velocity_from_crd"):
+        getattr(L, name).argtypes = [ip]
+    L.ogo_cancel_com.argtypes = [ip, C.POINTER(C.c_double)]
+    L.ogo_shake.argtypes = [ip, C.POINTER(Pbc)]
+    L.ogo_thermostat_with_shake.argtypes = [ip, C.POINTER(Pbc)]
+    L.ogo_revise_pbc.argtypes = [C.POINTER(Pbc), C.c_int, f64p]
+    L.ogo_kinetic.argtypes = [ip, C.c_void_p]
+    L.ogo_kinetic.restype = C.c_double
+    L._integ_bound = True
+
+
+class OracleMD:
+    """The reference's leapfrog-presto step (DynamicsModePresto::calc_in_each_step,
+    DynamicsMode.cpp:468-560) on the C oracle, with FP64 forces: pair LJ + ZD over the
+    reference's cell-pair list evaluated on the list's (unwrapped) grid positions, excess ZD
+    pairs and bonds/angles with the minimum image.  ``params`` uses engine.DEFAULT_PARAMS keys."""
+
+    def __init__(self, system, params, mcmd=None):
+        from omegagene_b200 import cls_io  # local import: oracle stays importable alone
+        self.L = L = lib()
+        _bind_integ(L)
+        t = system["topol"]
+        self.n = n = int(system["n_atoms"])
+        self.p = dict(params)
+        self.pbc = make_pbc(system["pbc_val"])
+        self.Ld = np.array(self.pbc.L, np.float32).astype(np.float64)
+        self.geom = make_geom(self.pbc, n, self.p["nsgrid_cutoff"])
+        self.nb = cls_io.nb15off_table(n, t["nb15off_pairs"])
+        self.ep = excess_pairs(n, self.nb).reshape(-1).astype(np.int32)
+        self.q64 = np.ascontiguousarray(t["charge"], np.float64)
+        self.q32 = self.q64.astype(np.float32)
+        self.ty = np.ascontiguousarray(t["atom_type"], np.int32)
+        c6, c12 = cls_io.lj_tables(t)
+        self.c6, self.c12, self.nt = c6.reshape(-1).copy(), c12.reshape(-1).copy(), int(t["n_lj_types"])
+        z, b, f = zd_constants(self.p["cutoff"])
+        self.zcore = z
+        self.self_e = L.ogo_self_energy(n, len(self.ep) // 2, self.ep, self.q32, z)
+        self.mass = np.ascontiguousarray(t["mass"], np.float64).astype(np.float32)
+        self.mass_inv = (1.0 / self.mass.astype(np.float64)).astype(np.float32)
+        crd = wrap_inbox(self.pbc, system["crd"]).reshape(-1)
+        self.crd = np.ascontiguousarray(crd)
+        L.ogo_revise_pbc(C.byref(self.pbc), n, self.crd)
+        self.crd_prev = np.zeros(3 * n)
+        self.vel = np.zeros(3 * n)
+        self.vel_next = np.ascontiguousarray(np.asarray(system["vel"], np.float64).reshape(-1)).copy()
+        self.work = np.zeros(3 * n)
+        self.buf = np.zeros(3 * n)
+        b = t.get("bonds")
+        self.bonds = None
+        if b is not None and len(b):
+            self.bonds = (np.stack([b["a1"], b["a2"]], 1).astype(np.int32).reshape(-1), np.asarray(b["k"], np.float64),
+                          np.asarray(b["r0"], np.float64))
+        a = t.get("angles")
+        self.angles = None
+        if a is not None and len(a):
+            self.angles = (np.stack([a["a1"], a["a2"], a["a3"]], 1).astype(np.int32).reshape(-1),
+                           np.asarray(a["k"], np.float64), np.asarray(a["t0"], np.float64))
+        cons = system.get("constraint")
+        use_cons = cons is not None and self.p.get("constraint", "shake") != "none"
+        self.pa = np.asarray(cons["pair_atoms"], np.int32).reshape(-1) if use_cons else np.zeros(0, np.int32)
+        self.pd2 = (np.asarray(cons["pair_dist"], np.float64) ** 2).reshape(-1) if use_cons else np.zeros(0)
+        self.ta = np.asarray(cons["trio_atoms"], np.int32).reshape(-1) if use_cons else np.zeros(0, np.int32)
+        self.td2 = (np.asarray(cons["trio_dist"], np.float64) ** 2).reshape(-1) if use_cons else np.zeros(0)
+        self.has_cons = len(self.pd2) + len(self.td2) > 0
+        n_cdist = len(self.pd2) + len(self.td2)
+        self.d_free = 3 * n - 3 - n_cdist
+        gs, ga, gmi = [0], [], []
+        if self.p.get("com_motion", "cancel") == "cancel" and "groups" in system:
+            names = self.p.get("com_cancel_groups") or system["groups"]["names"]
+            for nm in names:
+                atoms = np.asarray(system["groups"]["atoms"][system["groups"]["names"].index(nm)], np.int32)
+                ga.extend(atoms.tolist())
+                gs.append(len(ga))
+                ms = np.float32(0)
+                for x in atoms:
+                    ms = np.float32(ms + self.mass[x])
+                gmi.append(np.float32(1.0 / np.float64(ms)))
+        self.gs, self.ga, self.gmi = (np.asarray(gs, np.int32), np.asarray(ga if ga else [0], np.int32),
+                                      np.asarray(gmi if gmi else [1.0], np.float32))
+        self.t0 = self.p["temperature"]
+        self.tinit = self.p["temperature"] if self.p.get("temperature_init", -1) < 0 else self.p["temperature_init"]
+        tau = self.p.get("berendsen_tau", 0.0)
+        if self.p["time_step"] < tau:
+            tau = self.p["time_step"]
+        self.tau_inv = (1.0 / tau) if tau > 0 else float("inf")
+        self.mcmd = mcmd
+        self.step_i = 0
+        self.cl = None
+        self.slot_crd = None
+        self.I = Integ()
+        I = self.I
+        I.n, I.dt = n, self.p["time_step"]
+        for nm in ("crd", "crd_prev", "vel", "vel_next", "work"):
+            setattr(I, nm, getattr(self, nm).ctypes.data_as(C.POINTER(C.c_double)))
+        I.buf_crd = self.buf.ctypes.data_as(C.POINTER(C.c_double))
+        I.mass = self.mass.ctypes.data_as(C.POINTER(C.c_float))
+        I.mass_inv = self.mass_inv.ctypes.data_as(C.POINTER(C.c_float))
+        I.n_pair, I.n_trio = len(self.pd2), len(self.td2) // 3
+        I.pair_atoms = self.pa.ctypes.data_as(C.POINTER(C.c_int))
+        I.pair_dist2 = self.pd2.ctypes.data_as(C.POINTER(C.c_double))
+        I.trio_atoms = self.ta.ctypes.data_as(C.POINTER(C.c_int))
+        I.trio_dist2 = self.td2.ctypes.data_as(C.POINTER(C.c_double))
+        I.shake_max_loops, I.shake_tol = self.p["const_max_loops"], self.p["const_tolerance"]
+        I.n_com_groups = len(self.gs) - 1
+        I.com_group_start = self.gs.ctypes.data_as(C.POINTER(C.c_int))
+        I.com_group_atoms = self.ga.ctypes.data_as(C.POINTER(C.c_int))
+        I.com_mass_inv = self.gmi.ctypes.data_as(C.POINTER(C.c_float))
+        I.thermostat = 1 if self.p["thermostat"] == "scaling" else 0
+        I.temperature = self.t0
+        I.temperature_coeff = (2.0 * 4.184 * 1e3) / (8.31451 * self.d_free) * ((1e7 / (4.184 * 1e3)) * 0.5)
+        I.tau_inv = self.tau_inv
+        I.thermo_max_loops, I.thermo_tol = self.p["thermo_const_max_loops"], self.p["thermo_const_tolerance"]
+        self.energies = {}
+
+    def rebuild(self):
+        self.cl = CellList(self.pbc, self.geom, self.crd, self.nb)
+        self.slot_crd = self.cl.slot_crd.copy()
+
+    def forces(self, virial=False):
+        """FP64 forces at the current positions into self.work; returns energies."""
+        if self.cl is None or self.step_i % self.p["nsgrid_update_intvl"] == 0:
+            self.rebuild()
+        n = self.n
+        pos = np.ascontiguousarray(self.slot_crd[self.cl.atomids_rev].reshape(-1))
+        w = np.zeros(3 * n)
+        e = np.zeros(2)
+        vir = np.zeros(9)
+        self.L.ogo_pair_cells_f64(self.Ld, self.cl._grid, self.cl._cps, pos, self.q64, self.ty, self.nt, self.c6,
+                                  self.c12, float(self.p["cutoff"]), w, e, vir)
+        vexc = np.zeros(9)
+        exc = self.L.ogo_excess_f64(self.Ld, len(self.ep) // 2, self.ep, self.crd, self.q64, float(self.p["cutoff"]),
+                                    w, vexc)
+        eb = ea = 0.0
+        if self.bonds is not None:
+            eb = self.L.ogo_bonds(self.pbc, len(self.bonds[1]), self.bonds[0], self.bonds[1], self.bonds[2], self.crd, w)
+        if self.angles is not None:
+            ea = self.L.ogo_angles(self.pbc, len(self.angles[1]), self.angles[0], self.angles[1], self.angles[2],
+                                   self.crd, w)
+        self.work[:] = w
+        ene = {"vdw": e[0], "ele": e[1] + exc + self.self_e, "bond": eb, "angle": ea, "ele_excess": exc,
+               "ele_self": self.self_e}
+        ene["potential"] = ene["vdw"] + ene["ele"] + eb + ea
+        if virial:
+            ene["virial"] = (vir + vexc).reshape(3, 3)
+        return ene
+
+    def step(self):
+        L, I = self.L, self.I
+        ene = self.forces()
+        if self.mcmd is not None:
+            m = self.mcmd
+            coef = np.ascontiguousarray(m["coef"], np.float64)
+            ene["mcmd_factor"] = L.ogo_mcmd_scale(ene["potential"], m["lambda_low"], m["lambda_high"], len(coef) - 1,
+                                                  coef, m["temperature"], self.n, self.work)
+        L.ogo_update_velocities(C.byref(I))
+        L.ogo_cancel_com(C.byref(I), I.vel_next)
+        if I.thermostat == 1:
+            hs = self.p.get("heating_steps", 0)
+            I.temperature = (self.tinit + ((self.t0 - self.tinit) / hs) * self.step_i) if self.step_i < hs else self.t0
+            if not self.has_cons:
+                L.ogo_thermostat_scaling(C.byref(I))
+        L.ogo_update_coordinates(C.byref(I))
+        if self.has_cons:
+            if I.thermostat == 1:
+                L.ogo_thermostat_with_shake(C.byref(I), C.byref(self.pbc))
+            else:
+                L.ogo_shake(C.byref(I), C.byref(self.pbc))
+                L.ogo_set_velocity_from_crd(C.byref(I))
+        # MiniCell::move_atom, then the PBC wrap
+        self.slot_crd[self.cl.atomids_rev] += (self.crd - self.crd_prev).reshape(-1, 3)
+        L.ogo_revise_pbc(C.byref(self.pbc), self.n, self.crd)
+        kin = L.ogo_kinetic(C.byref(I), None)
+        ene["kinetic"] = kin
+        ene["temperature"] = kin * (1.0 / (8.31451 * self.d_free) * 4.184 * 1e3 * 2.0)
+        ene["total"] = ene["potential"] + kin
+        self.step_i += 1
+        self.energies = ene
+        return ene

@@ -1,0 +1,206 @@
+"""Parity of the CUDA engine (through the C ABI) with the CPU oracle.
+
+Integer / index results (grid assignment, cell-pair list, masks) must be bit-exact; forces,
+energies and the virial are compared with the FP64 oracle within the stated tolerances:
+  * force RMS relative error  sqrt(sum|F - F64|^2 / sum|F64|^2) <= 1e-5
+  * potential energy terms    |E - E64| <= 1e-6 |E64| + 2e-3 kcal/mol
+  * virial                    ||W - W64||_F <= 1e-5 ||W64||_F
+"""
+import numpy as np
+import pytest
+
+from omegagene_b200 import engine, systems
+from oracle import ogo
+
+pytestmark = pytest.mark.gpu
+
+FORCE_RTOL = 1e-5
+
+
+def _params(**kw):
+    p = dict(engine.DEFAULT_PARAMS)
+    p.update(kw)
+    return p
+
+
+def _oracle_cells(s, p):
+    from omegagene_b200 import cls_io
+    nb = cls_io.nb15off_table(s["n_atoms"], s["topol"]["nb15off_pairs"])
+    pbc = ogo.make_pbc(s["pbc_val"])
+    crd = ogo.wrap_inbox(pbc, s["crd"])
+    geom = ogo.make_geom(pbc, s["n_atoms"], p["nsgrid_cutoff"])
+    return ogo.CellList(pbc, geom, crd, nb)
+
+
+def _engine(systems_and_params):
+    eng = engine.Engine(0)
+    for s, p, m in systems_and_params:
+        eng.add_system(s, p, m)
+    eng.finalize()
+    return eng
+
+
+def _rel_rms(a, b):
+    return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
+
+
+SMALL = [
+    ("water3000", lambda: systems.water_system(3000, box=44.8, seed=0, lattice_m=15)),
+    ("water1500", lambda: systems.water_system(1500, seed=5)),
+    ("water700", lambda: systems.water_system(700, seed=9)),
+    ("chain300", lambda: systems.chain_water_system(300, 2500, seed=4, radius=12.0)),
+]
+
+
+@pytest.mark.parametrize("name,make", SMALL, ids=[n for n, _ in SMALL])
+def test_cell_list_bit_exact(name, make):
+    s = make()
+    p = _params()
+    eng = _engine([(s, p, None)])
+    ref = _oracle_cells(s, p)
+    g = eng.get_grid(0)
+    cp = eng.get_cell_pairs(0)
+    assert g["n_cells"] == ref.n_cells
+    np.testing.assert_array_equal(g["slot_atomid"], ref.slot_atomid)
+    np.testing.assert_array_equal(g["slot_crd"], ref.slot_crd)
+    np.testing.assert_array_equal(g["col_head_cell"], ref.col_head_cell)
+    assert cp["n_pairs"] == ref.n_pairs
+    for k in ("idx_head", "cell1", "cell2", "image", "mask"):
+        np.testing.assert_array_equal(cp[k], getattr(ref, k), err_msg=k)
+
+
+def test_batched_cell_lists_equal_single():
+    ss = [make() for _, make in SMALL]
+    p = _params()
+    eng = _engine([(s, p, None) for s in ss])
+    for i, s in enumerate(ss):
+        ref = _oracle_cells(s, p)
+        cp = eng.get_cell_pairs(i)
+        g = eng.get_grid(i)
+        np.testing.assert_array_equal(g["slot_atomid"], ref.slot_atomid)
+        for k in ("idx_head", "cell1", "cell2", "image", "mask"):
+            np.testing.assert_array_equal(cp[k], getattr(ref, k), err_msg="%d %s" % (i, k))
+
+
+@pytest.mark.parametrize("name,make", SMALL, ids=[n for n, _ in SMALL])
+def test_forces_energies_virial_vs_fp64(name, make):
+    s = make()
+    p = _params()
+    eng = _engine([(s, p, None)])
+    eng.compute_forces()
+    work, ene, vir = eng.get_forces(0)
+    md = ogo.OracleMD(s, p)
+    e64 = md.forces(virial=True)
+    err = _rel_rms(work, md.work.reshape(-1, 3))
+    assert err <= FORCE_RTOL, err
+    for k in ("vdw", "ele", "bond", "angle", "potential"):
+        assert abs(ene[k] - e64[k]) <= 1e-6 * abs(e64[k]) + 2e-3, (k, ene[k], e64[k])
+    w64 = e64["virial"]
+    assert np.linalg.norm(vir - w64) <= 1e-5 * np.linalg.norm(w64), (vir, w64)
+
+
+def test_forces_bitwise_reproducible():
+    s = systems.water_system(3000, box=44.8, seed=0, lattice_m=15)
+    eng = _engine([(s, _params(), None)])
+    eng.compute_forces()
+    w1, e1, _ = eng.get_forces(0)
+    eng.compute_forces()
+    w2, e2, _ = eng.get_forces(0)
+    assert np.array_equal(w1, w2)
+    assert e1 == e2
+
+
+def _run_both(s, p, n_steps, mcmd=None):
+    eng = _engine([(s, p, mcmd)])
+    eng.set_trace(n_steps)
+    md = ogo.OracleMD(s, p, mcmd)
+    ref = [md.step() for _ in range(n_steps)]
+    eng.step(n_steps)
+    tr = eng.get_trace(n_steps)[:, 0, :]
+    return eng, md, ref, tr
+
+
+def test_one_step_state_matches_oracle():
+    s = systems.water_system(1500, seed=5)
+    p = _params(nsgrid_update_intvl=10, time_step=2.0)
+    eng, md, ref, tr = _run_both(s, p, 1)
+    crd, vel = eng.get_state(0)
+    assert np.max(np.abs(crd.reshape(-1) - md.crd)) < 1e-6
+    assert np.max(np.abs(vel.reshape(-1) - md.vel_next)) < 1e-6
+
+
+@pytest.mark.parametrize("thermostat,dt", [("none", 2.0), ("scaling", 0.5)])
+def test_energy_trace_matches_oracle(thermostat, dt):
+    s = systems.water_system(1500, seed=5)
+    p = _params(nsgrid_update_intvl=10, time_step=dt, thermostat=thermostat, temperature=300.0)
+    eng, md, ref, tr = _run_both(s, p, 12)
+    names = engine.ENERGY_NAMES
+    for i, r in enumerate(ref):
+        for k in ("potential", "kinetic", "total", "vdw", "ele"):
+            got = tr[i, names.index(k)]
+            assert abs(got - r[k]) <= 1e-5 * abs(r[k]) + 5e-3, (i, k, got, r[k])
+
+
+def test_chain_with_bonds_angles_shake_pairs_matches_oracle():
+    s = systems.chain_water_system(300, 2500, seed=4, radius=12.0)
+    p = _params(nsgrid_update_intvl=10, time_step=2.0, thermostat="scaling", temperature=300.0)
+    eng, md, ref, tr = _run_both(s, p, 8)
+    names = engine.ENERGY_NAMES
+    for i, r in enumerate(ref):
+        for k in ("potential", "kinetic", "bond", "angle"):
+            got = tr[i, names.index(k)]
+            assert abs(got - r[k]) <= 1e-5 * abs(r[k]) + 5e-3, (i, k, got, r[k])
+
+
+def test_mcmd_scaling_matches_oracle():
+    s = systems.chain_water_system(300, 2500, seed=6, radius=12.0)
+    p = _params(nsgrid_update_intvl=10, time_step=2.0)
+    md0 = ogo.OracleMD(s, p)
+    e0 = md0.forces()["potential"]
+    mcmd = {"coef": [1.0, 2e-5, 1e-9, 0, 0, 0, 1e-24], "lambda_low": e0 - 2000.0, "lambda_high": e0 + 2000.0,
+            "temperature": 300.0}
+    eng, md, ref, tr = _run_both(s, p, 6, mcmd)
+    names = engine.ENERGY_NAMES
+    for i, r in enumerate(ref):
+        assert abs(tr[i, names.index("mcmd_factor")] - r["mcmd_factor"]) <= 1e-9 * abs(r["mcmd_factor"])
+        assert abs(tr[i, names.index("potential")] - r["potential"]) <= 1e-5 * abs(r["potential"]) + 5e-3
+
+
+def test_batch_invariance_bitwise():
+    """A system gives the same trajectory alone and batched with others (fixed-point forces,
+    per-system fixed-order reductions)."""
+    a = systems.water_system(1500, seed=5)
+    others = [systems.water_system(700, seed=9), systems.chain_water_system(300, 2500, seed=4, radius=12.0)]
+    p = _params(nsgrid_update_intvl=10, time_step=2.0)
+    alone = _engine([(a, p, None)])
+    alone.set_trace(25)
+    alone.step(25)
+    mixed = _engine([(others[0], p, None), (a, p, None), (others[1], p, None)])
+    mixed.set_trace(25)
+    mixed.step(25)
+    np.testing.assert_array_equal(alone.get_trace(25)[:, 0, :], mixed.get_trace(25)[:, 1, :])
+    c1, v1 = alone.get_state(0)
+    c2, v2 = mixed.get_state(1)
+    assert np.array_equal(c1, c2) and np.array_equal(v1, v2)
+
+
+def test_nve_drift_small():
+    """Config-0 water: short velocity-rescaled warm-up at 0.5 fs, then NVE at 2 fs; the total
+    energy drift stays within 0.01 kcal/mol/ns per degree of freedom."""
+    s = systems.water_system(3000, box=44.8, seed=0, lattice_m=15)
+    warm = _params(nsgrid_update_intvl=10, time_step=0.5, thermostat="scaling", temperature=300.0)
+    eng = _engine([(s, warm, None)])
+    eng.step(600)
+    crd, vel = eng.get_state(0)
+    s2 = dict(s)
+    s2["crd"], s2["vel"] = crd, vel
+    nve = _params(nsgrid_update_intvl=10, time_step=2.0)
+    eng2 = _engine([(s2, nve, None)])
+    eng2.set_trace(1000)
+    eng2.step(1000)
+    tr = eng2.get_trace(1000)[:, 0, :]
+    tot = tr[:, engine.ENERGY_NAMES.index("total")]
+    t_ns = np.arange(len(tot)) * 2.0 * 1e-6
+    slope = np.polyfit(t_ns[100:], tot[100:], 1)[0]
+    dof = 3 * s["n_atoms"] - 3 - 3 * 3000
+    assert abs(slope) / dof <= 0.01, slope / dof
