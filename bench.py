@@ -1,0 +1,342 @@
+"""Benchmark of the omegagene per-step MD hot path on B200.
+
+Default workload (N=1): 333,334 rigid TIP3P waters (1,000,002 atoms) in a 215.5 A periodic box,
+NVE, dt 2 fs, SHAKE trio per water, cutoff 12 A / pair-list 13 A (list rebuilt every 10 steps),
+zero-dipole alpha 0.  Inputs are seeded synthetic (a jittered lattice, random orientations).
+
+Prints ONE JSON line.  `value` is ns/day (simulated time per wall-clock day) from CUDA events on
+the engine's stream around the timed og_step calls; `e2e` is the same metric through the C ABI
+with the state in pinned host memory, copied host->device before and device->host after every
+step.  With --gpus N (torchrun) every rank advances its own replica (replicas only: the path has
+no exchange step), `value` sums the replicas' simulated time and the time is the max over ranks.
+
+--impl reference times the reference's CPU cell-list build (oracle/_ref/omegagene_ns, compiled
+from the reference sources) on the host cores: one 9,000-atom water box per core, converted to
+the same unit (atom-steps/s at 1M atoms).
+"""
+import argparse
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ns/day@1M atoms"
+UNIT = "ns/day"
+DT_FS = 2.0
+INTVL = 10
+N_WATERS = 333334
+BOX = 215.5
+LATTICE = 70
+FLOP_PER_PAIR = 40  # FP32 FLOP per interacting pair (sub 3, r2 5, rsqrt 1, powers 4, LJ 5, ZD 6, force 3, accum 6, energy 7)
+WORKLOAD = ("333334 TIP3P waters (1000002 atoms), 215.5 A cubic box, NVE dt 2 fs, SHAKE-trio rigid water, "
+            "cutoff 12 A, pair-list cutoff 13 A rebuilt every 10 steps, zero-dipole alpha 0")
+
+
+def ns_per_day(steps_per_s, dt_fs=DT_FS):
+    return dt_fs * steps_per_s * 86400.0 / 1e6
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return None
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ reference CPU program
+
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "omegagene_ns")
+REF_RUN = """--mode md
+--integrator leapfrog-presto
+--cutoff 12.0
+--n-steps {n_steps}
+--time-step 2.0
+--electrostatic zero-dipole
+--ele-alpha 0
+--thermostat none
+--temperature 300
+--com-motion cancel
+--com-cancel-group-name all
+--print-interval-log 1
+--print-interval-coord 100000
+--fn-o-coord run.cod
+--format-o-coord presto
+--fn-o-log md.log
+--fn-o-energy md.ene
+--fn-o-restart run_o.restart
+--nsgrid-cutoff 13.0
+--nsgrid-update-intvl 10
+--constraint shake
+--const-max-loops 1000
+--const-tolerance 0.0000001
+--expected-num-density 1.0
+"""
+
+
+def reference_cpu(n_steps, warmup, cores=None, n_waters=3000, box=44.8):
+    """Runs the reference cell-list CPU program, one process (one 9,000-atom box) per core.
+    Per-step times come from its own "Comput Time" log lines (cumulative CPU seconds of the MD
+    loop, DynamicsMode.cpp:339-340).  Returns atom-steps/s summed over processes."""
+    from omegagene_b200 import cls_io, systems  # the generator and the .cls writer
+    if not os.path.exists(REF_BIN):
+        return None, "oracle/_ref/omegagene_ns was not built (reference sources absent at build time)"
+    cores = cores or os.cpu_count() or 1
+    work = tempfile.mkdtemp(prefix="ogref_")
+    procs = []
+    n_atoms = 3 * n_waters
+    for c in range(cores):
+        d = os.path.join(work, "p%d" % c)
+        os.makedirs(d)
+        s = systems.water_system(n_waters, box=box, seed=100 + c, lattice_m=15)
+        # empty restraint sections: the reference allocates the restraint arrays only while
+        # loading them and frees them at exit (Read.cpp:86-95, DynamicsMode.cpp:178-179)
+        s["raw"] = {"dist_restraint": b"\0\0\0\0", "pos_restraint": b"\0\0\0\0"}
+        cls_io.write_cls(os.path.join(d, "md.inp.cls"), s)
+        open(os.path.join(d, "md.inp.run"), "w").write(REF_RUN.format(n_steps=n_steps + warmup))
+        procs.append(subprocess.Popen([REF_BIN, "--cfg", "md.inp.run", "--inp", "md.inp.cls"], cwd=d,
+                                      stdout=open(os.path.join(d, "out.txt"), "w"), stderr=subprocess.STDOUT))
+    per_step = []
+    for c, p in enumerate(procs):
+        p.wait()
+        txt = open(os.path.join(work, "p%d" % c, "out.txt")).read()
+        t = [float(x) for x in re.findall(r"Comput Time:\s+([0-9.eE+-]+)", txt)]
+        if p.returncode != 0 or len(t) < n_steps + warmup:
+            shutil.rmtree(work, ignore_errors=True)
+            return None, "reference program failed (rc=%s, %d steps logged)" % (p.returncode, len(t))
+        per_step.append((t[warmup + n_steps - 1] - t[warmup - 1]) / n_steps if warmup > 0 else t[n_steps - 1] / n_steps)
+    shutil.rmtree(work, ignore_errors=True)
+    atom_steps = sum(n_atoms / s for s in per_step)
+    return {"atom_steps_per_s": atom_steps, "cores": cores, "s_per_step": statistics.median(per_step),
+            "sample": "%d processes x %d-atom water box (44.8 A), %d timed steps after %d warm-up, reference "
+                      "CPU cell-list build (oracle/_ref/omegagene_ns)" % (cores, n_atoms, n_steps, warmup)}, None
+
+
+def cpu_ns_per_day_at_1m(atom_steps_per_s):
+    return ns_per_day(atom_steps_per_s / 1e6)
+
+
+# ------------------------------------------------------------------ distributed helpers
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(pg, x):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+# ------------------------------------------------------------------ our arm
+
+def run_ours(args, world, rank, local, pg):
+    import torch
+    from omegagene_b200 import engine, systems
+    torch.cuda.set_device(local)
+    s = systems.water_system(N_WATERS, box=BOX, seed=20 + rank, lattice_m=LATTICE)
+    p = dict(engine.DEFAULT_PARAMS)
+    p.update(nsgrid_update_intvl=INTVL, time_step=DT_FS, thermostat="none", com_cancel_groups=["all"])
+    eng = engine.Engine(local)
+    eng.add_system(s, p)
+    eng.finalize()
+    n_atoms = s["n_atoms"]
+    del s
+    # warm-up (untimed)
+    eng.step(args.warmup)
+    # interacting pairs of the current configuration (roofline numerator)
+    eng.compute_forces()
+    n_int = eng.pair_count(0)
+    n_cell_pairs = eng.grid_info(0)[2]
+    # keep the trajectory phase aligned with the list rebuild interval
+    rem = (-args.warmup) % INTVL
+    if rem:
+        eng.step(rem)
+    eng.set_timing(True)
+    clocks = ClockSampler(local)
+    barrier(pg)
+    torch.cuda.synchronize()
+    clocks.start()
+    eng.step(args.steps)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    st = eng.stats()
+    barrier(pg)
+    ms_total = max_over_ranks(pg, st["step_ms"])
+    pair_ms = st["pair_kernel_ms"] / args.steps
+    launches = st["kernel_launches"]
+    steps_per_s = args.steps / (ms_total / 1e3)
+    value = ns_per_day(steps_per_s) * world
+    # ---- end to end through the C ABI with host state (pinned) copied every step
+    eng.set_timing(False)
+    crd_h = torch.empty(3 * n_atoms, dtype=torch.float64, pin_memory=True)
+    vel_h = torch.empty(3 * n_atoms, dtype=torch.float64, pin_memory=True)
+    ene_h = torch.empty(11, dtype=torch.float64, pin_memory=True)
+    eng.get_state_async_ptr(0, crd_h.data_ptr(), vel_h.data_ptr(), ene_h.data_ptr())
+    eng.synchronize()
+    e2e_steps = max(10, min(args.steps, 100))
+    barrier(pg)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        eng.put_state_ptr(0, crd_h.data_ptr(), vel_h.data_ptr())
+        eng.step_async(1)
+        eng.get_state_async_ptr(0, crd_h.data_ptr(), vel_h.data_ptr(), ene_h.data_ptr())
+        eng.synchronize()
+    t_e2e = max_over_ranks(pg, time.perf_counter() - t0)
+    flags = eng.flags()
+    e2e = {"value": ns_per_day(e2e_steps / t_e2e) * world, "unit": UNIT,
+           "h2d_bytes_per_step": 2 * 8 * 3 * n_atoms, "d2h_bytes_per_step": 2 * 8 * 3 * n_atoms + 8 * 11,
+           "steps": e2e_steps}
+    eng.close()
+    pk = peaks()
+    sm_max = (pk or {}).get("sm_max_mhz", 1965.0)
+    fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12  # TFLOP/s: SMs x FP32 lanes x FMA x max clock
+    achieved = FLOP_PER_PAIR * n_int / (pair_ms / 1e3) / 1e12
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "pair_kernel_traffic.json")
+    if os.path.exists(tp):
+        try:
+            tj = json.load(open(tp))
+            traffic = tj["dram_bytes_per_launch_per_1M_atoms"] * n_atoms / 1e6
+        except Exception:
+            traffic = None
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_total / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "atoms_per_gpu": n_atoms, "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (cell-pair list %.0f MB, slot arrays %.0f MB)" % (
+                       n_cell_pairs * 16 / 1e6, n_atoms * 1.07 * 64 / 1e6),
+                   "arithmetic": "pair forces FP32 with int64 fixed-point accumulation; FP64 integrator, SHAKE, "
+                                 "energies"},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                     "frac": achieved / fp32_peak, "traffic": traffic,
+                     "kernel": "k_pair_ljzd", "pair_kernel_ms": pair_ms, "interacting_pairs": n_int,
+                     "flop_per_pair": FLOP_PER_PAIR,
+                     "peak_note": "FP32 CUDA-core peak = 148 SMs x 128 lanes x 2 x %.0f MHz (nominal at the "
+                                  "measured max SM clock; MEASURED_PEAKS.json has no FP32 figure)" % sm_max},
+        "e2e": e2e, "gpu_launches": launches, "clocks": clk, "device_flags": flags,
+    }
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local, pg = dist_setup(args)
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        steps = min(args.steps, 60)
+        res, why = reference_cpu(steps, min(args.warmup, 10))
+        if res is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return
+        v = cpu_ns_per_day_at_1m(res["atom_steps_per_s"])
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0, "steps": steps,
+            "warmup": min(args.warmup, 10), "ms_per_step": res["s_per_step"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": WORKLOAD + " (measured on the bounded sample below, scaled by atom count)"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": res["cores"], "kind": "reference",
+                             "sample": res["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
+        return
+    out = run_ours(args, world, rank, local, pg)
+    if rank == 0:
+        if not args.no_cpu_baseline:
+            res, why = reference_cpu(args.cpu_steps, 3)
+            if res is not None:
+                out["cpu_baseline"] = {"value": cpu_ns_per_day_at_1m(res["atom_steps_per_s"]), "unit": UNIT,
+                                       "cores": res["cores"], "kind": "reference", "sample": res["sample"]}
+            else:
+                out["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": why}
+        print(json.dumps(out))
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -130,12 +130,28 @@ og_status og_step(og_engine *e, int32_t n_steps);
  * forces and energies without advancing time (SubBox::nsgrid_update + SubBox::calc_energy). */
 og_status og_compute_forces(og_engine *e);
 
+/* Replaces a system's coordinates / velocities and marks the cell list for a rebuild at the
+ * next step (synchronous). */
 og_status og_set_state(og_engine *e, int32_t sys, const double *crd, const double *vel_next);
+/* Continues the trajectory from host coordinates / velocities without re-enumerating cell
+ * pairs (asynchronous, stream-ordered): the role of the reference's per-step
+ * cuda_memcpy_htod_crd + cuda_set_crd (cuda_setup.cu:124-136, 380-402).  The grid copy moves
+ * by the minimum-image displacement, as MiniCell::move_atom does (MiniCell.cpp:1312-1325).
+ * Host buffers should be pinned for the copy to overlap. */
+og_status og_put_state(og_engine *e, int32_t sys, const double *crd, const double *vel_next);
+/* Stream-ordered device->host copies of state and energies (NULL pointers are skipped);
+ * complete after og_synchronize.  The role of cuda_memcpy_dtoh_work (cuda_setup.cu:803-823). */
+og_status og_get_state_async(og_engine *e, int32_t sys, double *crd, double *vel_next, double *energies);
+/* Steps without the end-of-call synchronisation (see og_step); flags are read with og_get_flags. */
+og_status og_step_async(og_engine *e, int32_t n_steps);
+og_status og_synchronize(og_engine *e);
 og_status og_get_state(og_engine *e, int32_t sys, double *crd, double *vel_next);
 /* work[3n] = dE/dx of the last force evaluation (pair + excess + bonded, before McMD scaling),
  * energies[OG_N_ENERGY], virial[9] = sum_pairs d_a f_b of the nonbonded (LJ + ZD) terms. */
 og_status og_get_forces(og_engine *e, int32_t sys, double *work, double *energies, double *virial);
 og_status og_get_energies(og_engine *e, int32_t sys, double *energies);
+/* Interacting pairs (r < cutoff, not excluded) counted by the last og_compute_forces. */
+og_status og_get_pair_count(og_engine *e, int32_t sys, int64_t *n_pairs);
 
 /* Cell grid of the last list build (MiniCell's arrays in canonical order):
  * n_cells; slot_atomid[8*n_cells] (-1 dummy); col_head_cell[n_columns+1] (-1 empty column). */

@@ -30,15 +30,16 @@ __global__ void k_count_pairs(const int *, int, int, const int *, const int *, c
 __global__ void k_fill_pairs(int *, int, int, long long, const int *, const int *, const SysDev *, const int *,
                              const int *, const int *, const float2 *, const int2 *, const int *, const int *,
                              const unsigned char *, const int *, const int *, const int *, const int *, const int *,
-                             int2 *, unsigned long long *);
+                             int2 *, unsigned long long *, const double *, float4 *);
 __global__ void k_pair_heads(int *, int, int, const int *, int *);
 __global__ void k_scan_block(const int *, int *, long long, int *);
 __global__ void k_scan_add(int *, long long, const int *);
 // og_pair.cu
 template <bool VIR>
-__global__ void k_pair_ljzd(const int *, const int *, const SysDev *, const double *, const float4 *, const int *,
-                            const int *, const int2 *, const unsigned long long *, const float2 *,
+__global__ void k_pair_ljzd(const int *, const int *, const SysDev *, const float4 *, const float4 *, const int *,
+                            const int *, const float4 *, const int2 *, const unsigned long long *, const float2 *,
                             unsigned long long *, double *, long long);
+__global__ void k_cell_bbox(const int *, int, const float4 *, const unsigned char *, float4 *);
 // og_integrate.cu
 __global__ void k_excess(int, const int2 *, const int *, const SysDev *, const double *, const double *, const int *,
                          unsigned long long *, double *, double *);
@@ -48,13 +49,13 @@ __global__ void k_angles(int, const int4 *, const double2 *, const SysDev *, con
                          unsigned long long *, double *);
 __global__ void k_atom_virial(int, const int *, const unsigned long long *, const float4 *, const double *, double *);
 __global__ void k_collect(int, const int *, unsigned long long *, double *);
-__global__ void k_reduce_potential(const SysDev *, const int *, const double *, const double *, const double *,
-                                   const double *, double *, double *);
-__global__ void k_reduce_virial(const SysDev *, const int *, const double *, const double *, const double *,
-                                double *);
-__global__ void k_group_moment(const int *, const int *, const float *, const float *, const double *, const int *,
-                               const int *, double *);
-__global__ void k_reduce_atoms(const SysDev *, const double *, double *, int, int);
+template <int NV>
+__global__ void k_part(const double *, int, int, const int *, int, double *);
+__global__ void k_part_momentum(const int *, const int *, const float *, const double *, const int *, const int *,
+                                int, double *);
+template <int NV>
+__global__ void k_part_final(const double *, int, double *, int, int, const float *, int);
+__global__ void k_mcmd_factor(int, const SysDev *, const double *, double *);
 __global__ void k_update_velocities(int, const int *, const SysDev *, const double *, double *, const float *,
                                     double *, double *);
 __global__ void k_com_apply(int, const int *, const double *, const int *, const int *, double *);
@@ -84,6 +85,8 @@ __global__ void k_slot_refresh(const int *, int, const int *, const double *, co
 __global__ void k_energies(int, const SysDev *, const double *, const double *, double *, double *, int,
                            long long *);
 __global__ void k_trace_advance(long long *, long long *);
+__global__ void k_put_state(int, int, const int *, const SysDev *, const double *, const double *, double *, double *,
+                            const int *, double *, const double *, float4 *);
 
 __global__ void k_fill_int(int *p, long long n, int v) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -159,6 +162,8 @@ struct og_engine {
     std::vector<long long> scan_len;
     int2 *d_cp_c2img = nullptr;
     unsigned long long *d_cp_mask = nullptr;
+    float4 *d_cp_shift = nullptr;  // pair-kernel record: FP64-formed shift + cell2
+    float4 *d_bbox = nullptr;      // per-cell bounding boxes (2 per cell)
     int *d_excl_start = nullptr, *d_excl_list = nullptr;
     int2 *d_excess = nullptr;
     int *d_excess_sys = nullptr;
@@ -182,6 +187,10 @@ struct og_engine {
     double *d_sys_acc = nullptr, *d_mcmd = nullptr, *d_energies = nullptr, *d_thermo = nullptr,
            *d_sum_tmp = nullptr;
     int *d_mask_plain = nullptr, *d_mask_thermo = nullptr, *d_active = nullptr, *d_any = nullptr;
+    // segment bases for the two-level reductions and their chunk counts
+    int *d_seg_atoms = nullptr, *d_seg_exc = nullptr, *d_seg_bond = nullptr, *d_seg_angle = nullptr;
+    int mc_atoms = 1, mc_cells = 1, mc_exc = 1, mc_bond = 1, mc_angle = 1, mc_grp = 1;
+    double *d_part = nullptr;
     // trace
     double *d_trace = nullptr;
     int trace_cap = 0;
@@ -192,6 +201,9 @@ struct og_engine {
     // stats
     long long launches = 0;
     cudaEvent_t ev_pair0 = nullptr, ev_pair1 = nullptr, ev_step0 = nullptr, ev_step1 = nullptr;
+    std::vector<cudaEvent_t> pev0, pev1;  // per pair-kernel launch of one og_step
+    int pev_used = 0;
+    double *d_stage = nullptr;            // og_put_state staging (6 doubles per atom)
     double pair_ms = 0.0, step_ms = 0.0;
     bool timing = false;
     std::vector<void *> allocs;
@@ -425,27 +437,42 @@ og_status build_list(og_engine *e) {
         e->d_counters, e->cells_cap, e->nnc, e->pair_cap, e->d_cell_sys, e->d_sys_cell_base, e->d_sys, e->d_cell_col,
         e->d_col_cell_start, e->d_col_head_cell, e->d_cell_zr, e->d_cell_uni, e->d_uni_lo, e->d_uni_hi,
         e->d_cell_valid, e->d_slot_atom, e->d_atom_slot, e->d_excl_start, e->d_excl_list, e->d_offset, e->d_cp_c2img,
-        e->d_cp_mask);
+        e->d_cp_mask, e->d_cell_origin, e->d_cp_shift);
     LAUNCH_CHECK();
     return OG_OK;
 }
 
 // ---------------------------------------------------------- forces
 
+og_status reduce_potential(og_engine *e);
+og_status reduce_virial(og_engine *e);
+
 og_status compute_forces(og_engine *e, bool vir) {
     cudaStream_t st = e->stream;
     const unsigned pair_blocks = blocks((long long)e->cells_cap * 32, 256);
-    if (e->timing) CK(cudaEventRecord(e->ev_pair0, st));
+    k_cell_bbox<<<blocks(e->cells_cap, 256), 256, 0, st>>>(e->d_counters, e->cells_cap, e->d_xq, e->d_cell_valid,
+                                                            e->d_bbox);
+    LAUNCH_CHECK();
+    if (e->timing) {
+        if (e->pev_used >= (int)e->pev0.size()) {
+            cudaEvent_t a, b;
+            CK(cudaEventCreate(&a));
+            CK(cudaEventCreate(&b));
+            e->pev0.push_back(a);
+            e->pev1.push_back(b);
+        }
+        CK(cudaEventRecord(e->pev0[e->pev_used], st));
+    }
     if (vir)
-        k_pair_ljzd<true><<<pair_blocks, 256, 0, st>>>(e->d_counters, e->d_cell_sys, e->d_sys, e->d_cell_origin,
-                                                       e->d_xq, e->d_slot_type, e->d_cp_head, e->d_cp_c2img,
+        k_pair_ljzd<true><<<pair_blocks, 256, 0, st>>>(e->d_counters, e->d_cell_sys, e->d_sys, e->d_bbox, e->d_xq,
+                                                       e->d_slot_type, e->d_cp_head, e->d_cp_shift, e->d_cp_c2img,
                                                        e->d_cp_mask, e->d_lj, e->d_frc, e->d_cell_acc, e->pair_cap);
     else
-        k_pair_ljzd<false><<<pair_blocks, 256, 0, st>>>(e->d_counters, e->d_cell_sys, e->d_sys, e->d_cell_origin,
-                                                        e->d_xq, e->d_slot_type, e->d_cp_head, e->d_cp_c2img,
+        k_pair_ljzd<false><<<pair_blocks, 256, 0, st>>>(e->d_counters, e->d_cell_sys, e->d_sys, e->d_bbox, e->d_xq,
+                                                        e->d_slot_type, e->d_cp_head, e->d_cp_shift, e->d_cp_c2img,
                                                         e->d_cp_mask, e->d_lj, e->d_frc, e->d_cell_acc, e->pair_cap);
     LAUNCH_CHECK();
-    if (e->timing) CK(cudaEventRecord(e->ev_pair1, st));
+    if (e->timing) CK(cudaEventRecord(e->pev1[e->pev_used++], st));
     if (vir) {
         if (!e->d_vir_atom) {
             og_status s = dalloc(e, &e->d_vir_atom, 9 * (size_t)e->n_atoms);
@@ -475,21 +502,65 @@ og_status compute_forces(og_engine *e, bool vir) {
     }
     k_collect<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_slot, e->d_frc, e->d_work);
     LAUNCH_CHECK();
-    k_reduce_potential<<<e->n_sys, 256, 0, st>>>(e->d_sys, e->d_sys_cell_base, e->d_cell_acc, e->d_e_exc,
-                                                  e->d_e_bond, e->d_e_angle, e->d_sys_acc, e->d_mcmd);
+    og_status rs = reduce_potential(e);
+    if (rs) return rs;
+    if (vir && (rs = reduce_virial(e))) return rs;
+    return OG_OK;
+}
+
+// Two-level fixed-order sum of NV fields over every system's segment into out[s*stride + off].
+template <int NV>
+og_status seg_sum(og_engine *e, const double *v, int vstride, int field0, const int *base, int max_chunks,
+                  double *out, int out_stride, int out_off, int accumulate) {
+    dim3 grid(max_chunks, e->n_sys);
+    k_part<NV><<<grid, 256, 0, e->stream>>>(v, vstride, field0, base, max_chunks, e->d_part);
     LAUNCH_CHECK();
-    if (vir) {
-        k_reduce_virial<<<e->n_sys, 256, 0, st>>>(e->d_sys, e->d_sys_cell_base, e->d_cell_acc, e->d_vir_atom,
-                                                   e->d_vir_exc, e->d_sys_acc);
-        LAUNCH_CHECK();
-    }
+    k_part_final<NV><<<e->n_sys, 256, 0, e->stream>>>(e->d_part, max_chunks, out, out_stride, out_off, nullptr,
+                                                      accumulate);
+    LAUNCH_CHECK();
+    return OG_OK;
+}
+
+og_status reduce_potential(og_engine *e) {
+    og_status s;
+    if ((s = seg_sum<2>(e, e->d_cell_acc, OG_CELL_ACC, 0, e->d_sys_cell_base, e->mc_cells, e->d_sys_acc, OG_ACC_SIZE,
+                        OG_ACC_VDW, 0)))
+        return s;
+    if (e->n_excess && (s = seg_sum<1>(e, e->d_e_exc, 1, 0, e->d_seg_exc, e->mc_exc, e->d_sys_acc, OG_ACC_SIZE,
+                                       OG_ACC_EXCESS, 0)))
+        return s;
+    if (e->n_bonds && (s = seg_sum<1>(e, e->d_e_bond, 1, 0, e->d_seg_bond, e->mc_bond, e->d_sys_acc, OG_ACC_SIZE,
+                                      OG_ACC_BOND, 0)))
+        return s;
+    if (e->n_angles && (s = seg_sum<1>(e, e->d_e_angle, 1, 0, e->d_seg_angle, e->mc_angle, e->d_sys_acc,
+                                       OG_ACC_SIZE, OG_ACC_ANGLE, 0)))
+        return s;
+    k_mcmd_factor<<<blocks(e->n_sys, 128), 128, 0, e->stream>>>(e->n_sys, e->d_sys, e->d_sys_acc, e->d_mcmd);
+    LAUNCH_CHECK();
+    return OG_OK;
+}
+
+og_status reduce_virial(og_engine *e) {
+    og_status s;
+    if ((s = seg_sum<10>(e, e->d_cell_acc, OG_CELL_ACC, 2, e->d_sys_cell_base, e->mc_cells, e->d_sys_acc,
+                         OG_ACC_SIZE, OG_ACC_VIR, 0)))
+        return s;
+    if ((s = seg_sum<9>(e, e->d_vir_atom, 9, 0, e->d_seg_atoms, e->mc_atoms, e->d_sys_acc, OG_ACC_SIZE, OG_ACC_VIR,
+                        1)))
+        return s;
+    if (e->n_excess && (s = seg_sum<9>(e, e->d_vir_exc, 9, 0, e->d_seg_exc, e->mc_exc, e->d_sys_acc, OG_ACC_SIZE,
+                                       OG_ACC_VIR, 1)))
+        return s;
     return OG_OK;
 }
 
 og_status com_cancel(og_engine *e, double *v, const int *active) {
     if (!e->any_groups) return OG_OK;
-    k_group_moment<<<e->n_groups, 256, 0, e->stream>>>(e->d_grp_start, e->d_grp_atoms, e->d_grp_mass_inv, e->d_mass,
-                                                        v, e->d_grp_sys, active, e->d_moment);
+    dim3 grid(e->mc_grp, e->n_groups);
+    k_part_momentum<<<grid, 256, 0, e->stream>>>(e->d_grp_start, e->d_grp_atoms, e->d_mass, v, e->d_grp_sys, active,
+                                                 e->mc_grp, e->d_part);
+    LAUNCH_CHECK();
+    k_part_final<3><<<e->n_groups, 256, 0, e->stream>>>(e->d_part, e->mc_grp, e->d_moment, 3, 0, e->d_grp_mass_inv, 0);
     LAUNCH_CHECK();
     k_com_apply<<<blocks(e->n_atoms, 256), 256, 0, e->stream>>>(e->n_atoms, e->d_atom_group, e->d_moment,
                                                                  e->d_atom_sys, active, v);
@@ -521,13 +592,13 @@ og_status thermostat_with_shake(og_engine *e) {
     CK(cudaMemcpyAsync(e->d_active, e->d_mask_thermo, sizeof(int) * e->n_sys, cudaMemcpyDeviceToDevice, st));
     k_copy_double<<<blocks(3LL * e->n_atoms, 256), 256, 0, st>>>(e->d_buf_crd, e->d_crd, 3LL * e->n_atoms);
     LAUNCH_CHECK();
+    og_status s;
     for (int it = 0; it < e->thermo_max_loops; it++) {
-        og_status s = shake(e, e->d_active);
+        s = shake(e, e->d_active);
         if (s) return s;
         k_ke_mid<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_mass, e->d_vel, e->d_vel_next, e->d_ke);
         LAUNCH_CHECK();
-        k_reduce_atoms<<<e->n_sys, 256, 0, st>>>(e->d_sys, e->d_ke, e->d_sum_tmp, 1, 0);
-        LAUNCH_CHECK();
+        if ((s = seg_sum<1>(e, e->d_ke, 1, 0, e->d_seg_atoms, e->mc_atoms, e->d_sum_tmp, 1, 0, 0))) return s;
         CK(cudaMemsetAsync(e->d_any, 0, sizeof(int), st));
         k_thermo_check<<<blocks(e->n_sys, 128), 128, 0, st>>>(e->n_sys, e->d_sys, e->d_sum_tmp, e->d_thermo, e->d_step,
                                                                it, e->thermo_max_loops, e->thermo_tol, e->d_active,
@@ -540,8 +611,7 @@ og_status thermostat_with_shake(og_engine *e) {
                                                                 e->d_work, e->d_mass, e->d_mass_inv, e->d_crd,
                                                                 e->d_buf_crd, e->d_vel, e->d_vel_next, e->d_ke);
         LAUNCH_CHECK();
-        k_reduce_atoms<<<e->n_sys, 256, 0, st>>>(e->d_sys, e->d_ke, e->d_sum_tmp, 1, 0);
-        LAUNCH_CHECK();
+        if ((s = seg_sum<1>(e, e->d_ke, 1, 0, e->d_seg_atoms, e->mc_atoms, e->d_sum_tmp, 1, 0, 0))) return s;
         k_thermo_rescale<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys, e->d_active,
                                                                    e->d_sum_tmp, e->d_thermo, e->d_step, e->d_work,
                                                                    e->d_mass_inv, e->d_crd, e->d_buf_crd, e->d_vel,
@@ -575,8 +645,7 @@ og_status run_step(og_engine *e) {
         k_thermo_scaling_ke<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys, e->d_work,
                                                                       e->d_mass, e->d_mass_inv, e->d_vel, e->d_ke);
         LAUNCH_CHECK();
-        k_reduce_atoms<<<e->n_sys, 256, 0, st>>>(e->d_sys, e->d_ke, e->d_sum_tmp, 1, 0);
-        LAUNCH_CHECK();
+        if ((s = seg_sum<1>(e, e->d_ke, 1, 0, e->d_seg_atoms, e->mc_atoms, e->d_sum_tmp, 1, 0, 0))) return s;
         k_thermo_scaling_apply<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys,
                                                                          e->d_sum_tmp, e->d_thermo, e->d_step,
                                                                          e->d_work, e->d_mass_inv, e->d_vel,
@@ -598,8 +667,8 @@ og_status run_step(og_engine *e) {
                                                        e->d_crd_prev, e->d_vel, e->d_vel_next, e->d_atom_slot,
                                                        e->d_slot_crd, e->d_cell_origin, e->d_xq, e->d_mass, e->d_ke);
     LAUNCH_CHECK();
-    k_reduce_atoms<<<e->n_sys, 256, 0, st>>>(e->d_sys, e->d_ke, e->d_sys_acc, OG_ACC_SIZE, OG_ACC_KIN);
-    LAUNCH_CHECK();
+    if ((s = seg_sum<1>(e, e->d_ke, 1, 0, e->d_seg_atoms, e->mc_atoms, e->d_sys_acc, OG_ACC_SIZE, OG_ACC_KIN, 0)))
+        return s;
     k_energies<<<blocks(e->n_sys, 128), 128, 0, st>>>(e->n_sys, e->d_sys, e->d_sys_acc, e->d_mcmd, e->d_energies,
                                                        e->d_trace, e->trace_cap, e->d_trace_count);
     LAUNCH_CHECK();
@@ -633,11 +702,15 @@ og_status grow_pairs(og_engine *e, long long need) {
     long long cap = need + need / 2 + 4096;
     dfree(e, e->d_cp_c2img);
     dfree(e, e->d_cp_mask);
+    dfree(e, e->d_cp_shift);
     e->d_cp_c2img = nullptr;
     e->d_cp_mask = nullptr;
+    e->d_cp_shift = nullptr;
     og_status s = dalloc(e, &e->d_cp_c2img, (size_t)cap);
     if (s) return s;
     s = dalloc(e, &e->d_cp_mask, (size_t)cap);
+    if (s) return s;
+    s = dalloc(e, &e->d_cp_shift, (size_t)cap);
     if (s) return s;
     e->pair_cap = cap;
     return OG_OK;
@@ -703,6 +776,8 @@ og_status og_destroy(og_engine *e) {
     for (void *p : e->allocs) cudaFree(p);
     e->allocs.clear();
     if (e->h_pinned) cudaFreeHost(e->h_pinned);
+    for (auto ev : e->pev0) cudaEventDestroy(ev);
+    for (auto ev : e->pev1) cudaEventDestroy(ev);
     if (e->ev_pair0) cudaEventDestroy(e->ev_pair0);
     if (e->ev_pair1) cudaEventDestroy(e->ev_pair1);
     if (e->ev_step0) cudaEventDestroy(e->ev_step0);
@@ -970,8 +1045,9 @@ og_status og_finalize(og_engine *e) {
         (s = dalloc(e, &e->d_sys_cell_base, S + 1)) || (s = dalloc(e, &e->d_cell_col, cells_cap)) ||
         (s = dalloc(e, &e->d_cell_sys, cells_cap)) || (s = dalloc(e, &e->d_cp_head, cells_cap + 1)) ||
         (s = dalloc(e, &e->d_cell_origin, 3 * (size_t)cells_cap)) ||
-        (s = dalloc(e, &e->d_cell_acc, 11 * (size_t)cells_cap)) || (s = dalloc(e, &e->d_cell_zr, cells_cap)) ||
+        (s = dalloc(e, &e->d_cell_acc, OG_CELL_ACC * (size_t)cells_cap)) || (s = dalloc(e, &e->d_cell_zr, cells_cap)) ||
         (s = dalloc(e, &e->d_cell_uni, cells_cap)) || (s = dalloc(e, &e->d_cell_valid, cells_cap)) ||
+        (s = dalloc(e, &e->d_bbox, 2 * (size_t)cells_cap)) ||
         (s = dalloc(e, &e->d_slot_atom, e->slots_cap)) || (s = dalloc(e, &e->d_slot_type, e->slots_cap)) ||
         (s = dalloc(e, &e->d_slot_crd, 3 * (size_t)e->slots_cap)) || (s = dalloc(e, &e->d_xq, e->slots_cap)) ||
         (s = dalloc(e, &e->d_frc, 3 * (size_t)e->slots_cap)) || (s = dalloc(e, &e->d_uni_lo, e->n_uni)) ||
@@ -993,6 +1069,41 @@ og_status og_finalize(og_engine *e) {
         (s = upload(e, &e->d_mask_thermo, mask_thermo)) || (s = dalloc(e, &e->d_active, S)) ||
         (s = dalloc(e, &e->d_any, 1)))
         return s;
+    {
+        std::vector<int> sa(S + 1), se(S + 1), sb(S + 1), sg(S + 1);
+        int ma = 1, mcl = 1, me = 1, mb = 1, mg = 1;
+        for (int k = 0; k < S; k++) {
+            const SysDev &D = sd[k];
+            sa[k] = D.atom_base;
+            se[k] = D.excess_base;
+            sb[k] = D.bond_base;
+            sg[k] = D.angle_base;
+            auto ch = [](long long n) { return (int)((n + 4095) / 4096); };
+            ma = std::max(ma, ch(D.n_atoms));
+            mcl = std::max(mcl, ch(D.n_atoms / OG_CELL + D.n_columns + 1));
+            me = std::max(me, ch(D.n_excess));
+            mb = std::max(mb, ch(D.n_bonds));
+            mg = std::max(mg, ch(D.n_angles));
+        }
+        sa[S] = e->n_atoms;
+        se[S] = (int)excess.size();
+        sb[S] = (int)bondv.size();
+        sg[S] = (int)anglev.size();
+        int mgr = 1;
+        for (int g = 0; g < e->n_groups; g++) mgr = std::max(mgr, (grp_start[g + 1] - grp_start[g] + 4095) / 4096);
+        e->mc_atoms = ma;
+        e->mc_cells = mcl;
+        e->mc_exc = me;
+        e->mc_bond = mb;
+        e->mc_angle = mg;
+        e->mc_grp = mgr;
+        size_t part = (size_t)S * std::max(std::max(ma, mcl), std::max(me, std::max(mb, mg))) * 10;
+        part = std::max(part, (size_t)(e->n_groups + 1) * mgr * 3);
+        if ((s = upload(e, &e->d_seg_atoms, sa)) || (s = upload(e, &e->d_seg_exc, se)) ||
+            (s = upload(e, &e->d_seg_bond, sb)) || (s = upload(e, &e->d_seg_angle, sg)) ||
+            (s = dalloc(e, &e->d_part, part)))
+            return s;
+    }
     const long long n_items = (long long)cells_cap * nnc + 1;
     if ((s = dalloc(e, &e->d_count, n_items)) || (s = dalloc(e, &e->d_offset, n_items))) return s;
     for (long long len = n_items; len > 1;) {
@@ -1008,7 +1119,7 @@ og_status og_finalize(og_engine *e) {
     CK(cudaMemsetAsync(e->d_trace_count, 0, sizeof(long long), e->stream));
     CK(cudaMemsetAsync(e->d_count + (n_items - 1), 0, sizeof(int), e->stream));
     CK(cudaMemsetAsync(e->d_frc, 0, sizeof(unsigned long long) * 3 * (size_t)e->slots_cap, e->stream));
-    CK(cudaMemsetAsync(e->d_cell_acc, 0, sizeof(double) * 11 * (size_t)cells_cap, e->stream));
+    CK(cudaMemsetAsync(e->d_cell_acc, 0, sizeof(double) * OG_CELL_ACC * (size_t)cells_cap, e->stream));
     CK(cudaMemsetAsync(e->d_sys_acc, 0, sizeof(double) * OG_ACC_SIZE * S, e->stream));
     CK(cudaMemsetAsync(e->d_slot_crd, 0, sizeof(double) * 3 * (size_t)e->slots_cap, e->stream));
     if ((s = grow_pairs(e, (long long)cells_cap * 180))) return s;
@@ -1039,22 +1150,21 @@ og_status og_step(og_engine *e, int32_t n_steps) {
         CK(cudaMemcpyAsync(e->d_snap + 3 * (size_t)e->n_atoms, e->d_vel_next, sizeof(double) * 3 * e->n_atoms,
                            cudaMemcpyDeviceToDevice, e->stream));
         if ((s = clear_flags(e))) return s;
+        e->pev_used = 0;
         if (e->timing) CK(cudaEventRecord(e->ev_step0, e->stream));
-        for (int i = 0; i < n_steps; i++) {
+        for (int i = 0; i < n_steps; i++)
             if ((s = run_step(e))) return s;
-            if (e->timing) {
-                CK(cudaEventSynchronize(e->ev_pair1));
-                float ms = 0.f;
-                CK(cudaEventElapsedTime(&ms, e->ev_pair0, e->ev_pair1));
-                e->pair_ms += ms;
-            }
-        }
         if (e->timing) {
             CK(cudaEventRecord(e->ev_step1, e->stream));
             CK(cudaEventSynchronize(e->ev_step1));
             float ms = 0.f;
             CK(cudaEventElapsedTime(&ms, e->ev_step0, e->ev_step1));
             e->step_ms = ms;
+            e->pair_ms = 0.0;
+            for (int i = 0; i < e->pev_used; i++) {
+                CK(cudaEventElapsedTime(&ms, e->pev0[i], e->pev1[i]));
+                e->pair_ms += ms;
+            }
         }
         int c[OG_CNT_SIZE];
         if ((s = read_counters(e, c))) return s;
@@ -1296,5 +1406,66 @@ extern "C" og_status og_get_flags(og_engine *e, int32_t *flags) {
     og_status s = read_counters(e, c);
     if (s) return s;
     *flags = c[OG_CNT_FLAGS];
+    return OG_OK;
+}
+
+extern "C" og_status og_put_state(og_engine *e, int32_t sys, const double *crd, const double *vel_next) {
+    if (!e || !e->finalized) return fail(e, OG_ERR_STATE, "og_put_state before og_finalize");
+    if (sys < 0 || sys >= e->n_sys) return fail(e, OG_ERR_INVALID, "bad system id");
+    const SysDev &D = e->sys[sys].dev;
+    if (!e->d_stage) {
+        og_status s = dalloc(e, &e->d_stage, 6 * (size_t)e->n_atoms);
+        if (s) return s;
+    }
+    double *sc = e->d_stage, *sv = e->d_stage + 3 * (size_t)e->n_atoms;
+    if (crd) CK(cudaMemcpyAsync(sc, crd, sizeof(double) * 3 * D.n_atoms, cudaMemcpyHostToDevice, e->stream));
+    if (vel_next) CK(cudaMemcpyAsync(sv, vel_next, sizeof(double) * 3 * D.n_atoms, cudaMemcpyHostToDevice, e->stream));
+    k_put_state<<<blocks(D.n_atoms, 256), 256, 0, e->stream>>>(D.n_atoms, D.atom_base, e->d_atom_sys, e->d_sys,
+                                                                crd ? sc : nullptr, vel_next ? sv : nullptr, e->d_crd,
+                                                                e->d_vel_next, e->d_atom_slot, e->d_slot_crd,
+                                                                e->d_cell_origin, e->d_xq);
+    LAUNCH_CHECK();
+    return OG_OK;
+}
+
+extern "C" og_status og_get_state_async(og_engine *e, int32_t sys, double *crd, double *vel_next, double *energies) {
+    if (!e || !e->finalized) return fail(e, OG_ERR_STATE, "og_get_state_async before og_finalize");
+    if (sys < 0 || sys >= e->n_sys) return fail(e, OG_ERR_INVALID, "bad system id");
+    const SysDev &D = e->sys[sys].dev;
+    if (crd)
+        CK(cudaMemcpyAsync(crd, e->d_crd + 3 * (size_t)D.atom_base, sizeof(double) * 3 * D.n_atoms,
+                           cudaMemcpyDeviceToHost, e->stream));
+    if (vel_next)
+        CK(cudaMemcpyAsync(vel_next, e->d_vel_next + 3 * (size_t)D.atom_base, sizeof(double) * 3 * D.n_atoms,
+                           cudaMemcpyDeviceToHost, e->stream));
+    if (energies)
+        CK(cudaMemcpyAsync(energies, e->d_energies + 11 * (size_t)sys, sizeof(double) * OG_N_ENERGY,
+                           cudaMemcpyDeviceToHost, e->stream));
+    return OG_OK;
+}
+
+extern "C" og_status og_synchronize(og_engine *e) {
+    if (!e) return OG_ERR_INVALID;
+    CK(cudaStreamSynchronize(e->stream));
+    return OG_OK;
+}
+
+extern "C" og_status og_step_async(og_engine *e, int32_t n_steps) {
+    // og_step without the end-of-call flag check and without the capacity retry: the caller
+    // checks og_get_flags at its own sync points
+    if (!e || !e->finalized) return fail(e, OG_ERR_STATE, "og_step_async before og_finalize");
+    for (int i = 0; i < n_steps; i++) {
+        og_status s = run_step(e);
+        if (s) return s;
+    }
+    return OG_OK;
+}
+
+extern "C" og_status og_get_pair_count(og_engine *e, int32_t sys, int64_t *n_pairs) {
+    if (!e || !e->finalized || !n_pairs) return OG_ERR_INVALID;
+    if (sys < 0 || sys >= e->n_sys) return fail(e, OG_ERR_INVALID, "bad system id");
+    double v = 0;
+    CK(cudaMemcpy(&v, e->d_sys_acc + OG_ACC_SIZE * sys + OG_ACC_PAIRS, sizeof(double), cudaMemcpyDeviceToHost));
+    *n_pairs = (int64_t)v;
     return OG_OK;
 }

@@ -352,7 +352,8 @@ __global__ void k_fill_pairs(int *__restrict__ counters, int cells_cap, int nnc,
                              const unsigned char *__restrict__ cell_valid, const int *__restrict__ slot_atom,
                              const int *__restrict__ atom_slot, const int *__restrict__ excl_start,
                              const int *__restrict__ excl_list, const int *__restrict__ offset,
-                             int2 *__restrict__ cp_c2img, unsigned long long *__restrict__ cp_mask) {
+                             int2 *__restrict__ cp_c2img, unsigned long long *__restrict__ cp_mask,
+                             const double *__restrict__ cell_origin, float4 *__restrict__ cp_shift) {
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int n_cells = counters[OG_CNT_N_CELLS];
     if (idx >= (long long)n_cells * nnc) return;
@@ -366,6 +367,19 @@ __global__ void k_fill_pairs(int *__restrict__ counters, int cells_cap, int nnc,
                              uni_lo, uni_hi, cell_valid, slot_atom, atom_slot, excl_start, excl_list,
                              cp_c2img + off, cp_mask + off, cap);
     if (off + n > pair_cap) og_set_flag(counters, OG_FLAG_PAIR_CAPACITY);
+    // pair-kernel record: shift from cell1's origin to cell2's image origin, formed in FP64
+    const int nw = min(n, cap);
+    const double o1x = cell_origin[3 * c1], o1y = cell_origin[3 * c1 + 1], o1z = cell_origin[3 * c1 + 2];
+    for (int k = 0; k < nw; k++) {
+        const int2 ci = cp_c2img[off + k];
+        const int c2 = ci.x, img = ci.y;
+        const double shx = (img & 1) ? -S.L[0] : ((img & 2) ? S.L[0] : 0.0);
+        const double shy = (img & 4) ? -S.L[1] : ((img & 8) ? S.L[1] : 0.0);
+        const double shz = (img & 16) ? -S.L[2] : ((img & 32) ? S.L[2] : 0.0);
+        cp_shift[off + k] = make_float4((float)(cell_origin[3 * c2] + shx - o1x),
+                                        (float)(cell_origin[3 * c2 + 1] + shy - o1y),
+                                        (float)(cell_origin[3 * c2 + 2] + shz - o1z), __int_as_float(c2));
+    }
 }
 
 // CSR heads from the scanned counts; also publishes the total.

@@ -149,99 +149,102 @@ __device__ void block_sum(double (&v)[NV], double *sh) {
     __syncthreads();
 }
 
-// One block (256 threads) per system: potential-energy terms, then the McMD scaling factor
-// (Extend.cpp:178-203) and the total potential used for it (MmSystem::set_potential_e).
-__global__ void k_reduce_potential(const SysDev *__restrict__ sys, const int *__restrict__ sys_cell_base,
-                                   const double *__restrict__ cell_acc, const double *__restrict__ e_exc,
-                                   const double *__restrict__ e_bond, const double *__restrict__ e_angle,
-                                   double *__restrict__ sys_acc, double *__restrict__ mcmd_factor) {
-    __shared__ double sh[5 * 256];
-    const int s = blockIdx.x;
-    const SysDev &S = sys[s];
-    double v[5] = {0, 0, 0, 0, 0};
-    for (int c = sys_cell_base[s] + threadIdx.x; c < sys_cell_base[s + 1]; c += blockDim.x) {
-        v[0] += cell_acc[11 * (size_t)c];
-        v[1] += cell_acc[11 * (size_t)c + 1];
-    }
-    for (int k = threadIdx.x; k < S.n_excess; k += blockDim.x) v[2] += e_exc[S.excess_base + k];
-    for (int k = threadIdx.x; k < S.n_bonds; k += blockDim.x) v[3] += e_bond[S.bond_base + k];
-    for (int k = threadIdx.x; k < S.n_angles; k += blockDim.x) v[4] += e_angle[S.angle_base + k];
-    block_sum<5>(v, sh);
-    if (threadIdx.x == 0) {
-        double *acc = sys_acc + OG_ACC_SIZE * s;
-        acc[OG_ACC_VDW] = v[0];
-        acc[OG_ACC_ELE] = v[1];
-        acc[OG_ACC_EXCESS] = v[2];
-        acc[OG_ACC_BOND] = v[3];
-        acc[OG_ACC_ANGLE] = v[4];
-        double f = 1.0;
-        if (S.mcmd_order >= 0) {
-            const double lambda = v[0] + v[1] + v[2] + S.self_energy + v[3] + v[4];
-            double param = lambda;
-            if (lambda <= S.mcmd_lo) param = S.mcmd_lo;
-            else if (lambda >= S.mcmd_hi) param = S.mcmd_hi;
-            double dlnp = S.mcmd_coef[0], t = 1.0;
-            for (int i = 1; i < S.mcmd_order + 1; i++) {
-                t *= param;
-                dlnp += S.mcmd_coef[i] * t;
-            }
-            f = S.mcmd_k * dlnp;
-        }
-        mcmd_factor[s] = f;
-    }
-}
-
-// One block per system: virial = sum_atoms x (x) F + sum_cell-pairs shift (x) F_j + excess.
-__global__ void k_reduce_virial(const SysDev *__restrict__ sys, const int *__restrict__ sys_cell_base,
-                                const double *__restrict__ cell_acc, const double *__restrict__ vir_atom,
-                                const double *__restrict__ vir_exc, double *__restrict__ sys_acc) {
-    __shared__ double sh[9 * 256];
-    const int s = blockIdx.x;
-    const SysDev &S = sys[s];
-    double v[9];
-    for (int q = 0; q < 9; q++) v[q] = 0;
-    for (int c = sys_cell_base[s] + threadIdx.x; c < sys_cell_base[s + 1]; c += blockDim.x)
-        for (int q = 0; q < 9; q++) v[q] += cell_acc[11 * (size_t)c + 2 + q];
-    for (int a = S.atom_base + threadIdx.x; a < S.atom_base + S.n_atoms; a += blockDim.x)
-        for (int q = 0; q < 9; q++) v[q] += vir_atom[9 * (size_t)a + q];
-    for (int k = S.excess_base + threadIdx.x; k < S.excess_base + S.n_excess; k += blockDim.x)
-        for (int q = 0; q < 9; q++) v[q] += vir_exc[9 * (size_t)k + q];
-    block_sum<9>(v, sh);
+// Two-level fixed-order reductions.  Level 1: block (chunk, segment) sums NV fields of the
+// items [base[s] + chunk*OG_RCHUNK, ...) of segment s; level 2: one block per segment sums its
+// chunks in order.  Chunks are relative to the segment start, so a system's sums do not depend
+// on what else is in the batch.
+#define OG_RCHUNK 4096
+template <int NV>
+__global__ void k_part(const double *__restrict__ v, int stride, int field0, const int *__restrict__ base,
+                       int max_chunks, double *__restrict__ part) {
+    __shared__ double sh[NV * 256];
+    const int s = blockIdx.y, ch = blockIdx.x;
+    const long long b = (long long)base[s] + (long long)ch * OG_RCHUNK;
+    const long long e = min((long long)base[s + 1], b + OG_RCHUNK);
+    double acc[NV];
+    for (int q = 0; q < NV; q++) acc[q] = 0.0;
+    for (long long i = b + threadIdx.x; i < e; i += blockDim.x)
+        for (int q = 0; q < NV; q++) acc[q] += v[i * stride + field0 + q];
+    block_sum<NV>(acc, sh);
     if (threadIdx.x == 0)
-        for (int q = 0; q < 9; q++) sys_acc[OG_ACC_SIZE * s + OG_ACC_VIR + q] = v[q];
+        for (int q = 0; q < NV; q++) part[((size_t)s * max_chunks + ch) * NV + q] = acc[q];
 }
 
-// One block per COM group: moment = (sum m v) / M_group (COMMotion.cpp:30-55).
-__global__ void k_group_moment(const int *__restrict__ grp_start, const int *__restrict__ grp_atoms,
-                               const float *__restrict__ grp_mass_inv, const float *__restrict__ mass,
-                               const double *__restrict__ v, const int *__restrict__ grp_sys,
-                               const int *__restrict__ sys_active, double *__restrict__ moment) {
+// Level 1 for COM groups: momentum sum m v over a group's atom list.
+__global__ void k_part_momentum(const int *__restrict__ grp_start, const int *__restrict__ grp_atoms,
+                                const float *__restrict__ mass, const double *__restrict__ v,
+                                const int *__restrict__ grp_sys, const int *__restrict__ sys_active, int max_chunks,
+                                double *__restrict__ part) {
     __shared__ double sh[3 * 256];
-    const int g = blockIdx.x;
+    const int g = blockIdx.y, ch = blockIdx.x;
+    const int b = grp_start[g] + ch * OG_RCHUNK;
+    const int e = min(grp_start[g + 1], b + OG_RCHUNK);
     double m[3] = {0, 0, 0};
-    if (sys_active == nullptr || sys_active[grp_sys[g]]) {
-        for (int k = grp_start[g] + threadIdx.x; k < grp_start[g + 1]; k += blockDim.x) {
+    if (sys_active == nullptr || sys_active[grp_sys[g]])
+        for (int k = b + threadIdx.x; k < e; k += blockDim.x) {
             const int a = grp_atoms[k];
             for (int q = 0; q < 3; q++) m[q] += v[3 * a + q] * (double)mass[a];
         }
-    }
     block_sum<3>(m, sh);
     if (threadIdx.x == 0)
-        for (int q = 0; q < 3; q++) moment[3 * g + q] = m[q] * (double)grp_mass_inv[g];
+        for (int q = 0; q < 3; q++) part[((size_t)g * max_chunks + ch) * 3 + q] = m[q];
 }
 
-// One block per system: sum over atoms of a per-atom scalar.
-__global__ void k_reduce_atoms(const SysDev *__restrict__ sys, const double *__restrict__ val,
-                               double *__restrict__ out, int out_stride, int out_index) {
-    __shared__ double sh[256];
+// Level 2: out[s*out_stride + out_off + q] = (sum over chunks of part) * (scale ? scale[s] : 1).
+template <int NV>
+__global__ void k_part_final(const double *__restrict__ part, int max_chunks, double *__restrict__ out,
+                             int out_stride, int out_off, const float *__restrict__ scale, int accumulate) {
+    __shared__ double sh[NV * 256];
     const int s = blockIdx.x;
-    const SysDev &S = sys[s];
-    double v[1] = {0};
-    for (int a = S.atom_base + threadIdx.x; a < S.atom_base + S.n_atoms; a += blockDim.x) v[0] += val[a];
-    block_sum<1>(v, sh);
-    if (threadIdx.x == 0) out[out_stride * s + out_index] = v[0];
+    double acc[NV];
+    for (int q = 0; q < NV; q++) acc[q] = 0.0;
+    for (int c = threadIdx.x; c < max_chunks; c += blockDim.x)
+        for (int q = 0; q < NV; q++) acc[q] += part[((size_t)s * max_chunks + c) * NV + q];
+    block_sum<NV>(acc, sh);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < NV; q++) {
+            const double r = acc[q] * (scale ? (double)scale[s] : 1.0);
+            double &o = out[(size_t)s * out_stride + out_off + q];
+            o = accumulate ? o + r : r;
+        }
 }
 
+template __global__ void k_part<1>(const double *, int, int, const int *, int, double *);
+template __global__ void k_part<2>(const double *, int, int, const int *, int, double *);
+template __global__ void k_part<9>(const double *, int, int, const int *, int, double *);
+template __global__ void k_part<10>(const double *, int, int, const int *, int, double *);
+template __global__ void k_part_final<1>(const double *, int, double *, int, int, const float *, int);
+template __global__ void k_part_final<2>(const double *, int, double *, int, int, const float *, int);
+template __global__ void k_part_final<3>(const double *, int, double *, int, int, const float *, int);
+template __global__ void k_part_final<9>(const double *, int, double *, int, int, const float *, int);
+template __global__ void k_part_final<10>(const double *, int, double *, int, int, const float *, int);
+
+// McMD factor and the potential used for it, one thread per system (Extend.cpp:178-203,
+// MmSystem::set_potential_e).
+__global__ void k_mcmd_factor(int n_sys, const SysDev *__restrict__ sys, const double *__restrict__ sys_acc,
+                              double *__restrict__ mcmd_factor) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_sys) return;
+    const SysDev &S = sys[s];
+    const double *acc = sys_acc + OG_ACC_SIZE * s;
+    double f = 1.0;
+    if (S.mcmd_order >= 0) {
+        const double lambda = acc[OG_ACC_VDW] + acc[OG_ACC_ELE] + acc[OG_ACC_EXCESS] + S.self_energy +
+                              acc[OG_ACC_BOND] + acc[OG_ACC_ANGLE];
+        double param = lambda;
+        if (lambda <= S.mcmd_lo) param = S.mcmd_lo;
+        else if (lambda >= S.mcmd_hi) param = S.mcmd_hi;
+        double dlnp = S.mcmd_coef[0], t = 1.0;
+        for (int i = 1; i < S.mcmd_order + 1; i++) {
+            t *= param;
+            dlnp += S.mcmd_coef[i] * t;
+        }
+        f = S.mcmd_k * dlnp;
+    }
+    mcmd_factor[s] = f;
+}
+
+// vel_next -= moment of the atom's COM group (moment already divided by the group mass).
 // ------------------------------------------------------------- integrator
 
 // SubBox::cpy_vel_prev + update_velocities (SubBox.cpp:1427-1454) with McMD scaling of the
@@ -603,6 +606,42 @@ __global__ void k_energies(int n_sys, const SysDev *__restrict__ sys, const doub
     if (trace && trace_cap > 0) {
         const long long row = *trace_count % trace_cap;
         for (int q = 0; q < 11; q++) trace[(row * n_sys + s) * 11 + q] = e[q];
+    }
+}
+
+// og_put_state: continue the trajectory from host coordinates without re-enumerating pairs
+// (the role of cuda_memcpy_htod_crd + kernel_set_crd, cuda_setup.cu:124-136, 380-402): the
+// grid copy moves by the minimum-image displacement, as MiniCell::move_atom does.
+__global__ void k_put_state(int n_atoms, int atom0, const int *__restrict__ atom_sys,
+                            const SysDev *__restrict__ sys, const double *__restrict__ new_crd,
+                            const double *__restrict__ new_vel, double *__restrict__ crd,
+                            double *__restrict__ vel_next, const int *__restrict__ atom_slot,
+                            double *__restrict__ slot_crd, const double *__restrict__ cell_origin,
+                            float4 *__restrict__ xq) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_atoms) return;
+    const int a = atom0 + i;
+    const SysDev &S = sys[atom_sys[a]];
+    const int sl = atom_slot[a], c = sl >> 3;
+    float4 p = xq[sl];
+    float r[3];
+    for (int q = 0; q < 3; q++) {
+        if (new_crd) {
+            const double x = new_crd[3 * i + q];
+            double d = x - crd[3 * a + q];
+            d -= S.L[q] * nearbyint(d / S.L[q]);
+            const double g = slot_crd[3 * (size_t)sl + q] + d;
+            slot_crd[3 * (size_t)sl + q] = g;
+            r[q] = (float)(g - cell_origin[3 * c + q]);
+            crd[3 * a + q] = x;
+        }
+        if (new_vel) vel_next[3 * a + q] = new_vel[3 * i + q];
+    }
+    if (new_crd) {
+        p.x = r[0];
+        p.y = r[1];
+        p.z = r[2];
+        xq[sl] = p;
     }
 }
 

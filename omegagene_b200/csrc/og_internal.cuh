@@ -82,7 +82,10 @@ struct SysDev {
 #define OG_ACC_ANGLE 4
 #define OG_ACC_KIN 5
 #define OG_ACC_VIR 6     // 9 entries
+#define OG_ACC_PAIRS 15  // interacting pair count of the last virial-mode evaluation
 #define OG_ACC_SIZE 16
+// per-cell accumulator slots written by the pair kernel: vdw, ele, virial[9], pair count
+#define OG_CELL_ACC 12
 
 __device__ __forceinline__ unsigned int og_float_order(float f) {
     f = f + 0.0f;  // -0 -> +0 so that equal values give equal keys

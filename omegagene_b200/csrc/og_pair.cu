@@ -9,22 +9,48 @@
 //
 // B200 layout: one warp per cell1; lane = (i-group g = lane>>3, j-slot jj = lane&7); each lane
 // evaluates i = g and i = g+4 against j = jj of every cell2 in cell1's CSR range.
-// Coordinates are float offsets from a per-cell FP64 origin, so the pair distance carries the
-// rounding of a ~10 A quantity instead of the absolute coordinate.  The per-cell-pair shift
-// (origin2 + image - origin1) is formed in FP64.  Work on j is reduced over the 4 i-groups
-// with shuffles and added to an int64 fixed-point accumulator (2^-32 kcal/mol/A), which makes
-// the per-atom sums independent of launch order; i-work is summed in FP64 registers and
-// added once at the end.  Energies and the virial go to per-cell slots that a fixed-order
-// reduction sums later.
+// Coordinates are float offsets from a per-cell FP64 origin, and each cell pair carries the
+// float shift origin2 + image - origin1 formed in FP64 when the list was built, so a pair
+// distance carries the rounding of a ~10 A quantity instead of an absolute coordinate.
+// A warp-uniform test on per-step cell bounding boxes skips cell pairs that are entirely
+// beyond the cutoff (the list itself is the reference's 13 A slab list, unchanged).
+// Work on j is reduced over the 4 i-groups with shuffles and added to an int64 fixed-point
+// accumulator (2^-32 kcal/mol/A), which makes per-atom sums independent of launch order;
+// i-work and energies are summed in FP32 over at most 16 cell pairs and then folded into FP64
+// registers; energies and the virial go to per-cell slots reduced later in a fixed order.
 #include "og_internal.cuh"
 
 namespace og {
 
+// Per-cell bounding box of the real atoms (cell-relative coordinates), refreshed every step.
+__global__ void k_cell_bbox(const int *__restrict__ counters, int cells_cap, const float4 *__restrict__ xq,
+                            const unsigned char *__restrict__ cell_valid, float4 *__restrict__ bbox) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n_cells = counters[OG_CNT_N_CELLS];
+    if (c >= n_cells || c >= cells_cap) return;
+    const unsigned v = cell_valid[c];
+    float lx = 3e38f, ly = 3e38f, lz = 3e38f, hx = -3e38f, hy = -3e38f, hz = -3e38f;
+    for (int k = 0; k < OG_CELL; k++) {
+        if (!((v >> k) & 1u)) continue;
+        const float4 p = xq[c * OG_CELL + k];
+        lx = fminf(lx, p.x);
+        ly = fminf(ly, p.y);
+        lz = fminf(lz, p.z);
+        hx = fmaxf(hx, p.x);
+        hy = fmaxf(hy, p.y);
+        hz = fmaxf(hz, p.z);
+    }
+    bbox[2 * c] = make_float4(lx, ly, lz, 0.f);
+    bbox[2 * c + 1] = make_float4(hx, hy, hz, 0.f);
+}
+
+#define OG_FLUSH 16
+
 template <bool VIR>
 __global__ void __launch_bounds__(256)
 k_pair_ljzd(const int *__restrict__ counters, const int *__restrict__ cell_sys, const SysDev *__restrict__ sys,
-            const double *__restrict__ cell_origin, const float4 *__restrict__ xq, const int *__restrict__ slot_type,
-            const int *__restrict__ cp_head, const int2 *__restrict__ cp_c2img,
+            const float4 *__restrict__ bbox, const float4 *__restrict__ xq, const int *__restrict__ slot_type,
+            const int *__restrict__ cp_head, const float4 *__restrict__ cp_shift, const int2 *__restrict__ cp_c2img,
             const unsigned long long *__restrict__ cp_mask, const float2 *__restrict__ lj,
             unsigned long long *__restrict__ frc, double *__restrict__ cell_acc, long long pair_cap) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -34,33 +60,39 @@ k_pair_ljzd(const int *__restrict__ counters, const int *__restrict__ cell_sys, 
     const int c1 = warp;
     const int jj = lane & 7, g = lane >> 3;
     const SysDev &S = sys[cell_sys[c1]];
-    const double o1x = cell_origin[3 * c1], o1y = cell_origin[3 * c1 + 1], o1z = cell_origin[3 * c1 + 2];
     const float4 xi0 = xq[c1 * OG_CELL + g], xi1 = xq[c1 * OG_CELL + g + 4];
     const int ti0 = slot_type[c1 * OG_CELL + g] * S.n_types + S.lj_base;
     const int ti1 = slot_type[c1 * OG_CELL + g + 4] * S.n_types + S.lj_base;
     const float qc0 = xi0.w * (float)OG_CHARGE_COEFF, qc1 = xi1.w * (float)OG_CHARGE_COEFF;
     const float rc2 = S.cutoff2, zcore = S.zcore, bco = S.bcoeff, fco = S.fcoeff;
+    // skip threshold with a margin for the float rounding of boxes and shifts
+    const float rskip = sqrtf(rc2) + 1e-3f, rskip2 = rskip * rskip;
+    const float4 b1l = bbox[2 * c1], b1h = bbox[2 * c1 + 1];
     double f0x = 0, f0y = 0, f0z = 0, f1x = 0, f1y = 0, f1z = 0;
     double e_vdw = 0, e_ele = 0;
+    float a0x = 0.f, a0y = 0.f, a0z = 0.f, a1x = 0.f, a1y = 0.f, a1z = 0.f, av = 0.f, ae = 0.f;
+    int n_acc = 0;
+    int n_act = 0;  // interacting pairs (VIR mode only)
     double v[9];
     if (VIR)
         for (int q = 0; q < 9; q++) v[q] = 0;
     // a list that overflowed its buffer is flagged and redone; never read past the buffer
     const int k_end = (int)min((long long)cp_head[c1 + 1], pair_cap);
     for (int k = cp_head[c1]; k < k_end; k++) {
-        const int2 ci = cp_c2img[k];
+        const float4 sp = cp_shift[k];
+        const int c2 = __float_as_int(sp.w);
+        {
+            const float4 l2 = bbox[2 * c2], h2 = bbox[2 * c2 + 1];
+            const float gx = fmaxf(0.f, fmaxf(l2.x + sp.x - b1h.x, b1l.x - (h2.x + sp.x)));
+            const float gy = fmaxf(0.f, fmaxf(l2.y + sp.y - b1h.y, b1l.y - (h2.y + sp.y)));
+            const float gz = fmaxf(0.f, fmaxf(l2.z + sp.z - b1h.z, b1l.z - (h2.z + sp.z)));
+            if (gx * gx + gy * gy + gz * gz >= rskip2) continue;  // same value in every lane
+        }
         const unsigned long long m = cp_mask[k];
-        const int c2 = ci.x, img = ci.y;
-        const double shx = (img & 1) ? -S.L[0] : ((img & 2) ? S.L[0] : 0.0);
-        const double shy = (img & 4) ? -S.L[1] : ((img & 8) ? S.L[1] : 0.0);
-        const double shz = (img & 16) ? -S.L[2] : ((img & 32) ? S.L[2] : 0.0);
-        const float sx = (float)(cell_origin[3 * c2] - o1x + shx);
-        const float sy = (float)(cell_origin[3 * c2 + 1] - o1y + shy);
-        const float sz = (float)(cell_origin[3 * c2 + 2] - o1z + shz);
         const float4 xj = xq[c2 * OG_CELL + jj];
         const int tj = slot_type[c2 * OG_CELL + jj];
-        const float rjx = xj.x + sx, rjy = xj.y + sy, rjz = xj.z + sz;
-        float wjx = 0.f, wjy = 0.f, wjz = 0.f, ev = 0.f, ee = 0.f;
+        const float rjx = xj.x + sp.x, rjy = xj.y + sp.y, rjz = xj.z + sp.z;
+        float wjx = 0.f, wjy = 0.f, wjz = 0.f;
 #pragma unroll
         for (int t = 0; t < 2; t++) {
             const float4 xi = t ? xi1 : xi0;
@@ -69,7 +101,12 @@ k_pair_ljzd(const int *__restrict__ counters, const int *__restrict__ cell_sys, 
             const int bit = jj * OG_CELL + g + 4 * t;
             const bool act = (((m >> bit) & 1ull) == 0ull) && (r2 < rc2);
             const float r2s = act ? r2 : 1.0f;
-            const float rinv = rsqrtf(r2s);
+            // hardware estimate + one Newton step on the exact residual 1 - r2 y^2 (FMA):
+            // the estimate alone carries a one-sided error that adds up over millions of
+            // Coulomb pairs in the energy
+            float rinv = rsqrtf(r2s);
+            const float hres = fmaf(-r2s * rinv, rinv, 1.0f);
+            rinv = fmaf(0.5f * rinv, hres, rinv);
             const float r2inv = rinv * rinv;
             const float r6inv = r2inv * r2inv * r2inv;
             const float2 p = __ldg(&lj[(t ? ti1 : ti0) + tj]);
@@ -79,17 +116,24 @@ k_pair_ljzd(const int *__restrict__ counters, const int *__restrict__ cell_sys, 
             float pe = cc * (rinv - zcore + bco * r2s);
             float wc = r2inv * (6.0f * t6 - 12.0f * t12) - cc * (rinv * r2inv - fco);
             if (!act) { pv = 0.f; pe = 0.f; wc = 0.f; }
+            if (VIR) n_act += act ? 1 : 0;
             const float wx = wc * dx, wy = wc * dy, wz = wc * dz;
-            ev += pv;
-            ee += pe;
+            av += pv;
+            ae += pe;
             wjx -= wx;
             wjy -= wy;
             wjz -= wz;
-            if (t) { f1x += wx; f1y += wy; f1z += wz; }
-            else { f0x += wx; f0y += wy; f0z += wz; }
+            if (t) { a1x += wx; a1y += wy; a1z += wz; }
+            else { a0x += wx; a0y += wy; a0z += wz; }
         }
-        e_vdw += ev;
-        e_ele += ee;
+        if (++n_acc == OG_FLUSH) {
+            f0x += a0x; f0y += a0y; f0z += a0z;
+            f1x += a1x; f1y += a1y; f1z += a1z;
+            e_vdw += av;
+            e_ele += ae;
+            a0x = a0y = a0z = a1x = a1y = a1z = av = ae = 0.f;
+            n_acc = 0;
+        }
         // work on j: sum over the four i-groups (lanes jj, jj+8, jj+16, jj+24)
         wjx += __shfl_xor_sync(0xffffffffu, wjx, 8);
         wjy += __shfl_xor_sync(0xffffffffu, wjy, 8);
@@ -102,15 +146,24 @@ k_pair_ljzd(const int *__restrict__ counters, const int *__restrict__ cell_sys, 
             atomicAdd(fj + 0, (unsigned long long)__float2ll_rn(wjx * (float)OG_FIX_SCALE));
             atomicAdd(fj + 1, (unsigned long long)__float2ll_rn(wjy * (float)OG_FIX_SCALE));
             atomicAdd(fj + 2, (unsigned long long)__float2ll_rn(wjz * (float)OG_FIX_SCALE));
-            if (VIR && img != 0) {
-                // sum over pairs of d (x) f = sum_atoms x (x) F + sum_cell-pairs shift (x) F_j
-                const double sh[3] = {shx, shy, shz};
-                const double fjv[3] = {-(double)wjx, -(double)wjy, -(double)wjz};
-                for (int a = 0; a < 3; a++)
-                    for (int b = 0; b < 3; b++) v[a * 3 + b] += sh[a] * fjv[b];
+            if (VIR) {
+                const int img = cp_c2img[k].y;
+                if (img != 0) {
+                    // sum over pairs of d (x) f = sum_atoms x (x) F + sum_cell-pairs shift (x) F_j
+                    const double sh[3] = {(img & 1) ? -S.L[0] : ((img & 2) ? S.L[0] : 0.0),
+                                          (img & 4) ? -S.L[1] : ((img & 8) ? S.L[1] : 0.0),
+                                          (img & 16) ? -S.L[2] : ((img & 32) ? S.L[2] : 0.0)};
+                    const double fjv[3] = {-(double)wjx, -(double)wjy, -(double)wjz};
+                    for (int a = 0; a < 3; a++)
+                        for (int b = 0; b < 3; b++) v[a * 3 + b] += sh[a] * fjv[b];
+                }
             }
         }
     }
+    f0x += a0x; f0y += a0y; f0z += a0z;
+    f1x += a1x; f1y += a1y; f1z += a1z;
+    e_vdw += av;
+    e_ele += ae;
     // work on i: sum over the 8 j lanes of each i-group
 #pragma unroll
     for (int o = 1; o < 8; o <<= 1) {
@@ -143,21 +196,26 @@ k_pair_ljzd(const int *__restrict__ counters, const int *__restrict__ cell_sys, 
     if (VIR) {
         for (int q = 0; q < 9; q++)
             for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+        for (int o = 16; o > 0; o >>= 1) n_act += __shfl_xor_sync(0xffffffffu, n_act, o);
     }
     if (lane == 0) {
-        double *acc = cell_acc + (size_t)c1 * 11;
+        double *acc = cell_acc + (size_t)c1 * OG_CELL_ACC;
         acc[0] = e_vdw;
         acc[1] = e_ele;
-        if (VIR)
+        if (VIR) {
             for (int q = 0; q < 9; q++) acc[2 + q] = v[q];
+            acc[11] = (double)n_act;
+        }
     }
 }
 
-template __global__ void k_pair_ljzd<true>(const int *, const int *, const SysDev *, const double *, const float4 *,
-                                           const int *, const int *, const int2 *, const unsigned long long *,
-                                           const float2 *, unsigned long long *, double *, long long);
-template __global__ void k_pair_ljzd<false>(const int *, const int *, const SysDev *, const double *, const float4 *,
-                                            const int *, const int *, const int2 *, const unsigned long long *,
-                                            const float2 *, unsigned long long *, double *, long long);
+template __global__ void k_pair_ljzd<true>(const int *, const int *, const SysDev *, const float4 *, const float4 *,
+                                           const int *, const int *, const float4 *, const int2 *,
+                                           const unsigned long long *, const float2 *, unsigned long long *,
+                                           double *, long long);
+template __global__ void k_pair_ljzd<false>(const int *, const int *, const SysDev *, const float4 *, const float4 *,
+                                            const int *, const int *, const float4 *, const int2 *,
+                                            const unsigned long long *, const float2 *, unsigned long long *,
+                                            double *, long long);
 
 }  // namespace og

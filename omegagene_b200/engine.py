@@ -79,7 +79,10 @@ def load_library():
         "og_set_trace": [E, C.c_int32], "og_get_trace": [E, C.c_void_p, C.c_int32, _p(C.c_int32)],
         "og_get_stats": [E, _p(C.c_int64), _p(C.c_double), _p(C.c_double)],
         "og_get_sizes": [E, _p(C.c_int32), _p(C.c_int64)], "og_set_timing": [E, C.c_int32],
-        "og_get_flags": [E, _p(C.c_int32)],
+        "og_get_flags": [E, _p(C.c_int32)], "og_put_state": [E, C.c_int32, C.c_void_p, C.c_void_p],
+        "og_get_state_async": [E, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p],
+        "og_step_async": [E, C.c_int32], "og_synchronize": [E],
+        "og_get_pair_count": [E, C.c_int32, _p(C.c_int64)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -355,3 +358,22 @@ class Engine:
         f = C.c_int32()
         self._check(self.L.og_get_flags(self.h, C.byref(f)), "og_get_flags")
         return f.value
+
+    # ---- stream-ordered calls for callers that keep state in (pinned) host memory
+    def put_state_ptr(self, sys, crd_ptr, vel_ptr):
+        self._check(self.L.og_put_state(self.h, sys, crd_ptr, vel_ptr), "og_put_state")
+
+    def get_state_async_ptr(self, sys, crd_ptr, vel_ptr, ene_ptr):
+        self._check(self.L.og_get_state_async(self.h, sys, crd_ptr, vel_ptr, ene_ptr), "og_get_state_async")
+
+    def step_async(self, n=1):
+        self._check(self.L.og_step_async(self.h, int(n)), "og_step_async")
+
+    def synchronize(self):
+        self._check(self.L.og_synchronize(self.h), "og_synchronize")
+
+    def pair_count(self, sys):
+        """Interacting pairs (r < cutoff, not excluded) of the last og_compute_forces."""
+        n = C.c_int64()
+        self._check(self.L.og_get_pair_count(self.h, sys, C.byref(n)), "og_get_pair_count")
+        return n.value

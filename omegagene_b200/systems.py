@@ -120,13 +120,18 @@ def _assemble(crd, vel, box, charge, mass, atom_type, lj_types, bonds, angles, e
     lo = -0.5 * box
     # box centred on the origin (pbc_val[9..11] is the box centre, PBC.cpp:36)
     crd = _wrap(crd - 0.5 * box, lo, box)
+    lj_pairs = _lj_records(lj_types)
+    # Read::load_ls_tpl reads one HPS record per LJ type pair whatever the section size says
+    # (Read.cpp:323-334), so the records are written (unused by the LJ model)
+    hps = np.zeros(len(lj_pairs), dtype=[("t1", "<i4"), ("t2", "<i4"), ("cutoff", "<f8"), ("lambda", "<f8")])
+    hps["t1"], hps["t2"] = lj_pairs["t1"], lj_pairs["t2"]
     topol = {
         "charge": np.asarray(charge, np.float64),
         "mass": np.asarray(mass, np.float64),
         "atom_type": np.asarray(atom_type, np.int32),
         "n_lj_types": len(lj_types),
-        "lj_pairs": _lj_records(lj_types),
-        "lj_hps_raw": b"",
+        "lj_pairs": lj_pairs,
+        "lj_hps_raw": hps.tobytes(),
         "bonds": bonds if bonds is not None else np.zeros(0, [("a1", "<i4"), ("a2", "<i4"), ("k", "<f8"), ("r0", "<f8")]),
         "angles": angles if angles is not None else np.zeros(0, [("a1", "<i4"), ("a2", "<i4"), ("a3", "<i4"), ("k", "<f8"), ("t0", "<f8")]),
         "torsions_raw": b"\0\0\0\0", "impros_raw": b"\0\0\0\0", "nb14_raw": b"\0\0\0\0",
@@ -145,15 +150,19 @@ def _assemble(crd, vel, box, charge, mass, atom_type, lj_types, bonds, angles, e
     return out
 
 
-def _saw_chain(rng, n_backbone, radius, bond=1.53, angle_deg=111.0, min_dist=2.4, max_tries=200):
+def _saw_chain(rng, n_backbone, radius, bond=1.53, angle_deg=111.0, min_dist=3.2, max_tries=200):
     """Self-avoiding random walk with fixed bond length and bond angle, confined to a sphere."""
     theta = math.radians(angle_deg)
     pts = [np.zeros(3)]
     d0 = rng.normal(size=3)
     d0 /= np.linalg.norm(d0)
     pts.append(pts[0] + bond * d0)
+    restarts = 0
     while len(pts) < n_backbone:
         ok = False
+        if restarts > 50:  # dense packing: relax the exclusion distance instead of looping
+            min_dist *= 0.9
+            restarts = 0
         for _ in range(max_tries):
             prev = pts[-1] - pts[-2]
             prev /= np.linalg.norm(prev)
@@ -173,6 +182,7 @@ def _saw_chain(rng, n_backbone, radius, bond=1.53, angle_deg=111.0, min_dist=2.4
             break
         if not ok:  # restart the walk from a shorter prefix
             del pts[max(2, len(pts) - 20):]
+            restarts += 1
     return np.asarray(pts)
 
 
@@ -182,7 +192,7 @@ def chain_water_system(n_chain=2000, n_waters=30000, seed=1, radius=30.0, box=No
     the preceding backbone atom; backbone bonds 1.53 A / 310, angles 111 deg / 63 (E = k(x-x0)^2,
     ForceField.cpp:108-177).  Charges ~ N(0, 0.25) shifted to zero net; sigma ~ U(2.5, 3.8),
     epsilon ~ U(0.02, 0.2) binned into n_sigma_bins x n_eps_bins LJ types with Lorentz-Berthelot
-    mixing.  Waters within 2.4 A of the solute are removed.  Exclusions: 1-2 and 1-3 pairs."""
+    mixing.  Waters within 2.4 A of the solute are removed.  Exclusions: 1-2, 1-3 and 1-4 pairs."""
     rng = np.random.default_rng(seed)
     n_h = n_chain // 3
     n_bb = n_chain - n_h
@@ -204,10 +214,32 @@ def chain_water_system(n_chain=2000, n_waters=30000, seed=1, radius=30.0, box=No
     n_c = idx
     crd_c = np.zeros((n_c, 3))
     crd_c[bb_index] = bb
+    pos_of_bb = {idx: k for k, idx in enumerate(bb_index)}
+    placed = list(bb_index)
     for h, p in parent_of_h.items():
-        v = rng.normal(size=3)
-        v /= np.linalg.norm(v)
-        crd_c[h] = crd_c[p] + 1.09 * v
+        # start on the outer bisector of the parent's backbone angle; keep the direction that
+        # leaves the H farthest from every other chain atom
+        k = pos_of_bb[p]
+        v0 = np.zeros(3)
+        for kk in (k - 1, k + 1):
+            if 0 <= kk < n_bb:
+                d = bb[k] - bb[kk]
+                v0 += d / np.linalg.norm(d)
+        if np.linalg.norm(v0) < 1e-6:
+            v0 = rng.normal(size=3)
+        best, best_d = None, -1.0
+        others = np.asarray([crd_c[i] for i in placed if i != p])
+        for t in range(64):
+            v = v0 / np.linalg.norm(v0) if t == 0 else v0 / np.linalg.norm(v0) + 0.8 * rng.normal(size=3)
+            v /= np.linalg.norm(v)
+            cand = crd_c[p] + 1.09 * v
+            dmin = np.min(np.linalg.norm(others - cand, axis=1)) if len(others) else 9.0
+            if dmin > best_d:
+                best, best_d = cand, dmin
+            if dmin >= 2.6:
+                break
+        crd_c[h] = best
+        placed.append(h)
     sig = rng.uniform(2.5, 3.8, n_c)
     eps = rng.uniform(0.02, 0.2, n_c)
     sb = np.minimum((sig - 2.5) / 1.3 * n_sigma_bins, n_sigma_bins - 1).astype(int)
@@ -239,19 +271,24 @@ def chain_water_system(n_chain=2000, n_waters=30000, seed=1, radius=30.0, box=No
     angles = [(bb_index[i], bb_index[i + 1], bb_index[i + 2], 63.0, math.radians(111.0)) for i in range(n_bb - 2)]
     bonds = np.array(bonds, dtype=[("a1", "<i4"), ("a2", "<i4"), ("k", "<f8"), ("r0", "<f8")])
     angles = np.array(angles, dtype=[("a1", "<i4"), ("a2", "<i4"), ("a3", "<i4"), ("k", "<f8"), ("t0", "<f8")])
-    excl = set()
+    # 1-2, 1-3 and 1-4 pairs are excluded from the pair list (the reference's "nb15off")
+    adj = {i: set() for i in range(n_c)}
     for b in bonds:
-        excl.add((int(b["a1"]), int(b["a2"])))
-    for a in angles:
-        excl.add((int(a["a1"]), int(a["a3"])))
+        adj[int(b["a1"])].add(int(b["a2"]))
+        adj[int(b["a2"])].add(int(b["a1"]))
     for h, p in parent_of_h.items():
-        excl.add((p, h))
-        # the H and the backbone neighbours of its parent are 1-3
-        k = bb_index.index(p)
-        for kk in (k - 1, k + 1):
-            if 0 <= kk < n_bb:
-                excl.add((min(h, bb_index[kk]), max(h, bb_index[kk])))
-    excl = np.array(sorted((min(a, b), max(a, b)) for a, b in excl), np.int64)
+        adj[h].add(p)
+        adj[p].add(h)
+    excl = set()
+    for i in range(n_c):
+        frontier, seen = {i}, {i}
+        for _ in range(3):
+            frontier = {j for f in frontier for j in adj[f]} - seen
+            seen |= frontier
+        for j in seen:
+            if j > i:
+                excl.add((i, j))
+    excl = np.array(sorted(excl), np.int64).reshape(-1, 2)
     excl = np.concatenate([excl, _water_exclusions(n_c, nw)])
     pairs = (np.array([(p, h) for h, p in sorted(parent_of_h.items())], np.int32),
              np.full(len(parent_of_h), 1.09))

@@ -356,13 +356,13 @@ class OracleMD:
         b = t.get("bonds")
         self.bonds = None
         if b is not None and len(b):
-            self.bonds = (np.stack([b["a1"], b["a2"]], 1).astype(np.int32).reshape(-1), np.asarray(b["k"], np.float64),
-                          np.asarray(b["r0"], np.float64))
+            self.bonds = (np.ascontiguousarray(np.stack([b["a1"], b["a2"]], 1).astype(np.int32).reshape(-1)),
+                          np.ascontiguousarray(b["k"], np.float64), np.ascontiguousarray(b["r0"], np.float64))
         a = t.get("angles")
         self.angles = None
         if a is not None and len(a):
-            self.angles = (np.stack([a["a1"], a["a2"], a["a3"]], 1).astype(np.int32).reshape(-1),
-                           np.asarray(a["k"], np.float64), np.asarray(a["t0"], np.float64))
+            self.angles = (np.ascontiguousarray(np.stack([a["a1"], a["a2"], a["a3"]], 1).astype(np.int32).reshape(-1)),
+                           np.ascontiguousarray(a["k"], np.float64), np.ascontiguousarray(a["t0"], np.float64))
         cons = system.get("constraint")
         use_cons = cons is not None and self.p.get("constraint", "shake") != "none"
         self.pa = np.asarray(cons["pair_atoms"], np.int32).reshape(-1) if use_cons else np.zeros(0, np.int32)

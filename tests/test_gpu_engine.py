@@ -157,12 +157,14 @@ def test_mcmd_scaling_matches_oracle():
     p = _params(nsgrid_update_intvl=10, time_step=2.0)
     md0 = ogo.OracleMD(s, p)
     e0 = md0.forces()["potential"]
-    mcmd = {"coef": [1.0, 2e-5, 1e-9, 0, 0, 0, 1e-24], "lambda_low": e0 - 2000.0, "lambda_high": e0 + 2000.0,
+    # d lnP / dE as a polynomial in E with RT dlnP/dE = O(1), as a McMD run uses it
+    mcmd = {"coef": [1.678, 2e-5, 1e-9, 0, 0, 0, 1e-24], "lambda_low": e0 - 2000.0, "lambda_high": e0 + 2000.0,
             "temperature": 300.0}
     eng, md, ref, tr = _run_both(s, p, 6, mcmd)
     names = engine.ENERGY_NAMES
     for i, r in enumerate(ref):
-        assert abs(tr[i, names.index("mcmd_factor")] - r["mcmd_factor"]) <= 1e-9 * abs(r["mcmd_factor"])
+        assert 0.5 < r["mcmd_factor"] < 2.0
+        assert abs(tr[i, names.index("mcmd_factor")] - r["mcmd_factor"]) <= 1e-7 * abs(r["mcmd_factor"])
         assert abs(tr[i, names.index("potential")] - r["potential"]) <= 1e-5 * abs(r["potential"]) + 5e-3
 
 
@@ -171,7 +173,7 @@ def test_batch_invariance_bitwise():
     per-system fixed-order reductions)."""
     a = systems.water_system(1500, seed=5)
     others = [systems.water_system(700, seed=9), systems.chain_water_system(300, 2500, seed=4, radius=12.0)]
-    p = _params(nsgrid_update_intvl=10, time_step=2.0)
+    p = _params(nsgrid_update_intvl=10, time_step=2.0, thermostat="scaling", temperature=300.0)
     alone = _engine([(a, p, None)])
     alone.set_trace(25)
     alone.step(25)
@@ -190,7 +192,7 @@ def test_nve_drift_small():
     s = systems.water_system(3000, box=44.8, seed=0, lattice_m=15)
     warm = _params(nsgrid_update_intvl=10, time_step=0.5, thermostat="scaling", temperature=300.0)
     eng = _engine([(s, warm, None)])
-    eng.step(600)
+    eng.step(2000)
     crd, vel = eng.get_state(0)
     s2 = dict(s)
     s2["crd"], s2["vel"] = crd, vel
