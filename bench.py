@@ -214,6 +214,7 @@ def run_ours(args, world, rank, local, pg):
     eng = engine.Engine(local)
     eng.add_system(s, p)
     eng.finalize()
+    tuning = eng.tuning()
     n_atoms = s["n_atoms"]
     del s
     # warm-up (untimed)
@@ -286,7 +287,7 @@ def run_ours(args, world, rank, local, pg):
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp32_peak, "traffic": traffic,
                      "kernel": "k_pair_ljzd", "pair_kernel_ms": pair_ms, "interacting_pairs": n_int,
-                     "flop_per_pair": FLOP_PER_PAIR,
+                     "flop_per_pair": FLOP_PER_PAIR, "autotune": tuning,
                      "peak_note": "FP32 CUDA-core peak = 148 SMs x 128 lanes x 2 x %.0f MHz (nominal at the "
                                   "measured max SM clock; MEASURED_PEAKS.json has no FP32 figure)" % sm_max},
         "e2e": e2e, "gpu_launches": launches, "clocks": clk, "device_flags": flags,

@@ -176,6 +176,9 @@ og_status og_set_timing(og_engine *e, int32_t on);
  * bit 16 = the thermostat loop hit thermo_const_max_loops (both non-fatal, as in the reference,
  * which prints a warning and continues: ConstraintShake.cpp:135-139, Thermostat.cpp:168). */
 og_status og_get_flags(og_engine *e, int32_t *flags);
+/* Autotuner result: the pair-kernel variant in use (register budget 100/80/64 per thread) and
+ * the best time of each variant on the first list, in ms. */
+og_status og_get_tuning(og_engine *e, int32_t *pair_variant, double *variant_ms);
 /* Number of systems and atoms held. */
 og_status og_get_sizes(og_engine *e, int32_t *n_systems, int64_t *n_atoms_total);
 

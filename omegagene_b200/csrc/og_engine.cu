@@ -3,7 +3,9 @@
 // Owns every device buffer of a batch of systems, computes the MiniCell geometry on the host
 // with the reference's float arithmetic (MiniCell.cpp:221-290, 1279-1303), and sequences the
 // kernels of one DynamicsModePresto step (DynamicsMode.cpp:468-560) on one CUDA stream.
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -35,7 +37,7 @@ __global__ void k_pair_heads(int *, int, int, const int *, int *);
 __global__ void k_scan_block(const int *, int *, long long, int *);
 __global__ void k_scan_add(int *, long long, const int *);
 // og_pair.cu
-template <bool VIR>
+template <bool VIR, int MINB>
 __global__ void k_pair_ljzd(const int *, const int *, const SysDev *, const float4 *, const float4 *, const int *,
                             const int *, const float4 *, const int2 *, const unsigned long long *, const float2 *,
                             unsigned long long *, double *, long long);
@@ -205,6 +207,8 @@ struct og_engine {
     int pev_used = 0;
     double *d_stage = nullptr;            // og_put_state staging (6 doubles per atom)
     double pair_ms = 0.0, step_ms = 0.0;
+    int pair_variant = 0;
+    double variant_ms[3] = {0, 0, 0};
     bool timing = false;
     std::vector<void *> allocs;
 };
@@ -444,6 +448,22 @@ og_status build_list(og_engine *e) {
 
 // ---------------------------------------------------------- forces
 
+#define PAIR_ARGS                                                                                            \
+    e->d_counters, e->d_cell_sys, e->d_sys, e->d_bbox, e->d_xq, e->d_slot_type, e->d_cp_head, e->d_cp_shift, \
+        e->d_cp_c2img, e->d_cp_mask, e->d_lj, e->d_frc, e->d_cell_acc, e->pair_cap
+
+// Pair kernel variants differ in the register budget per thread (resident blocks per SM).
+og_status launch_pair(og_engine *e, bool vir, int variant) {
+    const unsigned nb = blocks((long long)e->cells_cap * 32, 256);
+    cudaStream_t st = e->stream;
+    if (vir) k_pair_ljzd<true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    else if (variant == 1) k_pair_ljzd<false, 3><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    else if (variant == 2) k_pair_ljzd<false, 4><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    else k_pair_ljzd<false, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    LAUNCH_CHECK();
+    return OG_OK;
+}
+
 og_status reduce_potential(og_engine *e);
 og_status reduce_virial(og_engine *e);
 
@@ -463,15 +483,10 @@ og_status compute_forces(og_engine *e, bool vir) {
         }
         CK(cudaEventRecord(e->pev0[e->pev_used], st));
     }
-    if (vir)
-        k_pair_ljzd<true><<<pair_blocks, 256, 0, st>>>(e->d_counters, e->d_cell_sys, e->d_sys, e->d_bbox, e->d_xq,
-                                                       e->d_slot_type, e->d_cp_head, e->d_cp_shift, e->d_cp_c2img,
-                                                       e->d_cp_mask, e->d_lj, e->d_frc, e->d_cell_acc, e->pair_cap);
-    else
-        k_pair_ljzd<false><<<pair_blocks, 256, 0, st>>>(e->d_counters, e->d_cell_sys, e->d_sys, e->d_bbox, e->d_xq,
-                                                        e->d_slot_type, e->d_cp_head, e->d_cp_shift, e->d_cp_c2img,
-                                                        e->d_cp_mask, e->d_lj, e->d_frc, e->d_cell_acc, e->pair_cap);
-    LAUNCH_CHECK();
+    {
+        og_status ps = launch_pair(e, vir, vir ? 0 : e->pair_variant);
+        if (ps) return ps;
+    }
     if (e->timing) CK(cudaEventRecord(e->pev1[e->pev_used++], st));
     if (vir) {
         if (!e->d_vir_atom) {
@@ -740,6 +755,41 @@ og_status build_list_checked(og_engine *e) {
         return check_flags(e);
     }
     return fail(e, OG_ERR_CAPACITY, "cell-pair list did not fit after growing");
+}
+
+// Times each pair-kernel variant on the first list (3 launches each, best of three) and keeps
+// the fastest; OG_PAIR_VARIANT=0/1/2 in the environment fixes the choice.  The trial launches
+// write the force accumulators, which are cleared afterwards.
+og_status autotune_pair(og_engine *e) {
+    const char *env = getenv("OG_PAIR_VARIANT");
+    if (env && *env) {
+        e->pair_variant = atoi(env) % 3;
+        return OG_OK;
+    }
+    k_cell_bbox<<<blocks(e->cells_cap, 256), 256, 0, e->stream>>>(e->d_counters, e->cells_cap, e->d_xq,
+                                                                   e->d_cell_valid, e->d_bbox);
+    LAUNCH_CHECK();
+    double best = 1e30;
+    for (int v = 0; v < 3; v++) {
+        double vbest = 1e30;
+        for (int rep = 0; rep < 3; rep++) {
+            CK(cudaEventRecord(e->ev_pair0, e->stream));
+            og_status s = launch_pair(e, false, v);
+            if (s) return s;
+            CK(cudaEventRecord(e->ev_pair1, e->stream));
+            CK(cudaEventSynchronize(e->ev_pair1));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, e->ev_pair0, e->ev_pair1));
+            vbest = std::min(vbest, (double)ms);
+        }
+        e->variant_ms[v] = vbest;
+        if (vbest < best) {
+            best = vbest;
+            e->pair_variant = v;
+        }
+    }
+    CK(cudaMemsetAsync(e->d_frc, 0, sizeof(unsigned long long) * 3 * (size_t)e->slots_cap, e->stream));
+    return OG_OK;
 }
 
 }  // namespace
@@ -1127,6 +1177,7 @@ og_status og_finalize(og_engine *e) {
     e->host_step = 0;
     // initial list + forces (DynamicsMode::initial_preprocess -> calc_energy_force)
     if ((s = build_list_checked(e))) return s;
+    if ((s = autotune_pair(e))) return s;
     if ((s = compute_forces(e, false))) return s;
     CK(cudaStreamSynchronize(e->stream));
     return check_flags(e);
@@ -1467,5 +1518,13 @@ extern "C" og_status og_get_pair_count(og_engine *e, int32_t sys, int64_t *n_pai
     double v = 0;
     CK(cudaMemcpy(&v, e->d_sys_acc + OG_ACC_SIZE * sys + OG_ACC_PAIRS, sizeof(double), cudaMemcpyDeviceToHost));
     *n_pairs = (int64_t)v;
+    return OG_OK;
+}
+
+extern "C" og_status og_get_tuning(og_engine *e, int32_t *pair_variant, double *variant_ms) {
+    if (!e) return OG_ERR_INVALID;
+    if (pair_variant) *pair_variant = e->pair_variant;
+    if (variant_ms)
+        for (int v = 0; v < 3; v++) variant_ms[v] = e->variant_ms[v];
     return OG_OK;
 }

@@ -46,8 +46,10 @@ __global__ void k_cell_bbox(const int *__restrict__ counters, int cells_cap, con
 
 #define OG_FLUSH 16
 
-template <bool VIR>
-__global__ void __launch_bounds__(256)
+// MINB = minimum resident blocks per SM the register allocation must allow (2: ~100 registers,
+// 3: 80, 4: 64 with a few spills); the engine's autotuner times the variants on the first list.
+template <bool VIR, int MINB>
+__global__ void __launch_bounds__(256, MINB)
 k_pair_ljzd(const int *__restrict__ counters, const int *__restrict__ cell_sys, const SysDev *__restrict__ sys,
             const float4 *__restrict__ bbox, const float4 *__restrict__ xq, const int *__restrict__ slot_type,
             const int *__restrict__ cp_head, const float4 *__restrict__ cp_shift, const int2 *__restrict__ cp_c2img,
@@ -68,87 +70,149 @@ k_pair_ljzd(const int *__restrict__ counters, const int *__restrict__ cell_sys, 
     // skip threshold with a margin for the float rounding of boxes and shifts
     const float rskip = sqrtf(rc2) + 1e-3f, rskip2 = rskip * rskip;
     const float4 b1l = bbox[2 * c1], b1h = bbox[2 * c1 + 1];
-    double f0x = 0, f0y = 0, f0z = 0, f1x = 0, f1y = 0, f1z = 0;
-    double e_vdw = 0, e_ele = 0;
+    // FP64 accumulators of this warp's cell1 in shared memory: work of its 8 atoms and the two
+    // energies; FP32 partials in registers are folded in every OG_FLUSH cell pairs
+    __shared__ double s_acc[8][OG_CELL * 3 + 2];
+    double *acc_w = s_acc[(threadIdx.x >> 5) & 7];
+    if (lane < OG_CELL * 3 + 2) acc_w[lane] = 0.0;
+    __syncwarp();
     float a0x = 0.f, a0y = 0.f, a0z = 0.f, a1x = 0.f, a1y = 0.f, a1z = 0.f, av = 0.f, ae = 0.f;
     int n_acc = 0;
+    auto flush = [&]() {
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+            a0x += __shfl_xor_sync(0xffffffffu, a0x, o);
+            a0y += __shfl_xor_sync(0xffffffffu, a0y, o);
+            a0z += __shfl_xor_sync(0xffffffffu, a0z, o);
+            a1x += __shfl_xor_sync(0xffffffffu, a1x, o);
+            a1y += __shfl_xor_sync(0xffffffffu, a1y, o);
+            a1z += __shfl_xor_sync(0xffffffffu, a1z, o);
+        }
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            av += __shfl_xor_sync(0xffffffffu, av, o);
+            ae += __shfl_xor_sync(0xffffffffu, ae, o);
+        }
+        if (jj == 0) {
+            acc_w[3 * g + 0] += a0x;
+            acc_w[3 * g + 1] += a0y;
+            acc_w[3 * g + 2] += a0z;
+            acc_w[3 * (g + 4) + 0] += a1x;
+            acc_w[3 * (g + 4) + 1] += a1y;
+            acc_w[3 * (g + 4) + 2] += a1z;
+        }
+        if (lane == 0) {
+            acc_w[OG_CELL * 3] += av;
+            acc_w[OG_CELL * 3 + 1] += ae;
+        }
+        a0x = a0y = a0z = a1x = a1y = a1z = av = ae = 0.f;
+        n_acc = 0;
+    };
     int n_act = 0;  // interacting pairs (VIR mode only)
     double v[9];
     if (VIR)
         for (int q = 0; q < 9; q++) v[q] = 0;
     // a list that overflowed its buffer is flagged and redone; never read past the buffer
+    const int k_beg = cp_head[c1];
     const int k_end = (int)min((long long)cp_head[c1 + 1], pair_cap);
-    for (int k = cp_head[c1]; k < k_end; k++) {
-        const float4 sp = cp_shift[k];
-        const int c2 = __float_as_int(sp.w);
-        {
+    for (int chunk = k_beg; chunk < k_end; chunk += 32) {
+        // each lane fetches one cell-pair record and tests its bounding boxes; the warp then
+        // walks the surviving pairs with the next pair's j atom prefetched
+        const int kk = chunk + lane;
+        float4 my_sp = make_float4(0.f, 0.f, 0.f, 0.f);
+        unsigned long long my_m = ~0ull;
+        int my_img = 0;
+        bool keep = false;
+        if (kk < k_end) {
+            my_sp = cp_shift[kk];
+            const int c2 = __float_as_int(my_sp.w);
             const float4 l2 = bbox[2 * c2], h2 = bbox[2 * c2 + 1];
-            const float gx = fmaxf(0.f, fmaxf(l2.x + sp.x - b1h.x, b1l.x - (h2.x + sp.x)));
-            const float gy = fmaxf(0.f, fmaxf(l2.y + sp.y - b1h.y, b1l.y - (h2.y + sp.y)));
-            const float gz = fmaxf(0.f, fmaxf(l2.z + sp.z - b1h.z, b1l.z - (h2.z + sp.z)));
-            if (gx * gx + gy * gy + gz * gz >= rskip2) continue;  // same value in every lane
+            const float gx = fmaxf(0.f, fmaxf(l2.x + my_sp.x - b1h.x, b1l.x - (h2.x + my_sp.x)));
+            const float gy = fmaxf(0.f, fmaxf(l2.y + my_sp.y - b1h.y, b1l.y - (h2.y + my_sp.y)));
+            const float gz = fmaxf(0.f, fmaxf(l2.z + my_sp.z - b1h.z, b1l.z - (h2.z + my_sp.z)));
+            keep = gx * gx + gy * gy + gz * gz < rskip2;
+            if (keep) my_m = cp_mask[kk];
+            if (VIR && keep) my_img = cp_c2img[kk].y;
         }
-        const unsigned long long m = cp_mask[k];
-        const float4 xj = xq[c2 * OG_CELL + jj];
-        const int tj = slot_type[c2 * OG_CELL + jj];
-        const float rjx = xj.x + sp.x, rjy = xj.y + sp.y, rjz = xj.z + sp.z;
-        float wjx = 0.f, wjy = 0.f, wjz = 0.f;
+        unsigned ballot = __ballot_sync(0xffffffffu, keep);
+        if (!ballot) continue;
+        int src = __ffs(ballot) - 1;
+        ballot &= ballot - 1;
+        float4 sp;
+        sp.x = __shfl_sync(0xffffffffu, my_sp.x, src);
+        sp.y = __shfl_sync(0xffffffffu, my_sp.y, src);
+        sp.z = __shfl_sync(0xffffffffu, my_sp.z, src);
+        sp.w = __shfl_sync(0xffffffffu, my_sp.w, src);
+        int c2 = __float_as_int(sp.w);
+        float4 xj = xq[c2 * OG_CELL + jj];
+        int tj = slot_type[c2 * OG_CELL + jj];
+        while (true) {
+            const unsigned long long m = __shfl_sync(0xffffffffu, my_m, src);
+            const int img = VIR ? __shfl_sync(0xffffffffu, my_img, src) : 0;
+            const int cur_c2 = c2;
+            const float4 cur_sp = sp, cur_xj = xj;
+            const int cur_tj = tj;
+            const bool more = ballot != 0;
+            if (more) {  // prefetch the next surviving pair
+                src = __ffs(ballot) - 1;
+                ballot &= ballot - 1;
+                sp.x = __shfl_sync(0xffffffffu, my_sp.x, src);
+                sp.y = __shfl_sync(0xffffffffu, my_sp.y, src);
+                sp.z = __shfl_sync(0xffffffffu, my_sp.z, src);
+                sp.w = __shfl_sync(0xffffffffu, my_sp.w, src);
+                c2 = __float_as_int(sp.w);
+                xj = xq[c2 * OG_CELL + jj];
+                tj = slot_type[c2 * OG_CELL + jj];
+            }
+            const float rjx = cur_xj.x + cur_sp.x, rjy = cur_xj.y + cur_sp.y, rjz = cur_xj.z + cur_sp.z;
+            float wjx = 0.f, wjy = 0.f, wjz = 0.f;
 #pragma unroll
-        for (int t = 0; t < 2; t++) {
-            const float4 xi = t ? xi1 : xi0;
-            const float dx = xi.x - rjx, dy = xi.y - rjy, dz = xi.z - rjz;
-            const float r2 = dx * dx + dy * dy + dz * dz;
-            const int bit = jj * OG_CELL + g + 4 * t;
-            const bool act = (((m >> bit) & 1ull) == 0ull) && (r2 < rc2);
-            const float r2s = act ? r2 : 1.0f;
-            // hardware estimate + one Newton step on the exact residual 1 - r2 y^2 (FMA):
-            // the estimate alone carries a one-sided error that adds up over millions of
-            // Coulomb pairs in the energy
-            float rinv = rsqrtf(r2s);
-            const float hres = fmaf(-r2s * rinv, rinv, 1.0f);
-            rinv = fmaf(0.5f * rinv, hres, rinv);
-            const float r2inv = rinv * rinv;
-            const float r6inv = r2inv * r2inv * r2inv;
-            const float2 p = __ldg(&lj[(t ? ti1 : ti0) + tj]);
-            const float t6 = p.x * r6inv, t12 = p.y * r6inv * r6inv;
-            const float cc = (t ? qc1 : qc0) * xj.w;
-            float pv = t12 - t6;
-            float pe = cc * (rinv - zcore + bco * r2s);
-            float wc = r2inv * (6.0f * t6 - 12.0f * t12) - cc * (rinv * r2inv - fco);
-            if (!act) { pv = 0.f; pe = 0.f; wc = 0.f; }
-            if (VIR) n_act += act ? 1 : 0;
-            const float wx = wc * dx, wy = wc * dy, wz = wc * dz;
-            av += pv;
-            ae += pe;
-            wjx -= wx;
-            wjy -= wy;
-            wjz -= wz;
-            if (t) { a1x += wx; a1y += wy; a1z += wz; }
-            else { a0x += wx; a0y += wy; a0z += wz; }
-        }
-        if (++n_acc == OG_FLUSH) {
-            f0x += a0x; f0y += a0y; f0z += a0z;
-            f1x += a1x; f1y += a1y; f1z += a1z;
-            e_vdw += av;
-            e_ele += ae;
-            a0x = a0y = a0z = a1x = a1y = a1z = av = ae = 0.f;
-            n_acc = 0;
-        }
-        // work on j: sum over the four i-groups (lanes jj, jj+8, jj+16, jj+24)
-        wjx += __shfl_xor_sync(0xffffffffu, wjx, 8);
-        wjy += __shfl_xor_sync(0xffffffffu, wjy, 8);
-        wjz += __shfl_xor_sync(0xffffffffu, wjz, 8);
-        wjx += __shfl_xor_sync(0xffffffffu, wjx, 16);
-        wjy += __shfl_xor_sync(0xffffffffu, wjy, 16);
-        wjz += __shfl_xor_sync(0xffffffffu, wjz, 16);
-        if (g == 0 && (wjx != 0.f || wjy != 0.f || wjz != 0.f)) {
-            unsigned long long *fj = frc + 3 * (size_t)(c2 * OG_CELL + jj);
-            atomicAdd(fj + 0, (unsigned long long)__float2ll_rn(wjx * (float)OG_FIX_SCALE));
-            atomicAdd(fj + 1, (unsigned long long)__float2ll_rn(wjy * (float)OG_FIX_SCALE));
-            atomicAdd(fj + 2, (unsigned long long)__float2ll_rn(wjz * (float)OG_FIX_SCALE));
-            if (VIR) {
-                const int img = cp_c2img[k].y;
-                if (img != 0) {
+            for (int t = 0; t < 2; t++) {
+                const float4 xi = t ? xi1 : xi0;
+                const float dx = xi.x - rjx, dy = xi.y - rjy, dz = xi.z - rjz;
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                const int bit = jj * OG_CELL + g + 4 * t;
+                const bool act = (((m >> bit) & 1ull) == 0ull) && (r2 < rc2);
+                const float r2s = act ? r2 : 1.0f;
+                // hardware estimate + one Newton step on the exact residual 1 - r2 y^2 (FMA):
+                // the estimate alone carries a one-sided error that adds up over millions of
+                // Coulomb pairs in the energy
+                float rinv = rsqrtf(r2s);
+                const float hres = fmaf(-r2s * rinv, rinv, 1.0f);
+                rinv = fmaf(0.5f * rinv, hres, rinv);
+                const float r2inv = rinv * rinv;
+                const float r6inv = r2inv * r2inv * r2inv;
+                const float2 p = __ldg(&lj[(t ? ti1 : ti0) + cur_tj]);
+                const float t6 = p.x * r6inv, t12 = p.y * r6inv * r6inv;
+                const float cc = (t ? qc1 : qc0) * cur_xj.w;
+                float pv = t12 - t6;
+                float pe = cc * (rinv - zcore + bco * r2s);
+                float wc = r2inv * (6.0f * t6 - 12.0f * t12) - cc * (rinv * r2inv - fco);
+                if (!act) { pv = 0.f; pe = 0.f; wc = 0.f; }
+                if (VIR) n_act += act ? 1 : 0;
+                const float wx = wc * dx, wy = wc * dy, wz = wc * dz;
+                av += pv;
+                ae += pe;
+                wjx -= wx;
+                wjy -= wy;
+                wjz -= wz;
+                if (t) { a1x += wx; a1y += wy; a1z += wz; }
+                else { a0x += wx; a0y += wy; a0z += wz; }
+            }
+            if (++n_acc == OG_FLUSH) flush();
+            // work on j: sum over the four i-groups (lanes jj, jj+8, jj+16, jj+24)
+            wjx += __shfl_xor_sync(0xffffffffu, wjx, 8);
+            wjy += __shfl_xor_sync(0xffffffffu, wjy, 8);
+            wjz += __shfl_xor_sync(0xffffffffu, wjz, 8);
+            wjx += __shfl_xor_sync(0xffffffffu, wjx, 16);
+            wjy += __shfl_xor_sync(0xffffffffu, wjy, 16);
+            wjz += __shfl_xor_sync(0xffffffffu, wjz, 16);
+            if (g == 0 && (wjx != 0.f || wjy != 0.f || wjz != 0.f)) {
+                unsigned long long *fj = frc + 3 * (size_t)(cur_c2 * OG_CELL + jj);
+                atomicAdd(fj + 0, (unsigned long long)__float2ll_rn(wjx * (float)OG_FIX_SCALE));
+                atomicAdd(fj + 1, (unsigned long long)__float2ll_rn(wjy * (float)OG_FIX_SCALE));
+                atomicAdd(fj + 2, (unsigned long long)__float2ll_rn(wjz * (float)OG_FIX_SCALE));
+                if (VIR && img != 0) {
                     // sum over pairs of d (x) f = sum_atoms x (x) F + sum_cell-pairs shift (x) F_j
                     const double sh[3] = {(img & 1) ? -S.L[0] : ((img & 2) ? S.L[0] : 0.0),
                                           (img & 4) ? -S.L[1] : ((img & 8) ? S.L[1] : 0.0),
@@ -158,41 +222,22 @@ k_pair_ljzd(const int *__restrict__ counters, const int *__restrict__ cell_sys, 
                         for (int b = 0; b < 3; b++) v[a * 3 + b] += sh[a] * fjv[b];
                 }
             }
+            if (!more) break;
         }
     }
-    f0x += a0x; f0y += a0y; f0z += a0z;
-    f1x += a1x; f1y += a1y; f1z += a1z;
-    e_vdw += av;
-    e_ele += ae;
-    // work on i: sum over the 8 j lanes of each i-group
-#pragma unroll
-    for (int o = 1; o < 8; o <<= 1) {
-        f0x += __shfl_xor_sync(0xffffffffu, f0x, o);
-        f0y += __shfl_xor_sync(0xffffffffu, f0y, o);
-        f0z += __shfl_xor_sync(0xffffffffu, f0z, o);
-        f1x += __shfl_xor_sync(0xffffffffu, f1x, o);
-        f1y += __shfl_xor_sync(0xffffffffu, f1y, o);
-        f1z += __shfl_xor_sync(0xffffffffu, f1z, o);
-    }
-    if (jj == 0) {
-        unsigned long long *fa = frc + 3 * (size_t)(c1 * OG_CELL + g);
-        unsigned long long *fb = frc + 3 * (size_t)(c1 * OG_CELL + g + 4);
-        if (f0x != 0.0 || f0y != 0.0 || f0z != 0.0) {
-            atomicAdd(fa + 0, (unsigned long long)og_to_fix(f0x));
-            atomicAdd(fa + 1, (unsigned long long)og_to_fix(f0y));
-            atomicAdd(fa + 2, (unsigned long long)og_to_fix(f0z));
-        }
-        if (f1x != 0.0 || f1y != 0.0 || f1z != 0.0) {
-            atomicAdd(fb + 0, (unsigned long long)og_to_fix(f1x));
-            atomicAdd(fb + 1, (unsigned long long)og_to_fix(f1y));
-            atomicAdd(fb + 2, (unsigned long long)og_to_fix(f1z));
+    flush();
+    __syncwarp();
+    // work on i: one fixed-point add per component of each of the 8 atoms
+    if (lane < OG_CELL) {
+        const double wx = acc_w[3 * lane], wy = acc_w[3 * lane + 1], wz = acc_w[3 * lane + 2];
+        if (wx != 0.0 || wy != 0.0 || wz != 0.0) {
+            unsigned long long *fa = frc + 3 * (size_t)(c1 * OG_CELL + lane);
+            atomicAdd(fa + 0, (unsigned long long)og_to_fix(wx));
+            atomicAdd(fa + 1, (unsigned long long)og_to_fix(wy));
+            atomicAdd(fa + 2, (unsigned long long)og_to_fix(wz));
         }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        e_vdw += __shfl_xor_sync(0xffffffffu, e_vdw, o);
-        e_ele += __shfl_xor_sync(0xffffffffu, e_ele, o);
-    }
+    const double e_vdw = acc_w[OG_CELL * 3], e_ele = acc_w[OG_CELL * 3 + 1];
     if (VIR) {
         for (int q = 0; q < 9; q++)
             for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
@@ -209,13 +254,29 @@ k_pair_ljzd(const int *__restrict__ counters, const int *__restrict__ cell_sys, 
     }
 }
 
-template __global__ void k_pair_ljzd<true>(const int *, const int *, const SysDev *, const float4 *, const float4 *,
-                                           const int *, const int *, const float4 *, const int2 *,
-                                           const unsigned long long *, const float2 *, unsigned long long *,
-                                           double *, long long);
-template __global__ void k_pair_ljzd<false>(const int *, const int *, const SysDev *, const float4 *, const float4 *,
-                                            const int *, const int *, const float4 *, const int2 *,
-                                            const unsigned long long *, const float2 *, unsigned long long *,
-                                            double *, long long);
+template __global__ void k_pair_ljzd<true, 2>(const int *, const int *, const SysDev *, const float4 *,
+                                                const float4 *, const int *, const int *, const float4 *,
+                                                const int2 *, const unsigned long long *, const float2 *,
+                                                unsigned long long *, double *, long long);
+template __global__ void k_pair_ljzd<true, 3>(const int *, const int *, const SysDev *, const float4 *,
+                                                const float4 *, const int *, const int *, const float4 *,
+                                                const int2 *, const unsigned long long *, const float2 *,
+                                                unsigned long long *, double *, long long);
+template __global__ void k_pair_ljzd<true, 4>(const int *, const int *, const SysDev *, const float4 *,
+                                                const float4 *, const int *, const int *, const float4 *,
+                                                const int2 *, const unsigned long long *, const float2 *,
+                                                unsigned long long *, double *, long long);
+template __global__ void k_pair_ljzd<false, 2>(const int *, const int *, const SysDev *, const float4 *,
+                                                const float4 *, const int *, const int *, const float4 *,
+                                                const int2 *, const unsigned long long *, const float2 *,
+                                                unsigned long long *, double *, long long);
+template __global__ void k_pair_ljzd<false, 3>(const int *, const int *, const SysDev *, const float4 *,
+                                                const float4 *, const int *, const int *, const float4 *,
+                                                const int2 *, const unsigned long long *, const float2 *,
+                                                unsigned long long *, double *, long long);
+template __global__ void k_pair_ljzd<false, 4>(const int *, const int *, const SysDev *, const float4 *,
+                                                const float4 *, const int *, const int *, const float4 *,
+                                                const int2 *, const unsigned long long *, const float2 *,
+                                                unsigned long long *, double *, long long);
 
 }  // namespace og

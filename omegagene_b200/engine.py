@@ -83,6 +83,7 @@ def load_library():
         "og_get_state_async": [E, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p],
         "og_step_async": [E, C.c_int32], "og_synchronize": [E],
         "og_get_pair_count": [E, C.c_int32, _p(C.c_int64)],
+        "og_get_tuning": [E, _p(C.c_int32), C.c_void_p],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -377,3 +378,9 @@ class Engine:
         n = C.c_int64()
         self._check(self.L.og_get_pair_count(self.h, sys, C.byref(n)), "og_get_pair_count")
         return n.value
+
+    def tuning(self):
+        v = C.c_int32()
+        ms = np.zeros(3)
+        self._check(self.L.og_get_tuning(self.h, C.byref(v), ms.ctypes.data), "og_get_tuning")
+        return {"pair_variant": v.value, "variant_ms": ms.tolist()}
