@@ -179,6 +179,14 @@ og_status og_get_flags(og_engine *e, int32_t *flags);
 /* Autotuner result: the pair-kernel variant in use (register budget 100/80/64 per thread) and
  * the best time of each variant on the first list, in ms. */
 og_status og_get_tuning(og_engine *e, int32_t *pair_variant, double *variant_ms);
+/* Fixed-order FP64 sums of d_values[i*stride] over the segments [d_seg_base[s], d_seg_base[s+1])
+ * of a device array, s < n_seg, into d_out[s] (device).  max_seg_len bounds every segment's
+ * length.  The engine's own energy / kinetic-energy reduction (two levels: 4096-item chunks,
+ * then chunks in order), so a segment's sum does not depend on the other segments.
+ * Stream-ordered on cuda_stream (a cudaStream_t, NULL = default); its scratch is a
+ * stream-ordered allocation released before return. */
+og_status og_segment_sum(const double *d_values, int32_t stride, const int32_t *d_seg_base, int32_t n_seg,
+                         int32_t max_seg_len, double *d_out, void *cuda_stream);
 /* Number of systems and atoms held. */
 og_status og_get_sizes(og_engine *e, int32_t *n_systems, int64_t *n_atoms_total);
 

@@ -1528,3 +1528,23 @@ extern "C" og_status og_get_tuning(og_engine *e, int32_t *pair_variant, double *
         for (int v = 0; v < 3; v++) variant_ms[v] = e->variant_ms[v];
     return OG_OK;
 }
+
+// Fixed-order FP64 sum of value[i*stride] over each segment [seg_base[s], seg_base[s+1]) of a
+// device array: the engine's two-level reduction (k_part / k_part_final), exposed for callers
+// that keep per-item quantities on the device.  The partial sums live in a stream-ordered
+// allocation released before return; the result does not depend on how segments are batched.
+extern "C" og_status og_segment_sum(const double *d_values, int32_t stride, const int32_t *d_seg_base, int32_t n_seg,
+                                    int32_t max_seg_len, double *d_out, void *cuda_stream) {
+    if (!d_values || !d_seg_base || !d_out || n_seg <= 0 || stride <= 0 || max_seg_len < 0) return OG_ERR_INVALID;
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    const int max_chunks = std::max(1, (max_seg_len + 4095) / 4096);
+    double *part = nullptr;
+    if (cudaMallocAsync((void **)&part, sizeof(double) * (size_t)n_seg * max_chunks, st) != cudaSuccess)
+        return OG_ERR_NOMEM;
+    dim3 grid(max_chunks, n_seg);
+    k_part<1><<<grid, 256, 0, st>>>(d_values, stride, 0, d_seg_base, max_chunks, part);
+    k_part_final<1><<<n_seg, 256, 0, st>>>(part, max_chunks, d_out, 1, 0, nullptr, 0);
+    cudaError_t r = cudaGetLastError();
+    cudaFreeAsync(part, st);
+    return r == cudaSuccess ? OG_OK : OG_ERR_CUDA;
+}
