@@ -187,6 +187,15 @@ og_status og_get_tuning(og_engine *e, int32_t *pair_variant, double *variant_ms)
  * stream-ordered allocation released before return. */
 og_status og_segment_sum(const double *d_values, int32_t stride, const int32_t *d_seg_base, int32_t n_seg,
                          int32_t max_seg_len, double *d_out, void *cuda_stream);
+/* og_segment_sum without any device allocation, for callers that cannot allocate at call time
+ * (all free device memory already handed to another allocator's pool, or an allocation call not
+ * acceptable on their path).  No counterpart in the reference.  Scratch is a fixed 512 KiB
+ * array in device memory (n_seg * ceil(max_seg_len / 4096) <= 65536, else OG_ERR_CAPACITY),
+ * held by every GPU that loads the library until the process exits.  The first call on a device
+ * (with that device current) looks up the array's device address; make that first call before
+ * any stream capture.  All calls share the array: calls that overlap on the GPU race. */
+og_status og_segment_sum_noalloc(const double *d_values, int32_t stride, const int32_t *d_seg_base, int32_t n_seg,
+                                 int32_t max_seg_len, double *d_out, void *cuda_stream);
 /* Number of systems and atoms held. */
 og_status og_get_sizes(og_engine *e, int32_t *n_systems, int64_t *n_atoms_total);
 

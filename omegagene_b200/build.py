@@ -7,7 +7,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libomegagene_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
-SOURCES = ["og_grid.cu", "og_pair.cu", "og_integrate.cu", "og_engine.cu"]
+SOURCES = ["og_grid.cu", "og_pair.cu", "og_integrate.cu", "og_engine.cu", "og_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
