@@ -104,6 +104,11 @@ typedef struct {
     int32_t mcmd_order;
     double mcmd_lambda_low, mcmd_lambda_high, mcmd_temperature;
     const double *mcmd_coef;     /* [order+1] */
+    /* Step number of this system's first og_step (0 for a new run).  A run handed over between
+     * engines (a serving loop re-forming its batch) passes the steps already done, a multiple of
+     * nsgrid_update_intvl, so the heating schedule and the list-rebuild phase continue unchanged.
+     * No counterpart in the reference, whose run always starts at step 0. */
+    int64_t first_step;
 } og_system_desc;
 
 /* Creates an engine on a CUDA device (cuda_set_device, cuda_setup.cu:1085-1093). */
@@ -179,6 +184,10 @@ og_status og_get_flags(og_engine *e, int32_t *flags);
 /* Autotuner result: the pair-kernel variant in use (register budget 100/80/64 per thread) and
  * the best time of each variant on the first list, in ms. */
 og_status og_get_tuning(og_engine *e, int32_t *pair_variant, double *variant_ms);
+/* Fixes the pair-kernel variant (0/1/2) before og_finalize and skips the autotuner, e.g. when a
+ * serving loop re-creates engines for new batches; -1 restores autotuning.  No counterpart in
+ * the reference, which has one pair kernel. */
+og_status og_set_tuning(og_engine *e, int32_t pair_variant);
 /* Fixed-order FP64 sums of d_values[i*stride] over the segments [d_seg_base[s], d_seg_base[s+1])
  * of a device array, s < n_seg, into d_out[s] (device).  max_seg_len bounds every segment's
  * length.  The engine's own energy / kinetic-energy reduction (two levels: 4096-item chunks,

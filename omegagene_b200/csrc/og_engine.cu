@@ -208,6 +208,7 @@ struct og_engine {
     double *d_stage = nullptr;            // og_put_state staging (6 doubles per atom)
     double pair_ms = 0.0, step_ms = 0.0;
     int pair_variant = 0;
+    int fixed_variant = -1;  // og_set_tuning: variant chosen by the caller, -1 = autotune
     double variant_ms[3] = {0, 0, 0};
     bool timing = false;
     std::vector<void *> allocs;
@@ -761,6 +762,10 @@ og_status build_list_checked(og_engine *e) {
 // the fastest; OG_PAIR_VARIANT=0/1/2 in the environment fixes the choice.  The trial launches
 // write the force accumulators, which are cleared afterwards.
 og_status autotune_pair(og_engine *e) {
+    if (e->fixed_variant >= 0) {
+        e->pair_variant = e->fixed_variant;
+        return OG_OK;
+    }
     const char *env = getenv("OG_PAIR_VARIANT");
     if (env && *env) {
         e->pair_variant = atoi(env) % 3;
@@ -851,6 +856,8 @@ og_status og_add_system(og_engine *e, const og_system_desc *d, int32_t *sys_id) 
     if (!e->sys.empty() && d->nsgrid_update_intvl != e->intvl)
         return fail(e, OG_ERR_INVALID, "all systems of one engine share nsgrid_update_intvl");
     if (d->mcmd_order > 7) return fail(e, OG_ERR_INVALID, "McMD polynomial order above 7");
+    if (d->first_step < 0 || d->first_step % d->nsgrid_update_intvl != 0)
+        return fail(e, OG_ERR_INVALID, "first_step must be a non-negative multiple of nsgrid_update_intvl");
     e->sys.emplace_back();
     HostSystem &h = e->sys.back();
     h.d = *d;
@@ -975,7 +982,7 @@ og_status og_finalize(og_engine *e) {
         thermo.push_back(d.temperature);
         thermo.push_back(d.temperature_init < 0 ? d.temperature : d.temperature_init);
         thermo.push_back((double)d.heating_steps);
-        thermo.push_back(0.0);
+        thermo.push_back((double)d.first_step);
         mask_plain[k] = D.has_constraints && d.thermostat != OG_THERMOSTAT_SCALING;
         mask_thermo[k] = D.has_constraints && d.thermostat == OG_THERMOSTAT_SCALING;
         e->any_plain_cons |= mask_plain[k] != 0;
@@ -1547,4 +1554,12 @@ extern "C" og_status og_segment_sum(const double *d_values, int32_t stride, cons
     cudaError_t r = cudaGetLastError();
     cudaFreeAsync(part, st);
     return r == cudaSuccess ? OG_OK : OG_ERR_CUDA;
+}
+
+extern "C" og_status og_set_tuning(og_engine *e, int32_t pair_variant) {
+    if (!e) return OG_ERR_INVALID;
+    if (e->finalized) return fail(e, OG_ERR_STATE, "og_set_tuning after og_finalize");
+    if (pair_variant < -1 || pair_variant > 2) return fail(e, OG_ERR_INVALID, "pair variant must be -1, 0, 1 or 2");
+    e->fixed_variant = pair_variant;
+    return OG_OK;
 }

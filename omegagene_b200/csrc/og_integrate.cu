@@ -300,8 +300,11 @@ __global__ void k_thermo_scaling_ke(int n_atoms, const int *__restrict__ atom_sy
 }
 
 // SubBox::update_thermostat target (SubBox.cpp:1745-1757).
-__device__ __forceinline__ double target_temperature(const double *thermo, int s, long long step) {
+// thermo[4s..4s+3] = temperature, initial temperature, heating steps, the system's first step
+// (the heating ramp of SubBox.cpp:1746-1751, with the step counted from the run's start).
+__device__ __forceinline__ double target_temperature(const double *thermo, int s, long long engine_step) {
     const double t0 = thermo[4 * s], tinit = thermo[4 * s + 1], heat = thermo[4 * s + 2];
+    const long long step = engine_step + (long long)thermo[4 * s + 3];
     if ((double)step < heat) return tinit + ((t0 - tinit) / heat) * (double)step;
     return t0;
 }

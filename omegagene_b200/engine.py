@@ -51,6 +51,7 @@ class SystemDesc(C.Structure):
         ("thermo_const_max_loops", C.c_int32), ("thermo_const_tolerance", C.c_double),
         ("mcmd_order", C.c_int32), ("mcmd_lambda_low", C.c_double), ("mcmd_lambda_high", C.c_double),
         ("mcmd_temperature", C.c_double), ("mcmd_coef", _p(C.c_double)),
+        ("first_step", C.c_int64),
     ]
 
 
@@ -83,7 +84,7 @@ def load_library():
         "og_get_state_async": [E, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p],
         "og_step_async": [E, C.c_int32], "og_synchronize": [E],
         "og_get_pair_count": [E, C.c_int32, _p(C.c_int64)],
-        "og_get_tuning": [E, _p(C.c_int32), C.c_void_p],
+        "og_get_tuning": [E, _p(C.c_int32), C.c_void_p], "og_set_tuning": [E, C.c_int32],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -177,7 +178,7 @@ class _Keep:
     """Holds the numpy arrays a SystemDesc points into."""
 
 
-def make_desc(system, params=None, mcmd=None):
+def make_desc(system, params=None, mcmd=None, first_step=0):
     """Builds an og_system_desc from a launch-set dict (cls_io.read_cls or systems.*)."""
     prm = dict(DEFAULT_PARAMS)
     prm.update(params or {})
@@ -237,6 +238,7 @@ def make_desc(system, params=None, mcmd=None):
     d.heating_steps, d.berendsen_tau = prm["heating_steps"], prm["berendsen_tau"]
     d.const_max_loops, d.const_tolerance = prm["const_max_loops"], prm["const_tolerance"]
     d.thermo_const_max_loops, d.thermo_const_tolerance = prm["thermo_const_max_loops"], prm["thermo_const_tolerance"]
+    d.first_step = int(first_step)
     d.mcmd_order = -1
     if mcmd is not None:
         keep.mcoef = np.ascontiguousarray(mcmd["coef"], np.float64)
@@ -273,8 +275,8 @@ class Engine:
         except Exception:
             pass
 
-    def add_system(self, system, params=None, mcmd=None):
-        d, keep = make_desc(system, params, mcmd)
+    def add_system(self, system, params=None, mcmd=None, first_step=0):
+        d, keep = make_desc(system, params, mcmd, first_step)
         sid = C.c_int32()
         self._check(self.L.og_add_system(self.h, C.byref(d), C.byref(sid)), "og_add_system")
         self._keep.append(keep)
@@ -384,3 +386,7 @@ class Engine:
         ms = np.zeros(3)
         self._check(self.L.og_get_tuning(self.h, C.byref(v), ms.ctypes.data), "og_get_tuning")
         return {"pair_variant": v.value, "variant_ms": ms.tolist()}
+
+    def set_tuning(self, variant):
+        """Fixes the pair-kernel variant (0/1/2) before finalize(); -1 = autotune."""
+        self._check(self.L.og_set_tuning(self.h, int(variant)), "og_set_tuning")

@@ -1,0 +1,185 @@
+"""Continuous-batching MD job server on one GPU.
+
+Jobs (a system, run parameters and a step count) arrive over time. The server keeps every running
+job in one engine, so all their atoms advance in the same kernel launches. At each window
+boundary (a multiple of the pair-list interval) it does the following:
+* retires finished jobs;
+* admits queued jobs, first come first served, while the device-memory budget and the job cap allow;
+* re-creates the engine for the new batch. Each continuing job carries over its positions,
+  velocities and its own step number, so its list-rebuild phase and heating schedule continue
+  unchanged.
+
+A job's trajectory is therefore the one it would have had alone. The engine's forces are
+fixed-point sums and its reductions are per system, so the match is exact;
+tests/test_gpu_serve.py checks it.
+
+Latency of a job = completion time - arrival time (wall clock). Throughput = atom-steps of all
+jobs / (last completion - first arrival).
+"""
+import collections
+import time
+
+import numpy as np
+
+from . import engine
+
+BYTES_PER_ATOM = 1400  # device footprint per atom: state, grid, cell pairs, list scratch
+
+
+class Job:
+    def __init__(self, job_id, system, params, n_steps, arrival_s=0.0, mcmd=None):
+        self.id = job_id
+        self.system = system
+        self.params = dict(params)
+        self.n_steps = int(n_steps)
+        self.arrival_s = float(arrival_s)
+        self.mcmd = mcmd
+        self.n_atoms = int(system["n_atoms"])
+        self.crd = np.asarray(system["crd"], np.float64).copy()
+        self.vel = np.asarray(system["vel"], np.float64).copy()
+        self.steps_done = 0
+        self.t_admit = None
+        self.t_done = None
+        self.energies = None
+        intvl = self.params.get("nsgrid_update_intvl", 1)
+        if self.n_steps % intvl:
+            raise ValueError("job %s: n_steps must be a multiple of nsgrid_update_intvl" % job_id)
+
+    @property
+    def bytes(self):
+        return self.n_atoms * BYTES_PER_ATOM
+
+    @property
+    def latency_s(self):
+        return None if self.t_done is None else self.t_done - self.arrival_s
+
+
+class Server:
+    def __init__(self, device=0, hbm_budget_bytes=None, max_jobs=64, window=100, pair_variant=1,
+                 clock=time.perf_counter, sleep=time.sleep, engine_factory=None):
+        self.device = device
+        if hbm_budget_bytes is None:
+            import torch
+            free, _ = torch.cuda.mem_get_info(device)
+            hbm_budget_bytes = int(0.5 * free)
+        self.budget = hbm_budget_bytes
+        self.max_jobs = max_jobs
+        self.window = window
+        self.pair_variant = pair_variant
+        self.clock = clock
+        self.sleep = sleep
+        self.n_relayouts = 0
+        self.relayout_s = 0.0
+        self.batch_sizes = []
+        self.engine_factory = engine_factory or engine.Engine
+
+    def _build(self, active):
+        eng = self.engine_factory(self.device)
+        if self.pair_variant is not None:
+            eng.set_tuning(self.pair_variant)
+        for j in active:
+            s = dict(j.system)
+            s["crd"], s["vel"] = j.crd, j.vel
+            eng.add_system(s, j.params, j.mcmd, first_step=j.steps_done)
+        eng.finalize()
+        self.n_relayouts += 1
+        return eng
+
+    def run(self, jobs):
+        """Runs every job to completion; returns a summary dict (throughput, latencies)."""
+        intvls = {j.params.get("nsgrid_update_intvl", 1) for j in jobs}
+        if len(intvls) != 1:
+            raise ValueError("all jobs of one server share nsgrid_update_intvl")
+        intvl = intvls.pop()
+        if self.window % intvl:
+            raise ValueError("window must be a multiple of nsgrid_update_intvl")
+        future = collections.deque(sorted(jobs, key=lambda j: j.arrival_s))
+        queue = collections.deque()
+        active, done = [], []
+        eng = None
+        t0 = self.clock()
+        first_arrival = future[0].arrival_s if future else 0.0
+        while future or queue or active:
+            now = self.clock() - t0
+            while future and future[0].arrival_s <= now:
+                queue.append(future.popleft())
+            finished = [j for j in active if j.steps_done >= j.n_steps]
+            used = sum(j.bytes for j in active if j.steps_done < j.n_steps)
+            n_run = len(active) - len(finished)
+            admit = []
+            while queue and n_run + len(admit) < self.max_jobs and used + queue[0].bytes <= self.budget:
+                admit.append(queue.popleft())
+                used += admit[-1].bytes
+            if finished or admit:
+                t_re = self.clock()
+                if eng is not None:
+                    for i, j in enumerate(active):
+                        j.crd, j.vel = eng.get_state(i)
+                        j.energies = eng.get_energies(i)
+                    eng.close()
+                    eng = None
+                now = self.clock() - t0
+                for j in finished:
+                    j.t_done = now
+                    done.append(j)
+                active = [j for j in active if j.steps_done < j.n_steps] + admit
+                for j in admit:
+                    j.t_admit = now
+                if active:
+                    eng = self._build(active)
+                    self.batch_sizes.append(len(active))
+                self.relayout_s += self.clock() - t_re
+            if not active:
+                if future:
+                    wait = future[0].arrival_s - (self.clock() - t0)
+                    if wait > 0:
+                        self.sleep(wait)
+                continue
+            w = min(self.window, min(j.n_steps - j.steps_done for j in active))
+            eng.step(w)
+            for j in active:
+                j.steps_done += w
+        t_end = max(j.t_done for j in done) if done else 0.0
+        lat = np.array([j.latency_s for j in done])
+        atom_steps = sum(j.n_atoms * j.n_steps for j in done)
+        span = t_end - first_arrival
+        return {"n_jobs": len(done), "atom_steps": atom_steps, "span_s": span,
+                "atom_steps_per_s": atom_steps / span if span > 0 else 0.0,
+                "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+                "relayouts": self.n_relayouts, "relayout_s": self.relayout_s,
+                "mean_batch": float(np.mean(self.batch_sizes)) if self.batch_sizes else 0.0,
+                "jobs": done}
+
+
+def run_alone(job, device=0, pair_variant=1, warmup=0):
+    """The plain path: one job, one engine, start to finish; returns (seconds, final energies,
+    final positions, final velocities).  `warmup` extra steps run first, untimed (a timing aid:
+    the returned state is then `warmup` steps further on)."""
+    eng = engine.Engine(device)
+    if pair_variant is not None:
+        eng.set_tuning(pair_variant)
+    s = dict(job.system)
+    eng.add_system(s, job.params, job.mcmd)
+    eng.finalize()
+    if warmup:
+        eng.step(warmup)
+    t = time.perf_counter()
+    eng.step(job.n_steps)
+    dt = time.perf_counter() - t
+    crd, vel = eng.get_state(0)
+    ene = eng.get_energies(0)
+    eng.close()
+    return dt, ene, crd, vel
+
+
+def fifo_latencies(arrivals, service_s):
+    """Latencies of a one-at-a-time server (first come first served) for the given arrival
+    times and per-job service times; also returns the span from the first arrival to the last
+    completion."""
+    t = 0.0
+    out = []
+    for a, s in sorted(zip(arrivals, service_s)):
+        start = max(t, a)
+        t = start + s
+        out.append(t - a)
+    return np.array(out), t - min(arrivals)

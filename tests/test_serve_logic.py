@@ -1,0 +1,116 @@
+"""Host logic of the continuous-batching server, on the CPU with a fake engine and clock:
+admission order, job and memory caps, window boundaries, state hand-over and latencies."""
+import numpy as np
+import pytest
+
+from omegagene_b200 import serve
+
+
+class FakeClock:
+    def __init__(self):
+        self.t = 0.0
+
+    def __call__(self):
+        return self.t
+
+    def sleep(self, dt):
+        self.t += dt
+
+
+class FakeEngine:
+    """Advances every system's coordinates by +1 per step; one step costs 1 ms per 1000 atoms
+    of the batch on the fake clock."""
+    log = []
+
+    def __init__(self, clock):
+        self.clock = clock
+        self.systems = []
+
+    def set_tuning(self, v):
+        pass
+
+    def add_system(self, s, params, mcmd=None, first_step=0):
+        self.systems.append({"crd": np.array(s["crd"], float), "vel": np.array(s["vel"], float),
+                             "first_step": first_step, "n": s["n_atoms"]})
+
+    def finalize(self):
+        FakeEngine.log.append([(s["n"], s["first_step"]) for s in self.systems])
+
+    def step(self, n):
+        for s in self.systems:
+            s["crd"] += n
+        self.clock.t += n * 1e-3 * sum(s["n"] for s in self.systems) / 1000.0
+
+    def get_state(self, i):
+        return self.systems[i]["crd"].copy(), self.systems[i]["vel"].copy()
+
+    def get_energies(self, i):
+        return {"step": float(self.systems[i]["crd"][0, 0])}
+
+    def close(self):
+        pass
+
+
+def _system(n):
+    return {"n_atoms": n, "crd": np.zeros((n, 3)), "vel": np.zeros((n, 3))}
+
+
+def _server(clock, **kw):
+    FakeEngine.log = []
+    return serve.Server(0, hbm_budget_bytes=kw.pop("budget", 10 ** 12), clock=clock, sleep=clock.sleep,
+                        engine_factory=lambda dev: FakeEngine(clock), **kw)
+
+
+def test_every_job_runs_exactly_its_steps():
+    clock = FakeClock()
+    p = {"nsgrid_update_intvl": 10}
+    jobs = [serve.Job(k, _system(100 * (k + 1)), p, 10 * (k + 1), arrival_s=0.001 * k) for k in range(6)]
+    res = _server(clock, max_jobs=3, window=20).run(jobs)
+    assert res["n_jobs"] == 6
+    for j in jobs:
+        assert np.all(j.crd == j.n_steps)  # the fake engine adds 1 per step: no step lost or repeated
+        assert j.steps_done == j.n_steps
+        assert j.latency_s > 0
+
+
+def test_first_step_carried_over_at_relayout():
+    clock = FakeClock()
+    p = {"nsgrid_update_intvl": 10}
+    jobs = [serve.Job(0, _system(100), p, 60), serve.Job(1, _system(100), p, 20),
+            serve.Job(2, _system(100), p, 20, arrival_s=0.0)]
+    _server(clock, max_jobs=2, window=20).run(jobs)
+    # job 0 starts at step 0, then continues at 20 beside job 2 after job 1 leaves
+    assert FakeEngine.log[0] == [(100, 0), (100, 0)]
+    assert FakeEngine.log[1] == [(100, 20), (100, 0)]
+    assert all(fs % 10 == 0 for batch in FakeEngine.log for _, fs in batch)
+
+
+def test_memory_budget_and_job_cap():
+    clock = FakeClock()
+    p = {"nsgrid_update_intvl": 10}
+    jobs = [serve.Job(k, _system(1000), p, 20) for k in range(5)]
+    srv = _server(clock, max_jobs=4, window=20, budget=2 * 1000 * serve.BYTES_PER_ATOM)
+    res = srv.run(jobs)
+    assert res["n_jobs"] == 5 and max(srv.batch_sizes) == 2
+
+
+def test_idle_server_waits_for_arrivals():
+    clock = FakeClock()
+    p = {"nsgrid_update_intvl": 10}
+    jobs = [serve.Job(0, _system(100), p, 10, arrival_s=5.0)]
+    res = _server(clock, max_jobs=4, window=10).run(jobs)
+    assert jobs[0].t_admit >= 5.0 and res["n_jobs"] == 1
+
+
+def test_bad_window_and_steps_rejected():
+    clock = FakeClock()
+    with pytest.raises(ValueError):
+        serve.Job(0, _system(10), {"nsgrid_update_intvl": 10}, 15)
+    jobs = [serve.Job(0, _system(10), {"nsgrid_update_intvl": 10}, 20)]
+    with pytest.raises(ValueError):
+        _server(clock, window=15).run(jobs)
+
+
+def test_fifo_latencies():
+    lat, span = serve.fifo_latencies([0.0, 1.0, 1.5], [2.0, 1.0, 1.0])
+    assert np.allclose(lat, [2.0, 2.0, 2.5]) and span == pytest.approx(4.0)
