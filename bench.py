@@ -295,6 +295,128 @@ def run_ours(args, world, rank, local, pg):
     return out
 
 
+# ------------------------------------------------------------------ serving workload
+
+def run_serve(args):
+    """Batched serving stream: jobs of 500-10,000 TIP3P waters (log-uniform, box at 0.997 g/cm^3),
+    300 K velocity rescaling, SHAKE, dt 2 fs.  Two runs of the continuous-batching server over
+    the same jobs: all jobs queued at t=0 (aggregate capacity, the `value`), then Poisson arrivals
+    at 80% of that capacity (p50/p99 latency).  The plain path (one job at a time, one engine
+    each) is timed on a sample of jobs across the size range, fitted as a + b*atoms, and queued
+    first come first served on the same arrivals."""
+    import torch
+    from omegagene_b200 import engine, serve, systems
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(3)
+    n_jobs, steps = args.jobs, args.job_steps
+    counts = np.exp(rng.uniform(np.log(500), np.log(10000), n_jobs)).astype(int)
+    p = dict(engine.DEFAULT_PARAMS)
+    p.update(nsgrid_update_intvl=INTVL, time_step=DT_FS, thermostat="scaling", temperature=300.0)
+    built = [systems.water_system(int(c), seed=1000 + k) for k, c in enumerate(counts)]
+
+    def jobs_at(arrivals):
+        return [serve.Job(k, built[k], p, steps, arrival_s=float(arrivals[k])) for k in range(n_jobs)]
+
+    total = float(sum(3 * counts) * steps)
+    sat = serve.Server(0, max_jobs=args.max_jobs, window=args.window).run(jobs_at(np.zeros(n_jobs)))
+    cap = sat["atom_steps_per_s"]
+    inter = total / n_jobs / (0.8 * cap)
+    arrivals = np.cumsum(rng.exponential(inter, n_jobs))
+    arrivals -= arrivals[0]
+    stream = serve.Server(0, max_jobs=args.max_jobs, window=args.window).run(jobs_at(arrivals))
+    # plain path: one engine per job; a sample across the size range, service time a + b*atoms
+    order = np.argsort(counts)
+    sample = order[np.linspace(0, n_jobs - 1, min(args.plain_sample, n_jobs)).astype(int)]
+    ts, na = [], []
+    for k in sample:
+        dt, _, _, _ = serve.run_alone(serve.Job(int(k), built[int(k)], p, steps))
+        ts.append(dt)
+        na.append(3 * int(counts[k]))
+    b, a = np.polyfit(na, ts, 1)
+    service = a + b * 3 * counts
+    plain_cap = total / float(service.sum())
+    lat_plain, _ = serve.fifo_latencies(arrivals, service)
+    return {
+        "metric": "batch atom-steps/s", "value": cap, "unit": "atom-steps/s", "n_gpus": 1,
+        "steps": steps, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": "%d TIP3P water jobs, 500-10000 waters log-uniform (seed 3), %d steps each, dt 2 fs, "
+                               "SHAKE, 300 K rescaling" % (n_jobs, steps),
+                   "max_jobs": args.max_jobs, "window_steps": args.window,
+                   "timing": "wall clock from the first arrival to the last completion, engine creation, "
+                             "graph capture and state hand-over included"},
+        "saturated": {"span_s": sat["span_s"], "relayouts": sat["relayouts"], "relayout_s": sat["relayout_s"],
+                      "mean_batch": sat["mean_batch"], "p50_latency_s": sat["latency_p50_s"],
+                      "p99_latency_s": sat["latency_p99_s"]},
+        "serving": {"arrivals": "Poisson, mean inter-arrival %.4f s (80%% of the saturated capacity)" % inter,
+                    "atom_steps_per_s": stream["atom_steps_per_s"], "p50_latency_s": stream["latency_p50_s"],
+                    "p99_latency_s": stream["latency_p99_s"], "span_s": stream["span_s"],
+                    "relayouts": stream["relayouts"], "relayout_s": stream["relayout_s"],
+                    "mean_batch": stream["mean_batch"]},
+        "plain": {"atom_steps_per_s": plain_cap, "p50_latency_s": float(np.percentile(lat_plain, 50)),
+                  "p99_latency_s": float(np.percentile(lat_plain, 99)),
+                  "service_fit_s": {"a": float(a), "b_per_atom": float(b)},
+                  "sample": "%d jobs run alone (one engine each, graph capture included)" % len(sample)},
+        "speedup_vs_plain": cap / plain_cap,
+    }
+
+
+# ------------------------------------------------------------------ McMD workload
+
+def run_mcmd(args):
+    """64 V-McMD walkers (a 300-atom synthetic chain in 2,500 TIP3P waters each, own seeds),
+    300 K velocity rescaling, dt 2 fs, in one engine; the order-6 polynomial of each walker
+    covers mean +- 4 sd of its potential energy over a 100-step unscaled prerun.  Compared with
+    the same walkers run one at a time."""
+    import torch
+    from omegagene_b200 import engine, serve, systems
+    torch.cuda.set_device(0)
+    walkers = [systems.chain_water_system(300, 2500, seed=args.walker_seed0 + w, radius=12.0)
+               for w in range(args.walkers)]
+    p = dict(engine.DEFAULT_PARAMS)
+    p.update(nsgrid_update_intvl=INTVL, time_step=DT_FS, thermostat="scaling", temperature=300.0)
+    pre = engine.Engine(0)
+    pre.set_tuning(1)
+    for w in walkers:
+        pre.add_system(w, p)
+    pre.finalize()
+    pre.set_trace(100)
+    pre.step(100)
+    tr = pre.get_trace(100)[:, :, engine.ENERGY_NAMES.index("potential")]
+    pre.close()
+    polys = [systems.mcmd_polynomial(tr[:, w].mean(), max(tr[:, w].std(), 1.0), seed=900 + w)
+             for w in range(len(walkers))]
+    eng = engine.Engine(0)
+    eng.set_tuning(1)
+    for w, m in zip(walkers, polys):
+        eng.add_system(w, p, m)
+    eng.finalize()
+    warm = -(-max(args.warmup, INTVL) // INTVL) * INTVL  # whole list intervals: the graph is captured here
+    eng.step(warm)
+    eng.set_timing("step")
+    torch.cuda.synchronize()
+    eng.step(args.steps)
+    st = eng.stats()
+    graphs = eng.graph_info()
+    n_atoms = sum(w["n_atoms"] for w in walkers)
+    batched = n_atoms * args.steps / (st["step_ms"] / 1e3)
+    eng.close()
+    ts = []
+    for w, m in list(zip(walkers, polys))[:2]:
+        job = serve.Job(0, w, p, args.steps, mcmd=m)
+        dt, _, _, _ = serve.run_alone(job, warmup=warm)
+        ts.append(job.n_atoms * job.n_steps / dt)
+    plain = float(np.mean(ts))
+    return {"metric": "batch atom-steps/s", "value": batched, "unit": "atom-steps/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": warm, "ms_per_step": st["step_ms"] / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": "%d McMD walkers, 300-atom chain in 2500 TIP3P waters each (%d atoms total), "
+                                   "dt 2 fs, 300 K velocity rescaling, V-McMD force scaling (order-6 polynomial)"
+                                   % (len(walkers), n_atoms)},
+            "plain": {"atom_steps_per_s": plain, "sample": "2 walkers run alone (wall clock around og_step)"},
+            "speedup_vs_plain": batched / plain, "gpu_launches": st["kernel_launches"], "graphs": graphs}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -303,8 +425,22 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="water1m", choices=["water1m", "serve", "mcmd"],
+                    help="water1m: the 1M-atom step (default); serve: batched job stream; mcmd: McMD walkers")
+    ap.add_argument("--jobs", type=int, default=256)
+    ap.add_argument("--job-steps", type=int, default=5000)
+    ap.add_argument("--max-jobs", type=int, default=64)
+    ap.add_argument("--window", type=int, default=100)
+    ap.add_argument("--plain-sample", type=int, default=8)
+    ap.add_argument("--walkers", type=int, default=64)
+    ap.add_argument("--walker-seed0", type=int, default=500)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.workload in ("serve", "mcmd") and args.impl == "ours":
+        if int(os.environ.get("RANK", "0")) == 0:
+            out = run_serve(args) if args.workload == "serve" else run_mcmd(args)
+            print(json.dumps(out))
+        return
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":
         if rank != 0:

@@ -174,8 +174,9 @@ og_status og_get_trace(og_engine *e, double *out, int32_t max_steps, int32_t *n_
 
 /* Launch statistics: kernels launched by the last og_step and device time of its pair kernel. */
 og_status og_get_stats(og_engine *e, int64_t *kernel_launches, double *pair_kernel_ms, double *step_ms);
-/* Enables CUDA-event timing of the pair kernel and of whole og_step calls (read with
- * og_get_stats); adds one host synchronisation per step while on. */
+/* CUDA-event timing read with og_get_stats: on = 1 times every pair-kernel launch and the whole
+ * og_step call (steps then launch kernel by kernel); on = 2 times only the whole og_step call
+ * (graph replays stay on); 0 turns timing off. */
 og_status og_set_timing(og_engine *e, int32_t on);
 /* Device flags raised since the last og_step began: bit 8 = a SHAKE trio hit const_max_loops,
  * bit 16 = the thermostat loop hit thermo_const_max_loops (both non-fatal, as in the reference,
@@ -188,6 +189,17 @@ og_status og_get_tuning(og_engine *e, int32_t *pair_variant, double *variant_ms)
  * serving loop re-creates engines for new batches; -1 restores autotuning.  No counterpart in
  * the reference, which has one pair kernel. */
 og_status og_set_tuning(og_engine *e, int32_t pair_variant);
+/* CUDA graphs (no counterpart in the reference, whose host loop launches every kernel each step):
+ * og_step replays one captured graph per whole list interval -- the rebuild step and the
+ * nsgrid_update_intvl-1 steps after it, the thermostat-with-SHAKE loop as a device-side WHILE
+ * node -- when the step count covers it; other steps, and every step while og_set_timing(e, 1) is
+ * on, launch kernel by kernel with identical results.  og_set_graphs(e, 0) turns graphs off
+ * (default on).  og_get_graph_info reports whether graphs are on, how many replays ran and how
+ * many kernel launches one replay stands for; `note` (may be NULL, 256 bytes) says why capture
+ * turned graphs off, if it did. */
+og_status og_set_graphs(og_engine *e, int32_t on);
+og_status og_get_graph_info(og_engine *e, int32_t *enabled, int64_t *replays, int64_t *kernels_per_replay,
+                            char *note);
 /* Fixed-order FP64 sums of d_values[i*stride] over the segments [d_seg_base[s], d_seg_base[s+1])
  * of a device array, s < n_seg, into d_out[s] (device).  max_seg_len bounds every segment's
  * length.  The engine's own energy / kinetic-energy reduction (two levels: 4096-item chunks,

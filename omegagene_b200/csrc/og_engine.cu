@@ -71,8 +71,9 @@ __global__ void k_shake_pair(int, const int2 *, const double *, const int *, con
 __global__ void k_shake_trio(int, const int4 *, const double *, const SysDev *, const int *, const float *, double *,
                              const double *, int, double, int *);
 __global__ void k_ke_mid(int, const float *, const double *, const double *, double *);
-__global__ void k_thermo_check(int, const SysDev *, const double *, const double *, const long long *, int, int,
-                               double, int *, int *, int *);
+__global__ void k_thermo_check(int, const SysDev *, const double *, const double *, const long long *, const int *,
+                               int, double, int *, int *, int *);
+__global__ void k_thermo_next(int *, int *, int, cudaGraphConditionalHandle, int);
 __global__ void k_thermo_half(int, const int *, const SysDev *, const int *, const double *, const float *,
                               const float *, const double *, const double *, const double *, double *, double *);
 __global__ void k_thermo_rescale(int, const int *, const SysDev *, const int *, const double *, const double *,
@@ -188,7 +189,15 @@ struct og_engine {
     float2 *d_lj = nullptr;
     double *d_sys_acc = nullptr, *d_mcmd = nullptr, *d_energies = nullptr, *d_thermo = nullptr,
            *d_sum_tmp = nullptr;
-    int *d_mask_plain = nullptr, *d_mask_thermo = nullptr, *d_active = nullptr, *d_any = nullptr;
+    int *d_mask_plain = nullptr, *d_mask_thermo = nullptr, *d_active = nullptr, *d_any = nullptr,
+        *d_thermo_it = nullptr;
+    // CUDA graph of one list interval (a rebuild step + intvl-1 steps), replayed by og_step
+    cudaStream_t side = nullptr;       // captures the thermostat loop body
+    cudaGraphExec_t graph_exec = nullptr;
+    bool use_graphs = true, capturing = false;
+    std::string graph_note;           // why graph capture turned graphs off, if it did
+    long long graph_kernels = 0;      // kernel launches one replay stands for
+    long long graph_replays = 0;
     // segment bases for the two-level reductions and their chunk counts
     int *d_seg_atoms = nullptr, *d_seg_exc = nullptr, *d_seg_bond = nullptr, *d_seg_angle = nullptr;
     int mc_atoms = 1, mc_cells = 1, mc_exc = 1, mc_bond = 1, mc_angle = 1, mc_grp = 1;
@@ -210,7 +219,7 @@ struct og_engine {
     int pair_variant = 0;
     int fixed_variant = -1;  // og_set_tuning: variant chosen by the caller, -1 = autotune
     double variant_ms[3] = {0, 0, 0};
-    bool timing = false;
+    int timing = 0;  // 1: step + per-pair-kernel events (kernel by kernel); 2: step events only
     std::vector<void *> allocs;
 };
 
@@ -474,7 +483,7 @@ og_status compute_forces(og_engine *e, bool vir) {
     k_cell_bbox<<<blocks(e->cells_cap, 256), 256, 0, st>>>(e->d_counters, e->cells_cap, e->d_xq, e->d_cell_valid,
                                                             e->d_bbox);
     LAUNCH_CHECK();
-    if (e->timing) {
+    if (e->timing == 1) {
         if (e->pev_used >= (int)e->pev0.size()) {
             cudaEvent_t a, b;
             CK(cudaEventCreate(&a));
@@ -488,7 +497,7 @@ og_status compute_forces(og_engine *e, bool vir) {
         og_status ps = launch_pair(e, vir, vir ? 0 : e->pair_variant);
         if (ps) return ps;
     }
-    if (e->timing) CK(cudaEventRecord(e->pev1[e->pev_used++], st));
+    if (e->timing == 1) CK(cudaEventRecord(e->pev1[e->pev_used++], st));
     if (vir) {
         if (!e->d_vir_atom) {
             og_status s = dalloc(e, &e->d_vir_atom, 9 * (size_t)e->n_atoms);
@@ -601,44 +610,92 @@ og_status shake(og_engine *e, const int *active) {
     return OG_OK;
 }
 
+// One pass of ThermostatScaling::apply_thermostat_with_shake's loop (Thermostat.cpp:105-170) for
+// the systems still in d_active: constraint, temperature test, rescale, COM cancel, positions.
+// In a graph, the pass in which every system leaves the loop still launches the later kernels;
+// they skip inactive systems, so the state is the one the reference's `break` leaves.
+og_status thermo_pass(og_engine *e, cudaGraphConditionalHandle cond, int use_cond) {
+    cudaStream_t st = e->stream;
+    og_status s = shake(e, e->d_active);
+    if (s) return s;
+    k_ke_mid<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_mass, e->d_vel, e->d_vel_next, e->d_ke);
+    LAUNCH_CHECK();
+    if ((s = seg_sum<1>(e, e->d_ke, 1, 0, e->d_seg_atoms, e->mc_atoms, e->d_sum_tmp, 1, 0, 0))) return s;
+    k_thermo_check<<<blocks(e->n_sys, 128), 128, 0, st>>>(e->n_sys, e->d_sys, e->d_sum_tmp, e->d_thermo, e->d_step,
+                                                           e->d_thermo_it, e->thermo_max_loops, e->thermo_tol,
+                                                           e->d_active, e->d_any, e->d_counters);
+    LAUNCH_CHECK();
+    if (!use_cond) CK(cudaMemcpyAsync(e->h_pinned, e->d_any, sizeof(int), cudaMemcpyDeviceToHost, st));
+    k_thermo_next<<<1, 32, 0, st>>>(e->d_any, e->d_thermo_it, e->thermo_max_loops, cond, use_cond);
+    LAUNCH_CHECK();
+    if (!use_cond) {
+        CK(cudaStreamSynchronize(st));
+        if (e->h_pinned[0] == 0) return OG_OK;
+    }
+    k_thermo_half<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys, e->d_active,
+                                                            e->d_work, e->d_mass, e->d_mass_inv, e->d_crd,
+                                                            e->d_buf_crd, e->d_vel, e->d_vel_next, e->d_ke);
+    LAUNCH_CHECK();
+    if ((s = seg_sum<1>(e, e->d_ke, 1, 0, e->d_seg_atoms, e->mc_atoms, e->d_sum_tmp, 1, 0, 0))) return s;
+    k_thermo_rescale<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys, e->d_active,
+                                                               e->d_sum_tmp, e->d_thermo, e->d_step, e->d_work,
+                                                               e->d_mass_inv, e->d_crd, e->d_buf_crd, e->d_vel,
+                                                               e->d_vel_next);
+    LAUNCH_CHECK();
+    s = com_cancel(e, e->d_vel_next, e->d_active);
+    if (s) return s;
+    k_thermo_crd<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys, e->d_active, e->d_crd,
+                                                           e->d_crd_prev, e->d_vel_next);
+    LAUNCH_CHECK();
+    return OG_OK;
+}
+
 // ThermostatScaling::apply_thermostat_with_shake (Thermostat.cpp:86-170) for every system that
-// has constraints and the scaling thermostat; the loop ends when all have converged.
+// has constraints and the scaling thermostat; the loop ends when all have converged or after
+// thermo_const_max_loops passes.  Launched directly, the host reads the "still iterating"
+// count after every pass.  Under graph capture the loop becomes a conditional WHILE node whose
+// body is one pass; k_thermo_next sets its condition on the device.
 og_status thermostat_with_shake(og_engine *e) {
     cudaStream_t st = e->stream;
+    if (e->thermo_max_loops <= 0) return OG_OK;
     CK(cudaMemcpyAsync(e->d_active, e->d_mask_thermo, sizeof(int) * e->n_sys, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemsetAsync(e->d_any, 0, sizeof(int), st));
+    CK(cudaMemsetAsync(e->d_thermo_it, 0, sizeof(int), st));
     k_copy_double<<<blocks(3LL * e->n_atoms, 256), 256, 0, st>>>(e->d_buf_crd, e->d_crd, 3LL * e->n_atoms);
     LAUNCH_CHECK();
-    og_status s;
-    for (int it = 0; it < e->thermo_max_loops; it++) {
-        s = shake(e, e->d_active);
-        if (s) return s;
-        k_ke_mid<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_mass, e->d_vel, e->d_vel_next, e->d_ke);
-        LAUNCH_CHECK();
-        if ((s = seg_sum<1>(e, e->d_ke, 1, 0, e->d_seg_atoms, e->mc_atoms, e->d_sum_tmp, 1, 0, 0))) return s;
-        CK(cudaMemsetAsync(e->d_any, 0, sizeof(int), st));
-        k_thermo_check<<<blocks(e->n_sys, 128), 128, 0, st>>>(e->n_sys, e->d_sys, e->d_sum_tmp, e->d_thermo, e->d_step,
-                                                               it, e->thermo_max_loops, e->thermo_tol, e->d_active,
-                                                               e->d_any, e->d_counters);
-        LAUNCH_CHECK();
-        CK(cudaMemcpyAsync(e->h_pinned, e->d_any, sizeof(int), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        if (e->h_pinned[0] == 0) break;
-        k_thermo_half<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys, e->d_active,
-                                                                e->d_work, e->d_mass, e->d_mass_inv, e->d_crd,
-                                                                e->d_buf_crd, e->d_vel, e->d_vel_next, e->d_ke);
-        LAUNCH_CHECK();
-        if ((s = seg_sum<1>(e, e->d_ke, 1, 0, e->d_seg_atoms, e->mc_atoms, e->d_sum_tmp, 1, 0, 0))) return s;
-        k_thermo_rescale<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys, e->d_active,
-                                                                   e->d_sum_tmp, e->d_thermo, e->d_step, e->d_work,
-                                                                   e->d_mass_inv, e->d_crd, e->d_buf_crd, e->d_vel,
-                                                                   e->d_vel_next);
-        LAUNCH_CHECK();
-        s = com_cancel(e, e->d_vel_next, e->d_active);
-        if (s) return s;
-        k_thermo_crd<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys, e->d_active,
-                                                               e->d_crd, e->d_crd_prev, e->d_vel_next);
-        LAUNCH_CHECK();
+    if (!e->capturing) {
+        for (int it = 0; it < e->thermo_max_loops; it++) {
+            og_status s = thermo_pass(e, cudaGraphConditionalHandle(), 0);
+            if (s) return s;
+            if (e->h_pinned[0] == 0) break;
+        }
+        return OG_OK;
     }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t n_deps = 0;
+    CK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &n_deps));
+    if (cs != cudaStreamCaptureStatusActive || !g) return fail(e, OG_ERR_STATE, "thermostat loop: stream not capturing");
+    cudaGraphConditionalHandle cond;
+    CK(cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = cond;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, deps, n_deps, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    CK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    CK(cudaStreamBeginCaptureToGraph(e->side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    e->stream = e->side;
+    og_status s = thermo_pass(e, cond, 1);
+    e->stream = st;
+    cudaGraph_t captured = nullptr;
+    cudaError_t r = cudaStreamEndCapture(e->side, &captured);
+    if (s) return s;
+    CK(r);
     return OG_OK;
 }
 
@@ -714,7 +771,13 @@ og_status check_flags(og_engine *e) {
     return OG_OK;
 }
 
+void drop_graph(og_engine *e) {
+    if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
+    e->graph_exec = nullptr;
+}
+
 og_status grow_pairs(og_engine *e, long long need) {
+    drop_graph(e);  // the graph holds the old list buffers
     long long cap = need + need / 2 + 4096;
     dfree(e, e->d_cp_c2img);
     dfree(e, e->d_cp_mask);
@@ -729,6 +792,34 @@ og_status grow_pairs(og_engine *e, long long need) {
     s = dalloc(e, &e->d_cp_shift, (size_t)cap);
     if (s) return s;
     e->pair_cap = cap;
+    return OG_OK;
+}
+
+// Captures one list interval -- the rebuild step and the intvl-1 steps after it -- into a graph.
+// Kernel arguments are device pointers and sizes fixed at og_finalize; the step number, the
+// thermostat loop index and every per-step decision live on the device, so the graph replays
+// any interval.  A failed capture turns graphs off for the engine (kernel-by-kernel steps give
+// the same results) and records why.
+og_status capture_interval(og_engine *e) {
+    const long long step0 = e->host_step, launches0 = e->launches;
+    CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeRelaxed));
+    e->capturing = true;
+    og_status s = OG_OK;
+    for (int i = 0; i < e->intvl && s == OG_OK; i++) s = run_step(e);
+    e->capturing = false;
+    cudaGraph_t g = nullptr;
+    cudaError_t r = cudaStreamEndCapture(e->stream, &g);
+    e->host_step = step0;
+    e->graph_kernels = e->launches - launches0;
+    e->launches = launches0;
+    if (s == OG_OK && r == cudaSuccess && g) r = cudaGraphInstantiate(&e->graph_exec, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (s != OG_OK || r != cudaSuccess || !e->graph_exec) {
+        cudaGetLastError();
+        e->graph_exec = nullptr;
+        e->use_graphs = false;
+        e->graph_note = s != OG_OK ? e->err : std::string(cudaGetErrorString(r));
+    }
     return OG_OK;
 }
 
@@ -814,6 +905,7 @@ og_status og_create(int device, og_engine **out) {
         return OG_ERR_CUDA;
     }
     if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&e->ev_pair0) != cudaSuccess || cudaEventCreate(&e->ev_pair1) != cudaSuccess ||
         cudaEventCreate(&e->ev_step0) != cudaSuccess || cudaEventCreate(&e->ev_step1) != cudaSuccess ||
         cudaMallocHost((void **)&e->h_pinned, 64 * sizeof(int)) != cudaSuccess) {
@@ -837,7 +929,9 @@ og_status og_destroy(og_engine *e) {
     if (e->ev_pair1) cudaEventDestroy(e->ev_pair1);
     if (e->ev_step0) cudaEventDestroy(e->ev_step0);
     if (e->ev_step1) cudaEventDestroy(e->ev_step1);
+    if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
     if (e->stream) cudaStreamDestroy(e->stream);
+    if (e->side) cudaStreamDestroy(e->side);
     delete e;
     return OG_OK;
 }
@@ -1124,7 +1218,7 @@ og_status og_finalize(og_engine *e) {
         (s = dalloc(e, &e->d_energies, 11 * (size_t)S)) || (s = upload(e, &e->d_thermo, thermo)) ||
         (s = dalloc(e, &e->d_sum_tmp, S)) || (s = upload(e, &e->d_mask_plain, mask_plain)) ||
         (s = upload(e, &e->d_mask_thermo, mask_thermo)) || (s = dalloc(e, &e->d_active, S)) ||
-        (s = dalloc(e, &e->d_any, 1)))
+        (s = dalloc(e, &e->d_any, 1)) || (s = dalloc(e, &e->d_thermo_it, 1)))
         return s;
     {
         std::vector<int> sa(S + 1), se(S + 1), sb(S + 1), sg(S + 1);
@@ -1210,8 +1304,22 @@ og_status og_step(og_engine *e, int32_t n_steps) {
         if ((s = clear_flags(e))) return s;
         e->pev_used = 0;
         if (e->timing) CK(cudaEventRecord(e->ev_step0, e->stream));
-        for (int i = 0; i < n_steps; i++)
+        for (int i = 0; i < n_steps;) {
+            // whole list intervals replay the captured graph (not while per-kernel timing is on)
+            if (e->use_graphs && e->timing != 1 && e->host_step % e->intvl == 0 && n_steps - i >= e->intvl) {
+                if (!e->graph_exec && (s = capture_interval(e))) return s;
+                if (e->graph_exec) {
+                    CK(cudaGraphLaunch(e->graph_exec, e->stream));
+                    e->launches += e->graph_kernels;
+                    e->graph_replays++;
+                    e->host_step += e->intvl;
+                    i += e->intvl;
+                    continue;
+                }
+            }
             if ((s = run_step(e))) return s;
+            i++;
+        }
         if (e->timing) {
             CK(cudaEventRecord(e->ev_step1, e->stream));
             CK(cudaEventSynchronize(e->ev_step1));
@@ -1393,6 +1501,7 @@ og_status og_get_cell_pairs(og_engine *e, int32_t sys, int32_t *idx_head, int32_
 og_status og_set_trace(og_engine *e, int32_t capacity) {
     if (!e || !e->finalized) return fail(e, OG_ERR_STATE, "og_set_trace before og_finalize");
     if (capacity < 0) return fail(e, OG_ERR_INVALID, "negative capacity");
+    drop_graph(e);  // the graph holds the trace buffer and its capacity
     if (e->d_trace) {
         dfree(e, e->d_trace);
         e->d_trace = nullptr;
@@ -1452,7 +1561,7 @@ og_status og_get_sizes(og_engine *e, int32_t *n_systems, int64_t *n_atoms_total)
 // header's main list: enabled by the benchmark.
 og_status og_set_timing(og_engine *e, int32_t on) {
     if (!e) return OG_ERR_INVALID;
-    e->timing = on != 0;
+    e->timing = on == 2 ? 2 : (on != 0 ? 1 : 0);
     return OG_OK;
 }
 
@@ -1561,5 +1670,23 @@ extern "C" og_status og_set_tuning(og_engine *e, int32_t pair_variant) {
     if (e->finalized) return fail(e, OG_ERR_STATE, "og_set_tuning after og_finalize");
     if (pair_variant < -1 || pair_variant > 2) return fail(e, OG_ERR_INVALID, "pair variant must be -1, 0, 1 or 2");
     e->fixed_variant = pair_variant;
+    return OG_OK;
+}
+
+extern "C" og_status og_set_graphs(og_engine *e, int32_t on) {
+    if (!e) return OG_ERR_INVALID;
+    e->use_graphs = on != 0;
+    if (!e->use_graphs) drop_graph(e);
+    e->graph_note.clear();
+    return OG_OK;
+}
+
+extern "C" og_status og_get_graph_info(og_engine *e, int32_t *enabled, int64_t *replays, int64_t *kernels_per_replay,
+                                       char *note) {
+    if (!e) return OG_ERR_INVALID;
+    if (enabled) *enabled = e->use_graphs ? 1 : 0;
+    if (replays) *replays = e->graph_replays;
+    if (kernels_per_replay) *kernels_per_replay = e->graph_kernels;
+    if (note) snprintf(note, 256, "%s", e->graph_note.c_str());
     return OG_OK;
 }

@@ -450,14 +450,17 @@ __global__ void k_ke_mid(int n_atoms, const float *__restrict__ mass, const doub
 }
 
 // Convergence test of the thermostat loop, one thread per system (Thermostat.cpp:124-131).
-// sys_active[s] stays 1 while the system still iterates; *any receives the count.
+// sys_active[s] stays 1 while the system still iterates; *any receives the count.  The loop
+// index lives on the device (*it_ptr, advanced by k_thermo_next) so that the loop can run
+// inside a graph without the host.
 __global__ void k_thermo_check(int n_sys, const SysDev *__restrict__ sys, const double *__restrict__ sum_ke,
-                               const double *__restrict__ thermo, const long long *__restrict__ step, int it,
-                               int max_loops, double tol, int *__restrict__ sys_active, int *__restrict__ any,
-                               int *__restrict__ counters) {
+                               const double *__restrict__ thermo, const long long *__restrict__ step,
+                               const int *__restrict__ it_ptr, int max_loops, double tol, int *__restrict__ sys_active,
+                               int *__restrict__ any, int *__restrict__ counters) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_sys) return;
     if (!sys_active[s]) return;
+    const int it = *it_ptr;
     const SysDev &S = sys[s];
     const double tcur = sum_ke[s] * S.temperature_coeff_thermo;
     const double tt = target_temperature(thermo, s, *step);
@@ -646,6 +649,20 @@ __global__ void k_put_state(int n_atoms, int atom0, const int *__restrict__ atom
         p.z = r[2];
         xq[sl] = p;
     }
+}
+
+// Advances the thermostat loop index and clears the "still iterating" count for the next
+// pass.  Inside a graph (use_cond) it also sets the loop's conditional node: another pass only
+// while some system still iterates and fewer than max_loops passes have run, so the device-side
+// loop ends after max_loops passes at most, whatever the data.
+__global__ void k_thermo_next(int *__restrict__ any, int *__restrict__ it, int max_loops,
+                              cudaGraphConditionalHandle cond, int use_cond) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int next = *it + 1;
+    const int still = *any;
+    *it = next;
+    *any = 0;
+    if (use_cond) cudaGraphSetConditional(cond, (still != 0 && next < max_loops) ? 1u : 0u);
 }
 
 __global__ void k_trace_advance(long long *trace_count, long long *step) {

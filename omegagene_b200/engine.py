@@ -85,6 +85,8 @@ def load_library():
         "og_step_async": [E, C.c_int32], "og_synchronize": [E],
         "og_get_pair_count": [E, C.c_int32, _p(C.c_int64)],
         "og_get_tuning": [E, _p(C.c_int32), C.c_void_p], "og_set_tuning": [E, C.c_int32],
+        "og_set_graphs": [E, C.c_int32],
+        "og_get_graph_info": [E, _p(C.c_int32), _p(C.c_int64), _p(C.c_int64), C.c_char_p],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -350,7 +352,10 @@ class Engine:
         return out[:n.value]
 
     def set_timing(self, on=True):
-        self._check(self.L.og_set_timing(self.h, 1 if on else 0), "og_set_timing")
+        """on=True: per-pair-kernel and per-call events (kernel-by-kernel steps); "step": per-call
+        events only (graph replays stay on); False: off."""
+        mode = 2 if on == "step" else (1 if on else 0)
+        self._check(self.L.og_set_timing(self.h, mode), "og_set_timing")
 
     def stats(self):
         k, p, s = C.c_int64(), C.c_double(), C.c_double()
@@ -390,3 +395,13 @@ class Engine:
     def set_tuning(self, variant):
         """Fixes the pair-kernel variant (0/1/2) before finalize(); -1 = autotune."""
         self._check(self.L.og_set_tuning(self.h, int(variant)), "og_set_tuning")
+
+    def set_graphs(self, on=True):
+        self._check(self.L.og_set_graphs(self.h, 1 if on else 0), "og_set_graphs")
+
+    def graph_info(self):
+        en, rep, k = C.c_int32(), C.c_int64(), C.c_int64()
+        note = C.create_string_buffer(256)
+        self._check(self.L.og_get_graph_info(self.h, C.byref(en), C.byref(rep), C.byref(k), note), "og_get_graph_info")
+        return {"enabled": bool(en.value), "replays": rep.value, "kernels_per_replay": k.value,
+                "note": note.value.decode()}

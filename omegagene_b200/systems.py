@@ -309,3 +309,23 @@ def poisson_job_stream(n_jobs=256, seed=3, lo=500, hi=10000, mean_interarrival_s
     arrivals = np.cumsum(rng.exponential(mean_interarrival_s, n_jobs))
     return [{"job": i, "n_waters": int(c), "seed": 1000 + i, "arrival_s": float(t)}
             for i, (c, t) in enumerate(zip(counts, arrivals))]
+
+
+def mcmd_polynomial(e_mean, e_sd, seed, temperature=300.0, order=6):
+    """V-McMD parameters for one walker: a seeded order-`order` polynomial for d lnP / dE over
+    [mean - 4 sd, mean + 4 sd], in powers of E as the reference's virtual-state files give it
+    (Extend.cpp:178-203, where the factor is R T * sum c_i E^i with E clamped to the range).
+    In the scaled variable x = (E - mean) / (4 sd) the coefficients are 1/(R T) for x^0 and
+    U(-0.02, 0.02)/(R T) for the others, so R T dlnP/dE stays near 1 over the range."""
+    rng = np.random.default_rng(seed)
+    const_k = KB_KCAL * temperature
+    lo, hi = e_mean - 4.0 * e_sd, e_mean + 4.0 * e_sd
+    half = 0.5 * (hi - lo)
+    a = np.zeros(order + 1)
+    a[0] = 1.0 / const_k
+    a[1:] = rng.uniform(-0.02, 0.02, order) / const_k
+    c = np.zeros(order + 1)
+    for k in range(order + 1):
+        for i in range(k + 1):
+            c[i] += a[k] * math.comb(k, i) * (-e_mean) ** (k - i) / half ** k
+    return {"coef": c.tolist(), "lambda_low": lo, "lambda_high": hi, "temperature": temperature}

@@ -1,0 +1,69 @@
+"""CUDA-graph replay of whole list intervals against kernel-by-kernel stepping.
+
+og_step replays one captured graph per list interval (rebuild step + intvl-1 steps; the
+thermostat-with-SHAKE loop is a device-side WHILE node).  Every per-step decision lives on the
+device, so replayed and directly launched steps must give bitwise identical trajectories.
+"""
+import numpy as np
+import pytest
+
+from omegagene_b200 import engine, systems
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(**kw):
+    p = dict(engine.DEFAULT_PARAMS)
+    p.update(kw)
+    return p
+
+
+def _mixed_batch():
+    """Thermostat + SHAKE water, NVE water, and a McMD-scaled chain with SHAKE pairs under the
+    thermostat: every branch of the step in one engine."""
+    thermo = _params(nsgrid_update_intvl=10, time_step=2.0, thermostat="scaling", temperature=300.0)
+    nve = _params(nsgrid_update_intvl=10, time_step=2.0)
+    chain = systems.chain_water_system(300, 2500, seed=4, radius=12.0)
+    mcmd = systems.mcmd_polynomial(-9000.0, 400.0, seed=7)
+    return [(systems.water_system(1500, seed=5), thermo, None),
+            (systems.water_system(700, seed=9), nve, None),
+            (chain, thermo, mcmd)]
+
+
+def _run(batch, n_steps, graphs, chunks=None):
+    eng = engine.Engine(0)
+    eng.set_graphs(graphs)
+    for s, p, m in batch:
+        eng.add_system(s, p, m)
+    eng.finalize()
+    eng.set_trace(n_steps)
+    for n in chunks or [n_steps]:
+        eng.step(n)
+    states = [eng.get_state(i) for i in range(len(batch))]
+    return eng, eng.get_trace(n_steps), states
+
+
+def test_graph_replay_equals_kernel_by_kernel():
+    batch = _mixed_batch()
+    n = 35  # three whole intervals replayed, five steps launched directly
+    eg, tg, sg = _run(batch, n, True)
+    ek, tk, sk = _run(batch, n, False)
+    info = eg.graph_info()
+    assert info["enabled"], info["note"]
+    assert info["replays"] == 3 and info["kernels_per_replay"] > 100
+    assert ek.graph_info()["replays"] == 0
+    np.testing.assert_array_equal(tg, tk)
+    for (c1, v1), (c2, v2) in zip(sg, sk):
+        assert np.array_equal(c1, c2) and np.array_equal(v1, v2)
+    assert eg.flags() == ek.flags()
+
+
+def test_graph_split_calls_equal_one_call():
+    """Calls of any length, aligned to the list interval or not, give the trajectory of one
+    long call."""
+    batch = _mixed_batch()[:2]
+    _, t1, s1 = _run(batch, 40, True)
+    _, t2, s2 = _run(batch, 40, True, chunks=[3, 7, 10, 20])
+    np.testing.assert_array_equal(t1, t2)
+    for (c1, v1), (c2, v2) in zip(s1, s2):
+        assert np.array_equal(c1, c2) and np.array_equal(v1, v2)
