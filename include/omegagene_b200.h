@@ -198,6 +198,12 @@ og_status og_set_tuning(og_engine *e, int32_t pair_variant);
  * many kernel launches one replay stands for; `note` (may be NULL, 256 bytes) says why capture
  * turned graphs off, if it did. */
 og_status og_set_graphs(og_engine *e, int32_t on);
+/* Engines take device memory from one stream-ordered pool per device, which keeps what
+ * og_destroy frees for the next engine of the process (a serving loop re-creates engines for
+ * every new batch).  This returns the pool's unused reserve on `device` to the driver; it
+ * synchronises that device first.  No counterpart in the reference, which allocates once per
+ * run with cudaMalloc. */
+og_status og_release_pool_memory(int32_t device);
 og_status og_get_graph_info(og_engine *e, int32_t *enabled, int64_t *replays, int64_t *kernels_per_replay,
                             char *note);
 /* Fixed-order FP64 sums of d_values[i*stride] over the segments [d_seg_base[s], d_seg_base[s+1])

@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -251,12 +252,46 @@ og_status fail(og_engine *e, og_status s, const char *fmt, ...) {
             return fail(e, OG_ERR_CUDA, "kernel launch: %s (%s:%d)", cudaGetErrorString(_e), __FILE__, __LINE__); \
     } while (0)
 
+// Device memory comes from one stream-ordered pool per device that keeps what engines free
+// (release threshold = unlimited): a serving loop that re-creates engines for every new batch
+// then reuses the same memory without returning it to the driver and mapping it again, and an
+// engine's teardown does not wait on the whole device.  og_release_pool_memory gives the
+// reserve back.
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[256] = {};
+
+cudaError_t engine_pool(int device, cudaMemPool_t *out) {
+    if (device < 0 || device >= 256) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (!g_pool[device]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t pool = nullptr;
+        cudaError_t r = cudaMemPoolCreate(&pool, &props);
+        if (r != cudaSuccess) return r;
+        uint64_t keep = UINT64_MAX;
+        r = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (r != cudaSuccess) {
+            cudaMemPoolDestroy(pool);
+            return r;
+        }
+        g_pool[device] = pool;
+    }
+    *out = g_pool[device];
+    return cudaSuccess;
+}
+
 template <class T>
 og_status dalloc(og_engine *e, T **p, size_t n) {
     if (n == 0) n = 1;
     void *q = nullptr;
-    cudaError_t r = cudaMalloc(&q, n * sizeof(T));
-    if (r != cudaSuccess) return fail(e, OG_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(r));
+    cudaMemPool_t pool = nullptr;
+    cudaError_t r = engine_pool(e->device, &pool);
+    if (r == cudaSuccess) r = cudaMallocFromPoolAsync(&q, n * sizeof(T), pool, e->stream);
+    if (r != cudaSuccess)
+        return fail(e, OG_ERR_NOMEM, "device allocation (%zu bytes): %s", n * sizeof(T), cudaGetErrorString(r));
     e->allocs.push_back(q);
     *p = (T *)q;
     return OG_OK;
@@ -269,7 +304,7 @@ void dfree(og_engine *e, void *p) {
             e->allocs.erase(e->allocs.begin() + i);
             break;
         }
-    cudaFree(p);
+    cudaFreeAsync(p, e->stream);
 }
 
 template <class T>
@@ -919,8 +954,11 @@ og_status og_create(int device, og_engine **out) {
 og_status og_destroy(og_engine *e) {
     if (!e) return OG_OK;
     cudaSetDevice(e->device);
-    if (e->stream) cudaStreamSynchronize(e->stream);
-    for (void *p : e->allocs) cudaFree(p);
+    if (e->stream) {
+        cudaStreamSynchronize(e->stream);
+        for (void *p : e->allocs) cudaFreeAsync(p, e->stream);
+        cudaStreamSynchronize(e->stream);
+    }
     e->allocs.clear();
     if (e->h_pinned) cudaFreeHost(e->h_pinned);
     for (auto ev : e->pev0) cudaEventDestroy(ev);
@@ -1689,4 +1727,20 @@ extern "C" og_status og_get_graph_info(og_engine *e, int32_t *enabled, int64_t *
     if (kernels_per_replay) *kernels_per_replay = e->graph_kernels;
     if (note) snprintf(note, 256, "%s", e->graph_note.c_str());
     return OG_OK;
+}
+
+extern "C" og_status og_release_pool_memory(int32_t device) {
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        if (device < 0 || device >= 256) return OG_ERR_INVALID;
+        pool = g_pool[device];
+    }
+    if (!pool) return OG_OK;
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess) return OG_ERR_CUDA;
+    cudaError_t r = cudaDeviceSynchronize();
+    if (r == cudaSuccess) r = cudaMemPoolTrimTo(pool, 0);
+    cudaSetDevice(prev);
+    return r == cudaSuccess ? OG_OK : OG_ERR_CUDA;
 }

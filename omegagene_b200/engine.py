@@ -85,7 +85,7 @@ def load_library():
         "og_step_async": [E, C.c_int32], "og_synchronize": [E],
         "og_get_pair_count": [E, C.c_int32, _p(C.c_int64)],
         "og_get_tuning": [E, _p(C.c_int32), C.c_void_p], "og_set_tuning": [E, C.c_int32],
-        "og_set_graphs": [E, C.c_int32],
+        "og_set_graphs": [E, C.c_int32], "og_release_pool_memory": [C.c_int32],
         "og_get_graph_info": [E, _p(C.c_int32), _p(C.c_int64), _p(C.c_int64), C.c_char_p],
     }
     for name, args in sig.items():
@@ -249,6 +249,13 @@ def make_desc(system, params=None, mcmd=None, first_step=0):
         d.mcmd_temperature = mcmd["temperature"]
         d.mcmd_coef = _ptr(keep.mcoef, C.c_double)
     return d, keep
+
+
+def release_pool_memory(device=0):
+    """Returns the device memory that destroyed engines left in the per-device pool."""
+    st = load_library().og_release_pool_memory(int(device))
+    if st != OG_OK:
+        raise OgError(st, "og_release_pool_memory")
 
 
 class Engine:

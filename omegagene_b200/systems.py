@@ -187,7 +187,7 @@ def _saw_chain(rng, n_backbone, radius, bond=1.53, angle_deg=111.0, min_dist=3.2
 
 
 def chain_water_system(n_chain=2000, n_waters=30000, seed=1, radius=30.0, box=None, temperature=300.0,
-                       n_sigma_bins=8, n_eps_bins=8):
+                       n_sigma_bins=8, n_eps_bins=8, h_angles=False):
     """Solvated synthetic chain: every third atom is a hydrogen bonded (SHAKE pair, 1.09 A) to
     the preceding backbone atom; backbone bonds 1.53 A / 310, angles 111 deg / 63 (E = k(x-x0)^2,
     ForceField.cpp:108-177).  Charges ~ N(0, 0.25) shifted to zero net; sigma ~ U(2.5, 3.8),
@@ -269,6 +269,12 @@ def chain_water_system(n_chain=2000, n_waters=30000, seed=1, radius=30.0, box=No
     atom_type = np.concatenate([type_c, np.tile([0, 1, 1], nw)])
     bonds = [(bb_index[i], bb_index[i + 1], 310.0, 1.53) for i in range(n_bb - 1)]
     angles = [(bb_index[i], bb_index[i + 1], bb_index[i + 2], 63.0, math.radians(111.0)) for i in range(n_bb - 2)]
+    if h_angles:  # hold each hydrogen's direction: backbone neighbour - parent - H, 109.5 deg, k 35
+        for h, p in sorted(parent_of_h.items()):
+            k = pos_of_bb[p]
+            for kk in (k - 1, k + 1):
+                if 0 <= kk < n_bb:
+                    angles.append((bb_index[kk], p, h, 35.0, math.radians(109.5)))
     bonds = np.array(bonds, dtype=[("a1", "<i4"), ("a2", "<i4"), ("k", "<f8"), ("r0", "<f8")])
     angles = np.array(angles, dtype=[("a1", "<i4"), ("a2", "<i4"), ("a3", "<i4"), ("k", "<f8"), ("t0", "<f8")])
     # 1-2, 1-3 and 1-4 pairs are excluded from the pair list (the reference's "nb15off")
