@@ -28,7 +28,8 @@ typedef enum {
     OG_ERR_CAPACITY = 3,  /* a device buffer is too small (cell pairs, column size) */
     OG_ERR_STATE = 4,     /* call out of order (e.g. step before finalize) */
     OG_ERR_NOMEM = 5,     /* device allocation failed */
-    OG_ERR_NOT_CONVERGED = 6 /* SHAKE / thermostat loop hit its iteration limit */
+    OG_ERR_NOT_CONVERGED = 6, /* SHAKE / thermostat loop hit its iteration limit */
+    OG_ERR_SYSTEM_FAULT = 7   /* og_step: some systems faulted, see og_get_system_faults */
 } og_status;
 
 typedef struct og_engine og_engine;
@@ -198,6 +199,14 @@ og_status og_set_tuning(og_engine *e, int32_t pair_variant);
  * many kernel launches one replay stands for; `note` (may be NULL, 256 bytes) says why capture
  * turned graphs off, if it did. */
 og_status og_set_graphs(og_engine *e, int32_t on);
+/* After og_step returned OG_ERR_SYSTEM_FAULT: per system (faults[n_systems]) the bits of what went
+ * wrong in it -- 4 = a non-finite or far out-of-box coordinate (the reference has no check and
+ * carries on with NaNs), 2 = more atoms in one MiniCell column than the engine sorts.  og_step
+ * undid the whole call for every system (positions, velocities, step and trace counters are
+ * those of the call's start); systems are independent, so a caller drops the faulted ones and
+ * steps the rest in a new handle with the same results they would have had.  No counterpart in
+ * the reference, which runs one system per process. */
+og_status og_get_system_faults(og_engine *e, int32_t *faults);
 /* Engines take device memory from one stream-ordered pool per device, which keeps what
  * og_destroy frees for the next engine of the process (a serving loop re-creates engines for
  * every new batch).  This returns the pool's unused reserve on `device` to the driver; it

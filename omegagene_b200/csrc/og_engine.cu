@@ -19,12 +19,12 @@
 namespace og {
 // og_grid.cu
 __global__ void k_assign_columns(const SysDev *, const int *, const double *, int, int *, unsigned long long *,
-                                 int *, int *);
+                                 int *, int *, int *);
 __global__ void k_scan_columns(const int *, int, int *, int *, int *, int *, const int *, int, int *);
 __global__ void k_scatter_columns(const int *, const unsigned long long *, int, const int *, int *,
                                   unsigned long long *);
 __global__ void k_sort_columns(const int *, const int *, const int *, const int *, const unsigned long long *,
-                               const SysDev *, const double *, int *, double *, int *, int *, int *, int *);
+                               const SysDev *, const double *, int *, double *, int *, int *, int *, int *, int *);
 __global__ void k_cell_info(const int *, int, const int *, const int *, const int *, const SysDev *, const double *,
                             const int *, double *, float2 *, int2 *, unsigned char *, int *, int *);
 __global__ void k_count_pairs(const int *, int, int, const int *, const int *, const SysDev *, const int *,
@@ -192,6 +192,9 @@ struct og_engine {
            *d_sum_tmp = nullptr;
     int *d_mask_plain = nullptr, *d_mask_thermo = nullptr, *d_active = nullptr, *d_any = nullptr,
         *d_thermo_it = nullptr;
+    int *d_sys_fault = nullptr;           // per system: OG_FLAG_BAD_COORD / OG_FLAG_COLUMN_CAPACITY
+    long long *d_snap_ctr = nullptr;      // step and trace counters at the start of og_step
+    std::vector<int32_t> faults;          // per-system fault bits of the last failed call
     // CUDA graph of one list interval (a rebuild step + intvl-1 steps), replayed by og_step
     cudaStream_t side = nullptr;       // captures the thermostat loop body
     cudaGraphExec_t graph_exec = nullptr;
@@ -444,7 +447,7 @@ og_status build_list(og_engine *e) {
     CK(cudaMemsetAsync(e->d_col_fill, 0, sizeof(int) * e->n_cols, st));
     k_assign_columns<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->d_sys, e->d_atom_sys, e->d_crd, e->n_atoms,
                                                                e->d_atom_col, e->d_atom_key, e->d_col_count,
-                                                               e->d_counters);
+                                                               e->d_counters, e->d_sys_fault);
     LAUNCH_CHECK();
     k_scan_columns<<<1, 1024, 0, st>>>(e->d_col_count, e->n_cols, e->d_col_atom_start, e->d_col_cell_start,
                                        e->d_col_head_cell, e->d_counters, e->d_sys_col_base, e->n_sys,
@@ -455,7 +458,8 @@ og_status build_list(og_engine *e) {
     LAUNCH_CHECK();
     k_sort_columns<<<e->n_cols, 512, 0, st>>>(e->d_col_count, e->d_col_atom_start, e->d_col_cell_start, e->d_col_sys,
                                               e->d_col_keys, e->d_sys, e->d_crd, e->d_slot_atom, e->d_slot_crd,
-                                              e->d_atom_slot, e->d_cell_col, e->d_cell_sys, e->d_counters);
+                                              e->d_atom_slot, e->d_cell_col, e->d_cell_sys, e->d_counters,
+                                              e->d_sys_fault);
     LAUNCH_CHECK();
     k_fill_int<<<blocks(e->n_uni, 256), 256, 0, st>>>(e->d_uni_lo, e->n_uni, 0x7fffffff);
     LAUNCH_CHECK();
@@ -860,6 +864,7 @@ og_status capture_interval(og_engine *e) {
 
 og_status clear_flags(og_engine *e) {
     CK(cudaMemsetAsync(e->d_counters + OG_CNT_FLAGS, 0, sizeof(int), e->stream));
+    CK(cudaMemsetAsync(e->d_sys_fault, 0, sizeof(int) * e->n_sys, e->stream));
     return OG_OK;
 }
 
@@ -1256,7 +1261,8 @@ og_status og_finalize(og_engine *e) {
         (s = dalloc(e, &e->d_energies, 11 * (size_t)S)) || (s = upload(e, &e->d_thermo, thermo)) ||
         (s = dalloc(e, &e->d_sum_tmp, S)) || (s = upload(e, &e->d_mask_plain, mask_plain)) ||
         (s = upload(e, &e->d_mask_thermo, mask_thermo)) || (s = dalloc(e, &e->d_active, S)) ||
-        (s = dalloc(e, &e->d_any, 1)) || (s = dalloc(e, &e->d_thermo_it, 1)))
+        (s = dalloc(e, &e->d_any, 1)) || (s = dalloc(e, &e->d_thermo_it, 1)) ||
+        (s = dalloc(e, &e->d_sys_fault, S)) || (s = dalloc(e, &e->d_snap_ctr, 2)))
         return s;
     {
         std::vector<int> sa(S + 1), se(S + 1), sb(S + 1), sg(S + 1);
@@ -1329,6 +1335,7 @@ og_status og_step(og_engine *e, int32_t n_steps) {
     CK(cudaSetDevice(e->device));
     og_status s;
     e->launches = 0;
+    e->faults.clear();
     if (e->timing) {
         e->pair_ms = 0.0;
     }
@@ -1339,6 +1346,9 @@ og_status og_step(og_engine *e, int32_t n_steps) {
         CK(cudaMemcpyAsync(e->d_snap, e->d_crd, sizeof(double) * 3 * e->n_atoms, cudaMemcpyDeviceToDevice, e->stream));
         CK(cudaMemcpyAsync(e->d_snap + 3 * (size_t)e->n_atoms, e->d_vel_next, sizeof(double) * 3 * e->n_atoms,
                            cudaMemcpyDeviceToDevice, e->stream));
+        CK(cudaMemcpyAsync(e->d_snap_ctr, e->d_step, sizeof(long long), cudaMemcpyDeviceToDevice, e->stream));
+        CK(cudaMemcpyAsync(e->d_snap_ctr + 1, e->d_trace_count, sizeof(long long), cudaMemcpyDeviceToDevice,
+                           e->stream));
         if ((s = clear_flags(e))) return s;
         e->pev_used = 0;
         if (e->timing) CK(cudaEventRecord(e->ev_step0, e->stream));
@@ -1372,19 +1382,38 @@ og_status og_step(og_engine *e, int32_t n_steps) {
         }
         int c[OG_CNT_SIZE];
         if ((s = read_counters(e, c))) return s;
-        if (!(c[OG_CNT_FLAGS] & OG_FLAG_PAIR_CAPACITY)) return check_flags(e);
-        // capacity miss: grow, restore the state of the call's start and redo
-        if ((s = grow_pairs(e, (long long)c[OG_CNT_N_PAIRS] * 5 / 4))) return s;
+        const int f = c[OG_CNT_FLAGS];
+        const bool fault = (f & (OG_FLAG_BAD_COORD | OG_FLAG_COLUMN_CAPACITY)) != 0;
+        if (!fault && !(f & OG_FLAG_PAIR_CAPACITY)) return check_flags(e);
+        if (fault) {
+            // A system left its box or packed a column beyond capacity.  Systems are
+            // independent, so the others are sound; the call is undone for all of them and the
+            // faulted systems are named, for the caller to drop them and step the rest again.
+            e->faults.assign(e->n_sys, 0);
+            CK(cudaMemcpy(e->faults.data(), e->d_sys_fault, sizeof(int) * e->n_sys, cudaMemcpyDeviceToHost));
+        } else if ((s = grow_pairs(e, (long long)c[OG_CNT_N_PAIRS] * 5 / 4))) {
+            return s;
+        }
+        // restore the state of the call's start (and redo it after a capacity miss)
         CK(cudaMemcpyAsync(e->d_crd, e->d_snap, sizeof(double) * 3 * e->n_atoms, cudaMemcpyDeviceToDevice, e->stream));
         CK(cudaMemcpyAsync(e->d_vel_next, e->d_snap + 3 * (size_t)e->n_atoms, sizeof(double) * 3 * e->n_atoms,
                            cudaMemcpyDeviceToDevice, e->stream));
-        long long st = step0;
-        CK(cudaMemcpyAsync(e->d_step, &st, sizeof(long long), cudaMemcpyHostToDevice, e->stream));
+        CK(cudaMemcpyAsync(e->d_step, e->d_snap_ctr, sizeof(long long), cudaMemcpyDeviceToDevice, e->stream));
+        CK(cudaMemcpyAsync(e->d_trace_count, e->d_snap_ctr + 1, sizeof(long long), cudaMemcpyDeviceToDevice,
+                           e->stream));
         CK(cudaStreamSynchronize(e->stream));
         e->host_step = step0;
         // the list must be rebuilt from the restored coordinates before the first step
         if (step0 % e->intvl != 0) {
             if ((s = build_list_checked(e))) return s;
+        }
+        if (fault) {
+            std::string who;
+            for (int k = 0; k < e->n_sys; k++)
+                if (e->faults[k]) who += (who.empty() ? "" : ", ") + std::to_string(k);
+            return fail(e, OG_ERR_SYSTEM_FAULT, "system(s) %s faulted (non-finite or far out-of-box coordinate, or a "
+                        "column beyond %d atoms); all systems are back at the call's start", who.c_str(),
+                        OG_MAX_COLUMN_ATOMS);
         }
     }
     return fail(e, OG_ERR_CAPACITY, "cell-pair list kept overflowing");
@@ -1743,4 +1772,10 @@ extern "C" og_status og_release_pool_memory(int32_t device) {
     if (r == cudaSuccess) r = cudaMemPoolTrimTo(pool, 0);
     cudaSetDevice(prev);
     return r == cudaSuccess ? OG_OK : OG_ERR_CUDA;
+}
+
+extern "C" og_status og_get_system_faults(og_engine *e, int32_t *faults) {
+    if (!e || !e->finalized || !faults) return OG_ERR_INVALID;
+    for (int k = 0; k < e->n_sys; k++) faults[k] = k < (int)e->faults.size() ? e->faults[k] : 0;
+    return OG_OK;
 }

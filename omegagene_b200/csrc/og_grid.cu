@@ -20,7 +20,8 @@ namespace og {
 __global__ void k_assign_columns(const SysDev *__restrict__ sys, const int *__restrict__ atom_sys,
                                  const double *__restrict__ crd, int n_atoms,
                                  int *__restrict__ atom_col, unsigned long long *__restrict__ atom_key,
-                                 int *__restrict__ col_count, int *__restrict__ counters) {
+                                 int *__restrict__ col_count, int *__restrict__ counters,
+                                 int *__restrict__ sys_fault) {
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= n_atoms) return;
     const SysDev &S = sys[atom_sys[a]];
@@ -39,7 +40,10 @@ __global__ void k_assign_columns(const SysDev *__restrict__ sys, const int *__re
         if (ci < 0 || ci >= nd) { bad = true; ci = 0; }
         c[d] = ci;
     }
-    if (bad) og_set_flag(counters, OG_FLAG_BAD_COORD);
+    if (bad) {
+        og_set_flag(counters, OG_FLAG_BAD_COORD);
+        atomicOr(&sys_fault[atom_sys[a]], OG_FLAG_BAD_COORD);
+    }
     int col = S.col_base + c[0] + c[1] * S.nx;
     atom_col[a] = col;
     float zf = __double2float_rn(crd[3 * a + 2]);
@@ -114,13 +118,17 @@ __global__ void k_sort_columns(const int *__restrict__ col_count, const int *__r
                                const unsigned long long *__restrict__ col_keys, const SysDev *__restrict__ sys,
                                const double *__restrict__ crd, int *__restrict__ slot_atom,
                                double *__restrict__ slot_crd, int *__restrict__ atom_slot,
-                               int *__restrict__ cell_col, int *__restrict__ cell_sys, int *__restrict__ counters) {
+                               int *__restrict__ cell_col, int *__restrict__ cell_sys, int *__restrict__ counters,
+                               int *__restrict__ sys_fault) {
     __shared__ unsigned long long keys[OG_MAX_COLUMN_ATOMS];
     const int col = blockIdx.x;
     const int n = col_count[col];
     if (n == 0) return;
     if (n > OG_MAX_COLUMN_ATOMS) {
-        if (threadIdx.x == 0) og_set_flag(counters, OG_FLAG_COLUMN_CAPACITY);
+        if (threadIdx.x == 0) {
+            og_set_flag(counters, OG_FLAG_COLUMN_CAPACITY);
+            atomicOr(&sys_fault[col_sys[col]], OG_FLAG_COLUMN_CAPACITY);
+        }
         return;
     }
     int np2 = 1;

@@ -18,7 +18,8 @@ from . import cls_io
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libomegagene_b200.so")
 
-OG_OK, OG_ERR_INVALID, OG_ERR_CUDA, OG_ERR_CAPACITY, OG_ERR_STATE, OG_ERR_NOMEM, OG_ERR_NOT_CONVERGED = range(7)
+(OG_OK, OG_ERR_INVALID, OG_ERR_CUDA, OG_ERR_CAPACITY, OG_ERR_STATE, OG_ERR_NOMEM, OG_ERR_NOT_CONVERGED,
+ OG_ERR_SYSTEM_FAULT) = range(8)
 ENERGY_NAMES = ["vdw", "ele", "bond", "angle", "potential", "kinetic", "temperature", "total", "ele_excess",
                 "ele_self", "mcmd_factor"]
 N_ENERGY = len(ENERGY_NAMES)
@@ -86,6 +87,7 @@ def load_library():
         "og_get_pair_count": [E, C.c_int32, _p(C.c_int64)],
         "og_get_tuning": [E, _p(C.c_int32), C.c_void_p], "og_set_tuning": [E, C.c_int32],
         "og_set_graphs": [E, C.c_int32], "og_release_pool_memory": [C.c_int32],
+        "og_get_system_faults": [E, C.c_void_p],
         "og_get_graph_info": [E, _p(C.c_int32), _p(C.c_int64), _p(C.c_int64), C.c_char_p],
     }
     for name, args in sig.items():
@@ -412,3 +414,10 @@ class Engine:
         self._check(self.L.og_get_graph_info(self.h, C.byref(en), C.byref(rep), C.byref(k), note), "og_get_graph_info")
         return {"enabled": bool(en.value), "replays": rep.value, "kernels_per_replay": k.value,
                 "note": note.value.decode()}
+
+    def system_faults(self):
+        """Per-system fault bits of the last og_step that returned OG_ERR_SYSTEM_FAULT
+        (4 = bad coordinate, 2 = column over capacity); all zero otherwise."""
+        f = np.zeros(len(self.n_atoms), np.int32)
+        self._check(self.L.og_get_system_faults(self.h, f.ctypes.data), "og_get_system_faults")
+        return f

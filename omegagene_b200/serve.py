@@ -13,6 +13,10 @@ A job's trajectory is therefore the one it would have had alone. The engine's fo
 fixed-point sums and its reductions are per system, so the match is exact;
 tests/test_gpu_serve.py checks it.
 
+A job whose system faults (a coordinate leaves the box or turns non-finite) is retired as failed
+with its state at the start of the window; og_step undoes the window for every job, and the
+others are stepped again in a new engine, with the results they would have had anyway.
+
 Latency of a job = completion time - arrival time (wall clock). Throughput = atom-steps of all
 jobs / (last completion - first arrival).
 """
@@ -38,6 +42,8 @@ class Job:
         self.crd = np.asarray(system["crd"], np.float64).copy()
         self.vel = np.asarray(system["vel"], np.float64).copy()
         self.steps_done = 0
+        self.failed = False
+        self.fault = 0
         self.t_admit = None
         self.t_done = None
         self.energies = None
@@ -95,7 +101,7 @@ class Server:
             raise ValueError("window must be a multiple of nsgrid_update_intvl")
         future = collections.deque(sorted(jobs, key=lambda j: j.arrival_s))
         queue = collections.deque()
-        active, done = [], []
+        active, done, failed = [], [], []
         eng = None
         t0 = self.clock()
         first_arrival = future[0].arrival_s if future else 0.0
@@ -136,14 +142,35 @@ class Server:
                         self.sleep(wait)
                 continue
             w = min(self.window, min(j.n_steps - j.steps_done for j in active))
-            eng.step(w)
+            try:
+                eng.step(w)
+            except engine.OgError as ex:
+                if ex.status != engine.OG_ERR_SYSTEM_FAULT:
+                    raise
+                bad = eng.system_faults()
+                t_re = self.clock()
+                for i, j in enumerate(active):
+                    j.crd, j.vel = eng.get_state(i)
+                eng.close()
+                eng = None
+                now = self.clock() - t0
+                for i, j in enumerate(active):
+                    if bad[i]:
+                        j.failed, j.fault, j.t_done = True, int(bad[i]), now
+                        failed.append(j)
+                active = [j for i, j in enumerate(active) if not bad[i]]
+                if active:
+                    eng = self._build(active)
+                    self.batch_sizes.append(len(active))
+                self.relayout_s += self.clock() - t_re
+                continue
             for j in active:
                 j.steps_done += w
-        t_end = max(j.t_done for j in done) if done else 0.0
-        lat = np.array([j.latency_s for j in done])
+        t_end = max(j.t_done for j in done + failed) if done or failed else 0.0
+        lat = np.array([j.latency_s for j in done]) if done else np.zeros(1)
         atom_steps = sum(j.n_atoms * j.n_steps for j in done)
         span = t_end - first_arrival
-        return {"n_jobs": len(done), "atom_steps": atom_steps, "span_s": span,
+        return {"n_jobs": len(done), "n_failed": len(failed), "failed": failed, "atom_steps": atom_steps, "span_s": span,
                 "atom_steps_per_s": atom_steps / span if span > 0 else 0.0,
                 "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
                 "relayouts": self.n_relayouts, "relayout_s": self.relayout_s,

@@ -44,3 +44,41 @@ def test_memory_budget_limits_admission():
     res = srv.run(jobs)
     assert res["n_jobs"] == 5
     assert max(srv.batch_sizes) <= 2
+
+
+def _engine(batch):
+    eng = engine.Engine(0)
+    for s, p in batch:
+        eng.add_system(s, p)
+    eng.finalize()
+    return eng
+
+
+def test_faulted_system_is_isolated():
+    """A caller-placed coordinate far outside one system's box makes og_step fail with
+    OG_ERR_SYSTEM_FAULT naming that system only; every system is back at the call's start, and
+    the others, stepped again without it, match their runs alone bit for bit."""
+    p = _params(nsgrid_update_intvl=10, time_step=2.0, thermostat="scaling", temperature=300.0)
+    sy = [systems.water_system(n, seed=60 + k) for k, n in enumerate((900, 700, 800))]
+    eng = _engine([(s, p) for s in sy])
+    start = [eng.get_state(i) for i in range(3)]
+    crd, vel = start[1]
+    crd = crd.copy()
+    crd[5, 0] += 1.0e5
+    eng.set_state(1, crd, vel)
+    with pytest.raises(engine.OgError) as ex:
+        eng.step(20)
+    assert ex.value.status == engine.OG_ERR_SYSTEM_FAULT
+    f = eng.system_faults()
+    assert f[0] == 0 and f[2] == 0 and f[1] & 4
+    for i in (0, 2):
+        c, v = eng.get_state(i)
+        assert np.array_equal(c, start[i][0]) and np.array_equal(v, start[i][1])
+    rest = _engine([(sy[0], p), (sy[2], p)])
+    rest.step(20)
+    for k, i in enumerate((0, 2)):
+        alone = _engine([(sy[i], p)])
+        alone.step(20)
+        c1, v1 = alone.get_state(0)
+        c2, v2 = rest.get_state(k)
+        assert np.array_equal(c1, c2) and np.array_equal(v1, v2)

@@ -22,9 +22,11 @@ class FakeEngine:
     of the batch on the fake clock."""
     log = []
 
-    def __init__(self, clock):
+    def __init__(self, clock, fail_at=None):
         self.clock = clock
         self.systems = []
+        self.fail_at = fail_at or {}  # system size -> coordinate value at which it faults
+        self.faults = None
 
     def set_tuning(self, v):
         pass
@@ -37,9 +39,16 @@ class FakeEngine:
         FakeEngine.log.append([(s["n"], s["first_step"]) for s in self.systems])
 
     def step(self, n):
+        bad = [int(s["n"] in self.fail_at and s["crd"][0, 0] + n > self.fail_at[s["n"]]) * 4 for s in self.systems]
+        if any(bad):  # like og_step: nothing advances, the faulted systems are named
+            self.faults = np.array(bad, np.int32)
+            raise serve.engine.OgError(serve.engine.OG_ERR_SYSTEM_FAULT, "fault")
         for s in self.systems:
             s["crd"] += n
         self.clock.t += n * 1e-3 * sum(s["n"] for s in self.systems) / 1000.0
+
+    def system_faults(self):
+        return self.faults
 
     def get_state(self, i):
         return self.systems[i]["crd"].copy(), self.systems[i]["vel"].copy()
@@ -55,10 +64,10 @@ def _system(n):
     return {"n_atoms": n, "crd": np.zeros((n, 3)), "vel": np.zeros((n, 3))}
 
 
-def _server(clock, **kw):
+def _server(clock, fail_at=None, **kw):
     FakeEngine.log = []
     return serve.Server(0, hbm_budget_bytes=kw.pop("budget", 10 ** 12), clock=clock, sleep=clock.sleep,
-                        engine_factory=lambda dev: FakeEngine(clock), **kw)
+                        engine_factory=lambda dev: FakeEngine(clock, fail_at), **kw)
 
 
 def test_every_job_runs_exactly_its_steps():
@@ -114,3 +123,17 @@ def test_bad_window_and_steps_rejected():
 def test_fifo_latencies():
     lat, span = serve.fifo_latencies([0.0, 1.0, 1.5], [2.0, 1.0, 1.0])
     assert np.allclose(lat, [2.0, 2.0, 2.5]) and span == pytest.approx(4.0)
+
+
+def test_faulted_job_retired_others_finish():
+    """A job whose system faults mid-window leaves as failed with its state at the window's
+    start; the window is redone for the others, which still run exactly their steps."""
+    clock = FakeClock()
+    p = {"nsgrid_update_intvl": 10}
+    jobs = [serve.Job(k, _system(100 * (k + 1)), p, 60) for k in range(3)]
+    res = _server(clock, fail_at={200: 30}, max_jobs=3, window=20).run(jobs)
+    assert res["n_jobs"] == 2 and res["n_failed"] == 1
+    bad = jobs[1]
+    assert bad.failed and bad.fault == 4 and bad.steps_done == 20 and np.all(bad.crd == 20)
+    for j in (jobs[0], jobs[2]):
+        assert not j.failed and np.all(j.crd == 60)
