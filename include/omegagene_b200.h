@@ -183,10 +183,13 @@ og_status og_set_timing(og_engine *e, int32_t on);
  * bit 16 = the thermostat loop hit thermo_const_max_loops (both non-fatal, as in the reference,
  * which prints a warning and continues: ConstraintShake.cpp:135-139, Thermostat.cpp:168). */
 og_status og_get_flags(og_engine *e, int32_t *flags);
-/* Autotuner result: the pair-kernel variant in use (register budget 100/80/64 per thread) and
- * the best time of each variant on the first list, in ms. */
+/* Pair-kernel variants: 0-2 = one warp per 8x8 cell pair at register budgets 100/80/64 per
+ * thread; 3-4 = j-major (each lane one j atom against the 8 i atoms) at 100/80. */
+#define OG_N_PAIR_VARIANTS 5
+/* Autotuner result: the pair-kernel variant in use and the best time of each variant on the
+ * first list, in ms (variant_ms[OG_N_PAIR_VARIANTS]). */
 og_status og_get_tuning(og_engine *e, int32_t *pair_variant, double *variant_ms);
-/* Fixes the pair-kernel variant (0/1/2) before og_finalize and skips the autotuner, e.g. when a
+/* Fixes the pair-kernel variant (0..OG_N_PAIR_VARIANTS-1) before og_finalize and skips the autotuner, e.g. when a
  * serving loop re-creates engines for new batches; -1 restores autotuning.  No counterpart in
  * the reference, which has one pair kernel. */
 og_status og_set_tuning(og_engine *e, int32_t pair_variant);
@@ -201,7 +204,9 @@ og_status og_set_tuning(og_engine *e, int32_t pair_variant);
 og_status og_set_graphs(og_engine *e, int32_t on);
 /* After og_step returned OG_ERR_SYSTEM_FAULT: per system (faults[n_systems]) the bits of what went
  * wrong in it -- 4 = a non-finite or far out-of-box coordinate (the reference has no check and
- * carries on with NaNs), 2 = more atoms in one MiniCell column than the engine sorts.  og_step
+ * carries on with NaNs), 32 = an atom moved farther in one step than the pair-list margin
+ * (nsgrid_cutoff - cutoff, at least 1 A; the reference silently misses its pairs from then on),
+ * 2 = more atoms in one MiniCell column than the engine sorts.  og_step
  * undid the whole call for every system (positions, velocities, step and trace counters are
  * those of the call's start); systems are independent, so a caller drops the faulted ones and
  * steps the rest in a new handle with the same results they would have had.  No counterpart in

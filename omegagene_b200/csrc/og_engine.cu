@@ -33,7 +33,8 @@ __global__ void k_count_pairs(const int *, int, int, const int *, const int *, c
 __global__ void k_fill_pairs(int *, int, int, long long, const int *, const int *, const SysDev *, const int *,
                              const int *, const int *, const float2 *, const int2 *, const int *, const int *,
                              const unsigned char *, const int *, const int *, const int *, const int *, const int *,
-                             int2 *, unsigned long long *, const double *, float4 *);
+                             const int *, int2 *, unsigned long long *, const double *, float4 *);
+__global__ void k_cell_excl(const int *, int, const int *, const int *, const int *, const int *, int *);
 __global__ void k_pair_heads(int *, int, int, const int *, int *);
 __global__ void k_scan_block(const int *, int *, long long, int *);
 __global__ void k_scan_add(int *, long long, const int *);
@@ -42,6 +43,10 @@ template <bool VIR, int MINB>
 __global__ void k_pair_ljzd(const int *, const int *, const SysDev *, const float4 *, const float4 *, const int *,
                             const int *, const float4 *, const int2 *, const unsigned long long *, const float2 *,
                             unsigned long long *, double *, long long);
+template <bool VIR, int MINB>
+__global__ void k_pair_ljzd_jm(const int *, const int *, const SysDev *, const float4 *, const float4 *, const int *,
+                               const int *, const float4 *, const int2 *, const unsigned long long *, const float2 *,
+                               unsigned long long *, double *, long long);
 __global__ void k_cell_bbox(const int *, int, const float4 *, const unsigned char *, float4 *);
 // og_integrate.cu
 __global__ void k_excess(int, const int2 *, const int *, const SysDev *, const double *, const double *, const int *,
@@ -83,7 +88,7 @@ __global__ void k_thermo_rescale(int, const int *, const SysDev *, const int *, 
 __global__ void k_thermo_crd(int, const int *, const SysDev *, const int *, double *, const double *,
                              const double *);
 __global__ void k_finish(int, const int *, const SysDev *, int, double *, const double *, const double *, double *,
-                         const int *, double *, const double *, float4 *, const float *, double *);
+                         const int *, double *, const double *, float4 *, const float *, double *, int *, int *);
 __global__ void k_slot_refresh(const int *, int, const int *, const double *, const double *, const float *,
                                const int *, float4 *, int *);
 __global__ void k_energies(int, const SysDev *, const double *, const double *, double *, double *, int,
@@ -194,6 +199,7 @@ struct og_engine {
         *d_thermo_it = nullptr;
     int *d_sys_fault = nullptr;           // per system: OG_FLAG_BAD_COORD / OG_FLAG_COLUMN_CAPACITY
     long long *d_snap_ctr = nullptr;      // step and trace counters at the start of og_step
+    int *d_cell_excl = nullptr;           // per cell: excluded-partner (cell, bit) row, OG_CELL_EXCL ints
     std::vector<int32_t> faults;          // per-system fault bits of the last failed call
     // CUDA graph of one list interval (a rebuild step + intvl-1 steps), replayed by og_step
     cudaStream_t side = nullptr;       // captures the thermostat loop body
@@ -222,7 +228,7 @@ struct og_engine {
     double pair_ms = 0.0, step_ms = 0.0;
     int pair_variant = 0;
     int fixed_variant = -1;  // og_set_tuning: variant chosen by the caller, -1 = autotune
-    double variant_ms[3] = {0, 0, 0};
+    double variant_ms[OG_N_PAIR_VARIANTS] = {};
     int timing = 0;  // 1: step + per-pair-kernel events (kernel by kernel); 2: step events only
     std::vector<void *> allocs;
 };
@@ -375,6 +381,10 @@ og_status setup_geometry(og_engine *e, HostSystem &h) {
     S.zcore = erfcf(c * 0.0f) / c + S.bcoeff * c2;
     S.cutoff = (double)c;
     S.cutoff2 = (float)((double)d.cutoff * (double)d.cutoff);
+    // An atom that moves farther in one step than the list margin (nsgrid_cutoff - cutoff, at
+    // least 1 A) has left every list built for it: the system has blown up.
+    const double margin = std::max(d.nsgrid_cutoff - d.cutoff, 1.0);
+    S.max_step_disp2 = margin * margin;
     return OG_OK;
 }
 
@@ -474,6 +484,10 @@ og_status build_list(og_engine *e) {
                                                                e->d_slot_crd, e->d_cell_origin, e->d_charge_f,
                                                                e->d_atom_type, e->d_xq, e->d_slot_type);
     LAUNCH_CHECK();
+    k_cell_excl<<<blocks(e->cells_cap, 256), 256, 0, st>>>(e->d_counters, e->cells_cap, e->d_slot_atom,
+                                                            e->d_atom_slot, e->d_excl_start, e->d_excl_list,
+                                                            e->d_cell_excl);
+    LAUNCH_CHECK();
     const long long n_items = (long long)e->cells_cap * e->nnc;
     k_count_pairs<<<blocks(n_items, 256), 256, 0, st>>>(e->d_counters, e->cells_cap, e->nnc, e->d_cell_sys,
                                                          e->d_sys_cell_base, e->d_sys, e->d_cell_col,
@@ -489,8 +503,8 @@ og_status build_list(og_engine *e) {
     k_fill_pairs<<<blocks(n_items, 256), 256, 0, st>>>(
         e->d_counters, e->cells_cap, e->nnc, e->pair_cap, e->d_cell_sys, e->d_sys_cell_base, e->d_sys, e->d_cell_col,
         e->d_col_cell_start, e->d_col_head_cell, e->d_cell_zr, e->d_cell_uni, e->d_uni_lo, e->d_uni_hi,
-        e->d_cell_valid, e->d_slot_atom, e->d_atom_slot, e->d_excl_start, e->d_excl_list, e->d_offset, e->d_cp_c2img,
-        e->d_cp_mask, e->d_cell_origin, e->d_cp_shift);
+        e->d_cell_valid, e->d_slot_atom, e->d_atom_slot, e->d_excl_start, e->d_excl_list, e->d_cell_excl, e->d_offset,
+        e->d_cp_c2img, e->d_cp_mask, e->d_cell_origin, e->d_cp_shift);
     LAUNCH_CHECK();
     return OG_OK;
 }
@@ -505,9 +519,13 @@ og_status build_list(og_engine *e) {
 og_status launch_pair(og_engine *e, bool vir, int variant) {
     const unsigned nb = blocks((long long)e->cells_cap * 32, 256);
     cudaStream_t st = e->stream;
-    if (vir) k_pair_ljzd<true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    // variants 0-2: warp per 8x8 cell pair (register budgets 100/80/64); 3-4: j-major (100/80)
+    if (vir && variant >= 3) k_pair_ljzd_jm<true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    else if (vir) k_pair_ljzd<true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (variant == 1) k_pair_ljzd<false, 3><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (variant == 2) k_pair_ljzd<false, 4><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    else if (variant == 3) k_pair_ljzd_jm<false, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    else if (variant == 4) k_pair_ljzd_jm<false, 3><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else k_pair_ljzd<false, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
     LAUNCH_CHECK();
     return OG_OK;
@@ -777,7 +795,8 @@ og_status run_step(og_engine *e) {
     }
     k_finish<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys, 1, e->d_crd,
                                                        e->d_crd_prev, e->d_vel, e->d_vel_next, e->d_atom_slot,
-                                                       e->d_slot_crd, e->d_cell_origin, e->d_xq, e->d_mass, e->d_ke);
+                                                       e->d_slot_crd, e->d_cell_origin, e->d_xq, e->d_mass, e->d_ke,
+                                                       e->d_counters, e->d_sys_fault);
     LAUNCH_CHECK();
     if ((s = seg_sum<1>(e, e->d_ke, 1, 0, e->d_seg_atoms, e->mc_atoms, e->d_sys_acc, OG_ACC_SIZE, OG_ACC_KIN, 0)))
         return s;
@@ -899,14 +918,14 @@ og_status autotune_pair(og_engine *e) {
     }
     const char *env = getenv("OG_PAIR_VARIANT");
     if (env && *env) {
-        e->pair_variant = atoi(env) % 3;
+        e->pair_variant = atoi(env) % OG_N_PAIR_VARIANTS;
         return OG_OK;
     }
     k_cell_bbox<<<blocks(e->cells_cap, 256), 256, 0, e->stream>>>(e->d_counters, e->cells_cap, e->d_xq,
                                                                    e->d_cell_valid, e->d_bbox);
     LAUNCH_CHECK();
     double best = 1e30;
-    for (int v = 0; v < 3; v++) {
+    for (int v = 0; v < OG_N_PAIR_VARIANTS; v++) {
         double vbest = 1e30;
         for (int rep = 0; rep < 3; rep++) {
             CK(cudaEventRecord(e->ev_pair0, e->stream));
@@ -1262,7 +1281,8 @@ og_status og_finalize(og_engine *e) {
         (s = dalloc(e, &e->d_sum_tmp, S)) || (s = upload(e, &e->d_mask_plain, mask_plain)) ||
         (s = upload(e, &e->d_mask_thermo, mask_thermo)) || (s = dalloc(e, &e->d_active, S)) ||
         (s = dalloc(e, &e->d_any, 1)) || (s = dalloc(e, &e->d_thermo_it, 1)) ||
-        (s = dalloc(e, &e->d_sys_fault, S)) || (s = dalloc(e, &e->d_snap_ctr, 2)))
+        (s = dalloc(e, &e->d_sys_fault, S)) || (s = dalloc(e, &e->d_snap_ctr, 2)) ||
+        (s = dalloc(e, &e->d_cell_excl, (size_t)OG_CELL_EXCL * cells_cap)))
         return s;
     {
         std::vector<int> sa(S + 1), se(S + 1), sb(S + 1), sg(S + 1);
@@ -1383,7 +1403,7 @@ og_status og_step(og_engine *e, int32_t n_steps) {
         int c[OG_CNT_SIZE];
         if ((s = read_counters(e, c))) return s;
         const int f = c[OG_CNT_FLAGS];
-        const bool fault = (f & (OG_FLAG_BAD_COORD | OG_FLAG_COLUMN_CAPACITY)) != 0;
+        const bool fault = (f & (OG_FLAG_BAD_COORD | OG_FLAG_COLUMN_CAPACITY | OG_FLAG_DISPLACEMENT)) != 0;
         if (!fault && !(f & OG_FLAG_PAIR_CAPACITY)) return check_flags(e);
         if (fault) {
             // A system left its box or packed a column beyond capacity.  Systems are
@@ -1411,9 +1431,9 @@ og_status og_step(og_engine *e, int32_t n_steps) {
             std::string who;
             for (int k = 0; k < e->n_sys; k++)
                 if (e->faults[k]) who += (who.empty() ? "" : ", ") + std::to_string(k);
-            return fail(e, OG_ERR_SYSTEM_FAULT, "system(s) %s faulted (non-finite or far out-of-box coordinate, or a "
-                        "column beyond %d atoms); all systems are back at the call's start", who.c_str(),
-                        OG_MAX_COLUMN_ATOMS);
+            return fail(e, OG_ERR_SYSTEM_FAULT, "system(s) %s faulted (non-finite or far out-of-box coordinate, a "
+                        "one-step displacement beyond the list margin, or a column beyond %d atoms); all systems "
+                        "are back at the call's start", who.c_str(), OG_MAX_COLUMN_ATOMS);
         }
     }
     return fail(e, OG_ERR_CAPACITY, "cell-pair list kept overflowing");
@@ -1708,7 +1728,7 @@ extern "C" og_status og_get_tuning(og_engine *e, int32_t *pair_variant, double *
     if (!e) return OG_ERR_INVALID;
     if (pair_variant) *pair_variant = e->pair_variant;
     if (variant_ms)
-        for (int v = 0; v < 3; v++) variant_ms[v] = e->variant_ms[v];
+        for (int v = 0; v < OG_N_PAIR_VARIANTS; v++) variant_ms[v] = e->variant_ms[v];
     return OG_OK;
 }
 
@@ -1735,7 +1755,8 @@ extern "C" og_status og_segment_sum(const double *d_values, int32_t stride, cons
 extern "C" og_status og_set_tuning(og_engine *e, int32_t pair_variant) {
     if (!e) return OG_ERR_INVALID;
     if (e->finalized) return fail(e, OG_ERR_STATE, "og_set_tuning after og_finalize");
-    if (pair_variant < -1 || pair_variant > 2) return fail(e, OG_ERR_INVALID, "pair variant must be -1, 0, 1 or 2");
+    if (pair_variant < -1 || pair_variant >= OG_N_PAIR_VARIANTS)
+        return fail(e, OG_ERR_INVALID, "pair variant must be -1 or 0..%d", OG_N_PAIR_VARIANTS - 1);
     e->fixed_variant = pair_variant;
     return OG_OK;
 }

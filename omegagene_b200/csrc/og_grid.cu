@@ -215,16 +215,52 @@ __device__ __forceinline__ bool valid_pair(int c1, int c2) {
 }
 
 // 64-bit mask of a cell pair: bit a2*8+a1 set = pair skipped (MiniCell.cpp:1204-1237).
+// Per cell, once per list build: the excluded partners of its atoms as (partner cell << 6 |
+// mask bit) entries, so that the mask of each of the cell's ~100 cell pairs scans one short
+// contiguous row instead of chasing atom -> partner -> slot for all 8 atoms.  row[0] = entry
+// count, or -1 when the row is full or cell indices do not fit the packing (the mask then takes
+// the direct path).
+__global__ void k_cell_excl(const int *__restrict__ counters, int cells_cap, const int *__restrict__ slot_atom,
+                            const int *__restrict__ atom_slot, const int *__restrict__ excl_start,
+                            const int *__restrict__ excl_list, int *__restrict__ cell_excl) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n_cells = counters[OG_CNT_N_CELLS];
+    if (c >= n_cells || c >= cells_cap) return;
+    int *row = cell_excl + (size_t)c * OG_CELL_EXCL;
+    int n = 0;
+    bool full = cells_cap >= (1 << 25);
+    for (int i1 = 0; i1 < OG_CELL && !full; i1++) {
+        const int a = slot_atom[c * OG_CELL + i1];
+        if (a < 0) continue;
+        for (int e = excl_start[a]; e < excl_start[a + 1]; e++) {
+            const int sl = atom_slot[excl_list[e]];
+            if (n + 1 >= OG_CELL_EXCL) { full = true; break; }
+            row[1 + n++] = ((sl >> 3) << 6) | ((sl & 7) * 8 + i1);
+        }
+    }
+    row[0] = full ? -1 : n;
+}
+
 __device__ __forceinline__ unsigned long long pair_mask(int c1, int c2, unsigned v1, unsigned v2,
                                                         const int *__restrict__ slot_atom,
                                                         const int *__restrict__ atom_slot,
                                                         const int *__restrict__ excl_start,
-                                                        const int *__restrict__ excl_list) {
+                                                        const int *__restrict__ excl_list,
+                                                        const int *__restrict__ cell_excl) {
     unsigned long long valid = 0;
     for (int i2 = 0; i2 < OG_CELL; i2++)
         if ((v2 >> i2) & 1u) valid |= (unsigned long long)v1 << (8 * i2);
     unsigned long long m = ~valid;
     if (c1 == c2) m |= 0x80c0e0f0f8fcfeffull;  // bits i1 >= i2 of every row i2
+    const int *row = cell_excl + (size_t)c1 * OG_CELL_EXCL;
+    const int n = row[0];
+    if (n >= 0) {
+        for (int k = 1; k <= n; k++) {
+            const int e = row[k];
+            if ((e >> 6) == c2) m |= 1ull << (e & 63);
+        }
+        return m;
+    }
     for (int i1 = 0; i1 < OG_CELL; i1++) {
         int a = slot_atom[c1 * OG_CELL + i1];
         if (a < 0) continue;
@@ -245,7 +281,8 @@ __device__ int enumerate_column(int c1, int nb, const SysDev &S, int cell_base,
                                 const int *__restrict__ uni_hi, const unsigned char *__restrict__ cell_valid,
                                 const int *__restrict__ slot_atom, const int *__restrict__ atom_slot,
                                 const int *__restrict__ excl_start, const int *__restrict__ excl_list,
-                                int2 *out_c2img, unsigned long long *out_mask, int out_cap) {
+                                const int *__restrict__ cell_excl, int2 *out_c2img, unsigned long long *out_mask,
+                                int out_cap) {
     const int nx = S.nx, ny = S.ny, nuz = S.n_uni_z;
     const int wy = 2 * S.n_nb[1] + 1;
     const int dcx = nb / wy - S.n_nb[0];
@@ -318,7 +355,8 @@ __device__ int enumerate_column(int c1, int nb, const SysDev &S, int cell_base,
                     if (iy == -1) img |= 4; else if (iy == 1) img |= 8;
                     if (iz == -1) img |= 16; else if (iz == 1) img |= 32;
                     out_c2img[n] = make_int2(c2, img);
-                    out_mask[n] = pair_mask(c1, c2, v1, cell_valid[c2], slot_atom, atom_slot, excl_start, excl_list);
+                    out_mask[n] = pair_mask(c1, c2, v1, cell_valid[c2], slot_atom, atom_slot, excl_start, excl_list,
+                                            cell_excl);
                 }
             }
             n++;
@@ -346,7 +384,7 @@ __global__ void k_count_pairs(const int *__restrict__ counters, int cells_cap, i
         if (nb < S.n_nb_cols)
             n = enumerate_column(c1, nb, S, sys_cell_base[s], cell_col, col_cell_start, col_head_cell, cell_zr,
                                  cell_uni, uni_lo, uni_hi, cell_valid, nullptr, nullptr, nullptr, nullptr, nullptr,
-                                 nullptr, 0);
+                                 nullptr, nullptr, 0);
     }
     count[idx] = n;
 }
@@ -359,9 +397,10 @@ __global__ void k_fill_pairs(int *__restrict__ counters, int cells_cap, int nnc,
                              const int *__restrict__ uni_lo, const int *__restrict__ uni_hi,
                              const unsigned char *__restrict__ cell_valid, const int *__restrict__ slot_atom,
                              const int *__restrict__ atom_slot, const int *__restrict__ excl_start,
-                             const int *__restrict__ excl_list, const int *__restrict__ offset,
-                             int2 *__restrict__ cp_c2img, unsigned long long *__restrict__ cp_mask,
-                             const double *__restrict__ cell_origin, float4 *__restrict__ cp_shift) {
+                             const int *__restrict__ excl_list, const int *__restrict__ cell_excl,
+                             const int *__restrict__ offset, int2 *__restrict__ cp_c2img,
+                             unsigned long long *__restrict__ cp_mask, const double *__restrict__ cell_origin,
+                             float4 *__restrict__ cp_shift) {
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int n_cells = counters[OG_CNT_N_CELLS];
     if (idx >= (long long)n_cells * nnc) return;
@@ -372,7 +411,7 @@ __global__ void k_fill_pairs(int *__restrict__ counters, int cells_cap, int nnc,
     const long long off = offset[idx];
     const int cap = (int)max(0ll, min(pair_cap - off, (long long)1 << 30));
     int n = enumerate_column(c1, nb, S, sys_cell_base[s], cell_col, col_cell_start, col_head_cell, cell_zr, cell_uni,
-                             uni_lo, uni_hi, cell_valid, slot_atom, atom_slot, excl_start, excl_list,
+                             uni_lo, uni_hi, cell_valid, slot_atom, atom_slot, excl_start, excl_list, cell_excl,
                              cp_c2img + off, cp_mask + off, cap);
     if (off + n > pair_cap) og_set_flag(counters, OG_FLAG_PAIR_CAPACITY);
     // pair-kernel record: shift from cell1's origin to cell2's image origin, formed in FP64

@@ -541,16 +541,18 @@ __global__ void k_finish(int n_atoms, const int *__restrict__ atom_sys, const Sy
                          const double *__restrict__ vel, double *__restrict__ vel_next,
                          const int *__restrict__ atom_slot, double *__restrict__ slot_crd,
                          const double *__restrict__ cell_origin, float4 *__restrict__ xq,
-                         const float *__restrict__ mass, double *__restrict__ ke) {
+                         const float *__restrict__ mass, double *__restrict__ ke, int *__restrict__ counters,
+                         int *__restrict__ sys_fault) {
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= n_atoms) return;
     const SysDev &S = sys[atom_sys[a]];
     const int sl = atom_slot[a], c = sl >> 3;
-    double vn = 0.0;
+    double vn = 0.0, disp2 = 0.0;
     float r[3];
     for (int q = 0; q < 3; q++) {
         const int k = 3 * a + q;
         const double x = crd[k], xp = crd_prev[k];
+        disp2 += (x - xp) * (x - xp);
         if (vel_from_crd && S.has_constraints && S.thermostat != 1) vel_next[k] = (x - xp) * (1.0 / S.dt);
         const double gcrd = slot_crd[3 * (size_t)sl + q] + (x - xp);
         slot_crd[3 * (size_t)sl + q] = gcrd;
@@ -568,6 +570,10 @@ __global__ void k_finish(int n_atoms, const int *__restrict__ atom_sys, const Sy
     p.z = r[2];
     xq[sl] = p;
     ke[a] = vn * (double)mass[a];
+    if (!(disp2 <= S.max_step_disp2)) {  // also catches NaN
+        og_set_flag(counters, OG_FLAG_DISPLACEMENT);
+        atomicOr(&sys_fault[atom_sys[a]], OG_FLAG_DISPLACEMENT);
+    }
 }
 
 // Slot coordinates/charges/types after a list rebuild (cuda_setup.cu:364-402 roles).

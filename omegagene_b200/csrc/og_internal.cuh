@@ -16,6 +16,7 @@
 
 #define OG_CELL 8
 #define OG_MAX_COLUMN_ATOMS 4096     // per-column sort capacity (shared memory)
+#define OG_CELL_EXCL 32              // per-cell exclusion row: count + up to 31 (cell, bit) entries
 #define OG_FIX_SCALE 4294967296.0    // 2^32: work (kcal/mol/A) -> int64 fixed point
 #define OG_FIX_INV (1.0 / 4294967296.0)
 #define OG_CHARGE_COEFF 332.06378    // CelesteObject.cpp:35
@@ -30,6 +31,7 @@
 #define OG_FLAG_BAD_COORD 4
 #define OG_FLAG_SHAKE 8
 #define OG_FLAG_THERMO 16
+#define OG_FLAG_DISPLACEMENT 32      // an atom moved farther in one step than the list margin allows
 
 // d_counters slots
 #define OG_CNT_N_CELLS 0
@@ -56,6 +58,7 @@ struct SysDev {
     float cutoff2;               // interaction cutoff^2
     float zcore, bcoeff, fcoeff; // zero-dipole alpha=0 (ZeroMultipoleSum.cpp:150-202), float
     double cutoff;
+    double max_step_disp2;       // squared displacement per step beyond which a system is faulted
     int lj_base, n_types;
     // integrator
     double dt;

@@ -254,6 +254,187 @@ k_pair_ljzd(const int *__restrict__ counters, const int *__restrict__ cell_sys, 
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// j-major variant: one warp per cell1, four cell pairs at a time (8-lane group q = lane>>3 per
+// cell pair, lane jj = lane&7 holds j atom jj of that cell2) and every lane evaluates all 8 i
+// atoms against its j.  Per cell pair a lane then does 8 evaluations for one record fetch, one
+// j load and one fixed-point add per component (the warp-per-8x8 layout above does 2 and needs
+// a 4-lane shuffle reduction of the j work).  The i work stays in 24 FP32 registers per lane
+// over that lane's cell pairs (about a quarter of cell1's list) and is reduced across the warp
+// in FP64 at the end, in a fixed order.  i atoms are read from shared memory (broadcast).
+template <bool VIR, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+k_pair_ljzd_jm(const int *__restrict__ counters, const int *__restrict__ cell_sys, const SysDev *__restrict__ sys,
+               const float4 *__restrict__ bbox, const float4 *__restrict__ xq, const int *__restrict__ slot_type,
+               const int *__restrict__ cp_head, const float4 *__restrict__ cp_shift, const int2 *__restrict__ cp_c2img,
+               const unsigned long long *__restrict__ cp_mask, const float2 *__restrict__ lj,
+               unsigned long long *__restrict__ frc, double *__restrict__ cell_acc, long long pair_cap) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int wib = (threadIdx.x >> 5) & 7;
+    const int n_cells = counters[OG_CNT_N_CELLS];
+    if (warp >= n_cells) return;
+    const int c1 = warp;
+    const int jj = lane & 7, q = lane >> 3;
+    const SysDev &S = sys[cell_sys[c1]];
+    __shared__ float4 s_xi[8][OG_CELL];  // (x, y, z, q * 332.06378) of cell1's atoms, per warp
+    __shared__ int s_ti[8][OG_CELL];     // LJ table row of each cell1 atom
+    if (lane < OG_CELL) {
+        float4 x = xq[c1 * OG_CELL + lane];
+        x.w *= (float)OG_CHARGE_COEFF;
+        s_xi[wib][lane] = x;
+        s_ti[wib][lane] = slot_type[c1 * OG_CELL + lane] * S.n_types + S.lj_base;
+    }
+    __syncwarp();
+    const float rc2 = S.cutoff2, zcore = S.zcore, bco = S.bcoeff, fco = S.fcoeff;
+    const float rskip = sqrtf(rc2) + 1e-3f, rskip2 = rskip * rskip;
+    const float4 b1l = bbox[2 * c1], b1h = bbox[2 * c1 + 1];
+    float fi[OG_CELL][3];
+#pragma unroll
+    for (int i = 0; i < OG_CELL; i++) fi[i][0] = fi[i][1] = fi[i][2] = 0.f;
+    float av = 0.f, ae = 0.f;
+    int n_act = 0;
+    double v[9];
+    if (VIR)
+        for (int k = 0; k < 9; k++) v[k] = 0;
+    const int k_beg = cp_head[c1];
+    const int k_end = (int)min((long long)cp_head[c1 + 1], pair_cap);
+    for (int chunk = k_beg; chunk < k_end; chunk += 32) {
+        // one record per lane, bounding-box test, then the survivors four at a time
+        const int kk = chunk + lane;
+        float4 my_sp = make_float4(0.f, 0.f, 0.f, 0.f);
+        unsigned long long my_m = ~0ull;
+        int my_img = 0;
+        bool keep = false;
+        if (kk < k_end) {
+            my_sp = cp_shift[kk];
+            const int c2 = __float_as_int(my_sp.w);
+            const float4 l2 = bbox[2 * c2], h2 = bbox[2 * c2 + 1];
+            const float gx = fmaxf(0.f, fmaxf(l2.x + my_sp.x - b1h.x, b1l.x - (h2.x + my_sp.x)));
+            const float gy = fmaxf(0.f, fmaxf(l2.y + my_sp.y - b1h.y, b1l.y - (h2.y + my_sp.y)));
+            const float gz = fmaxf(0.f, fmaxf(l2.z + my_sp.z - b1h.z, b1l.z - (h2.z + my_sp.z)));
+            keep = gx * gx + gy * gy + gz * gz < rskip2;
+            if (keep) my_m = cp_mask[kk];
+            if (VIR && keep) my_img = cp_c2img[kk].y;
+        }
+        const unsigned ballot = __ballot_sync(0xffffffffu, keep);
+        const int n_keep = __popc(ballot);
+        for (int r = 0; r < n_keep; r += 4) {
+            const int idx = r + q;
+            const bool active = idx < n_keep;
+            const int src = active ? (int)__fns(ballot, 0, idx + 1) : 0;
+            float4 sp;
+            sp.x = __shfl_sync(0xffffffffu, my_sp.x, src);
+            sp.y = __shfl_sync(0xffffffffu, my_sp.y, src);
+            sp.z = __shfl_sync(0xffffffffu, my_sp.z, src);
+            sp.w = __shfl_sync(0xffffffffu, my_sp.w, src);
+            const unsigned long long m = __shfl_sync(0xffffffffu, my_m, src);
+            const int img = VIR ? __shfl_sync(0xffffffffu, my_img, src) : 0;
+            const int c2 = __float_as_int(sp.w);
+            float4 xj = make_float4(0.f, 0.f, 0.f, 0.f);
+            int tj = 0;
+            if (active) {
+                xj = xq[c2 * OG_CELL + jj];
+                tj = slot_type[c2 * OG_CELL + jj];
+            }
+            // bits jj*8 + i of the mask: excluded pairs and dummy slots of this j
+            const unsigned skip = active ? (unsigned)(m >> (jj * OG_CELL)) & 0xffu : 0xffu;
+            const float rjx = xj.x + sp.x, rjy = xj.y + sp.y, rjz = xj.z + sp.z;
+            float wjx = 0.f, wjy = 0.f, wjz = 0.f;
+#pragma unroll
+            for (int i = 0; i < OG_CELL; i++) {
+                const float4 xi = s_xi[wib][i];
+                const float dx = xi.x - rjx, dy = xi.y - rjy, dz = xi.z - rjz;
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                const bool act = ((skip >> i) & 1u) == 0u && r2 < rc2;
+                const float r2s = act ? r2 : 1.0f;
+                float rinv = rsqrtf(r2s);
+                const float hres = fmaf(-r2s * rinv, rinv, 1.0f);
+                rinv = fmaf(0.5f * rinv, hres, rinv);
+                const float r2inv = rinv * rinv;
+                const float r6inv = r2inv * r2inv * r2inv;
+                const float2 p = __ldg(&lj[s_ti[wib][i] + tj]);
+                const float t6 = p.x * r6inv, t12 = p.y * r6inv * r6inv;
+                const float cc = xi.w * xj.w;
+                float pv = t12 - t6;
+                float pe = cc * (rinv - zcore + bco * r2s);
+                float wc = r2inv * (6.0f * t6 - 12.0f * t12) - cc * (rinv * r2inv - fco);
+                if (!act) { pv = 0.f; pe = 0.f; wc = 0.f; }
+                if (VIR) n_act += act ? 1 : 0;
+                const float wx = wc * dx, wy = wc * dy, wz = wc * dz;
+                av += pv;
+                ae += pe;
+                fi[i][0] += wx;
+                fi[i][1] += wy;
+                fi[i][2] += wz;
+                wjx -= wx;
+                wjy -= wy;
+                wjz -= wz;
+            }
+            if (active && (wjx != 0.f || wjy != 0.f || wjz != 0.f)) {
+                unsigned long long *fj = frc + 3 * (size_t)(c2 * OG_CELL + jj);
+                atomicAdd(fj + 0, (unsigned long long)__float2ll_rn(wjx * (float)OG_FIX_SCALE));
+                atomicAdd(fj + 1, (unsigned long long)__float2ll_rn(wjy * (float)OG_FIX_SCALE));
+                atomicAdd(fj + 2, (unsigned long long)__float2ll_rn(wjz * (float)OG_FIX_SCALE));
+                if (VIR && img != 0) {
+                    const double sh[3] = {(img & 1) ? -S.L[0] : ((img & 2) ? S.L[0] : 0.0),
+                                          (img & 4) ? -S.L[1] : ((img & 8) ? S.L[1] : 0.0),
+                                          (img & 16) ? -S.L[2] : ((img & 32) ? S.L[2] : 0.0)};
+                    const double fjv[3] = {-(double)wjx, -(double)wjy, -(double)wjz};
+                    for (int a = 0; a < 3; a++)
+                        for (int b = 0; b < 3; b++) v[a * 3 + b] += sh[a] * fjv[b];
+                }
+            }
+        }
+    }
+    // i work: FP64 butterfly over the 32 lanes (fixed order), then one fixed-point add per
+    // component of each of the 8 atoms
+    double mine[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int i = 0; i < OG_CELL; i++) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            double x = (double)fi[i][d];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+            if (lane == i) mine[d] = x;
+        }
+    }
+    if (lane < OG_CELL && (mine[0] != 0.0 || mine[1] != 0.0 || mine[2] != 0.0)) {
+        unsigned long long *fa = frc + 3 * (size_t)(c1 * OG_CELL + lane);
+        atomicAdd(fa + 0, (unsigned long long)og_to_fix(mine[0]));
+        atomicAdd(fa + 1, (unsigned long long)og_to_fix(mine[1]));
+        atomicAdd(fa + 2, (unsigned long long)og_to_fix(mine[2]));
+    }
+    double e_vdw = (double)av, e_ele = (double)ae;
+    for (int o = 16; o > 0; o >>= 1) {
+        e_vdw += __shfl_xor_sync(0xffffffffu, e_vdw, o);
+        e_ele += __shfl_xor_sync(0xffffffffu, e_ele, o);
+    }
+    if (VIR) {
+        for (int k = 0; k < 9; k++)
+            for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+        for (int o = 16; o > 0; o >>= 1) n_act += __shfl_xor_sync(0xffffffffu, n_act, o);
+    }
+    if (lane == 0) {
+        double *acc = cell_acc + (size_t)c1 * OG_CELL_ACC;
+        acc[0] = e_vdw;
+        acc[1] = e_ele;
+        if (VIR) {
+            for (int k = 0; k < 9; k++) acc[2 + k] = v[k];
+            acc[11] = (double)n_act;
+        }
+    }
+}
+
+#define OG_PAIR_ARGS_DECL                                                                                   \
+    const int *, const int *, const SysDev *, const float4 *, const float4 *, const int *, const int *,      \
+        const float4 *, const int2 *, const unsigned long long *, const float2 *, unsigned long long *, double *, \
+        long long
+template __global__ void k_pair_ljzd_jm<true, 2>(OG_PAIR_ARGS_DECL);
+template __global__ void k_pair_ljzd_jm<false, 2>(OG_PAIR_ARGS_DECL);
+template __global__ void k_pair_ljzd_jm<false, 3>(OG_PAIR_ARGS_DECL);
+
 template __global__ void k_pair_ljzd<true, 2>(const int *, const int *, const SysDev *, const float4 *,
                                                 const float4 *, const int *, const int *, const float4 *,
                                                 const int2 *, const unsigned long long *, const float2 *,

@@ -23,6 +23,7 @@ LIB_PATH = os.path.join(HERE, "libomegagene_b200.so")
 ENERGY_NAMES = ["vdw", "ele", "bond", "angle", "potential", "kinetic", "temperature", "total", "ele_excess",
                 "ele_self", "mcmd_factor"]
 N_ENERGY = len(ENERGY_NAMES)
+N_PAIR_VARIANTS = 5  # OG_N_PAIR_VARIANTS
 
 
 class OgError(RuntimeError):
@@ -397,12 +398,12 @@ class Engine:
 
     def tuning(self):
         v = C.c_int32()
-        ms = np.zeros(3)
+        ms = np.zeros(N_PAIR_VARIANTS)
         self._check(self.L.og_get_tuning(self.h, C.byref(v), ms.ctypes.data), "og_get_tuning")
         return {"pair_variant": v.value, "variant_ms": ms.tolist()}
 
     def set_tuning(self, variant):
-        """Fixes the pair-kernel variant (0/1/2) before finalize(); -1 = autotune."""
+        """Fixes the pair-kernel variant (0..4) before finalize(); -1 = autotune."""
         self._check(self.L.og_set_tuning(self.h, int(variant)), "og_set_tuning")
 
     def set_graphs(self, on=True):
@@ -417,7 +418,8 @@ class Engine:
 
     def system_faults(self):
         """Per-system fault bits of the last og_step that returned OG_ERR_SYSTEM_FAULT
-        (4 = bad coordinate, 2 = column over capacity); all zero otherwise."""
+        (4 = bad coordinate, 32 = one-step displacement beyond the list margin, 2 = column over
+        capacity); all zero otherwise."""
         f = np.zeros(len(self.n_atoms), np.int32)
         self._check(self.L.og_get_system_faults(self.h, f.ctypes.data), "og_get_system_faults")
         return f

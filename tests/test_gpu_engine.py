@@ -32,8 +32,10 @@ def _oracle_cells(s, p):
     return ogo.CellList(pbc, geom, crd, nb)
 
 
-def _engine(systems_and_params):
+def _engine(systems_and_params, variant=None):
     eng = engine.Engine(0)
+    if variant is not None:
+        eng.set_tuning(variant)
     for s, p, m in systems_and_params:
         eng.add_system(s, p, m)
     eng.finalize()
@@ -82,11 +84,13 @@ def test_batched_cell_lists_equal_single():
             np.testing.assert_array_equal(cp[k], getattr(ref, k), err_msg="%d %s" % (i, k))
 
 
+@pytest.mark.parametrize("variant", [0, 3])
 @pytest.mark.parametrize("name,make", SMALL, ids=[n for n, _ in SMALL])
-def test_forces_energies_virial_vs_fp64(name, make):
+def test_forces_energies_virial_vs_fp64(name, make, variant):
+    """Both pair-kernel families (variant 0: warp per 8x8 cell pair, 3: j-major)."""
     s = make()
     p = _params()
-    eng = _engine([(s, p, None)])
+    eng = _engine([(s, p, None)], variant)
     eng.compute_forces()
     work, ene, vir = eng.get_forces(0)
     md = ogo.OracleMD(s, p)
@@ -110,8 +114,8 @@ def test_forces_bitwise_reproducible():
     assert e1 == e2
 
 
-def _run_both(s, p, n_steps, mcmd=None):
-    eng = _engine([(s, p, mcmd)])
+def _run_both(s, p, n_steps, mcmd=None, variant=None):
+    eng = _engine([(s, p, mcmd)], variant)
     eng.set_trace(n_steps)
     md = ogo.OracleMD(s, p, mcmd)
     ref = [md.step() for _ in range(n_steps)]
@@ -120,10 +124,12 @@ def _run_both(s, p, n_steps, mcmd=None):
     return eng, md, ref, tr
 
 
-def test_one_step_state_matches_oracle():
+@pytest.mark.parametrize("variant", range(engine.N_PAIR_VARIANTS))
+def test_one_step_state_matches_oracle(variant):
+    """Every pair-kernel variant: positions and velocities after one step."""
     s = systems.water_system(1500, seed=5)
     p = _params(nsgrid_update_intvl=10, time_step=2.0)
-    eng, md, ref, tr = _run_both(s, p, 1)
+    eng, md, ref, tr = _run_both(s, p, 1, variant=variant)
     crd, vel = eng.get_state(0)
     assert np.max(np.abs(crd.reshape(-1) - md.crd)) < 1e-6
     assert np.max(np.abs(vel.reshape(-1) - md.vel_next)) < 1e-6
