@@ -47,6 +47,10 @@ template <bool VIR, int MINB>
 __global__ void k_pair_ljzd_jm(const int *, const int *, const SysDev *, const float4 *, const float4 *, const int *,
                                const int *, const float4 *, const int2 *, const unsigned long long *, const float2 *,
                                unsigned long long *, double *, long long);
+template <bool VIR, int MINB>
+__global__ void k_pair_ljzd_jm2(const int *, const int *, const SysDev *, const float4 *, const float4 *, const int *,
+                                const int *, const float4 *, const int2 *, const unsigned long long *, const float2 *,
+                                unsigned long long *, double *, long long);
 __global__ void k_cell_bbox(const int *, int, const float4 *, const unsigned char *, float4 *);
 // og_integrate.cu
 __global__ void k_excess(int, const int2 *, const int *, const SysDev *, const double *, const double *, const int *,
@@ -56,7 +60,7 @@ __global__ void k_bonds(int, const int2 *, const double2 *, const int *, const S
 __global__ void k_angles(int, const int4 *, const double2 *, const SysDev *, const double *, const int *,
                          unsigned long long *, double *);
 __global__ void k_atom_virial(int, const int *, const unsigned long long *, const float4 *, const double *, double *);
-__global__ void k_collect(int, const int *, unsigned long long *, double *);
+__global__ void k_collect_slots(const int *, int, const int *, unsigned long long *, double *);
 template <int NV>
 __global__ void k_part(const double *, int, int, const int *, int, double *);
 __global__ void k_part_momentum(const int *, const int *, const float *, const double *, const int *, const int *,
@@ -519,13 +523,17 @@ og_status build_list(og_engine *e) {
 og_status launch_pair(og_engine *e, bool vir, int variant) {
     const unsigned nb = blocks((long long)e->cells_cap * 32, 256);
     cudaStream_t st = e->stream;
-    // variants 0-2: warp per 8x8 cell pair (register budgets 100/80/64); 3-4: j-major (100/80)
-    if (vir && variant >= 3) k_pair_ljzd_jm<true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    // variants 0-2: warp per 8x8 cell pair (register budgets 100/80/64); 3-4: j-major (100/80);
+    // 5-6: j-major with packed FP32x2 arithmetic (128/80)
+    if (vir && variant >= 5) k_pair_ljzd_jm2<true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    else if (vir && variant >= 3) k_pair_ljzd_jm<true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (vir) k_pair_ljzd<true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (variant == 1) k_pair_ljzd<false, 3><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (variant == 2) k_pair_ljzd<false, 4><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (variant == 3) k_pair_ljzd_jm<false, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (variant == 4) k_pair_ljzd_jm<false, 3><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    else if (variant == 5) k_pair_ljzd_jm2<false, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    else if (variant == 6) k_pair_ljzd_jm2<false, 3><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else k_pair_ljzd<false, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
     LAUNCH_CHECK();
     return OG_OK;
@@ -582,7 +590,8 @@ og_status compute_forces(og_engine *e, bool vir) {
                                                             e->d_crd, e->d_atom_slot, e->d_frc, e->d_e_angle);
         LAUNCH_CHECK();
     }
-    k_collect<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_slot, e->d_frc, e->d_work);
+    k_collect_slots<<<blocks(e->slots_cap, 256), 256, 0, st>>>(e->d_counters, e->slots_cap, e->d_slot_atom, e->d_frc,
+                                                                e->d_work);
     LAUNCH_CHECK();
     og_status rs = reduce_potential(e);
     if (rs) return rs;

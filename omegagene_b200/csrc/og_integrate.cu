@@ -120,16 +120,23 @@ __global__ void k_atom_virial(int n_atoms, const int *__restrict__ atom_slot,
         for (int j = 0; j < 3; j++) vir_out[9 * (size_t)a + i * 3 + j] = x[i] * F[j];
 }
 
-// Fixed-point accumulators -> FP64 work in atom order; clears the accumulators.
-__global__ void k_collect(int n_atoms, const int *__restrict__ atom_slot, unsigned long long *__restrict__ frc,
-                          double *__restrict__ work) {
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= n_atoms) return;
-    unsigned long long *f = frc + 3 * (size_t)atom_slot[a];
-    for (int q = 0; q < 3; q++) {
-        work[3 * a + q] = (double)(long long)f[q] * OG_FIX_INV;
-        f[q] = 0ull;
-    }
+// Fixed-point accumulators -> FP64 work in atom order, clearing the accumulators.  One thread
+// per slot: it reads its slot's three sums and clears them (coalesced), and writes the atom's
+// work in original order (one 24-byte scatter).
+__global__ void k_collect_slots(const int *__restrict__ counters, int slots_cap, const int *__restrict__ slot_atom,
+                                unsigned long long *__restrict__ frc, double *__restrict__ work) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= slots_cap || s >= counters[OG_CNT_N_CELLS] * OG_CELL) return;
+    const int a = slot_atom[s];
+    unsigned long long *f = frc + 3 * (size_t)s;
+    const long long f0 = (long long)f[0], f1 = (long long)f[1], f2 = (long long)f[2];
+    f[0] = 0ull;
+    f[1] = 0ull;
+    f[2] = 0ull;
+    if (a < 0) return;
+    work[3 * (size_t)a + 0] = (double)f0 * OG_FIX_INV;
+    work[3 * (size_t)a + 1] = (double)f1 * OG_FIX_INV;
+    work[3 * (size_t)a + 2] = (double)f2 * OG_FIX_INV;
 }
 
 // ------------------------------------------------------------- reductions

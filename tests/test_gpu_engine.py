@@ -84,10 +84,11 @@ def test_batched_cell_lists_equal_single():
             np.testing.assert_array_equal(cp[k], getattr(ref, k), err_msg="%d %s" % (i, k))
 
 
-@pytest.mark.parametrize("variant", [0, 3])
+@pytest.mark.parametrize("variant", [0, 3, 5])
 @pytest.mark.parametrize("name,make", SMALL, ids=[n for n, _ in SMALL])
 def test_forces_energies_virial_vs_fp64(name, make, variant):
-    """Both pair-kernel families (variant 0: warp per 8x8 cell pair, 3: j-major)."""
+    """The three pair-kernel families (0: warp per 8x8 cell pair, 3: j-major, 5: j-major with
+    packed FP32x2 arithmetic)."""
     s = make()
     p = _params()
     eng = _engine([(s, p, None)], variant)
