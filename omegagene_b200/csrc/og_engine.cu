@@ -47,7 +47,7 @@ template <bool VIR, int MINB>
 __global__ void k_pair_ljzd_jm(const int *, const int *, const SysDev *, const float4 *, const float4 *, const int *,
                                const int *, const float4 *, const int2 *, const unsigned long long *, const float2 *,
                                unsigned long long *, double *, long long);
-template <bool VIR, int MINB>
+template <bool VIR, bool ENE, int MINB>
 __global__ void k_pair_ljzd_jm2(const int *, const int *, const SysDev *, const float4 *, const float4 *, const int *,
                                 const int *, const float4 *, const int2 *, const unsigned long long *, const float2 *,
                                 unsigned long long *, double *, long long);
@@ -146,7 +146,7 @@ struct og_engine {
     int shake_max_loops = 1000, thermo_max_loops = 100;
     double shake_tol = 1e-7, thermo_tol = 1e-5;
     bool any_groups = false, any_thermo_free = false, any_thermo_cons = false, any_plain_cons = false;
-    bool any_bonds = false, any_angles = false;
+    bool any_bonds = false, any_angles = false, any_mcmd = false;
     long long host_step = 0;
     // device buffers
     SysDev *d_sys = nullptr;
@@ -520,20 +520,24 @@ og_status build_list(og_engine *e) {
         e->d_cp_c2img, e->d_cp_mask, e->d_lj, e->d_frc, e->d_cell_acc, e->pair_cap
 
 // Pair kernel variants differ in the register budget per thread (resident blocks per SM).
-og_status launch_pair(og_engine *e, bool vir, int variant) {
+// ene = false: the caller does not read this step's energies (only variants 5-6 skip them).
+og_status launch_pair(og_engine *e, bool vir, int variant, bool ene) {
     const unsigned nb = blocks((long long)e->cells_cap * 32, 256);
     cudaStream_t st = e->stream;
     // variants 0-2: warp per 8x8 cell pair (register budgets 100/80/64); 3-4: j-major (100/80);
-    // 5-6: j-major with packed FP32x2 arithmetic (128/80)
-    if (vir && variant >= 5) k_pair_ljzd_jm2<true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    // 5-6: j-major with packed FP32x2 arithmetic (128/80).  The virial kernel is that of the
+    // variant's family.
+    if (vir && variant >= 5) k_pair_ljzd_jm2<true, true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (vir && variant >= 3) k_pair_ljzd_jm<true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (vir) k_pair_ljzd<true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (variant == 1) k_pair_ljzd<false, 3><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (variant == 2) k_pair_ljzd<false, 4><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (variant == 3) k_pair_ljzd_jm<false, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (variant == 4) k_pair_ljzd_jm<false, 3><<<nb, 256, 0, st>>>(PAIR_ARGS);
-    else if (variant == 5) k_pair_ljzd_jm2<false, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
-    else if (variant == 6) k_pair_ljzd_jm2<false, 3><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    else if (variant == 5 && ene) k_pair_ljzd_jm2<false, true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    else if (variant == 5) k_pair_ljzd_jm2<false, false, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    else if (variant == 6 && ene) k_pair_ljzd_jm2<false, true, 3><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    else if (variant == 6) k_pair_ljzd_jm2<false, false, 3><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else k_pair_ljzd<false, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
     LAUNCH_CHECK();
     return OG_OK;
@@ -542,7 +546,8 @@ og_status launch_pair(og_engine *e, bool vir, int variant) {
 og_status reduce_potential(og_engine *e);
 og_status reduce_virial(og_engine *e);
 
-og_status compute_forces(og_engine *e, bool vir) {
+// ene = false: this step's energies are not read (see run_step); forces are the same.
+og_status compute_forces(og_engine *e, bool vir, bool ene = true) {
     cudaStream_t st = e->stream;
     const unsigned pair_blocks = blocks((long long)e->cells_cap * 32, 256);
     k_cell_bbox<<<blocks(e->cells_cap, 256), 256, 0, st>>>(e->d_counters, e->cells_cap, e->d_xq, e->d_cell_valid,
@@ -559,7 +564,7 @@ og_status compute_forces(og_engine *e, bool vir) {
         CK(cudaEventRecord(e->pev0[e->pev_used], st));
     }
     {
-        og_status ps = launch_pair(e, vir, vir ? 0 : e->pair_variant);
+        og_status ps = launch_pair(e, vir, e->pair_variant, ene || vir);
         if (ps) return ps;
     }
     if (e->timing == 1) CK(cudaEventRecord(e->pev1[e->pev_used++], st));
@@ -593,8 +598,8 @@ og_status compute_forces(og_engine *e, bool vir) {
     k_collect_slots<<<blocks(e->slots_cap, 256), 256, 0, st>>>(e->d_counters, e->slots_cap, e->d_slot_atom, e->d_frc,
                                                                 e->d_work);
     LAUNCH_CHECK();
-    og_status rs = reduce_potential(e);
-    if (rs) return rs;
+    og_status rs = OG_OK;
+    if ((ene || vir) && (rs = reduce_potential(e))) return rs;
     if (vir && (rs = reduce_virial(e))) return rs;
     return OG_OK;
 }
@@ -765,14 +770,17 @@ og_status thermostat_with_shake(og_engine *e) {
     return OG_OK;
 }
 
-og_status run_step(og_engine *e) {
+// ene: evaluate this step's energies.  They are needed on every step when a system is
+// McMD-scaled (the factor depends on the potential) or the energy trace is on, and otherwise
+// only on the last step of a call, whose energies og_get_energies reads.
+og_status run_step(og_engine *e, bool ene) {
     cudaStream_t st = e->stream;
     og_status s;
     if (e->host_step % e->intvl == 0) {
         s = build_list(e);
         if (s) return s;
     }
-    s = compute_forces(e, false);
+    s = compute_forces(e, false, ene || e->any_mcmd || e->trace_cap > 0);
     if (s) return s;
     k_update_velocities<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys, e->d_mcmd,
                                                                   e->d_work, e->d_mass_inv, e->d_vel,
@@ -872,7 +880,7 @@ og_status capture_interval(og_engine *e) {
     CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeRelaxed));
     e->capturing = true;
     og_status s = OG_OK;
-    for (int i = 0; i < e->intvl && s == OG_OK; i++) s = run_step(e);
+    for (int i = 0; i < e->intvl && s == OG_OK; i++) s = run_step(e, i == e->intvl - 1);
     e->capturing = false;
     cudaGraph_t g = nullptr;
     cudaError_t r = cudaStreamEndCapture(e->stream, &g);
@@ -938,7 +946,7 @@ og_status autotune_pair(og_engine *e) {
         double vbest = 1e30;
         for (int rep = 0; rep < 3; rep++) {
             CK(cudaEventRecord(e->ev_pair0, e->stream));
-            og_status s = launch_pair(e, false, v);
+            og_status s = launch_pair(e, false, v, false);
             if (s) return s;
             CK(cudaEventRecord(e->ev_pair1, e->stream));
             CK(cudaEventSynchronize(e->ev_pair1));
@@ -1129,6 +1137,7 @@ og_status og_finalize(og_engine *e) {
         if (d.time_step < tau) tau = d.time_step;
         D.tau_inv = 1.0 / tau;
         D.mcmd_order = d.mcmd_order;
+        e->any_mcmd |= d.mcmd_order >= 0;
         D.mcmd_lo = d.mcmd_lambda_low;
         D.mcmd_hi = d.mcmd_lambda_high;
         D.mcmd_k = (OG_GAS_CONST / OG_JOULE_CAL) * 1e-3 * d.mcmd_temperature;
@@ -1394,7 +1403,7 @@ og_status og_step(og_engine *e, int32_t n_steps) {
                     continue;
                 }
             }
-            if ((s = run_step(e))) return s;
+            if ((s = run_step(e, i == n_steps - 1))) return s;
             i++;
         }
         if (e->timing) {
@@ -1718,7 +1727,7 @@ extern "C" og_status og_step_async(og_engine *e, int32_t n_steps) {
     // checks og_get_flags at its own sync points
     if (!e || !e->finalized) return fail(e, OG_ERR_STATE, "og_step_async before og_finalize");
     for (int i = 0; i < n_steps; i++) {
-        og_status s = run_step(e);
+        og_status s = run_step(e, i == n_steps - 1);
         if (s) return s;
     }
     return OG_OK;

@@ -45,6 +45,7 @@ __global__ void k_cell_bbox(const int *__restrict__ counters, int cells_cap, con
 }
 
 #define OG_FLUSH 16
+#define OG_FOLD 1  // j-major kernels: rounds (a lane's 8 pairs of one cell pair) per FP64 fold of energies
 
 // MINB = minimum resident blocks per SM the register allocation must allow (2: ~100 registers,
 // 3: 80, 4: 64 with a few spills); the engine's autotuner times the variants on the first list.
@@ -292,7 +293,9 @@ k_pair_ljzd_jm(const int *__restrict__ counters, const int *__restrict__ cell_sy
     float fi[OG_CELL][3];
 #pragma unroll
     for (int i = 0; i < OG_CELL; i++) fi[i][0] = fi[i][1] = fi[i][2] = 0.f;
-    float av = 0.f, ae = 0.f;
+    float av = 0.f, ae = 0.f;     // FP32 energy partials of up to OG_FOLD rounds ...
+    double dv = 0.0, de = 0.0;    // ... folded into FP64
+    int n_round = 0;
     int n_act = 0;
     double v[9];
     if (VIR)
@@ -371,6 +374,12 @@ k_pair_ljzd_jm(const int *__restrict__ counters, const int *__restrict__ cell_sy
                 wjy -= wy;
                 wjz -= wz;
             }
+            if (++n_round == OG_FOLD) {
+                dv += (double)av;
+                de += (double)ae;
+                av = ae = 0.f;
+                n_round = 0;
+            }
             if (active && (wjx != 0.f || wjy != 0.f || wjz != 0.f)) {
                 unsigned long long *fj = frc + 3 * (size_t)(c2 * OG_CELL + jj);
                 atomicAdd(fj + 0, (unsigned long long)__float2ll_rn(wjx * (float)OG_FIX_SCALE));
@@ -406,7 +415,7 @@ k_pair_ljzd_jm(const int *__restrict__ counters, const int *__restrict__ cell_sy
         atomicAdd(fa + 1, (unsigned long long)og_to_fix(mine[1]));
         atomicAdd(fa + 2, (unsigned long long)og_to_fix(mine[2]));
     }
-    double e_vdw = (double)av, e_ele = (double)ae;
+    double e_vdw = dv + (double)av, e_ele = de + (double)ae;
     for (int o = 16; o > 0; o >>= 1) {
         e_vdw += __shfl_xor_sync(0xffffffffu, e_vdw, o);
         e_ele += __shfl_xor_sync(0xffffffffu, e_ele, o);
@@ -435,7 +444,9 @@ k_pair_ljzd_jm(const int *__restrict__ counters, const int *__restrict__ cell_sy
 // __ffma2_rn rounds like __fmaf_rn); only the order in which partial sums are added differs.
 __device__ __forceinline__ float2 og_f2(float a, float b) { return make_float2(a, b); }
 
-template <bool VIR, int MINB>
+// ENE = false skips the energies (pair terms, their sums and the per-cell energy slots): the
+// step path asks for them only on the steps whose energies are read.
+template <bool VIR, bool ENE, int MINB>
 __global__ void __launch_bounds__(256, MINB)
 k_pair_ljzd_jm2(const int *__restrict__ counters, const int *__restrict__ cell_sys, const SysDev *__restrict__ sys,
                 const float4 *__restrict__ bbox, const float4 *__restrict__ xq, const int *__restrict__ slot_type,
@@ -471,7 +482,9 @@ k_pair_ljzd_jm2(const int *__restrict__ counters, const int *__restrict__ cell_s
     float2 fx[OG_CELL / 2], fy[OG_CELL / 2], fz[OG_CELL / 2];
 #pragma unroll
     for (int p = 0; p < OG_CELL / 2; p++) fx[p] = fy[p] = fz[p] = og_f2(0.f, 0.f);
-    float2 av = og_f2(0.f, 0.f), ae = og_f2(0.f, 0.f);
+    float2 av = og_f2(0.f, 0.f), ae = og_f2(0.f, 0.f);  // FP32 partials of up to OG_FOLD rounds ...
+    double dv = 0.0, de = 0.0;                          // ... folded into FP64
+    int n_round = 0;
     int n_act = 0;
     double v[9];
     if (VIR)
@@ -552,14 +565,22 @@ k_pair_ljzd_jm2(const int *__restrict__ counters, const int *__restrict__ cell_s
                 wc = __fmul2_rn(wc, on);
                 if (VIR) n_act += (act_a ? 1 : 0) + (act_b ? 1 : 0);
                 const float2 wx = __fmul2_rn(wc, dx), wy = __fmul2_rn(wc, dy), wz = __fmul2_rn(wc, dz);
-                av = __fadd2_rn(av, pv);
-                ae = __fadd2_rn(ae, pe);
+                if (ENE) {
+                    av = __fadd2_rn(av, pv);
+                    ae = __fadd2_rn(ae, pe);
+                }
                 fx[p] = __fadd2_rn(fx[p], wx);
                 fy[p] = __fadd2_rn(fy[p], wy);
                 fz[p] = __fadd2_rn(fz[p], wz);
                 wjx = __fadd2_rn(wjx, wx);
                 wjy = __fadd2_rn(wjy, wy);
                 wjz = __fadd2_rn(wjz, wz);
+            }
+            if (ENE && ++n_round == OG_FOLD) {
+                dv += (double)av.x + (double)av.y;
+                de += (double)ae.x + (double)ae.y;
+                av = ae = og_f2(0.f, 0.f);
+                n_round = 0;
             }
             const float sx = -(wjx.x + wjx.y), sy = -(wjy.x + wjy.y), sz = -(wjz.x + wjz.y);
             if (active && (sx != 0.f || sy != 0.f || sz != 0.f)) {
@@ -571,7 +592,8 @@ k_pair_ljzd_jm2(const int *__restrict__ counters, const int *__restrict__ cell_s
                     const double sh[3] = {(img & 1) ? -S.L[0] : ((img & 2) ? S.L[0] : 0.0),
                                           (img & 4) ? -S.L[1] : ((img & 8) ? S.L[1] : 0.0),
                                           (img & 16) ? -S.L[2] : ((img & 32) ? S.L[2] : 0.0)};
-                    const double fjv[3] = {(double)sx, (double)sy, (double)sz};
+                    // sum over pairs of d (x) f: f on i is +w, so the shift term takes -(work on j)
+                    const double fjv[3] = {-(double)sx, -(double)sy, -(double)sz};
                     for (int a = 0; a < 3; a++)
                         for (int b = 0; b < 3; b++) v[a * 3 + b] += sh[a] * fjv[b];
                 }
@@ -600,7 +622,8 @@ k_pair_ljzd_jm2(const int *__restrict__ counters, const int *__restrict__ cell_s
         atomicAdd(fa + 1, (unsigned long long)og_to_fix(mine[1]));
         atomicAdd(fa + 2, (unsigned long long)og_to_fix(mine[2]));
     }
-    double e_vdw = (double)av.x + (double)av.y, e_ele = (double)ae.x + (double)ae.y;
+    if (!ENE) return;
+    double e_vdw = dv + (double)av.x + (double)av.y, e_ele = de + (double)ae.x + (double)ae.y;
     for (int o = 16; o > 0; o >>= 1) {
         e_vdw += __shfl_xor_sync(0xffffffffu, e_vdw, o);
         e_ele += __shfl_xor_sync(0xffffffffu, e_ele, o);
@@ -628,9 +651,11 @@ k_pair_ljzd_jm2(const int *__restrict__ counters, const int *__restrict__ cell_s
 template __global__ void k_pair_ljzd_jm<true, 2>(OG_PAIR_ARGS_DECL);
 template __global__ void k_pair_ljzd_jm<false, 2>(OG_PAIR_ARGS_DECL);
 template __global__ void k_pair_ljzd_jm<false, 3>(OG_PAIR_ARGS_DECL);
-template __global__ void k_pair_ljzd_jm2<true, 2>(OG_PAIR_ARGS_DECL);
-template __global__ void k_pair_ljzd_jm2<false, 2>(OG_PAIR_ARGS_DECL);
-template __global__ void k_pair_ljzd_jm2<false, 3>(OG_PAIR_ARGS_DECL);
+template __global__ void k_pair_ljzd_jm2<true, true, 2>(OG_PAIR_ARGS_DECL);
+template __global__ void k_pair_ljzd_jm2<false, true, 2>(OG_PAIR_ARGS_DECL);
+template __global__ void k_pair_ljzd_jm2<false, true, 3>(OG_PAIR_ARGS_DECL);
+template __global__ void k_pair_ljzd_jm2<false, false, 2>(OG_PAIR_ARGS_DECL);
+template __global__ void k_pair_ljzd_jm2<false, false, 3>(OG_PAIR_ARGS_DECL);
 
 template __global__ void k_pair_ljzd<true, 2>(const int *, const int *, const SysDev *, const float4 *,
                                                 const float4 *, const int *, const int *, const float4 *,
