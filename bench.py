@@ -374,14 +374,16 @@ def run_walkers(walkers, params, polys, n_steps, chunk, trace=False):
     state = {k: (walkers[k]["crd"], walkers[k]["vel"]) for k in keep}
     traces = {k: [] for k in keep}
     done, ms, atom_steps, dropped = 0, 0.0, 0, []
+    variant = -1  # the first engine autotunes; a re-formed one keeps its choice
     while done < n_steps:
         eng = engine.Engine(0)
-        eng.set_tuning(1)
+        eng.set_tuning(variant)
         for k in keep:
             s = dict(walkers[k])
             s["crd"], s["vel"] = state[k]
             eng.add_system(s, params, polys[k] if polys else None, first_step=done)
         eng.finalize()
+        variant = eng.tuning()["pair_variant"]
         eng.set_timing("step")
         if trace:
             eng.set_trace(n_steps)
@@ -457,7 +459,9 @@ def run_mcmd(args):
                                    % (args.walkers, n_atoms),
                        "timing": "CUDA events around every og_step call of %d steps, engine re-forming after a "
                                  "fault excluded" % args.chunk},
-            "walkers_dropped": {"warm_up": len(drop_warm), "prerun": len(drop_pre), "run": len(drop_run)},
+            "walkers_dropped": {"warm_up": len(drop_warm), "prerun": len(drop_pre), "run": len(drop_run),
+                                "note": "a walker whose system faults (og_get_system_faults) is retired; the "
+                                        "others are re-stepped from the undone call"},
             "plain": {"atom_steps_per_s": plain, "sample": "2 walkers run alone (wall clock around og_step)"},
             "speedup_vs_plain": batched / plain}
 

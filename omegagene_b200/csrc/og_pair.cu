@@ -644,6 +644,245 @@ k_pair_ljzd_jm2(const int *__restrict__ counters, const int *__restrict__ cell_s
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// j-queue: the packed j-major kernel with a second cull at the j-atom level.  Per warp, the
+// surviving cell pairs are expanded four at a time into their 8 j atoms; a j atom farther than
+// the cutoff from cell1's bounding box cannot interact with any i atom and is dropped, the rest
+// go into a per-warp ring of 64 entries in shared memory (j position relative to cell1's
+// frame, charge, type, slot, mask byte).  Whenever 32 entries are waiting, every lane takes one
+// and evaluates it against the 8 i atoms.  On water about 40% of the j atoms of a surviving cell
+// pair drop out, and every evaluation round runs with all 32 lanes busy.
+#define OG_JQ 64
+template <bool VIR, bool ENE, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+k_pair_ljzd_jq(const int *__restrict__ counters, const int *__restrict__ cell_sys, const SysDev *__restrict__ sys,
+               const float4 *__restrict__ bbox, const float4 *__restrict__ xq, const int *__restrict__ slot_type,
+               const int *__restrict__ cp_head, const float4 *__restrict__ cp_shift, const int2 *__restrict__ cp_c2img,
+               const unsigned long long *__restrict__ cp_mask, const float2 *__restrict__ lj,
+               unsigned long long *__restrict__ frc, double *__restrict__ cell_acc, long long pair_cap) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int wib = (threadIdx.x >> 5) & 7;
+    const int n_cells = counters[OG_CNT_N_CELLS];
+    if (warp >= n_cells) return;
+    const int c1 = warp;
+    const int jj = lane & 7, q = lane >> 3;
+    const SysDev &S = sys[cell_sys[c1]];
+    __shared__ float4 s_ab[8][OG_CELL / 2][2];
+    __shared__ int2 s_t2[8][OG_CELL / 2];
+    __shared__ float4 s_qx[8][OG_JQ];  // queued j: (x, y, z) in cell1's frame, charge
+    __shared__ int4 s_qi[8][OG_JQ];    // queued j: LJ type, slot, mask byte, image bits
+    if (lane < OG_CELL / 2) {
+        const float4 a = xq[c1 * OG_CELL + 2 * lane], b = xq[c1 * OG_CELL + 2 * lane + 1];
+        s_ab[wib][lane][0] = make_float4(a.x, b.x, a.y, b.y);
+        s_ab[wib][lane][1] = make_float4(a.z, b.z, a.w * (float)OG_CHARGE_COEFF, b.w * (float)OG_CHARGE_COEFF);
+        s_t2[wib][lane] = make_int2(slot_type[c1 * OG_CELL + 2 * lane] * S.n_types + S.lj_base,
+                                    slot_type[c1 * OG_CELL + 2 * lane + 1] * S.n_types + S.lj_base);
+    }
+    __syncwarp();
+    const float rc2 = S.cutoff2;
+    const float2 nzcore = og_f2(-S.zcore, -S.zcore), bco = og_f2(S.bcoeff, S.bcoeff);
+    const float2 nfco = og_f2(-S.fcoeff, -S.fcoeff);
+    const float2 one = og_f2(1.f, 1.f), half = og_f2(0.5f, 0.5f), six = og_f2(6.f, 6.f);
+    const float2 m12 = og_f2(-12.f, -12.f), mone = og_f2(-1.f, -1.f);
+    const float rskip = sqrtf(rc2) + 1e-3f, rskip2 = rskip * rskip;
+    const float4 b1l = bbox[2 * c1], b1h = bbox[2 * c1 + 1];
+    float2 fx[OG_CELL / 2], fy[OG_CELL / 2], fz[OG_CELL / 2];
+#pragma unroll
+    for (int p = 0; p < OG_CELL / 2; p++) fx[p] = fy[p] = fz[p] = og_f2(0.f, 0.f);
+    float2 av = og_f2(0.f, 0.f), ae = og_f2(0.f, 0.f);
+    double dv = 0.0, de = 0.0;
+    int n_act = 0;
+    double v[9];
+    if (VIR)
+        for (int k = 0; k < 9; k++) v[k] = 0;
+    int q_head = 0, q_len = 0;  // ring of queued j entries (warp-uniform)
+
+    // lane takes queue entry (q_head + lane) if lane < n_take and evaluates it against cell1
+    auto drain = [&](int n_take) {
+        const bool active = lane < n_take;
+        const int e = (q_head + lane) & (OG_JQ - 1);
+        float4 xj = make_float4(0.f, 0.f, 0.f, 0.f);
+        int4 ji = make_int4(0, 0, 0xff, 0);
+        if (active) {
+            xj = s_qx[wib][e];
+            ji = s_qi[wib][e];
+        }
+        const unsigned skip = (unsigned)ji.z;
+        const int tj = ji.x;
+        const float2 nrx = og_f2(-xj.x, -xj.x), nry = og_f2(-xj.y, -xj.y), nrz = og_f2(-xj.z, -xj.z);
+        const float2 qj = og_f2(xj.w, xj.w);
+        float2 wjx = og_f2(0.f, 0.f), wjy = og_f2(0.f, 0.f), wjz = og_f2(0.f, 0.f);
+#pragma unroll
+        for (int p = 0; p < OG_CELL / 2; p++) {
+            const float4 A = s_ab[wib][p][0], B = s_ab[wib][p][1];
+            const int2 T = s_t2[wib][p];
+            const float2 dx = __fadd2_rn(og_f2(A.x, A.y), nrx);
+            const float2 dy = __fadd2_rn(og_f2(A.z, A.w), nry);
+            const float2 dz = __fadd2_rn(og_f2(B.x, B.y), nrz);
+            const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+            const bool act_a = ((skip >> (2 * p)) & 1u) == 0u && r2.x < rc2;
+            const bool act_b = ((skip >> (2 * p + 1)) & 1u) == 0u && r2.y < rc2;
+            const float2 r2s = og_f2(act_a ? r2.x : 1.0f, act_b ? r2.y : 1.0f);
+            float2 y = og_f2(rsqrtf(r2s.x), rsqrtf(r2s.y));
+            const float2 h = __ffma2_rn(__fmul2_rn(__fmul2_rn(r2s, mone), y), y, one);
+            y = __ffma2_rn(__fmul2_rn(half, y), h, y);
+            const float2 r2inv = __fmul2_rn(y, y);
+            const float2 r6 = __fmul2_rn(__fmul2_rn(r2inv, r2inv), r2inv);
+            const float2 pa = __ldg(&lj[T.x + tj]), pb = __ldg(&lj[T.y + tj]);
+            const float2 t6 = __fmul2_rn(og_f2(pa.x, pb.x), r6);
+            const float2 t12 = __fmul2_rn(__fmul2_rn(og_f2(pa.y, pb.y), r6), r6);
+            const float2 cc = __fmul2_rn(og_f2(B.z, B.w), qj);
+            float2 wc = __ffma2_rn(__fmul2_rn(cc, mone), __ffma2_rn(y, r2inv, nfco),
+                                   __fmul2_rn(r2inv, __ffma2_rn(t12, m12, __fmul2_rn(six, t6))));
+            const float2 on = og_f2(act_a ? 1.f : 0.f, act_b ? 1.f : 0.f);
+            wc = __fmul2_rn(wc, on);
+            if (ENE) {
+                const float2 pv = __fmul2_rn(__ffma2_rn(t6, mone, t12), on);
+                const float2 pe = __fmul2_rn(__fmul2_rn(cc, __ffma2_rn(bco, r2s, __fadd2_rn(y, nzcore))), on);
+                av = __fadd2_rn(av, pv);
+                ae = __fadd2_rn(ae, pe);
+            }
+            if (VIR) n_act += (act_a ? 1 : 0) + (act_b ? 1 : 0);
+            const float2 wx = __fmul2_rn(wc, dx), wy = __fmul2_rn(wc, dy), wz = __fmul2_rn(wc, dz);
+            fx[p] = __fadd2_rn(fx[p], wx);
+            fy[p] = __fadd2_rn(fy[p], wy);
+            fz[p] = __fadd2_rn(fz[p], wz);
+            wjx = __fadd2_rn(wjx, wx);
+            wjy = __fadd2_rn(wjy, wy);
+            wjz = __fadd2_rn(wjz, wz);
+        }
+        if (ENE) {
+            dv += (double)av.x + (double)av.y;
+            de += (double)ae.x + (double)ae.y;
+            av = ae = og_f2(0.f, 0.f);
+        }
+        const float sx = -(wjx.x + wjx.y), sy = -(wjy.x + wjy.y), sz = -(wjz.x + wjz.y);
+        if (active && (sx != 0.f || sy != 0.f || sz != 0.f)) {
+            unsigned long long *fj = frc + 3 * (size_t)ji.y;
+            atomicAdd(fj + 0, (unsigned long long)__float2ll_rn(sx * (float)OG_FIX_SCALE));
+            atomicAdd(fj + 1, (unsigned long long)__float2ll_rn(sy * (float)OG_FIX_SCALE));
+            atomicAdd(fj + 2, (unsigned long long)__float2ll_rn(sz * (float)OG_FIX_SCALE));
+            const int img = ji.w;
+            if (VIR && img != 0) {
+                const double sh[3] = {(img & 1) ? -S.L[0] : ((img & 2) ? S.L[0] : 0.0),
+                                      (img & 4) ? -S.L[1] : ((img & 8) ? S.L[1] : 0.0),
+                                      (img & 16) ? -S.L[2] : ((img & 32) ? S.L[2] : 0.0)};
+                const double fjv[3] = {-(double)sx, -(double)sy, -(double)sz};
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++) v[a * 3 + b] += sh[a] * fjv[b];
+            }
+        }
+        __syncwarp();
+        q_head = (q_head + n_take) & (OG_JQ - 1);
+        q_len -= n_take;
+    };
+
+    const int k_beg = cp_head[c1];
+    const int k_end = (int)min((long long)cp_head[c1 + 1], pair_cap);
+    for (int chunk = k_beg; chunk < k_end; chunk += 32) {
+        const int kk = chunk + lane;
+        float4 my_sp = make_float4(0.f, 0.f, 0.f, 0.f);
+        unsigned long long my_m = ~0ull;
+        int my_img = 0;
+        bool keep = false;
+        if (kk < k_end) {
+            my_sp = cp_shift[kk];
+            const int c2 = __float_as_int(my_sp.w);
+            const float4 l2 = bbox[2 * c2], h2 = bbox[2 * c2 + 1];
+            const float gx = fmaxf(0.f, fmaxf(l2.x + my_sp.x - b1h.x, b1l.x - (h2.x + my_sp.x)));
+            const float gy = fmaxf(0.f, fmaxf(l2.y + my_sp.y - b1h.y, b1l.y - (h2.y + my_sp.y)));
+            const float gz = fmaxf(0.f, fmaxf(l2.z + my_sp.z - b1h.z, b1l.z - (h2.z + my_sp.z)));
+            keep = gx * gx + gy * gy + gz * gz < rskip2;
+            if (keep) my_m = cp_mask[kk];
+            if (VIR && keep) my_img = cp_c2img[kk].y;
+        }
+        const unsigned ballot = __ballot_sync(0xffffffffu, keep);
+        const int n_keep = __popc(ballot);
+        for (int r = 0; r < n_keep; r += 4) {
+            // expand four surviving cell pairs into their j atoms; queue those near cell1
+            const int idx = r + q;
+            const bool active = idx < n_keep;
+            const int src = active ? (int)__fns(ballot, 0, idx + 1) : 0;
+            float4 sp;
+            sp.x = __shfl_sync(0xffffffffu, my_sp.x, src);
+            sp.y = __shfl_sync(0xffffffffu, my_sp.y, src);
+            sp.z = __shfl_sync(0xffffffffu, my_sp.z, src);
+            sp.w = __shfl_sync(0xffffffffu, my_sp.w, src);
+            const unsigned long long m = __shfl_sync(0xffffffffu, my_m, src);
+            const int img = VIR ? __shfl_sync(0xffffffffu, my_img, src) : 0;
+            const int c2 = __float_as_int(sp.w);
+            bool push = false;
+            float4 xj = make_float4(0.f, 0.f, 0.f, 0.f);
+            int tj = 0;
+            const unsigned skip = active ? (unsigned)(m >> (jj * OG_CELL)) & 0xffu : 0xffu;
+            if (active && skip != 0xffu) {
+                xj = xq[c2 * OG_CELL + jj];
+                tj = slot_type[c2 * OG_CELL + jj];
+                xj.x += sp.x;
+                xj.y += sp.y;
+                xj.z += sp.z;
+                const float gx = fmaxf(0.f, fmaxf(xj.x - b1h.x, b1l.x - xj.x));
+                const float gy = fmaxf(0.f, fmaxf(xj.y - b1h.y, b1l.y - xj.y));
+                const float gz = fmaxf(0.f, fmaxf(xj.z - b1h.z, b1l.z - xj.z));
+                push = gx * gx + gy * gy + gz * gz < rskip2;
+            }
+            const unsigned pb = __ballot_sync(0xffffffffu, push);
+            if (push) {
+                const int e = (q_head + q_len + __popc(pb & ((1u << lane) - 1u))) & (OG_JQ - 1);
+                s_qx[wib][e] = xj;
+                s_qi[wib][e] = make_int4(tj, c2 * OG_CELL + jj, (int)skip, img);
+            }
+            q_len += __popc(pb);
+            __syncwarp();
+            if (q_len >= 32) drain(32);
+        }
+    }
+    if (q_len > 0) drain(q_len);
+    double mine[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int p = 0; p < OG_CELL / 2; p++) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            double w3[3] = {(double)(h ? fx[p].y : fx[p].x), (double)(h ? fy[p].y : fy[p].x),
+                            (double)(h ? fz[p].y : fz[p].x)};
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                double x = w3[d];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+                if (lane == 2 * p + h) mine[d] = x;
+            }
+        }
+    }
+    if (lane < OG_CELL && (mine[0] != 0.0 || mine[1] != 0.0 || mine[2] != 0.0)) {
+        unsigned long long *fa = frc + 3 * (size_t)(c1 * OG_CELL + lane);
+        atomicAdd(fa + 0, (unsigned long long)og_to_fix(mine[0]));
+        atomicAdd(fa + 1, (unsigned long long)og_to_fix(mine[1]));
+        atomicAdd(fa + 2, (unsigned long long)og_to_fix(mine[2]));
+    }
+    if (!ENE) return;
+    double e_vdw = dv, e_ele = de;
+    for (int o = 16; o > 0; o >>= 1) {
+        e_vdw += __shfl_xor_sync(0xffffffffu, e_vdw, o);
+        e_ele += __shfl_xor_sync(0xffffffffu, e_ele, o);
+    }
+    if (VIR) {
+        for (int k = 0; k < 9; k++)
+            for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+        for (int o = 16; o > 0; o >>= 1) n_act += __shfl_xor_sync(0xffffffffu, n_act, o);
+    }
+    if (lane == 0) {
+        double *acc = cell_acc + (size_t)c1 * OG_CELL_ACC;
+        acc[0] = e_vdw;
+        acc[1] = e_ele;
+        if (VIR) {
+            for (int k = 0; k < 9; k++) acc[2 + k] = v[k];
+            acc[11] = (double)n_act;
+        }
+    }
+}
+
 #define OG_PAIR_ARGS_DECL                                                                                   \
     const int *, const int *, const SysDev *, const float4 *, const float4 *, const int *, const int *,      \
         const float4 *, const int2 *, const unsigned long long *, const float2 *, unsigned long long *, double *, \
@@ -656,6 +895,11 @@ template __global__ void k_pair_ljzd_jm2<false, true, 2>(OG_PAIR_ARGS_DECL);
 template __global__ void k_pair_ljzd_jm2<false, true, 3>(OG_PAIR_ARGS_DECL);
 template __global__ void k_pair_ljzd_jm2<false, false, 2>(OG_PAIR_ARGS_DECL);
 template __global__ void k_pair_ljzd_jm2<false, false, 3>(OG_PAIR_ARGS_DECL);
+template __global__ void k_pair_ljzd_jq<true, true, 2>(OG_PAIR_ARGS_DECL);
+template __global__ void k_pair_ljzd_jq<false, true, 2>(OG_PAIR_ARGS_DECL);
+template __global__ void k_pair_ljzd_jq<false, true, 3>(OG_PAIR_ARGS_DECL);
+template __global__ void k_pair_ljzd_jq<false, false, 2>(OG_PAIR_ARGS_DECL);
+template __global__ void k_pair_ljzd_jq<false, false, 3>(OG_PAIR_ARGS_DECL);
 
 template __global__ void k_pair_ljzd<true, 2>(const int *, const int *, const SysDev *, const float4 *,
                                                 const float4 *, const int *, const int *, const float4 *,

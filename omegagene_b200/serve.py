@@ -61,8 +61,11 @@ class Job:
 
 
 class Server:
-    def __init__(self, device=0, hbm_budget_bytes=None, max_jobs=64, window=100, pair_variant=1,
+    def __init__(self, device=0, hbm_budget_bytes=None, max_jobs=64, window=100, pair_variant="auto",
                  clock=time.perf_counter, sleep=time.sleep, engine_factory=None):
+        """pair_variant: a fixed pair-kernel variant, or "auto": the first engine autotunes and
+        every later engine reuses its choice, so a job keeps one kernel (and bitwise results)
+        across re-formed batches."""
         self.device = device
         if hbm_budget_bytes is None:
             import torch
@@ -81,13 +84,15 @@ class Server:
 
     def _build(self, active):
         eng = self.engine_factory(self.device)
-        if self.pair_variant is not None:
+        if self.pair_variant != "auto":
             eng.set_tuning(self.pair_variant)
         for j in active:
             s = dict(j.system)
             s["crd"], s["vel"] = j.crd, j.vel
             eng.add_system(s, j.params, j.mcmd, first_step=j.steps_done)
         eng.finalize()
+        if self.pair_variant == "auto":
+            self.pair_variant = eng.tuning()["pair_variant"]
         self.n_relayouts += 1
         return eng
 
@@ -178,12 +183,12 @@ class Server:
                 "jobs": done}
 
 
-def run_alone(job, device=0, pair_variant=1, warmup=0):
+def run_alone(job, device=0, pair_variant="auto", warmup=0):
     """The plain path: one job, one engine, start to finish; returns (seconds, final energies,
     final positions, final velocities).  `warmup` extra steps run first, untimed (a timing aid:
     the returned state is then `warmup` steps further on)."""
     eng = engine.Engine(device)
-    if pair_variant is not None:
+    if pair_variant != "auto":
         eng.set_tuning(pair_variant)
     s = dict(job.system)
     eng.add_system(s, job.params, job.mcmd)

@@ -84,11 +84,11 @@ def test_batched_cell_lists_equal_single():
             np.testing.assert_array_equal(cp[k], getattr(ref, k), err_msg="%d %s" % (i, k))
 
 
-@pytest.mark.parametrize("variant", [0, 3, 5])
+@pytest.mark.parametrize("variant", [0, 3, 5, 7])
 @pytest.mark.parametrize("name,make", SMALL, ids=[n for n, _ in SMALL])
 def test_forces_energies_virial_vs_fp64(name, make, variant):
-    """The three pair-kernel families (0: warp per 8x8 cell pair, 3: j-major, 5: j-major with
-    packed FP32x2 arithmetic)."""
+    """The four pair-kernel families (0: warp per 8x8 cell pair, 3: j-major, 5: j-major with
+    packed FP32x2 arithmetic, 7: packed j-major fed by a queue of j atoms near the i cell)."""
     s = make()
     p = _params()
     eng = _engine([(s, p, None)], variant)
@@ -175,16 +175,18 @@ def test_mcmd_scaling_matches_oracle():
         assert abs(tr[i, names.index("potential")] - r["potential"]) <= 1e-5 * abs(r["potential"]) + 5e-3
 
 
-def test_batch_invariance_bitwise():
+@pytest.mark.parametrize("variant", [1, 6, 8])
+def test_batch_invariance_bitwise(variant):
     """A system gives the same trajectory alone and batched with others (fixed-point forces,
-    per-system fixed-order reductions)."""
+    per-system fixed-order reductions), for a given pair-kernel variant (variants of different
+    families add FP32 partial sums in different orders)."""
     a = systems.water_system(1500, seed=5)
     others = [systems.water_system(700, seed=9), systems.chain_water_system(300, 2500, seed=4, radius=12.0)]
     p = _params(nsgrid_update_intvl=10, time_step=2.0, thermostat="scaling", temperature=300.0)
-    alone = _engine([(a, p, None)])
+    alone = _engine([(a, p, None)], variant)
     alone.set_trace(25)
     alone.step(25)
-    mixed = _engine([(others[0], p, None), (a, p, None), (others[1], p, None)])
+    mixed = _engine([(others[0], p, None), (a, p, None), (others[1], p, None)], variant)
     mixed.set_trace(25)
     mixed.step(25)
     np.testing.assert_array_equal(alone.get_trace(25)[:, 0, :], mixed.get_trace(25)[:, 1, :])

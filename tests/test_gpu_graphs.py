@@ -30,8 +30,9 @@ def _mixed_batch():
             (chain, thermo, mcmd)]
 
 
-def _run(batch, n_steps, graphs, chunks=None):
+def _run(batch, n_steps, graphs, chunks=None, variant=6):
     eng = engine.Engine(0)
+    eng.set_tuning(variant)  # one pair kernel for every engine compared bitwise
     eng.set_graphs(graphs)
     for s, p, m in batch:
         eng.add_system(s, p, m)

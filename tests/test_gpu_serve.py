@@ -29,10 +29,10 @@ def _jobs():
 
 def test_served_jobs_equal_alone_runs():
     jobs = _jobs()
-    res = serve.Server(0, max_jobs=3, window=20).run(jobs)
+    res = serve.Server(0, max_jobs=3, window=20, pair_variant=6).run(jobs)
     assert res["n_jobs"] == 5 and res["relayouts"] >= 3
     for j in jobs:
-        _, ene, crd, vel = serve.run_alone(serve.Job(j.id, j.system, j.params, j.n_steps))
+        _, ene, crd, vel = serve.run_alone(serve.Job(j.id, j.system, j.params, j.n_steps), pair_variant=6)
         assert np.array_equal(j.crd, crd) and np.array_equal(j.vel, vel), j.id
         assert j.energies == ene, j.id
 
@@ -46,8 +46,9 @@ def test_memory_budget_limits_admission():
     assert max(srv.batch_sizes) <= 2
 
 
-def _engine(batch):
+def _engine(batch, variant=6):
     eng = engine.Engine(0)
+    eng.set_tuning(variant)  # one pair kernel for every engine compared bitwise
     for s, p in batch:
         eng.add_system(s, p)
     eng.finalize()

@@ -31,6 +31,9 @@ class FakeEngine:
     def set_tuning(self, v):
         pass
 
+    def tuning(self):
+        return {"pair_variant": 0}
+
     def add_system(self, s, params, mcmd=None, first_step=0):
         self.systems.append({"crd": np.array(s["crd"], float), "vel": np.array(s["vel"], float),
                              "first_step": first_step, "n": s["n_atoms"]})
