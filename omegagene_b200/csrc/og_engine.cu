@@ -126,6 +126,7 @@ struct HostSystem {
     SysDev dev;
     int n_excess = 0;
     std::vector<int32_t> excess;  // pairs (i<j) in MmSystem::set_excess_pairs order, local ids
+    std::vector<int32_t> xs, xl;  // exclusion partners per atom (CSR, insertion order), local ids
     int d_free = 0;
 };
 
@@ -417,24 +418,44 @@ double self_energy(const HostSystem &h) {
 
 // MmSystem::set_nb15off + set_excess_pairs (MmSystem.cpp:478-525, 700-736): rows in insertion
 // order, then pairs i < j walking the rows.
-og_status build_exclusions(og_engine *e, HostSystem &h, std::vector<std::vector<int>> &rows) {
+// Exclusion partners per atom as CSR (h.xs, h.xl): each row keeps the order in which the pairs
+// list its partners, without repeats, and the excluded ("excess") pairs i < j follow row by row
+// (MmSystem::set_excess_pairs, whose order the self energy's float running sum depends on).
+og_status build_exclusions(og_engine *e, HostSystem &h) {
     const int n = h.d.n_atoms;
-    rows.assign(n, {});
+    std::vector<int32_t> deg(n + 1, 0);
     for (int k = 0; k < h.d.n_excl; k++) {
         int a = h.excl[2 * k], b = h.excl[2 * k + 1];
         if (a < 0 || b < 0 || a >= n || b >= n || a == b) return fail(e, OG_ERR_INVALID, "bad exclusion pair %d", k);
-        bool ab = false, ba = false;
-        for (int x : rows[a]) ab |= x == b;
-        for (int x : rows[b]) ba |= x == a;
-        if (!ab) rows[a].push_back(b);
-        if (!ba) rows[b].push_back(a);
+        deg[a]++;
+        deg[b]++;
+    }
+    std::vector<int32_t> start(n + 1, 0);
+    for (int i = 0; i < n; i++) start[i + 1] = start[i] + deg[i];
+    std::vector<int32_t> fill(start.begin(), start.end() - 1), raw(start[n]);
+    for (int k = 0; k < h.d.n_excl; k++) {
+        int a = h.excl[2 * k], b = h.excl[2 * k + 1];
+        raw[fill[a]++] = b;
+        raw[fill[b]++] = a;
+    }
+    h.xs.assign(n + 1, 0);
+    h.xl.clear();
+    h.xl.reserve(raw.size());
+    for (int i = 0; i < n; i++) {
+        const size_t row0 = h.xl.size();
+        for (int p = start[i]; p < start[i + 1]; p++) {
+            bool seen = false;
+            for (size_t q = row0; q < h.xl.size(); q++) seen |= h.xl[q] == raw[p];
+            if (!seen) h.xl.push_back(raw[p]);
+        }
+        h.xs[i + 1] = (int32_t)h.xl.size();
     }
     h.excess.clear();
     for (int i = 0; i < n; i++)
-        for (int j : rows[i])
-            if (i < j) {
+        for (int p = h.xs[i]; p < h.xs[i + 1]; p++)
+            if (i < h.xl[p]) {
                 h.excess.push_back(i);
-                h.excess.push_back(j);
+                h.excess.push_back(h.xl[p]);
             }
     h.n_excess = (int)h.excess.size() / 2;
     return OG_OK;
@@ -1090,8 +1111,7 @@ og_status og_add_system(og_engine *e, const og_system_desc *d, int32_t *sys_id) 
             while (x < lo) x += L;
             while (x >= up) x -= L;
         }
-    std::vector<std::vector<int>> rows;
-    s = build_exclusions(e, h, rows);
+    s = build_exclusions(e, h);
     if (s) {
         e->sys.pop_back();
         return s;
@@ -1191,12 +1211,9 @@ og_status og_finalize(og_engine *e) {
             mass_inv.push_back((float)(1.0 / (double)(float)h.mass[i]));
             atom_type.push_back(h.type[i]);
         }
-        // exclusion CSR (global ids)
-        std::vector<std::vector<int>> rows;
-        s = build_exclusions(e, h, rows);
-        if (s) return s;
+        // exclusion CSR (global ids), built by og_add_system
         for (int i = 0; i < n; i++) {
-            for (int x : rows[i]) excl_list.push_back(atom_base + x);
+            for (int p = h.xs[i]; p < h.xs[i + 1]; p++) excl_list.push_back(atom_base + h.xl[p]);
             excl_start.push_back((int)excl_list.size());
         }
         for (int q = 0; q < h.n_excess; q++) {
