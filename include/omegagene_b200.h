@@ -186,8 +186,9 @@ og_status og_get_flags(og_engine *e, int32_t *flags);
 /* Pair-kernel variants: 0-2 = one warp per 8x8 cell pair at register budgets 100/80/64 per
  * thread; 3-4 = j-major (each lane one j atom against the 8 i atoms) at 100/80; 5-6 = j-major
  * with sm_100 packed FP32x2 arithmetic (two i atoms per instruction) at 128/80; 7-8 = packed
- * j-major fed by a per-warp queue of the j atoms within the cutoff of the i cell, at 128/80. */
-#define OG_N_PAIR_VARIANTS 9
+ * j-major fed by a per-warp queue of the j atoms within the cutoff of the i cell, at 128/80;
+ * 9 = the same at 102 registers in blocks of 128 threads. */
+#define OG_N_PAIR_VARIANTS 10
 /* Autotuner result: the pair-kernel variant in use and the best time of each variant on the
  * first list, in ms (variant_ms[OG_N_PAIR_VARIANTS]). */
 og_status og_get_tuning(og_engine *e, int32_t *pair_variant, double *variant_ms);

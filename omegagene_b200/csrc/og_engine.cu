@@ -47,7 +47,7 @@ template <bool VIR, int MINB>
 __global__ void k_pair_ljzd_jm(const int *, const int *, const SysDev *, const float4 *, const float4 *, const int *,
                                const int *, const float4 *, const int2 *, const unsigned long long *, const float2 *,
                                unsigned long long *, double *, long long);
-template <bool VIR, bool ENE, int MINB>
+template <bool VIR, bool ENE, int MINB, int NT>
 __global__ void k_pair_ljzd_jq(const int *, const int *, const SysDev *, const float4 *, const float4 *, const int *,
                                const int *, const float4 *, const int2 *, const unsigned long long *, const float2 *,
                                unsigned long long *, double *, long long);
@@ -550,9 +550,10 @@ og_status launch_pair(og_engine *e, bool vir, int variant, bool ene) {
     const unsigned nb = blocks((long long)e->cells_cap * 32, 256);
     cudaStream_t st = e->stream;
     // variants 0-2: warp per 8x8 cell pair (register budgets 100/80/64); 3-4: j-major (100/80);
-    // 5-6: j-major with packed FP32x2 arithmetic (128/80); 7-8: the same with a j-atom queue
-    // (128/80).  The virial kernel is that of the variant's family.
-    if (vir && variant >= 7) k_pair_ljzd_jq<true, true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    // 5-6: j-major with packed FP32x2 arithmetic (128/80); 7-9: the same with a j-atom queue
+    // (128/80 in blocks of 256, 102 in blocks of 128).  The virial kernel is that of the
+    // variant's family.
+    if (vir && variant >= 7) k_pair_ljzd_jq<true, true, 2, 256><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (vir && variant >= 5) k_pair_ljzd_jm2<true, true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (vir && variant >= 3) k_pair_ljzd_jm<true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (vir) k_pair_ljzd<true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
@@ -564,10 +565,12 @@ og_status launch_pair(og_engine *e, bool vir, int variant, bool ene) {
     else if (variant == 5) k_pair_ljzd_jm2<false, false, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (variant == 6 && ene) k_pair_ljzd_jm2<false, true, 3><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (variant == 6) k_pair_ljzd_jm2<false, false, 3><<<nb, 256, 0, st>>>(PAIR_ARGS);
-    else if (variant == 7 && ene) k_pair_ljzd_jq<false, true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
-    else if (variant == 7) k_pair_ljzd_jq<false, false, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
-    else if (variant == 8 && ene) k_pair_ljzd_jq<false, true, 3><<<nb, 256, 0, st>>>(PAIR_ARGS);
-    else if (variant == 8) k_pair_ljzd_jq<false, false, 3><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    else if (variant == 7 && ene) k_pair_ljzd_jq<false, true, 2, 256><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    else if (variant == 7) k_pair_ljzd_jq<false, false, 2, 256><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    else if (variant == 8 && ene) k_pair_ljzd_jq<false, true, 3, 256><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    else if (variant == 8) k_pair_ljzd_jq<false, false, 3, 256><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    else if (variant == 9 && ene) k_pair_ljzd_jq<false, true, 5, 128><<<2 * nb, 128, 0, st>>>(PAIR_ARGS);
+    else if (variant == 9) k_pair_ljzd_jq<false, false, 5, 128><<<2 * nb, 128, 0, st>>>(PAIR_ARGS);
     else k_pair_ljzd<false, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
     LAUNCH_CHECK();
     return OG_OK;

@@ -653,8 +653,8 @@ k_pair_ljzd_jm2(const int *__restrict__ counters, const int *__restrict__ cell_s
 // and evaluates it against the 8 i atoms.  On water about 40% of the j atoms of a surviving cell
 // pair drop out, and every evaluation round runs with all 32 lanes busy.
 #define OG_JQ 64
-template <bool VIR, bool ENE, int MINB>
-__global__ void __launch_bounds__(256, MINB)
+template <bool VIR, bool ENE, int MINB, int NT = 256>
+__global__ void __launch_bounds__(NT, MINB)
 k_pair_ljzd_jq(const int *__restrict__ counters, const int *__restrict__ cell_sys, const SysDev *__restrict__ sys,
                const float4 *__restrict__ bbox, const float4 *__restrict__ xq, const int *__restrict__ slot_type,
                const int *__restrict__ cp_head, const float4 *__restrict__ cp_shift, const int2 *__restrict__ cp_c2img,
@@ -662,16 +662,16 @@ k_pair_ljzd_jq(const int *__restrict__ counters, const int *__restrict__ cell_sy
                unsigned long long *__restrict__ frc, double *__restrict__ cell_acc, long long pair_cap) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    const int wib = (threadIdx.x >> 5) & 7;
+    const int wib = threadIdx.x >> 5;
     const int n_cells = counters[OG_CNT_N_CELLS];
     if (warp >= n_cells) return;
     const int c1 = warp;
     const int jj = lane & 7, q = lane >> 3;
     const SysDev &S = sys[cell_sys[c1]];
-    __shared__ float4 s_ab[8][OG_CELL / 2][2];
-    __shared__ int2 s_t2[8][OG_CELL / 2];
-    __shared__ float4 s_qx[8][OG_JQ];  // queued j: (x, y, z) in cell1's frame, charge
-    __shared__ int4 s_qi[8][OG_JQ];    // queued j: LJ type, slot, mask byte, image bits
+    __shared__ float4 s_ab[NT / 32][OG_CELL / 2][2];
+    __shared__ int2 s_t2[NT / 32][OG_CELL / 2];
+    __shared__ float4 s_qx[NT / 32][OG_JQ];  // queued j: (x, y, z) in cell1's frame, charge
+    __shared__ int4 s_qi[NT / 32][OG_JQ];    // queued j: LJ type, slot, mask byte, image bits
     if (lane < OG_CELL / 2) {
         const float4 a = xq[c1 * OG_CELL + 2 * lane], b = xq[c1 * OG_CELL + 2 * lane + 1];
         s_ab[wib][lane][0] = make_float4(a.x, b.x, a.y, b.y);
@@ -900,6 +900,8 @@ template __global__ void k_pair_ljzd_jq<false, true, 2>(OG_PAIR_ARGS_DECL);
 template __global__ void k_pair_ljzd_jq<false, true, 3>(OG_PAIR_ARGS_DECL);
 template __global__ void k_pair_ljzd_jq<false, false, 2>(OG_PAIR_ARGS_DECL);
 template __global__ void k_pair_ljzd_jq<false, false, 3>(OG_PAIR_ARGS_DECL);
+template __global__ void k_pair_ljzd_jq<false, true, 5, 128>(OG_PAIR_ARGS_DECL);
+template __global__ void k_pair_ljzd_jq<false, false, 5, 128>(OG_PAIR_ARGS_DECL);
 
 template __global__ void k_pair_ljzd<true, 2>(const int *, const int *, const SysDev *, const float4 *,
                                                 const float4 *, const int *, const int *, const float4 *,

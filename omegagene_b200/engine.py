@@ -23,7 +23,7 @@ LIB_PATH = os.path.join(HERE, "libomegagene_b200.so")
 ENERGY_NAMES = ["vdw", "ele", "bond", "angle", "potential", "kinetic", "temperature", "total", "ele_excess",
                 "ele_self", "mcmd_factor"]
 N_ENERGY = len(ENERGY_NAMES)
-N_PAIR_VARIANTS = 9  # OG_N_PAIR_VARIANTS
+N_PAIR_VARIANTS = 10  # OG_N_PAIR_VARIANTS
 
 
 class OgError(RuntimeError):
@@ -403,7 +403,7 @@ class Engine:
         return {"pair_variant": v.value, "variant_ms": ms.tolist()}
 
     def set_tuning(self, variant):
-        """Fixes the pair-kernel variant (0..8) before finalize(); -1 = autotune."""
+        """Fixes the pair-kernel variant (0..9) before finalize(); -1 = autotune."""
         self._check(self.L.og_set_tuning(self.h, int(variant)), "og_set_tuning")
 
     def set_graphs(self, on=True):
