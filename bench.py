@@ -7,7 +7,8 @@ zero-dipole alpha 0.  Inputs are seeded synthetic (a jittered lattice, random or
 Prints ONE JSON line.  `value` is ns/day (simulated time per wall-clock day) from CUDA events on
 the engine's stream around the timed og_step calls; `e2e` is the same metric through the C ABI
 with the state in pinned host memory, copied host->device before and device->host after every
-step.  With --gpus N (torchrun) every rank advances its own replica (replicas only: the path has
+step (coordinates in; coordinates and energies out, as the reference GPU path moves coordinates
+and work every step).  With --gpus N (torchrun) every rank advances its own replica (replicas only: the path has
 no exchange step), `value` sums the replicas' simulated time and the time is the max over ranks.
 
 --impl reference times the reference's CPU cell-list build (oracle/_ref/omegagene_ns, compiled
@@ -253,14 +254,18 @@ def run_ours(args, world, rank, local, pg):
     barrier(pg)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        eng.put_state_ptr(0, crd_h.data_ptr(), vel_h.data_ptr())
+        # the reference GPU path's per-step traffic: coordinates in; here coordinates and
+        # energies out (velocities stay on the device with the integrator)
+        eng.put_state_ptr(0, crd_h.data_ptr(), 0)
         eng.step_async(1)
-        eng.get_state_async_ptr(0, crd_h.data_ptr(), vel_h.data_ptr(), ene_h.data_ptr())
+        eng.get_state_async_ptr(0, crd_h.data_ptr(), 0, ene_h.data_ptr())
         eng.synchronize()
     t_e2e = max_over_ranks(pg, time.perf_counter() - t0)
     flags = eng.flags()
     e2e = {"value": ns_per_day(e2e_steps / t_e2e) * world, "unit": UNIT,
-           "h2d_bytes_per_step": 2 * 8 * 3 * n_atoms, "d2h_bytes_per_step": 2 * 8 * 3 * n_atoms + 8 * 11,
+           "h2d_bytes_per_step": 8 * 3 * n_atoms, "d2h_bytes_per_step": 8 * 3 * n_atoms + 8 * 11,
+           "protocol": "per step: og_put_state (coordinates, pinned host -> device), og_step_async(1), "
+                       "og_get_state_async (coordinates and energies, device -> pinned host), og_synchronize",
            "steps": e2e_steps}
     eng.close()
     pk = peaks()

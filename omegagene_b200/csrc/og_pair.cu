@@ -672,6 +672,9 @@ k_pair_ljzd_jq(const int *__restrict__ counters, const int *__restrict__ cell_sy
     __shared__ int2 s_t2[NT / 32][OG_CELL / 2];
     __shared__ float4 s_qx[NT / 32][OG_JQ];  // queued j: (x, y, z) in cell1's frame, charge
     __shared__ int4 s_qi[NT / 32][OG_JQ];    // queued j: LJ type, slot, mask byte, image bits
+    __shared__ float4 s_rsp[NT / 32][32];    // surviving records of the current chunk, in order:
+    __shared__ uint2 s_rm[NT / 32][32];      //   shift + cell2, exclusion mask,
+    __shared__ int s_rimg[NT / 32][VIR ? 32 : 1];  //   image bits (virial only)
     if (lane < OG_CELL / 2) {
         const float4 a = xq[c1 * OG_CELL + 2 * lane], b = xq[c1 * OG_CELL + 2 * lane + 1];
         s_ab[wib][lane][0] = make_float4(a.x, b.x, a.y, b.y);
@@ -799,18 +802,26 @@ k_pair_ljzd_jq(const int *__restrict__ counters, const int *__restrict__ cell_sy
         }
         const unsigned ballot = __ballot_sync(0xffffffffu, keep);
         const int n_keep = __popc(ballot);
+        if (keep) {  // compact the survivors in list order
+            const int rank = __popc(ballot & ((1u << lane) - 1u));
+            s_rsp[wib][rank] = my_sp;
+            s_rm[wib][rank] = make_uint2((unsigned)my_m, (unsigned)(my_m >> 32));
+            if (VIR) s_rimg[wib][rank] = my_img;
+        }
+        __syncwarp();
         for (int r = 0; r < n_keep; r += 4) {
             // expand four surviving cell pairs into their j atoms; queue those near cell1
             const int idx = r + q;
             const bool active = idx < n_keep;
-            const int src = active ? (int)__fns(ballot, 0, idx + 1) : 0;
-            float4 sp;
-            sp.x = __shfl_sync(0xffffffffu, my_sp.x, src);
-            sp.y = __shfl_sync(0xffffffffu, my_sp.y, src);
-            sp.z = __shfl_sync(0xffffffffu, my_sp.z, src);
-            sp.w = __shfl_sync(0xffffffffu, my_sp.w, src);
-            const unsigned long long m = __shfl_sync(0xffffffffu, my_m, src);
-            const int img = VIR ? __shfl_sync(0xffffffffu, my_img, src) : 0;
+            float4 sp = make_float4(0.f, 0.f, 0.f, 0.f);
+            unsigned long long m = ~0ull;
+            int img = 0;
+            if (active) {
+                sp = s_rsp[wib][idx];
+                const uint2 mm = s_rm[wib][idx];
+                m = ((unsigned long long)mm.y << 32) | mm.x;
+                if (VIR) img = s_rimg[wib][idx];
+            }
             const int c2 = __float_as_int(sp.w);
             bool push = false;
             float4 xj = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -837,6 +848,7 @@ k_pair_ljzd_jq(const int *__restrict__ counters, const int *__restrict__ cell_sy
             __syncwarp();
             if (q_len >= 32) drain(32);
         }
+        __syncwarp();  // the next chunk's survivors overwrite this chunk's
     }
     if (q_len > 0) drain(q_len);
     double mine[3] = {0.0, 0.0, 0.0};
