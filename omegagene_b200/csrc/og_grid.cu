@@ -282,7 +282,8 @@ __device__ int enumerate_column(int c1, int nb, const SysDev &S, int cell_base,
                                 const int *__restrict__ slot_atom, const int *__restrict__ atom_slot,
                                 const int *__restrict__ excl_start, const int *__restrict__ excl_list,
                                 const int *__restrict__ cell_excl, int2 *out_c2img, unsigned long long *out_mask,
-                                int out_cap) {
+                                int out_cap, const double *__restrict__ cell_origin = nullptr,
+                                float4 *out_shift = nullptr) {
     const int nx = S.nx, ny = S.ny, nuz = S.n_uni_z;
     const int wy = 2 * S.n_nb[1] + 1;
     const int dcx = nb / wy - S.n_nb[0];
@@ -357,6 +358,14 @@ __device__ int enumerate_column(int c1, int nb, const SysDev &S, int cell_base,
                     out_c2img[n] = make_int2(c2, img);
                     out_mask[n] = pair_mask(c1, c2, v1, cell_valid[c2], slot_atom, atom_slot, excl_start, excl_list,
                                             cell_excl);
+                    // pair-kernel record: shift from cell1's origin to cell2's image origin, in FP64
+                    const double shx = ix == -1 ? -S.L[0] : (ix == 1 ? S.L[0] : 0.0);
+                    const double shy = iy == -1 ? -S.L[1] : (iy == 1 ? S.L[1] : 0.0);
+                    const double shz2 = iz == -1 ? -S.L[2] : (iz == 1 ? S.L[2] : 0.0);
+                    out_shift[n] = make_float4((float)(cell_origin[3 * c2] + shx - cell_origin[3 * c1]),
+                                               (float)(cell_origin[3 * c2 + 1] + shy - cell_origin[3 * c1 + 1]),
+                                               (float)(cell_origin[3 * c2 + 2] + shz2 - cell_origin[3 * c1 + 2]),
+                                               __int_as_float(c2));
                 }
             }
             n++;
@@ -412,21 +421,8 @@ __global__ void k_fill_pairs(int *__restrict__ counters, int cells_cap, int nnc,
     const int cap = (int)max(0ll, min(pair_cap - off, (long long)1 << 30));
     int n = enumerate_column(c1, nb, S, sys_cell_base[s], cell_col, col_cell_start, col_head_cell, cell_zr, cell_uni,
                              uni_lo, uni_hi, cell_valid, slot_atom, atom_slot, excl_start, excl_list, cell_excl,
-                             cp_c2img + off, cp_mask + off, cap);
+                             cp_c2img + off, cp_mask + off, cap, cell_origin, cp_shift + off);
     if (off + n > pair_cap) og_set_flag(counters, OG_FLAG_PAIR_CAPACITY);
-    // pair-kernel record: shift from cell1's origin to cell2's image origin, formed in FP64
-    const int nw = min(n, cap);
-    const double o1x = cell_origin[3 * c1], o1y = cell_origin[3 * c1 + 1], o1z = cell_origin[3 * c1 + 2];
-    for (int k = 0; k < nw; k++) {
-        const int2 ci = cp_c2img[off + k];
-        const int c2 = ci.x, img = ci.y;
-        const double shx = (img & 1) ? -S.L[0] : ((img & 2) ? S.L[0] : 0.0);
-        const double shy = (img & 4) ? -S.L[1] : ((img & 8) ? S.L[1] : 0.0);
-        const double shz = (img & 16) ? -S.L[2] : ((img & 32) ? S.L[2] : 0.0);
-        cp_shift[off + k] = make_float4((float)(cell_origin[3 * c2] + shx - o1x),
-                                        (float)(cell_origin[3 * c2 + 1] + shy - o1y),
-                                        (float)(cell_origin[3 * c2 + 2] + shz - o1z), __int_as_float(c2));
-    }
 }
 
 // CSR heads from the scanned counts; also publishes the total.

@@ -783,22 +783,33 @@ k_pair_ljzd_jq(const int *__restrict__ counters, const int *__restrict__ cell_sy
 
     const int k_beg = cp_head[c1];
     const int k_end = (int)min((long long)cp_head[c1 + 1], pair_cap);
+    // each lane's record of the next chunk is loaded one chunk ahead
+    float4 nx_sp = make_float4(0.f, 0.f, 0.f, 0.f);
+    unsigned long long nx_m = ~0ull;
+    int nx_img = 0;
+    if (k_beg + lane < k_end) {
+        nx_sp = cp_shift[k_beg + lane];
+        nx_m = cp_mask[k_beg + lane];
+        if (VIR) nx_img = cp_c2img[k_beg + lane].y;
+    }
     for (int chunk = k_beg; chunk < k_end; chunk += 32) {
         const int kk = chunk + lane;
-        float4 my_sp = make_float4(0.f, 0.f, 0.f, 0.f);
-        unsigned long long my_m = ~0ull;
-        int my_img = 0;
+        const float4 my_sp = nx_sp;
+        const unsigned long long my_m = nx_m;
+        const int my_img = nx_img;
+        if (kk + 32 < k_end) {
+            nx_sp = cp_shift[kk + 32];
+            nx_m = cp_mask[kk + 32];
+            if (VIR) nx_img = cp_c2img[kk + 32].y;
+        }
         bool keep = false;
         if (kk < k_end) {
-            my_sp = cp_shift[kk];
             const int c2 = __float_as_int(my_sp.w);
             const float4 l2 = bbox[2 * c2], h2 = bbox[2 * c2 + 1];
             const float gx = fmaxf(0.f, fmaxf(l2.x + my_sp.x - b1h.x, b1l.x - (h2.x + my_sp.x)));
             const float gy = fmaxf(0.f, fmaxf(l2.y + my_sp.y - b1h.y, b1l.y - (h2.y + my_sp.y)));
             const float gz = fmaxf(0.f, fmaxf(l2.z + my_sp.z - b1h.z, b1l.z - (h2.z + my_sp.z)));
             keep = gx * gx + gy * gy + gz * gz < rskip2;
-            if (keep) my_m = cp_mask[kk];
-            if (VIR && keep) my_img = cp_c2img[kk].y;
         }
         const unsigned ballot = __ballot_sync(0xffffffffu, keep);
         const int n_keep = __popc(ballot);
