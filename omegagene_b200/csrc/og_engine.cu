@@ -1145,6 +1145,22 @@ og_status og_finalize(og_engine *e) {
     std::vector<double> spair_d2, strio_d2, thermo;
     std::vector<float> grp_mass_inv;
     std::vector<int> mask_plain(S), mask_thermo(S);
+    {
+        size_t n_all = 0, x_all = 0, e_all = 0;
+        for (const HostSystem &h : e->sys) {
+            n_all += h.d.n_atoms;
+            x_all += h.xl.size();
+            e_all += h.n_excess;
+        }
+        for (auto *v : {&atom_sys, &atom_type, &atom_group}) v->reserve(n_all);
+        for (auto *v : {&crd, &vel}) v->reserve(3 * n_all);
+        charge.reserve(n_all);
+        for (auto *v : {&charge_f, &mass, &mass_inv}) v->reserve(n_all);
+        excl_start.reserve(n_all + 1);
+        excl_list.reserve(x_all);
+        excess.reserve(e_all);
+        excess_sys.reserve(e_all);
+    }
     int atom_base = 0, col_base = 0, uni_base = 0, lj_base = 0, cells_cap = 0, nnc = 1;
     for (int k = 0; k < S; k++) {
         HostSystem &h = e->sys[k];

@@ -319,6 +319,12 @@ __device__ int enumerate_column(int c1, int nb, const SysDev &S, int cell_base,
     const int lc1 = c1 - cell_base;
     const int n_uni = S.n_columns * nuz;
     const unsigned v1 = cell_valid[c1];
+    double o1x = 0.0, o1y = 0.0, o1z = 0.0;
+    if (out_shift) {
+        o1x = cell_origin[3 * c1];
+        o1y = cell_origin[3 * c1 + 1];
+        o1z = cell_origin[3 * c1 + 2];
+    }
     int n = 0;
     for (int ii = 0; ii < 3; ii++) {
         const int iz = ii - 1;
@@ -362,10 +368,9 @@ __device__ int enumerate_column(int c1, int nb, const SysDev &S, int cell_base,
                     const double shx = ix == -1 ? -S.L[0] : (ix == 1 ? S.L[0] : 0.0);
                     const double shy = iy == -1 ? -S.L[1] : (iy == 1 ? S.L[1] : 0.0);
                     const double shz2 = iz == -1 ? -S.L[2] : (iz == 1 ? S.L[2] : 0.0);
-                    out_shift[n] = make_float4((float)(cell_origin[3 * c2] + shx - cell_origin[3 * c1]),
-                                               (float)(cell_origin[3 * c2 + 1] + shy - cell_origin[3 * c1 + 1]),
-                                               (float)(cell_origin[3 * c2 + 2] + shz2 - cell_origin[3 * c1 + 2]),
-                                               __int_as_float(c2));
+                    out_shift[n] = make_float4((float)(cell_origin[3 * c2] + shx - o1x),
+                                               (float)(cell_origin[3 * c2 + 1] + shy - o1y),
+                                               (float)(cell_origin[3 * c2 + 2] + shz2 - o1z), __int_as_float(c2));
                 }
             }
             n++;
