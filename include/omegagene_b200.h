@@ -50,7 +50,11 @@ typedef struct og_engine og_engine;
 #define OG_E_ELE_EXCESS 8 /* excluded-pair ZD part of OG_E_ELE */
 #define OG_E_ELE_SELF 9   /* constant self energy part of OG_E_ELE */
 #define OG_E_MCMD_FACTOR 10
-#define OG_N_ENERGY 11
+#define OG_E_TORSION 11
+#define OG_E_IMPROPER 12
+#define OG_E_VDW14 13     /* scaled 1-4 Lennard-Jones */
+#define OG_E_ELE14 14     /* scaled 1-4 Coulomb */
+#define OG_N_ENERGY 15    /* OG_E_POTENTIAL is the sum of VDW, ELE, BOND, ANGLE, TORSION, IMPROPER, VDW14, ELE14 */
 
 /*
  * One system.  Arrays are host pointers in original atom order, copied by og_add_system.
@@ -110,6 +114,31 @@ typedef struct {
      * nsgrid_update_intvl, so the heating schedule and the list-rebuild phase continue unchanged.
      * No counterpart in the reference, whose run always starts at step 0. */
     int64_t first_step;
+    /* Dihedrals, E = ene (1 + cos(symmetry phi - phase)) / overlaps (ForceField::calc_torsion,
+     * ForceField.cpp:179-300); torsions and impropers are reported separately. */
+    int32_t n_torsions;
+    const int32_t *torsion;          /* [4n] */
+    const double *torsion_ene, *torsion_phase;       /* [n] kcal/mol, rad */
+    const int32_t *torsion_overlaps, *torsion_symmetry; /* [n] */
+    int32_t n_impros;
+    const int32_t *impro;
+    const double *impro_ene, *impro_phase;
+    const int32_t *impro_overlaps, *impro_symmetry;
+    /* 1-4 pairs (ForceField::calc_14pair, ForceField.cpp:302-331): scaled LJ and Coulomb without a
+     * cutoff.  The factors are the ones the reference applies (its reader passes the .cls
+     * record's two factors swapped, Read.cpp:438 against MmSystem.cpp:395-401). */
+    int32_t n_nb14;
+    const int32_t *nb14;             /* [2n] atoms */
+    const int32_t *nb14_type;        /* [2n] 0-based LJ types */
+    const double *nb14_coeff_vdw, *nb14_coeff_ele; /* [n] */
+    /* SHAKE quads (ConstraintShake.cpp:151-276): centre + three partners; six distances in the
+     * pair order (0,1) (1,2) (2,0) (3,0) (2,3) (1,3). */
+    int32_t n_shake_quad;
+    const int32_t *shake_quad;       /* [4n] */
+    const double *shake_quad_dist;   /* [6n] A */
+    /* Added to the degrees of freedom: 3 when the .cls holds a position-restraint section, as
+     * Read.cpp:90-93 counts. */
+    int32_t dof_extra;
 } og_system_desc;
 
 /* Creates an engine on a CUDA device (cuda_set_device, cuda_setup.cu:1085-1093). */

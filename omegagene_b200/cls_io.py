@@ -6,9 +6,10 @@ section sizes in bytes, then the sections in header order.  Atom indices in the 
 angle, torsion, 1-4, 1-5-exclusion and constraint sections are 0-based; atom types,
 LJ type pairs and atom-group members are 1-based (Read.cpp:279, 306, 568).
 
-Sections the MD hot path does not use (torsions, impropers, 1-4 pairs, restraints, VcMD,
-group coordinates, potential tables) are kept as raw bytes so that a file read and
-written back is byte-identical.
+Torsions, impropers and 1-4 pairs are parsed (``torsions``, ``impros``, ``nb14``) and also kept
+as raw bytes; sections the MD path does not use (restraints, VcMD, group coordinates,
+potential tables) are kept as raw bytes only, so that a file read and written back is
+byte-identical.
 """
 import struct
 
@@ -61,6 +62,20 @@ class _Reader:
 BOND = np.dtype([("a1", "<i4"), ("a2", "<i4"), ("k", "<f8"), ("r0", "<f8")])
 ANGLE = np.dtype([("a1", "<i4"), ("a2", "<i4"), ("a3", "<i4"), ("k", "<f8"), ("t0", "<f8")])
 LJ = np.dtype([("t1", "<i4"), ("t2", "<i4"), ("p6", "<f8"), ("p12", "<f8")])
+# Read::load_ls_tpl torsion / improper records (Read.cpp:379-420): 4 atoms, energy, overlaps,
+# symmetry, phase, 1-4 flag; packed, 44 bytes
+DIHED = np.dtype([("a", "<i4", 4), ("ene", "<f8"), ("overlaps", "<i4"), ("symmetry", "<i4"), ("phase", "<f8"),
+                  ("flag14", "<i4")])
+# 1-4 pair records (Read.cpp:428-439): 2 atoms, 2 atom types (1-based), two scale factors
+NB14 = np.dtype([("a1", "<i4"), ("a2", "<i4"), ("t1", "<i4"), ("t2", "<i4"), ("f1", "<f8"), ("f2", "<f8")])
+
+
+def _parse_records(raw, dtype, what):
+    r = _Reader(raw)
+    n = r.i() if len(raw) >= 4 else 0
+    if len(raw) != 4 + dtype.itemsize * n:
+        raise ClsFormatError("inconsistent %s section" % what)
+    return r.rec(dtype, n)
 
 
 def _parse_topol(b, n_atoms):
@@ -89,6 +104,15 @@ def _parse_topol(b, n_atoms):
     for key in ("torsions_raw", "impros_raw", "nb14_raw"):
         size = r.i()
         t[key] = r.raw(size)
+    t["torsions"] = _parse_records(t["torsions_raw"], DIHED, "torsion")
+    t["impros"] = _parse_records(t["impros_raw"], DIHED, "improper")
+    nb14 = _parse_records(t["nb14_raw"], NB14, "1-4")
+    # MmSystem::set_nb14_param takes (coeff_vdw, coeff_ele) but Read.cpp:438 passes the record's
+    # second factor first: the factor the reference applies to the 1-4 van der Waals term is the
+    # record's second one, and the one it applies to the 1-4 electrostatics the first.
+    t["nb14"] = {"atoms": np.stack([nb14["a1"], nb14["a2"]], 1).astype(np.int32),
+                 "types": (np.stack([nb14["t1"], nb14["t2"]], 1) - 1).astype(np.int32),
+                 "coeff_vdw": nb14["f2"].copy(), "coeff_ele": nb14["f1"].copy()}
     size_15 = r.i()
     n15 = r.i()
     t["nb15off_pairs"] = r.i(2 * n15).reshape(n15, 2)
@@ -157,6 +181,9 @@ def read_cls(path):
     if r.o != len(buf):
         raise ClsFormatError("%s: trailing bytes" % path)
     out = {"version_len": ln, "raw": raw}
+    # Read::load_launch_set adds 3 degrees of freedom when a position-restraint section is
+    # present, whatever it holds (Read.cpp:90-93)
+    out["dof_extra"] = 3 if len(raw["pos_restraint"]) > 0 else 0
     if raw["box"]:
         out["pbc_val"] = np.frombuffer(raw["box"], dtype="<f8").copy()
     if raw["crd"]:

@@ -95,6 +95,12 @@ __global__ void k_thermo_rescale(int, const int *, const SysDev *, const int *, 
                                  const double *, double *);
 __global__ void k_thermo_crd(int, const int *, const SysDev *, const int *, double *, const double *,
                              const double *);
+__global__ void k_dihedrals(int, const int4 *, const double4 *, const int *, const SysDev *, const double *, const int *,
+                            unsigned long long *, double *);
+__global__ void k_nb14(int, const int2 *, const int2 *, const double2 *, const int *, const SysDev *, const double *,
+                       const float *, const float2 *, const int *, unsigned long long *, double *);
+__global__ void k_shake_quad(int, const int4 *, const double *, const int *, const SysDev *, const int *, const float *,
+                             double *, const double *, int, double, int *);
 __global__ void k_finish(int, const int *, const SysDev *, int, double *, const double *, const double *, double *,
                          const int *, double *, const double *, float4 *, const float *, double *, int *, int *);
 __global__ void k_slot_refresh(const int *, int, const int *, const double *, const double *, const float *,
@@ -127,6 +133,8 @@ struct HostSystem {
     int n_excess = 0;
     std::vector<int32_t> excess;  // pairs (i<j) in MmSystem::set_excess_pairs order, local ids
     std::vector<int32_t> xs, xl;  // exclusion partners per atom (CSR, insertion order), local ids
+    std::vector<int32_t> tq, tov, tsym, iq, iov, isym, p14, t14, qa;  // dihedrals, 1-4 pairs, SHAKE quads
+    std::vector<double> tene, tph, iene, iph, cv14, ce14, qd;
     int d_free = 0;
 };
 
@@ -193,6 +201,15 @@ struct og_engine {
     int4 *d_angle = nullptr;
     double2 *d_angle_kt = nullptr;
     double *d_e_angle = nullptr;
+    int4 *d_tors = nullptr, *d_impro = nullptr, *d_squad = nullptr;
+    double4 *d_tors_p = nullptr, *d_impro_p = nullptr;
+    int *d_tors_sys = nullptr, *d_impro_sys = nullptr, *d_nb14_sys = nullptr, *d_squad_sys = nullptr;
+    double *d_e_tors = nullptr, *d_e_impro = nullptr, *d_e_nb14 = nullptr, *d_squad_d2 = nullptr;
+    int2 *d_nb14 = nullptr, *d_nb14_t = nullptr;
+    double2 *d_nb14_c = nullptr;
+    int n_tors = 0, n_impro = 0, n_nb14 = 0, n_squad = 0;
+    int *d_seg_tors = nullptr, *d_seg_impro = nullptr, *d_seg_nb14 = nullptr;
+    int mc_tors = 1, mc_impro = 1, mc_nb14 = 1;
     int2 *d_spair = nullptr;
     int *d_spair_sys = nullptr;
     double *d_spair_d2 = nullptr;
@@ -628,6 +645,23 @@ og_status compute_forces(og_engine *e, bool vir, bool ene = true) {
                                                             e->d_crd, e->d_atom_slot, e->d_frc, e->d_e_angle);
         LAUNCH_CHECK();
     }
+    if (e->n_tors) {
+        k_dihedrals<<<blocks(e->n_tors, 128), 128, 0, st>>>(e->n_tors, e->d_tors, e->d_tors_p, e->d_tors_sys, e->d_sys,
+                                                             e->d_crd, e->d_atom_slot, e->d_frc, e->d_e_tors);
+        LAUNCH_CHECK();
+    }
+    if (e->n_impro) {
+        k_dihedrals<<<blocks(e->n_impro, 128), 128, 0, st>>>(e->n_impro, e->d_impro, e->d_impro_p, e->d_impro_sys,
+                                                              e->d_sys, e->d_crd, e->d_atom_slot, e->d_frc,
+                                                              e->d_e_impro);
+        LAUNCH_CHECK();
+    }
+    if (e->n_nb14) {
+        k_nb14<<<blocks(e->n_nb14, 128), 128, 0, st>>>(e->n_nb14, e->d_nb14, e->d_nb14_t, e->d_nb14_c, e->d_nb14_sys,
+                                                        e->d_sys, e->d_crd, e->d_charge_f, e->d_lj, e->d_atom_slot,
+                                                        e->d_frc, e->d_e_nb14);
+        LAUNCH_CHECK();
+    }
     k_collect_slots<<<blocks(e->slots_cap, 256), 256, 0, st>>>(e->d_counters, e->slots_cap, e->d_slot_atom, e->d_frc,
                                                                 e->d_work);
     LAUNCH_CHECK();
@@ -663,6 +697,15 @@ og_status reduce_potential(og_engine *e) {
         return s;
     if (e->n_angles && (s = seg_sum<1>(e, e->d_e_angle, 1, 0, e->d_seg_angle, e->mc_angle, e->d_sys_acc,
                                        OG_ACC_SIZE, OG_ACC_ANGLE, 0)))
+        return s;
+    if (e->n_tors && (s = seg_sum<1>(e, e->d_e_tors, 1, 0, e->d_seg_tors, e->mc_tors, e->d_sys_acc, OG_ACC_SIZE,
+                                     OG_ACC_TORSION, 0)))
+        return s;
+    if (e->n_impro && (s = seg_sum<1>(e, e->d_e_impro, 1, 0, e->d_seg_impro, e->mc_impro, e->d_sys_acc,
+                                      OG_ACC_SIZE, OG_ACC_IMPRO, 0)))
+        return s;
+    if (e->n_nb14 && (s = seg_sum<2>(e, e->d_e_nb14, 2, 0, e->d_seg_nb14, e->mc_nb14, e->d_sys_acc, OG_ACC_SIZE,
+                                     OG_ACC_VDW14, 0)))
         return s;
     k_mcmd_factor<<<blocks(e->n_sys, 128), 128, 0, e->stream>>>(e->n_sys, e->d_sys, e->d_sys_acc, e->d_mcmd);
     LAUNCH_CHECK();
@@ -709,6 +752,12 @@ og_status shake(og_engine *e, const int *active) {
         k_shake_trio<<<blocks(e->n_strio, 128), 128, 0, st>>>(e->n_strio, e->d_strio, e->d_strio_d2, e->d_sys,
                                                                active, e->d_mass_inv, e->d_crd, e->d_crd_prev,
                                                                e->shake_max_loops, e->shake_tol, e->d_counters);
+        LAUNCH_CHECK();
+    }
+    if (e->n_squad) {
+        k_shake_quad<<<blocks(e->n_squad, 64), 64, 0, st>>>(e->n_squad, e->d_squad, e->d_squad_d2, e->d_squad_sys,
+                                                             e->d_sys, active, e->d_mass_inv, e->d_crd, e->d_crd_prev,
+                                                             e->shake_max_loops, e->shake_tol, e->d_counters);
         LAUNCH_CHECK();
     }
     return OG_OK;
@@ -1091,6 +1140,48 @@ og_status og_add_system(og_engine *e, const og_system_desc *d, int32_t *sys_id) 
     cp(h.gstart, d->com_group_start, d->n_com_groups > 0 ? d->n_com_groups + 1 : 0);
     if (d->n_com_groups > 0) cp(h.gatoms, d->com_group_atoms, d->com_group_start[d->n_com_groups]);
     if (d->mcmd_order >= 0) cp(h.mcoef, d->mcmd_coef, d->mcmd_order + 1);
+    if ((d->n_torsions > 0 && (!d->torsion || !d->torsion_ene || !d->torsion_phase || !d->torsion_overlaps ||
+                               !d->torsion_symmetry)) ||
+        (d->n_impros > 0 && (!d->impro || !d->impro_ene || !d->impro_phase || !d->impro_overlaps ||
+                             !d->impro_symmetry)) ||
+        (d->n_nb14 > 0 && (!d->nb14 || !d->nb14_type || !d->nb14_coeff_vdw || !d->nb14_coeff_ele)) ||
+        (d->n_shake_quad > 0 && (!d->shake_quad || !d->shake_quad_dist)) || d->n_torsions < 0 || d->n_impros < 0 ||
+        d->n_nb14 < 0 || d->n_shake_quad < 0 || d->dof_extra < 0) {
+        e->sys.pop_back();
+        return fail(e, OG_ERR_INVALID, "dihedral, 1-4 or SHAKE-quad arrays missing or negative counts");
+    }
+    cp(h.tq, d->torsion, 4 * (size_t)d->n_torsions);
+    cp(h.tene, d->torsion_ene, d->n_torsions);
+    cp(h.tph, d->torsion_phase, d->n_torsions);
+    cp(h.tov, d->torsion_overlaps, d->n_torsions);
+    cp(h.tsym, d->torsion_symmetry, d->n_torsions);
+    cp(h.iq, d->impro, 4 * (size_t)d->n_impros);
+    cp(h.iene, d->impro_ene, d->n_impros);
+    cp(h.iph, d->impro_phase, d->n_impros);
+    cp(h.iov, d->impro_overlaps, d->n_impros);
+    cp(h.isym, d->impro_symmetry, d->n_impros);
+    cp(h.p14, d->nb14, 2 * (size_t)d->n_nb14);
+    cp(h.t14, d->nb14_type, 2 * (size_t)d->n_nb14);
+    cp(h.cv14, d->nb14_coeff_vdw, d->n_nb14);
+    cp(h.ce14, d->nb14_coeff_ele, d->n_nb14);
+    cp(h.qa, d->shake_quad, 4 * (size_t)d->n_shake_quad);
+    cp(h.qd, d->shake_quad_dist, 6 * (size_t)d->n_shake_quad);
+    {
+        auto bad_atoms = [n](const std::vector<int32_t> &v) {
+            for (int32_t a : v)
+                if (a < 0 || a >= n) return true;
+            return false;
+        };
+        bool bad = bad_atoms(h.tq) || bad_atoms(h.iq) || bad_atoms(h.p14) || bad_atoms(h.qa);
+        for (int32_t t : h.t14) bad |= t < 0 || t >= d->n_lj_types;
+        for (int32_t o : h.tov) bad |= o == 0;
+        for (int32_t o : h.iov) bad |= o == 0;
+        for (double q : h.qd) bad |= !(q > 0);
+        if (bad) {
+            e->sys.pop_back();
+            return fail(e, OG_ERR_INVALID, "dihedral, 1-4 or SHAKE-quad entry out of range");
+        }
+    }
     for (int i = 0; i < n; i++)
         if (h.type[i] < 0 || h.type[i] >= d->n_lj_types || !(h.mass[i] > 0)) {
             e->sys.pop_back();
@@ -1145,6 +1236,12 @@ og_status og_finalize(og_engine *e) {
     std::vector<double> spair_d2, strio_d2, thermo;
     std::vector<float> grp_mass_inv;
     std::vector<int> mask_plain(S), mask_thermo(S);
+    std::vector<int4> torsv, improv, squadv;
+    std::vector<double4> tors_p, impro_p;
+    std::vector<int> tors_sys, impro_sys, nb14_sys, squad_sys;
+    std::vector<int2> nb14v, nb14t;
+    std::vector<double2> nb14c;
+    std::vector<double> squad_d2;
     {
         size_t n_all = 0, x_all = 0, e_all = 0;
         for (const HostSystem &h : e->sys) {
@@ -1175,8 +1272,8 @@ og_status og_finalize(og_engine *e) {
         D.n_types = d.n_lj_types;
         D.dt = d.time_step;
         D.thermostat = d.thermostat;
-        D.has_constraints = (d.n_shake_pair + d.n_shake_trio) > 0;
-        h.d_free = 3 * n - 3 - (d.n_shake_pair + 3 * d.n_shake_trio);
+        D.has_constraints = (d.n_shake_pair + d.n_shake_trio + d.n_shake_quad) > 0;
+        h.d_free = 3 * n - 3 - (d.n_shake_pair + 3 * d.n_shake_trio + 6 * d.n_shake_quad) + d.dof_extra;
         if (h.d_free <= 0) return fail(e, OG_ERR_INVALID, "system %d has no degrees of freedom", k);
         D.temperature_coeff_thermo =
             (2.0 * OG_JOULE_CAL * 1e+3) / (OG_GAS_CONST * (double)h.d_free) * OG_KINETIC_COEFF;
@@ -1201,6 +1298,36 @@ og_status og_finalize(og_engine *e) {
         D.n_trio = d.n_shake_trio;
         D.pair_base = (int)spair.size();
         D.n_pair = d.n_shake_pair;
+        D.tors_base = (int)torsv.size();
+        D.n_tors = d.n_torsions;
+        D.impro_base = (int)improv.size();
+        D.n_impro = d.n_impros;
+        D.nb14_base = (int)nb14v.size();
+        D.n_nb14 = d.n_nb14;
+        for (int q = 0; q < d.n_torsions; q++) {
+            torsv.push_back(make_int4(atom_base + h.tq[4 * q], atom_base + h.tq[4 * q + 1], atom_base + h.tq[4 * q + 2],
+                                      atom_base + h.tq[4 * q + 3]));
+            tors_p.push_back(make_double4(h.tene[q], h.tph[q], (double)h.tov[q], (double)h.tsym[q]));
+            tors_sys.push_back(k);
+        }
+        for (int q = 0; q < d.n_impros; q++) {
+            improv.push_back(make_int4(atom_base + h.iq[4 * q], atom_base + h.iq[4 * q + 1], atom_base + h.iq[4 * q + 2],
+                                       atom_base + h.iq[4 * q + 3]));
+            impro_p.push_back(make_double4(h.iene[q], h.iph[q], (double)h.iov[q], (double)h.isym[q]));
+            impro_sys.push_back(k);
+        }
+        for (int q = 0; q < d.n_nb14; q++) {
+            nb14v.push_back(make_int2(atom_base + h.p14[2 * q], atom_base + h.p14[2 * q + 1]));
+            nb14t.push_back(make_int2(h.t14[2 * q], h.t14[2 * q + 1]));
+            nb14c.push_back(make_double2(h.cv14[q], h.ce14[q]));
+            nb14_sys.push_back(k);
+        }
+        for (int q = 0; q < d.n_shake_quad; q++) {
+            squadv.push_back(make_int4(atom_base + h.qa[4 * q], atom_base + h.qa[4 * q + 1], atom_base + h.qa[4 * q + 2],
+                                       atom_base + h.qa[4 * q + 3]));
+            for (int r = 0; r < 6; r++) squad_d2.push_back(h.qd[6 * q + r] * h.qd[6 * q + r]);
+            squad_sys.push_back(k);
+        }
         thermo.push_back(d.temperature);
         thermo.push_back(d.temperature_init < 0 ? d.temperature : d.temperature_init);
         thermo.push_back((double)d.heating_steps);
@@ -1210,7 +1337,7 @@ og_status og_finalize(og_engine *e) {
         e->any_plain_cons |= mask_plain[k] != 0;
         e->any_thermo_cons |= mask_thermo[k] != 0;
         e->any_thermo_free |= (!D.has_constraints && d.thermostat == OG_THERMOSTAT_SCALING);
-        if (d.n_shake_trio || d.n_shake_pair) {
+        if (d.n_shake_trio || d.n_shake_pair || d.n_shake_quad) {
             e->shake_max_loops = d.const_max_loops > 0 ? d.const_max_loops : 1000;
             e->shake_tol = d.const_tolerance > 0 ? d.const_tolerance : 1e-7;
         }
@@ -1300,6 +1427,10 @@ og_status og_finalize(og_engine *e) {
     e->n_angles = (int)anglev.size();
     e->n_spair = (int)spair.size();
     e->n_strio = (int)strio.size();
+    e->n_tors = (int)torsv.size();
+    e->n_impro = (int)improv.size();
+    e->n_nb14 = (int)nb14v.size();
+    e->n_squad = (int)squadv.size();
     e->n_groups = (int)grp_mass_inv.size();
     e->any_groups = e->n_groups > 0;
     // ---- allocation + upload
@@ -1336,11 +1467,19 @@ og_status og_finalize(og_engine *e) {
         (s = dalloc(e, &e->d_e_angle, anglev.size())) || (s = upload(e, &e->d_spair, spair)) ||
         (s = upload(e, &e->d_spair_sys, spair_sys)) || (s = upload(e, &e->d_spair_d2, spair_d2)) ||
         (s = upload(e, &e->d_strio, strio)) || (s = upload(e, &e->d_strio_d2, strio_d2)) ||
+        (s = upload(e, &e->d_tors, torsv)) || (s = upload(e, &e->d_tors_p, tors_p)) ||
+        (s = upload(e, &e->d_tors_sys, tors_sys)) || (s = dalloc(e, &e->d_e_tors, torsv.size())) ||
+        (s = upload(e, &e->d_impro, improv)) || (s = upload(e, &e->d_impro_p, impro_p)) ||
+        (s = upload(e, &e->d_impro_sys, impro_sys)) || (s = dalloc(e, &e->d_e_impro, improv.size())) ||
+        (s = upload(e, &e->d_nb14, nb14v)) || (s = upload(e, &e->d_nb14_t, nb14t)) ||
+        (s = upload(e, &e->d_nb14_c, nb14c)) || (s = upload(e, &e->d_nb14_sys, nb14_sys)) ||
+        (s = dalloc(e, &e->d_e_nb14, 2 * nb14v.size())) || (s = upload(e, &e->d_squad, squadv)) ||
+        (s = upload(e, &e->d_squad_d2, squad_d2)) || (s = upload(e, &e->d_squad_sys, squad_sys)) ||
         (s = upload(e, &e->d_grp_start, grp_start)) || (s = upload(e, &e->d_grp_atoms, grp_atoms)) ||
         (s = upload(e, &e->d_grp_sys, grp_sys)) || (s = upload(e, &e->d_grp_mass_inv, grp_mass_inv)) ||
         (s = dalloc(e, &e->d_moment, 3 * (size_t)(e->n_groups + 1))) || (s = upload(e, &e->d_lj, lj)) ||
         (s = dalloc(e, &e->d_sys_acc, OG_ACC_SIZE * (size_t)S)) || (s = dalloc(e, &e->d_mcmd, S)) ||
-        (s = dalloc(e, &e->d_energies, 11 * (size_t)S)) || (s = upload(e, &e->d_thermo, thermo)) ||
+        (s = dalloc(e, &e->d_energies, OG_N_ENERGY * (size_t)S)) || (s = upload(e, &e->d_thermo, thermo)) ||
         (s = dalloc(e, &e->d_sum_tmp, S)) || (s = upload(e, &e->d_mask_plain, mask_plain)) ||
         (s = upload(e, &e->d_mask_thermo, mask_thermo)) || (s = dalloc(e, &e->d_active, S)) ||
         (s = dalloc(e, &e->d_any, 1)) || (s = dalloc(e, &e->d_thermo_it, 1)) ||
@@ -1348,15 +1487,21 @@ og_status og_finalize(og_engine *e) {
         (s = dalloc(e, &e->d_cell_excl, (size_t)OG_CELL_EXCL * cells_cap)))
         return s;
     {
-        std::vector<int> sa(S + 1), se(S + 1), sb(S + 1), sg(S + 1);
-        int ma = 1, mcl = 1, me = 1, mb = 1, mg = 1;
+        std::vector<int> sa(S + 1), se(S + 1), sb(S + 1), sg(S + 1), st(S + 1), si(S + 1), s14(S + 1);
+        int ma = 1, mcl = 1, me = 1, mb = 1, mg = 1, mt = 1, mi = 1, m14 = 1;
         for (int k = 0; k < S; k++) {
             const SysDev &D = sd[k];
             sa[k] = D.atom_base;
             se[k] = D.excess_base;
             sb[k] = D.bond_base;
             sg[k] = D.angle_base;
+            st[k] = D.tors_base;
+            si[k] = D.impro_base;
+            s14[k] = D.nb14_base;
             auto ch = [](long long n) { return (int)((n + 4095) / 4096); };
+            mt = std::max(mt, ch(D.n_tors));
+            mi = std::max(mi, ch(D.n_impro));
+            m14 = std::max(m14, ch(D.n_nb14));
             ma = std::max(ma, ch(D.n_atoms));
             mcl = std::max(mcl, ch(D.n_atoms / OG_CELL + D.n_columns + 1));
             me = std::max(me, ch(D.n_excess));
@@ -1367,6 +1512,12 @@ og_status og_finalize(og_engine *e) {
         se[S] = (int)excess.size();
         sb[S] = (int)bondv.size();
         sg[S] = (int)anglev.size();
+        st[S] = (int)torsv.size();
+        si[S] = (int)improv.size();
+        s14[S] = (int)nb14v.size();
+        e->mc_tors = mt;
+        e->mc_impro = mi;
+        e->mc_nb14 = m14;
         int mgr = 1;
         for (int g = 0; g < e->n_groups; g++) mgr = std::max(mgr, (grp_start[g + 1] - grp_start[g] + 4095) / 4096);
         e->mc_atoms = ma;
@@ -1375,10 +1526,14 @@ og_status og_finalize(og_engine *e) {
         e->mc_bond = mb;
         e->mc_angle = mg;
         e->mc_grp = mgr;
-        size_t part = (size_t)S * std::max(std::max(ma, mcl), std::max(me, std::max(mb, mg))) * 10;
+        size_t part = (size_t)S *
+                      std::max(std::max(std::max(ma, mcl), std::max(me, std::max(mb, mg))),
+                               std::max(mt, std::max(mi, m14))) * 10;
         part = std::max(part, (size_t)(e->n_groups + 1) * mgr * 3);
         if ((s = upload(e, &e->d_seg_atoms, sa)) || (s = upload(e, &e->d_seg_exc, se)) ||
             (s = upload(e, &e->d_seg_bond, sb)) || (s = upload(e, &e->d_seg_angle, sg)) ||
+            (s = upload(e, &e->d_seg_tors, st)) || (s = upload(e, &e->d_seg_impro, si)) ||
+            (s = upload(e, &e->d_seg_nb14, s14)) ||
             (s = dalloc(e, &e->d_part, part)))
             return s;
     }
@@ -1566,7 +1721,13 @@ og_status og_get_forces(og_engine *e, int32_t sys, double *work, double *energie
         energies[OG_E_ELE] = acc[OG_ACC_ELE] + acc[OG_ACC_EXCESS] + D.self_energy;
         energies[OG_E_BOND] = acc[OG_ACC_BOND];
         energies[OG_E_ANGLE] = acc[OG_ACC_ANGLE];
-        energies[OG_E_POTENTIAL] = energies[0] + energies[1] + energies[2] + energies[3];
+        energies[OG_E_TORSION] = acc[OG_ACC_TORSION];
+        energies[OG_E_IMPROPER] = acc[OG_ACC_IMPRO];
+        energies[OG_E_VDW14] = acc[OG_ACC_VDW14];
+        energies[OG_E_ELE14] = acc[OG_ACC_ELE14];
+        energies[OG_E_POTENTIAL] = energies[OG_E_VDW] + energies[OG_E_ELE] + energies[OG_E_BOND] + energies[OG_E_ANGLE] +
+                                   energies[OG_E_TORSION] + energies[OG_E_IMPROPER] + energies[OG_E_VDW14] +
+                                   energies[OG_E_ELE14];
         energies[OG_E_ELE_EXCESS] = acc[OG_ACC_EXCESS];
         energies[OG_E_ELE_SELF] = D.self_energy;
     }
@@ -1578,7 +1739,7 @@ og_status og_get_forces(og_engine *e, int32_t sys, double *work, double *energie
 og_status og_get_energies(og_engine *e, int32_t sys, double *energies) {
     if (!e || !e->finalized) return fail(e, OG_ERR_STATE, "og_get_energies before og_finalize");
     if (sys < 0 || sys >= e->n_sys || !energies) return fail(e, OG_ERR_INVALID, "bad arguments");
-    CK(cudaMemcpyAsync(energies, e->d_energies + 11 * (size_t)sys, sizeof(double) * OG_N_ENERGY,
+    CK(cudaMemcpyAsync(energies, e->d_energies + OG_N_ENERGY * (size_t)sys, sizeof(double) * OG_N_ENERGY,
                        cudaMemcpyDeviceToHost, e->stream));
     CK(cudaStreamSynchronize(e->stream));
     return OG_OK;
@@ -1756,7 +1917,7 @@ extern "C" og_status og_get_state_async(og_engine *e, int32_t sys, double *crd, 
         CK(cudaMemcpyAsync(vel_next, e->d_vel_next + 3 * (size_t)D.atom_base, sizeof(double) * 3 * D.n_atoms,
                            cudaMemcpyDeviceToHost, e->stream));
     if (energies)
-        CK(cudaMemcpyAsync(energies, e->d_energies + 11 * (size_t)sys, sizeof(double) * OG_N_ENERGY,
+        CK(cudaMemcpyAsync(energies, e->d_energies + OG_N_ENERGY * (size_t)sys, sizeof(double) * OG_N_ENERGY,
                            cudaMemcpyDeviceToHost, e->stream));
     return OG_OK;
 }

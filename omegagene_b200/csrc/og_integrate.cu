@@ -104,6 +104,111 @@ __global__ void k_angles(int n, const int4 *__restrict__ a, const double2 *__res
     add_fix(frc + 3 * (size_t)atom_slot[l], w2[0], w2[1], w2[2]);
 }
 
+__device__ __forceinline__ void cross3(const double a[3], const double b[3], double c[3]) {
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// Dihedral terms, E = ene (1 + cos(n phi - phase)) / overlaps, in FP64 (ForceField::calc_torsion,
+// ForceField.cpp:179-300, applied as SubBox::calc_energy_torsions / calc_energy_impros,
+// SubBox.cpp:1273-1320); one launch for torsions and one for impropers.  prm[k] = (ene, phase,
+// overlaps, symmetry).  The reference's PI (CelesteObject.cpp:27) and its table of 2k for even
+// multiplicities (ForceField.cpp:7-17) are part of the arithmetic.
+__global__ void k_dihedrals(int n, const int4 *__restrict__ q4, const double4 *__restrict__ prm,
+                            const int *__restrict__ dsys, const SysDev *__restrict__ sys,
+                            const double *__restrict__ crd, const int *__restrict__ atom_slot,
+                            unsigned long long *__restrict__ frc, double *__restrict__ e_out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const SysDev &S = sys[dsys[k]];
+    const int a1 = q4[k].x, a2 = q4[k].y, a3 = q4[k].z, a4 = q4[k].w;
+    const double4 P = prm[k];
+    double w1[3] = {0, 0, 0}, w2[3] = {0, 0, 0}, w3[3] = {0, 0, 0}, e = 0.0;
+    if (P.x > 1e-10) {
+        double d21[3], d32[3], d43[3], p12[3], p23[3], p123[3];
+        for (int q = 0; q < 3; q++) {
+            d21[q] = minim(crd[3 * a2 + q] - crd[3 * a1 + q], S.Lf[q], S.L_half_inv_f[q]);
+            d32[q] = minim(crd[3 * a3 + q] - crd[3 * a2 + q], S.Lf[q], S.L_half_inv_f[q]);
+            d43[q] = minim(crd[3 * a4 + q] - crd[3 * a3 + q], S.Lf[q], S.L_half_inv_f[q]);
+        }
+        cross3(d21, d32, p12);
+        cross3(d32, d43, p23);
+        const double p12_2 = p12[0] * p12[0] + p12[1] * p12[1] + p12[2] * p12[2];
+        const double p23_2 = p23[0] * p23[0] + p23[1] * p23[1] + p23[2] * p23[2];
+        const double p12p23 = sqrt(p12_2 * p23_2);
+        if (p12p23 > 0.0) {
+            const double inv = 1.0 / p12p23;
+            const double s1223 = p12[0] * p23[0] + p12[1] * p23[1] + p12[2] * p23[2];
+            const double cosp = fmax(-1.0, fmin(1.0, s1223 * inv));
+            cross3(p12, p23, p123);
+            double phi = acos(cosp);
+            if (d32[0] * p123[0] + d32[1] * p123[1] + d32[2] * p123[2] < 0.0) phi = 2.0 * 3.14159265 - phi;
+            const double sym = P.w, div = 1.0 / P.z;
+            e = P.x * (1.0 + cos(sym * phi - P.y)) * div;
+            const int nrot = (int)sym;
+            const double gm = (nrot >= 0 && nrot <= 10 && nrot % 2 == 0) ? (double)nrot : 0.0;
+            const double sinp = sin(phi);
+            const double sf = sin(P.y), cf = cos(P.y), sr = sin(sym * phi), cr = cos(sym * phi);
+            const double dflim = cf * (sym - gm + gm * cosp);
+            const double df0 = cf * sr - sf * cr;
+            const double df1 = (1e-10 <= fabs(sinp)) ? df0 / sinp : dflim;
+            const double wc = sym * P.x * div * df1 * inv;
+            const double r12 = 1.0 / p12_2 * s1223, r23 = 1.0 / p23_2 * s1223;
+            double a[3], b[3], c[3], dd[3];
+            cross3(p23, d32, a);
+            cross3(p12, d32, b);
+            for (int i = 0; i < 3; i++) w1[i] = wc * (a[i] - r12 * b[i]);
+            const double d2132[3] = {d21[0] + d32[0], d21[1] + d32[1], d21[2] + d32[2]};
+            cross3(d2132, p23, a);
+            cross3(d2132, p12, b);
+            cross3(p12, d43, c);
+            cross3(p23, d43, dd);
+            for (int i = 0; i < 3; i++) w2[i] = wc * (a[i] + c[i] - r12 * b[i] - r23 * dd[i]);
+            cross3(p12, d32, a);
+            cross3(p23, d32, b);
+            for (int i = 0; i < 3; i++) w3[i] = wc * (a[i] - r23 * b[i]);
+        }
+    }
+    e_out[k] = e;
+    add_fix(frc + 3 * (size_t)atom_slot[a1], w1[0], w1[1], w1[2]);
+    add_fix(frc + 3 * (size_t)atom_slot[a2], w2[0], w2[1], w2[2]);
+    add_fix(frc + 3 * (size_t)atom_slot[a3], -(w1[0] + w2[0] + w3[0]), -(w1[1] + w2[1] + w3[1]),
+            -(w1[2] + w2[2] + w3[2]));
+    add_fix(frc + 3 * (size_t)atom_slot[a4], w3[0], w3[1], w3[2]);
+}
+
+// 1-4 pairs (ForceField::calc_14pair, ForceField.cpp:302-331, via SubBox::calc_energy_14nb,
+// SubBox.cpp:1321-1345): scaled LJ and Coulomb without cutoff, FP64 on the reference's float
+// charges and LJ terms.  e_out[2k] = vdw, e_out[2k+1] = ele.
+__global__ void k_nb14(int n, const int2 *__restrict__ pr, const int2 *__restrict__ ty,
+                       const double2 *__restrict__ coef, const int *__restrict__ psys,
+                       const SysDev *__restrict__ sys, const double *__restrict__ crd,
+                       const float *__restrict__ charge_f, const float2 *__restrict__ lj,
+                       const int *__restrict__ atom_slot, unsigned long long *__restrict__ frc,
+                       double *__restrict__ e_out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const SysDev &S = sys[psys[k]];
+    const int i = pr[k].x, j = pr[k].y;
+    double d[3];
+    for (int q = 0; q < 3; q++) d[q] = minim(crd[3 * i + q] - crd[3 * j + q], S.Lf[q], S.L_half_inv_f[q]);
+    const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    const double r2i = 1.0 / r2, ri = sqrt(r2i);
+    const double r6i = r2i * r2i * r2i, r12i = r6i * r6i;
+    const float2 p = lj[S.lj_base + ty[k].x * S.n_types + ty[k].y];
+    const double t6 = (double)p.x * r6i, t12 = (double)p.y * r12i;
+    const double cv = coef[k].x, ce = coef[k].y;
+    e_out[2 * k] = (-t6 + t12) * cv;
+    const double cw = r2i * cv * (-12.0 * t12 + 6.0 * t6);
+    const double cc = (double)charge_f[i] * (double)charge_f[j] * OG_CHARGE_COEFF * ce;
+    e_out[2 * k + 1] = cc * ri;
+    const double cel = -cc * r2i * ri;
+    const double w[3] = {cw * d[0] + cel * d[0], cw * d[1] + cel * d[1], cw * d[2] + cel * d[2]};
+    add_fix(frc + 3 * (size_t)atom_slot[i], w[0], w[1], w[2]);
+    add_fix(frc + 3 * (size_t)atom_slot[j], -w[0], -w[1], -w[2]);
+}
+
 // Per-atom x (x) F of the pair forces alone (virial, single-sum form); positions are the
 // cell-relative coordinates the pair kernel used plus their cell origin.
 __global__ void k_atom_virial(int n_atoms, const int *__restrict__ atom_slot,
@@ -237,7 +342,8 @@ __global__ void k_mcmd_factor(int n_sys, const SysDev *__restrict__ sys, const d
     double f = 1.0;
     if (S.mcmd_order >= 0) {
         const double lambda = acc[OG_ACC_VDW] + acc[OG_ACC_ELE] + acc[OG_ACC_EXCESS] + S.self_energy +
-                              acc[OG_ACC_BOND] + acc[OG_ACC_ANGLE];
+                              acc[OG_ACC_BOND] + acc[OG_ACC_ANGLE] + acc[OG_ACC_TORSION] + acc[OG_ACC_IMPRO] +
+                              acc[OG_ACC_VDW14] + acc[OG_ACC_ELE14];
         double param = lambda;
         if (lambda <= S.mcmd_lo) param = S.mcmd_lo;
         else if (lambda >= S.mcmd_hi) param = S.mcmd_hi;
@@ -483,6 +589,107 @@ __global__ void k_thermo_check(int n_sys, const SysDev *__restrict__ sys, const 
     atomicAdd(any, 1);
 }
 
+// ConstraintShake::shake_quad (ConstraintShake.cpp:151-276): a centre and three partners, six
+// squared distances in the pair order (0,1) (1,2) (2,0) (3,0) (2,3) (1,3) (Constraint.cpp:4),
+// Newton steps solved with ConstraintObject::calc_linear_eq's elimination (Constraint.cpp:141).
+__device__ int og_solve6(double a[6][6], double x[6], const double b[6]) {
+    int piv[6] = {0, 1, 2, 3, 4, 5};
+    for (int i = 0; i < 6; i++) {
+        int idx = i;
+        double mx = fabs(a[i][piv[i]]);
+        for (int j = i + 1; j < 6; j++) {
+            const double t = fabs(a[i][piv[j]]);
+            if (t > mx) { idx = j; mx = t; }
+        }
+        if (idx != i) { const int t = piv[i]; piv[i] = piv[idx]; piv[idx] = t; }
+        if (fabs(a[i][piv[i]]) < 1e-30) return 1;
+        a[i][piv[i]] = 1.0 / a[i][piv[i]];
+        for (int j = i + 1; j < 6; j++) {
+            a[i][piv[j]] *= a[i][piv[i]];
+            for (int k = i + 1; k < 6; k++) a[k][piv[j]] -= a[i][piv[j]] * a[k][piv[i]];
+        }
+    }
+    for (int i = 0; i < 6; i++) {
+        double v = b[piv[i]];
+        for (int j = 0; j < i; j++) v -= a[j][piv[i]] * x[j];
+        x[i] = v;
+    }
+    for (int i = 5; i >= 0; i--) {
+        double v = x[i];
+        for (int j = i + 1; j < 6; j++) v -= a[j][piv[i]] * x[j];
+        x[i] = v * a[i][piv[i]];
+    }
+    return 0;
+}
+
+__global__ void k_shake_quad(int n, const int4 *__restrict__ q4, const double *__restrict__ qd,
+                             const int *__restrict__ qsys, const SysDev *__restrict__ sys,
+                             const int *__restrict__ sys_active, const float *__restrict__ mass_inv,
+                             double *__restrict__ crd, const double *__restrict__ crd_prev, int max_loops,
+                             double tol, int *__restrict__ counters) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int s = qsys[k];
+    if (sys_active && !sys_active[s]) return;
+    const SysDev &S = sys[s];
+    const int at[4] = {q4[k].x, q4[k].y, q4[k].z, q4[k].w};
+    const int P[6][2] = {{0, 1}, {1, 2}, {2, 0}, {3, 0}, {2, 3}, {1, 3}};
+    double mi[4];
+    for (int i = 0; i < 4; i++) mi[i] = (double)mass_inv[at[i]];
+    const double w[6][6] = {{mi[0] + mi[1], -mi[1], -mi[0], -mi[0], 0.0, -mi[1]},
+                            {-mi[1], mi[1] + mi[2], -mi[2], 0.0, -mi[2], mi[1]},
+                            {-mi[0], -mi[2], mi[2] + mi[0], mi[0], mi[2], 0.0},
+                            {-mi[0], 0.0, mi[0], mi[3] + mi[0], -mi[3], -mi[3]},
+                            {0.0, -mi[2], mi[2], -mi[3], mi[2] + mi[3], mi[3]},
+                            {-mi[1], mi[1], 0.0, -mi[3], mi[3], mi[1] + mi[3]}};
+    double dc[6][3], dp[6][3];
+    for (int c = 0; c < 6; c++)
+        for (int q = 0; q < 3; q++) {
+            dc[c][q] = minim(crd[3 * at[P[c][0]] + q] - crd[3 * at[P[c][1]] + q], S.Lf[q], S.L_half_inv_f[q]);
+            dp[c][q] = minim(crd_prev[3 * at[P[c][0]] + q] - crd_prev[3 * at[P[c][1]] + q], S.Lf[q],
+                             S.L_half_inv_f[q]);
+        }
+    const double *d2 = qd + 6 * (size_t)k;
+    double coef[6] = {0, 0, 0, 0, 0, 0}, post[6] = {0, 0, 0, 0, 0, 0};
+    bool conv = false;
+    for (int it = 0; it < max_loops; it++) {
+        for (int c = 0; c < 6; c++) coef[c] = post[c];
+        double dv[6][3];
+        for (int i = 0; i < 6; i++) {
+            for (int q = 0; q < 3; q++) dv[i][q] = dc[i][q];
+            for (int j = 0; j < 6; j++)
+                for (int q = 0; q < 3; q++) dv[i][q] += w[j][i] * dp[j][q] * coef[j];
+        }
+        double g[6][6];
+        for (int i = 0; i < 6; i++)
+            for (int j = 0; j < 6; j++)
+                g[i][j] = 2.0 * w[j][i] * (dv[j][0] * dp[i][0] + dv[j][1] * dp[i][1] + dv[j][2] * dp[i][2]);
+        bool ok = true;
+        double sd[6];
+        for (int i = 0; i < 6; i++) {
+            sd[i] = d2[i] - (dv[i][0] * dv[i][0] + dv[i][1] * dv[i][1] + dv[i][2] * dv[i][2]);
+            ok = ok && (fabs(sd[i] / d2[i]) < tol);
+        }
+        if (ok) {
+            conv = true;
+            break;
+        }
+        double rhs[6];
+        for (int i = 0; i < 6; i++) {
+            rhs[i] = sd[i];
+            for (int j = 0; j < 6; j++) rhs[i] += g[j][i] * coef[j];
+        }
+        og_solve6(g, post, rhs);
+    }
+    if (!conv) og_set_flag(counters, OG_FLAG_SHAKE);
+    for (int q = 0; q < 3; q++) {
+        crd[3 * at[0] + q] += mi[0] * (coef[0] * dp[0][q] - coef[2] * dp[2][q] - coef[3] * dp[3][q]);
+        crd[3 * at[1] + q] += mi[1] * (-coef[0] * dp[0][q] + coef[1] * dp[1][q] + coef[5] * dp[5][q]);
+        crd[3 * at[2] + q] += mi[2] * (-coef[1] * dp[1][q] + coef[2] * dp[2][q] + coef[4] * dp[4][q]);
+        crd[3 * at[3] + q] += mi[3] * (coef[3] * dp[3][q] - coef[4] * dp[4][q] - coef[5] * dp[5][q]);
+    }
+}
+
 // Half-step velocities with the constraint acceleration (Thermostat.cpp:133-148).
 __global__ void k_thermo_half(int n_atoms, const int *__restrict__ atom_sys, const SysDev *__restrict__ sys,
                               const int *__restrict__ sys_active, const double *__restrict__ work,
@@ -610,21 +817,26 @@ __global__ void k_energies(int n_sys, const SysDev *__restrict__ sys, const doub
     if (s >= n_sys) return;
     const SysDev &S = sys[s];
     const double *acc = sys_acc + OG_ACC_SIZE * s;
-    double *e = energies + 11 * s;
-    e[0] = acc[OG_ACC_VDW];
-    e[1] = acc[OG_ACC_ELE] + acc[OG_ACC_EXCESS] + S.self_energy;
-    e[2] = acc[OG_ACC_BOND];
-    e[3] = acc[OG_ACC_ANGLE];
-    e[4] = e[0] + e[1] + e[2] + e[3];
-    e[5] = acc[OG_ACC_KIN] * OG_KINETIC_COEFF;
-    e[6] = e[5] * S.temperature_coeff_dyn;
-    e[7] = e[4] + e[5];
-    e[8] = acc[OG_ACC_EXCESS];
-    e[9] = S.self_energy;
-    e[10] = mcmd_factor[s];
+    double *e = energies + OG_N_ENERGY * s;
+    e[OG_E_VDW] = acc[OG_ACC_VDW];
+    e[OG_E_ELE] = acc[OG_ACC_ELE] + acc[OG_ACC_EXCESS] + S.self_energy;
+    e[OG_E_BOND] = acc[OG_ACC_BOND];
+    e[OG_E_ANGLE] = acc[OG_ACC_ANGLE];
+    e[OG_E_TORSION] = acc[OG_ACC_TORSION];
+    e[OG_E_IMPROPER] = acc[OG_ACC_IMPRO];
+    e[OG_E_VDW14] = acc[OG_ACC_VDW14];
+    e[OG_E_ELE14] = acc[OG_ACC_ELE14];
+    e[OG_E_POTENTIAL] = e[OG_E_VDW] + e[OG_E_ELE] + e[OG_E_BOND] + e[OG_E_ANGLE] + e[OG_E_TORSION] +
+                        e[OG_E_IMPROPER] + e[OG_E_VDW14] + e[OG_E_ELE14];
+    e[OG_E_KINETIC] = acc[OG_ACC_KIN] * OG_KINETIC_COEFF;
+    e[OG_E_TEMPERATURE] = e[OG_E_KINETIC] * S.temperature_coeff_dyn;
+    e[OG_E_TOTAL] = e[OG_E_POTENTIAL] + e[OG_E_KINETIC];
+    e[OG_E_ELE_EXCESS] = acc[OG_ACC_EXCESS];
+    e[OG_E_ELE_SELF] = S.self_energy;
+    e[OG_E_MCMD_FACTOR] = mcmd_factor[s];
     if (trace && trace_cap > 0) {
         const long long row = *trace_count % trace_cap;
-        for (int q = 0; q < 11; q++) trace[(row * n_sys + s) * 11 + q] = e[q];
+        for (int q = 0; q < OG_N_ENERGY; q++) trace[(row * n_sys + s) * OG_N_ENERGY + q] = e[q];
     }
 }
 

@@ -14,6 +14,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "../../include/omegagene_b200.h"
+
 #define OG_CELL 8
 #define OG_MAX_COLUMN_ATOMS 4096     // per-column sort capacity (shared memory)
 #define OG_CELL_EXCL 32              // per-cell exclusion row: count + up to 31 (cell, bit) entries
@@ -75,6 +77,7 @@ struct SysDev {
     // constraint / term ranges (global index spaces of their own arrays)
     int trio_base, n_trio, pair_base, n_pair;
     int excess_base, n_excess, bond_base, n_bonds, angle_base, n_angles;
+    int tors_base, n_tors, impro_base, n_impro, nb14_base, n_nb14;
 };
 
 // per-system reduction slots in d_sys_acc (double)
@@ -86,7 +89,11 @@ struct SysDev {
 #define OG_ACC_KIN 5
 #define OG_ACC_VIR 6     // 9 entries
 #define OG_ACC_PAIRS 15  // interacting pair count of the last virial-mode evaluation
-#define OG_ACC_SIZE 16
+#define OG_ACC_TORSION 16
+#define OG_ACC_IMPRO 17
+#define OG_ACC_VDW14 18
+#define OG_ACC_ELE14 19
+#define OG_ACC_SIZE 20
 // per-cell accumulator slots written by the pair kernel: vdw, ele, virial[9], pair count
 #define OG_CELL_ACC 12
 

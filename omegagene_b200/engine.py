@@ -21,7 +21,7 @@ LIB_PATH = os.path.join(HERE, "libomegagene_b200.so")
 (OG_OK, OG_ERR_INVALID, OG_ERR_CUDA, OG_ERR_CAPACITY, OG_ERR_STATE, OG_ERR_NOMEM, OG_ERR_NOT_CONVERGED,
  OG_ERR_SYSTEM_FAULT) = range(8)
 ENERGY_NAMES = ["vdw", "ele", "bond", "angle", "potential", "kinetic", "temperature", "total", "ele_excess",
-                "ele_self", "mcmd_factor"]
+                "ele_self", "mcmd_factor", "torsion", "improper", "vdw14", "ele14"]
 N_ENERGY = len(ENERGY_NAMES)
 N_PAIR_VARIANTS = 10  # OG_N_PAIR_VARIANTS
 
@@ -54,6 +54,14 @@ class SystemDesc(C.Structure):
         ("mcmd_order", C.c_int32), ("mcmd_lambda_low", C.c_double), ("mcmd_lambda_high", C.c_double),
         ("mcmd_temperature", C.c_double), ("mcmd_coef", _p(C.c_double)),
         ("first_step", C.c_int64),
+        ("n_torsions", C.c_int32), ("torsion", _p(C.c_int32)), ("torsion_ene", _p(C.c_double)),
+        ("torsion_phase", _p(C.c_double)), ("torsion_overlaps", _p(C.c_int32)), ("torsion_symmetry", _p(C.c_int32)),
+        ("n_impros", C.c_int32), ("impro", _p(C.c_int32)), ("impro_ene", _p(C.c_double)),
+        ("impro_phase", _p(C.c_double)), ("impro_overlaps", _p(C.c_int32)), ("impro_symmetry", _p(C.c_int32)),
+        ("n_nb14", C.c_int32), ("nb14", _p(C.c_int32)), ("nb14_type", _p(C.c_int32)),
+        ("nb14_coeff_vdw", _p(C.c_double)), ("nb14_coeff_ele", _p(C.c_double)),
+        ("n_shake_quad", C.c_int32), ("shake_quad", _p(C.c_int32)), ("shake_quad_dist", _p(C.c_double)),
+        ("dof_extra", C.c_int32),
     ]
 
 
@@ -216,8 +224,11 @@ def make_desc(system, params=None, mcmd=None, first_step=0):
         keep.spd = np.ascontiguousarray(np.asarray(cons["pair_dist"], np.float64).reshape(-1))
         keep.st = np.ascontiguousarray(np.asarray(cons["trio_atoms"], np.int32).reshape(-1))
         keep.std = np.ascontiguousarray(np.asarray(cons["trio_dist"], np.float64).reshape(-1))
-        if len(np.asarray(cons.get("quad_atoms", np.zeros((0, 4))))):
-            raise ValueError("SHAKE quads are not on the hot path of these workloads")
+        qa = np.asarray(cons.get("quad_atoms", np.zeros((0, 4))), np.int32).reshape(-1)
+        if len(qa):
+            keep.qa = np.ascontiguousarray(qa)
+            keep.qd = np.ascontiguousarray(np.asarray(cons["quad_dist"], np.float64).reshape(-1))
+            d.n_shake_quad, d.shake_quad, d.shake_quad_dist = len(qa) // 4, _ptr(keep.qa, C.c_int32), _ptr(keep.qd, C.c_double)
         d.n_shake_pair, d.shake_pair, d.shake_pair_dist = len(keep.spd), _ptr(keep.sp, C.c_int32), _ptr(keep.spd, C.c_double)
         d.n_shake_trio, d.shake_trio, d.shake_trio_dist = len(keep.st) // 3, _ptr(keep.st, C.c_int32), _ptr(keep.std, C.c_double)
     b = t.get("bonds")
@@ -243,6 +254,28 @@ def make_desc(system, params=None, mcmd=None, first_step=0):
     d.heating_steps, d.berendsen_tau = prm["heating_steps"], prm["berendsen_tau"]
     d.const_max_loops, d.const_tolerance = prm["const_max_loops"], prm["const_tolerance"]
     d.thermo_const_max_loops, d.thermo_const_tolerance = prm["thermo_const_max_loops"], prm["thermo_const_tolerance"]
+    for key, pre in (("torsions", "torsion"), ("impros", "impro")):
+        recs = t.get(key)
+        if recs is not None and len(recs):
+            arrs = (np.ascontiguousarray(recs["a"], np.int32).reshape(-1), np.ascontiguousarray(recs["ene"], np.float64),
+                    np.ascontiguousarray(recs["phase"], np.float64), np.ascontiguousarray(recs["overlaps"], np.int32),
+                    np.ascontiguousarray(recs["symmetry"], np.int32))
+            setattr(keep, key, arrs)
+            setattr(d, "n_" + ("torsions" if pre == "torsion" else "impros"), len(recs))
+            setattr(d, pre, _ptr(arrs[0], C.c_int32))
+            setattr(d, pre + "_ene", _ptr(arrs[1], C.c_double))
+            setattr(d, pre + "_phase", _ptr(arrs[2], C.c_double))
+            setattr(d, pre + "_overlaps", _ptr(arrs[3], C.c_int32))
+            setattr(d, pre + "_symmetry", _ptr(arrs[4], C.c_int32))
+    n14 = t.get("nb14")
+    if n14 is not None and len(n14["atoms"]):
+        keep.n14 = (np.ascontiguousarray(n14["atoms"], np.int32).reshape(-1),
+                    np.ascontiguousarray(n14["types"], np.int32).reshape(-1),
+                    np.ascontiguousarray(n14["coeff_vdw"], np.float64), np.ascontiguousarray(n14["coeff_ele"], np.float64))
+        d.n_nb14 = len(keep.n14[2])
+        d.nb14, d.nb14_type = _ptr(keep.n14[0], C.c_int32), _ptr(keep.n14[1], C.c_int32)
+        d.nb14_coeff_vdw, d.nb14_coeff_ele = _ptr(keep.n14[2], C.c_double), _ptr(keep.n14[3], C.c_double)
+    d.dof_extra = int(system.get("dof_extra", 0))
     d.first_step = int(first_step)
     d.mcmd_order = -1
     if mcmd is not None:

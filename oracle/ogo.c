@@ -693,6 +693,108 @@ double ogo_bonds(const ogo_pbc *p, int nb, const int *pairs, const double *k, co
     return e;
 }
 
+static void cross3(const double a[3], const double b[3], double c[3]) {
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+/* ForceField::calc_torsion: the reference's PI constant (CelesteObject.cpp:27) and gmul table
+ * (ForceField.cpp:7-17, 2k for even k, 0 otherwise) are part of the arithmetic. */
+#define REF_PI 3.14159265
+#define REF_EPS 1e-10
+double ogo_dihedrals(const ogo_pbc *p, int n, const int *quads, const double *ene, const int *overlaps,
+                     const int *symmetry, const double *phase, const double *crd, double *work) {
+    double e_sum = 0.0;
+    for (int t = 0; t < n; t++) {
+        const int a1 = quads[4 * t], a2 = quads[4 * t + 1], a3 = quads[4 * t + 2], a4 = quads[4 * t + 3];
+        double w1[3] = {0, 0, 0}, w2[3] = {0, 0, 0}, w3[3] = {0, 0, 0}, e = 0.0;
+        if (ene[t] > REF_EPS) {
+            double d21[3], d32[3], d43[3], p12[3], p23[3], p123[3];
+            diff_minim_d(p, d21, crd + 3 * a2, crd + 3 * a1);
+            diff_minim_d(p, d32, crd + 3 * a3, crd + 3 * a2);
+            diff_minim_d(p, d43, crd + 3 * a4, crd + 3 * a3);
+            cross3(d21, d32, p12);
+            cross3(d32, d43, p23);
+            double p12_2 = p12[0] * p12[0] + p12[1] * p12[1] + p12[2] * p12[2];
+            double p23_2 = p23[0] * p23[0] + p23[1] * p23[1] + p23[2] * p23[2];
+            double p12p23 = sqrt(p12_2 * p23_2);
+            if (p12p23 > 0.0) {
+                double inv = 1.0 / p12p23;
+                double s1223 = p12[0] * p23[0] + p12[1] * p23[1] + p12[2] * p23[2];
+                double cosp = s1223 * inv;
+                if (cosp > 1.0) cosp = 1.0;
+                if (cosp < -1.0) cosp = -1.0;
+                cross3(p12, p23, p123);
+                double phi = acos(cosp);
+                if (d32[0] * p123[0] + d32[1] * p123[1] + d32[2] * p123[2] < 0.0) phi = 2.0 * REF_PI - phi;
+                const double sym = (double)symmetry[t];
+                const double div = 1.0 / (double)overlaps[t];
+                e = ene[t] * (1.0 + cos(sym * phi - phase[t])) * div;
+                const int nrot = symmetry[t];
+                const double gm = (nrot >= 0 && nrot <= 10 && nrot % 2 == 0) ? (double)nrot : 0.0;
+                const double sinp = sin(phi);
+                const double sf = sin(phase[t]), cf = cos(phase[t]);
+                const double sr = sin(sym * phi), cr = cos(sym * phi);
+                const double dflim = cf * (sym - gm + gm * cosp);
+                const double df0 = cf * sr - sf * cr;
+                const double df1 = (REF_EPS <= fabs(sinp)) ? df0 / sinp : dflim;
+                const double wc = sym * ene[t] * div * df1 * inv;
+                const double r12 = 1.0 / p12_2 * s1223, r23 = 1.0 / p23_2 * s1223;
+                double a[3], b[3], c[3], dd[3], f[3], g[3];
+                cross3(p23, d32, a);
+                cross3(p12, d32, b);
+                for (int i = 0; i < 3; i++) w1[i] = wc * (a[i] - r12 * b[i]);
+                double d2132[3] = {d21[0] + d32[0], d21[1] + d32[1], d21[2] + d32[2]};
+                cross3(d2132, p23, a);
+                cross3(d2132, p12, b);
+                cross3(p12, d43, c);
+                cross3(p23, d43, dd);
+                for (int i = 0; i < 3; i++) w2[i] = wc * (a[i] + c[i] - r12 * b[i] - r23 * dd[i]);
+                cross3(p12, d32, f);
+                cross3(p23, d32, g);
+                for (int i = 0; i < 3; i++) w3[i] = wc * (f[i] - r23 * g[i]);
+            }
+        }
+        e_sum += e;
+        for (int d = 0; d < 3; d++) {
+            work[3 * a1 + d] += w1[d];
+            work[3 * a2 + d] += w2[d];
+            work[3 * a3 + d] -= w1[d] + w2[d] + w3[d];
+            work[3 * a4 + d] += w3[d];
+        }
+    }
+    return e_sum;
+}
+
+void ogo_nb14(const ogo_pbc *p, int n, const int *pairs, const int *types, int n_types, const float *lj6,
+              const float *lj12, const float *charge, const double *coeff_vdw, const double *coeff_ele,
+              const double *crd, double *work, double *e_vdw, double *e_ele) {
+    double ev = 0.0, ee = 0.0;
+    for (int k = 0; k < n; k++) {
+        const int i = pairs[2 * k], j = pairs[2 * k + 1];
+        const int tt = types[2 * k] * n_types + types[2 * k + 1];
+        double d[3];
+        diff_minim_d(p, d, crd + 3 * i, crd + 3 * j);
+        const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+        const double r2i = 1.0 / r2, ri = sqrt(r2i);
+        const double r6i = r2i * r2i * r2i, r12i = r6i * r6i;
+        const double t6 = (double)lj6[tt] * r6i, t12 = (double)lj12[tt] * r12i;
+        ev += (-t6 + t12) * coeff_vdw[k];
+        const double cw = r2i * coeff_vdw[k] * (-12.0 * t12 + 6.0 * t6);
+        const double cc = (double)charge[i] * (double)charge[j] * CHARGE_COEFF * coeff_ele[k];
+        ee += cc * ri;
+        const double ce = -cc * r2i * ri;
+        for (int q = 0; q < 3; q++) {
+            const double w = cw * d[q] + ce * d[q];
+            work[3 * i + q] += w;
+            work[3 * j + q] -= w;
+        }
+    }
+    *e_vdw = ev;
+    *e_ele = ee;
+}
+
 double ogo_angles(const ogo_pbc *p, int na, const int *t, const double *k, const double *t0,
                   const double *crd, double *work) {
     double e = 0.0;
@@ -849,9 +951,99 @@ static void shake_trios(ogo_integ *s, const ogo_pbc *p) {
     }
 }
 
+/* ConstraintObject::calc_linear_eq (Constraint.cpp:141-202): elimination with the pivot
+ * permutation applied to the column index, a[6][6] overwritten.  Returns 1 if singular. */
+static int solve6(double a[6][6], double x[6], const double b[6]) {
+    int piv[6] = {0, 1, 2, 3, 4, 5};
+    for (int i = 0; i < 6; i++) {
+        int idx = i;
+        double mx = fabs(a[i][piv[i]]);
+        for (int j = i + 1; j < 6; j++) {
+            double t = fabs(a[i][piv[j]]);
+            if (t > mx) { idx = j; mx = t; }
+        }
+        if (idx != i) { int t = piv[i]; piv[i] = piv[idx]; piv[idx] = t; }
+        if (fabs(a[i][piv[i]]) < 1e-30) return 1;
+        a[i][piv[i]] = 1.0 / a[i][piv[i]];
+        for (int j = i + 1; j < 6; j++) {
+            a[i][piv[j]] *= a[i][piv[i]];
+            for (int k = i + 1; k < 6; k++) a[k][piv[j]] -= a[i][piv[j]] * a[k][piv[i]];
+        }
+    }
+    for (int i = 0; i < 6; i++) {
+        double v = b[piv[i]];
+        for (int j = 0; j < i; j++) v -= a[j][piv[i]] * x[j];
+        x[i] = v;
+    }
+    for (int i = 5; i >= 0; i--) {
+        double v = x[i];
+        for (int j = i + 1; j < 6; j++) v -= a[j][piv[i]] * x[j];
+        x[i] = v * a[i][piv[i]];
+    }
+    return 0;
+}
+
+/* ConstraintShake::shake_quad (ConstraintShake.cpp:151-276): one centre and three partners,
+ * six distances (Constraint.cpp:4 pair order), Newton steps with a 6x6 solve. */
+static void shake_quads(ogo_integ *s, const ogo_pbc *p) {
+    static const int PI2[6][2] = {{0, 1}, {1, 2}, {2, 0}, {3, 0}, {2, 3}, {1, 3}};
+    for (int c = 0; c < s->n_quad; c++) {
+        const int *at = s->quad_atoms + 4 * c;
+        const double *qd = s->quad_dist2 + 6 * c;
+        double mi[4];
+        for (int i = 0; i < 4; i++) mi[i] = (double)s->mass_inv[at[i]];
+        const double w[6][6] = {{mi[0] + mi[1], -mi[1], -mi[0], -mi[0], 0.0, -mi[1]},
+                                {-mi[1], mi[1] + mi[2], -mi[2], 0.0, -mi[2], mi[1]},
+                                {-mi[0], -mi[2], mi[2] + mi[0], mi[0], mi[2], 0.0},
+                                {-mi[0], 0.0, mi[0], mi[3] + mi[0], -mi[3], -mi[3]},
+                                {0.0, -mi[2], mi[2], -mi[3], mi[2] + mi[3], mi[3]},
+                                {-mi[1], mi[1], 0.0, -mi[3], mi[3], mi[1] + mi[3]}};
+        double dc[6][3], dp[6][3];
+        for (int k = 0; k < 6; k++) {
+            diff_minim_d(p, dc[k], s->crd + 3 * at[PI2[k][0]], s->crd + 3 * at[PI2[k][1]]);
+            diff_minim_d(p, dp[k], s->crd_prev + 3 * at[PI2[k][0]], s->crd_prev + 3 * at[PI2[k][1]]);
+        }
+        double coef[6] = {0, 0, 0, 0, 0, 0}, coef_post[6] = {0, 0, 0, 0, 0, 0};
+        for (int it = 0; it < s->shake_max_loops; it++) {
+            for (int k = 0; k < 6; k++) coef[k] = coef_post[k];
+            double dv[6][3];
+            for (int i = 0; i < 6; i++) {
+                for (int d = 0; d < 3; d++) dv[i][d] = dc[i][d];
+                for (int j = 0; j < 6; j++)
+                    for (int d = 0; d < 3; d++) dv[i][d] += w[j][i] * dp[j][d] * coef[j];
+            }
+            double g[6][6];
+            for (int i = 0; i < 6; i++)
+                for (int j = 0; j < 6; j++)
+                    g[i][j] = 2.0 * w[j][i] * (dv[j][0] * dp[i][0] + dv[j][1] * dp[i][1] + dv[j][2] * dp[i][2]);
+            int conv = 1;
+            double sd[6];
+            for (int i = 0; i < 6; i++) {
+                double nrm = dv[i][0] * dv[i][0] + dv[i][1] * dv[i][1] + dv[i][2] * dv[i][2];
+                sd[i] = qd[i] - nrm;
+                conv = conv && (fabs(sd[i] / qd[i]) < s->shake_tol);
+            }
+            if (conv) break;
+            double rhs[6];
+            for (int i = 0; i < 6; i++) {
+                rhs[i] = sd[i];
+                for (int j = 0; j < 6; j++) rhs[i] += g[j][i] * coef[j];
+            }
+            solve6(g, coef_post, rhs);
+        }
+        for (int d = 0; d < 3; d++) {
+            s->crd[3 * at[0] + d] += mi[0] * (coef[0] * dp[0][d] - coef[2] * dp[2][d] - coef[3] * dp[3][d]);
+            s->crd[3 * at[1] + d] += mi[1] * (-coef[0] * dp[0][d] + coef[1] * dp[1][d] + coef[5] * dp[5][d]);
+            s->crd[3 * at[2] + d] += mi[2] * (-coef[1] * dp[1][d] + coef[2] * dp[2][d] + coef[4] * dp[4][d]);
+            s->crd[3 * at[3] + d] += mi[3] * (coef[3] * dp[3][d] - coef[4] * dp[4][d] - coef[5] * dp[5][d]);
+        }
+    }
+}
+
 void ogo_shake(ogo_integ *s, const ogo_pbc *p) {
     shake_pairs(s, p);
     shake_trios(s, p);
+    shake_quads(s, p);
 }
 
 void ogo_set_velocity_from_crd(ogo_integ *s) {

@@ -132,6 +132,17 @@ double ogo_bonds(const ogo_pbc *p, int n_bonds, const int *pairs, const double *
 double ogo_angles(const ogo_pbc *p, int n_angles, const int *triads, const double *k, const double *t0,
                   const double *crd, double *work);
 
+/* ForceField::calc_torsion (ForceField.cpp:179-300) summed as SubBox::calc_energy_torsions /
+ * calc_energy_impros (SubBox.cpp:1273-1320): E = ene (1 + cos(sym phi - phase)) / overlaps;
+ * the same routine serves torsions and impropers.  Returns the energy, adds the work. */
+double ogo_dihedrals(const ogo_pbc *p, int n, const int *quads, const double *ene, const int *overlaps,
+                     const int *symmetry, const double *phase, const double *crd, double *work);
+/* ForceField::calc_14pair (ForceField.cpp:302-331) summed as SubBox::calc_energy_14nb
+ * (SubBox.cpp:1321-1345); charges and LJ terms are the reference's float values. */
+void ogo_nb14(const ogo_pbc *p, int n, const int *pairs, const int *types, int n_types, const float *lj6,
+              const float *lj12, const float *charge, const double *coeff_vdw, const double *coeff_ele,
+              const double *crd, double *work, double *e_vdw, double *e_ele);
+
 /* ---------------- integrator (DynamicsMode.cpp:468-560) ---------------- */
 typedef struct {
     int     n;
@@ -146,6 +157,9 @@ typedef struct {
     const double *pair_dist2;   /* squared */
     const int    *trio_atoms;   /* [3*n_trio] */
     const double *trio_dist2;   /* [3*n_trio] squared: d12, d23, d31 */
+    int     n_quad;
+    const int    *quad_atoms;   /* [4*n_quad] */
+    const double *quad_dist2;   /* [6*n_quad] squared, pairs (0,1) (1,2) (2,0) (3,0) (2,3) (1,3) */
     int     shake_max_loops;
     double  shake_tol;
     /* COM cancel groups (COMMotion.cpp:30-55) */

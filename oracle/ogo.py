@@ -82,6 +82,10 @@ def lib():
         L.ogo_bonds.restype = C.c_double
         L.ogo_angles.argtypes = [C.POINTER(Pbc), C.c_int, i32p, f64p, f64p, f64p, f64p]
         L.ogo_angles.restype = C.c_double
+        L.ogo_dihedrals.argtypes = [C.POINTER(Pbc), C.c_int, i32p, f64p, i32p, i32p, f64p, f64p, f64p]
+        L.ogo_dihedrals.restype = C.c_double
+        L.ogo_nb14.argtypes = [C.POINTER(Pbc), C.c_int, i32p, i32p, C.c_int, f32p, f32p, f32p, f64p, f64p, f64p,
+                               f64p, f64p, f64p]
         L.ogo_mcmd_scale.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int, f64p, C.c_double, C.c_int, f64p]
         L.ogo_mcmd_scale.restype = C.c_double
         _lib = L
@@ -293,7 +297,8 @@ class Integ(C.Structure):
                 ("mass", C.POINTER(C.c_float)), ("mass_inv", C.POINTER(C.c_float)),
                 ("n_pair", C.c_int), ("n_trio", C.c_int), ("pair_atoms", C.POINTER(C.c_int)),
                 ("pair_dist2", C.POINTER(C.c_double)), ("trio_atoms", C.POINTER(C.c_int)),
-                ("trio_dist2", C.POINTER(C.c_double)), ("shake_max_loops", C.c_int), ("shake_tol", C.c_double),
+                ("trio_dist2", C.POINTER(C.c_double)), ("n_quad", C.c_int), ("quad_atoms", C.POINTER(C.c_int)),
+                ("quad_dist2", C.POINTER(C.c_double)), ("shake_max_loops", C.c_int), ("shake_tol", C.c_double),
                 ("n_com_groups", C.c_int), ("com_group_start", C.POINTER(C.c_int)),
                 ("com_group_atoms", C.POINTER(C.c_int)), ("com_mass_inv", C.POINTER(C.c_float)),
                 ("thermostat", C.c_int), ("temperature", C.c_double), ("temperature_coeff", C.c_double),
@@ -317,13 +322,25 @@ def _bind_integ(L):
     L._integ_bound = True
 
 
+def _dihedral_arrays(recs):
+    """Torsion or improper records (cls_io.DIHED) as the flat arrays ogo_dihedrals takes."""
+    if recs is None or not len(recs):
+        return None
+    return (np.ascontiguousarray(recs["a"], np.int32).reshape(-1), np.ascontiguousarray(recs["ene"], np.float64),
+            np.ascontiguousarray(recs["overlaps"], np.int32), np.ascontiguousarray(recs["symmetry"], np.int32),
+            np.ascontiguousarray(recs["phase"], np.float64))
+
+
 class OracleMD:
     """The reference's leapfrog-presto step (DynamicsModePresto::calc_in_each_step,
-    DynamicsMode.cpp:468-560) on the C oracle, with FP64 forces: pair LJ + ZD over the
-    reference's cell-pair list evaluated on the list's (unwrapped) grid positions, excess ZD
-    pairs and bonds/angles with the minimum image.  ``params`` uses engine.DEFAULT_PARAMS keys."""
+    DynamicsMode.cpp:468-560) on the C oracle.  Forces: pair LJ + ZD, excess ZD pairs, bonds,
+    angles, torsions, impropers and 1-4 pairs.  ``pair_mode`` "cells_f64" (default) evaluates
+    the pair terms in FP64 over the reference's cell-pair list on the list's (unwrapped) grid
+    positions; "allpairs_f32" restates the reference's all-pairs build (FP32 pair and excess
+    terms, ``-DF_WO_NS``), whose output the ala3 sample log records.  ``params`` uses
+    engine.DEFAULT_PARAMS keys."""
 
-    def __init__(self, system, params, mcmd=None):
+    def __init__(self, system, params, mcmd=None, pair_mode="cells_f64"):
         from omegagene_b200 import cls_io  # local import: oracle stays importable alone
         self.L = L = lib()
         _bind_integ(L)
@@ -363,15 +380,31 @@ class OracleMD:
         if a is not None and len(a):
             self.angles = (np.ascontiguousarray(np.stack([a["a1"], a["a2"], a["a3"]], 1).astype(np.int32).reshape(-1)),
                            np.ascontiguousarray(a["k"], np.float64), np.ascontiguousarray(a["t0"], np.float64))
+        self.pair_mode = pair_mode
+        self.torsions = _dihedral_arrays(t.get("torsions"))
+        self.impros = _dihedral_arrays(t.get("impros"))
+        n14 = t.get("nb14")
+        self.nb14 = None
+        if n14 is not None and len(n14["atoms"]):
+            self.nb14 = (np.ascontiguousarray(n14["atoms"], np.int32).reshape(-1),
+                         np.ascontiguousarray(n14["types"], np.int32).reshape(-1),
+                         np.ascontiguousarray(n14["coeff_vdw"], np.float64),
+                         np.ascontiguousarray(n14["coeff_ele"], np.float64))
+        self.c6f, self.c12f = self.c6.astype(np.float32), self.c12.astype(np.float32)
         cons = system.get("constraint")
         use_cons = cons is not None and self.p.get("constraint", "shake") != "none"
         self.pa = np.asarray(cons["pair_atoms"], np.int32).reshape(-1) if use_cons else np.zeros(0, np.int32)
         self.pd2 = (np.asarray(cons["pair_dist"], np.float64) ** 2).reshape(-1) if use_cons else np.zeros(0)
         self.ta = np.asarray(cons["trio_atoms"], np.int32).reshape(-1) if use_cons else np.zeros(0, np.int32)
         self.td2 = (np.asarray(cons["trio_dist"], np.float64) ** 2).reshape(-1) if use_cons else np.zeros(0)
-        self.has_cons = len(self.pd2) + len(self.td2) > 0
-        n_cdist = len(self.pd2) + len(self.td2)
-        self.d_free = 3 * n - 3 - n_cdist
+        qa = np.asarray(cons.get("quad_atoms", np.zeros((0, 4))), np.int32).reshape(-1) if use_cons else None
+        self.qa = qa if qa is not None and len(qa) else np.zeros(0, np.int32)
+        self.qd2 = ((np.asarray(cons["quad_dist"], np.float64) ** 2).reshape(-1) if len(self.qa)
+                    else np.zeros(0))
+        self.has_cons = len(self.pd2) + len(self.td2) + len(self.qd2) > 0
+        n_cdist = len(self.pd2) + len(self.td2) + len(self.qd2)
+        # a position-restraint section adds 3 (Read.cpp:90-93)
+        self.d_free = 3 * n - 3 - n_cdist + int(system.get("dof_extra", 0))
         gs, ga, gmi = [0], [], []
         if self.p.get("com_motion", "cancel") == "cancel" and "groups" in system:
             names = self.p.get("com_cancel_groups") or system["groups"]["names"]
@@ -408,6 +441,9 @@ class OracleMD:
         I.pair_dist2 = self.pd2.ctypes.data_as(C.POINTER(C.c_double))
         I.trio_atoms = self.ta.ctypes.data_as(C.POINTER(C.c_int))
         I.trio_dist2 = self.td2.ctypes.data_as(C.POINTER(C.c_double))
+        I.n_quad = len(self.qd2) // 6
+        I.quad_atoms = self.qa.ctypes.data_as(C.POINTER(C.c_int))
+        I.quad_dist2 = self.qd2.ctypes.data_as(C.POINTER(C.c_double))
         I.shake_max_loops, I.shake_tol = self.p["const_max_loops"], self.p["const_tolerance"]
         I.n_com_groups = len(self.gs) - 1
         I.com_group_start = self.gs.ctypes.data_as(C.POINTER(C.c_int))
@@ -425,29 +461,46 @@ class OracleMD:
         self.slot_crd = self.cl.slot_crd.copy()
 
     def forces(self, virial=False):
-        """FP64 forces at the current positions into self.work; returns energies."""
-        if self.cl is None or self.step_i % self.p["nsgrid_update_intvl"] == 0:
-            self.rebuild()
+        """Forces at the current positions into self.work; returns energies."""
         n = self.n
-        pos = np.ascontiguousarray(self.slot_crd[self.cl.atomids_rev].reshape(-1))
         w = np.zeros(3 * n)
         e = np.zeros(2)
         vir = np.zeros(9)
-        self.L.ogo_pair_cells_f64(self.Ld, self.cl._grid, self.cl._cps, pos, self.q64, self.ty, self.nt, self.c6,
-                                  self.c12, float(self.p["cutoff"]), w, e, vir)
         vexc = np.zeros(9)
-        exc = self.L.ogo_excess_f64(self.Ld, len(self.ep) // 2, self.ep, self.crd, self.q64, float(self.p["cutoff"]),
-                                    w, vexc)
+        if self.pair_mode == "allpairs_f32":
+            z, b, f = zd_constants(self.p["cutoff"])
+            self.L.ogo_pair_allpairs_f32(self.pbc, n, self.crd, self.q32, self.ty, self.nt, self.c6f, self.c12f,
+                                         self.nb.reshape(-1), self.nb.shape[1], float(self.p["cutoff"]), z, b, f, w, e)
+            exc = self.L.ogo_excess_f32(self.pbc, len(self.ep) // 2, self.ep, self.crd, self.q32, b, f, w)
+        else:
+            if self.cl is None or self.step_i % self.p["nsgrid_update_intvl"] == 0:
+                self.rebuild()
+            pos = np.ascontiguousarray(self.slot_crd[self.cl.atomids_rev].reshape(-1))
+            self.L.ogo_pair_cells_f64(self.Ld, self.cl._grid, self.cl._cps, pos, self.q64, self.ty, self.nt, self.c6,
+                                      self.c12, float(self.p["cutoff"]), w, e, vir)
+            exc = self.L.ogo_excess_f64(self.Ld, len(self.ep) // 2, self.ep, self.crd, self.q64,
+                                        float(self.p["cutoff"]), w, vexc)
         eb = ea = 0.0
         if self.bonds is not None:
             eb = self.L.ogo_bonds(self.pbc, len(self.bonds[1]), self.bonds[0], self.bonds[1], self.bonds[2], self.crd, w)
         if self.angles is not None:
             ea = self.L.ogo_angles(self.pbc, len(self.angles[1]), self.angles[0], self.angles[1], self.angles[2],
                                    self.crd, w)
+        et = ei = ev14 = ee14 = 0.0
+        if self.torsions is not None:
+            et = self.L.ogo_dihedrals(self.pbc, len(self.torsions[1]), *self.torsions, self.crd, w)
+        if self.impros is not None:
+            ei = self.L.ogo_dihedrals(self.pbc, len(self.impros[1]), *self.impros, self.crd, w)
+        if self.nb14 is not None:
+            o1, o2 = np.zeros(1), np.zeros(1)
+            a, ty, cv, ce = self.nb14
+            self.L.ogo_nb14(self.pbc, len(cv), a, ty, self.nt, self.c6f, self.c12f, self.q32, cv, ce, self.crd, w,
+                            o1, o2)
+            ev14, ee14 = float(o1[0]), float(o2[0])
         self.work[:] = w
         ene = {"vdw": e[0], "ele": e[1] + exc + self.self_e, "bond": eb, "angle": ea, "ele_excess": exc,
-               "ele_self": self.self_e}
-        ene["potential"] = ene["vdw"] + ene["ele"] + eb + ea
+               "ele_self": self.self_e, "torsion": et, "improper": ei, "vdw14": ev14, "ele14": ee14}
+        ene["potential"] = ene["vdw"] + ene["ele"] + eb + ea + et + ei + ev14 + ee14
         if virial:
             ene["virial"] = (vir + vexc).reshape(3, 3)
         return ene
@@ -475,7 +528,8 @@ class OracleMD:
                 L.ogo_shake(C.byref(I), C.byref(self.pbc))
                 L.ogo_set_velocity_from_crd(C.byref(I))
         # MiniCell::move_atom, then the PBC wrap
-        self.slot_crd[self.cl.atomids_rev] += (self.crd - self.crd_prev).reshape(-1, 3)
+        if self.cl is not None:
+            self.slot_crd[self.cl.atomids_rev] += (self.crd - self.crd_prev).reshape(-1, 3)
         L.ogo_revise_pbc(C.byref(self.pbc), self.n, self.crd)
         kin = L.ogo_kinetic(C.byref(I), None)
         ene["kinetic"] = kin

@@ -116,3 +116,29 @@ def test_fp32_cell_path_close_to_fp64_oracle():
     np.testing.assert_allclose(w64c, w64, rtol=0, atol=1e-9)
     np.testing.assert_allclose(e64c, e64, rtol=1e-12)
     np.testing.assert_allclose(v64c, v64, rtol=1e-10, atol=1e-7)
+
+
+def _ala3_golden():
+    sys_path = os.path.join(HERE, "golden")
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_ala3_golden", os.path.join(sys_path, "make_ala3_golden.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    gold = json.load(open(os.path.join(sys_path, "ala3_log.json")))
+    return mod.load_system(), gold
+
+
+def test_oracle_reproduces_ala3_log_trajectory():
+    """The oracle's all-pairs mode against every energy the reference printed for the first ten
+    steps of its ala3 sample (bond, angle, torsion, improper, 1-4 VDW/Ele, VDW, Ele, kinetic,
+    total, temperature): equal to the printed 11 significant digits.  This pins the integrator,
+    SHAKE pair/trio/quad, COM cancel and the bonded terms, not only the pair energies."""
+    s, gold = _ala3_golden()
+    md = ogo.OracleMD(s, gold["params"], pair_mode="allpairs_f32")
+    assert md.d_free == 12417
+    for row in gold["steps"][:10]:
+        got = md.step()
+        for key, ref in row.items():
+            if key == "step":
+                continue
+            assert float("%.10e" % got[key]) == ref, (row["step"], key, got[key], ref)
