@@ -35,6 +35,7 @@ METRIC = "ns/day@1M atoms"
 UNIT = "ns/day"
 DT_FS = 2.0
 INTVL = 10
+VMCMD_TRANS_INTERVAL = 100  # V-McMD walkers: steps between virtual-state transition trials
 N_WATERS = 333334
 BOX = 215.5
 LATTICE = 70
@@ -368,15 +369,28 @@ def run_serve(args):
 
 # ------------------------------------------------------------------ McMD workload
 
-def run_walkers(walkers, params, polys, n_steps, chunk, trace=False):
+def run_walkers(walkers, params, polys, n_steps, chunk, trace=False, vs_logs=None):
     """Steps all walkers in one engine, `chunk` steps per og_step call.  A walker whose system
     faults is dropped: og_step undoes the chunk for every walker, the rest are re-formed into a
     new engine (same step number, so the same trajectories) and the chunk is redone.  Returns
     the surviving indices, their states, the per-step trace of the survivors (or None), the
-    device time of every og_step call (failed ones included) and the atom-steps completed."""
+    device time of every og_step call (failed ones included) and the atom-steps completed.
+    With V-McMD sections in `polys`, walker k draws with random_seed + k; a re-formed engine
+    gets each walker's virtual state and generator, and the virtual-state logs are collected into
+    `vs_logs` (walker -> list of states) when given."""
     from omegagene_b200 import engine
     keep = list(range(len(walkers)))
     state = {k: (walkers[k]["crd"], walkers[k]["vel"]) for k in keep}
+    polys = list(polys) if polys else None
+    vm = bool(polys) and "states" in polys[0]
+
+    def collect(eng):
+        for i, k in enumerate(keep):
+            cur, mt = eng.vmcmd_state(i)
+            polys[k] = dict(polys[k], cur_vs=cur, mt_state=mt)
+            if vs_logs is not None:
+                vs_logs.setdefault(k, []).extend(eng.take_vs_log(i)[1].tolist())
+
     traces = {k: [] for k in keep}
     done, ms, atom_steps, dropped = 0, 0.0, 0, []
     variant = -1  # the first engine autotunes; a re-formed one keeps its choice
@@ -386,7 +400,8 @@ def run_walkers(walkers, params, polys, n_steps, chunk, trace=False):
         for k in keep:
             s = dict(walkers[k])
             s["crd"], s["vel"] = state[k]
-            eng.add_system(s, params, polys[k] if polys else None, first_step=done)
+            pk = dict(params, random_seed=params.get("random_seed", 0) + k) if vm else params
+            eng.add_system(s, pk, polys[k] if polys else None, first_step=done)
         eng.finalize()
         variant = eng.tuning()["pair_variant"]
         eng.set_timing("step")
@@ -404,6 +419,8 @@ def run_walkers(walkers, params, polys, n_steps, chunk, trace=False):
                 f = eng.system_faults()
                 for i, k in enumerate(keep):
                     state[k] = eng.get_state(i)
+                if vm:
+                    collect(eng)
                 dropped += [k for i, k in enumerate(keep) if f[i]]
                 keep = [k for i, k in enumerate(keep) if not f[i]]
                 faulted = True
@@ -418,6 +435,8 @@ def run_walkers(walkers, params, polys, n_steps, chunk, trace=False):
                 eng.set_trace(n_steps)
             for i, k in enumerate(keep):
                 state[k] = eng.get_state(i)
+        if vm and not faulted:
+            collect(eng)
         eng.close()
         if not faulted:
             break
@@ -429,8 +448,10 @@ def run_mcmd(args):
     """64 V-McMD walkers (a 300-atom synthetic chain in 2,500 TIP3P waters each, own seeds,
     hydrogens held by angle terms), 300 K velocity rescaling, in one engine.  Protocol: 400
     steps at 0.5 fs (the generator's contacts relax), a 100-step unscaled prerun at 2 fs whose
-    potential energies give each walker's polynomial range (mean +- 4 sd), then the timed McMD
-    run at 2 fs.  Compared with the same walkers run one at a time."""
+    potential energies give each walker's virtual-state ladder (four overlapping windows over
+    mean +- 4 sd, each with its own order-6 polynomial, a transition trial every 100 steps and
+    the lambda logged every step, as the reference's sample V-McMD run logs it), then the timed
+    V-McMD run at 2 fs.  Compared with the same walkers run one at a time."""
     import torch
     from omegagene_b200 import engine, serve, systems
     torch.cuda.set_device(0)
@@ -444,11 +465,14 @@ def run_mcmd(args):
     keep, states, tr, _, _, drop_pre = run_walkers(walkers, p, None, 100, 100, trace=True)
     walkers = [dict(walkers[k], crd=c, vel=v) for k, (c, v) in zip(keep, states)]
     pot = tr[:, :, engine.ENERGY_NAMES.index("potential")]
-    polys = [systems.mcmd_polynomial(pot[:, w].mean(), max(pot[:, w].std(), 1.0), seed=900 + w)
-             for w in range(len(walkers))]
+    polys = [systems.vmcmd_ladder(pot[:, w].mean(), max(pot[:, w].std(), 1.0), seed=900 + w, n_vs=4,
+                                  interval=VMCMD_TRANS_INTERVAL) for w in range(len(walkers))]
+    p = dict(p, random_seed=1000 * args.walker_seed0 + 1, print_intvl_extended_lambda=1)
     # timed run: whole list intervals, so og_step replays the captured graph
-    keep, _, _, ms, atom_steps, drop_run = run_walkers(walkers, p, polys, args.steps, args.chunk)
+    vs_logs = {}
+    keep, _, _, ms, atom_steps, drop_run = run_walkers(walkers, p, polys, args.steps, args.chunk, vs_logs=vs_logs)
     batched = atom_steps / (ms / 1e3)
+    moves = [int(np.count_nonzero(np.diff([polys[k]["init_vs"] - 1] + vs_logs.get(k, [])))) for k in keep]
     ts = []
     for w, m in list(zip(walkers, polys))[:2]:
         job = serve.Job(0, w, p, min(args.steps, 2000), mcmd=m)
@@ -460,13 +484,16 @@ def run_mcmd(args):
             "steps": args.steps, "warmup": 500, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
             "config": {"workload": "%d McMD walkers, 300-atom chain in 2500 TIP3P waters each (%d atoms total), "
-                                   "dt 2 fs, 300 K velocity rescaling, V-McMD force scaling (order-6 polynomial)"
-                                   % (args.walkers, n_atoms),
+                                   "dt 2 fs, 300 K velocity rescaling, V-McMD: 4 virtual states per walker "
+                                   "(order-6 polynomials), a transition trial every %d steps, lambda logged every "
+                                   "step" % (args.walkers, n_atoms, VMCMD_TRANS_INTERVAL),
                        "timing": "CUDA events around every og_step call of %d steps, engine re-forming after a "
                                  "fault excluded" % args.chunk},
             "walkers_dropped": {"warm_up": len(drop_warm), "prerun": len(drop_pre), "run": len(drop_run),
                                 "note": "a walker whose system faults (og_get_system_faults) is retired; the "
                                         "others are re-stepped from the undone call"},
+            "vstate_moves": {"mean_per_walker": float(np.mean(moves)) if moves else 0.0,
+                             "trials_per_walker": args.steps // VMCMD_TRANS_INTERVAL},
             "plain": {"atom_steps_per_s": plain, "sample": "2 walkers run alone (wall clock around og_step)"},
             "speedup_vs_plain": batched / plain}
 

@@ -139,7 +139,33 @@ typedef struct {
     /* Added to the degrees of freedom: 3 when the .cls holds a position-restraint section, as
      * Read.cpp:90-93 counts. */
     int32_t dof_extra;
+    /* V-McMD with virtual-state transitions (ExtendedVMcMD, Extend.cpp:56-203; the .cls
+     * "extended" section of Read::load_ls_vmcmd, Read.cpp:521-560).  n_vstates > 0 replaces the
+     * one-state mcmd_* fields above (mcmd_temperature still gives const_k).  At every step s > 0
+     * with s % vmcmd_trans_interval == 0 the system's state tries a move up, then down, with the
+     * potential energy of that step as lambda (set_current_vstate / trial_transition,
+     * Extend.cpp:144-177), and the forces are scaled with the polynomial of the state it is in
+     * afterwards (scale_force, Extend.cpp:178-203).  Each trial draws from the system's own
+     * std::mt19937 (random::Random, src/celeste/random/Random.cpp:20-28) seeded with vmcmd_seed:
+     * the run's --random-seed (MmSystem::set_random, MmSystem.cpp:818-821; the seed stored in the
+     * .cls section is not the one the reference draws with).  Steps count from the run's start,
+     * first_step included. */
+    int32_t n_vstates;
+    int32_t vmcmd_trans_interval;     /* >= 1 */
+    int32_t vmcmd_init_vs;            /* 0-based (the .cls holds it 1-based) */
+    int32_t vmcmd_lambda_log_interval; /* --print-intvl-extended-lambda; 0: no lambda log */
+    uint32_t vmcmd_seed;
+    const int32_t *vs_order;          /* [n_vstates], each 0..7 */
+    const double *vs_lambda;          /* [2 n_vstates]: low, high of each state's lambda range */
+    const double *vs_prob;            /* [2 n_vstates]: down, up transition probability */
+    const double *vs_coef;            /* polynomials, concatenated: [sum(order + 1)] */
+    /* NULL for a new run; else [OG_MT_WORDS] generator words and position as og_get_vmcmd_state
+     * returns them, so a run handed over between engines continues its random sequence. */
+    const uint32_t *vmcmd_mt_state;
 } og_system_desc;
+
+/* std::mt19937 state: 624 words and the next position (624 = twist before the next draw). */
+#define OG_MT_WORDS 625
 
 /* Creates an engine on a CUDA device (cuda_set_device, cuda_setup.cu:1085-1093). */
 og_status og_create(int device, og_engine **out);
@@ -271,6 +297,21 @@ og_status og_segment_sum_noalloc(const double *d_values, int32_t stride, const i
                                  int32_t max_seg_len, double *d_out, void *cuda_stream);
 /* Number of systems and atoms held. */
 og_status og_get_sizes(og_engine *e, int32_t *n_systems, int64_t *n_atoms_total);
+
+/* V-McMD state of a system after the last completed step: the 0-based virtual state
+ * (ExtendedVMcMD::cur_vs) and, when mt_state is not NULL, the generator (OG_MT_WORDS words),
+ * to hand the run to another engine through og_system_desc.vmcmd_init_vs / vmcmd_mt_state. */
+og_status og_get_vmcmd_state(og_engine *e, int32_t sys, int32_t *cur_vs, uint32_t *mt_state);
+/* Takes up to `max` of the oldest V-McMD log entries of a system that the caller has not taken
+ * yet; *n receives how many were taken (with max = 0, how many there are).  Virtual-state log:
+ * one entry per transition step, the step number and the 0-based state after the trial (the
+ * reference writes "step<TAB>state+1" lines, WriteTTPVMcMDLog::write_ttpvMcMDLog,
+ * Write.cpp:41-44, from apply_bias, Extend.cpp:128-131).  Lambda log: the step's potential
+ * energy every vmcmd_lambda_log_interval steps (write_lambda, Extend.cpp:136, 252-255).  Entries
+ * of a call undone by OG_ERR_SYSTEM_FAULT are dropped with it.  step / vs / lambda may be NULL
+ * when max = 0. */
+og_status og_take_vs_log(og_engine *e, int32_t sys, int64_t max, int64_t *step, int32_t *vs, int64_t *n);
+og_status og_take_lambda_log(og_engine *e, int32_t sys, int64_t max, int64_t *step, double *lambda, int64_t *n);
 
 #ifdef __cplusplus
 }

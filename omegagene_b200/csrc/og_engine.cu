@@ -4,6 +4,7 @@
 // with the reference's float arithmetic (MiniCell.cpp:221-290, 1279-1303), and sequences the
 // kernels of one DynamicsModePresto step (DynamicsMode.cpp:468-560) on one CUDA stream.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdlib>
 #include <cstdarg>
@@ -71,7 +72,8 @@ __global__ void k_part_momentum(const int *, const int *, const float *, const d
                                 int, double *);
 template <int NV>
 __global__ void k_part_final(const double *, int, double *, int, int, const float *, int);
-__global__ void k_mcmd_factor(int, const SysDev *, const double *, double *);
+__global__ void k_vmcmd(int, const SysDev *, const VsDev *, const double *, const long long *, int, int *, unsigned *,
+                        int *, double *, int, double *);
 __global__ void k_update_velocities(int, const int *, const SysDev *, const double *, double *, const float *,
                                     double *, double *);
 __global__ void k_com_apply(int, const int *, const double *, const int *, const int *, double *);
@@ -135,7 +137,20 @@ struct HostSystem {
     std::vector<int32_t> xs, xl;  // exclusion partners per atom (CSR, insertion order), local ids
     std::vector<int32_t> tq, tov, tsym, iq, iov, isym, p14, t14, qa;  // dihedrals, 1-4 pairs, SHAKE quads
     std::vector<double> tene, tph, iene, iph, cv14, ce14, qd;
+    std::vector<VsDev> vstates;   // V-McMD states (one for the one-state mcmd_* form)
+    std::vector<uint32_t> mt;     // generator at the system's first step ([OG_MT_WORDS])
     int d_free = 0;
+};
+
+// Host side of one system's V-McMD logs: entries moved off the device ring and not yet taken.
+// Entry k (1-based) of a log belongs to step k * interval; next_k is the first entry still on
+// the ring only.
+struct VmLog {
+    long long vs_next_k = 1, lam_next_k = 1;
+    std::vector<long long> vs_step, lam_step;
+    std::vector<int32_t> vs;
+    std::vector<double> lam;
+    size_t vs_head = 0, lam_head = 0;  // entries before the head were taken
 };
 
 template <class T>
@@ -257,6 +272,15 @@ struct og_engine {
     double variant_ms[OG_N_PAIR_VARIANTS] = {};
     int timing = 0;  // 1: step + per-pair-kernel events (kernel by kernel); 2: step events only
     std::vector<void *> allocs;
+    // V-McMD: state table, per-system current state, per-slot generators and log rings
+    VsDev *d_vstates = nullptr;
+    int *d_vs_cur = nullptr, *d_vs_log = nullptr, *d_vm_snap_cur = nullptr;
+    unsigned *d_mt = nullptr, *d_vm_snap_mt = nullptr;
+    double *d_lambda_log = nullptr;
+    int n_vm = 0, vm_log_cap = 0, vm_advance = 0;
+    std::vector<int> vm_sys;      // system of each slot
+    std::vector<VmLog> vm;        // per slot
+    long long vm_limit = 0;       // host_step up to which no ring overflows before a drain
 };
 
 namespace {
@@ -707,7 +731,9 @@ og_status reduce_potential(og_engine *e) {
     if (e->n_nb14 && (s = seg_sum<2>(e, e->d_e_nb14, 2, 0, e->d_seg_nb14, e->mc_nb14, e->d_sys_acc, OG_ACC_SIZE,
                                      OG_ACC_VDW14, 0)))
         return s;
-    k_mcmd_factor<<<blocks(e->n_sys, 128), 128, 0, e->stream>>>(e->n_sys, e->d_sys, e->d_sys_acc, e->d_mcmd);
+    k_vmcmd<<<e->n_sys, 32, 0, e->stream>>>(e->n_sys, e->d_sys, e->d_vstates, e->d_sys_acc, e->d_step, e->vm_advance,
+                                             e->d_vs_cur, e->d_mt, e->d_vs_log, e->d_lambda_log, e->vm_log_cap,
+                                             e->d_mcmd);
     LAUNCH_CHECK();
     return OG_OK;
 }
@@ -862,7 +888,9 @@ og_status run_step(og_engine *e, bool ene) {
         s = build_list(e);
         if (s) return s;
     }
+    e->vm_advance = 1;  // V-McMD transitions and logs belong to steps only
     s = compute_forces(e, false, ene || e->any_mcmd || e->trace_cap > 0);
+    e->vm_advance = 0;
     if (s) return s;
     k_update_velocities<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys, e->d_mcmd,
                                                                   e->d_work, e->d_mass_inv, e->d_vel,
@@ -905,6 +933,93 @@ og_status run_step(og_engine *e, bool ene) {
     k_trace_advance<<<1, 32, 0, st>>>(e->d_trace_count, e->d_step);
     LAUNCH_CHECK();
     e->host_step++;
+    return OG_OK;
+}
+
+// ---- V-McMD logs: the device rings hold the entries of recent steps; these move them to the
+// host before a ring would wrap.
+long long vm_entries_end(long long g, int intvl) {  // entries of steps 0..g-1: k = 1..result
+    return g > 0 ? (g - 1) / intvl : 0;
+}
+
+void vm_update_limit(og_engine *e) {
+    long long lim = LLONG_MAX;
+    for (int m = 0; m < e->n_vm; m++) {
+        const SysDev &D = e->sys[e->vm_sys[m]].dev;
+        const VmLog &L = e->vm[m];
+        lim = std::min(lim, (L.vs_next_k + e->vm_log_cap) * D.vs_trans_intvl - D.first_step);
+        if (D.vs_lambda_intvl > 0)
+            lim = std::min(lim, (L.lam_next_k + e->vm_log_cap) * D.vs_lambda_intvl - D.first_step);
+    }
+    e->vm_limit = lim;
+}
+
+// Synchronises the stream and moves every ring entry of the steps run so far to the host.
+og_status vm_drain(og_engine *e) {
+    if (e->n_vm == 0) return OG_OK;
+    const size_t n = (size_t)e->n_vm * e->vm_log_cap;
+    std::vector<int32_t> vs(n);
+    std::vector<double> lam(n);
+    CK(cudaMemcpyAsync(vs.data(), e->d_vs_log, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaMemcpyAsync(lam.data(), e->d_lambda_log, sizeof(double) * n, cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    for (int m = 0; m < e->n_vm; m++) {
+        const SysDev &D = e->sys[e->vm_sys[m]].dev;
+        VmLog &L = e->vm[m];
+        const long long g = D.first_step + e->host_step;
+        const size_t ring = (size_t)m * e->vm_log_cap;
+        for (long long k = L.vs_next_k, ke = vm_entries_end(g, D.vs_trans_intvl); k <= ke; k++) {
+            L.vs_step.push_back(k * D.vs_trans_intvl);
+            L.vs.push_back(vs[ring + (size_t)((k - 1) % e->vm_log_cap)]);
+            L.vs_next_k = k + 1;
+        }
+        if (D.vs_lambda_intvl > 0)
+            for (long long k = L.lam_next_k, ke = vm_entries_end(g, D.vs_lambda_intvl); k <= ke; k++) {
+                L.lam_step.push_back(k * D.vs_lambda_intvl);
+                L.lam.push_back(lam[ring + (size_t)((k - 1) % e->vm_log_cap)]);
+                L.lam_next_k = k + 1;
+            }
+    }
+    vm_update_limit(e);
+    return OG_OK;
+}
+
+// Before steps [host_step, host_step + n): drain first when a ring would wrap during them.
+og_status vm_reserve(og_engine *e, long long n) {
+    if (e->n_vm == 0 || e->host_step + n <= e->vm_limit) return OG_OK;
+    return vm_drain(e);
+}
+
+template <class T>
+og_status vm_take(og_engine *e, int32_t sys, int64_t max, int64_t *step, T *val, int64_t *n, bool vs_log) {
+    if (!e || !e->finalized) return fail(e, OG_ERR_STATE, "V-McMD log read before og_finalize");
+    if (sys < 0 || sys >= e->n_sys || max < 0 || !n || (max > 0 && (!step || !val)))
+        return fail(e, OG_ERR_INVALID, "bad system id or output arrays");
+    const int m = e->sys[sys].dev.vm_slot;
+    if (m < 0) return fail(e, OG_ERR_INVALID, "system %d has no V-McMD transitions", sys);
+    og_status s = vm_drain(e);
+    if (s) return s;
+    VmLog &L = e->vm[m];
+    std::vector<long long> &st = vs_log ? L.vs_step : L.lam_step;
+    std::vector<T> &v = *reinterpret_cast<std::vector<T> *>(vs_log ? (void *)&L.vs : (void *)&L.lam);
+    size_t &head = vs_log ? L.vs_head : L.lam_head;
+    const int64_t avail = (int64_t)(st.size() - head);
+    if (max == 0) {
+        *n = avail;
+        return OG_OK;
+    }
+    const int64_t k = std::min(max, avail);
+    for (int64_t i = 0; i < k; i++) {
+        step[i] = st[head + i];
+        val[i] = v[head + i];
+    }
+    head += (size_t)k;
+    if (head == st.size()) {
+        st.clear();
+        v.clear();
+        head = 0;
+    }
+    *n = k;
     return OG_OK;
 }
 
@@ -1111,6 +1226,16 @@ og_status og_add_system(og_engine *e, const og_system_desc *d, int32_t *sys_id) 
     if (!e->sys.empty() && d->nsgrid_update_intvl != e->intvl)
         return fail(e, OG_ERR_INVALID, "all systems of one engine share nsgrid_update_intvl");
     if (d->mcmd_order > 7) return fail(e, OG_ERR_INVALID, "McMD polynomial order above 7");
+    if (d->n_vstates < 0 || (d->n_vstates > 0 && (!d->vs_order || !d->vs_lambda || !d->vs_prob || !d->vs_coef ||
+                                                   d->vmcmd_trans_interval < 1 || d->vmcmd_init_vs < 0 ||
+                                                   d->vmcmd_init_vs >= d->n_vstates ||
+                                                   d->vmcmd_lambda_log_interval < 0)))
+        return fail(e, OG_ERR_INVALID, "V-McMD needs state arrays, trans_interval >= 1 and an initial state in range");
+    for (int v = 0; v < d->n_vstates; v++)
+        if (d->vs_order[v] < 0 || d->vs_order[v] > 7)
+            return fail(e, OG_ERR_INVALID, "virtual state %d: polynomial order outside 0..7", v);
+    if (d->n_vstates > 0 && d->vmcmd_mt_state && d->vmcmd_mt_state[624] > 624)
+        return fail(e, OG_ERR_INVALID, "V-McMD generator position above 624");
     if (d->first_step < 0 || d->first_step % d->nsgrid_update_intvl != 0)
         return fail(e, OG_ERR_INVALID, "first_step must be a non-negative multiple of nsgrid_update_intvl");
     e->sys.emplace_back();
@@ -1140,6 +1265,37 @@ og_status og_add_system(og_engine *e, const og_system_desc *d, int32_t *sys_id) 
     cp(h.gstart, d->com_group_start, d->n_com_groups > 0 ? d->n_com_groups + 1 : 0);
     if (d->n_com_groups > 0) cp(h.gatoms, d->com_group_atoms, d->com_group_start[d->n_com_groups]);
     if (d->mcmd_order >= 0) cp(h.mcoef, d->mcmd_coef, d->mcmd_order + 1);
+    if (d->n_vstates > 0) {
+        // ExtendedVMcMD::set_vs_params / set_vs_poly_param (Extend.cpp:266-283)
+        int c0 = 0;
+        for (int v = 0; v < d->n_vstates; v++) {
+            VsDev V{};
+            V.lo = d->vs_lambda[2 * v];
+            V.hi = d->vs_lambda[2 * v + 1];
+            V.p_down = d->vs_prob[2 * v];
+            V.p_up = d->vs_prob[2 * v + 1];
+            V.order = d->vs_order[v];
+            for (int i = 0; i <= V.order; i++) V.coef[i] = d->vs_coef[c0 + i];
+            c0 += V.order + 1;
+            h.vstates.push_back(V);
+        }
+        h.mt.resize(OG_MT_WORDS);
+        if (d->vmcmd_mt_state) {
+            std::copy(d->vmcmd_mt_state, d->vmcmd_mt_state + OG_MT_WORDS, h.mt.begin());
+        } else {
+            // std::mt19937::seed: x0 = seed, x_i = 1812433253 (x_{i-1} ^ (x_{i-1} >> 30)) + i
+            h.mt[0] = d->vmcmd_seed;
+            for (uint32_t i = 1; i < 624; i++) h.mt[i] = 1812433253u * (h.mt[i - 1] ^ (h.mt[i - 1] >> 30)) + i;
+            h.mt[624] = 624;
+        }
+    } else if (d->mcmd_order >= 0) {
+        VsDev V{};
+        V.lo = d->mcmd_lambda_low;
+        V.hi = d->mcmd_lambda_high;
+        V.order = d->mcmd_order;
+        for (int i = 0; i <= V.order; i++) V.coef[i] = h.mcoef[i];
+        h.vstates.push_back(V);
+    }
     if ((d->n_torsions > 0 && (!d->torsion || !d->torsion_ene || !d->torsion_phase || !d->torsion_overlaps ||
                                !d->torsion_symmetry)) ||
         (d->n_impros > 0 && (!d->impro || !d->impro_ene || !d->impro_phase || !d->impro_overlaps ||
@@ -1242,6 +1398,9 @@ og_status og_finalize(og_engine *e) {
     std::vector<int2> nb14v, nb14t;
     std::vector<double2> nb14c;
     std::vector<double> squad_d2;
+    std::vector<VsDev> vstates;
+    std::vector<int> vs_cur;
+    std::vector<uint32_t> mt_all;
     {
         size_t n_all = 0, x_all = 0, e_all = 0;
         for (const HostSystem &h : e->sys) {
@@ -1281,12 +1440,22 @@ og_status og_finalize(og_engine *e) {
         double tau = d.berendsen_tau;
         if (d.time_step < tau) tau = d.time_step;
         D.tau_inv = 1.0 / tau;
-        D.mcmd_order = d.mcmd_order;
-        e->any_mcmd |= d.mcmd_order >= 0;
-        D.mcmd_lo = d.mcmd_lambda_low;
-        D.mcmd_hi = d.mcmd_lambda_high;
+        D.n_vs = (int)h.vstates.size();
+        e->any_mcmd |= D.n_vs > 0;
+        D.vs_base = (int)vstates.size();
+        vstates.insert(vstates.end(), h.vstates.begin(), h.vstates.end());
         D.mcmd_k = (OG_GAS_CONST / OG_JOULE_CAL) * 1e-3 * d.mcmd_temperature;
-        for (int i = 0; i < 8; i++) D.mcmd_coef[i] = (d.mcmd_order >= 0 && i <= d.mcmd_order) ? h.mcoef[i] : 0.0;
+        D.first_step = d.first_step;
+        D.vm_slot = -1;
+        D.vs_trans_intvl = D.vs_lambda_intvl = 0;
+        vs_cur.push_back(d.n_vstates > 0 ? d.vmcmd_init_vs : 0);
+        if (d.n_vstates > 0) {
+            D.vm_slot = (int)e->vm_sys.size();
+            D.vs_trans_intvl = d.vmcmd_trans_interval;
+            D.vs_lambda_intvl = d.vmcmd_lambda_log_interval;
+            e->vm_sys.push_back(k);
+            mt_all.insert(mt_all.end(), h.mt.begin(), h.mt.end());
+        }
         D.self_energy = self_energy(h);
         D.excess_base = (int)excess.size();
         D.n_excess = h.n_excess;
@@ -1486,6 +1655,25 @@ og_status og_finalize(og_engine *e) {
         (s = dalloc(e, &e->d_sys_fault, S)) || (s = dalloc(e, &e->d_snap_ctr, 2)) ||
         (s = dalloc(e, &e->d_cell_excl, (size_t)OG_CELL_EXCL * cells_cap)))
         return s;
+    // V-McMD: a ring of log entries per slot, long enough for one list interval of entries, so
+    // that og_step can drain it between graph replays
+    e->n_vm = (int)e->vm_sys.size();
+    e->vm_log_cap = std::max(4096, e->intvl + 2);
+    e->vm.assign(e->n_vm, VmLog{});
+    for (int m = 0; m < e->n_vm; m++) {
+        const SysDev &D = sd[e->vm_sys[m]];
+        // the first entries this engine writes: steps k * interval >= first_step, k >= 1
+        e->vm[m].vs_next_k = std::max(1LL, (D.first_step + D.vs_trans_intvl - 1) / D.vs_trans_intvl);
+        if (D.vs_lambda_intvl > 0)
+            e->vm[m].lam_next_k = std::max(1LL, (D.first_step + D.vs_lambda_intvl - 1) / D.vs_lambda_intvl);
+    }
+    vm_update_limit(e);
+    if ((s = upload(e, &e->d_vstates, vstates)) || (s = upload(e, &e->d_vs_cur, vs_cur)) ||
+        (s = dalloc(e, &e->d_vm_snap_cur, S)) || (s = upload(e, &e->d_mt, mt_all)) ||
+        (s = dalloc(e, &e->d_vm_snap_mt, mt_all.size())) ||
+        (s = dalloc(e, &e->d_vs_log, (size_t)e->n_vm * e->vm_log_cap)) ||
+        (s = dalloc(e, &e->d_lambda_log, (size_t)e->n_vm * e->vm_log_cap)))
+        return s;
     {
         std::vector<int> sa(S + 1), se(S + 1), sb(S + 1), sg(S + 1), st(S + 1), si(S + 1), s14(S + 1);
         int ma = 1, mcl = 1, me = 1, mb = 1, mg = 1, mt = 1, mi = 1, m14 = 1;
@@ -1580,7 +1768,21 @@ og_status og_step(og_engine *e, int32_t n_steps) {
     // snapshot for a capacity retry: crd, vel_next and the step counters
     if (!e->d_snap && (s = dalloc(e, &e->d_snap, 6 * (size_t)e->n_atoms))) return s;
     const long long step0 = e->host_step;
+    // V-McMD log positions at the call's start, for an undo
+    struct VmMark {
+        long long vs_k, lam_k;
+        size_t vs_n, lam_n;
+    };
+    std::vector<VmMark> vm0(e->n_vm);
+    for (int m = 0; m < e->n_vm; m++)
+        vm0[m] = {e->vm[m].vs_next_k, e->vm[m].lam_next_k, e->vm[m].vs.size(), e->vm[m].lam.size()};
     for (int attempt = 0; attempt < 3; attempt++) {
+        if (e->n_vm) {
+            CK(cudaMemcpyAsync(e->d_vm_snap_cur, e->d_vs_cur, sizeof(int) * e->n_sys, cudaMemcpyDeviceToDevice,
+                               e->stream));
+            CK(cudaMemcpyAsync(e->d_vm_snap_mt, e->d_mt, sizeof(unsigned) * OG_MT_WORDS * e->n_vm,
+                               cudaMemcpyDeviceToDevice, e->stream));
+        }
         CK(cudaMemcpyAsync(e->d_snap, e->d_crd, sizeof(double) * 3 * e->n_atoms, cudaMemcpyDeviceToDevice, e->stream));
         CK(cudaMemcpyAsync(e->d_snap + 3 * (size_t)e->n_atoms, e->d_vel_next, sizeof(double) * 3 * e->n_atoms,
                            cudaMemcpyDeviceToDevice, e->stream));
@@ -1593,6 +1795,7 @@ og_status og_step(og_engine *e, int32_t n_steps) {
         for (int i = 0; i < n_steps;) {
             // whole list intervals replay the captured graph (not while per-kernel timing is on)
             if (e->use_graphs && e->timing != 1 && e->host_step % e->intvl == 0 && n_steps - i >= e->intvl) {
+                if ((s = vm_reserve(e, e->intvl))) return s;
                 if (!e->graph_exec && (s = capture_interval(e))) return s;
                 if (e->graph_exec) {
                     CK(cudaGraphLaunch(e->graph_exec, e->stream));
@@ -1603,6 +1806,7 @@ og_status og_step(og_engine *e, int32_t n_steps) {
                     continue;
                 }
             }
+            if ((s = vm_reserve(e, 1))) return s;
             if ((s = run_step(e, i == n_steps - 1))) return s;
             i++;
         }
@@ -1639,8 +1843,24 @@ og_status og_step(og_engine *e, int32_t n_steps) {
         CK(cudaMemcpyAsync(e->d_step, e->d_snap_ctr, sizeof(long long), cudaMemcpyDeviceToDevice, e->stream));
         CK(cudaMemcpyAsync(e->d_trace_count, e->d_snap_ctr + 1, sizeof(long long), cudaMemcpyDeviceToDevice,
                            e->stream));
+        if (e->n_vm) {
+            CK(cudaMemcpyAsync(e->d_vs_cur, e->d_vm_snap_cur, sizeof(int) * e->n_sys, cudaMemcpyDeviceToDevice,
+                               e->stream));
+            CK(cudaMemcpyAsync(e->d_mt, e->d_vm_snap_mt, sizeof(unsigned) * OG_MT_WORDS * e->n_vm,
+                               cudaMemcpyDeviceToDevice, e->stream));
+            for (int m = 0; m < e->n_vm; m++) {
+                VmLog &L = e->vm[m];
+                L.vs_next_k = vm0[m].vs_k;
+                L.lam_next_k = vm0[m].lam_k;
+                L.vs.resize(vm0[m].vs_n);
+                L.vs_step.resize(vm0[m].vs_n);
+                L.lam.resize(vm0[m].lam_n);
+                L.lam_step.resize(vm0[m].lam_n);
+            }
+        }
         CK(cudaStreamSynchronize(e->stream));
         e->host_step = step0;
+        vm_update_limit(e);
         // the list must be rebuilt from the restored coordinates before the first step
         if (step0 % e->intvl != 0) {
             if ((s = build_list_checked(e))) return s;
@@ -1868,6 +2088,30 @@ og_status og_get_sizes(og_engine *e, int32_t *n_systems, int64_t *n_atoms_total)
     return OG_OK;
 }
 
+og_status og_get_vmcmd_state(og_engine *e, int32_t sys, int32_t *cur_vs, uint32_t *mt_state) {
+    if (!e || !e->finalized) return fail(e, OG_ERR_STATE, "og_get_vmcmd_state before og_finalize");
+    if (sys < 0 || sys >= e->n_sys) return fail(e, OG_ERR_INVALID, "bad system id");
+    const SysDev &D = e->sys[sys].dev;
+    if (D.n_vs == 0) return fail(e, OG_ERR_INVALID, "system %d has no V-McMD", sys);
+    if (cur_vs) CK(cudaMemcpyAsync(cur_vs, e->d_vs_cur + sys, sizeof(int32_t), cudaMemcpyDeviceToHost, e->stream));
+    if (mt_state) {
+        if (D.vm_slot < 0) return fail(e, OG_ERR_INVALID, "system %d has one virtual state and no generator", sys);
+        CK(cudaMemcpyAsync(mt_state, e->d_mt + (size_t)OG_MT_WORDS * D.vm_slot, sizeof(uint32_t) * OG_MT_WORDS,
+                           cudaMemcpyDeviceToHost, e->stream));
+    }
+    CK(cudaStreamSynchronize(e->stream));
+    return OG_OK;
+}
+
+
+og_status og_take_vs_log(og_engine *e, int32_t sys, int64_t max, int64_t *step, int32_t *vs, int64_t *n) {
+    return vm_take<int32_t>(e, sys, max, step, vs, n, true);
+}
+
+og_status og_take_lambda_log(og_engine *e, int32_t sys, int64_t max, int64_t *step, double *lambda, int64_t *n) {
+    return vm_take<double>(e, sys, max, step, lambda, n, false);
+}
+
 // Per-step timing of the pair kernel (CUDA events on the engine's stream).  Not in the public
 // header's main list: enabled by the benchmark.
 og_status og_set_timing(og_engine *e, int32_t on) {
@@ -1933,7 +2177,9 @@ extern "C" og_status og_step_async(og_engine *e, int32_t n_steps) {
     // checks og_get_flags at its own sync points
     if (!e || !e->finalized) return fail(e, OG_ERR_STATE, "og_step_async before og_finalize");
     for (int i = 0; i < n_steps; i++) {
-        og_status s = run_step(e, i == n_steps - 1);
+        og_status s = vm_reserve(e, 1);  // synchronises only when a V-McMD log ring is full
+        if (s) return s;
+        s = run_step(e, i == n_steps - 1);
         if (s) return s;
     }
     return OG_OK;

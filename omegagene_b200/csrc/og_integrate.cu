@@ -331,30 +331,129 @@ template __global__ void k_part_final<3>(const double *, int, double *, int, int
 template __global__ void k_part_final<9>(const double *, int, double *, int, int, const float *, int);
 template __global__ void k_part_final<10>(const double *, int, double *, int, int, const float *, int);
 
-// McMD factor and the potential used for it, one thread per system (Extend.cpp:178-203,
-// MmSystem::set_potential_e).
-__global__ void k_mcmd_factor(int n_sys, const SysDev *__restrict__ sys, const double *__restrict__ sys_acc,
-                              double *__restrict__ mcmd_factor) {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
+// ------------------------------------------------------------------ V-McMD
+// std::mt19937: the Mersenne Twister of Matsumoto & Nishimura (ACM TOMACS 8, 1998) with the
+// parameters the C++ standard gives mt19937 ([rand.predef]: n 624, m 397, r 31, a 0x9908b0df,
+// tempering u 11, s 7 b 0x9d2c5680, t 15 c 0xefc60000, l 18).  The reference draws
+// generator() / double(generator.max()) (random::Random::operator(), Random.cpp:25-28).
+// State: 624 words and the next position in word 624.  One warp advances a generator; the
+// twist runs in two data-parallel ranges: words 0..226 read only old words, words 227..622 read
+// the word 227 places back, already new, and word 623 reads new words 396 and 0.
+__device__ __forceinline__ unsigned og_mt_mix(unsigned a, unsigned b, unsigned c) {
+    const unsigned y = (a & 0x80000000u) | (b & 0x7fffffffu);
+    return c ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+}
+
+__device__ void og_mt_twist_warp(unsigned *st, int lane) {
+    for (int b = 0; b < 227; b += 32) {
+        const int i = b + lane;
+        unsigned v = 0;
+        if (i < 227) v = og_mt_mix(st[i], st[i + 1], st[i + 397]);
+        __syncwarp();
+        if (i < 227) st[i] = v;
+        __syncwarp();
+    }
+    // a 32-word block [b, b+32) with b >= 227 reads words i-227 < b: all rewritten before it
+    for (int b = 227; b < 623; b += 32) {
+        const int i = b + lane;
+        unsigned v = 0;
+        if (i < 623) v = og_mt_mix(st[i], st[i + 1], st[i - 227]);
+        __syncwarp();
+        if (i < 623) st[i] = v;
+        __syncwarp();
+    }
+    if (lane == 0) st[623] = og_mt_mix(st[623], st[0], st[396]);
+    __syncwarp();
+}
+
+// Next tempered word; every lane of the warp calls it with the same position.
+__device__ unsigned og_mt_next(unsigned *st, int &pos, int lane) {
+    if (pos >= 624) {
+        og_mt_twist_warp(st, lane);
+        pos = 0;
+    }
+    unsigned y = st[pos++];
+    y ^= y >> 11;
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    y ^= y >> 18;
+    return y;
+}
+
+__device__ __forceinline__ bool og_vs_in_range(const VsDev &v, double lambda) {
+    return lambda >= v.lo && lambda <= v.hi;  // VirtualState::is_in_range, Extend.cpp:53-55
+}
+
+// ExtendedVMcMD::trial_transition (Extend.cpp:160-177): a draw is made only when the neighbour
+// state exists and holds lambda; the move is taken when the draw exceeds 1 - probability.
+__device__ int og_vs_trial(const VsDev *V, int n_vs, int src, int rel, double lambda, unsigned *st, int &pos,
+                           int lane) {
+    if (!og_vs_in_range(V[src], lambda)) return src;
+    if (src == 0 && rel == -1) return src;
+    if (src == n_vs - 1 && rel == 1) return src;
+    if (og_vs_in_range(V[src + rel], lambda)) {
+        const double rnd = (double)og_mt_next(st, pos, lane) / 4294967295.0;
+        const double prob = rel == 1 ? V[src].p_up : V[src].p_down;
+        if (rnd > (1.0 - prob)) return src + rel;
+    }
+    return src;
+}
+
+// V-McMD per step, one warp per system (ExtendedVMcMD::apply_bias, Extend.cpp:126-143): the
+// step's potential is lambda (MmSystem::set_potential_e); at a transition step the state moves
+// (set_current_vstate, Extend.cpp:144-158) and is logged, every lambda-log step lambda is logged,
+// and the force factor is const_k * the state's polynomial at lambda clamped to the state's range
+// (scale_force, Extend.cpp:178-203).  advance = 0 (a force evaluation outside a step) leaves the
+// state, generator and logs alone.
+__global__ void k_vmcmd(int n_sys, const SysDev *__restrict__ sys, const VsDev *__restrict__ vstates,
+                        const double *__restrict__ sys_acc, const long long *__restrict__ step, int advance,
+                        int *__restrict__ vs_cur, unsigned *__restrict__ mt, int *__restrict__ vs_log,
+                        double *__restrict__ lambda_log, int log_cap, double *__restrict__ mcmd_factor) {
+    const int s = blockIdx.x, lane = threadIdx.x;
     if (s >= n_sys) return;
     const SysDev &S = sys[s];
-    const double *acc = sys_acc + OG_ACC_SIZE * s;
-    double f = 1.0;
-    if (S.mcmd_order >= 0) {
-        const double lambda = acc[OG_ACC_VDW] + acc[OG_ACC_ELE] + acc[OG_ACC_EXCESS] + S.self_energy +
-                              acc[OG_ACC_BOND] + acc[OG_ACC_ANGLE] + acc[OG_ACC_TORSION] + acc[OG_ACC_IMPRO] +
-                              acc[OG_ACC_VDW14] + acc[OG_ACC_ELE14];
-        double param = lambda;
-        if (lambda <= S.mcmd_lo) param = S.mcmd_lo;
-        else if (lambda >= S.mcmd_hi) param = S.mcmd_hi;
-        double dlnp = S.mcmd_coef[0], t = 1.0;
-        for (int i = 1; i < S.mcmd_order + 1; i++) {
-            t *= param;
-            dlnp += S.mcmd_coef[i] * t;
-        }
-        f = S.mcmd_k * dlnp;
+    if (S.n_vs == 0) {
+        if (lane == 0) mcmd_factor[s] = 1.0;
+        return;
     }
-    mcmd_factor[s] = f;
+    const double *acc = sys_acc + OG_ACC_SIZE * s;
+    // MmSystem::set_potential_e's order (MmSystem.cpp:738-742)
+    const double lambda = acc[OG_ACC_BOND] + acc[OG_ACC_ANGLE] + acc[OG_ACC_TORSION] + acc[OG_ACC_IMPRO] +
+                          acc[OG_ACC_VDW14] + acc[OG_ACC_ELE14] + acc[OG_ACC_VDW] +
+                          (acc[OG_ACC_ELE] + acc[OG_ACC_EXCESS] + S.self_energy);
+    const VsDev *V = vstates + S.vs_base;
+    int cur = vs_cur[s];
+    if (advance && S.vm_slot >= 0) {
+        const long long g = *step + S.first_step;
+        const size_t ring = (size_t)S.vm_slot * log_cap;
+        if (g > 0 && g % S.vs_trans_intvl == 0) {
+            unsigned *st = mt + (size_t)OG_MT_WORDS * S.vm_slot;
+            int pos = (int)st[624];
+            int dest = og_vs_trial(V, S.n_vs, cur, 1, lambda, st, pos, lane);
+            if (dest == cur) dest = og_vs_trial(V, S.n_vs, cur, -1, lambda, st, pos, lane);
+            cur = dest;
+            __syncwarp();
+            if (lane == 0) {
+                st[624] = (unsigned)pos;
+                vs_cur[s] = cur;
+                vs_log[ring + (size_t)((g / S.vs_trans_intvl - 1) % log_cap)] = cur;
+            }
+        }
+        if (lane == 0 && g > 0 && S.vs_lambda_intvl > 0 && g % S.vs_lambda_intvl == 0)
+            lambda_log[ring + (size_t)((g / S.vs_lambda_intvl - 1) % log_cap)] = lambda;
+    }
+    if (lane == 0) {
+        const VsDev &v = V[cur];
+        double param = lambda;
+        if (lambda <= v.lo) param = v.lo;
+        else if (lambda >= v.hi) param = v.hi;
+        double dlnp = v.coef[0], t = 1.0;
+        for (int i = 1; i < v.order + 1; i++) {
+            t *= param;
+            dlnp += v.coef[i] * t;
+        }
+        mcmd_factor[s] = S.mcmd_k * dlnp;
+    }
 }
 
 // vel_next -= moment of the atom's COM group (moment already divided by the group mass).
@@ -374,7 +473,7 @@ __global__ void k_update_velocities(int n_atoms, const int *__restrict__ atom_sy
     for (int q = 0; q < 3; q++) {
         const int k = 3 * a + q;
         double w = work[k];
-        if (S.mcmd_order >= 0) {
+        if (S.n_vs > 0) {
             w *= f;
             work[k] = w;
         }

@@ -70,14 +70,23 @@ struct SysDev {
     double self_energy;
     int thermostat;
     int has_constraints;
-    // McMD
-    int mcmd_order;
-    double mcmd_lo, mcmd_hi, mcmd_k;  // const_k = (GAS_CONST/JOULE_CAL) 1e-3 T
-    double mcmd_coef[8];
+    // V-McMD (ExtendedVMcMD, Extend.cpp:56-203): n_vs virtual states from vs_base of the state
+    // table, n_vs = 0 when off.  vm_slot indexes the generator and log rings (-1: no transitions).
+    int n_vs, vs_base, vm_slot, vs_trans_intvl, vs_lambda_intvl;
+    long long first_step;             // step number of the engine's first step for this system
+    double mcmd_k;                    // const_k = (GAS_CONST/JOULE_CAL) 1e-3 T
     // constraint / term ranges (global index spaces of their own arrays)
     int trio_base, n_trio, pair_base, n_pair;
     int excess_base, n_excess, bond_base, n_bonds, angle_base, n_angles;
     int tors_base, n_tors, impro_base, n_impro, nb14_base, n_nb14;
+};
+
+// One virtual state (VirtualState, Extend.cpp:20-55): lambda range, transition probabilities
+// (trans_prob[0] down, trans_prob[1] up) and the d ln P / d lambda polynomial in raw powers.
+struct VsDev {
+    double lo, hi, p_down, p_up;
+    double coef[8];
+    int order;
 };
 
 // per-system reduction slots in d_sys_acc (double)

@@ -62,7 +62,13 @@ class SystemDesc(C.Structure):
         ("nb14_coeff_vdw", _p(C.c_double)), ("nb14_coeff_ele", _p(C.c_double)),
         ("n_shake_quad", C.c_int32), ("shake_quad", _p(C.c_int32)), ("shake_quad_dist", _p(C.c_double)),
         ("dof_extra", C.c_int32),
+        ("n_vstates", C.c_int32), ("vmcmd_trans_interval", C.c_int32), ("vmcmd_init_vs", C.c_int32),
+        ("vmcmd_lambda_log_interval", C.c_int32), ("vmcmd_seed", C.c_uint32),
+        ("vs_order", _p(C.c_int32)), ("vs_lambda", _p(C.c_double)), ("vs_prob", _p(C.c_double)),
+        ("vs_coef", _p(C.c_double)), ("vmcmd_mt_state", _p(C.c_uint32)),
     ]
+
+OG_MT_WORDS = 625
 
 
 _lib = None
@@ -98,6 +104,9 @@ def load_library():
         "og_set_graphs": [E, C.c_int32], "og_release_pool_memory": [C.c_int32],
         "og_get_system_faults": [E, C.c_void_p],
         "og_get_graph_info": [E, _p(C.c_int32), _p(C.c_int64), _p(C.c_int64), C.c_char_p],
+        "og_get_vmcmd_state": [E, C.c_int32, _p(C.c_int32), C.c_void_p],
+        "og_take_vs_log": [E, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, _p(C.c_int64)],
+        "og_take_lambda_log": [E, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, _p(C.c_int64)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -118,6 +127,8 @@ DEFAULT_PARAMS = {
     "temperature": 300.0, "temperature_init": -1.0, "heating_steps": 0, "berendsen_tau": 0.0,
     "const_max_loops": 1000, "const_tolerance": 1e-7, "thermo_const_max_loops": 100,
     "thermo_const_tolerance": 1e-5, "com_motion": "cancel", "com_cancel_groups": None, "constraint": "shake",
+    "extended_ensemble": "none", "random_seed": -1, "print_intvl_extended_lambda": 0,
+    "fn_o_vmcmd_log": None, "fn_o_extended_lambda": None, "format_o_extended_lambda": "binary",
 }
 
 
@@ -135,7 +146,7 @@ def parse_run_config(text):
     accepted_ignored = {"--processor", "--gpu-device-id", "--mode", "--n-steps", "--print-interval-log",
                         "--print-interval-coord", "--fn-o-coord", "--format-o-coord", "--group-o-coord",
                         "--fn-o-log", "--fn-o-energy", "--fn-o-restart", "--integrator", "--electrostatic",
-                        "--ele-alpha", "--expected-num-density", "--random-seed"}
+                        "--ele-alpha", "--expected-num-density"}
     i = 0
     while i < len(toks):
         k = toks[i]
@@ -173,6 +184,21 @@ def parse_run_config(text):
             groups.append(v)
         elif k == "--constraint":
             p["constraint"] = v
+        elif k == "--extended-ensemble":
+            # Config.cpp:145-157; V-AUS and VcMD are not on this path
+            if v not in ("none", "v-mcmd"):
+                raise ValueError("--extended-ensemble %s is not on the hot path (none, v-mcmd)" % v)
+            p["extended_ensemble"] = v
+        elif k == "--random-seed":
+            p["random_seed"] = int(v)
+        elif k == "--print-interval-extended-lambda":
+            p["print_intvl_extended_lambda"] = int(v)
+        elif k == "--fn-o-vmcmd-log":
+            p["fn_o_vmcmd_log"] = v
+        elif k == "--fn-o-extended-lambda":
+            p["fn_o_extended_lambda"] = v
+        elif k == "--format-o-extended-lambda":
+            p["format_o_extended_lambda"] = v
         elif k in accepted_ignored:
             if k == "--integrator" and v != "leapfrog-presto":
                 raise ValueError("only --integrator leapfrog-presto is on the hot path")
@@ -278,13 +304,48 @@ def make_desc(system, params=None, mcmd=None, first_step=0):
     d.dof_extra = int(system.get("dof_extra", 0))
     d.first_step = int(first_step)
     d.mcmd_order = -1
-    if mcmd is not None:
+    if mcmd is not None and "states" in mcmd:
+        _vmcmd_desc(d, keep, mcmd, prm)
+    elif mcmd is not None:
         keep.mcoef = np.ascontiguousarray(mcmd["coef"], np.float64)
         d.mcmd_order = len(keep.mcoef) - 1
         d.mcmd_lambda_low, d.mcmd_lambda_high = mcmd["lambda_low"], mcmd["lambda_high"]
         d.mcmd_temperature = mcmd["temperature"]
         d.mcmd_coef = _ptr(keep.mcoef, C.c_double)
     return d, keep
+
+
+def vmcmd_seed(params):
+    """The generator seed of a V-McMD run: --random-seed, or, when it is negative, a fresh one
+    from the OS (the reference seeds from std::random_device then, DynamicsMode.cpp:79-84)."""
+    seed = int(params.get("random_seed", -1))
+    if seed < 0:
+        seed = int.from_bytes(os.urandom(4), "little") & 0x7FFFFFFF
+    return seed & 0xFFFFFFFF
+
+
+def _vmcmd_desc(d, keep, v, prm):
+    """Fills the V-McMD fields from the .cls section dict (cls_io: states, interval, temperature,
+    init_vs 1-based as in the file).  Optional keys: cur_vs (0-based) and mt_state, a run's state
+    handed over from another engine (Engine.vmcmd_state)."""
+    st = v["states"]
+    keep.vs_order = np.ascontiguousarray([len(x["coef"]) - 1 for x in st], np.int32)
+    keep.vs_lambda = np.ascontiguousarray([[x["lambda_low"], x["lambda_high"]] for x in st], np.float64).reshape(-1)
+    keep.vs_prob = np.ascontiguousarray([[x["prob_low"], x["prob_high"]] for x in st], np.float64).reshape(-1)
+    keep.vs_coef = np.ascontiguousarray(np.concatenate([np.asarray(x["coef"], np.float64) for x in st]))
+    d.n_vstates = len(st)
+    d.vmcmd_trans_interval = int(v["interval"])
+    d.vmcmd_init_vs = int(v["cur_vs"]) if "cur_vs" in v else int(v["init_vs"]) - 1
+    d.vmcmd_lambda_log_interval = int(prm.get("print_intvl_extended_lambda", 0) or 0)
+    d.vmcmd_seed = vmcmd_seed(prm)
+    d.mcmd_temperature = float(v["temperature"])
+    d.vs_order, d.vs_lambda = _ptr(keep.vs_order, C.c_int32), _ptr(keep.vs_lambda, C.c_double)
+    d.vs_prob, d.vs_coef = _ptr(keep.vs_prob, C.c_double), _ptr(keep.vs_coef, C.c_double)
+    if v.get("mt_state") is not None:
+        keep.mt = np.ascontiguousarray(v["mt_state"], np.uint32)
+        if keep.mt.shape != (OG_MT_WORDS,):
+            raise ValueError("mt_state needs %d words" % OG_MT_WORDS)
+        d.vmcmd_mt_state = _ptr(keep.mt, C.c_uint32)
 
 
 def release_pool_memory(device=0):
@@ -448,6 +509,33 @@ class Engine:
         self._check(self.L.og_get_graph_info(self.h, C.byref(en), C.byref(rep), C.byref(k), note), "og_get_graph_info")
         return {"enabled": bool(en.value), "replays": rep.value, "kernels_per_replay": k.value,
                 "note": note.value.decode()}
+
+    def vmcmd_state(self, sys):
+        """(current 0-based virtual state, generator words [625] or None for a one-state system)."""
+        cur = C.c_int32()
+        mt = np.zeros(OG_MT_WORDS, np.uint32)
+        st = self.L.og_get_vmcmd_state(self.h, sys, C.byref(cur), mt.ctypes.data)
+        if st == OG_ERR_INVALID:
+            self._check(self.L.og_get_vmcmd_state(self.h, sys, C.byref(cur), None), "og_get_vmcmd_state")
+            return cur.value, None
+        self._check(st, "og_get_vmcmd_state")
+        return cur.value, mt
+
+    def _take(self, fn, sys, dtype):
+        n = C.c_int64()
+        self._check(fn(self.h, sys, 0, None, None, C.byref(n)), "V-McMD log")
+        steps, vals = np.zeros(n.value, np.int64), np.zeros(n.value, dtype)
+        if n.value:
+            self._check(fn(self.h, sys, n.value, steps.ctypes.data, vals.ctypes.data, C.byref(n)), "V-McMD log")
+        return steps[:n.value], vals[:n.value]
+
+    def take_vs_log(self, sys):
+        """(steps, 0-based virtual states) logged since the last take (WriteTTPVMcMDLog lines)."""
+        return self._take(self.L.og_take_vs_log, sys, np.int32)
+
+    def take_lambda_log(self, sys):
+        """(steps, lambda) logged since the last take (ExtendedVMcMD::write_lambda rows)."""
+        return self._take(self.L.og_take_lambda_log, sys, np.float64)
 
     def system_faults(self):
         """Per-system fault bits of the last og_step that returned OG_ERR_SYSTEM_FAULT

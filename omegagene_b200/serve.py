@@ -9,6 +9,9 @@ boundary (a multiple of the pair-list interval) it does the following:
   velocities and its own step number, so its list-rebuild phase and heating schedule continue
   unchanged.
 
+A V-McMD job also carries its virtual state and its generator (og_get_vmcmd_state), and its
+virtual-state and lambda logs are collected into the job at every boundary.
+
 A job's trajectory is therefore the one it would have had alone. The engine's forces are
 fixed-point sums and its reductions are per system, so the match is exact;
 tests/test_gpu_serve.py checks it.
@@ -47,9 +50,24 @@ class Job:
         self.t_admit = None
         self.t_done = None
         self.energies = None
+        self.vs_log, self.lambda_log = [], []  # (step, 0-based state) / (step, lambda) of a V-McMD job
         intvl = self.params.get("nsgrid_update_intvl", 1)
         if self.n_steps % intvl:
             raise ValueError("job %s: n_steps must be a multiple of nsgrid_update_intvl" % job_id)
+
+    @property
+    def vmcmd(self):
+        return self.mcmd is not None and "states" in self.mcmd
+
+    def collect_vmcmd(self, eng, i):
+        """Moves this job's V-McMD logs out of engine slot i and keeps its virtual state and
+        generator, so that the next engine continues the run."""
+        st, vs = eng.take_vs_log(i)
+        self.vs_log += list(zip(st.tolist(), vs.tolist()))
+        st, lam = eng.take_lambda_log(i)
+        self.lambda_log += list(zip(st.tolist(), lam.tolist()))
+        cur, mt = eng.vmcmd_state(i)
+        self.mcmd = dict(self.mcmd, cur_vs=cur, mt_state=mt)
 
     @property
     def bytes(self):
@@ -127,6 +145,8 @@ class Server:
                     for i, j in enumerate(active):
                         j.crd, j.vel = eng.get_state(i)
                         j.energies = eng.get_energies(i)
+                        if j.vmcmd:
+                            j.collect_vmcmd(eng, i)
                     eng.close()
                     eng = None
                 now = self.clock() - t0
@@ -156,6 +176,8 @@ class Server:
                 t_re = self.clock()
                 for i, j in enumerate(active):
                     j.crd, j.vel = eng.get_state(i)
+                    if j.vmcmd:
+                        j.collect_vmcmd(eng, i)  # the undone call's entries are gone already
                 eng.close()
                 eng = None
                 now = self.clock() - t0
@@ -183,10 +205,11 @@ class Server:
                 "jobs": done}
 
 
-def run_alone(job, device=0, pair_variant="auto", warmup=0):
+def run_alone(job, device=0, pair_variant="auto", warmup=0, logs=None):
     """The plain path: one job, one engine, start to finish; returns (seconds, final energies,
     final positions, final velocities).  `warmup` extra steps run first, untimed (a timing aid:
-    the returned state is then `warmup` steps further on)."""
+    the returned state is then `warmup` steps further on).  For a V-McMD job, `logs` (a dict)
+    receives the "vs" and "lambda" logs as (step, value) lists."""
     eng = engine.Engine(device)
     if pair_variant != "auto":
         eng.set_tuning(pair_variant)
@@ -200,6 +223,11 @@ def run_alone(job, device=0, pair_variant="auto", warmup=0):
     dt = time.perf_counter() - t
     crd, vel = eng.get_state(0)
     ene = eng.get_energies(0)
+    if logs is not None and job.vmcmd:
+        st, vs = eng.take_vs_log(0)
+        logs["vs"] = list(zip(st.tolist(), vs.tolist()))
+        st, lam = eng.take_lambda_log(0)
+        logs["lambda"] = list(zip(st.tolist(), lam.tolist()))
     eng.close()
     return dt, ene, crd, vel
 

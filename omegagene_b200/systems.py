@@ -335,3 +335,23 @@ def mcmd_polynomial(e_mean, e_sd, seed, temperature=300.0, order=6):
         for i in range(k + 1):
             c[i] += a[k] * math.comb(k, i) * (-e_mean) ** (k - i) / half ** k
     return {"coef": c.tolist(), "lambda_low": lo, "lambda_high": hi, "temperature": temperature}
+
+
+def vmcmd_ladder(e_mean, e_sd, seed, n_vs=4, interval=10, temperature=300.0, order=6, prob=0.5):
+    """A V-McMD section for one walker, in the layout of the .cls "extended" section (cls_io;
+    Read::load_ls_vmcmd, Read.cpp:521-560): n_vs windows over [mean - 4 sd, mean + 4 sd], each
+    2 / (n_vs + 1) of the range wide, so that neighbours overlap by half a window; each window has
+    its own seeded polynomial (mcmd_polynomial over the window); moves to a neighbour are tried
+    with probability `prob` (0 off the ends of the ladder).  init_vs is 1-based as in the file."""
+    lo, hi = e_mean - 4.0 * e_sd, e_mean + 4.0 * e_sd
+    width = 2.0 * (hi - lo) / (n_vs + 1)
+    states = []
+    for v in range(n_vs):
+        a = lo + 0.5 * width * v
+        b = a + width
+        poly = mcmd_polynomial(0.5 * (a + b), width / 8.0, seed=seed * 31 + v, temperature=temperature, order=order)
+        states.append(dict(order=order, lambda_low=a, lambda_high=b, prob_low=0.0 if v == 0 else prob,
+                           prob_high=0.0 if v == n_vs - 1 else prob, coef=poly["coef"], alpha_low=0.0,
+                           alpha_high=0.0))
+    return {"n_vs": n_vs, "interval": interval, "temperature": temperature, "states": states,
+            "init_vs": 1 + n_vs // 2, "seed": seed}

@@ -1140,3 +1140,54 @@ double ogo_mcmd_scale(double lambda, double lo, double hi, int order, const doub
     for (int i = 0; i < 3 * n; i++) work[i] *= dew;
     return dew;
 }
+
+/* ------------------------------------------------------------------ V-McMD transitions */
+
+/* std::mt19937::seed (the C++ standard's [rand.eng.mers] initialisation): x0 = value,
+ * x_i = 1812433253 * (x_{i-1} xor (x_{i-1} >> 30)) + i; the next draw twists first. */
+void ogo_mt_seed(uint32_t *st, uint32_t seed) {
+    st[0] = seed;
+    for (uint32_t i = 1; i < 624; i++) st[i] = 1812433253u * (st[i - 1] ^ (st[i - 1] >> 30)) + i;
+    st[624] = 624;
+}
+
+/* One draw of mt19937 (Matsumoto & Nishimura 1998, genrand_int32), written word by word. */
+uint32_t ogo_mt_next(uint32_t *st) {
+    if (st[624] >= 624) {
+        for (int k = 0; k < 624; k++) {
+            uint32_t y = (st[k] & 0x80000000u) | (st[(k + 1) % 624] & 0x7fffffffu);
+            st[k] = st[(k + 397) % 624] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+        }
+        st[624] = 0;
+    }
+    uint32_t y = st[st[624]++];
+    y ^= y >> 11;
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    y ^= y >> 18;
+    return y;
+}
+
+static int vs_in_range(const double *lam, int v, double lambda) { /* Extend.cpp:53-55 */
+    return lambda >= lam[2 * v] && lambda <= lam[2 * v + 1];
+}
+
+/* ExtendedVMcMD::trial_transition (Extend.cpp:160-177); Random::operator() = draw / max. */
+static int vs_trial(int n_vs, const double *lam, const double *prob, int src, int rel, double lambda,
+                    uint32_t *st) {
+    if (!vs_in_range(lam, src, lambda)) return src;
+    if (src == 0 && rel == -1) return src;
+    if (src == n_vs - 1 && rel == 1) return src;
+    int up_down = rel == -1 ? 0 : rel;
+    if (vs_in_range(lam, src + rel, lambda)) {
+        double r = ogo_mt_next(st) / (double)0xffffffffu;
+        if (r > (1.0 - prob[2 * src + up_down])) return src + rel;
+    }
+    return src;
+}
+
+int ogo_vmcmd_transition(int n_vs, const double *lam, const double *prob, int cur, double lambda, uint32_t *st) {
+    int dest = vs_trial(n_vs, lam, prob, cur, 1, lambda, st);   /* Extend.cpp:144-158 */
+    if (dest != cur) return dest;
+    return vs_trial(n_vs, lam, prob, cur, -1, lambda, st);
+}

@@ -191,6 +191,13 @@ double ogo_kinetic(const ogo_integ *s, double *vel_just);          /* SubBox.cpp
 /* V-McMD force scaling (Extend.cpp:114-117,178-203); returns the factor. */
 double ogo_mcmd_scale(double lambda, double lam_low, double lam_high, int order, const double *coef,
                       double temperature, int n, double *work);
+/* std::mt19937 as random::Random draws it (src/celeste/random/Random.cpp:20-28): st[0..623] the
+ * words, st[624] the next position.  ogo_mt_seed = std::mt19937::seed(value). */
+void     ogo_mt_seed(uint32_t *st, uint32_t seed);
+uint32_t ogo_mt_next(uint32_t *st);
+/* ExtendedVMcMD::set_current_vstate + trial_transition (Extend.cpp:144-177): the state after one
+ * transition step; lam[2n] = low/high, prob[2n] = down/up of each state. */
+int ogo_vmcmd_transition(int n_vs, const double *lam, const double *prob, int cur, double lambda, uint32_t *st);
 
 #ifdef __cplusplus
 }

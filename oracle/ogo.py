@@ -88,6 +88,11 @@ def lib():
                                f64p, f64p, f64p]
         L.ogo_mcmd_scale.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int, f64p, C.c_double, C.c_int, f64p]
         L.ogo_mcmd_scale.restype = C.c_double
+        L.ogo_mt_seed.argtypes = [u32p, C.c_uint32]
+        L.ogo_mt_next.argtypes = [u32p]
+        L.ogo_mt_next.restype = C.c_uint32
+        L.ogo_vmcmd_transition.argtypes = [C.c_int, f64p, f64p, C.c_int, C.c_double, u32p]
+        L.ogo_vmcmd_transition.restype = C.c_int
         _lib = L
     return _lib
 
@@ -338,7 +343,10 @@ class OracleMD:
     the pair terms in FP64 over the reference's cell-pair list on the list's (unwrapped) grid
     positions; "allpairs_f32" restates the reference's all-pairs build (FP32 pair and excess
     terms, ``-DF_WO_NS``), whose output the ala3 sample log records.  ``params`` uses
-    engine.DEFAULT_PARAMS keys."""
+    engine.DEFAULT_PARAMS keys.  ``mcmd``: a one-state dict (coef, lambda_low, lambda_high,
+    temperature) or the .cls V-McMD section (cls_io: states, interval, temperature, init_vs),
+    whose transitions draw from std::mt19937 seeded with params["random_seed"]
+    (ExtendedVMcMD::apply_bias, Extend.cpp:126-143)."""
 
     def __init__(self, system, params, mcmd=None, pair_mode="cells_f64"):
         from omegagene_b200 import cls_io  # local import: oracle stays importable alone
@@ -425,6 +433,15 @@ class OracleMD:
             tau = self.p["time_step"]
         self.tau_inv = (1.0 / tau) if tau > 0 else float("inf")
         self.mcmd = mcmd
+        self.vm = mcmd if mcmd is not None and "states" in mcmd else None
+        if self.vm is not None:
+            st = self.vm["states"]
+            self.vs_lam = np.ascontiguousarray([[x["lambda_low"], x["lambda_high"]] for x in st], np.float64).reshape(-1)
+            self.vs_prob = np.ascontiguousarray([[x["prob_low"], x["prob_high"]] for x in st], np.float64).reshape(-1)
+            self.vs_cur = int(self.vm["init_vs"]) - 1
+            self.mt = np.zeros(625, np.uint32)
+            L.ogo_mt_seed(self.mt, int(self.p["random_seed"]) & 0xFFFFFFFF)
+            self.vs_log, self.lambda_log = [], []
         self.step_i = 0
         self.cl = None
         self.slot_crd = None
@@ -508,7 +525,23 @@ class OracleMD:
     def step(self):
         L, I = self.L, self.I
         ene = self.forces()
-        if self.mcmd is not None:
+        if self.vm is not None:
+            # MmSystem::set_potential_e's order (MmSystem.cpp:738-742)
+            lam = (ene["bond"] + ene["angle"] + ene["torsion"] + ene["improper"] + ene["vdw14"] + ene["ele14"] +
+                   ene["vdw"] + ene["ele"])
+            g = self.step_i
+            if g > 0 and g % int(self.vm["interval"]) == 0:
+                self.vs_cur = L.ogo_vmcmd_transition(len(self.vm["states"]), self.vs_lam, self.vs_prob, self.vs_cur,
+                                                     lam, self.mt)
+                self.vs_log.append((g, self.vs_cur))
+            li = int(self.p.get("print_intvl_extended_lambda", 0) or 0)
+            if g > 0 and li > 0 and g % li == 0:
+                self.lambda_log.append((g, lam))
+            v = self.vm["states"][self.vs_cur]
+            coef = np.ascontiguousarray(v["coef"], np.float64)
+            ene["mcmd_factor"] = L.ogo_mcmd_scale(lam, v["lambda_low"], v["lambda_high"], len(coef) - 1, coef,
+                                                  float(self.vm["temperature"]), self.n, self.work)
+        elif self.mcmd is not None:
             m = self.mcmd
             coef = np.ascontiguousarray(m["coef"], np.float64)
             ene["mcmd_factor"] = L.ogo_mcmd_scale(ene["potential"], m["lambda_low"], m["lambda_high"], len(coef) - 1,

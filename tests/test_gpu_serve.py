@@ -83,3 +83,28 @@ def test_faulted_system_is_isolated():
         c1, v1 = alone.get_state(0)
         c2, v2 = rest.get_state(k)
         assert np.array_equal(c1, c2) and np.array_equal(v1, v2)
+
+
+def test_served_vmcmd_jobs_equal_alone_runs():
+    """V-McMD jobs handed between engines keep their virtual state and generator: the served
+    virtual-state and lambda logs and final states equal the alone runs' bit for bit."""
+    rt = 8.31451 / 4.184 * 1e-3 * 300.0
+    jobs = []
+    for k, (n, steps) in enumerate(((500, 60), (400, 40), (600, 80))):
+        states = [dict(order=0, lambda_low=-1e9, lambda_high=1e9, prob_low=0.0 if v == 0 else 0.5,
+                       prob_high=0.0 if v == 2 else 0.5, coef=[(0.98 + 0.02 * v) / rt], alpha_low=0.0,
+                       alpha_high=0.0) for v in range(3)]
+        vm = {"n_vs": 3, "interval": 3, "temperature": 300.0, "states": states, "init_vs": 2, "seed": 0}
+        p = _params(nsgrid_update_intvl=10, time_step=2.0, thermostat="scaling", temperature=300.0,
+                    random_seed=300 + k, print_intvl_extended_lambda=2)
+        jobs.append(serve.Job(k, systems.water_system(n, seed=80 + k), p, steps, mcmd=vm))
+    res = serve.Server(0, max_jobs=2, window=20, pair_variant=6).run(jobs)
+    assert res["n_jobs"] == 3 and res["relayouts"] >= 3
+    for j in jobs:
+        logs = {}
+        fresh = serve.Job(j.id, j.system, j.params, j.n_steps, mcmd={k: v for k, v in j.mcmd.items()
+                                                                      if k not in ("cur_vs", "mt_state")})
+        _, ene, crd, vel = serve.run_alone(fresh, pair_variant=6, logs=logs)
+        assert np.array_equal(j.crd, crd) and np.array_equal(j.vel, vel), j.id
+        assert j.vs_log == logs["vs"] and j.lambda_log == logs["lambda"], j.id
+        assert len(j.vs_log) == (j.n_steps - 1) // 3 and len({v for _, v in j.vs_log}) > 1  # steps 3, 6 .. < n
