@@ -313,6 +313,22 @@ og_status og_get_vmcmd_state(og_engine *e, int32_t sys, int32_t *cur_vs, uint32_
 og_status og_take_vs_log(og_engine *e, int32_t sys, int64_t max, int64_t *step, int32_t *vs, int64_t *n);
 og_status og_take_lambda_log(og_engine *e, int32_t sys, int64_t max, int64_t *step, double *lambda, int64_t *n);
 
+/* Trajectory frames recorded on the device (DynamicsMode::sub_output, DynamicsMode.cpp:264-300;
+ * --print-interval-coord / --group-o-coord).  Set before og_finalize: every `interval` steps
+ * (0 = none) a frame of the group's atoms (n_group = 0: all atoms, local ids otherwise).  The
+ * frame labelled step k (k > 0, k % interval == 0) holds what the reference writes there: the
+ * coordinates at which step k-1's forces were computed (SubBox::crd_prev) rounded to FP32, as
+ * WriteTrrPresto / WriteTrrGromacs store them, and step k-1's energies.  It is recorded at the
+ * end of step k-1 inside og_step (graph replays included) and moved to the host before the
+ * device ring wraps. */
+og_status og_set_trajectory(og_engine *e, int32_t sys, int32_t interval, const int32_t *group_atoms,
+                            int32_t n_group);
+/* Takes up to `max` of the oldest frames not yet taken: steps[max], crd[max][n_group][3],
+ * energies[max][OG_N_ENERGY] (may be NULL); *n = frames taken (with max = 0: frames waiting).
+ * Frames of a call undone by OG_ERR_SYSTEM_FAULT are dropped with it. */
+og_status og_take_frames(og_engine *e, int32_t sys, int32_t max, int64_t *step, float *crd, double *energies,
+                         int32_t *n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -110,6 +110,8 @@ __global__ void k_slot_refresh(const int *, int, const int *, const double *, co
 __global__ void k_energies(int, const SysDev *, const double *, const double *, double *, double *, int,
                            long long *);
 __global__ void k_trace_advance(long long *, long long *);
+__global__ void k_capture_frames(int, const int *, const int *, const int *, const SysDev *, const long long *,
+                                 const double *, const double *, float *, double *);
 __global__ void k_put_state(int, int, const int *, const SysDev *, const double *, const double *, double *, double *,
                             const int *, double *, const double *, float4 *);
 
@@ -139,7 +141,19 @@ struct HostSystem {
     std::vector<double> tene, tph, iene, iph, cv14, ce14, qd;
     std::vector<VsDev> vstates;   // V-McMD states (one for the one-state mcmd_* form)
     std::vector<uint32_t> mt;     // generator at the system's first step ([OG_MT_WORDS])
+    std::vector<int32_t> tr_group;  // trajectory group (local atom ids), og_set_trajectory
+    int tr_interval = 0;
     int d_free = 0;
+};
+
+// Host side of one system's trajectory frames: frames moved off the device ring, not yet taken.
+// Frame k (1-based) is labelled step k * interval; next_k is the first frame still on the ring.
+struct TrLog {
+    long long next_k = 1;
+    std::vector<long long> step;
+    std::vector<float> crd;    // [frames][group][3]
+    std::vector<double> ene;   // [frames][OG_N_ENERGY]
+    size_t head = 0;           // frames before the head were taken
 };
 
 // Host side of one system's V-McMD logs: entries moved off the device ring and not yet taken.
@@ -280,7 +294,14 @@ struct og_engine {
     int n_vm = 0, vm_log_cap = 0, vm_advance = 0;
     std::vector<int> vm_sys;      // system of each slot
     std::vector<VmLog> vm;        // per slot
-    long long vm_limit = 0;       // host_step up to which no ring overflows before a drain
+    long long log_limit = 0;       // host_step up to which no ring overflows before a drain
+    // trajectory frames: entries (group atom, system, index in group), rings, host side
+    int *d_tr_atom = nullptr, *d_tr_sys = nullptr, *d_tr_idx = nullptr;
+    float *d_frames = nullptr;
+    double *d_frame_ene = nullptr;
+    int n_tr = 0, n_tr_entries = 0;
+    std::vector<int> tr_sys;      // system of each trajectory slot
+    std::vector<TrLog> tr;        // per slot
 };
 
 namespace {
@@ -930,6 +951,13 @@ og_status run_step(og_engine *e, bool ene) {
     k_energies<<<blocks(e->n_sys, 128), 128, 0, st>>>(e->n_sys, e->d_sys, e->d_sys_acc, e->d_mcmd, e->d_energies,
                                                        e->d_trace, e->trace_cap, e->d_trace_count);
     LAUNCH_CHECK();
+    if (e->n_tr_entries) {
+        k_capture_frames<<<blocks(e->n_tr_entries, 256), 256, 0, st>>>(e->n_tr_entries, e->d_tr_atom, e->d_tr_sys,
+                                                                        e->d_tr_idx, e->d_sys, e->d_step,
+                                                                        e->d_crd_prev, e->d_energies, e->d_frames,
+                                                                        e->d_frame_ene);
+        LAUNCH_CHECK();
+    }
     k_trace_advance<<<1, 32, 0, st>>>(e->d_trace_count, e->d_step);
     LAUNCH_CHECK();
     e->host_step++;
@@ -942,7 +970,7 @@ long long vm_entries_end(long long g, int intvl) {  // entries of steps 0..g-1: 
     return g > 0 ? (g - 1) / intvl : 0;
 }
 
-void vm_update_limit(og_engine *e) {
+void logs_update_limit(og_engine *e) {
     long long lim = LLONG_MAX;
     for (int m = 0; m < e->n_vm; m++) {
         const SysDev &D = e->sys[e->vm_sys[m]].dev;
@@ -951,12 +979,48 @@ void vm_update_limit(og_engine *e) {
         if (D.vs_lambda_intvl > 0)
             lim = std::min(lim, (L.lam_next_k + e->vm_log_cap) * D.vs_lambda_intvl - D.first_step);
     }
-    e->vm_limit = lim;
+    // frame k is written at the end of step k * interval - 1
+    for (int m = 0; m < e->n_tr; m++) {
+        const SysDev &D = e->sys[e->tr_sys[m]].dev;
+        lim = std::min(lim, (e->tr[m].next_k + D.tr_frames) * D.tr_interval - 1 - D.first_step);
+    }
+    e->log_limit = lim;
+}
+
+// Moves the trajectory frames of the steps run so far to the host (the stream is synchronised).
+og_status frames_drain(og_engine *e) {
+    for (int m = 0; m < e->n_tr; m++) {
+        const SysDev &D = e->sys[e->tr_sys[m]].dev;
+        TrLog &T = e->tr[m];
+        const long long ke = (D.first_step + e->host_step) / D.tr_interval;  // frames of steps < g
+        const size_t fc = 3 * (size_t)D.tr_n;
+        for (long long k = T.next_k; k <= ke; k++) {
+            const long long slot = (k - 1) % D.tr_frames;
+            const size_t c0 = T.crd.size(), e0 = T.ene.size();
+            T.crd.resize(c0 + fc);
+            T.ene.resize(e0 + OG_N_ENERGY);
+            CK(cudaMemcpyAsync(T.crd.data() + c0, e->d_frames + D.tr_crd_base + slot * fc, sizeof(float) * fc,
+                               cudaMemcpyDeviceToHost, e->stream));
+            CK(cudaMemcpyAsync(T.ene.data() + e0, e->d_frame_ene + D.tr_ene_base + slot * OG_N_ENERGY,
+                               sizeof(double) * OG_N_ENERGY, cudaMemcpyDeviceToHost, e->stream));
+            T.step.push_back(k * D.tr_interval);
+            T.next_k = k + 1;
+        }
+    }
+    CK(cudaStreamSynchronize(e->stream));
+    return OG_OK;
 }
 
 // Synchronises the stream and moves every ring entry of the steps run so far to the host.
-og_status vm_drain(og_engine *e) {
-    if (e->n_vm == 0) return OG_OK;
+og_status logs_drain(og_engine *e) {
+    if (e->n_tr) {
+        og_status s = frames_drain(e);
+        if (s) return s;
+    }
+    if (e->n_vm == 0) {
+        logs_update_limit(e);
+        return OG_OK;
+    }
     const size_t n = (size_t)e->n_vm * e->vm_log_cap;
     std::vector<int32_t> vs(n);
     std::vector<double> lam(n);
@@ -980,14 +1044,14 @@ og_status vm_drain(og_engine *e) {
                 L.lam_next_k = k + 1;
             }
     }
-    vm_update_limit(e);
+    logs_update_limit(e);
     return OG_OK;
 }
 
 // Before steps [host_step, host_step + n): drain first when a ring would wrap during them.
-og_status vm_reserve(og_engine *e, long long n) {
-    if (e->n_vm == 0 || e->host_step + n <= e->vm_limit) return OG_OK;
-    return vm_drain(e);
+og_status logs_reserve(og_engine *e, long long n) {
+    if ((e->n_vm == 0 && e->n_tr == 0) || e->host_step + n <= e->log_limit) return OG_OK;
+    return logs_drain(e);
 }
 
 template <class T>
@@ -997,7 +1061,7 @@ og_status vm_take(og_engine *e, int32_t sys, int64_t max, int64_t *step, T *val,
         return fail(e, OG_ERR_INVALID, "bad system id or output arrays");
     const int m = e->sys[sys].dev.vm_slot;
     if (m < 0) return fail(e, OG_ERR_INVALID, "system %d has no V-McMD transitions", sys);
-    og_status s = vm_drain(e);
+    og_status s = logs_drain(e);
     if (s) return s;
     VmLog &L = e->vm[m];
     std::vector<long long> &st = vs_log ? L.vs_step : L.lam_step;
@@ -1401,6 +1465,8 @@ og_status og_finalize(og_engine *e) {
     std::vector<VsDev> vstates;
     std::vector<int> vs_cur;
     std::vector<uint32_t> mt_all;
+    std::vector<int> tr_atom, tr_sysv, tr_idx;
+    long long tr_crd_total = 0, tr_ene_total = 0;
     {
         size_t n_all = 0, x_all = 0, e_all = 0;
         for (const HostSystem &h : e->sys) {
@@ -1446,6 +1512,26 @@ og_status og_finalize(og_engine *e) {
         vstates.insert(vstates.end(), h.vstates.begin(), h.vstates.end());
         D.mcmd_k = (OG_GAS_CONST / OG_JOULE_CAL) * 1e-3 * d.mcmd_temperature;
         D.first_step = d.first_step;
+        D.tr_slot = -1;
+        D.tr_interval = D.tr_n = D.tr_frames = 0;
+        D.tr_crd_base = D.tr_ene_base = 0;
+        if (h.tr_interval > 0) {
+            // a ring of frames long enough for the frames of one list interval
+            D.tr_slot = (int)e->tr_sys.size();
+            D.tr_interval = h.tr_interval;
+            D.tr_n = (int)h.tr_group.size();
+            D.tr_frames = e->intvl / h.tr_interval + 2;
+            D.tr_crd_base = tr_crd_total;
+            D.tr_ene_base = tr_ene_total;
+            tr_crd_total += (long long)D.tr_frames * D.tr_n * 3;
+            tr_ene_total += (long long)D.tr_frames * OG_N_ENERGY;
+            for (int j = 0; j < D.tr_n; j++) {
+                tr_atom.push_back(atom_base + h.tr_group[j]);
+                tr_sysv.push_back(k);
+                tr_idx.push_back(j);
+            }
+            e->tr_sys.push_back(k);
+        }
         D.vm_slot = -1;
         D.vs_trans_intvl = D.vs_lambda_intvl = 0;
         vs_cur.push_back(d.n_vstates > 0 ? d.vmcmd_init_vs : 0);
@@ -1667,12 +1753,24 @@ og_status og_finalize(og_engine *e) {
         if (D.vs_lambda_intvl > 0)
             e->vm[m].lam_next_k = std::max(1LL, (D.first_step + D.vs_lambda_intvl - 1) / D.vs_lambda_intvl);
     }
-    vm_update_limit(e);
+    // trajectory frames: the first frame this engine writes is labelled k * interval with
+    // k * interval - 1 >= first_step
+    e->n_tr = (int)e->tr_sys.size();
+    e->n_tr_entries = (int)tr_atom.size();
+    e->tr.assign(e->n_tr, TrLog{});
+    for (int m = 0; m < e->n_tr; m++) {
+        const SysDev &D = sd[e->tr_sys[m]];
+        e->tr[m].next_k = (D.first_step + D.tr_interval) / D.tr_interval;
+    }
+    logs_update_limit(e);
     if ((s = upload(e, &e->d_vstates, vstates)) || (s = upload(e, &e->d_vs_cur, vs_cur)) ||
         (s = dalloc(e, &e->d_vm_snap_cur, S)) || (s = upload(e, &e->d_mt, mt_all)) ||
         (s = dalloc(e, &e->d_vm_snap_mt, mt_all.size())) ||
         (s = dalloc(e, &e->d_vs_log, (size_t)e->n_vm * e->vm_log_cap)) ||
-        (s = dalloc(e, &e->d_lambda_log, (size_t)e->n_vm * e->vm_log_cap)))
+        (s = dalloc(e, &e->d_lambda_log, (size_t)e->n_vm * e->vm_log_cap)) ||
+        (s = upload(e, &e->d_tr_atom, tr_atom)) || (s = upload(e, &e->d_tr_sys, tr_sysv)) ||
+        (s = upload(e, &e->d_tr_idx, tr_idx)) || (s = dalloc(e, &e->d_frames, (size_t)tr_crd_total)) ||
+        (s = dalloc(e, &e->d_frame_ene, (size_t)tr_ene_total)))
         return s;
     {
         std::vector<int> sa(S + 1), se(S + 1), sb(S + 1), sg(S + 1), st(S + 1), si(S + 1), s14(S + 1);
@@ -1776,6 +1874,8 @@ og_status og_step(og_engine *e, int32_t n_steps) {
     std::vector<VmMark> vm0(e->n_vm);
     for (int m = 0; m < e->n_vm; m++)
         vm0[m] = {e->vm[m].vs_next_k, e->vm[m].lam_next_k, e->vm[m].vs.size(), e->vm[m].lam.size()};
+    std::vector<VmMark> tr0(e->n_tr);  // trajectory: next frame and frames held
+    for (int m = 0; m < e->n_tr; m++) tr0[m] = {e->tr[m].next_k, 0, e->tr[m].step.size(), 0};
     for (int attempt = 0; attempt < 3; attempt++) {
         if (e->n_vm) {
             CK(cudaMemcpyAsync(e->d_vm_snap_cur, e->d_vs_cur, sizeof(int) * e->n_sys, cudaMemcpyDeviceToDevice,
@@ -1795,7 +1895,7 @@ og_status og_step(og_engine *e, int32_t n_steps) {
         for (int i = 0; i < n_steps;) {
             // whole list intervals replay the captured graph (not while per-kernel timing is on)
             if (e->use_graphs && e->timing != 1 && e->host_step % e->intvl == 0 && n_steps - i >= e->intvl) {
-                if ((s = vm_reserve(e, e->intvl))) return s;
+                if ((s = logs_reserve(e, e->intvl))) return s;
                 if (!e->graph_exec && (s = capture_interval(e))) return s;
                 if (e->graph_exec) {
                     CK(cudaGraphLaunch(e->graph_exec, e->stream));
@@ -1806,7 +1906,7 @@ og_status og_step(og_engine *e, int32_t n_steps) {
                     continue;
                 }
             }
-            if ((s = vm_reserve(e, 1))) return s;
+            if ((s = logs_reserve(e, 1))) return s;
             if ((s = run_step(e, i == n_steps - 1))) return s;
             i++;
         }
@@ -1858,9 +1958,17 @@ og_status og_step(og_engine *e, int32_t n_steps) {
                 L.lam_step.resize(vm0[m].lam_n);
             }
         }
+        for (int m = 0; m < e->n_tr; m++) {
+            TrLog &T = e->tr[m];
+            const size_t fc = 3 * (size_t)e->sys[e->tr_sys[m]].dev.tr_n;
+            T.next_k = tr0[m].vs_k;
+            T.step.resize(tr0[m].vs_n);
+            T.crd.resize(tr0[m].vs_n * fc);
+            T.ene.resize(tr0[m].vs_n * OG_N_ENERGY);
+        }
         CK(cudaStreamSynchronize(e->stream));
         e->host_step = step0;
-        vm_update_limit(e);
+        logs_update_limit(e);
         // the list must be rebuilt from the restored coordinates before the first step
         if (step0 % e->intvl != 0) {
             if ((s = build_list_checked(e))) return s;
@@ -2112,6 +2220,64 @@ og_status og_take_lambda_log(og_engine *e, int32_t sys, int64_t max, int64_t *st
     return vm_take<double>(e, sys, max, step, lambda, n, false);
 }
 
+og_status og_set_trajectory(og_engine *e, int32_t sys, int32_t interval, const int32_t *group_atoms,
+                            int32_t n_group) {
+    if (!e) return OG_ERR_INVALID;
+    if (e->finalized) return fail(e, OG_ERR_STATE, "og_set_trajectory after og_finalize");
+    if (sys < 0 || sys >= (int)e->sys.size()) return fail(e, OG_ERR_INVALID, "bad system id");
+    HostSystem &h = e->sys[sys];
+    const int n = h.d.n_atoms;
+    if (interval < 0 || n_group < 0 || (n_group > 0 && !group_atoms))
+        return fail(e, OG_ERR_INVALID, "negative interval or group size, or no group array");
+    h.tr_interval = interval;
+    h.tr_group.clear();
+    if (interval == 0) return OG_OK;
+    if (n_group == 0) {
+        for (int a = 0; a < n; a++) h.tr_group.push_back(a);
+    } else {
+        for (int j = 0; j < n_group; j++) {
+            if (group_atoms[j] < 0 || group_atoms[j] >= n) {
+                h.tr_interval = 0;
+                h.tr_group.clear();
+                return fail(e, OG_ERR_INVALID, "trajectory group atom %d out of range", group_atoms[j]);
+            }
+            h.tr_group.push_back(group_atoms[j]);
+        }
+    }
+    return OG_OK;
+}
+
+og_status og_take_frames(og_engine *e, int32_t sys, int32_t max, int64_t *step, float *crd, double *energies,
+                         int32_t *n) {
+    if (!e || !e->finalized) return fail(e, OG_ERR_STATE, "og_take_frames before og_finalize");
+    if (sys < 0 || sys >= e->n_sys || max < 0 || !n || (max > 0 && (!step || !crd)))
+        return fail(e, OG_ERR_INVALID, "bad system id or output arrays");
+    const int m = e->sys[sys].dev.tr_slot;
+    if (m < 0) return fail(e, OG_ERR_INVALID, "system %d has no trajectory output", sys);
+    og_status s = logs_drain(e);
+    if (s) return s;
+    TrLog &T = e->tr[m];
+    const size_t fc = 3 * (size_t)e->sys[sys].dev.tr_n;
+    const int32_t avail = (int32_t)(T.step.size() - T.head);
+    if (max == 0) {
+        *n = avail;
+        return OG_OK;
+    }
+    const int32_t k = std::min(max, avail);
+    for (int32_t i = 0; i < k; i++) step[i] = T.step[T.head + i];
+    memcpy(crd, T.crd.data() + T.head * fc, sizeof(float) * fc * k);
+    if (energies) memcpy(energies, T.ene.data() + T.head * OG_N_ENERGY, sizeof(double) * OG_N_ENERGY * k);
+    T.head += (size_t)k;
+    if (T.head == T.step.size()) {
+        T.step.clear();
+        T.crd.clear();
+        T.ene.clear();
+        T.head = 0;
+    }
+    *n = k;
+    return OG_OK;
+}
+
 // Per-step timing of the pair kernel (CUDA events on the engine's stream).  Not in the public
 // header's main list: enabled by the benchmark.
 og_status og_set_timing(og_engine *e, int32_t on) {
@@ -2177,7 +2343,7 @@ extern "C" og_status og_step_async(og_engine *e, int32_t n_steps) {
     // checks og_get_flags at its own sync points
     if (!e || !e->finalized) return fail(e, OG_ERR_STATE, "og_step_async before og_finalize");
     for (int i = 0; i < n_steps; i++) {
-        og_status s = vm_reserve(e, 1);  // synchronises only when a V-McMD log ring is full
+        og_status s = logs_reserve(e, 1);  // synchronises only when a V-McMD log ring is full
         if (s) return s;
         s = run_step(e, i == n_steps - 1);
         if (s) return s;

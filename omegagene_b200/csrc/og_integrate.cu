@@ -996,4 +996,34 @@ __global__ void k_trace_advance(long long *trace_count, long long *step) {
     }
 }
 
+
+// Trajectory frames (DynamicsMode::sub_output, DynamicsMode.cpp:264-300), captured at the end
+// of step g for the frame labelled k = g + 1 when k is a multiple of the system's interval: the
+// coordinates at which step g's forces were computed (SubBox::crd_prev, which is what the
+// reference writes), rounded to FP32 as WriteTrrPresto / WriteTrrGromacs store them, and step
+// g's energies.  One thread per (group atom, system entry); frame k sits in ring slot
+// (k / interval - 1) mod frames.  Launched before the step counter advances.
+__global__ void k_capture_frames(int n_entries, const int *__restrict__ tr_atom, const int *__restrict__ tr_sys,
+                                 const int *__restrict__ tr_idx, const SysDev *__restrict__ sys,
+                                 const long long *__restrict__ step, const double *__restrict__ crd_prev,
+                                 const double *__restrict__ energies, float *__restrict__ frames,
+                                 double *__restrict__ frame_ene) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_entries) return;
+    const int s = tr_sys[i];
+    const SysDev &S = sys[s];
+    const long long k = *step + S.first_step + 1;
+    if (k % S.tr_interval != 0) return;
+    const long long slot = (k / S.tr_interval - 1) % S.tr_frames;
+    const int a = tr_atom[i], j = tr_idx[i];
+    float *f = frames + S.tr_crd_base + (slot * S.tr_n + j) * 3;
+    f[0] = (float)crd_prev[3 * a];
+    f[1] = (float)crd_prev[3 * a + 1];
+    f[2] = (float)crd_prev[3 * a + 2];
+    if (j == 0) {
+        double *e = frame_ene + S.tr_ene_base + slot * OG_N_ENERGY;
+        for (int q = 0; q < OG_N_ENERGY; q++) e[q] = energies[OG_N_ENERGY * s + q];
+    }
+}
+
 }  // namespace og

@@ -74,6 +74,10 @@ struct SysDev {
     // table, n_vs = 0 when off.  vm_slot indexes the generator and log rings (-1: no transitions).
     int n_vs, vs_base, vm_slot, vs_trans_intvl, vs_lambda_intvl;
     long long first_step;             // step number of the engine's first step for this system
+    // trajectory frames (DynamicsMode::sub_output): ring slot (-1: none), interval, group size,
+    // and the offsets of the system's frame ring in the frame buffers
+    int tr_slot, tr_interval, tr_n, tr_frames;
+    long long tr_crd_base, tr_ene_base;
     double mcmd_k;                    // const_k = (GAS_CONST/JOULE_CAL) 1e-3 T
     // constraint / term ranges (global index spaces of their own arrays)
     int trio_base, n_trio, pair_base, n_pair;

@@ -107,6 +107,8 @@ def load_library():
         "og_get_vmcmd_state": [E, C.c_int32, _p(C.c_int32), C.c_void_p],
         "og_take_vs_log": [E, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, _p(C.c_int64)],
         "og_take_lambda_log": [E, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, _p(C.c_int64)],
+        "og_set_trajectory": [E, C.c_int32, C.c_int32, C.c_void_p, C.c_int32],
+        "og_take_frames": [E, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, _p(C.c_int32)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -129,6 +131,8 @@ DEFAULT_PARAMS = {
     "thermo_const_tolerance": 1e-5, "com_motion": "cancel", "com_cancel_groups": None, "constraint": "shake",
     "extended_ensemble": "none", "random_seed": -1, "print_intvl_extended_lambda": 0,
     "fn_o_vmcmd_log": None, "fn_o_extended_lambda": None, "format_o_extended_lambda": "binary",
+    "n_steps": 0, "print_intvl_log": 0, "print_intvl_crd": [], "fn_o_crd": [], "format_o_crd": "presto",
+    "group_o_crd": [], "fn_o_restart": "md_o.restart", "print_intvl_restart": 0,
 }
 
 
@@ -143,10 +147,9 @@ def parse_run_config(text):
         toks += line.split()
     p = dict(DEFAULT_PARAMS)
     groups = []
-    accepted_ignored = {"--processor", "--gpu-device-id", "--mode", "--n-steps", "--print-interval-log",
-                        "--print-interval-coord", "--fn-o-coord", "--format-o-coord", "--group-o-coord",
-                        "--fn-o-log", "--fn-o-energy", "--fn-o-restart", "--integrator", "--electrostatic",
-                        "--ele-alpha", "--expected-num-density"}
+    accepted_ignored = {"--processor", "--gpu-device-id", "--mode", "--fn-o-log", "--fn-o-energy", "--integrator",
+                        "--electrostatic", "--ele-alpha", "--expected-num-density"}
+    lists = {"print_intvl_crd": [], "fn_o_crd": [], "group_o_crd": []}
     i = 0
     while i < len(toks):
         k = toks[i]
@@ -191,6 +194,24 @@ def parse_run_config(text):
             p["extended_ensemble"] = v
         elif k == "--random-seed":
             p["random_seed"] = int(v)
+        elif k == "--n-steps":
+            p["n_steps"] = int(v)
+        elif k == "--print-interval-log":
+            p["print_intvl_log"] = int(v)
+        elif k == "--print-interval-coord":   # Config.cpp:204-205, one entry per output
+            lists["print_intvl_crd"].append(int(v))
+        elif k == "--fn-o-coord":
+            lists["fn_o_crd"].append(v)
+        elif k == "--group-o-coord":
+            lists["group_o_crd"].append(v)
+        elif k == "--format-o-coord":
+            if v not in ("presto", "gromacs"):
+                raise ValueError("--format-o-coord %s (presto, gromacs)" % v)
+            p["format_o_crd"] = v
+        elif k == "--fn-o-restart":
+            p["fn_o_restart"] = v
+        elif k == "--print-interval-restart":
+            p["print_intvl_restart"] = int(v)
         elif k == "--print-interval-extended-lambda":
             p["print_intvl_extended_lambda"] = int(v)
         elif k == "--fn-o-vmcmd-log":
@@ -210,6 +231,9 @@ def parse_run_config(text):
             raise ValueError("unsupported config key %s" % k)
     if groups:
         p["com_cancel_groups"] = groups
+    for key, val in lists.items():
+        if val:
+            p[key] = val
     return p
 
 
@@ -536,6 +560,28 @@ class Engine:
     def take_lambda_log(self, sys):
         """(steps, lambda) logged since the last take (ExtendedVMcMD::write_lambda rows)."""
         return self._take(self.L.og_take_lambda_log, sys, np.float64)
+
+    def set_trajectory(self, sys, interval, group=None):
+        """Frames every `interval` steps of the group's atoms (None: all), recorded on the device;
+        call before finalize."""
+        g = None if group is None else np.ascontiguousarray(group, np.int32)
+        self._check(self.L.og_set_trajectory(self.h, sys, int(interval), None if g is None else g.ctypes.data,
+                                             0 if g is None else len(g)), "og_set_trajectory")
+        self._tr_n = getattr(self, "_tr_n", {})
+        self._tr_n[sys] = len(g) if g is not None else None
+
+    def take_frames(self, sys):
+        """(steps, crd [frames][group][3] float32, energies [frames][N_ENERGY]) not yet taken."""
+        n = C.c_int32()
+        self._check(self.L.og_take_frames(self.h, sys, 0, None, None, None, C.byref(n)), "og_take_frames")
+        g = self._tr_n.get(sys) or self.n_atoms[sys]
+        steps = np.zeros(n.value, np.int64)
+        crd = np.zeros((n.value, g, 3), np.float32)
+        ene = np.zeros((n.value, N_ENERGY), np.float64)
+        if n.value:
+            self._check(self.L.og_take_frames(self.h, sys, n.value, steps.ctypes.data, crd.ctypes.data,
+                                              ene.ctypes.data, C.byref(n)), "og_take_frames")
+        return steps[:n.value], crd[:n.value], ene[:n.value]
 
     def system_faults(self):
         """Per-system fault bits of the last og_step that returned OG_ERR_SYSTEM_FAULT
