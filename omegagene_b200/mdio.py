@@ -61,6 +61,14 @@ def read_restart(path):
             "e_total": e_total, "e_kinetic": e_kin, "e_potential": e_pot, "crd": crd, "vel": vel}
 
 
+def apply_restart(system, restart):
+    """The system with a restart's coordinates and velocities, as the reference's toolkit puts a
+    restart into the next run's .cls (kkmmsystem.set_crd_vel_from_restart)."""
+    if restart["n_atoms"] != int(system["n_atoms"]):
+        raise ValueError("restart holds %d atoms, the system %d" % (restart["n_atoms"], system["n_atoms"]))
+    return dict(system, crd=restart["crd"].copy(), vel=restart["vel"].copy())
+
+
 def presto_frame(step, time, energies, crd, cpu_time=0.0):
     """One WriteTrrPresto frame: energies is the engine's energy dict of the step the frame's
     coordinates belong to.  The header record's leading marker is 44 and its trailing one 0, as

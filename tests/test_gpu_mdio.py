@@ -67,3 +67,19 @@ def test_ala3_run_outputs_match_reference_files(tmp_path):
     for r, g in zip(rows, gold["steps"]):
         for key in ("potential", "kinetic", "total", "vdw", "ele", "bond", "torsion"):
             assert abs(r[key] - g[key]) <= 1e-5 * abs(g[key]) + 1e-4, (r["step"], key, r[key], g[key])
+
+
+def test_ala3_vmcmd_run_writes_reference_logs(tmp_path):
+    """mdio.run with the reference's V-McMD settings writes the virtual-state log line for line
+    as the reference did (ala3_vmcmd.json) and its ascii lambda log within 1e-4 relative."""
+    g = json.load(open(os.path.join(GOLD, "ala3_vmcmd.json")))
+    _, s, _ = _golden()
+    p = dict(g["params"], print_intvl_crd=[], fn_o_crd=[], fn_o_restart=str(tmp_path / "o.restart"),
+             fn_o_vmcmd_log=str(tmp_path / "vs.log"), fn_o_extended_lambda=str(tmp_path / "lambda.out"),
+             format_o_extended_lambda="ascii")
+    mdio.run(s, p, mcmd=g["vmcmd"])
+    assert open(tmp_path / "vs.log").read() == "".join("%d\t%d\n" % (a, b) for a, b in g["vs"])
+    lam = np.loadtxt(tmp_path / "lambda.out")
+    ref = np.array(g["lambda"])
+    assert lam.shape == ref.shape and np.max(np.abs(lam - ref) / np.abs(ref)) <= 1e-4
+    assert mdio.read_restart(tmp_path / "o.restart")["n_steps"] == g["n_steps"]

@@ -81,3 +81,10 @@ def test_run_config_output_keys():
 
 def test_lambda_log_header():
     assert mdio.lambda_log_header() == struct.pack("<iii", 66261, 8, 1)
+
+
+def test_apply_restart():
+    r = mdio.read_restart(os.path.join(GOLD, "ala3_run_o.restart"))
+    s = {"n_atoms": 6207, "crd": np.zeros((6207, 3)), "vel": np.zeros((6207, 3))}
+    t = mdio.apply_restart(s, r)
+    assert np.array_equal(t["crd"], r["crd"]) and np.array_equal(t["vel"], r["vel"]) and not s["crd"].any()
