@@ -33,8 +33,10 @@ __global__ void k_count_pairs(const int *, int, int, const int *, const int *, c
                               const unsigned char *, int *);
 __global__ void k_fill_pairs(int *, int, int, long long, const int *, const int *, const SysDev *, const int *,
                              const int *, const int *, const float2 *, const int2 *, const int *, const int *,
-                             const unsigned char *, const int *, const int *, const int *, const int *, const int *,
-                             const int *, int2 *, unsigned long long *, const double *, float4 *);
+                             const int *, int2 *);
+__global__ void k_pair_records(const int *, long long, const int *, const SysDev *, const int *, const int2 *,
+                               const unsigned char *, const int *, const int *, const int *, const int *, const int *,
+                               const double *, unsigned long long *, float4 *);
 __global__ void k_cell_excl(const int *, int, const int *, const int *, const int *, const int *, int *);
 __global__ void k_pair_heads(int *, int, int, const int *, int *);
 __global__ void k_scan_block(const int *, int *, long long, int *);
@@ -593,9 +595,13 @@ og_status build_list(og_engine *e) {
     LAUNCH_CHECK();
     k_fill_pairs<<<blocks(n_items, 256), 256, 0, st>>>(
         e->d_counters, e->cells_cap, e->nnc, e->pair_cap, e->d_cell_sys, e->d_sys_cell_base, e->d_sys, e->d_cell_col,
-        e->d_col_cell_start, e->d_col_head_cell, e->d_cell_zr, e->d_cell_uni, e->d_uni_lo, e->d_uni_hi,
-        e->d_cell_valid, e->d_slot_atom, e->d_atom_slot, e->d_excl_start, e->d_excl_list, e->d_cell_excl, e->d_offset,
-        e->d_cp_c2img, e->d_cp_mask, e->d_cell_origin, e->d_cp_shift);
+        e->d_col_cell_start, e->d_col_head_cell, e->d_cell_zr, e->d_cell_uni, e->d_uni_lo, e->d_uni_hi, e->d_offset,
+        e->d_cp_c2img);
+    LAUNCH_CHECK();
+    k_pair_records<<<blocks((long long)e->cells_cap * 32, 256), 256, 0, st>>>(
+        e->d_counters, e->pair_cap, e->d_cell_sys, e->d_sys, e->d_cp_head, e->d_cp_c2img, e->d_cell_valid,
+        e->d_slot_atom, e->d_atom_slot, e->d_excl_start, e->d_excl_list, e->d_cell_excl, e->d_cell_origin,
+        e->d_cp_mask, e->d_cp_shift);
     LAUNCH_CHECK();
     return OG_OK;
 }

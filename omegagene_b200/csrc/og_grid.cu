@@ -273,17 +273,13 @@ __device__ __forceinline__ unsigned long long pair_mask(int c1, int c2, unsigned
 }
 
 // Enumerates the cell pairs of one (cell1, neighbour column) exactly like the reference's
-// loop body (MiniCell.cpp:968-1140).  With out == nullptr it only counts.
+// loop body (MiniCell.cpp:968-1140).  With out_c2img == nullptr it only counts; otherwise it
+// writes (cell2, image bits) of each pair, and k_pair_records forms the rest of the record.
 __device__ int enumerate_column(int c1, int nb, const SysDev &S, int cell_base,
                                 const int *__restrict__ cell_col, const int *__restrict__ col_cell_start,
                                 const int *__restrict__ col_head_cell, const float2 *__restrict__ cell_zr,
                                 const int2 *__restrict__ cell_uni, const int *__restrict__ uni_lo,
-                                const int *__restrict__ uni_hi, const unsigned char *__restrict__ cell_valid,
-                                const int *__restrict__ slot_atom, const int *__restrict__ atom_slot,
-                                const int *__restrict__ excl_start, const int *__restrict__ excl_list,
-                                const int *__restrict__ cell_excl, int2 *out_c2img, unsigned long long *out_mask,
-                                int out_cap, const double *__restrict__ cell_origin = nullptr,
-                                float4 *out_shift = nullptr) {
+                                const int *__restrict__ uni_hi, int2 *out_c2img, int out_cap) {
     const int nx = S.nx, ny = S.ny, nuz = S.n_uni_z;
     const int wy = 2 * S.n_nb[1] + 1;
     const int dcx = nb / wy - S.n_nb[0];
@@ -318,13 +314,6 @@ __device__ int enumerate_column(int c1, int nb, const SysDev &S, int cell_base,
     const float2 z1 = cell_zr[c1];
     const int lc1 = c1 - cell_base;
     const int n_uni = S.n_columns * nuz;
-    const unsigned v1 = cell_valid[c1];
-    double o1x = 0.0, o1y = 0.0, o1z = 0.0;
-    if (out_shift) {
-        o1x = cell_origin[3 * c1];
-        o1y = cell_origin[3 * c1 + 1];
-        o1z = cell_origin[3 * c1 + 2];
-    }
     int n = 0;
     for (int ii = 0; ii < 3; ii++) {
         const int iz = ii - 1;
@@ -355,23 +344,12 @@ __device__ int enumerate_column(int c1, int nb, const SysDev &S, int cell_base,
             else dz = 0.0f;
             if (__fadd_rn(dxy, dz) > S.cutoff_pair2) continue;
             if (!valid_pair(lc1, c2 - cell_base)) continue;
-            if (out_c2img) {
-                if (n < out_cap) {
-                    int img = 0;
-                    if (ix == -1) img |= 1; else if (ix == 1) img |= 2;
-                    if (iy == -1) img |= 4; else if (iy == 1) img |= 8;
-                    if (iz == -1) img |= 16; else if (iz == 1) img |= 32;
-                    out_c2img[n] = make_int2(c2, img);
-                    out_mask[n] = pair_mask(c1, c2, v1, cell_valid[c2], slot_atom, atom_slot, excl_start, excl_list,
-                                            cell_excl);
-                    // pair-kernel record: shift from cell1's origin to cell2's image origin, in FP64
-                    const double shx = ix == -1 ? -S.L[0] : (ix == 1 ? S.L[0] : 0.0);
-                    const double shy = iy == -1 ? -S.L[1] : (iy == 1 ? S.L[1] : 0.0);
-                    const double shz2 = iz == -1 ? -S.L[2] : (iz == 1 ? S.L[2] : 0.0);
-                    out_shift[n] = make_float4((float)(cell_origin[3 * c2] + shx - o1x),
-                                               (float)(cell_origin[3 * c2 + 1] + shy - o1y),
-                                               (float)(cell_origin[3 * c2 + 2] + shz2 - o1z), __int_as_float(c2));
-                }
+            if (out_c2img && n < out_cap) {
+                int img = 0;
+                if (ix == -1) img |= 1; else if (ix == 1) img |= 2;
+                if (iy == -1) img |= 4; else if (iy == 1) img |= 8;
+                if (iz == -1) img |= 16; else if (iz == 1) img |= 32;
+                out_c2img[n] = make_int2(c2, img);
             }
             n++;
         }
@@ -397,8 +375,7 @@ __global__ void k_count_pairs(const int *__restrict__ counters, int cells_cap, i
         const SysDev &S = sys[s];
         if (nb < S.n_nb_cols)
             n = enumerate_column(c1, nb, S, sys_cell_base[s], cell_col, col_cell_start, col_head_cell, cell_zr,
-                                 cell_uni, uni_lo, uni_hi, cell_valid, nullptr, nullptr, nullptr, nullptr, nullptr,
-                                 nullptr, nullptr, 0);
+                                 cell_uni, uni_lo, uni_hi, nullptr, 0);
     }
     count[idx] = n;
 }
@@ -409,12 +386,7 @@ __global__ void k_fill_pairs(int *__restrict__ counters, int cells_cap, int nnc,
                              const int *__restrict__ col_cell_start, const int *__restrict__ col_head_cell,
                              const float2 *__restrict__ cell_zr, const int2 *__restrict__ cell_uni,
                              const int *__restrict__ uni_lo, const int *__restrict__ uni_hi,
-                             const unsigned char *__restrict__ cell_valid, const int *__restrict__ slot_atom,
-                             const int *__restrict__ atom_slot, const int *__restrict__ excl_start,
-                             const int *__restrict__ excl_list, const int *__restrict__ cell_excl,
-                             const int *__restrict__ offset, int2 *__restrict__ cp_c2img,
-                             unsigned long long *__restrict__ cp_mask, const double *__restrict__ cell_origin,
-                             float4 *__restrict__ cp_shift) {
+                             const int *__restrict__ offset, int2 *__restrict__ cp_c2img) {
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int n_cells = counters[OG_CNT_N_CELLS];
     if (idx >= (long long)n_cells * nnc) return;
@@ -425,9 +397,39 @@ __global__ void k_fill_pairs(int *__restrict__ counters, int cells_cap, int nnc,
     const long long off = offset[idx];
     const int cap = (int)max(0ll, min(pair_cap - off, (long long)1 << 30));
     int n = enumerate_column(c1, nb, S, sys_cell_base[s], cell_col, col_cell_start, col_head_cell, cell_zr, cell_uni,
-                             uni_lo, uni_hi, cell_valid, slot_atom, atom_slot, excl_start, excl_list, cell_excl,
-                             cp_c2img + off, cp_mask + off, cap, cell_origin, cp_shift + off);
+                             uni_lo, uni_hi, cp_c2img + off, cap);
     if (off + n > pair_cap) og_set_flag(counters, OG_FLAG_PAIR_CAPACITY);
+}
+
+// The rest of every record once the enumeration has written (cell2, image): the 64-bit
+// exclusion mask (the reference's CellPair::pair_mask) and the pair kernel's record (the shift
+// from cell1's origin to cell2's image origin, formed in FP64, and cell2).  One warp per
+// cell1, lanes over its records: cell1's exclusion row is read once per warp and the writes
+// are coalesced.
+__global__ void k_pair_records(const int *__restrict__ counters, long long pair_cap, const int *__restrict__ cell_sys,
+                               const SysDev *__restrict__ sys, const int *__restrict__ cp_head,
+                               const int2 *__restrict__ cp_c2img, const unsigned char *__restrict__ cell_valid,
+                               const int *__restrict__ slot_atom, const int *__restrict__ atom_slot,
+                               const int *__restrict__ excl_start, const int *__restrict__ excl_list,
+                               const int *__restrict__ cell_excl, const double *__restrict__ cell_origin,
+                               unsigned long long *__restrict__ cp_mask, float4 *__restrict__ cp_shift) {
+    const int c1 = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (c1 >= counters[OG_CNT_N_CELLS]) return;
+    const SysDev &S = sys[cell_sys[c1]];
+    const long long k1 = min((long long)cp_head[c1 + 1], pair_cap);
+    const unsigned v1 = cell_valid[c1];
+    const double o1x = cell_origin[3 * c1], o1y = cell_origin[3 * c1 + 1], o1z = cell_origin[3 * c1 + 2];
+    for (long long k = (long long)cp_head[c1] + lane; k < k1; k += 32) {
+        const int2 ci = cp_c2img[k];
+        const int c2 = ci.x, img = ci.y;
+        cp_mask[k] = pair_mask(c1, c2, v1, cell_valid[c2], slot_atom, atom_slot, excl_start, excl_list, cell_excl);
+        const double shx = (img & 1) ? -S.L[0] : ((img & 2) ? S.L[0] : 0.0);
+        const double shy = (img & 4) ? -S.L[1] : ((img & 8) ? S.L[1] : 0.0);
+        const double shz = (img & 16) ? -S.L[2] : ((img & 32) ? S.L[2] : 0.0);
+        cp_shift[k] = make_float4((float)(cell_origin[3 * c2] + shx - o1x), (float)(cell_origin[3 * c2 + 1] + shy - o1y),
+                                  (float)(cell_origin[3 * c2 + 2] + shz - o1z), __int_as_float(c2));
+    }
 }
 
 // CSR heads from the scanned counts; also publishes the total.

@@ -74,7 +74,7 @@ def test_ala3_vmcmd_run_writes_reference_logs(tmp_path):
     as the reference did (ala3_vmcmd.json) and its ascii lambda log within 1e-4 relative."""
     g = json.load(open(os.path.join(GOLD, "ala3_vmcmd.json")))
     _, s, _ = _golden()
-    p = dict(g["params"], print_intvl_crd=[], fn_o_crd=[], fn_o_restart=str(tmp_path / "o.restart"),
+    p = dict(g["params"], n_steps=g["n_steps"], print_intvl_crd=[], fn_o_crd=[], fn_o_restart=str(tmp_path / "o.restart"),
              fn_o_vmcmd_log=str(tmp_path / "vs.log"), fn_o_extended_lambda=str(tmp_path / "lambda.out"),
              format_o_extended_lambda="ascii")
     mdio.run(s, p, mcmd=g["vmcmd"])
