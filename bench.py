@@ -294,6 +294,8 @@ def run_ours(args, world, rank, local, pg):
                      "frac": achieved / fp32_peak, "traffic": traffic,
                      "kernel": "k_pair_ljzd", "pair_kernel_ms": pair_ms, "interacting_pairs": n_int,
                      "flop_per_pair": FLOP_PER_PAIR, "autotune": tuning,
+                     "cell_pairs": n_cell_pairs,
+                     "cluster_efficiency": n_int / (64.0 * n_cell_pairs) if n_cell_pairs else None,
                      "peak_note": "FP32 CUDA-core peak = 148 SMs x 128 lanes x 2 x %.0f MHz (nominal at the "
                                   "measured max SM clock; MEASURED_PEAKS.json has no FP32 figure)" % sm_max},
         "e2e": e2e, "gpu_launches": launches, "clocks": clk, "device_flags": flags,
