@@ -301,6 +301,32 @@ def write_cls(path, s):
             f.write(raw.get(k, b""))
 
 
+HPS = np.dtype([("t1", "<i4"), ("t2", "<i4"), ("cut", "<f8"), ("lam", "<f8")])
+
+
+def hps_tables(topol):
+    """Dense n_types x n_types HPS cutoff and lambda tables from the topology's HPS records
+    (Read.cpp:322-334 reads one record per LJ type pair; MmSystem::set_lj_pair_hps_param,
+    MmSystem.cpp:320-325, sets both orders, so a later record of a pair wins)."""
+    nt = int(topol["n_lj_types"])
+    cut = np.zeros((nt, nt), np.float64)
+    lam = np.zeros((nt, nt), np.float64)
+    raw = topol.get("lj_hps_raw", b"")
+    n = min(len(raw) // HPS.itemsize, len(topol["lj_pairs"]))
+    for rec in np.frombuffer(raw[:n * HPS.itemsize], HPS):
+        i, j = int(rec["t1"]) - 1, int(rec["t2"]) - 1
+        cut[i, j] = cut[j, i] = rec["cut"]
+        lam[i, j] = lam[j, i] = rec["lam"]
+    return cut, lam
+
+
+def pack_hps(t1, t2, cut, lam):
+    """HPS records (1-based types) as the topology section holds them."""
+    rec = np.zeros(len(t1), HPS)
+    rec["t1"], rec["t2"], rec["cut"], rec["lam"] = t1, t2, cut, lam
+    return rec.tobytes()
+
+
 def lj_tables(topol):
     """Dense n_types x n_types C6/C12 tables from the LJ type-pair records
     (MmSystem::set_lj_pair_param, MmSystem.cpp:313-319)."""

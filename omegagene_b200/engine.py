@@ -133,7 +133,12 @@ DEFAULT_PARAMS = {
     "fn_o_vmcmd_log": None, "fn_o_extended_lambda": None, "format_o_extended_lambda": "binary",
     "n_steps": 0, "print_intvl_log": 0, "print_intvl_crd": [], "fn_o_crd": [], "format_o_crd": "presto",
     "group_o_crd": [], "fn_o_restart": "md_o.restart", "print_intvl_restart": 0,
+    "electrostatic": "zero-dipole", "ele_alpha": 0.0, "dh_dielectric": 0.0, "dh_ionic_strength": 0.0,
+    "dh_temperature": 0.0, "nonbond": "lennard-jones", "hps_epsilon": 0.0,
 }
+
+# --electrostatic values (Config.cpp:114-128) and their engine codes
+ELECTROSTATIC = {"zero-dipole": 0, "zero-quadrupole": 1, "zero-octupole": 2, "zero-hexadecapole": 3, "debye-huckel": 4}
 
 
 def parse_run_config(text):
@@ -148,7 +153,7 @@ def parse_run_config(text):
     p = dict(DEFAULT_PARAMS)
     groups = []
     accepted_ignored = {"--processor", "--gpu-device-id", "--mode", "--fn-o-log", "--fn-o-energy", "--integrator",
-                        "--electrostatic", "--ele-alpha", "--expected-num-density"}
+                        "--expected-num-density"}
     lists = {"print_intvl_crd": [], "fn_o_crd": [], "group_o_crd": []}
     i = 0
     while i < len(toks):
@@ -187,6 +192,24 @@ def parse_run_config(text):
             groups.append(v)
         elif k == "--constraint":
             p["constraint"] = v
+        elif k == "--electrostatic":
+            if v not in ELECTROSTATIC:
+                raise ValueError("--electrostatic %s (%s)" % (v, ", ".join(ELECTROSTATIC)))
+            p["electrostatic"] = v
+        elif k == "--ele-alpha":
+            p["ele_alpha"] = float(v)
+        elif k == "--debye-huckel-dielectric":
+            p["dh_dielectric"] = float(v)
+        elif k == "--debye-huckel-ionic-strength":
+            p["dh_ionic_strength"] = float(v)
+        elif k == "--debye-huckel-temperature":
+            p["dh_temperature"] = float(v)
+        elif k == "--nonbond":   # Config.cpp:334-339
+            if v not in ("lennard-jones", "hydrophobicity-scale-lj"):
+                raise ValueError("--nonbond %s (lennard-jones, hydrophobicity-scale-lj)" % v)
+            p["nonbond"] = v
+        elif k == "--hydrophobicity-scale-epsiron":
+            p["hps_epsilon"] = float(v)
         elif k == "--extended-ensemble":
             # Config.cpp:145-157; V-AUS and VcMD are not on this path
             if v not in ("none", "v-mcmd"):
@@ -223,10 +246,6 @@ def parse_run_config(text):
         elif k in accepted_ignored:
             if k == "--integrator" and v != "leapfrog-presto":
                 raise ValueError("only --integrator leapfrog-presto is on the hot path")
-            if k == "--electrostatic" and v != "zero-dipole":
-                raise ValueError("only --electrostatic zero-dipole is on the hot path")
-            if k == "--ele-alpha" and float(v) != 0.0:
-                raise ValueError("only --ele-alpha 0 is on the hot path")
         else:
             raise ValueError("unsupported config key %s" % k)
     if groups:

@@ -1191,3 +1191,522 @@ int ogo_vmcmd_transition(int n_vs, const double *lam, const double *prob, int cu
     if (dest != cur) return dest;
     return vs_trial(n_vs, lam, prob, cur, -1, lambda, st);
 }
+
+/* ------------------------------------------------ other electrostatics / nonbond models */
+
+#define OGO_PI 3.14159265                /* CelesteObject.cpp:27 */
+#define OGO_EPS 1e-10                    /* CelesteObject.cpp:30 */
+#define OGO_ELEM_CHARGE 1.60217657e-19   /* CelesteObject.cpp:32 */
+#define OGO_AVOGADRO 6.0221413e23        /* CelesteObject.cpp:33 */
+#define OGO_PERMITTIVITY 8.85418782e-12  /* CelesteObject.cpp:34 */
+#define OGO_BOLTZMAN 1.380658e-23        /* CelesteObject.cpp:39 */
+
+/* ZeroMultipoleSum::set_zms_params (ZeroMultipoleSum.cpp:108-202): members are float, the
+ * literals double, so each expression is evaluated as the C++ code evaluates it. */
+void ogo_ele_init(ogo_ele *m, int mode, double alpha, double cutoff, double dh_dielectric,
+                  double dh_ionic_strength, double dh_temperature) {
+    memset(m, 0, sizeof(*m));
+    m->mode = mode;
+    m->alpha = (float)alpha;
+    m->cutoff = (float)cutoff;
+    const float c = m->cutoff, a = m->alpha;
+    const float c2 = c * c, c3 = c2 * c, c4 = c2 * c2, c5 = c3 * c2, c6 = c3 * c3, c7 = c3 * c4;
+    const float tmp = c * a;
+    const float erc = erfcf(tmp);
+    const float expterm = expf(-tmp * tmp);
+    float fcoeff, bcoeff, hzqrc, d1, d2, d3, d4, piewald = 0.0f;
+    m->alpha0 = (double)a < OGO_EPS;
+    if (m->alpha0) {
+        fcoeff = (float)(1.0 / c3);
+        bcoeff = (float)(0.5 * fcoeff);
+        hzqrc = (float)(2.0 / c3);
+        d1 = (float)(1.0 / c2);
+        d2 = (float)(2.0 / c3);
+        d3 = (float)(6.0 / c4);
+        d4 = (float)(24.0 / c5);
+    } else {
+        const float root_pi = (float)sqrt(OGO_PI);
+        piewald = (float)(2.0 / root_pi * a);
+        fcoeff = erc / c3 + piewald * expterm / c2;
+        bcoeff = (float)(0.5 * fcoeff);
+        const float t3 = tmp * tmp * tmp, t5 = t3 * tmp * tmp, t7 = t5 * tmp * tmp;
+        hzqrc = (float)((erc + expterm * (tmp + t3) * 2.0 / root_pi) * 2.0 / c3);
+        d1 = (float)((erc + expterm * tmp * 2.0 / root_pi) / c2);
+        d2 = (float)((erc + expterm * (tmp + t3) * 2.0 / root_pi) * 2.0 / c3);
+        d3 = (float)((erc + expterm * (tmp + 2.0 / 3.0 * t3 + 2.0 / 3.0 * t5) * 2.0 / root_pi) * 6.0 / c4);
+        /* "+ 1.0 / 3.0 + tmp_7" as the reference writes it */
+        d4 = (float)((erc + expterm * (tmp + 2.0 / 3.0 * t3 + 1.0 / 6.0 * t5 + 1.0 / 3.0 + t7) * 2.0 / root_pi) * 24.0 /
+                     c5);
+    }
+    m->fcoeff = fcoeff;
+    m->bcoeff = bcoeff;
+    m->piewald = piewald;
+    m->zqcoeff2 = (float)(-3.0 / 4.0 * fcoeff - hzqrc / 4.0);
+    m->zqcoeff4 = (float)(fcoeff / 8.0 / c2 + hzqrc / 8.0 / c2);
+    m->zqcoeff22 = (float)(2.0 * m->zqcoeff2);
+    m->zqcoeff44 = (float)(4.0 * m->zqcoeff4);
+    m->zocoeff2 = (float)(-15.0 / 16.0 * d1 / c - 7.0 / 16.0 * d2 - 1.0 / 16.0 * d3 * c);
+    m->zocoeff4 = (float)(5.0 / 16.0 * d1 / c3 + 5.0 / 16.0 * d2 / c2 + 1.0 / 16.0 * d3 / c);
+    m->zocoeff6 = (float)(-1.0 / 16.0 * d1 / c5 - 1.0 / 16.0 * d2 / c4 - 1.0 / 48.0 * d3 / c3);
+    m->zocoeff22 = (float)(2.0 * m->zocoeff2);
+    m->zocoeff44 = (float)(4.0 * m->zocoeff4);
+    m->zocoeff66 = (float)(6.0 * m->zocoeff6);
+    m->zhcoeff2 = (float)(-35.0 / 32.0 * d1 / c - 19.0 / 32.0 * d2 - 1.0 / 96.0 * d4 * c2 - 1.0 / 8.0 * d3 * c);
+    m->zhcoeff4 = (float)(1.0 / 64.0 * d4 + 35.0 / 64.0 * d1 / c3 + 35.0 / 64.0 * d2 / c2 + 5.0 / 32.0 * d3 / c);
+    m->zhcoeff6 = (float)(-7.0 / 32.0 * d1 / c5 - 7.0 / 32.0 * d2 / c4 - 1.0 / 12.0 * d3 / c3 - 1.0 / 96.0 * d4 / c2);
+    m->zhcoeff8 = (float)(5.0 / 128.0 * d2 / c6 + 5.0 / 128.0 * d1 / c7 + 1.0 / 64.0 * d3 / c5 + 1.0 / 384.0 * d4 / c4);
+    m->zhcoeff22 = (float)(2.0 * m->zhcoeff2);
+    m->zhcoeff44 = (float)(4.0 * m->zhcoeff4);
+    m->zhcoeff66 = (float)(6.0 * m->zhcoeff6);
+    m->zhcoeff88 = (float)(8.0 * m->zhcoeff8);
+    m->zcore = erc / c + bcoeff * c2;
+    m->zqcore = erc / c - m->zqcoeff2 * c2 - m->zqcoeff4 * c4;
+    m->zocore = erc / c - m->zocoeff2 * c2 - m->zocoeff4 * c4 - m->zocoeff6 * c6;
+    m->zhcore = erc / c - m->zhcoeff2 * c2 - m->zhcoeff4 * c4 - m->zhcoeff6 * c6 - m->zhcoeff8 * c6 * c2;
+    switch (mode) {  /* ZeroMultipoleSum::cal_self_energy (ZeroMultipoleSum.cpp:71-77) */
+        case OGO_ELE_ZD: m->zmcore = m->zcore; break;
+        case OGO_ELE_ZQ: m->zmcore = m->zqcore; break;
+        case OGO_ELE_ZO: m->zmcore = m->zocore; break;
+        case OGO_ELE_ZH: m->zmcore = m->zhcore; break;
+        default: m->zmcore = 0.0f;
+    }
+    if (mode == OGO_ELE_DH) { /* the constructor's members (ZeroMultipoleSum.cpp:20-24) */
+        m->dielectric_inv = (float)(1.0 / dh_dielectric);
+        m->debye_length_inv =
+            (float)(1.0 / (sqrt(OGO_PERMITTIVITY * dh_dielectric * OGO_BOLTZMAN * dh_temperature /
+                                (2 * OGO_AVOGADRO * OGO_ELEM_CHARGE * OGO_ELEM_CHARGE * dh_ionic_strength)) *
+                           1e10));
+    }
+}
+
+void ogo_ele_init64(ogo_ele64 *m, int mode, double alpha, double cutoff, double dh_dielectric,
+                    double dh_ionic_strength, double dh_temperature) {
+    memset(m, 0, sizeof(*m));
+    m->mode = mode;
+    m->alpha = alpha;
+    m->cutoff = cutoff;
+    const double c = cutoff, a = alpha;
+    const double c2 = c * c, c3 = c2 * c, c4 = c2 * c2, c5 = c3 * c2, c6 = c3 * c3, c7 = c3 * c4;
+    const double tmp = c * a, erc = erfc(tmp), expterm = exp(-tmp * tmp);
+    double hzqrc, d1, d2, d3, d4;
+    m->alpha0 = a < OGO_EPS;
+    if (m->alpha0) {
+        m->fcoeff = 1.0 / c3;
+        hzqrc = 2.0 / c3;
+        d1 = 1.0 / c2;
+        d2 = 2.0 / c3;
+        d3 = 6.0 / c4;
+        d4 = 24.0 / c5;
+    } else {
+        const double root_pi = sqrt(OGO_PI);
+        m->piewald = 2.0 / root_pi * a;
+        m->fcoeff = erc / c3 + m->piewald * expterm / c2;
+        const double t3 = tmp * tmp * tmp, t5 = t3 * tmp * tmp, t7 = t5 * tmp * tmp;
+        hzqrc = (erc + expterm * (tmp + t3) * 2.0 / root_pi) * 2.0 / c3;
+        d1 = (erc + expterm * tmp * 2.0 / root_pi) / c2;
+        d2 = (erc + expterm * (tmp + t3) * 2.0 / root_pi) * 2.0 / c3;
+        d3 = (erc + expterm * (tmp + 2.0 / 3.0 * t3 + 2.0 / 3.0 * t5) * 2.0 / root_pi) * 6.0 / c4;
+        d4 = (erc + expterm * (tmp + 2.0 / 3.0 * t3 + 1.0 / 6.0 * t5 + 1.0 / 3.0 + t7) * 2.0 / root_pi) * 24.0 / c5;
+    }
+    const double f = m->fcoeff;
+    m->bcoeff = 0.5 * f;
+    m->zqcoeff2 = -3.0 / 4.0 * f - hzqrc / 4.0;
+    m->zqcoeff4 = f / 8.0 / c2 + hzqrc / 8.0 / c2;
+    m->zqcoeff22 = 2.0 * m->zqcoeff2;
+    m->zqcoeff44 = 4.0 * m->zqcoeff4;
+    m->zocoeff2 = -15.0 / 16.0 * d1 / c - 7.0 / 16.0 * d2 - 1.0 / 16.0 * d3 * c;
+    m->zocoeff4 = 5.0 / 16.0 * d1 / c3 + 5.0 / 16.0 * d2 / c2 + 1.0 / 16.0 * d3 / c;
+    m->zocoeff6 = -1.0 / 16.0 * d1 / c5 - 1.0 / 16.0 * d2 / c4 - 1.0 / 48.0 * d3 / c3;
+    m->zocoeff22 = 2.0 * m->zocoeff2;
+    m->zocoeff44 = 4.0 * m->zocoeff4;
+    m->zocoeff66 = 6.0 * m->zocoeff6;
+    m->zhcoeff2 = -35.0 / 32.0 * d1 / c - 19.0 / 32.0 * d2 - 1.0 / 96.0 * d4 * c2 - 1.0 / 8.0 * d3 * c;
+    m->zhcoeff4 = 1.0 / 64.0 * d4 + 35.0 / 64.0 * d1 / c3 + 35.0 / 64.0 * d2 / c2 + 5.0 / 32.0 * d3 / c;
+    m->zhcoeff6 = -7.0 / 32.0 * d1 / c5 - 7.0 / 32.0 * d2 / c4 - 1.0 / 12.0 * d3 / c3 - 1.0 / 96.0 * d4 / c2;
+    m->zhcoeff8 = 5.0 / 128.0 * d2 / c6 + 5.0 / 128.0 * d1 / c7 + 1.0 / 64.0 * d3 / c5 + 1.0 / 384.0 * d4 / c4;
+    m->zhcoeff22 = 2.0 * m->zhcoeff2;
+    m->zhcoeff44 = 4.0 * m->zhcoeff4;
+    m->zhcoeff66 = 6.0 * m->zhcoeff6;
+    m->zhcoeff88 = 8.0 * m->zhcoeff8;
+    m->zcore = erc / c + m->bcoeff * c2;
+    m->zqcore = erc / c - m->zqcoeff2 * c2 - m->zqcoeff4 * c4;
+    m->zocore = erc / c - m->zocoeff2 * c2 - m->zocoeff4 * c4 - m->zocoeff6 * c6;
+    m->zhcore = erc / c - m->zhcoeff2 * c2 - m->zhcoeff4 * c4 - m->zhcoeff6 * c6 - m->zhcoeff8 * c6 * c2;
+    m->zmcore = mode == OGO_ELE_ZD ? m->zcore : mode == OGO_ELE_ZQ ? m->zqcore : mode == OGO_ELE_ZO ? m->zocore
+              : mode == OGO_ELE_ZH ? m->zhcore : 0.0;
+    if (mode == OGO_ELE_DH) {
+        m->dielectric_inv = 1.0 / dh_dielectric;
+        m->debye_length_inv = 1.0 / (sqrt(OGO_PERMITTIVITY * dh_dielectric * OGO_BOLTZMAN * dh_temperature /
+                                          (2 * OGO_AVOGADRO * OGO_ELEM_CHARGE * OGO_ELEM_CHARGE * dh_ionic_strength)) *
+                                     1e10);
+    }
+}
+
+/* The pair functions of ZeroMultipoleSum.cpp:309-455 (func_calc_zms), float. */
+static void ele_pair_f(const ogo_ele *m, float *e, float *g, float r, float r2, float ri, float r2i, float r3i,
+                       float cc) {
+    const float r4 = r2 * r2, r6 = r4 * r2, r8 = r4 * r4;
+    if (m->mode == OGO_ELE_DH) {
+        const float ld = expf(-r * m->debye_length_inv);
+        *e = cc * ri * m->dielectric_inv * ld;
+        *g = -*e * (ri + m->debye_length_inv);
+        return;
+    }
+    float erc = 1.0f, ex = 0.0f;
+    if (!m->alpha0) {
+        const float t = r * m->alpha;
+        erc = erfcf(t);
+        ex = m->piewald * expf(-t * t) * r2i;
+    }
+    switch (m->mode) {
+        case OGO_ELE_ZD:
+            if (m->alpha0) {
+                *e = cc * (ri - m->zcore + m->bcoeff * r2);
+                *g = -cc * (r3i - m->fcoeff);
+            } else {
+                *e = cc * (ri * erc - m->zcore + m->bcoeff * r2);
+                *g = -cc * (erc * r3i + ex - m->fcoeff);
+            }
+            break;
+        case OGO_ELE_ZQ:
+            if (m->alpha0) {
+                *e = cc * (ri - m->zqcore - m->zqcoeff2 * r2 - m->zqcoeff4 * r4);
+                *g = -cc * (r3i + m->zqcoeff22 + m->zqcoeff44 * r2);
+            } else {
+                *e = cc * (ri * erc - m->zqcore - m->zqcoeff2 * r2 - m->zqcoeff4 * r4);
+                *g = -cc * (r3i * erc + ex + m->zqcoeff22 + m->zqcoeff44 * r2);
+            }
+            break;
+        case OGO_ELE_ZO:
+            if (m->alpha0) {
+                *e = cc * (ri - m->zocore - m->zocoeff2 * r2 - m->zocoeff4 * r4 - m->zocoeff6 * r6);
+                *g = -cc * (r3i + m->zocoeff22 + m->zocoeff44 * r2 + m->zocoeff66 * r4);
+            } else {  /* gradient with the hexadecapole coefficients (ZeroMultipoleSum.cpp:396-398) */
+                *e = cc * (ri * erc - m->zocore - m->zocoeff2 * r2 - m->zocoeff4 * r4 - m->zocoeff6 * r6);
+                *g = -cc * (r3i * erc + ex + m->zhcoeff22 + m->zhcoeff44 * r2 + m->zhcoeff66 * r4);
+            }
+            break;
+        default:  /* OGO_ELE_ZH */
+            if (m->alpha0) {
+                *e = cc * (ri - m->zhcore - m->zhcoeff2 * r2 - m->zhcoeff4 * r4 - m->zhcoeff6 * r6 - m->zhcoeff8 * r8);
+                *g = -cc * (r3i + m->zhcoeff22 + m->zhcoeff44 * r2 + m->zhcoeff66 * r4 + m->zhcoeff88 * r6);
+            } else {
+                *e = cc * (ri * erc - m->zhcore - m->zhcoeff2 * r2 - m->zhcoeff4 * r4 - m->zhcoeff6 * r6 -
+                           m->zhcoeff8 * r8);
+                *g = -cc * (r3i * erc + ex + m->zhcoeff22 + m->zhcoeff44 * r2 + m->zhcoeff66 * r4 + m->zhcoeff88 * r6);
+            }
+    }
+}
+
+/* The excess functions (func_calc_zms_excess, ZeroMultipoleSum.cpp:204-307; calc_null for
+ * Debye-Hueckel), float; r4 of the octupole alpha = 0 form is a double in the reference. */
+static void ele_excess_f(const ogo_ele *m, float *e, float *g, float r, float r2, float ri, float r2i, float r3i,
+                         float cc) {
+    if (m->mode == OGO_ELE_DH) {
+        *e = 0.0f;
+        *g = 0.0f;
+        return;
+    }
+    float erc = 1.0f, erfn = 0.0f, ex = 0.0f;
+    if (!m->alpha0) {
+        const float t = m->alpha * r;
+        erc = erfcf(t);
+        erfn = (float)(1.0 - erc);
+        ex = m->piewald * expf(-t * t) * r2i;
+    }
+    const float r4 = r2 * r2;
+    switch (m->mode) {
+        case OGO_ELE_ZD:
+            if (m->alpha0) {
+                *e = cc * m->bcoeff * r2;
+                *g = cc * m->fcoeff;
+            } else {  /* "-errorfn * r12" as written (ZeroMultipoleSum.cpp:215) */
+                *e = cc * (-erfn * r + m->bcoeff * r2);
+                *g = -cc * (erc * r3i + ex - m->fcoeff - r3i);
+            }
+            break;
+        case OGO_ELE_ZQ:
+            if (m->alpha0) {
+                *e = cc * (-m->zqcoeff2 * r2 - m->zqcoeff4 * r2 * r2);
+                *g = -cc * (m->zqcoeff22 + m->zqcoeff44 * r2);
+            } else {
+                *e = cc * (-erfn * ri - m->zqcoeff2 * r2 - m->zqcoeff4 * r2 * r2);
+                *g = -cc * (erc * r3i + ex + m->zqcoeff22 + m->zqcoeff44 * r2 - r3i);
+            }
+            break;
+        case OGO_ELE_ZO:
+            if (m->alpha0) {
+                const double r4d = (double)(r2 * r2);  /* a float product stored in a double */
+                *e = (float)(cc * (-m->zocoeff2 * r2 - m->zocoeff4 * r4d - m->zocoeff6 * r4d * r));
+                *g = (float)(-cc * (m->zocoeff22 + m->zocoeff44 * r2 + m->zocoeff66 * r4d));
+            } else {
+                *e = cc * (-erfn * ri - m->zocoeff2 * r2 - m->zocoeff4 * r4 - m->zocoeff6 * r4 * r);
+                *g = -cc * (erc * r3i + ex + m->zocoeff22 + m->zocoeff44 * r2 + m->zocoeff66 * r4 - r3i);
+            }
+            break;
+        default: {  /* OGO_ELE_ZH */
+            const float r6 = r4 * r2, r8 = r4 * r4;
+            if (m->alpha0) {
+                *e = cc * (-m->zhcoeff2 * r2 - m->zhcoeff4 * r4 - m->zhcoeff6 * r6 - m->zhcoeff8 * r8);
+                *g = -cc * (m->zhcoeff22 + m->zhcoeff44 * r2 + m->zhcoeff66 * r2 + m->zhcoeff88 * r6 - r3i);
+            } else {
+                *e = cc * (-erfn * ri - m->zhcoeff2 * r2 - m->zhcoeff4 * r4);
+                *g = -cc * (erc * r3i + ex + m->zhcoeff22 + m->zhcoeff44 * r2 + m->zhcoeff66 * r4 + m->zhcoeff88 * r6 -
+                            r3i);
+            }
+        }
+    }
+}
+
+/* ForceField::calc_pairwise with the model's electrostatics and HPS (ForceField.cpp:333-418). */
+static void calc_pair_f32_m(float *ev, float *ee, double w[3], const float c1[3], const float c2[3], float p6,
+                            float p12, float hcut, float hlam, float q1, float q2, double cutoff, const ogo_ele *m,
+                            const ogo_hps *h) {
+    float d[3];
+    for (int k = 0; k < 3; k++) d[k] = c1[k] - c2[k];
+    float r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    float r  = sqrtf(r2);
+    *ev = *ee = 0.0f;
+    w[0] = w[1] = w[2] = 0.0;
+    if ((double)r >= cutoff) return;
+    float r_inv = (float)(1.0 / (double)r), r2_inv = (float)(1.0 / (double)r2);
+    float r3_inv = r_inv * r2_inv, r6_inv = r3_inv * r3_inv, r12_inv = r6_inv * r6_inv;
+    float t6 = p6 * r6_inv, t12 = p12 * r12_inv;
+    *ev = -t6 + t12;
+    float wc = (float)((double)r2_inv * (-12.0 * (double)t12 + 6.0 * (double)t6));
+    if (h && h->on) {
+        if (r > hcut) {
+            *ev *= hlam;
+            wc *= hlam;
+        } else {
+            *ev += (1 - hlam) * h->eps;
+        }
+    }
+    float cc = (float)((double)(q1 * q2) * CHARGE_COEFF);
+    float gc;
+    ele_pair_f(m, ee, &gc, r, r2, r_inv, r2_inv, r3_inv, cc);
+    for (int k = 0; k < 3; k++) w[k] = (double)(wc * d[k] + gc * d[k]);
+}
+
+void ogo_pair_allpairs_f32_m(const ogo_pbc *p, int n, const double *crd, const float *charge, const int *atom_type,
+                             int n_types, const float *lj6, const float *lj12, const int *nb15off, int max_nb15off,
+                             double cutoff, const ogo_ele *m, const ogo_hps *h, double *work, double ene[2]) {
+    memset(work, 0, sizeof(double) * 3 * (size_t)n);
+    ene[0] = ene[1] = 0.0;
+    for (int a1 = 0; a1 < n; a1++) {
+        float x1[3] = {(float)crd[a1 * 3], (float)crd[a1 * 3 + 1], (float)crd[a1 * 3 + 2]};
+        for (int a2 = 0; a2 < a1; a2++) {
+            float x2[3] = {(float)crd[a2 * 3], (float)crd[a2 * 3 + 1], (float)crd[a2 * 3 + 2]};
+            int excl = 0;
+            for (int k = 0; k < max_nb15off; k++)
+                if (nb15off[(size_t)a1 * max_nb15off + k] == a2) excl = 1;
+            if (excl) continue;
+            int ti = atom_type[a1] * n_types + atom_type[a2];
+            for (int d = 0; d < 3; d++) {
+                if (x2[d] - x1[d] >= p->L_half[d]) x2[d] -= p->L[d];
+                else if (x2[d] - x1[d] <= -p->L_half[d]) x2[d] += p->L[d];
+            }
+            float ev, ee;
+            double w[3];
+            calc_pair_f32_m(&ev, &ee, w, x1, x2, lj6[ti], lj12[ti], h && h->on ? h->cut[ti] : 0.0f,
+                            h && h->on ? h->lambda[ti] : 1.0f, charge[a1], charge[a2], cutoff, m, h);
+            ene[0] += (double)ev;
+            ene[1] += (double)ee;
+            for (int d = 0; d < 3; d++) {
+                work[a1 * 3 + d] += w[d];
+                work[a2 * 3 + d] -= w[d];
+            }
+        }
+    }
+}
+
+double ogo_excess_f32_m(const ogo_pbc *p, int n_excess, const int *ep, const double *crd, const float *charge,
+                        const ogo_ele *m, double *work) {
+    double sum = 0.0;
+    for (int k = 0; k < n_excess; k++) {
+        int i = ep[2 * k], j = ep[2 * k + 1];
+        float c1[3] = {(float)crd[i * 3], (float)crd[i * 3 + 1], (float)crd[i * 3 + 2]};
+        float c2[3] = {(float)crd[j * 3], (float)crd[j * 3 + 1], (float)crd[j * 3 + 2]};
+        float d[3];
+        diff_minim_f(p, d, c1, c2);
+        /* ForceField::calc_zms_excess (ForceField.cpp:420-437) */
+        float r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+        float r = sqrtf(r2);
+        float ri = (float)(1.0 / (double)r);
+        float r2i = ri * ri, r3i = r2i * ri;
+        float cc = (float)((double)(charge[i] * charge[j]) * CHARGE_COEFF);
+        float e, g;
+        ele_excess_f(m, &e, &g, r, r2, ri, r2i, r3i, cc);
+        sum += (double)e;
+        for (int q = 0; q < 3; q++) {
+            double w = (double)(g * d[q]);
+            work[i * 3 + q] += w;
+            work[j * 3 + q] -= w;
+        }
+    }
+    return sum;
+}
+
+double ogo_self_energy_m(int n, int n_excess, const int *ep, const float *charge, const ogo_ele *m) {
+    double *dw = (double *)calloc((size_t)(n > 0 ? n : 1), sizeof(double));
+    for (int k = 0; k < n_excess; k++) {
+        dw[ep[2 * k]] += (double)charge[ep[2 * k + 1]];
+        dw[ep[2 * k + 1]] += (double)charge[ep[2 * k]];
+    }
+    float mon = 0.0f;
+    const double zmcore = (double)m->zmcore;
+    for (int i = 0; i < n; i++) {
+        const double q = (double)charge[i];
+        const double es = ((double)(-m->piewald * charge[i] * charge[i]) - zmcore * q * (q + dw[i])) * 0.5 * CHARGE_COEFF;
+        mon = (float)((double)mon + es);
+    }
+    free(dw);
+    return (double)mon;
+}
+
+/* FP64 forms of the same functions, for the parity oracle. */
+static void ele_pair_d(const ogo_ele64 *m, double *e, double *g, double r, double r2, double cc) {
+    const double ri = 1.0 / r, r2i = 1.0 / r2, r3i = ri * r2i, r4 = r2 * r2, r6 = r4 * r2, r8 = r4 * r4;
+    if (m->mode == OGO_ELE_DH) {
+        *e = cc * ri * m->dielectric_inv * exp(-r * m->debye_length_inv);
+        *g = -*e * (ri + m->debye_length_inv);
+        return;
+    }
+    double erc = 1.0, ex = 0.0;
+    if (!m->alpha0) {
+        const double t = r * m->alpha;
+        erc = erfc(t);
+        ex = m->piewald * exp(-t * t) * r2i;
+    }
+    switch (m->mode) {
+        case OGO_ELE_ZD:
+            *e = cc * (ri * erc - m->zcore + m->bcoeff * r2);
+            *g = -cc * (erc * r3i + ex - m->fcoeff);
+            break;
+        case OGO_ELE_ZQ:
+            *e = cc * (ri * erc - m->zqcore - m->zqcoeff2 * r2 - m->zqcoeff4 * r4);
+            *g = -cc * (r3i * erc + ex + m->zqcoeff22 + m->zqcoeff44 * r2);
+            break;
+        case OGO_ELE_ZO:
+            *e = cc * (ri * erc - m->zocore - m->zocoeff2 * r2 - m->zocoeff4 * r4 - m->zocoeff6 * r6);
+            if (m->alpha0) *g = -cc * (r3i + m->zocoeff22 + m->zocoeff44 * r2 + m->zocoeff66 * r4);
+            else *g = -cc * (r3i * erc + ex + m->zhcoeff22 + m->zhcoeff44 * r2 + m->zhcoeff66 * r4);
+            break;
+        default:
+            *e = cc * (ri * erc - m->zhcore - m->zhcoeff2 * r2 - m->zhcoeff4 * r4 - m->zhcoeff6 * r6 - m->zhcoeff8 * r8);
+            *g = -cc * (r3i * erc + ex + m->zhcoeff22 + m->zhcoeff44 * r2 + m->zhcoeff66 * r4 + m->zhcoeff88 * r6);
+    }
+}
+
+static void ele_excess_d(const ogo_ele64 *m, double *e, double *g, double r, double r2, double cc) {
+    *e = *g = 0.0;
+    if (m->mode == OGO_ELE_DH) return;
+    const double ri = 1.0 / r, r2i = ri * ri, r3i = r2i * ri, r4 = r2 * r2, r6 = r4 * r2, r8 = r4 * r4;
+    double erc = 1.0, erfn = 0.0, ex = 0.0;
+    if (!m->alpha0) {
+        const double t = m->alpha * r;
+        erc = erfc(t);
+        erfn = 1.0 - erc;
+        ex = m->piewald * exp(-t * t) * r2i;
+    }
+    switch (m->mode) {
+        case OGO_ELE_ZD:
+            if (m->alpha0) {
+                *e = cc * m->bcoeff * r2;
+                *g = cc * m->fcoeff;
+            } else {
+                *e = cc * (-erfn * r + m->bcoeff * r2);
+                *g = -cc * (erc * r3i + ex - m->fcoeff - r3i);
+            }
+            break;
+        case OGO_ELE_ZQ:
+            *e = cc * (-erfn * ri - m->zqcoeff2 * r2 - m->zqcoeff4 * r4);
+            *g = -cc * (m->alpha0 ? (m->zqcoeff22 + m->zqcoeff44 * r2)
+                                  : (erc * r3i + ex + m->zqcoeff22 + m->zqcoeff44 * r2 - r3i));
+            break;
+        case OGO_ELE_ZO:
+            *e = cc * (-erfn * ri - m->zocoeff2 * r2 - m->zocoeff4 * r4 - m->zocoeff6 * r4 * r);
+            *g = -cc * (m->alpha0 ? (m->zocoeff22 + m->zocoeff44 * r2 + m->zocoeff66 * r4)
+                                  : (erc * r3i + ex + m->zocoeff22 + m->zocoeff44 * r2 + m->zocoeff66 * r4 - r3i));
+            break;
+        default:
+            if (m->alpha0) {
+                *e = cc * (-m->zhcoeff2 * r2 - m->zhcoeff4 * r4 - m->zhcoeff6 * r6 - m->zhcoeff8 * r8);
+                *g = -cc * (m->zhcoeff22 + m->zhcoeff44 * r2 + m->zhcoeff66 * r2 + m->zhcoeff88 * r6 - r3i);
+            } else {
+                *e = cc * (-erfn * ri - m->zhcoeff2 * r2 - m->zhcoeff4 * r4);
+                *g = -cc * (erc * r3i + ex + m->zhcoeff22 + m->zhcoeff44 * r2 + m->zhcoeff66 * r4 + m->zhcoeff88 * r6 -
+                            r3i);
+            }
+    }
+}
+
+void ogo_pair_cells_f64_m(const double L[3], const ogo_grid *gr, const ogo_cellpairs *cp, const double *crd,
+                          const double *charge, const int *atom_type, int n_types, const double *lj6,
+                          const double *lj12, double cutoff, const ogo_ele64 *m, const ogo_hps64 *h, double *work,
+                          double ene[2], double vir[9]) {
+    ene[0] = ene[1] = 0.0;
+    for (int k = 0; k < 9; k++) vir[k] = 0.0;
+    for (int k = 0; k < cp->n_pairs; k++) {
+        int c1 = cp->cell1[k], c2 = cp->cell2[k], img = cp->image[k];
+        double sh[3] = {(img & 1) ? -L[0] : (img & 2) ? L[0] : 0.0, (img & 4) ? -L[1] : (img & 8) ? L[1] : 0.0,
+                        (img & 16) ? -L[2] : (img & 32) ? L[2] : 0.0};
+        for (int a2 = 0; a2 < OGO_N_ATOM_CELL; a2++) {
+            int id2 = gr->slot_atomid[c2 * OGO_N_ATOM_CELL + a2];
+            for (int a1 = 0; a1 < OGO_N_ATOM_CELL; a1++) {
+                if ((cp->mask[k] >> (a2 * OGO_N_ATOM_CELL + a1)) & 1) continue;
+                int id1 = gr->slot_atomid[c1 * OGO_N_ATOM_CELL + a1];
+                double d[3];
+                for (int q = 0; q < 3; q++) d[q] = crd[id1 * 3 + q] - (crd[id2 * 3 + q] + sh[q]);
+                double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+                if (r2 >= cutoff * cutoff) continue;
+                int ti = atom_type[id1] * n_types + atom_type[id2];
+                double r = sqrt(r2), r2i = 1.0 / r2, r6i = r2i * r2i * r2i;
+                double t6 = lj6[ti] * r6i, t12 = lj12[ti] * r6i * r6i;
+                double ev = t12 - t6, wl = r2i * (-12.0 * t12 + 6.0 * t6);
+                if (h && h->on) {
+                    if (r > h->cut[ti]) {
+                        ev *= h->lambda[ti];
+                        wl *= h->lambda[ti];
+                    } else {
+                        ev += (1.0 - h->lambda[ti]) * h->eps;
+                    }
+                }
+                double ee, ge, w[3];
+                ele_pair_d(m, &ee, &ge, r, r2, charge[id1] * charge[id2] * CHARGE_COEFF);
+                ene[0] += ev;
+                ene[1] += ee;
+                for (int q = 0; q < 3; q++) {
+                    w[q] = (wl + ge) * d[q];
+                    work[id1 * 3 + q] += w[q];
+                    work[id2 * 3 + q] -= w[q];
+                }
+                add_vir(vir, d, w);
+            }
+        }
+    }
+}
+
+double ogo_excess_f64_m(const double L[3], int n_excess, const int *ep, const double *crd, const double *charge,
+                        const ogo_ele64 *m, double *work, double vir[9]) {
+    double sum = 0.0;
+    for (int k = 0; k < n_excess; k++) {
+        int i = ep[2 * k], j = ep[2 * k + 1];
+        double d[3], w[3];
+        for (int q = 0; q < 3; q++) {
+            d[q] = crd[i * 3 + q] - crd[j * 3 + q];
+            d[q] -= L[q] * nearbyint(d[q] / L[q]);
+        }
+        double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+        double e, g;
+        ele_excess_d(m, &e, &g, sqrt(r2), r2, charge[i] * charge[j] * CHARGE_COEFF);
+        sum += e;
+        for (int q = 0; q < 3; q++) {
+            w[q] = g * d[q];
+            work[i * 3 + q] += w[q];
+            work[j * 3 + q] -= w[q];
+        }
+        if (vir) add_vir(vir, d, w);
+    }
+    return sum;
+}

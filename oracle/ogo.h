@@ -123,6 +123,60 @@ double ogo_excess_f64(const double L[3], int n_excess, const int *excess_pairs, 
 /* Self energy sum (ZeroMultipoleSum.cpp:43-106) with the float running sum. */
 double ogo_self_energy(int n, int n_excess, const int *excess_pairs, const float *charge, float zcore);
 
+/* ---- electrostatics and nonbond models other than zero-dipole alpha = 0 (ZeroMultipoleSum.cpp:
+ * 108-466, ForceField.cpp:30-100,333-418).  Modes: --electrostatic zero-dipole / -quadrupole /
+ * -octupole / -hexadecapole (alpha = --ele-alpha, 0 or > 0) and debye-huckel; HPS (--nonbond
+ * hydrophobicity-scale-lj) scales the LJ term per type pair.  The formulas are the reference's,
+ * including the places where they depart from the textbook forms (which the pin fixtures
+ * confirm): the octupole alpha > 0 gradient uses the hexadecapole coefficients, and several
+ * excess functions keep truncated or mismatched terms. */
+#define OGO_ELE_ZD 0
+#define OGO_ELE_ZQ 1
+#define OGO_ELE_ZO 2
+#define OGO_ELE_ZH 3
+#define OGO_ELE_DH 4
+typedef struct {
+    int mode, alpha0;
+    float alpha, cutoff, bcoeff, fcoeff, piewald, zmcore;
+    float zcore, zqcore, zocore, zhcore;
+    float zqcoeff2, zqcoeff4, zqcoeff22, zqcoeff44;
+    float zocoeff2, zocoeff4, zocoeff6, zocoeff22, zocoeff44, zocoeff66;
+    float zhcoeff2, zhcoeff4, zhcoeff6, zhcoeff8, zhcoeff22, zhcoeff44, zhcoeff66, zhcoeff88;
+    float dielectric_inv, debye_length_inv;
+} ogo_ele;
+/* the same coefficients in double precision (FP64 oracle) */
+typedef struct {
+    int mode, alpha0;
+    double alpha, cutoff, bcoeff, fcoeff, piewald, zmcore;
+    double zcore, zqcore, zocore, zhcore;
+    double zqcoeff2, zqcoeff4, zqcoeff22, zqcoeff44;
+    double zocoeff2, zocoeff4, zocoeff6, zocoeff22, zocoeff44, zocoeff66;
+    double zhcoeff2, zhcoeff4, zhcoeff6, zhcoeff8, zhcoeff22, zhcoeff44, zhcoeff66, zhcoeff88;
+    double dielectric_inv, debye_length_inv;
+} ogo_ele64;
+/* HPS parameters: per type pair (n_types^2) cutoff and lambda; off when on == 0 */
+typedef struct { int on; float eps; const float *cut, *lambda; } ogo_hps;
+typedef struct { int on; double eps; const double *cut, *lambda; } ogo_hps64;
+
+/* ZeroMultipoleSum constructor + set_zms_params (ZeroMultipoleSum.cpp:6-28,108-202) with the
+ * reference's float members and double intermediates. */
+void ogo_ele_init(ogo_ele *m, int mode, double alpha, double cutoff, double dh_dielectric,
+                  double dh_ionic_strength, double dh_temperature);
+void ogo_ele_init64(ogo_ele64 *m, int mode, double alpha, double cutoff, double dh_dielectric,
+                    double dh_ionic_strength, double dh_temperature);
+void ogo_pair_allpairs_f32_m(const ogo_pbc *p, int n, const double *crd, const float *charge, const int *atom_type,
+                             int n_types, const float *lj6, const float *lj12, const int *nb15off, int max_nb15off,
+                             double cutoff, const ogo_ele *m, const ogo_hps *h, double *work, double ene[2]);
+void ogo_pair_cells_f64_m(const double L[3], const ogo_grid *gr, const ogo_cellpairs *cp, const double *crd,
+                          const double *charge, const int *atom_type, int n_types, const double *lj6,
+                          const double *lj12, double cutoff, const ogo_ele64 *m, const ogo_hps64 *h, double *work,
+                          double ene[2], double vir[9]);
+double ogo_excess_f32_m(const ogo_pbc *p, int n_excess, const int *excess_pairs, const double *crd,
+                        const float *charge, const ogo_ele *m, double *work);
+double ogo_excess_f64_m(const double L[3], int n_excess, const int *excess_pairs, const double *crd,
+                        const double *charge, const ogo_ele64 *m, double *work, double vir[9]);
+double ogo_self_energy_m(int n, int n_excess, const int *excess_pairs, const float *charge, const ogo_ele *m);
+
 /* Excess pairs as MmSystem::set_excess_pairs builds them (MmSystem.cpp:700-736). */
 int ogo_excess_pairs(int n, const int *nb15off, int max_nb15off, int *out_pairs /* [2*cap] */, int cap);
 

@@ -25,6 +25,41 @@ class Pbc(C.Structure):
     _fields_ = [(k, C.c_float * 3) for k in ("L", "L_half", "L_inv", "L_half_inv", "lower", "upper")]
 
 
+class Hps(C.Structure):
+    _fields_ = [("on", C.c_int), ("eps", C.c_float), ("cut", C.POINTER(C.c_float)), ("lam", C.POINTER(C.c_float))]
+
+
+class Hps64(C.Structure):
+    _fields_ = [("on", C.c_int), ("eps", C.c_double), ("cut", C.POINTER(C.c_double)), ("lam", C.POINTER(C.c_double))]
+
+
+class EleModel:
+    """The electrostatics / nonbond model of a run (ogo_ele_init; engine.ELECTROSTATIC codes):
+    float coefficients for the FP32 restatement, double ones for the FP64 oracle, HPS tables."""
+
+    def __init__(self, params, topol):
+        from omegagene_b200 import cls_io, engine
+        self.mode = engine.ELECTROSTATIC[params.get("electrostatic", "zero-dipole")]
+        self.alpha = float(params.get("ele_alpha", 0.0))
+        self.hps_on = params.get("nonbond", "lennard-jones") == "hydrophobicity-scale-lj"
+        self.default = self.mode == 0 and self.alpha < 1e-10 and not self.hps_on
+        L = lib()
+        dh = (float(params.get("dh_dielectric", 0.0)), float(params.get("dh_ionic_strength", 0.0)),
+              float(params.get("dh_temperature", 0.0)))
+        self.m32 = C.create_string_buffer(512)
+        self.m64 = C.create_string_buffer(512)
+        L.ogo_ele_init(self.m32, self.mode, self.alpha, float(params["cutoff"]), *dh)
+        L.ogo_ele_init64(self.m64, self.mode, self.alpha, float(params["cutoff"]), *dh)
+        cut, lam = cls_io.hps_tables(topol)
+        self.cut64, self.lam64 = np.ascontiguousarray(cut.reshape(-1)), np.ascontiguousarray(lam.reshape(-1))
+        self.cut32, self.lam32 = self.cut64.astype(np.float32), self.lam64.astype(np.float32)
+        eps = float(params.get("hps_epsilon", 0.0))
+        self.h32 = Hps(int(self.hps_on), eps, self.cut32.ctypes.data_as(C.POINTER(C.c_float)),
+                       self.lam32.ctypes.data_as(C.POINTER(C.c_float)))
+        self.h64 = Hps64(int(self.hps_on), eps, self.cut64.ctypes.data_as(C.POINTER(C.c_double)),
+                         self.lam64.ctypes.data_as(C.POINTER(C.c_double)))
+
+
 class Geom(C.Structure):
     _fields_ = [("n_atoms", C.c_int), ("cutoff_pair", C.c_float), ("cutoff_pair_half", C.c_float),
                 ("cutoff_pair2", C.c_float), ("exbox_l", C.c_float * 3), ("box_lower", C.c_float * 3),
@@ -88,6 +123,19 @@ def lib():
                                f64p, f64p, f64p]
         L.ogo_mcmd_scale.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int, f64p, C.c_double, C.c_int, f64p]
         L.ogo_mcmd_scale.restype = C.c_double
+        vp = C.c_void_p
+        L.ogo_ele_init.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]
+        L.ogo_ele_init64.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]
+        L.ogo_pair_allpairs_f32_m.argtypes = [C.POINTER(Pbc), C.c_int, f64p, f32p, i32p, C.c_int, f32p, f32p, i32p,
+                                              C.c_int, C.c_double, vp, C.POINTER(Hps), f64p, f64p]
+        L.ogo_pair_cells_f64_m.argtypes = [f64p, C.POINTER(Grid), C.POINTER(CellPairs), f64p, f64p, i32p, C.c_int,
+                                           f64p, f64p, C.c_double, vp, C.POINTER(Hps64), f64p, f64p, f64p]
+        L.ogo_excess_f32_m.argtypes = [C.POINTER(Pbc), C.c_int, i32p, f64p, f32p, vp, f64p]
+        L.ogo_excess_f32_m.restype = C.c_double
+        L.ogo_excess_f64_m.argtypes = [f64p, C.c_int, i32p, f64p, f64p, vp, f64p, f64p]
+        L.ogo_excess_f64_m.restype = C.c_double
+        L.ogo_self_energy_m.argtypes = [C.c_int, C.c_int, i32p, f32p, vp]
+        L.ogo_self_energy_m.restype = C.c_double
         L.ogo_mt_seed.argtypes = [u32p, C.c_uint32]
         L.ogo_mt_next.argtypes = [u32p]
         L.ogo_mt_next.restype = C.c_uint32
@@ -367,7 +415,11 @@ class OracleMD:
         self.c6, self.c12, self.nt = c6.reshape(-1).copy(), c12.reshape(-1).copy(), int(t["n_lj_types"])
         z, b, f = zd_constants(self.p["cutoff"])
         self.zcore = z
-        self.self_e = L.ogo_self_energy(n, len(self.ep) // 2, self.ep, self.q32, z)
+        self.model = EleModel(self.p, t)
+        if self.model.default:
+            self.self_e = L.ogo_self_energy(n, len(self.ep) // 2, self.ep, self.q32, z)
+        else:
+            self.self_e = L.ogo_self_energy_m(n, len(self.ep) // 2, self.ep, self.q32, self.model.m32)
         self.mass = np.ascontiguousarray(t["mass"], np.float64).astype(np.float32)
         self.mass_inv = (1.0 / self.mass.astype(np.float64)).astype(np.float32)
         crd = wrap_inbox(self.pbc, system["crd"]).reshape(-1)
@@ -484,7 +536,13 @@ class OracleMD:
         e = np.zeros(2)
         vir = np.zeros(9)
         vexc = np.zeros(9)
-        if self.pair_mode == "allpairs_f32":
+        M = self.model
+        if self.pair_mode == "allpairs_f32" and not M.default:
+            self.L.ogo_pair_allpairs_f32_m(self.pbc, n, self.crd, self.q32, self.ty, self.nt, self.c6f, self.c12f,
+                                           self.nb.reshape(-1), self.nb.shape[1], float(self.p["cutoff"]), M.m32,
+                                           C.byref(M.h32), w, e)
+            exc = self.L.ogo_excess_f32_m(self.pbc, len(self.ep) // 2, self.ep, self.crd, self.q32, M.m32, w)
+        elif self.pair_mode == "allpairs_f32":
             z, b, f = zd_constants(self.p["cutoff"])
             self.L.ogo_pair_allpairs_f32(self.pbc, n, self.crd, self.q32, self.ty, self.nt, self.c6f, self.c12f,
                                          self.nb.reshape(-1), self.nb.shape[1], float(self.p["cutoff"]), z, b, f, w, e)
@@ -493,10 +551,17 @@ class OracleMD:
             if self.cl is None or self.step_i % self.p["nsgrid_update_intvl"] == 0:
                 self.rebuild()
             pos = np.ascontiguousarray(self.slot_crd[self.cl.atomids_rev].reshape(-1))
-            self.L.ogo_pair_cells_f64(self.Ld, self.cl._grid, self.cl._cps, pos, self.q64, self.ty, self.nt, self.c6,
-                                      self.c12, float(self.p["cutoff"]), w, e, vir)
-            exc = self.L.ogo_excess_f64(self.Ld, len(self.ep) // 2, self.ep, self.crd, self.q64,
-                                        float(self.p["cutoff"]), w, vexc)
+            if M.default:
+                self.L.ogo_pair_cells_f64(self.Ld, self.cl._grid, self.cl._cps, pos, self.q64, self.ty, self.nt,
+                                          self.c6, self.c12, float(self.p["cutoff"]), w, e, vir)
+                exc = self.L.ogo_excess_f64(self.Ld, len(self.ep) // 2, self.ep, self.crd, self.q64,
+                                            float(self.p["cutoff"]), w, vexc)
+            else:
+                self.L.ogo_pair_cells_f64_m(self.Ld, self.cl._grid, self.cl._cps, pos, self.q64, self.ty, self.nt,
+                                            self.c6, self.c12, float(self.p["cutoff"]), M.m64, C.byref(M.h64), w, e,
+                                            vir)
+                exc = self.L.ogo_excess_f64_m(self.Ld, len(self.ep) // 2, self.ep, self.crd, self.q64, M.m64, w,
+                                              vexc)
         eb = ea = 0.0
         if self.bonds is not None:
             eb = self.L.ogo_bonds(self.pbc, len(self.bonds[1]), self.bonds[0], self.bonds[1], self.bonds[2], self.crd, w)

@@ -53,7 +53,7 @@ def main(ref_root):
            "lj_pairs": t["lj_pairs"], "bonds": t["bonds"], "angles": t["angles"], "torsions": t["torsions"],
            "impros": t["impros"], "nb14_atoms": t["nb14"]["atoms"], "nb14_types": t["nb14"]["types"],
            "nb14_coeff_vdw": t["nb14"]["coeff_vdw"], "nb14_coeff_ele": t["nb14"]["coeff_ele"],
-           "nb15off_pairs": t["nb15off_pairs"]}
+           "nb15off_pairs": t["nb15off_pairs"], "lj_hps_raw": np.frombuffer(t["lj_hps_raw"], np.uint8)}
     for k in ("pair_atoms", "pair_dist", "trio_atoms", "trio_dist", "quad_atoms", "quad_dist"):
         arr["cons_" + k] = c[k]
     arr["group_names"] = np.array(g["names"])
@@ -72,7 +72,8 @@ def load_system(path=os.path.join(HERE, "ala3_system.npz")):
              "impros": z["impros"],
              "nb14": {"atoms": z["nb14_atoms"], "types": z["nb14_types"], "coeff_vdw": z["nb14_coeff_vdw"],
                       "coeff_ele": z["nb14_coeff_ele"]},
-             "nb15off_pairs": z["nb15off_pairs"]}
+             "nb15off_pairs": z["nb15off_pairs"],
+             "lj_hps_raw": z["lj_hps_raw"].tobytes() if "lj_hps_raw" in z else b""}
     cons = {k: z["cons_" + k] for k in ("pair_atoms", "pair_dist", "trio_atoms", "trio_dist", "quad_atoms", "quad_dist")}
     return {"pbc_val": z["pbc_val"], "n_atoms": len(z["crd"]), "crd": z["crd"], "vel": z["vel"], "topol": topol,
             "constraint": cons, "groups": {"names": names, "atoms": [z["group_atoms_%d" % i] for i in range(len(names))]},
