@@ -162,7 +162,28 @@ typedef struct {
     /* NULL for a new run; else [OG_MT_WORDS] generator words and position as og_get_vmcmd_state
      * returns them, so a run handed over between engines continues its random sequence. */
     const uint32_t *vmcmd_mt_state;
+    /* Electrostatics and nonbond model (ForceField::set_config_parameters, ForceField.cpp:30-100;
+     * ZeroMultipoleSum.cpp:6-28,108-466).  ele_mode OG_ELE_* (--electrostatic) with ele_alpha
+     * (--ele-alpha) for the zero-multipole orders; Debye-Hueckel takes the three dh_* options
+     * (--debye-huckel-dielectric / -ionic-strength [M] / -temperature [K]).  hps = 1
+     * (--nonbond hydrophobicity-scale-lj) scales the LJ term per type pair: beyond the pair's
+     * cutoff energy and force times lambda, inside it the energy plus (1 - lambda) hps_epsilon
+     * (--hydrophobicity-scale-epsiron; ForceField.cpp:380-391); lj_hps_* are
+     * [n_lj_types^2] tables as MmSystem::set_lj_pair_hps_param fills them.  All zero: the
+     * zero-dipole alpha = 0 model with plain LJ. */
+    int32_t ele_mode;
+    double ele_alpha;
+    double dh_dielectric, dh_ionic_strength, dh_temperature;
+    int32_t hps;
+    double hps_epsilon;
+    const double *lj_hps_cutoff, *lj_hps_lambda;
 } og_system_desc;
+
+#define OG_ELE_ZD 0   /* zero-dipole */
+#define OG_ELE_ZQ 1   /* zero-quadrupole */
+#define OG_ELE_ZO 2   /* zero-octupole */
+#define OG_ELE_ZH 3   /* zero-hexadecapole */
+#define OG_ELE_DH 4   /* Debye-Hueckel */
 
 /* std::mt19937 state: 624 words and the next position (624 = twist before the next draw). */
 #define OG_MT_WORDS 625

@@ -50,18 +50,18 @@ template <bool VIR, int MINB>
 __global__ void k_pair_ljzd_jm(const int *, const int *, const SysDev *, const float4 *, const float4 *, const int *,
                                const int *, const float4 *, const int2 *, const unsigned long long *, const float2 *,
                                unsigned long long *, double *, long long);
-template <bool VIR, bool ENE, int MINB, int NT>
+template <bool VIR, bool ENE, int MINB, int NT, bool GEN>
 __global__ void k_pair_ljzd_jq(const int *, const int *, const SysDev *, const float4 *, const float4 *, const int *,
                                const int *, const float4 *, const int2 *, const unsigned long long *, const float2 *,
-                               unsigned long long *, double *, long long);
+                               unsigned long long *, double *, long long, const EleDev *, const float2 *);
 template <bool VIR, bool ENE, int MINB>
 __global__ void k_pair_ljzd_jm2(const int *, const int *, const SysDev *, const float4 *, const float4 *, const int *,
                                 const int *, const float4 *, const int2 *, const unsigned long long *, const float2 *,
                                 unsigned long long *, double *, long long);
 __global__ void k_cell_bbox(const int *, int, const float4 *, const unsigned char *, float4 *);
 // og_integrate.cu
-__global__ void k_excess(int, const int2 *, const int *, const SysDev *, const double *, const double *, const int *,
-                         unsigned long long *, double *, double *);
+__global__ void k_excess(int, const int2 *, const int *, const SysDev *, const EleDev *, const double *,
+                         const double *, const int *, unsigned long long *, double *, double *);
 __global__ void k_bonds(int, const int2 *, const double2 *, const int *, const SysDev *, const double *, const int *,
                         unsigned long long *, double *);
 __global__ void k_angles(int, const int4 *, const double2 *, const SysDev *, const double *, const int *,
@@ -145,6 +145,8 @@ struct HostSystem {
     std::vector<uint32_t> mt;     // generator at the system's first step ([OG_MT_WORDS])
     std::vector<int32_t> tr_group;  // trajectory group (local atom ids), og_set_trajectory
     int tr_interval = 0;
+    std::vector<double> hcut, hlam;  // HPS tables [n_lj_types^2]
+    EleDev ele{};                    // electrostatics / nonbond model
     int d_free = 0;
 };
 
@@ -304,6 +306,10 @@ struct og_engine {
     int n_tr = 0, n_tr_entries = 0;
     std::vector<int> tr_sys;      // system of each trajectory slot
     std::vector<TrLog> tr;        // per slot
+    // electrostatics / nonbond models (EleDev per system) and HPS tables (aligned with d_lj)
+    EleDev *d_ele = nullptr;
+    float2 *d_hps = nullptr;
+    bool any_gen = false;         // some system needs the generic pair-kernel path
 };
 
 namespace {
@@ -471,13 +477,131 @@ double self_energy(const HostSystem &h) {
         dw[j] += (double)(float)h.charge[i];
     }
     float mon = 0.0f;
-    const double zm = (double)h.dev.zcore;
+    const double zm = (double)(h.ele.generic ? h.ele.zmcore : h.dev.zcore);
+    const float piew = h.ele.generic ? h.ele.piewald : 0.0f;
     for (int i = 0; i < n; i++) {
         double q = (double)(float)h.charge[i];
-        double es = ((double)(-0.0f * (float)q * (float)q) - zm * q * (q + dw[i])) * 0.5 * OG_CHARGE_COEFF;
+        double es = ((double)(-piew * (float)q * (float)q) - zm * q * (q + dw[i])) * 0.5 * OG_CHARGE_COEFF;
         mon = (float)((double)mon + es);
     }
     return (double)mon;
+}
+
+// ZeroMultipoleSum's constructor and set_zms_params (ZeroMultipoleSum.cpp:6-28,108-202): the
+// float coefficients as the reference's float members hold them (float operands, double
+// literals), the same formulas in double for the FP64 excluded-pair term, and the self energy's
+// core constant of the order (cal_self_energy, ZeroMultipoleSum.cpp:71-77).
+void ele_setup(EleDev &E, const og_system_desc &d) {
+    E = EleDev{};
+    E.mode = d.ele_mode;
+    E.hps = d.hps != 0;
+    const float c = (float)d.cutoff, a = (float)d.ele_alpha;
+    E.alpha = a;
+    E.alpha0 = (double)a < 1e-10;
+    E.generic = !(E.mode == OG_ELE_ZD && E.alpha0 && !E.hps);
+    E.hps_eps = (float)d.hps_epsilon;
+    {
+        const float c2 = c * c, c3 = c2 * c, c4 = c2 * c2, c5 = c3 * c2, c6 = c3 * c3, c7 = c3 * c4;
+        const float tmp = c * a, erc = erfcf(tmp), expterm = expf(-tmp * tmp);
+        float f, hz, d1, d2, d3, d4;
+        if (E.alpha0) {
+            f = (float)(1.0 / c3);
+            hz = (float)(2.0 / c3);
+            d1 = (float)(1.0 / c2);
+            d2 = (float)(2.0 / c3);
+            d3 = (float)(6.0 / c4);
+            d4 = (float)(24.0 / c5);
+        } else {
+            const float root_pi = (float)sqrt(3.14159265);  // CelesteObject::PI
+            E.piewald = (float)(2.0 / root_pi * a);
+            f = erc / c3 + E.piewald * expterm / c2;
+            const float t3 = tmp * tmp * tmp, t5 = t3 * tmp * tmp, t7 = t5 * tmp * tmp;
+            hz = (float)((erc + expterm * (tmp + t3) * 2.0 / root_pi) * 2.0 / c3);
+            d1 = (float)((erc + expterm * tmp * 2.0 / root_pi) / c2);
+            d2 = (float)((erc + expterm * (tmp + t3) * 2.0 / root_pi) * 2.0 / c3);
+            d3 = (float)((erc + expterm * (tmp + 2.0 / 3.0 * t3 + 2.0 / 3.0 * t5) * 2.0 / root_pi) * 6.0 / c4);
+            d4 = (float)((erc + expterm * (tmp + 2.0 / 3.0 * t3 + 1.0 / 6.0 * t5 + 1.0 / 3.0 + t7) * 2.0 / root_pi) *
+                         24.0 / c5);
+        }
+        E.fcoeff = f;
+        E.bcoeff = (float)(0.5 * f);
+        E.zq2 = (float)(-3.0 / 4.0 * f - hz / 4.0);
+        E.zq4 = (float)(f / 8.0 / c2 + hz / 8.0 / c2);
+        E.zq22 = (float)(2.0 * E.zq2);
+        E.zq44 = (float)(4.0 * E.zq4);
+        E.zo2 = (float)(-15.0 / 16.0 * d1 / c - 7.0 / 16.0 * d2 - 1.0 / 16.0 * d3 * c);
+        E.zo4 = (float)(5.0 / 16.0 * d1 / c3 + 5.0 / 16.0 * d2 / c2 + 1.0 / 16.0 * d3 / c);
+        E.zo6 = (float)(-1.0 / 16.0 * d1 / c5 - 1.0 / 16.0 * d2 / c4 - 1.0 / 48.0 * d3 / c3);
+        E.zo22 = (float)(2.0 * E.zo2);
+        E.zo44 = (float)(4.0 * E.zo4);
+        E.zo66 = (float)(6.0 * E.zo6);
+        E.zh2 = (float)(-35.0 / 32.0 * d1 / c - 19.0 / 32.0 * d2 - 1.0 / 96.0 * d4 * c2 - 1.0 / 8.0 * d3 * c);
+        E.zh4 = (float)(1.0 / 64.0 * d4 + 35.0 / 64.0 * d1 / c3 + 35.0 / 64.0 * d2 / c2 + 5.0 / 32.0 * d3 / c);
+        E.zh6 = (float)(-7.0 / 32.0 * d1 / c5 - 7.0 / 32.0 * d2 / c4 - 1.0 / 12.0 * d3 / c3 - 1.0 / 96.0 * d4 / c2);
+        E.zh8 = (float)(5.0 / 128.0 * d2 / c6 + 5.0 / 128.0 * d1 / c7 + 1.0 / 64.0 * d3 / c5 + 1.0 / 384.0 * d4 / c4);
+        E.zh22 = (float)(2.0 * E.zh2);
+        E.zh44 = (float)(4.0 * E.zh4);
+        E.zh66 = (float)(6.0 * E.zh6);
+        E.zh88 = (float)(8.0 * E.zh8);
+        E.zcore = erc / c + E.bcoeff * c2;
+        E.zqcore = erc / c - E.zq2 * c2 - E.zq4 * c4;
+        E.zocore = erc / c - E.zo2 * c2 - E.zo4 * c4 - E.zo6 * c6;
+        E.zhcore = erc / c - E.zh2 * c2 - E.zh4 * c4 - E.zh6 * c6 - E.zh8 * c6 * c2;
+    }
+    E.zmcore = E.mode == OG_ELE_ZD ? E.zcore : E.mode == OG_ELE_ZQ ? E.zqcore : E.mode == OG_ELE_ZO ? E.zocore
+             : E.mode == OG_ELE_ZH ? E.zhcore : 0.0f;
+    if (E.mode == OG_ELE_DH) {
+        // CelesteObject.cpp:31-39 constants
+        E.dielectric_inv = (float)(1.0 / d.dh_dielectric);
+        E.debye_inv = (float)(1.0 / (sqrt(8.85418782e-12 * d.dh_dielectric * 1.380658e-23 * d.dh_temperature /
+                                          (2 * 6.0221413e23 * 1.60217657e-19 * 1.60217657e-19 * d.dh_ionic_strength)) *
+                                     1e10));
+    }
+    {  // double precision
+        const double c = d.cutoff, a = d.ele_alpha;
+        const double c2 = c * c, c3 = c2 * c, c4 = c2 * c2, c5 = c3 * c2, c6 = c3 * c3, c7 = c3 * c4;
+        const double tmp = c * a, erc = erfc(tmp), expterm = exp(-tmp * tmp);
+        double hz, d1, d2, d3, d4;
+        E.d_alpha = a;
+        if (E.alpha0) {
+            E.d_fcoeff = 1.0 / c3;
+            hz = 2.0 / c3;
+            d1 = 1.0 / c2;
+            d2 = 2.0 / c3;
+            d3 = 6.0 / c4;
+            d4 = 24.0 / c5;
+        } else {
+            const double root_pi = sqrt(3.14159265);
+            E.d_piewald = 2.0 / root_pi * a;
+            E.d_fcoeff = erc / c3 + E.d_piewald * expterm / c2;
+            const double t3 = tmp * tmp * tmp, t5 = t3 * tmp * tmp, t7 = t5 * tmp * tmp;
+            hz = (erc + expterm * (tmp + t3) * 2.0 / root_pi) * 2.0 / c3;
+            d1 = (erc + expterm * tmp * 2.0 / root_pi) / c2;
+            d2 = (erc + expterm * (tmp + t3) * 2.0 / root_pi) * 2.0 / c3;
+            d3 = (erc + expterm * (tmp + 2.0 / 3.0 * t3 + 2.0 / 3.0 * t5) * 2.0 / root_pi) * 6.0 / c4;
+            d4 = (erc + expterm * (tmp + 2.0 / 3.0 * t3 + 1.0 / 6.0 * t5 + 1.0 / 3.0 + t7) * 2.0 / root_pi) * 24.0 / c5;
+        }
+        const double f = E.d_fcoeff;
+        E.d_bcoeff = 0.5 * f;
+        E.d_zq2 = -3.0 / 4.0 * f - hz / 4.0;
+        E.d_zq4 = f / 8.0 / c2 + hz / 8.0 / c2;
+        E.d_zq22 = 2.0 * E.d_zq2;
+        E.d_zq44 = 4.0 * E.d_zq4;
+        E.d_zo2 = -15.0 / 16.0 * d1 / c - 7.0 / 16.0 * d2 - 1.0 / 16.0 * d3 * c;
+        E.d_zo4 = 5.0 / 16.0 * d1 / c3 + 5.0 / 16.0 * d2 / c2 + 1.0 / 16.0 * d3 / c;
+        E.d_zo6 = -1.0 / 16.0 * d1 / c5 - 1.0 / 16.0 * d2 / c4 - 1.0 / 48.0 * d3 / c3;
+        E.d_zo22 = 2.0 * E.d_zo2;
+        E.d_zo44 = 4.0 * E.d_zo4;
+        E.d_zo66 = 6.0 * E.d_zo6;
+        E.d_zh2 = -35.0 / 32.0 * d1 / c - 19.0 / 32.0 * d2 - 1.0 / 96.0 * d4 * c2 - 1.0 / 8.0 * d3 * c;
+        E.d_zh4 = 1.0 / 64.0 * d4 + 35.0 / 64.0 * d1 / c3 + 35.0 / 64.0 * d2 / c2 + 5.0 / 32.0 * d3 / c;
+        E.d_zh6 = -7.0 / 32.0 * d1 / c5 - 7.0 / 32.0 * d2 / c4 - 1.0 / 12.0 * d3 / c3 - 1.0 / 96.0 * d4 / c2;
+        E.d_zh8 = 5.0 / 128.0 * d2 / c6 + 5.0 / 128.0 * d1 / c7 + 1.0 / 64.0 * d3 / c5 + 1.0 / 384.0 * d4 / c4;
+        E.d_zh22 = 2.0 * E.d_zh2;
+        E.d_zh44 = 4.0 * E.d_zh4;
+        E.d_zh66 = 6.0 * E.d_zh6;
+        E.d_zh88 = 8.0 * E.d_zh8;
+    }
 }
 
 // MmSystem::set_nb15off + set_excess_pairs (MmSystem.cpp:478-525, 700-736): rows in insertion
@@ -611,6 +735,7 @@ og_status build_list(og_engine *e) {
 #define PAIR_ARGS                                                                                            \
     e->d_counters, e->d_cell_sys, e->d_sys, e->d_bbox, e->d_xq, e->d_slot_type, e->d_cp_head, e->d_cp_shift, \
         e->d_cp_c2img, e->d_cp_mask, e->d_lj, e->d_frc, e->d_cell_acc, e->pair_cap
+#define JQ_ARGS PAIR_ARGS, e->d_ele, e->d_hps
 
 // Pair kernel variants differ in the register budget per thread (resident blocks per SM).
 // ene = false: the caller does not read this step's energies (only variants 5-6 skip them).
@@ -621,7 +746,15 @@ og_status launch_pair(og_engine *e, bool vir, int variant, bool ene) {
     // 5-6: j-major with packed FP32x2 arithmetic (128/80); 7-9: the same with a j-atom queue
     // (128/80 in blocks of 256, 102 in blocks of 128).  The virial kernel is that of the
     // variant's family.
-    if (vir && variant >= 7) k_pair_ljzd_jq<true, true, 2, 256><<<nb, 256, 0, st>>>(PAIR_ARGS);
+    // a system with another electrostatics / nonbond model: the generic j-queue kernel for all
+    if (e->any_gen) {
+        if (vir) k_pair_ljzd_jq<true, true, 2, 256, true><<<nb, 256, 0, st>>>(JQ_ARGS);
+        else if (ene) k_pair_ljzd_jq<false, true, 5, 128, true><<<2 * nb, 128, 0, st>>>(JQ_ARGS);
+        else k_pair_ljzd_jq<false, false, 5, 128, true><<<2 * nb, 128, 0, st>>>(JQ_ARGS);
+        LAUNCH_CHECK();
+        return OG_OK;
+    }
+    if (vir && variant >= 7) k_pair_ljzd_jq<true, true, 2, 256, false><<<nb, 256, 0, st>>>(JQ_ARGS);
     else if (vir && variant >= 5) k_pair_ljzd_jm2<true, true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (vir && variant >= 3) k_pair_ljzd_jm<true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (vir) k_pair_ljzd<true, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
@@ -633,12 +766,12 @@ og_status launch_pair(og_engine *e, bool vir, int variant, bool ene) {
     else if (variant == 5) k_pair_ljzd_jm2<false, false, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (variant == 6 && ene) k_pair_ljzd_jm2<false, true, 3><<<nb, 256, 0, st>>>(PAIR_ARGS);
     else if (variant == 6) k_pair_ljzd_jm2<false, false, 3><<<nb, 256, 0, st>>>(PAIR_ARGS);
-    else if (variant == 7 && ene) k_pair_ljzd_jq<false, true, 2, 256><<<nb, 256, 0, st>>>(PAIR_ARGS);
-    else if (variant == 7) k_pair_ljzd_jq<false, false, 2, 256><<<nb, 256, 0, st>>>(PAIR_ARGS);
-    else if (variant == 8 && ene) k_pair_ljzd_jq<false, true, 3, 256><<<nb, 256, 0, st>>>(PAIR_ARGS);
-    else if (variant == 8) k_pair_ljzd_jq<false, false, 3, 256><<<nb, 256, 0, st>>>(PAIR_ARGS);
-    else if (variant == 9 && ene) k_pair_ljzd_jq<false, true, 5, 128><<<2 * nb, 128, 0, st>>>(PAIR_ARGS);
-    else if (variant == 9) k_pair_ljzd_jq<false, false, 5, 128><<<2 * nb, 128, 0, st>>>(PAIR_ARGS);
+    else if (variant == 7 && ene) k_pair_ljzd_jq<false, true, 2, 256, false><<<nb, 256, 0, st>>>(JQ_ARGS);
+    else if (variant == 7) k_pair_ljzd_jq<false, false, 2, 256, false><<<nb, 256, 0, st>>>(JQ_ARGS);
+    else if (variant == 8 && ene) k_pair_ljzd_jq<false, true, 3, 256, false><<<nb, 256, 0, st>>>(JQ_ARGS);
+    else if (variant == 8) k_pair_ljzd_jq<false, false, 3, 256, false><<<nb, 256, 0, st>>>(JQ_ARGS);
+    else if (variant == 9 && ene) k_pair_ljzd_jq<false, true, 5, 128, false><<<2 * nb, 128, 0, st>>>(JQ_ARGS);
+    else if (variant == 9) k_pair_ljzd_jq<false, false, 5, 128, false><<<2 * nb, 128, 0, st>>>(JQ_ARGS);
     else k_pair_ljzd<false, 2><<<nb, 256, 0, st>>>(PAIR_ARGS);
     LAUNCH_CHECK();
     return OG_OK;
@@ -682,7 +815,7 @@ og_status compute_forces(og_engine *e, bool vir, bool ene = true) {
     }
     if (e->n_excess) {
         k_excess<<<blocks(e->n_excess, 256), 256, 0, st>>>(e->n_excess, e->d_excess, e->d_excess_sys, e->d_sys,
-                                                            e->d_crd, e->d_charge, e->d_atom_slot, e->d_frc,
+                                                            e->d_ele, e->d_crd, e->d_charge, e->d_atom_slot, e->d_frc,
                                                             e->d_e_exc, vir ? e->d_vir_exc : nullptr);
         LAUNCH_CHECK();
     }
@@ -1196,6 +1329,10 @@ og_status build_list_checked(og_engine *e) {
 // the fastest; OG_PAIR_VARIANT=0/1/2 in the environment fixes the choice.  The trial launches
 // write the force accumulators, which are cleared afterwards.
 og_status autotune_pair(og_engine *e) {
+    if (e->any_gen) {  // one kernel serves the other models
+        e->pair_variant = 9;
+        return OG_OK;
+    }
     if (e->fixed_variant >= 0) {
         e->pair_variant = e->fixed_variant;
         return OG_OK;
@@ -1306,6 +1443,12 @@ og_status og_add_system(og_engine *e, const og_system_desc *d, int32_t *sys_id) 
             return fail(e, OG_ERR_INVALID, "virtual state %d: polynomial order outside 0..7", v);
     if (d->n_vstates > 0 && d->vmcmd_mt_state && d->vmcmd_mt_state[624] > 624)
         return fail(e, OG_ERR_INVALID, "V-McMD generator position above 624");
+    if (d->ele_mode < OG_ELE_ZD || d->ele_mode > OG_ELE_DH || !(d->ele_alpha >= 0.0) ||
+        (d->ele_mode == OG_ELE_DH &&
+         !(d->dh_dielectric > 0.0 && d->dh_ionic_strength > 0.0 && d->dh_temperature > 0.0)) ||
+        (d->hps && (!d->lj_hps_cutoff || !d->lj_hps_lambda)))
+        return fail(e, OG_ERR_INVALID, "electrostatics model: mode 0..4, alpha >= 0, positive Debye-Hueckel "
+                    "parameters, HPS tables when hps is on");
     if (d->first_step < 0 || d->first_step % d->nsgrid_update_intvl != 0)
         return fail(e, OG_ERR_INVALID, "first_step must be a non-negative multiple of nsgrid_update_intvl");
     e->sys.emplace_back();
@@ -1335,6 +1478,11 @@ og_status og_add_system(og_engine *e, const og_system_desc *d, int32_t *sys_id) 
     cp(h.gstart, d->com_group_start, d->n_com_groups > 0 ? d->n_com_groups + 1 : 0);
     if (d->n_com_groups > 0) cp(h.gatoms, d->com_group_atoms, d->com_group_start[d->n_com_groups]);
     if (d->mcmd_order >= 0) cp(h.mcoef, d->mcmd_coef, d->mcmd_order + 1);
+    if (d->hps) {
+        cp(h.hcut, d->lj_hps_cutoff, (size_t)d->n_lj_types * d->n_lj_types);
+        cp(h.hlam, d->lj_hps_lambda, (size_t)d->n_lj_types * d->n_lj_types);
+    }
+    ele_setup(h.ele, *d);
     if (d->n_vstates > 0) {
         // ExtendedVMcMD::set_vs_params / set_vs_poly_param (Extend.cpp:266-283)
         int c0 = 0;
@@ -1454,7 +1602,8 @@ og_status og_finalize(og_engine *e) {
     std::vector<int> atom_sys, col_sys, sys_col_base(S + 1), atom_type, atom_group, excl_start(1, 0), excl_list;
     std::vector<double> crd, vel, charge;
     std::vector<float> charge_f, mass, mass_inv;
-    std::vector<float2> lj;
+    std::vector<float2> lj, hps_tab;
+    std::vector<EleDev> ele_tab;
     std::vector<int2> excess, bondv, spair;
     std::vector<int> excess_sys, bond_sys, spair_sys, grp_start(1, 0), grp_atoms, grp_sys;
     std::vector<double2> bond_kr, angle_kt;
@@ -1666,6 +1815,13 @@ og_status og_finalize(og_engine *e) {
         for (int i = 0; i < d.n_lj_types; i++)
             for (int j = 0; j < d.n_lj_types; j++)
                 lj.push_back(make_float2((float)h.lj6[i * d.n_lj_types + j], (float)h.lj12[i * d.n_lj_types + j]));
+        for (int i = 0; i < d.n_lj_types; i++)
+            for (int j = 0; j < d.n_lj_types; j++)
+                hps_tab.push_back(h.ele.hps ? make_float2((float)h.hcut[i * d.n_lj_types + j],
+                                                          (float)h.hlam[i * d.n_lj_types + j])
+                                            : make_float2(0.f, 1.f));
+        ele_tab.push_back(h.ele);
+        e->any_gen |= h.ele.generic != 0;
         for (int c = 0; c < D.n_columns; c++) col_sys.push_back(k);
         sys_col_base[k] = col_base;
         cells_cap += n / OG_CELL + D.n_columns + 1;
@@ -1739,6 +1895,7 @@ og_status og_finalize(og_engine *e) {
         (s = upload(e, &e->d_grp_start, grp_start)) || (s = upload(e, &e->d_grp_atoms, grp_atoms)) ||
         (s = upload(e, &e->d_grp_sys, grp_sys)) || (s = upload(e, &e->d_grp_mass_inv, grp_mass_inv)) ||
         (s = dalloc(e, &e->d_moment, 3 * (size_t)(e->n_groups + 1))) || (s = upload(e, &e->d_lj, lj)) ||
+        (s = upload(e, &e->d_hps, hps_tab)) || (s = upload(e, &e->d_ele, ele_tab)) ||
         (s = dalloc(e, &e->d_sys_acc, OG_ACC_SIZE * (size_t)S)) || (s = dalloc(e, &e->d_mcmd, S)) ||
         (s = dalloc(e, &e->d_energies, OG_N_ENERGY * (size_t)S)) || (s = upload(e, &e->d_thermo, thermo)) ||
         (s = dalloc(e, &e->d_sum_tmp, S)) || (s = upload(e, &e->d_mask_plain, mask_plain)) ||

@@ -28,22 +28,75 @@ __device__ __forceinline__ void add_fix(unsigned long long *f, double wx, double
 
 // Excluded-pair ("excess") zero-dipole term, E = cc bcoeff r^2, dE/dx = cc fcoeff d
 // (ForceField.cpp:420-437, ZeroMultipoleSum.cpp:191-202, SubBox.cpp:1347-1367), in FP64.
+// The excluded-pair term of models other than zero-dipole alpha = 0 in FP64
+// (ZeroMultipoleSum.cpp:204-307; Debye-Hueckel has none, calc_null), with the reference's forms:
+// the zero-dipole alpha > 0 energy takes -erf(alpha r) r, the octupole energies r^4 r, the
+// hexadecapole alpha = 0 gradient zh66 r^2 and -1/r^3, the hexadecapole alpha > 0 energy stops at r^4.
+__device__ void og_ele_excess(const EleDev &E, double r, double r2, double cc, double &e, double &g) {
+    e = g = 0.0;
+    if (E.mode == OG_ELE_DH) return;
+    const double ri = 1.0 / r, r2i = ri * ri, r3i = r2i * ri, r4 = r2 * r2, r6 = r4 * r2, r8 = r4 * r4;
+    double erc = 1.0, erfn = 0.0, ex = 0.0;
+    if (!E.alpha0) {
+        const double t = E.d_alpha * r;
+        erc = erfc(t);
+        erfn = 1.0 - erc;
+        ex = E.d_piewald * exp(-t * t) * r2i;
+    }
+    switch (E.mode) {
+        case OG_ELE_ZD:
+            if (E.alpha0) {
+                e = cc * E.d_bcoeff * r2;
+                g = cc * E.d_fcoeff;
+            } else {
+                e = cc * (-erfn * r + E.d_bcoeff * r2);
+                g = -cc * (erc * r3i + ex - E.d_fcoeff - r3i);
+            }
+            break;
+        case OG_ELE_ZQ:
+            e = cc * (-erfn * ri - E.d_zq2 * r2 - E.d_zq4 * r4);
+            g = -cc * (E.alpha0 ? (E.d_zq22 + E.d_zq44 * r2) : (erc * r3i + ex + E.d_zq22 + E.d_zq44 * r2 - r3i));
+            break;
+        case OG_ELE_ZO:
+            e = cc * (-erfn * ri - E.d_zo2 * r2 - E.d_zo4 * r4 - E.d_zo6 * r4 * r);
+            g = -cc * (E.alpha0 ? (E.d_zo22 + E.d_zo44 * r2 + E.d_zo66 * r4)
+                                : (erc * r3i + ex + E.d_zo22 + E.d_zo44 * r2 + E.d_zo66 * r4 - r3i));
+            break;
+        default:
+            if (E.alpha0) {
+                e = cc * (-E.d_zh2 * r2 - E.d_zh4 * r4 - E.d_zh6 * r6 - E.d_zh8 * r8);
+                g = -cc * (E.d_zh22 + E.d_zh44 * r2 + E.d_zh66 * r2 + E.d_zh88 * r6 - r3i);
+            } else {
+                e = cc * (-erfn * ri - E.d_zh2 * r2 - E.d_zh4 * r4);
+                g = -cc * (erc * r3i + ex + E.d_zh22 + E.d_zh44 * r2 + E.d_zh66 * r4 + E.d_zh88 * r6 - r3i);
+            }
+    }
+}
+
 __global__ void k_excess(int n_pairs, const int2 *__restrict__ pairs, const int *__restrict__ pair_sys,
-                         const SysDev *__restrict__ sys, const double *__restrict__ crd,
-                         const double *__restrict__ charge, const int *__restrict__ atom_slot,
-                         unsigned long long *__restrict__ frc, double *__restrict__ e_out,
-                         double *__restrict__ vir_out) {
+                         const SysDev *__restrict__ sys, const EleDev *__restrict__ ele,
+                         const double *__restrict__ crd, const double *__restrict__ charge,
+                         const int *__restrict__ atom_slot, unsigned long long *__restrict__ frc,
+                         double *__restrict__ e_out, double *__restrict__ vir_out) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n_pairs) return;
-    const SysDev &S = sys[pair_sys[k]];
+    const int s = pair_sys[k];
+    const SysDev &S = sys[s];
     const int i = pairs[k].x, j = pairs[k].y;
     double d[3];
     for (int q = 0; q < 3; q++) d[q] = minim(crd[3 * i + q] - crd[3 * j + q], S.Lf[q], S.L_half_inv_f[q]);
     const double cc = charge[i] * charge[j] * OG_CHARGE_COEFF;
-    const double fco = 1.0 / (S.cutoff * S.cutoff * S.cutoff);
     const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
-    e_out[k] = cc * 0.5 * fco * r2;
-    const double gc = cc * fco;
+    double gc;
+    if (!ele[s].generic) {
+        const double fco = 1.0 / (S.cutoff * S.cutoff * S.cutoff);
+        e_out[k] = cc * 0.5 * fco * r2;
+        gc = cc * fco;
+    } else {
+        double e;
+        og_ele_excess(ele[s], sqrt(r2), r2, cc, e, gc);
+        e_out[k] = e;
+    }
     add_fix(frc + 3 * (size_t)atom_slot[i], gc * d[0], gc * d[1], gc * d[2]);
     add_fix(frc + 3 * (size_t)atom_slot[j], -gc * d[0], -gc * d[1], -gc * d[2]);
     if (vir_out)

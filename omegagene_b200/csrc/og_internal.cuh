@@ -93,6 +93,20 @@ struct VsDev {
     int order;
 };
 
+// Electrostatics / nonbond model of a system other than zero-dipole alpha = 0 with plain LJ
+// (ZeroMultipoleSum.cpp:108-466, ForceField.cpp:333-418).  FP32 coefficients for the pair
+// kernel, as the reference's float members hold them; FP64 ones for the excluded-pair term.
+struct EleDev {
+    int mode, alpha0, hps, generic;
+    float alpha, piewald, bcoeff, fcoeff, zcore, zqcore, zocore, zhcore;
+    float zq2, zq4, zq22, zq44, zo2, zo4, zo6, zo22, zo44, zo66;
+    float zh2, zh4, zh6, zh8, zh22, zh44, zh66, zh88;
+    float dielectric_inv, debye_inv, hps_eps, zmcore;
+    double d_alpha, d_piewald, d_bcoeff, d_fcoeff;
+    double d_zq2, d_zq4, d_zq22, d_zq44, d_zo2, d_zo4, d_zo6, d_zo22, d_zo44, d_zo66;
+    double d_zh2, d_zh4, d_zh6, d_zh8, d_zh22, d_zh44, d_zh66, d_zh88;
+};
+
 // per-system reduction slots in d_sys_acc (double)
 #define OG_ACC_VDW 0
 #define OG_ACC_ELE 1

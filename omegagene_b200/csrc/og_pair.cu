@@ -653,13 +653,56 @@ k_pair_ljzd_jm2(const int *__restrict__ counters, const int *__restrict__ cell_s
 // and evaluates it against the 8 i atoms.  On water about 40% of the j atoms of a surviving cell
 // pair drop out, and every evaluation round runs with all 32 lanes busy.
 #define OG_JQ 64
-template <bool VIR, bool ENE, int MINB, int NT = 256>
+
+// The electrostatics of one pair for models other than zero-dipole alpha = 0
+// (ZeroMultipoleSum.cpp:309-455 and calc_debye_huckel): energy e and gradient coefficient g
+// (work = g d), in FP32 with CUDA's erfcf / expf where alpha > 0.  The octupole alpha > 0
+// gradient takes the hexadecapole coefficients, as the reference's does.
+__device__ __forceinline__ void og_ele_pair(const EleDev &E, float r, float r2, float ri, float r2i, float r3i,
+                                            float cc, float &e, float &g) {
+    if (E.mode == OG_ELE_DH) {
+        const float ld = expf(-r * E.debye_inv);
+        e = cc * ri * E.dielectric_inv * ld;
+        g = -e * (ri + E.debye_inv);
+        return;
+    }
+    float erc = 1.f, ex = 0.f;
+    if (!E.alpha0) {
+        const float t = r * E.alpha;
+        erc = erfcf(t);
+        ex = E.piewald * expf(-t * t) * r2i;
+    }
+    const float r4 = r2 * r2, r6 = r4 * r2, r8 = r4 * r4;
+    switch (E.mode) {
+        case OG_ELE_ZD:
+            e = cc * (ri * erc - E.zcore + E.bcoeff * r2);
+            g = -cc * (erc * r3i + ex - E.fcoeff);
+            break;
+        case OG_ELE_ZQ:
+            e = cc * (ri * erc - E.zqcore - E.zq2 * r2 - E.zq4 * r4);
+            g = -cc * (r3i * erc + ex + E.zq22 + E.zq44 * r2);
+            break;
+        case OG_ELE_ZO:
+            e = cc * (ri * erc - E.zocore - E.zo2 * r2 - E.zo4 * r4 - E.zo6 * r6);
+            g = E.alpha0 ? -cc * (r3i + E.zo22 + E.zo44 * r2 + E.zo66 * r4)
+                         : -cc * (r3i * erc + ex + E.zh22 + E.zh44 * r2 + E.zh66 * r4);
+            break;
+        default:
+            e = cc * (ri * erc - E.zhcore - E.zh2 * r2 - E.zh4 * r4 - E.zh6 * r6 - E.zh8 * r8);
+            g = -cc * (r3i * erc + ex + E.zh22 + E.zh44 * r2 + E.zh66 * r4 + E.zh88 * r6);
+    }
+}
+
+// GEN: the system's EleDev model and HPS table (ele, hps) instead of the packed zero-dipole
+// alpha = 0 evaluation; both halves of a packed pair are evaluated one after the other.
+template <bool VIR, bool ENE, int MINB, int NT = 256, bool GEN = false>
 __global__ void __launch_bounds__(NT, MINB)
 k_pair_ljzd_jq(const int *__restrict__ counters, const int *__restrict__ cell_sys, const SysDev *__restrict__ sys,
                const float4 *__restrict__ bbox, const float4 *__restrict__ xq, const int *__restrict__ slot_type,
                const int *__restrict__ cp_head, const float4 *__restrict__ cp_shift, const int2 *__restrict__ cp_c2img,
                const unsigned long long *__restrict__ cp_mask, const float2 *__restrict__ lj,
-               unsigned long long *__restrict__ frc, double *__restrict__ cell_acc, long long pair_cap) {
+               unsigned long long *__restrict__ frc, double *__restrict__ cell_acc, long long pair_cap,
+               const EleDev *__restrict__ ele, const float2 *__restrict__ hps) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -668,6 +711,7 @@ k_pair_ljzd_jq(const int *__restrict__ counters, const int *__restrict__ cell_sy
     const int c1 = warp;
     const int jj = lane & 7, q = lane >> 3;
     const SysDev &S = sys[cell_sys[c1]];
+    const EleDev &E = ele[GEN ? cell_sys[c1] : 0];
     __shared__ float4 s_ab[NT / 32][OG_CELL / 2][2];
     __shared__ int2 s_t2[NT / 32][OG_CELL / 2];
     __shared__ float4 s_qx[NT / 32][OG_JQ];  // queued j: (x, y, z) in cell1's frame, charge
@@ -736,15 +780,46 @@ k_pair_ljzd_jq(const int *__restrict__ counters, const int *__restrict__ cell_sy
             const float2 t6 = __fmul2_rn(og_f2(pa.x, pb.x), r6);
             const float2 t12 = __fmul2_rn(__fmul2_rn(og_f2(pa.y, pb.y), r6), r6);
             const float2 cc = __fmul2_rn(og_f2(B.z, B.w), qj);
-            float2 wc = __ffma2_rn(__fmul2_rn(cc, mone), __ffma2_rn(y, r2inv, nfco),
-                                   __fmul2_rn(r2inv, __ffma2_rn(t12, m12, __fmul2_rn(six, t6))));
             const float2 on = og_f2(act_a ? 1.f : 0.f, act_b ? 1.f : 0.f);
-            wc = __fmul2_rn(wc, on);
-            if (ENE) {
-                const float2 pv = __fmul2_rn(__ffma2_rn(t6, mone, t12), on);
-                const float2 pe = __fmul2_rn(__fmul2_rn(cc, __ffma2_rn(bco, r2s, __fadd2_rn(y, nzcore))), on);
-                av = __fadd2_rn(av, pv);
-                ae = __fadd2_rn(ae, pe);
+            float2 wc;
+            if (!GEN) {
+                wc = __ffma2_rn(__fmul2_rn(cc, mone), __ffma2_rn(y, r2inv, nfco),
+                                __fmul2_rn(r2inv, __ffma2_rn(t12, m12, __fmul2_rn(six, t6))));
+                wc = __fmul2_rn(wc, on);
+                if (ENE) {
+                    const float2 pv = __fmul2_rn(__ffma2_rn(t6, mone, t12), on);
+                    const float2 pe = __fmul2_rn(__fmul2_rn(cc, __ffma2_rn(bco, r2s, __fadd2_rn(y, nzcore))), on);
+                    av = __fadd2_rn(av, pv);
+                    ae = __fadd2_rn(ae, pe);
+                }
+            } else {
+                float w2[2], v2[2], e2[2];
+#pragma unroll
+                for (int hh = 0; hh < 2; hh++) {
+                    const float r2h = hh ? r2s.y : r2s.x, yh = hh ? y.y : y.x;
+                    const float r2i = yh * yh, r3i = yh * r2i, rr = r2h * yh;
+                    const float t6h = hh ? t6.y : t6.x, t12h = hh ? t12.y : t12.x;
+                    float ev = t12h - t6h, wl = r2i * (6.f * t6h - 12.f * t12h);
+                    if (E.hps) {  // ForceField.cpp:380-391
+                        const float2 hp = __ldg(&hps[(hh ? T.y : T.x) + tj]);
+                        if (rr > hp.x) {
+                            ev *= hp.y;
+                            wl *= hp.y;
+                        } else {
+                            ev += (1.f - hp.y) * E.hps_eps;
+                        }
+                    }
+                    float ee, ge;
+                    og_ele_pair(E, rr, r2h, yh, r2i, r3i, hh ? cc.y : cc.x, ee, ge);
+                    w2[hh] = wl + ge;
+                    v2[hh] = ev;
+                    e2[hh] = ee;
+                }
+                wc = __fmul2_rn(og_f2(w2[0], w2[1]), on);
+                if (ENE) {
+                    av = __fadd2_rn(av, __fmul2_rn(og_f2(v2[0], v2[1]), on));
+                    ae = __fadd2_rn(ae, __fmul2_rn(og_f2(e2[0], e2[1]), on));
+                }
             }
             if (VIR) n_act += (act_a ? 1 : 0) + (act_b ? 1 : 0);
             const float2 wx = __fmul2_rn(wc, dx), wy = __fmul2_rn(wc, dy), wz = __fmul2_rn(wc, dz);
@@ -918,13 +993,17 @@ template __global__ void k_pair_ljzd_jm2<false, true, 2>(OG_PAIR_ARGS_DECL);
 template __global__ void k_pair_ljzd_jm2<false, true, 3>(OG_PAIR_ARGS_DECL);
 template __global__ void k_pair_ljzd_jm2<false, false, 2>(OG_PAIR_ARGS_DECL);
 template __global__ void k_pair_ljzd_jm2<false, false, 3>(OG_PAIR_ARGS_DECL);
-template __global__ void k_pair_ljzd_jq<true, true, 2>(OG_PAIR_ARGS_DECL);
-template __global__ void k_pair_ljzd_jq<false, true, 2>(OG_PAIR_ARGS_DECL);
-template __global__ void k_pair_ljzd_jq<false, true, 3>(OG_PAIR_ARGS_DECL);
-template __global__ void k_pair_ljzd_jq<false, false, 2>(OG_PAIR_ARGS_DECL);
-template __global__ void k_pair_ljzd_jq<false, false, 3>(OG_PAIR_ARGS_DECL);
-template __global__ void k_pair_ljzd_jq<false, true, 5, 128>(OG_PAIR_ARGS_DECL);
-template __global__ void k_pair_ljzd_jq<false, false, 5, 128>(OG_PAIR_ARGS_DECL);
+#define OG_JQ_ARGS_DECL OG_PAIR_ARGS_DECL, const EleDev *, const float2 *
+template __global__ void k_pair_ljzd_jq<true, true, 2, 256, false>(OG_JQ_ARGS_DECL);
+template __global__ void k_pair_ljzd_jq<false, true, 2, 256, false>(OG_JQ_ARGS_DECL);
+template __global__ void k_pair_ljzd_jq<false, true, 3, 256, false>(OG_JQ_ARGS_DECL);
+template __global__ void k_pair_ljzd_jq<false, false, 2, 256, false>(OG_JQ_ARGS_DECL);
+template __global__ void k_pair_ljzd_jq<false, false, 3, 256, false>(OG_JQ_ARGS_DECL);
+template __global__ void k_pair_ljzd_jq<false, true, 5, 128, false>(OG_JQ_ARGS_DECL);
+template __global__ void k_pair_ljzd_jq<false, false, 5, 128, false>(OG_JQ_ARGS_DECL);
+template __global__ void k_pair_ljzd_jq<true, true, 2, 256, true>(OG_JQ_ARGS_DECL);
+template __global__ void k_pair_ljzd_jq<false, true, 5, 128, true>(OG_JQ_ARGS_DECL);
+template __global__ void k_pair_ljzd_jq<false, false, 5, 128, true>(OG_JQ_ARGS_DECL);
 
 template __global__ void k_pair_ljzd<true, 2>(const int *, const int *, const SysDev *, const float4 *,
                                                 const float4 *, const int *, const int *, const float4 *,

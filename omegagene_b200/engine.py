@@ -66,6 +66,9 @@ class SystemDesc(C.Structure):
         ("vmcmd_lambda_log_interval", C.c_int32), ("vmcmd_seed", C.c_uint32),
         ("vs_order", _p(C.c_int32)), ("vs_lambda", _p(C.c_double)), ("vs_prob", _p(C.c_double)),
         ("vs_coef", _p(C.c_double)), ("vmcmd_mt_state", _p(C.c_uint32)),
+        ("ele_mode", C.c_int32), ("ele_alpha", C.c_double), ("dh_dielectric", C.c_double),
+        ("dh_ionic_strength", C.c_double), ("dh_temperature", C.c_double), ("hps", C.c_int32),
+        ("hps_epsilon", C.c_double), ("lj_hps_cutoff", _p(C.c_double)), ("lj_hps_lambda", _p(C.c_double)),
     ]
 
 OG_MT_WORDS = 625
@@ -346,6 +349,16 @@ def make_desc(system, params=None, mcmd=None, first_step=0):
         d.nb14_coeff_vdw, d.nb14_coeff_ele = _ptr(keep.n14[2], C.c_double), _ptr(keep.n14[3], C.c_double)
     d.dof_extra = int(system.get("dof_extra", 0))
     d.first_step = int(first_step)
+    # electrostatics / nonbond model (ForceField.cpp:30-100)
+    d.ele_mode = ELECTROSTATIC[prm.get("electrostatic", "zero-dipole")]
+    d.ele_alpha = float(prm.get("ele_alpha", 0.0))
+    d.dh_dielectric, d.dh_ionic_strength = float(prm.get("dh_dielectric", 0.0)), float(prm.get("dh_ionic_strength", 0.0))
+    d.dh_temperature = float(prm.get("dh_temperature", 0.0))
+    if prm.get("nonbond", "lennard-jones") == "hydrophobicity-scale-lj":
+        cut, lam = cls_io.hps_tables(t)
+        keep.hcut, keep.hlam = np.ascontiguousarray(cut.reshape(-1)), np.ascontiguousarray(lam.reshape(-1))
+        d.hps, d.hps_epsilon = 1, float(prm.get("hps_epsilon", 0.0))
+        d.lj_hps_cutoff, d.lj_hps_lambda = _ptr(keep.hcut, C.c_double), _ptr(keep.hlam, C.c_double)
     d.mcmd_order = -1
     if mcmd is not None and "states" in mcmd:
         _vmcmd_desc(d, keep, mcmd, prm)

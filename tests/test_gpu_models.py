@@ -1,0 +1,102 @@
+"""The other electrostatics / nonbond models on the engine (the generic j-queue kernel and the
+model-aware excluded-pair kernel), for each of the reference's ala3 runs in
+tests/golden/ala3_models.json: zero-quadrupole / -octupole / -hexadecapole at alpha 0, the four
+orders at alpha 0.1, Debye-Hueckel, HPS.
+
+* Forces at the start against the FP64 oracle (the same model evaluated in FP64 over the cell
+  list): RMS relative error <= 1e-5, through both the virial kernel (og_compute_forces) and the
+  step kernel (the work of the first step); VDW and Ele within 1e-6 |E| + 2e-3 kcal/mol.
+* Steps 0-2 against the energies the reference printed: within 1e-5 |E| + 1e-3 kcal/mol.  The
+  Debye-Hueckel energy is not shifted to zero at the cutoff, so a pair crossing 12 A steps the
+  energy by ~0.1 kcal/mol; trajectories ~1e-7 A apart can cross on different steps, so from step 2
+  on its Ele is held to 0.5 kcal/mol (the forces and the other terms keep the tight bound).
+* A batch of a zero-dipole system and a zero-octupole one: each matches its own model.
+"""
+import importlib.util
+import json
+import os
+
+import numpy as np
+import pytest
+
+from omegagene_b200 import engine
+from oracle import ogo
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = os.path.join(HERE, "golden")
+MODELS = json.load(open(os.path.join(GOLD, "ala3_models.json")))["models"]
+
+
+def _load(name):
+    spec = importlib.util.spec_from_file_location(name, os.path.join(GOLD, name + ".py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _system(name):
+    s = _load("make_ala3_golden").load_system()
+    return _load("make_ele_golden").with_hps_lambdas(s) if name == "hps" else s
+
+
+def _rms(a, b):
+    return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
+
+
+@pytest.mark.parametrize("name", sorted(MODELS))
+def test_model_forces_match_fp64_oracle(name):
+    s, p = _system(name), MODELS[name]["params"]
+    md = ogo.OracleMD(s, p)
+    ref = md.forces()
+    w64 = md.work.reshape(-1, 3)
+    eng = engine.Engine(0)
+    eng.add_system(s, p)
+    eng.finalize()
+    eng.compute_forces()
+    work, ene, _ = eng.get_forces(0)
+    assert _rms(work, w64) <= 1e-5, (name, _rms(work, w64))
+    for k in ("vdw", "ele"):
+        assert abs(ene[k] - ref[k]) <= 1e-6 * abs(ref[k]) + 2e-3, (name, k, ene[k], ref[k])
+    eng.step(1)  # the step kernel's work at the starting positions
+    work1, _, _ = eng.get_forces(0)
+    assert _rms(work1, w64) <= 1e-5, (name, _rms(work1, w64))
+    eng.close()
+
+
+@pytest.mark.parametrize("name", sorted(MODELS))
+def test_model_tracks_reference_log(name):
+    s, mdl = _system(name), MODELS[name]
+    eng = engine.Engine(0)
+    eng.add_system(s, mdl["params"])
+    eng.finalize()
+    eng.set_trace(3)
+    eng.step(3)
+    tr = eng.get_trace(3)
+    for k, row in enumerate(mdl["steps"]):
+        got = dict(zip(engine.ENERGY_NAMES, tr[k, 0]))
+        for key in ("vdw", "ele", "potential", "kinetic", "total"):
+            tol = 1e-5 * abs(row[key]) + 1e-3
+            if name == "dh" and k >= 2 and key in ("ele", "potential", "total"):
+                tol = 0.5
+            assert abs(got[key] - row[key]) <= tol, (name, k, key, got[key], row[key])
+    eng.close()
+
+
+def test_mixed_models_in_one_batch():
+    base = _load("make_ala3_golden").load_system()
+    p_zd = dict(MODELS["zq_a0"]["params"], electrostatic="zero-dipole")
+    p_zo = MODELS["zo_a01"]["params"]
+    eng = engine.Engine(0)
+    eng.add_system(base, p_zd)
+    eng.add_system(base, p_zo)
+    eng.finalize()
+    eng.compute_forces()
+    for i, p in enumerate((p_zd, p_zo)):
+        md = ogo.OracleMD(base, p)
+        ref = md.forces()
+        work, ene, _ = eng.get_forces(i)
+        assert _rms(work, md.work.reshape(-1, 3)) <= 1e-5
+        assert abs(ene["ele"] - ref["ele"]) <= 1e-6 * abs(ref["ele"]) + 2e-3, (i, ene["ele"], ref["ele"])
+    eng.close()
