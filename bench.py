@@ -468,7 +468,7 @@ def run_mcmd(args):
     walkers = [dict(walkers[k], crd=c, vel=v) for k, (c, v) in zip(keep, states)]
     pot = tr[:, :, engine.ENERGY_NAMES.index("potential")]
     polys = [systems.vmcmd_ladder(pot[:, w].mean(), max(pot[:, w].std(), 1.0), seed=900 + w, n_vs=4,
-                                  interval=VMCMD_TRANS_INTERVAL) for w in range(len(walkers))]
+                                  interval=VMCMD_TRANS_INTERVAL, e_start=pot[-1, w]) for w in range(len(walkers))]
     p = dict(p, random_seed=1000 * args.walker_seed0 + 1, print_intvl_extended_lambda=1)
     # timed run: whole list intervals, so og_step replays the captured graph
     vs_logs = {}

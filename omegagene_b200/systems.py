@@ -337,12 +337,13 @@ def mcmd_polynomial(e_mean, e_sd, seed, temperature=300.0, order=6):
     return {"coef": c.tolist(), "lambda_low": lo, "lambda_high": hi, "temperature": temperature}
 
 
-def vmcmd_ladder(e_mean, e_sd, seed, n_vs=4, interval=10, temperature=300.0, order=6, prob=0.5):
+def vmcmd_ladder(e_mean, e_sd, seed, n_vs=4, interval=10, temperature=300.0, order=6, prob=0.5, e_start=None):
     """A V-McMD section for one walker, in the layout of the .cls "extended" section (cls_io;
     Read::load_ls_vmcmd, Read.cpp:521-560): n_vs windows over [mean - 4 sd, mean + 4 sd], each
     2 / (n_vs + 1) of the range wide, so that neighbours overlap by half a window; each window has
     its own seeded polynomial (mcmd_polynomial over the window); moves to a neighbour are tried
-    with probability `prob` (0 off the ends of the ladder).  init_vs is 1-based as in the file."""
+    with probability `prob` (0 off the ends of the ladder).  init_vs (1-based, as in the file) is
+    the window whose centre lies nearest e_start, or the middle one."""
     lo, hi = e_mean - 4.0 * e_sd, e_mean + 4.0 * e_sd
     width = 2.0 * (hi - lo) / (n_vs + 1)
     states = []
@@ -353,5 +354,8 @@ def vmcmd_ladder(e_mean, e_sd, seed, n_vs=4, interval=10, temperature=300.0, ord
         states.append(dict(order=order, lambda_low=a, lambda_high=b, prob_low=0.0 if v == 0 else prob,
                            prob_high=0.0 if v == n_vs - 1 else prob, coef=poly["coef"], alpha_low=0.0,
                            alpha_high=0.0))
+    init = n_vs // 2
+    if e_start is not None:
+        init = int(np.argmin([abs(0.5 * (x["lambda_low"] + x["lambda_high"]) - e_start) for x in states]))
     return {"n_vs": n_vs, "interval": interval, "temperature": temperature, "states": states,
-            "init_vs": 1 + n_vs // 2, "seed": seed}
+            "init_vs": 1 + init, "seed": seed}
