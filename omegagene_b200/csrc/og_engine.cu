@@ -29,8 +29,7 @@ __global__ void k_sort_columns(const int *, const int *, const int *, const int 
 __global__ void k_cell_info(const int *, int, const int *, const int *, const int *, const SysDev *, const double *,
                             const int *, double *, float2 *, int2 *, unsigned char *, int *, int *);
 __global__ void k_count_pairs(const int *, int, int, const int *, const int *, const SysDev *, const int *,
-                              const int *, const int *, const float2 *, const int2 *, const int *, const int *,
-                              const unsigned char *, int *);
+                              const int *, const int *, const float2 *, const int2 *, const int *, const int *, int *);
 __global__ void k_fill_pairs(int *, int, int, long long, const int *, const int *, const SysDev *, const int *,
                              const int *, const int *, const float2 *, const int2 *, const int *, const int *,
                              const int *, int2 *);
@@ -709,8 +708,7 @@ og_status build_list(og_engine *e) {
     k_count_pairs<<<blocks(n_items, 256), 256, 0, st>>>(e->d_counters, e->cells_cap, e->nnc, e->d_cell_sys,
                                                          e->d_sys_cell_base, e->d_sys, e->d_cell_col,
                                                          e->d_col_cell_start, e->d_col_head_cell, e->d_cell_zr,
-                                                         e->d_cell_uni, e->d_uni_lo, e->d_uni_hi, e->d_cell_valid,
-                                                         e->d_count);
+                                                         e->d_cell_uni, e->d_uni_lo, e->d_uni_hi, e->d_count);
     LAUNCH_CHECK();
     og_status s = scan_exclusive(e, e->d_count, e->d_offset, n_items + 1, 0);
     if (s) return s;

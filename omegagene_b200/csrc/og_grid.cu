@@ -363,8 +363,7 @@ __global__ void k_count_pairs(const int *__restrict__ counters, int cells_cap, i
                               const SysDev *__restrict__ sys, const int *__restrict__ cell_col,
                               const int *__restrict__ col_cell_start, const int *__restrict__ col_head_cell,
                               const float2 *__restrict__ cell_zr, const int2 *__restrict__ cell_uni,
-                              const int *__restrict__ uni_lo, const int *__restrict__ uni_hi,
-                              const unsigned char *__restrict__ cell_valid, int *__restrict__ count) {
+                              const int *__restrict__ uni_lo, const int *__restrict__ uni_hi, int *__restrict__ count) {
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (long long)cells_cap * nnc) return;
     const int c1 = (int)(idx / nnc), nb = (int)(idx % nnc);
