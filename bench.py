@@ -36,12 +36,14 @@ UNIT = "ns/day"
 DT_FS = 2.0
 INTVL = 10
 VMCMD_TRANS_INTERVAL = 100  # V-McMD walkers: steps between virtual-state transition trials
+EQUIL_STEPS = 2000  # 1M water: untimed relaxation (0.5 fs, 300 K velocity rescaling) before the NVE run
 N_WATERS = 333334
 BOX = 215.5
 LATTICE = 70
 FLOP_PER_PAIR = 40  # FP32 FLOP per interacting pair (sub 3, r2 5, rsqrt 1, powers 4, LJ 5, ZD 6, force 3, accum 6, energy 7)
 WORKLOAD = ("333334 TIP3P waters (1000002 atoms), 215.5 A cubic box, NVE dt 2 fs, SHAKE-trio rigid water, "
-            "cutoff 12 A, pair-list cutoff 13 A rebuilt every 10 steps, zero-dipole alpha 0")
+            "cutoff 12 A, pair-list cutoff 13 A rebuilt every 10 steps, zero-dipole alpha 0; seeded lattice start "
+            "relaxed for 2000 untimed steps at 0.5 fs with 300 K velocity rescaling")
 
 
 def ns_per_day(steps_per_s, dt_fs=DT_FS):
@@ -213,12 +215,21 @@ def run_ours(args, world, rank, local, pg):
     s = systems.water_system(N_WATERS, box=BOX, seed=20 + rank, lattice_m=LATTICE)
     p = dict(engine.DEFAULT_PARAMS)
     p.update(nsgrid_update_intvl=INTVL, time_step=DT_FS, thermostat="none", com_cancel_groups=["all"])
+    # the lattice start melts and heats: relax it (untimed) with velocity rescaling to 300 K at
+    # 0.5 fs, so that the NVE run starts from liquid water
+    eq = engine.Engine(local)
+    eq.add_system(s, dict(p, thermostat="scaling", temperature=300.0, time_step=0.5))
+    eq.finalize()
+    eq.step(EQUIL_STEPS)
+    crd, vel = eq.get_state(0)
+    eq.close()
+    s = dict(s, crd=crd, vel=vel)
     eng = engine.Engine(local)
     eng.add_system(s, p)
     eng.finalize()
     tuning = eng.tuning()
     n_atoms = s["n_atoms"]
-    del s
+    n_dist = 3 * len(s["constraint"]["trio_atoms"]) + len(s["constraint"]["pair_atoms"])
     # warm-up (untimed)
     eng.step(args.warmup)
     # interacting pairs of the current configuration (roofline numerator)
@@ -263,6 +274,29 @@ def run_ours(args, world, rank, local, pg):
         eng.synchronize()
     t_e2e = max_over_ranks(pg, time.perf_counter() - t0)
     flags = eng.flags()
+    # ---- NVE drift of the engine over 500 further steps (untimed), from its per-step energies,
+    # in calls of 100 steps; a call that faults (the synthetic water's hydrogens carry no LJ term,
+    # and very rarely one collapses onto a neighbour's oxygen at 2 fs) ends the segment
+    n_drift, tot, drift_note = 500, [], ""
+    eng.set_trace(100)
+    for _ in range(n_drift // 100):
+        try:
+            eng.step(100)
+        except engine.OgError as ex:
+            if ex.status != engine.OG_ERR_SYSTEM_FAULT:
+                raise
+            drift_note = "; a system fault ended the segment after %d steps" % len(tot)
+            break
+        tot.extend(eng.get_trace(100)[:, 0, engine.ENERGY_NAMES.index("total")])
+        eng.set_trace(100)
+    t_ns = np.arange(len(tot)) * DT_FS * 1e-6
+    dof = 3 * n_atoms - 3 - n_dist
+    drift = float(np.polyfit(t_ns, np.asarray(tot), 1)[0]) / dof if len(tot) >= 100 else None
+    # forces and state of the last configuration, for the FP64 check in the CPU leg
+    eng.set_trace(0)
+    eng.compute_forces()
+    acc_work, acc_ene, _ = eng.get_forces(0)
+    acc_crd, _ = eng.get_state(0)
     e2e = {"value": ns_per_day(e2e_steps / t_e2e) * world, "unit": UNIT,
            "h2d_bytes_per_step": 8 * 3 * n_atoms, "d2h_bytes_per_step": 8 * 3 * n_atoms + 8 * 11,
            "protocol": "per step: og_put_state (coordinates, pinned host -> device), og_step_async(1), "
@@ -299,8 +333,30 @@ def run_ours(args, world, rank, local, pg):
                      "peak_note": "FP32 CUDA-core peak = 148 SMs x 128 lanes x 2 x %.0f MHz (nominal at the "
                                   "measured max SM clock; MEASURED_PEAKS.json has no FP32 figure)" % sm_max},
         "e2e": e2e, "gpu_launches": launches, "clocks": clk, "device_flags": flags,
+        "accuracy": {"nve_drift_kcal_mol_ns_dof": drift, "nve_drift_sample": "%d NVE steps after the timed region "
+                     "(total energy per step, least-squares slope / %d degrees of freedom)%s" % (len(tot), dof,
+                                                                                          drift_note)},
     }
+    out["_acc"] = (dict(s, crd=acc_crd), p, acc_work, acc_ene)
     return out
+
+
+def accuracy_vs_oracle(system, params, work, ene):
+    """The FP64 oracle (the cell-list evaluator of the same step in double precision) against the
+    engine's forces and energies at the configuration the bench ended on: per-atom force RMS
+    relative error and the potential's relative error.  Part of the CPU leg."""
+    import time as _t
+    from oracle import ogo
+    t0 = _t.perf_counter()
+    md = ogo.OracleMD(system, params)
+    ref = md.forces()
+    w64 = md.work.reshape(-1, 3)
+    err = float(np.sqrt(((work - w64) ** 2).sum() / (w64 ** 2).sum()))
+    return {"force_rms_rel_err": err, "potential_rel_err": abs(ene["potential"] - ref["potential"]) /
+            abs(ref["potential"]), "vdw_rel_err": abs(ene["vdw"] - ref["vdw"]) / abs(ref["vdw"]),
+            "ele_rel_err": abs(ene["ele"] - ref["ele"]) / abs(ref["ele"]),
+            "oracle": "FP64 over the reference's cell-pair list, all %d atoms (%.0f s on the host)" % (
+                len(w64), _t.perf_counter() - t0)}
 
 
 # ------------------------------------------------------------------ serving workload
@@ -546,8 +602,10 @@ def main():
         }))
         return
     out = run_ours(args, world, rank, local, pg)
+    acc = out.pop("_acc", None)
     if rank == 0:
         if not args.no_cpu_baseline:
+            out["accuracy"].update(accuracy_vs_oracle(*acc))
             res, why = reference_cpu(args.cpu_steps, 3)
             if res is not None:
                 out["cpu_baseline"] = {"value": cpu_ns_per_day_at_1m(res["atom_steps_per_s"]), "unit": UNIT,
