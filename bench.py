@@ -206,6 +206,12 @@ def barrier(pg):
         pg.barrier()
 
 
+def replica_value(steps, ms_max, world):
+    """Whole-job ns/day of `world` independent replicas: each ran `steps` steps, the slowest in
+    ms_max (max over ranks), and every replica's simulated time counts."""
+    return ns_per_day(steps / (ms_max / 1e3)) * world
+
+
 # ------------------------------------------------------------------ our arm
 
 def run_ours(args, world, rank, local, pg):
@@ -253,8 +259,7 @@ def run_ours(args, world, rank, local, pg):
     ms_total = max_over_ranks(pg, st["step_ms"])
     pair_ms = st["pair_kernel_ms"] / args.steps
     launches = st["kernel_launches"]
-    steps_per_s = args.steps / (ms_total / 1e3)
-    value = ns_per_day(steps_per_s) * world
+    value = replica_value(args.steps, ms_total, world)
     # ---- end to end through the C ABI with host state (pinned) copied every step
     eng.set_timing(False)
     crd_h = torch.empty(3 * n_atoms, dtype=torch.float64, pin_memory=True)
@@ -604,7 +609,7 @@ def main():
     out = run_ours(args, world, rank, local, pg)
     acc = out.pop("_acc", None)
     if rank == 0:
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:  # the CPU leg runs at N = 1 only
             out["accuracy"].update(accuracy_vs_oracle(*acc))
             res, why = reference_cpu(args.cpu_steps, 3)
             if res is not None:
