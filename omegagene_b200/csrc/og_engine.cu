@@ -57,6 +57,13 @@ template <bool VIR, bool ENE, int MINB>
 __global__ void k_pair_ljzd_jm2(const int *, const int *, const SysDev *, const float4 *, const float4 *, const int *,
                                 const int *, const float4 *, const int2 *, const unsigned long long *, const float2 *,
                                 unsigned long long *, double *, long long);
+template <bool VIR, bool ENE, int MINB, int NT, bool GEN>
+__global__ void k_pair_ljzd_jl(int *, const int *, const SysDev *, const float4 *, const int *, const int *,
+                               const float4 *, const int2 *, const int2 *, const int *, const float2 *,
+                               unsigned long long *, double *, const EleDev *, const float2 *);
+template <int NT>
+__global__ void k_jl_build(const int *, const int *, const SysDev *, const float4 *, const float4 *, const int *,
+                           const float4 *, const unsigned long long *, long long, float, int2 *, int *, float4 *);
 __global__ void k_cell_bbox(const int *, int, const float4 *, const unsigned char *, float4 *);
 // og_integrate.cu
 __global__ void k_excess(int, const int2 *, const int *, const SysDev *, const EleDev *, const double *,
@@ -105,7 +112,8 @@ __global__ void k_nb14(int, const int2 *, const int2 *, const double2 *, const i
 __global__ void k_shake_quad(int, const int4 *, const double *, const int *, const SysDev *, const int *, const float *,
                              double *, const double *, int, double, int *);
 __global__ void k_finish(int, const int *, const SysDev *, int, double *, const double *, const double *, double *,
-                         const int *, double *, const double *, float4 *, const float *, double *, int *, int *);
+                         const int *, double *, const double *, float4 *, const float *, double *, int *, int *,
+                         const float4 *, float);
 __global__ void k_slot_refresh(const int *, int, const int *, const double *, const double *, const float *,
                                const int *, float4 *, int *);
 __global__ void k_energies(int, const SysDev *, const double *, const double *, double *, double *, int,
@@ -114,7 +122,7 @@ __global__ void k_trace_advance(long long *, long long *);
 __global__ void k_capture_frames(int, const int *, const int *, const int *, const SysDev *, const long long *,
                                  const double *, const double *, float *, double *);
 __global__ void k_put_state(int, int, const int *, const SysDev *, const double *, const double *, double *, double *,
-                            const int *, double *, const double *, float4 *);
+                            const int *, double *, const double *, float4 *, const float4 *, float, int *);
 
 __global__ void k_fill_int(int *p, long long n, int v) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -127,6 +135,10 @@ __global__ void k_copy_double(double *dst, const double *src, long long n) {
 }  // namespace og
 
 using namespace og;
+
+// The pair variant over j lists, and the displacement (A) after which its lists are rebuilt.
+#define OG_JL_VARIANT 10
+#define OG_JL_SKIN 0.25f
 
 namespace {
 
@@ -213,6 +225,11 @@ struct og_engine {
     int *d_slot_atom = nullptr, *d_slot_type = nullptr;
     double *d_slot_crd = nullptr;
     float4 *d_xq = nullptr;
+    // j lists of the pair variant OG_JL_VARIANT: entries (8 per cell-pair record), per-cell
+    // counts, and the slot positions they were built from
+    int2 *d_jl = nullptr;
+    int *d_jl_count = nullptr;
+    float4 *d_xq_ref = nullptr;
     unsigned long long *d_frc = nullptr;
     int *d_uni_lo = nullptr, *d_uni_hi = nullptr;
     int *d_count = nullptr, *d_offset = nullptr;
@@ -725,6 +742,7 @@ og_status build_list(og_engine *e) {
         e->d_slot_atom, e->d_atom_slot, e->d_excl_start, e->d_excl_list, e->d_cell_excl, e->d_cell_origin,
         e->d_cp_mask, e->d_cp_shift);
     LAUNCH_CHECK();
+    if (e->d_jl) CK(cudaMemsetAsync(e->d_counters + OG_CNT_JL_STALE, 1, sizeof(int), st));  // new list: rebuild
     return OG_OK;
 }
 
@@ -734,6 +752,9 @@ og_status build_list(og_engine *e) {
     e->d_counters, e->d_cell_sys, e->d_sys, e->d_bbox, e->d_xq, e->d_slot_type, e->d_cp_head, e->d_cp_shift, \
         e->d_cp_c2img, e->d_cp_mask, e->d_lj, e->d_frc, e->d_cell_acc, e->pair_cap
 #define JQ_ARGS PAIR_ARGS, e->d_ele, e->d_hps
+#define JL_ARGS                                                                                                 \
+    e->d_counters, e->d_cell_sys, e->d_sys, e->d_xq, e->d_slot_type, e->d_cp_head, e->d_cp_shift, e->d_cp_c2img, \
+        e->d_jl, e->d_jl_count, e->d_lj, e->d_frc, e->d_cell_acc, e->d_ele, e->d_hps
 
 // Pair kernel variants differ in the register budget per thread (resident blocks per SM).
 // ene = false: the caller does not read this step's energies (only variants 5-6 skip them).
@@ -749,6 +770,18 @@ og_status launch_pair(og_engine *e, bool vir, int variant, bool ene) {
         if (vir) k_pair_ljzd_jq<true, true, 2, 256, true><<<nb, 256, 0, st>>>(JQ_ARGS);
         else if (ene) k_pair_ljzd_jq<false, true, 5, 128, true><<<2 * nb, 128, 0, st>>>(JQ_ARGS);
         else k_pair_ljzd_jq<false, false, 5, 128, true><<<2 * nb, 128, 0, st>>>(JQ_ARGS);
+        LAUNCH_CHECK();
+        return OG_OK;
+    }
+    if (variant == OG_JL_VARIANT) {
+        if (!e->d_jl) return fail(e, OG_ERR_STATE, "pair variant %d without its j lists", OG_JL_VARIANT);
+        k_jl_build<128><<<2 * nb, 128, 0, st>>>(e->d_counters, e->d_cell_sys, e->d_sys, e->d_bbox, e->d_xq,
+                                                 e->d_cp_head, e->d_cp_shift, e->d_cp_mask, e->pair_cap,
+                                                 2.0f * OG_JL_SKIN + 1e-3f, e->d_jl, e->d_jl_count, e->d_xq_ref);
+        LAUNCH_CHECK();
+        if (vir) k_pair_ljzd_jl<true, true, 2, 128, false><<<2 * nb, 128, 0, st>>>(JL_ARGS);
+        else if (ene) k_pair_ljzd_jl<false, true, 5, 128, false><<<2 * nb, 128, 0, st>>>(JL_ARGS);
+        else k_pair_ljzd_jl<false, false, 5, 128, false><<<2 * nb, 128, 0, st>>>(JL_ARGS);
         LAUNCH_CHECK();
         return OG_OK;
     }
@@ -1081,7 +1114,8 @@ og_status run_step(og_engine *e, bool ene) {
     k_finish<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->n_atoms, e->d_atom_sys, e->d_sys, 1, e->d_crd,
                                                        e->d_crd_prev, e->d_vel, e->d_vel_next, e->d_atom_slot,
                                                        e->d_slot_crd, e->d_cell_origin, e->d_xq, e->d_mass, e->d_ke,
-                                                       e->d_counters, e->d_sys_fault);
+                                                       e->d_counters, e->d_sys_fault, e->d_xq_ref,
+                                                       OG_JL_SKIN * OG_JL_SKIN);
     LAUNCH_CHECK();
     if ((s = seg_sum<1>(e, e->d_ke, 1, 0, e->d_seg_atoms, e->mc_atoms, e->d_sys_acc, OG_ACC_SIZE, OG_ACC_KIN, 0)))
         return s;
@@ -1265,7 +1299,37 @@ og_status grow_pairs(og_engine *e, long long need) {
     s = dalloc(e, &e->d_cp_shift, (size_t)cap);
     if (s) return s;
     e->pair_cap = cap;
+    if (e->d_jl) {
+        dfree(e, e->d_jl);
+        e->d_jl = nullptr;
+        s = dalloc(e, &e->d_jl, 8 * (size_t)cap);
+        if (s) return s;
+    }
     return OG_OK;
+}
+
+// The j lists of the pair variant OG_JL_VARIANT (8 entries per cell-pair record), their counts and
+// the positions they are built from; marked stale, so the first pair launch builds them.
+og_status jl_alloc(og_engine *e) {
+    if (e->d_jl) return OG_OK;
+    if ((long long)e->slots_cap >= (1ll << 24))
+        return fail(e, OG_ERR_INVALID, "pair variant %d needs fewer than 2^24 atom slots (engine has %d)",
+                    OG_JL_VARIANT, e->slots_cap);
+    og_status s;
+    if ((s = dalloc(e, &e->d_jl, 8 * (size_t)e->pair_cap)) || (s = dalloc(e, &e->d_jl_count, (size_t)e->cells_cap)) ||
+        (s = dalloc(e, &e->d_xq_ref, (size_t)e->slots_cap)))
+        return s;
+    CK(cudaMemsetAsync(e->d_counters + OG_CNT_JL_STALE, 1, sizeof(int), e->stream));
+    return OG_OK;
+}
+
+void jl_free(og_engine *e) {
+    dfree(e, e->d_jl);
+    dfree(e, e->d_jl_count);
+    dfree(e, e->d_xq_ref);
+    e->d_jl = nullptr;
+    e->d_jl_count = nullptr;
+    e->d_xq_ref = nullptr;
 }
 
 // Captures one list interval -- the rebuild step and the intvl-1 steps after it -- into a graph.
@@ -1331,21 +1395,26 @@ og_status autotune_pair(og_engine *e) {
         e->pair_variant = 9;
         return OG_OK;
     }
-    if (e->fixed_variant >= 0) {
-        e->pair_variant = e->fixed_variant;
-        return OG_OK;
-    }
     const char *env = getenv("OG_PAIR_VARIANT");
-    if (env && *env) {
-        e->pair_variant = atoi(env) % OG_N_PAIR_VARIANTS;
-        return OG_OK;
+    if (e->fixed_variant >= 0 || (env && *env)) {
+        e->pair_variant = e->fixed_variant >= 0 ? e->fixed_variant : atoi(env) % OG_N_PAIR_VARIANTS;
+        return e->pair_variant == OG_JL_VARIANT ? jl_alloc(e) : OG_OK;
     }
     k_cell_bbox<<<blocks(e->cells_cap, 256), 256, 0, e->stream>>>(e->d_counters, e->cells_cap, e->d_xq,
                                                                    e->d_cell_valid, e->d_bbox);
     LAUNCH_CHECK();
+    const bool try_jl = (long long)e->slots_cap < (1ll << 24);
+    if (try_jl) {
+        og_status s = jl_alloc(e);
+        if (s) return s;
+    }
     double best = 1e30;
     for (int v = 0; v < OG_N_PAIR_VARIANTS; v++) {
-        double vbest = 1e30;
+        if (v == OG_JL_VARIANT && !try_jl) {
+            e->variant_ms[v] = 0.0;
+            continue;
+        }
+        double vbest = 1e30, first = 0.0;
         for (int rep = 0; rep < 3; rep++) {
             CK(cudaEventRecord(e->ev_pair0, e->stream));
             og_status s = launch_pair(e, false, v, false);
@@ -1354,14 +1423,17 @@ og_status autotune_pair(og_engine *e) {
             CK(cudaEventSynchronize(e->ev_pair1));
             float ms = 0.f;
             CK(cudaEventElapsedTime(&ms, e->ev_pair0, e->ev_pair1));
-            vbest = std::min(vbest, (double)ms);
+            if (v == OG_JL_VARIANT && rep == 0) first = ms;  // the j lists are built once, here
+            else vbest = std::min(vbest, (double)ms);
         }
+        if (v == OG_JL_VARIANT) vbest += std::max(0.0, first - vbest) / e->intvl;
         e->variant_ms[v] = vbest;
         if (vbest < best) {
             best = vbest;
             e->pair_variant = v;
         }
     }
+    if (try_jl && e->pair_variant != OG_JL_VARIANT) jl_free(e);
     CK(cudaMemsetAsync(e->d_frc, 0, sizeof(unsigned long long) * 3 * (size_t)e->slots_cap, e->stream));
     return OG_OK;
 }
@@ -2472,7 +2544,8 @@ extern "C" og_status og_put_state(og_engine *e, int32_t sys, const double *crd, 
     k_put_state<<<blocks(D.n_atoms, 256), 256, 0, e->stream>>>(D.n_atoms, D.atom_base, e->d_atom_sys, e->d_sys,
                                                                 crd ? sc : nullptr, vel_next ? sv : nullptr, e->d_crd,
                                                                 e->d_vel_next, e->d_atom_slot, e->d_slot_crd,
-                                                                e->d_cell_origin, e->d_xq);
+                                                                e->d_cell_origin, e->d_xq, e->d_xq_ref,
+                                                                OG_JL_SKIN * OG_JL_SKIN, e->d_counters);
     LAUNCH_CHECK();
     return OG_OK;
 }

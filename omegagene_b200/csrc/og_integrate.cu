@@ -898,6 +898,16 @@ __global__ void k_thermo_crd(int n_atoms, const int *__restrict__ atom_sys, cons
     for (int q = 0; q < 3; q++) crd[3 * a + q] = crd_prev[3 * a + q] + dt * vel_next[3 * a + q];
 }
 
+// The pair kernel's j lists hold while every slot is within skin of the position they were
+// built from (xq_ref; null when the engine does not use them); otherwise they are marked stale.
+__device__ __forceinline__ void og_jl_check(const float4 &p, int sl, const float4 *__restrict__ xq_ref, float skin2,
+                                            int *__restrict__ counters) {
+    if (!xq_ref) return;
+    const float4 o = xq_ref[sl];
+    const float dx = p.x - o.x, dy = p.y - o.y, dz = p.z - o.z;
+    if (!(dx * dx + dy * dy + dz * dz <= skin2)) counters[OG_CNT_JL_STALE] = 1;
+}
+
 // End of step, per atom: velocities from the constrained displacement (SubBox.cpp:1462-1481,
 // only when the plain constraint path ran), MiniCell::move_atom (MiniCell.cpp:1312-1325) and the
 // refreshed cell-relative float coordinate, PBC wrap (SubBox.cpp:1482-1502) and the kinetic
@@ -908,7 +918,7 @@ __global__ void k_finish(int n_atoms, const int *__restrict__ atom_sys, const Sy
                          const int *__restrict__ atom_slot, double *__restrict__ slot_crd,
                          const double *__restrict__ cell_origin, float4 *__restrict__ xq,
                          const float *__restrict__ mass, double *__restrict__ ke, int *__restrict__ counters,
-                         int *__restrict__ sys_fault) {
+                         int *__restrict__ sys_fault, const float4 *__restrict__ xq_ref, float jl_skin2) {
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= n_atoms) return;
     const SysDev &S = sys[atom_sys[a]];
@@ -935,6 +945,7 @@ __global__ void k_finish(int n_atoms, const int *__restrict__ atom_sys, const Sy
     p.y = r[1];
     p.z = r[2];
     xq[sl] = p;
+    og_jl_check(p, sl, xq_ref, jl_skin2, counters);
     ke[a] = vn * (double)mass[a];
     if (!(disp2 <= S.max_step_disp2)) {  // also catches NaN
         og_set_flag(counters, OG_FLAG_DISPLACEMENT);
@@ -1000,7 +1011,8 @@ __global__ void k_put_state(int n_atoms, int atom0, const int *__restrict__ atom
                             const double *__restrict__ new_vel, double *__restrict__ crd,
                             double *__restrict__ vel_next, const int *__restrict__ atom_slot,
                             double *__restrict__ slot_crd, const double *__restrict__ cell_origin,
-                            float4 *__restrict__ xq) {
+                            float4 *__restrict__ xq, const float4 *__restrict__ xq_ref, float jl_skin2,
+                            int *__restrict__ counters) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_atoms) return;
     const int a = atom0 + i;
@@ -1025,6 +1037,7 @@ __global__ void k_put_state(int n_atoms, int atom0, const int *__restrict__ atom
         p.y = r[1];
         p.z = r[2];
         xq[sl] = p;
+        og_jl_check(p, sl, xq_ref, jl_skin2, counters);
     }
 }
 

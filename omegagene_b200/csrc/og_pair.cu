@@ -693,8 +693,221 @@ __device__ __forceinline__ void og_ele_pair(const EleDev &E, float r, float r2, 
     }
 }
 
+// Per-lane partial sums of one warp's i cell in the j-queue and j-list kernels: i forces of the
+// packed pair slots (2p, 2p+1), energies folded into FP64 after every evaluation round, and the
+// virial terms.
+template <bool VIR>
+struct OgIAcc {
+    float2 fx[OG_CELL / 2], fy[OG_CELL / 2], fz[OG_CELL / 2];
+    double dv, de;
+    int n_act;
+    double v[VIR ? 9 : 1];
+};
+
+template <bool VIR>
+__device__ __forceinline__ void og_iacc_zero(OgIAcc<VIR> &A) {
+#pragma unroll
+    for (int p = 0; p < OG_CELL / 2; p++) A.fx[p] = A.fy[p] = A.fz[p] = og_f2(0.f, 0.f);
+    A.dv = A.de = 0.0;
+    A.n_act = 0;
+#pragma unroll
+    for (int k = 0; k < (VIR ? 9 : 1); k++) A.v[k] = 0.0;
+}
+
+// A warp's i cell in shared memory: positions and scaled charges packed by pair (2p, 2p+1), and
+// the LJ-table row offsets of the atoms' types.
+struct OgICell {
+    float4 ab[OG_CELL / 2][2];
+    int2 t2[OG_CELL / 2];
+};
+
+__device__ __forceinline__ void og_load_icell(OgICell &ic, int c1, int lane, const float4 *__restrict__ xq,
+                                              const int *__restrict__ slot_type, const SysDev &S) {
+    if (lane < OG_CELL / 2) {
+        const float4 a = xq[c1 * OG_CELL + 2 * lane], b = xq[c1 * OG_CELL + 2 * lane + 1];
+        ic.ab[lane][0] = make_float4(a.x, b.x, a.y, b.y);
+        ic.ab[lane][1] = make_float4(a.z, b.z, a.w * (float)OG_CHARGE_COEFF, b.w * (float)OG_CHARGE_COEFF);
+        ic.t2[lane] = make_int2(slot_type[c1 * OG_CELL + 2 * lane] * S.n_types + S.lj_base,
+                                slot_type[c1 * OG_CELL + 2 * lane + 1] * S.n_types + S.lj_base);
+    }
+    __syncwarp();
+}
+
+// The zero-dipole constants of a system, packed for both halves of a pair.
+struct OgZdConst {
+    float rc2;
+    float2 nzcore, bco, nfco;
+};
+
+__device__ __forceinline__ OgZdConst og_zd_const(const SysDev &S) {
+    OgZdConst k;
+    k.rc2 = S.cutoff2;
+    k.nzcore = og_f2(-S.zcore, -S.zcore);
+    k.bco = og_f2(S.bcoeff, S.bcoeff);
+    k.nfco = og_f2(-S.fcoeff, -S.fcoeff);
+    return k;
+}
+
+// One lane evaluates one j atom against the warp's 8 i atoms: xj is the j position in cell1's
+// frame with its charge in w, tj its LJ type, skip its exclusion byte over the i atoms (bit i
+// set: no pair), slot its force slot and img the image bits of its cell pair (virial shift term).
+// i work goes to the lane's partial sums, j work to the fixed-point accumulator; a lane with
+// active = false evaluates a dummy entry whose pairs are all skipped.
 // GEN: the system's EleDev model and HPS table (ele, hps) instead of the packed zero-dipole
 // alpha = 0 evaluation; both halves of a packed pair are evaluated one after the other.
+template <bool VIR, bool ENE, bool GEN>
+__device__ __forceinline__ void og_eval_j(OgIAcc<VIR> &A, bool active, float4 xj, int tj, unsigned skip, int slot,
+                                          int img, const OgICell &ic, const OgZdConst &K, const SysDev &S,
+                                          const EleDev &E, const float2 *__restrict__ lj,
+                                          const float2 *__restrict__ hps, unsigned long long *__restrict__ frc) {
+    const float2 one = og_f2(1.f, 1.f), half = og_f2(0.5f, 0.5f), six = og_f2(6.f, 6.f);
+    const float2 m12 = og_f2(-12.f, -12.f), mone = og_f2(-1.f, -1.f);
+    const float2 nrx = og_f2(-xj.x, -xj.x), nry = og_f2(-xj.y, -xj.y), nrz = og_f2(-xj.z, -xj.z);
+    const float2 qj = og_f2(xj.w, xj.w);
+    float2 av = og_f2(0.f, 0.f), ae = og_f2(0.f, 0.f);
+    float2 wjx = og_f2(0.f, 0.f), wjy = og_f2(0.f, 0.f), wjz = og_f2(0.f, 0.f);
+#pragma unroll
+    for (int p = 0; p < OG_CELL / 2; p++) {
+        const float4 Ap = ic.ab[p][0], Bp = ic.ab[p][1];
+        const int2 T = ic.t2[p];
+        const float2 dx = __fadd2_rn(og_f2(Ap.x, Ap.y), nrx);
+        const float2 dy = __fadd2_rn(og_f2(Ap.z, Ap.w), nry);
+        const float2 dz = __fadd2_rn(og_f2(Bp.x, Bp.y), nrz);
+        const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+        const bool act_a = ((skip >> (2 * p)) & 1u) == 0u && r2.x < K.rc2;
+        const bool act_b = ((skip >> (2 * p + 1)) & 1u) == 0u && r2.y < K.rc2;
+        const float2 r2s = og_f2(act_a ? r2.x : 1.0f, act_b ? r2.y : 1.0f);
+        float2 y = og_f2(rsqrtf(r2s.x), rsqrtf(r2s.y));
+        const float2 h = __ffma2_rn(__fmul2_rn(__fmul2_rn(r2s, mone), y), y, one);
+        y = __ffma2_rn(__fmul2_rn(half, y), h, y);
+        const float2 r2inv = __fmul2_rn(y, y);
+        const float2 r6 = __fmul2_rn(__fmul2_rn(r2inv, r2inv), r2inv);
+        const float2 pa = __ldg(&lj[T.x + tj]), pb = __ldg(&lj[T.y + tj]);
+        const float2 t6 = __fmul2_rn(og_f2(pa.x, pb.x), r6);
+        const float2 t12 = __fmul2_rn(__fmul2_rn(og_f2(pa.y, pb.y), r6), r6);
+        const float2 cc = __fmul2_rn(og_f2(Bp.z, Bp.w), qj);
+        const float2 on = og_f2(act_a ? 1.f : 0.f, act_b ? 1.f : 0.f);
+        float2 wc;
+        if (!GEN) {
+            wc = __ffma2_rn(__fmul2_rn(cc, mone), __ffma2_rn(y, r2inv, K.nfco),
+                            __fmul2_rn(r2inv, __ffma2_rn(t12, m12, __fmul2_rn(six, t6))));
+            wc = __fmul2_rn(wc, on);
+            if (ENE) {
+                const float2 pv = __fmul2_rn(__ffma2_rn(t6, mone, t12), on);
+                const float2 pe = __fmul2_rn(__fmul2_rn(cc, __ffma2_rn(K.bco, r2s, __fadd2_rn(y, K.nzcore))), on);
+                av = __fadd2_rn(av, pv);
+                ae = __fadd2_rn(ae, pe);
+            }
+        } else {
+            float w2[2], v2[2], e2[2];
+#pragma unroll
+            for (int hh = 0; hh < 2; hh++) {
+                const float r2h = hh ? r2s.y : r2s.x, yh = hh ? y.y : y.x;
+                const float r2i = yh * yh, r3i = yh * r2i, rr = r2h * yh;
+                const float t6h = hh ? t6.y : t6.x, t12h = hh ? t12.y : t12.x;
+                float ev = t12h - t6h, wl = r2i * (6.f * t6h - 12.f * t12h);
+                if (E.hps) {  // ForceField.cpp:380-391
+                    const float2 hp = __ldg(&hps[(hh ? T.y : T.x) + tj]);
+                    if (rr > hp.x) {
+                        ev *= hp.y;
+                        wl *= hp.y;
+                    } else {
+                        ev += (1.f - hp.y) * E.hps_eps;
+                    }
+                }
+                float ee, ge;
+                og_ele_pair(E, rr, r2h, yh, r2i, r3i, hh ? cc.y : cc.x, ee, ge);
+                w2[hh] = wl + ge;
+                v2[hh] = ev;
+                e2[hh] = ee;
+            }
+            wc = __fmul2_rn(og_f2(w2[0], w2[1]), on);
+            if (ENE) {
+                av = __fadd2_rn(av, __fmul2_rn(og_f2(v2[0], v2[1]), on));
+                ae = __fadd2_rn(ae, __fmul2_rn(og_f2(e2[0], e2[1]), on));
+            }
+        }
+        if (VIR) A.n_act += (act_a ? 1 : 0) + (act_b ? 1 : 0);
+        const float2 wx = __fmul2_rn(wc, dx), wy = __fmul2_rn(wc, dy), wz = __fmul2_rn(wc, dz);
+        A.fx[p] = __fadd2_rn(A.fx[p], wx);
+        A.fy[p] = __fadd2_rn(A.fy[p], wy);
+        A.fz[p] = __fadd2_rn(A.fz[p], wz);
+        wjx = __fadd2_rn(wjx, wx);
+        wjy = __fadd2_rn(wjy, wy);
+        wjz = __fadd2_rn(wjz, wz);
+    }
+    if (ENE) {
+        A.dv += (double)av.x + (double)av.y;
+        A.de += (double)ae.x + (double)ae.y;
+    }
+    const float sx = -(wjx.x + wjx.y), sy = -(wjy.x + wjy.y), sz = -(wjz.x + wjz.y);
+    if (active && (sx != 0.f || sy != 0.f || sz != 0.f)) {
+        unsigned long long *fj = frc + 3 * (size_t)slot;
+        atomicAdd(fj + 0, (unsigned long long)__float2ll_rn(sx * (float)OG_FIX_SCALE));
+        atomicAdd(fj + 1, (unsigned long long)__float2ll_rn(sy * (float)OG_FIX_SCALE));
+        atomicAdd(fj + 2, (unsigned long long)__float2ll_rn(sz * (float)OG_FIX_SCALE));
+        if (VIR && img != 0) {
+            const double sh[3] = {(img & 1) ? -S.L[0] : ((img & 2) ? S.L[0] : 0.0),
+                                  (img & 4) ? -S.L[1] : ((img & 8) ? S.L[1] : 0.0),
+                                  (img & 16) ? -S.L[2] : ((img & 32) ? S.L[2] : 0.0)};
+            // sum over pairs of d (x) f: f on i is +w, so the shift term takes -(work on j)
+            const double fjv[3] = {-(double)sx, -(double)sy, -(double)sz};
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++) A.v[a * 3 + b] += sh[a] * fjv[b];
+        }
+    }
+}
+
+// End of a warp's i cell: the lanes' i work reduced in FP64 (fixed shuffle order) and added to
+// the fixed-point accumulator; energies, virial and the active-pair count to the cell's slots.
+template <bool VIR, bool ENE>
+__device__ __forceinline__ void og_flush_icell(OgIAcc<VIR> &A, int c1, int lane, unsigned long long *__restrict__ frc,
+                                               double *__restrict__ cell_acc) {
+    double mine[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int p = 0; p < OG_CELL / 2; p++) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            double w3[3] = {(double)(h ? A.fx[p].y : A.fx[p].x), (double)(h ? A.fy[p].y : A.fy[p].x),
+                            (double)(h ? A.fz[p].y : A.fz[p].x)};
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                double x = w3[d];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+                if (lane == 2 * p + h) mine[d] = x;
+            }
+        }
+    }
+    if (lane < OG_CELL && (mine[0] != 0.0 || mine[1] != 0.0 || mine[2] != 0.0)) {
+        unsigned long long *fa = frc + 3 * (size_t)(c1 * OG_CELL + lane);
+        atomicAdd(fa + 0, (unsigned long long)og_to_fix(mine[0]));
+        atomicAdd(fa + 1, (unsigned long long)og_to_fix(mine[1]));
+        atomicAdd(fa + 2, (unsigned long long)og_to_fix(mine[2]));
+    }
+    if (!ENE) return;
+    double e_vdw = A.dv, e_ele = A.de;
+    for (int o = 16; o > 0; o >>= 1) {
+        e_vdw += __shfl_xor_sync(0xffffffffu, e_vdw, o);
+        e_ele += __shfl_xor_sync(0xffffffffu, e_ele, o);
+    }
+    int n_act = A.n_act;
+    if (VIR) {
+        for (int k = 0; k < 9; k++)
+            for (int o = 16; o > 0; o >>= 1) A.v[k] += __shfl_xor_sync(0xffffffffu, A.v[k], o);
+        for (int o = 16; o > 0; o >>= 1) n_act += __shfl_xor_sync(0xffffffffu, n_act, o);
+    }
+    if (lane == 0) {
+        double *acc = cell_acc + (size_t)c1 * OG_CELL_ACC;
+        acc[0] = e_vdw;
+        acc[1] = e_ele;
+        if (VIR) {
+            for (int k = 0; k < 9; k++) acc[2 + k] = A.v[k];
+            acc[11] = (double)n_act;
+        }
+    }
+}
+
 template <bool VIR, bool ENE, int MINB, int NT = 256, bool GEN = false>
 __global__ void __launch_bounds__(NT, MINB)
 k_pair_ljzd_jq(const int *__restrict__ counters, const int *__restrict__ cell_sys, const SysDev *__restrict__ sys,
@@ -712,37 +925,18 @@ k_pair_ljzd_jq(const int *__restrict__ counters, const int *__restrict__ cell_sy
     const int jj = lane & 7, q = lane >> 3;
     const SysDev &S = sys[cell_sys[c1]];
     const EleDev &E = ele[GEN ? cell_sys[c1] : 0];
-    __shared__ float4 s_ab[NT / 32][OG_CELL / 2][2];
-    __shared__ int2 s_t2[NT / 32][OG_CELL / 2];
+    __shared__ OgICell s_i[NT / 32];
     __shared__ float4 s_qx[NT / 32][OG_JQ];  // queued j: (x, y, z) in cell1's frame, charge
     __shared__ int4 s_qi[NT / 32][OG_JQ];    // queued j: LJ type, slot, mask byte, image bits
     __shared__ float4 s_rsp[NT / 32][32];    // surviving records of the current chunk, in order:
     __shared__ uint2 s_rm[NT / 32][32];      //   shift + cell2, exclusion mask,
     __shared__ int s_rimg[NT / 32][VIR ? 32 : 1];  //   image bits (virial only)
-    if (lane < OG_CELL / 2) {
-        const float4 a = xq[c1 * OG_CELL + 2 * lane], b = xq[c1 * OG_CELL + 2 * lane + 1];
-        s_ab[wib][lane][0] = make_float4(a.x, b.x, a.y, b.y);
-        s_ab[wib][lane][1] = make_float4(a.z, b.z, a.w * (float)OG_CHARGE_COEFF, b.w * (float)OG_CHARGE_COEFF);
-        s_t2[wib][lane] = make_int2(slot_type[c1 * OG_CELL + 2 * lane] * S.n_types + S.lj_base,
-                                    slot_type[c1 * OG_CELL + 2 * lane + 1] * S.n_types + S.lj_base);
-    }
-    __syncwarp();
-    const float rc2 = S.cutoff2;
-    const float2 nzcore = og_f2(-S.zcore, -S.zcore), bco = og_f2(S.bcoeff, S.bcoeff);
-    const float2 nfco = og_f2(-S.fcoeff, -S.fcoeff);
-    const float2 one = og_f2(1.f, 1.f), half = og_f2(0.5f, 0.5f), six = og_f2(6.f, 6.f);
-    const float2 m12 = og_f2(-12.f, -12.f), mone = og_f2(-1.f, -1.f);
-    const float rskip = sqrtf(rc2) + 1e-3f, rskip2 = rskip * rskip;
+    og_load_icell(s_i[wib], c1, lane, xq, slot_type, S);
+    const OgZdConst K = og_zd_const(S);
+    const float rskip = sqrtf(K.rc2) + 1e-3f, rskip2 = rskip * rskip;
     const float4 b1l = bbox[2 * c1], b1h = bbox[2 * c1 + 1];
-    float2 fx[OG_CELL / 2], fy[OG_CELL / 2], fz[OG_CELL / 2];
-#pragma unroll
-    for (int p = 0; p < OG_CELL / 2; p++) fx[p] = fy[p] = fz[p] = og_f2(0.f, 0.f);
-    float2 av = og_f2(0.f, 0.f), ae = og_f2(0.f, 0.f);
-    double dv = 0.0, de = 0.0;
-    int n_act = 0;
-    double v[9];
-    if (VIR)
-        for (int k = 0; k < 9; k++) v[k] = 0;
+    OgIAcc<VIR> A;
+    og_iacc_zero(A);
     int q_head = 0, q_len = 0;  // ring of queued j entries (warp-uniform)
 
     // lane takes queue entry (q_head + lane) if lane < n_take and evaluates it against cell1
@@ -755,102 +949,7 @@ k_pair_ljzd_jq(const int *__restrict__ counters, const int *__restrict__ cell_sy
             xj = s_qx[wib][e];
             ji = s_qi[wib][e];
         }
-        const unsigned skip = (unsigned)ji.z;
-        const int tj = ji.x;
-        const float2 nrx = og_f2(-xj.x, -xj.x), nry = og_f2(-xj.y, -xj.y), nrz = og_f2(-xj.z, -xj.z);
-        const float2 qj = og_f2(xj.w, xj.w);
-        float2 wjx = og_f2(0.f, 0.f), wjy = og_f2(0.f, 0.f), wjz = og_f2(0.f, 0.f);
-#pragma unroll
-        for (int p = 0; p < OG_CELL / 2; p++) {
-            const float4 A = s_ab[wib][p][0], B = s_ab[wib][p][1];
-            const int2 T = s_t2[wib][p];
-            const float2 dx = __fadd2_rn(og_f2(A.x, A.y), nrx);
-            const float2 dy = __fadd2_rn(og_f2(A.z, A.w), nry);
-            const float2 dz = __fadd2_rn(og_f2(B.x, B.y), nrz);
-            const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-            const bool act_a = ((skip >> (2 * p)) & 1u) == 0u && r2.x < rc2;
-            const bool act_b = ((skip >> (2 * p + 1)) & 1u) == 0u && r2.y < rc2;
-            const float2 r2s = og_f2(act_a ? r2.x : 1.0f, act_b ? r2.y : 1.0f);
-            float2 y = og_f2(rsqrtf(r2s.x), rsqrtf(r2s.y));
-            const float2 h = __ffma2_rn(__fmul2_rn(__fmul2_rn(r2s, mone), y), y, one);
-            y = __ffma2_rn(__fmul2_rn(half, y), h, y);
-            const float2 r2inv = __fmul2_rn(y, y);
-            const float2 r6 = __fmul2_rn(__fmul2_rn(r2inv, r2inv), r2inv);
-            const float2 pa = __ldg(&lj[T.x + tj]), pb = __ldg(&lj[T.y + tj]);
-            const float2 t6 = __fmul2_rn(og_f2(pa.x, pb.x), r6);
-            const float2 t12 = __fmul2_rn(__fmul2_rn(og_f2(pa.y, pb.y), r6), r6);
-            const float2 cc = __fmul2_rn(og_f2(B.z, B.w), qj);
-            const float2 on = og_f2(act_a ? 1.f : 0.f, act_b ? 1.f : 0.f);
-            float2 wc;
-            if (!GEN) {
-                wc = __ffma2_rn(__fmul2_rn(cc, mone), __ffma2_rn(y, r2inv, nfco),
-                                __fmul2_rn(r2inv, __ffma2_rn(t12, m12, __fmul2_rn(six, t6))));
-                wc = __fmul2_rn(wc, on);
-                if (ENE) {
-                    const float2 pv = __fmul2_rn(__ffma2_rn(t6, mone, t12), on);
-                    const float2 pe = __fmul2_rn(__fmul2_rn(cc, __ffma2_rn(bco, r2s, __fadd2_rn(y, nzcore))), on);
-                    av = __fadd2_rn(av, pv);
-                    ae = __fadd2_rn(ae, pe);
-                }
-            } else {
-                float w2[2], v2[2], e2[2];
-#pragma unroll
-                for (int hh = 0; hh < 2; hh++) {
-                    const float r2h = hh ? r2s.y : r2s.x, yh = hh ? y.y : y.x;
-                    const float r2i = yh * yh, r3i = yh * r2i, rr = r2h * yh;
-                    const float t6h = hh ? t6.y : t6.x, t12h = hh ? t12.y : t12.x;
-                    float ev = t12h - t6h, wl = r2i * (6.f * t6h - 12.f * t12h);
-                    if (E.hps) {  // ForceField.cpp:380-391
-                        const float2 hp = __ldg(&hps[(hh ? T.y : T.x) + tj]);
-                        if (rr > hp.x) {
-                            ev *= hp.y;
-                            wl *= hp.y;
-                        } else {
-                            ev += (1.f - hp.y) * E.hps_eps;
-                        }
-                    }
-                    float ee, ge;
-                    og_ele_pair(E, rr, r2h, yh, r2i, r3i, hh ? cc.y : cc.x, ee, ge);
-                    w2[hh] = wl + ge;
-                    v2[hh] = ev;
-                    e2[hh] = ee;
-                }
-                wc = __fmul2_rn(og_f2(w2[0], w2[1]), on);
-                if (ENE) {
-                    av = __fadd2_rn(av, __fmul2_rn(og_f2(v2[0], v2[1]), on));
-                    ae = __fadd2_rn(ae, __fmul2_rn(og_f2(e2[0], e2[1]), on));
-                }
-            }
-            if (VIR) n_act += (act_a ? 1 : 0) + (act_b ? 1 : 0);
-            const float2 wx = __fmul2_rn(wc, dx), wy = __fmul2_rn(wc, dy), wz = __fmul2_rn(wc, dz);
-            fx[p] = __fadd2_rn(fx[p], wx);
-            fy[p] = __fadd2_rn(fy[p], wy);
-            fz[p] = __fadd2_rn(fz[p], wz);
-            wjx = __fadd2_rn(wjx, wx);
-            wjy = __fadd2_rn(wjy, wy);
-            wjz = __fadd2_rn(wjz, wz);
-        }
-        if (ENE) {
-            dv += (double)av.x + (double)av.y;
-            de += (double)ae.x + (double)ae.y;
-            av = ae = og_f2(0.f, 0.f);
-        }
-        const float sx = -(wjx.x + wjx.y), sy = -(wjy.x + wjy.y), sz = -(wjz.x + wjz.y);
-        if (active && (sx != 0.f || sy != 0.f || sz != 0.f)) {
-            unsigned long long *fj = frc + 3 * (size_t)ji.y;
-            atomicAdd(fj + 0, (unsigned long long)__float2ll_rn(sx * (float)OG_FIX_SCALE));
-            atomicAdd(fj + 1, (unsigned long long)__float2ll_rn(sy * (float)OG_FIX_SCALE));
-            atomicAdd(fj + 2, (unsigned long long)__float2ll_rn(sz * (float)OG_FIX_SCALE));
-            const int img = ji.w;
-            if (VIR && img != 0) {
-                const double sh[3] = {(img & 1) ? -S.L[0] : ((img & 2) ? S.L[0] : 0.0),
-                                      (img & 4) ? -S.L[1] : ((img & 8) ? S.L[1] : 0.0),
-                                      (img & 16) ? -S.L[2] : ((img & 32) ? S.L[2] : 0.0)};
-                const double fjv[3] = {-(double)sx, -(double)sy, -(double)sz};
-                for (int a = 0; a < 3; a++)
-                    for (int b = 0; b < 3; b++) v[a * 3 + b] += sh[a] * fjv[b];
-            }
-        }
+        og_eval_j<VIR, ENE, GEN>(A, active, xj, ji.x, (unsigned)ji.z, ji.y, ji.w, s_i[wib], K, S, E, lj, hps, frc);
         __syncwarp();
         q_head = (q_head + n_take) & (OG_JQ - 1);
         q_len -= n_take;
@@ -937,48 +1036,163 @@ k_pair_ljzd_jq(const int *__restrict__ counters, const int *__restrict__ cell_sy
         __syncwarp();  // the next chunk's survivors overwrite this chunk's
     }
     if (q_len > 0) drain(q_len);
-    double mine[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-    for (int p = 0; p < OG_CELL / 2; p++) {
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            double w3[3] = {(double)(h ? fx[p].y : fx[p].x), (double)(h ? fy[p].y : fy[p].x),
-                            (double)(h ? fz[p].y : fz[p].x)};
-#pragma unroll
-            for (int d = 0; d < 3; d++) {
-                double x = w3[d];
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-                if (lane == 2 * p + h) mine[d] = x;
+    og_flush_icell<VIR, ENE>(A, c1, lane, frc, cell_acc);
+}
+
+// ---------------------------------------------------------------------------------------------
+// j-list: the j-queue's two culls (cell2 box, then j atom, against cell1's box) done once per
+// list build instead of every step.  k_jl_build keeps, per cell1, the (j atom, cell pair)
+// entries whose j atom lies within cutoff + reach of cell1's bounding box; the step kernel
+// k_pair_ljzd_jl streams them, 32 per round, one per lane.  reach = 2 skin + 1e-3 A: while no
+// atom has moved farther than skin from the position the entries were built from (k_finish and
+// k_put_state check this every step against xq_ref and set the stale counter otherwise), a
+// dropped entry's pairs are farther apart than cutoff + 1e-3 A, so the step evaluates exactly
+// the pairs the j-queue kernel evaluates.  The build runs at the first step of every list and
+// after any stale mark; otherwise it returns at once.
+//
+// Entry: x = j slot | exclusion byte << 24 (slots below 2^24), y = cell-pair index.  Cell1's
+// entries start at 8 * cp_head[c1] (at most 8 per cell pair), with their count in jl_count.
+template <int NT>
+__global__ void __launch_bounds__(NT)
+k_jl_build(const int *__restrict__ counters, const int *__restrict__ cell_sys, const SysDev *__restrict__ sys,
+           const float4 *__restrict__ bbox, const float4 *__restrict__ xq, const int *__restrict__ cp_head,
+           const float4 *__restrict__ cp_shift, const unsigned long long *__restrict__ cp_mask, long long pair_cap,
+           float reach, int2 *__restrict__ jl, int *__restrict__ jl_count, float4 *__restrict__ xq_ref) {
+    if (counters[OG_CNT_JL_STALE] == 0) return;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    if (warp >= counters[OG_CNT_N_CELLS]) return;
+    const int c1 = warp;
+    const int jj = lane & 7, q = lane >> 3;
+    const SysDev &S = sys[cell_sys[c1]];
+    __shared__ float4 s_sp[NT / 32][32];
+    __shared__ uint2 s_m[NT / 32][32];
+    __shared__ int s_k[NT / 32][32];
+    if (lane < OG_CELL) xq_ref[c1 * OG_CELL + lane] = xq[c1 * OG_CELL + lane];
+    const float rb = sqrtf(S.cutoff2) + reach, rb2 = rb * rb;
+    const float4 b1l = bbox[2 * c1], b1h = bbox[2 * c1 + 1];
+    const long long k_beg = cp_head[c1];
+    const long long k_end = min((long long)cp_head[c1 + 1], pair_cap);
+    int2 *out = jl + 8 * k_beg;
+    int count = 0;
+    for (long long chunk = k_beg; chunk < k_end; chunk += 32) {
+        const long long kk = chunk + lane;
+        float4 sp = make_float4(0.f, 0.f, 0.f, 0.f);
+        unsigned long long m = ~0ull;
+        bool keep = false;
+        if (kk < k_end) {
+            sp = cp_shift[kk];
+            m = cp_mask[kk];
+            const int c2 = __float_as_int(sp.w);
+            const float4 l2 = bbox[2 * c2], h2 = bbox[2 * c2 + 1];
+            const float gx = fmaxf(0.f, fmaxf(l2.x + sp.x - b1h.x, b1l.x - (h2.x + sp.x)));
+            const float gy = fmaxf(0.f, fmaxf(l2.y + sp.y - b1h.y, b1l.y - (h2.y + sp.y)));
+            const float gz = fmaxf(0.f, fmaxf(l2.z + sp.z - b1h.z, b1l.z - (h2.z + sp.z)));
+            keep = gx * gx + gy * gy + gz * gz < rb2;
+        }
+        const unsigned ballot = __ballot_sync(0xffffffffu, keep);
+        const int n_keep = __popc(ballot);
+        if (keep) {
+            const int rank = __popc(ballot & ((1u << lane) - 1u));
+            s_sp[wib][rank] = sp;
+            s_m[wib][rank] = make_uint2((unsigned)m, (unsigned)(m >> 32));
+            s_k[wib][rank] = (int)kk;
+        }
+        __syncwarp();
+        for (int r = 0; r < n_keep; r += 4) {
+            const int idx = r + q;
+            const bool active = idx < n_keep;
+            float4 rsp = make_float4(0.f, 0.f, 0.f, 0.f);
+            unsigned long long rm = ~0ull;
+            int rk = 0;
+            if (active) {
+                rsp = s_sp[wib][idx];
+                const uint2 mm = s_m[wib][idx];
+                rm = ((unsigned long long)mm.y << 32) | mm.x;
+                rk = s_k[wib][idx];
             }
+            const int c2 = __float_as_int(rsp.w);
+            const unsigned skip = active ? (unsigned)(rm >> (jj * OG_CELL)) & 0xffu : 0xffu;
+            bool push = false;
+            if (active && skip != 0xffu) {
+                float4 xj = xq[c2 * OG_CELL + jj];
+                xj.x += rsp.x;
+                xj.y += rsp.y;
+                xj.z += rsp.z;
+                const float gx = fmaxf(0.f, fmaxf(xj.x - b1h.x, b1l.x - xj.x));
+                const float gy = fmaxf(0.f, fmaxf(xj.y - b1h.y, b1l.y - xj.y));
+                const float gz = fmaxf(0.f, fmaxf(xj.z - b1h.z, b1l.z - xj.z));
+                push = gx * gx + gy * gy + gz * gz < rb2;
+            }
+            const unsigned pb = __ballot_sync(0xffffffffu, push);
+            if (push)
+                out[count + __popc(pb & ((1u << lane) - 1u))] =
+                    make_int2((int)((unsigned)(c2 * OG_CELL + jj) | (skip << 24)), rk);
+            count += __popc(pb);
         }
+        __syncwarp();  // the next chunk's survivors overwrite this chunk's
     }
-    if (lane < OG_CELL && (mine[0] != 0.0 || mine[1] != 0.0 || mine[2] != 0.0)) {
-        unsigned long long *fa = frc + 3 * (size_t)(c1 * OG_CELL + lane);
-        atomicAdd(fa + 0, (unsigned long long)og_to_fix(mine[0]));
-        atomicAdd(fa + 1, (unsigned long long)og_to_fix(mine[1]));
-        atomicAdd(fa + 2, (unsigned long long)og_to_fix(mine[2]));
-    }
-    if (!ENE) return;
-    double e_vdw = dv, e_ele = de;
-    for (int o = 16; o > 0; o >>= 1) {
-        e_vdw += __shfl_xor_sync(0xffffffffu, e_vdw, o);
-        e_ele += __shfl_xor_sync(0xffffffffu, e_ele, o);
-    }
-    if (VIR) {
-        for (int k = 0; k < 9; k++)
-            for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
-        for (int o = 16; o > 0; o >>= 1) n_act += __shfl_xor_sync(0xffffffffu, n_act, o);
-    }
-    if (lane == 0) {
-        double *acc = cell_acc + (size_t)c1 * OG_CELL_ACC;
-        acc[0] = e_vdw;
-        acc[1] = e_ele;
-        if (VIR) {
-            for (int k = 0; k < 9; k++) acc[2 + k] = v[k];
-            acc[11] = (double)n_act;
+    if (lane == 0) jl_count[c1] = count;
+}
+
+// The step kernel over the j lists (see k_jl_build).  Each round, lane l takes entry r + l.
+// The first thread clears the stale counter: this launch follows the build that consumed it.
+template <bool VIR, bool ENE, int MINB, int NT = 128, bool GEN = false>
+__global__ void __launch_bounds__(NT, MINB)
+k_pair_ljzd_jl(int *__restrict__ counters, const int *__restrict__ cell_sys, const SysDev *__restrict__ sys,
+               const float4 *__restrict__ xq, const int *__restrict__ slot_type, const int *__restrict__ cp_head,
+               const float4 *__restrict__ cp_shift, const int2 *__restrict__ cp_c2img, const int2 *__restrict__ jl,
+               const int *__restrict__ jl_count, const float2 *__restrict__ lj, unsigned long long *__restrict__ frc,
+               double *__restrict__ cell_acc, const EleDev *__restrict__ ele, const float2 *__restrict__ hps) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    if (blockIdx.x == 0 && threadIdx.x == 0) counters[OG_CNT_JL_STALE] = 0;
+    const int n_cells = counters[OG_CNT_N_CELLS];
+    if (warp >= n_cells) return;
+    const int c1 = warp;
+    const SysDev &S = sys[cell_sys[c1]];
+    const EleDev &E = ele[GEN ? cell_sys[c1] : 0];
+    __shared__ OgICell s_i[NT / 32];
+    og_load_icell(s_i[wib], c1, lane, xq, slot_type, S);
+    const OgZdConst K = og_zd_const(S);
+    OgIAcc<VIR> A;
+    og_iacc_zero(A);
+    const int2 *ent = jl + 8LL * cp_head[c1];
+    const int n = jl_count[c1];
+    // entries are loaded two rounds ahead and their gathers issued one round ahead, so neither
+    // load of the entry -> position chain is waited on in the round that issues it
+    float4 g_xj = make_float4(0.f, 0.f, 0.f, 0.f);
+    int g_tj = 0, g_slot = 0, g_img = 0;
+    unsigned g_skip = 0xffu;
+    auto gather = [&](int2 e, bool ok) {
+        if (ok) {
+            g_slot = e.x & 0xffffff;
+            g_skip = (unsigned)e.x >> 24;
+            const float4 sp = cp_shift[e.y];
+            g_xj = xq[g_slot];
+            g_tj = slot_type[g_slot];
+            g_xj.x += sp.x;
+            g_xj.y += sp.y;
+            g_xj.z += sp.z;
+            if (VIR) g_img = cp_c2img[e.y].y;
         }
+    };
+    int2 e_ahead = make_int2(0, 0);
+    if (lane < n) gather(ent[lane], true);
+    if (32 + lane < n) e_ahead = ent[32 + lane];
+    for (int r = 0; r < n; r += 32) {
+        const bool active = r + lane < n;
+        const float4 xj = g_xj;
+        const int tj = g_tj, slot = g_slot, img = g_img;
+        const unsigned skip = active ? g_skip : 0xffu;
+        const int2 e1 = e_ahead;
+        if (r + 64 + lane < n) e_ahead = ent[r + 64 + lane];
+        gather(e1, r + 32 + lane < n);
+        og_eval_j<VIR, ENE, GEN>(A, active, xj, tj, skip, slot, img, s_i[wib], K, S, E, lj, hps, frc);
     }
+    og_flush_icell<VIR, ENE>(A, c1, lane, frc, cell_acc);
 }
 
 #define OG_PAIR_ARGS_DECL                                                                                   \
@@ -1004,6 +1218,15 @@ template __global__ void k_pair_ljzd_jq<false, false, 5, 128, false>(OG_JQ_ARGS_
 template __global__ void k_pair_ljzd_jq<true, true, 2, 256, true>(OG_JQ_ARGS_DECL);
 template __global__ void k_pair_ljzd_jq<false, true, 5, 128, true>(OG_JQ_ARGS_DECL);
 template __global__ void k_pair_ljzd_jq<false, false, 5, 128, true>(OG_JQ_ARGS_DECL);
+#define OG_JL_ARGS_DECL                                                                                    \
+    int *, const int *, const SysDev *, const float4 *, const int *, const int *, const float4 *, const int2 *, \
+        const int2 *, const int *, const float2 *, unsigned long long *, double *, const EleDev *, const float2 *
+template __global__ void k_pair_ljzd_jl<true, true, 2, 128, false>(OG_JL_ARGS_DECL);
+template __global__ void k_pair_ljzd_jl<false, true, 5, 128, false>(OG_JL_ARGS_DECL);
+template __global__ void k_pair_ljzd_jl<false, false, 5, 128, false>(OG_JL_ARGS_DECL);
+template __global__ void k_jl_build<128>(const int *, const int *, const SysDev *, const float4 *, const float4 *,
+                                         const int *, const float4 *, const unsigned long long *, long long, float,
+                                         int2 *, int *, float4 *);
 
 template __global__ void k_pair_ljzd<true, 2>(const int *, const int *, const SysDev *, const float4 *,
                                                 const float4 *, const int *, const int *, const float4 *,

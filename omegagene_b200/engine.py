@@ -23,7 +23,7 @@ LIB_PATH = os.path.join(HERE, "libomegagene_b200.so")
 ENERGY_NAMES = ["vdw", "ele", "bond", "angle", "potential", "kinetic", "temperature", "total", "ele_excess",
                 "ele_self", "mcmd_factor", "torsion", "improper", "vdw14", "ele14"]
 N_ENERGY = len(ENERGY_NAMES)
-N_PAIR_VARIANTS = 10  # OG_N_PAIR_VARIANTS
+N_PAIR_VARIANTS = 11  # OG_N_PAIR_VARIANTS
 
 
 class OgError(RuntimeError):

@@ -1,0 +1,91 @@
+"""The pair variant over j lists (variant 10) against the j-queue variant (9) and the oracle.
+
+Variant 10 culls the j atoms of each cell's cell pairs once per list build, with a margin of
+0.5 A (twice the 0.25 A skin), and rebuilds its lists whenever an atom has moved farther than
+the skin since.  It must evaluate exactly the pairs variant 9 evaluates; the two differ only
+in the order in which FP32 partial sums are added.
+* Over three list intervals the two give the same trajectory and the oracle's energies.  The
+  order of FP32 partial sums alone separates them by ~4e-7 A after 30 steps (measured), so
+  positions are compared within 1e-5 A.
+* One molecule moved by 1 A through og_put_state in the middle of an interval (no cell-pair
+  list rebuild) brings pairs that were beyond cutoff + margin inside the cutoff: two steps
+  later, positions still agree with variant 9's to 1e-6 A.  The ~50 pairs per moved atom that
+  lists left stale would miss (11.5-12 A, ~0.1 kcal/mol/A each) would move its hydrogens by
+  ~1e-3 A.
+* An og_put_state of unchanged coordinates (the end-to-end protocol) keeps the lists, and the
+  step after it matches variant 9's.
+"""
+import numpy as np
+import pytest
+
+from omegagene_b200 import engine, systems
+from oracle import ogo
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(**kw):
+    p = dict(engine.DEFAULT_PARAMS)
+    p.update(nsgrid_update_intvl=10, time_step=2.0, **kw)
+    return p
+
+
+def _engine(s, p, variant):
+    eng = engine.Engine(0)
+    eng.set_tuning(variant)
+    eng.add_system(s, p)
+    eng.finalize()
+    return eng
+
+
+def test_jlist_trajectory_matches_jqueue_and_oracle():
+    s = systems.water_system(3000, box=44.8, seed=0, lattice_m=15)
+    p = _params(thermostat="scaling", temperature=300.0)
+    n = 30
+    out = {}
+    for v in (9, 10):
+        eng = _engine(s, p, v)
+        assert eng.tuning()["pair_variant"] == v
+        eng.set_trace(n)
+        eng.step(n)
+        out[v] = (eng.get_state(0), eng.get_trace(n)[:, 0, :])
+        eng.close()
+    (c9, v9), t9 = out[9]
+    (c10, v10), t10 = out[10]
+    assert np.max(np.abs(c10 - c9)) < 1e-5
+    assert np.max(np.abs(v10 - v9)) < 1e-3
+    names = engine.ENERGY_NAMES
+    for k in ("potential", "vdw", "ele"):
+        i = names.index(k)
+        assert np.max(np.abs(t10[:, i] - t9[:, i]) / np.abs(t9[:, i])) < 1e-6, k
+    md = ogo.OracleMD(s, p)
+    ref = [md.step() for _ in range(n)]
+    for i, r in enumerate(ref):
+        for k in ("potential", "vdw", "ele", "kinetic"):
+            got = t10[i, names.index(k)]
+            assert abs(got - r[k]) <= 1e-5 * abs(r[k]) + 5e-3, (i, k, got, r[k])
+
+
+def _put(eng, crd):
+    buf = np.ascontiguousarray(crd, np.float64).reshape(-1)
+    eng.put_state_ptr(0, buf.ctypes.data, 0)
+    eng.synchronize()
+
+
+@pytest.mark.parametrize("shift", [0.0, 1.0])
+def test_jlist_rebuilds_after_a_move_beyond_the_skin(shift):
+    s = systems.water_system(3000, box=44.8, seed=0, lattice_m=15)
+    p = _params(thermostat="none")
+    res = {}
+    for v in (9, 10):
+        eng = _engine(s, p, v)
+        eng.step(4)  # mid-interval: the next list build is at step 10
+        crd, _ = eng.get_state(0)
+        crd = crd.copy()
+        crd[300:303, 0] += shift  # one water molecule
+        _put(eng, crd)
+        eng.step(2)
+        res[v] = eng.get_state(0)
+        eng.close()
+    assert np.max(np.abs(res[10][0] - res[9][0])) < 1e-6
+    assert np.max(np.abs(res[10][1] - res[9][1])) < 1e-3
