@@ -38,6 +38,10 @@ INTVL = 10
 VMCMD_TRANS_INTERVAL = 100  # V-McMD walkers: steps between virtual-state transition trials
 EQUIL_STEPS = 2000  # 1M water: untimed relaxation (0.5 fs, 300 K velocity rescaling) before the NVE run
 N_WATERS = 333334
+# the step's pair kernel by autotuned variant; pair_kernel_ms brackets everything one launch
+# issues (variant 10: its j-list build, which does work at the first step of a list)
+PAIR_KERNELS = {9: "k_pair_ljzd_jq<0,0,5,128,0>",
+                10: "k_pair_ljzd_jl<0,0,5,128,0> (+ k_jl_build at list builds)"}
 BOX = 215.5
 LATTICE = 70
 FLOP_PER_PAIR = 40  # FP32 FLOP per interacting pair (sub 3, r2 5, rsqrt 1, powers 4, LJ 5, ZD 6, force 3, accum 6, energy 7)
@@ -223,13 +227,14 @@ def run_ours(args, world, rank, local, pg):
     p.update(nsgrid_update_intvl=INTVL, time_step=DT_FS, thermostat="none", com_cancel_groups=["all"])
     # the lattice start melts and heats: relax it (untimed) with velocity rescaling to 300 K at
     # 0.5 fs, so that the NVE run starts from liquid water
-    eq = engine.Engine(local)
-    eq.add_system(s, dict(p, thermostat="scaling", temperature=300.0, time_step=0.5))
-    eq.finalize()
-    eq.step(EQUIL_STEPS)
-    crd, vel = eq.get_state(0)
-    eq.close()
-    s = dict(s, crd=crd, vel=vel)
+    if args.equil_steps > 0:
+        eq = engine.Engine(local)
+        eq.add_system(s, dict(p, thermostat="scaling", temperature=300.0, time_step=0.5))
+        eq.finalize()
+        eq.step(args.equil_steps)
+        crd, vel = eq.get_state(0)
+        eq.close()
+        s = dict(s, crd=crd, vel=vel)
     eng = engine.Engine(local)
     eng.add_system(s, p)
     eng.finalize()
@@ -316,7 +321,7 @@ def run_ours(args, world, rank, local, pg):
     tp = os.path.join(ROOT, "profiles", "pair_kernel_traffic.json")
     if os.path.exists(tp):
         try:
-            tj = json.load(open(tp))
+            tj = json.load(open(tp))["variants"][str(tuning["pair_variant"])]
             traffic = tj["dram_bytes_per_launch_per_1M_atoms"] * n_atoms / 1e6
         except Exception:
             traffic = None
@@ -331,7 +336,8 @@ def run_ours(args, world, rank, local, pg):
                                  "energies"},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp32_peak, "traffic": traffic,
-                     "kernel": "k_pair_ljzd", "pair_kernel_ms": pair_ms, "interacting_pairs": n_int,
+                     "kernel": PAIR_KERNELS.get(tuning["pair_variant"], "k_pair_ljzd"), "pair_kernel_ms": pair_ms,
+                     "interacting_pairs": n_int,
                      "flop_per_pair": FLOP_PER_PAIR, "autotune": tuning,
                      "cell_pairs": n_cell_pairs,
                      "cluster_efficiency": n_int / (64.0 * n_cell_pairs) if n_cell_pairs else None,
@@ -569,6 +575,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--equil-steps", type=int, default=EQUIL_STEPS,
+                    help="water1m: untimed relaxation steps before the NVE run (0: start from the lattice, "
+                         "e.g. for a short launch list under a profiler)")
     ap.add_argument("--workload", default="water1m", choices=["water1m", "serve", "mcmd"],
                     help="water1m: the 1M-atom step (default); serve: batched job stream; mcmd: McMD walkers")
     ap.add_argument("--jobs", type=int, default=256)

@@ -264,13 +264,17 @@ og_status og_get_flags(og_engine *e, int32_t *flags);
  * with sm_100 packed FP32x2 arithmetic (two i atoms per instruction) at 128/80; 7-8 = packed
  * j-major fed by a per-warp queue of the j atoms within the cutoff of the i cell, at 128/80;
  * 9 = the same at 102 registers in blocks of 128 threads; 10 = packed j-major over j lists
- * culled once per list build (cutoff + 0.5 A around the i cell, rebuilt whenever an atom has
- * moved 0.25 A since), at 102 registers (engines with fewer than 2^24 atom slots). */
+ * culled once per list build (cutoff + 0.7 A around the i cell, rebuilt whenever an atom has
+ * moved 0.35 A since), at 102 registers (engines with fewer than 2^24 atom slots). */
 #define OG_N_PAIR_VARIANTS 11
 /* Autotuner result: the pair-kernel variant in use and the best time of each variant on the
  * first list, in ms (variant_ms[OG_N_PAIR_VARIANTS]); for variant 10 the time is one step's
  * launch plus its share of the j-list build (build time / nsgrid_update_intvl). */
 og_status og_get_tuning(og_engine *e, int32_t *pair_variant, double *variant_ms);
+/* Pair variant 10: j-list builds since og_finalize -- one at each cell-pair list build, plus one
+ * whenever an atom has moved farther than the skin (0.35 A, or OG_JL_SKIN in the environment)
+ * since the last.  0 for the other variants. */
+og_status og_get_jlist_builds(og_engine *e, int64_t *n_builds);
 /* Fixes the pair-kernel variant (0..OG_N_PAIR_VARIANTS-1) before og_finalize and skips the autotuner, e.g. when a
  * serving loop re-creates engines for new batches; -1 restores autotuning.  No counterpart in
  * the reference, which has one pair kernel. */

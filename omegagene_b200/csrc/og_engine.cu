@@ -62,7 +62,7 @@ __global__ void k_pair_ljzd_jl(int *, const int *, const SysDev *, const float4 
                                const float4 *, const int2 *, const int2 *, const int *, const float2 *,
                                unsigned long long *, double *, const EleDev *, const float2 *);
 template <int NT>
-__global__ void k_jl_build(const int *, const int *, const SysDev *, const float4 *, const float4 *, const int *,
+__global__ void k_jl_build(int *, const int *, const SysDev *, const float4 *, const float4 *, const int *,
                            const float4 *, const unsigned long long *, long long, float, int2 *, int *, float4 *);
 __global__ void k_cell_bbox(const int *, int, const float4 *, const unsigned char *, float4 *);
 // og_integrate.cu
@@ -136,9 +136,10 @@ __global__ void k_copy_double(double *dst, const double *src, long long n) {
 
 using namespace og;
 
-// The pair variant over j lists, and the displacement (A) after which its lists are rebuilt.
+// The pair variant over j lists, and the default displacement (A) after which its lists are
+// rebuilt (OG_JL_SKIN in the environment overrides it, 0.05-2 A).
 #define OG_JL_VARIANT 10
-#define OG_JL_SKIN 0.25f
+#define OG_JL_SKIN 0.35f
 
 namespace {
 
@@ -230,6 +231,7 @@ struct og_engine {
     int2 *d_jl = nullptr;
     int *d_jl_count = nullptr;
     float4 *d_xq_ref = nullptr;
+    float jl_skin = OG_JL_SKIN;
     unsigned long long *d_frc = nullptr;
     int *d_uni_lo = nullptr, *d_uni_hi = nullptr;
     int *d_count = nullptr, *d_offset = nullptr;
@@ -775,9 +777,9 @@ og_status launch_pair(og_engine *e, bool vir, int variant, bool ene) {
     }
     if (variant == OG_JL_VARIANT) {
         if (!e->d_jl) return fail(e, OG_ERR_STATE, "pair variant %d without its j lists", OG_JL_VARIANT);
-        k_jl_build<128><<<2 * nb, 128, 0, st>>>(e->d_counters, e->d_cell_sys, e->d_sys, e->d_bbox, e->d_xq,
+        k_jl_build<256><<<nb, 256, 0, st>>>(e->d_counters, e->d_cell_sys, e->d_sys, e->d_bbox, e->d_xq,
                                                  e->d_cp_head, e->d_cp_shift, e->d_cp_mask, e->pair_cap,
-                                                 2.0f * OG_JL_SKIN + 1e-3f, e->d_jl, e->d_jl_count, e->d_xq_ref);
+                                                 2.0f * e->jl_skin + 1e-3f, e->d_jl, e->d_jl_count, e->d_xq_ref);
         LAUNCH_CHECK();
         if (vir) k_pair_ljzd_jl<true, true, 2, 128, false><<<2 * nb, 128, 0, st>>>(JL_ARGS);
         else if (ene) k_pair_ljzd_jl<false, true, 5, 128, false><<<2 * nb, 128, 0, st>>>(JL_ARGS);
@@ -1115,7 +1117,7 @@ og_status run_step(og_engine *e, bool ene) {
                                                        e->d_crd_prev, e->d_vel, e->d_vel_next, e->d_atom_slot,
                                                        e->d_slot_crd, e->d_cell_origin, e->d_xq, e->d_mass, e->d_ke,
                                                        e->d_counters, e->d_sys_fault, e->d_xq_ref,
-                                                       OG_JL_SKIN * OG_JL_SKIN);
+                                                       e->jl_skin * e->jl_skin);
     LAUNCH_CHECK();
     if ((s = seg_sum<1>(e, e->d_ke, 1, 0, e->d_seg_atoms, e->mc_atoms, e->d_sys_acc, OG_ACC_SIZE, OG_ACC_KIN, 0)))
         return s;
@@ -1315,6 +1317,8 @@ og_status jl_alloc(og_engine *e) {
     if ((long long)e->slots_cap >= (1ll << 24))
         return fail(e, OG_ERR_INVALID, "pair variant %d needs fewer than 2^24 atom slots (engine has %d)",
                     OG_JL_VARIANT, e->slots_cap);
+    const char *env = getenv("OG_JL_SKIN");
+    if (env && *env) e->jl_skin = std::min(2.0f, std::max(0.05f, (float)atof(env)));
     og_status s;
     if ((s = dalloc(e, &e->d_jl, 8 * (size_t)e->pair_cap)) || (s = dalloc(e, &e->d_jl_count, (size_t)e->cells_cap)) ||
         (s = dalloc(e, &e->d_xq_ref, (size_t)e->slots_cap)))
@@ -2545,7 +2549,7 @@ extern "C" og_status og_put_state(og_engine *e, int32_t sys, const double *crd, 
                                                                 crd ? sc : nullptr, vel_next ? sv : nullptr, e->d_crd,
                                                                 e->d_vel_next, e->d_atom_slot, e->d_slot_crd,
                                                                 e->d_cell_origin, e->d_xq, e->d_xq_ref,
-                                                                OG_JL_SKIN * OG_JL_SKIN, e->d_counters);
+                                                                e->jl_skin * e->jl_skin, e->d_counters);
     LAUNCH_CHECK();
     return OG_OK;
 }
@@ -2563,6 +2567,15 @@ extern "C" og_status og_get_state_async(og_engine *e, int32_t sys, double *crd, 
     if (energies)
         CK(cudaMemcpyAsync(energies, e->d_energies + OG_N_ENERGY * (size_t)sys, sizeof(double) * OG_N_ENERGY,
                            cudaMemcpyDeviceToHost, e->stream));
+    return OG_OK;
+}
+
+extern "C" og_status og_get_jlist_builds(og_engine *e, int64_t *n_builds) {
+    if (!e || !e->finalized || !n_builds) return OG_ERR_INVALID;
+    int c[OG_CNT_SIZE];
+    og_status s = read_counters(e, c);
+    if (s) return s;
+    *n_builds = c[OG_CNT_JL_BUILDS];
     return OG_OK;
 }
 

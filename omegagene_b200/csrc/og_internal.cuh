@@ -41,6 +41,7 @@
 #define OG_CNT_FLAGS 2
 #define OG_CNT_ACTIVE 3
 #define OG_CNT_JL_STALE 4   // nonzero: the j lists must be rebuilt before the next pair launch
+#define OG_CNT_JL_BUILDS 5  // j-list builds so far
 #define OG_CNT_SIZE 8
 
 // Per-system constants (read-only during a step).

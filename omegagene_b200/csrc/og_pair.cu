@@ -1054,21 +1054,22 @@ k_pair_ljzd_jq(const int *__restrict__ counters, const int *__restrict__ cell_sy
 // entries start at 8 * cp_head[c1] (at most 8 per cell pair), with their count in jl_count.
 template <int NT>
 __global__ void __launch_bounds__(NT)
-k_jl_build(const int *__restrict__ counters, const int *__restrict__ cell_sys, const SysDev *__restrict__ sys,
+k_jl_build(int *__restrict__ counters, const int *__restrict__ cell_sys, const SysDev *__restrict__ sys,
            const float4 *__restrict__ bbox, const float4 *__restrict__ xq, const int *__restrict__ cp_head,
            const float4 *__restrict__ cp_shift, const unsigned long long *__restrict__ cp_mask, long long pair_cap,
            float reach, int2 *__restrict__ jl, int *__restrict__ jl_count, float4 *__restrict__ xq_ref) {
     if (counters[OG_CNT_JL_STALE] == 0) return;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (blockIdx.x == 0 && threadIdx.x == 0) counters[OG_CNT_JL_BUILDS]++;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    if (warp >= counters[OG_CNT_N_CELLS]) return;
-    const int c1 = warp;
     const int jj = lane & 7, q = lane >> 3;
-    const SysDev &S = sys[cell_sys[c1]];
+    const int n_cells = counters[OG_CNT_N_CELLS];
     __shared__ float4 s_sp[NT / 32][32];
     __shared__ uint2 s_m[NT / 32][32];
     __shared__ int s_k[NT / 32][32];
+    const int c1 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (c1 >= n_cells) return;
+    const SysDev &S = sys[cell_sys[c1]];
     if (lane < OG_CELL) xq_ref[c1 * OG_CELL + lane] = xq[c1 * OG_CELL + lane];
     const float rb = sqrtf(S.cutoff2) + reach, rb2 = rb * rb;
     const float4 b1l = bbox[2 * c1], b1h = bbox[2 * c1 + 1];
@@ -1224,7 +1225,7 @@ template __global__ void k_pair_ljzd_jq<false, false, 5, 128, true>(OG_JQ_ARGS_D
 template __global__ void k_pair_ljzd_jl<true, true, 2, 128, false>(OG_JL_ARGS_DECL);
 template __global__ void k_pair_ljzd_jl<false, true, 5, 128, false>(OG_JL_ARGS_DECL);
 template __global__ void k_pair_ljzd_jl<false, false, 5, 128, false>(OG_JL_ARGS_DECL);
-template __global__ void k_jl_build<128>(const int *, const int *, const SysDev *, const float4 *, const float4 *,
+template __global__ void k_jl_build<256>(int *, const int *, const SysDev *, const float4 *, const float4 *,
                                          const int *, const float4 *, const unsigned long long *, long long, float,
                                          int2 *, int *, float4 *);
 

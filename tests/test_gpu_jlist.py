@@ -1,7 +1,7 @@
 """The pair variant over j lists (variant 10) against the j-queue variant (9) and the oracle.
 
 Variant 10 culls the j atoms of each cell's cell pairs once per list build, with a margin of
-0.5 A (twice the 0.25 A skin), and rebuilds its lists whenever an atom has moved farther than
+0.7 A (twice the 0.35 A skin), and rebuilds its lists whenever an atom has moved farther than
 the skin since.  It must evaluate exactly the pairs variant 9 evaluates; the two differ only
 in the order in which FP32 partial sums are added.
 * Over three list intervals the two give the same trajectory and the oracle's energies.  The
