@@ -8,12 +8,14 @@ in the order in which FP32 partial sums are added.
   order of FP32 partial sums alone separates them by ~4e-7 A after 30 steps (measured), so
   positions are compared within 1e-5 A.
 * One molecule moved by 1 A through og_put_state in the middle of an interval (no cell-pair
-  list rebuild) brings pairs that were beyond cutoff + margin inside the cutoff: two steps
-  later, positions still agree with variant 9's to 1e-6 A.  The ~50 pairs per moved atom that
-  lists left stale would miss (11.5-12 A, ~0.1 kcal/mol/A each) would move its hydrogens by
-  ~1e-3 A.
+  list rebuild) brings pairs that were beyond cutoff + margin inside the cutoff: the j lists are
+  rebuilt, and two steps later positions still agree with variant 9's to 1e-6 A.  The ~50 pairs
+  per moved atom that stale lists would miss (11.5-12 A, ~0.1 kcal/mol/A each) would move its
+  hydrogens by ~1e-3 A.
 * An og_put_state of unchanged coordinates (the end-to-end protocol) keeps the lists, and the
   step after it matches variant 9's.
+* Every atom translated by 0.7 A (9,000 and 18,000 atoms): the lists are rebuilt and the step
+  matches variant 9, energies included.
 """
 import numpy as np
 import pytest
@@ -83,9 +85,36 @@ def test_jlist_rebuilds_after_a_move_beyond_the_skin(shift):
         crd, _ = eng.get_state(0)
         crd = crd.copy()
         crd[300:303, 0] += shift  # one water molecule
+        b0 = eng.jlist_builds()
         _put(eng, crd)
         eng.step(2)
         res[v] = eng.get_state(0)
+        if v == 10 and shift > 0.35:
+            assert eng.jlist_builds() > b0  # the move beyond the skin rebuilt the j lists
         eng.close()
     assert np.max(np.abs(res[10][0] - res[9][0])) < 1e-6
     assert np.max(np.abs(res[10][1] - res[9][1])) < 1e-3
+
+
+@pytest.mark.parametrize("n_waters", [3000, 6000])
+def test_every_atom_moved_beyond_the_skin(n_waters):
+    box = 44.8 * (n_waters / 3000) ** (1 / 3)
+    s = systems.water_system(n_waters, box=box, seed=1, lattice_m=int(np.ceil(n_waters ** (1 / 3))) + 1)
+    p = _params(thermostat="none")
+    res = {}
+    for v in (9, 10):
+        eng = _engine(s, p, v)
+        eng.step(4)
+        crd, _ = eng.get_state(0)
+        crd = crd + np.array([0.7, 0.3, -0.4]) * 0.7 / np.sqrt(0.74)  # every atom moves 0.7 A
+        b0 = eng.jlist_builds()
+        _put(eng, crd)
+        eng.step(2)
+        res[v] = eng.get_state(0) + (eng.get_energies(0),)
+        if v == 10:
+            assert eng.jlist_builds() > b0
+        eng.close()
+    assert np.max(np.abs(res[10][0] - res[9][0])) < 1e-6
+    assert np.max(np.abs(res[10][1] - res[9][1])) < 1e-3
+    for k in ("potential", "vdw", "ele"):
+        assert abs(res[10][2][k] - res[9][2][k]) <= 1e-6 * abs(res[9][2][k]), k
