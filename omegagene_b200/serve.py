@@ -16,6 +16,15 @@ A job's trajectory is therefore the one it would have had alone. The engine's fo
 fixed-point sums and its reductions are per system, so the match is exact;
 tests/test_gpu_serve.py checks it.
 
+The next batch is built while the current window runs (prepare_ahead): which jobs finish at the
+window's end and which queued jobs the rules admit are known when the window starts, so a
+background thread creates and finalizes that engine, with the continuing jobs' step numbers and
+placeholder coordinates; when the window ends as planned, their positions and velocities are
+set with og_set_state (the list is built from them at the first step) and the engine takes over.
+The result is the same engine the boundary would have built.  A window that faults, a job
+arriving that the rules would admit, or a V-McMD job in the batch (its generator state is only
+known at the boundary) falls back to building the batch at the boundary.
+
 A job whose system faults (a coordinate leaves the box or turns non-finite) is retired as failed
 with its state at the start of the window; og_step undoes the window for every job, and the
 others are stepped again in a new engine, with the results they would have had anyway.
@@ -24,6 +33,7 @@ Latency of a job = completion time - arrival time (wall clock). Throughput = ato
 jobs / (last completion - first arrival).
 """
 import collections
+import concurrent.futures
 import time
 
 import numpy as np
@@ -80,10 +90,11 @@ class Job:
 
 class Server:
     def __init__(self, device=0, hbm_budget_bytes=None, max_jobs=64, window=100, pair_variant="auto",
-                 clock=time.perf_counter, sleep=time.sleep, engine_factory=None):
+                 clock=time.perf_counter, sleep=time.sleep, engine_factory=None, prepare_ahead=True):
         """pair_variant: a fixed pair-kernel variant, or "auto": the first engine autotunes and
         every later engine reuses its choice, so a job keeps one kernel (and bitwise results)
-        across re-formed batches."""
+        across re-formed batches.  prepare_ahead: build the next batch's engine during the
+        current window when the next batch is known (see the module docstring)."""
         self.device = device
         if hbm_budget_bytes is None:
             import torch
@@ -96,23 +107,66 @@ class Server:
         self.clock = clock
         self.sleep = sleep
         self.n_relayouts = 0
+        self.n_prepared = 0  # relayouts served by an engine built during the previous window
         self.relayout_s = 0.0
+        self.prepare_ahead = prepare_ahead
         self.batch_sizes = []
         self.engine_factory = engine_factory or engine.Engine
 
     def _build(self, active):
-        eng = self.engine_factory(self.device)
-        if self.pair_variant != "auto":
-            eng.set_tuning(self.pair_variant)
-        for j in active:
-            s = dict(j.system)
-            s["crd"], s["vel"] = j.crd, j.vel
-            eng.add_system(s, j.params, j.mcmd, first_step=j.steps_done)
-        eng.finalize()
+        eng = self._engine_for([(j, j.crd, j.vel, j.steps_done) for j in active])
         if self.pair_variant == "auto":
             self.pair_variant = eng.tuning()["pair_variant"]
         self.n_relayouts += 1
         return eng
+
+    def _engine_for(self, members):
+        """A finalized engine of (job, coordinates, velocities, first step) members, in order."""
+        eng = self.engine_factory(self.device)
+        if self.pair_variant != "auto":
+            eng.set_tuning(self.pair_variant)
+        for j, crd, vel, first in members:
+            s = dict(j.system)
+            s["crd"], s["vel"] = crd, vel
+            eng.add_system(s, j.params, j.mcmd, first_step=first)
+        eng.finalize()
+        return eng
+
+    def _admits(self, running, queue):
+        """Queued jobs the rules admit next to the running ones, first come first served."""
+        used = sum(j.bytes for j in running)
+        out = []
+        for j in queue:
+            if len(running) + len(out) >= self.max_jobs or used + j.bytes > self.budget:
+                break
+            out.append(j)
+            used += j.bytes
+        return out
+
+    def _prepare(self, pool, active, queue, w):
+        """Starts building the batch that follows a window of w steps ending as planned: returns
+        (continuing jobs, admitted jobs, future of the engine), or None."""
+        if not self.prepare_ahead or self.pair_variant == "auto":
+            return None
+        cont = [j for j in active if j.steps_done + w < j.n_steps]
+        admit = self._admits(cont, queue)
+        if len(cont) == len(active) and not admit:
+            return None  # no boundary after this window
+        if not cont and not admit:
+            return None
+        if any(j.vmcmd for j in cont + admit):
+            return None
+        members = [(j, j.crd, j.vel, j.steps_done + w) for j in cont] + [(j, j.crd, j.vel, j.steps_done)
+                                                                          for j in admit]
+        return cont, admit, pool.submit(self._engine_for, members)
+
+    @staticmethod
+    def _discard(prep):
+        if prep is not None:
+            try:
+                prep[2].result().close()
+            except Exception:
+                pass
 
     def run(self, jobs):
         """Runs every job to completion; returns a summary dict (throughput, latencies)."""
@@ -122,10 +176,15 @@ class Server:
         intvl = intvls.pop()
         if self.window % intvl:
             raise ValueError("window must be a multiple of nsgrid_update_intvl")
+        with concurrent.futures.ThreadPoolExecutor(max_workers=1) as pool:
+            return self._run(jobs, pool)
+
+    def _run(self, jobs, pool):
         future = collections.deque(sorted(jobs, key=lambda j: j.arrival_s))
         queue = collections.deque()
         active, done, failed = [], [], []
         eng = None
+        prep = None  # (continuing, admitted, engine future) built during the last window
         t0 = self.clock()
         first_arrival = future[0].arrival_s if future else 0.0
         while future or queue or active:
@@ -141,6 +200,8 @@ class Server:
                 used += admit[-1].bytes
             if finished or admit:
                 t_re = self.clock()
+                cont = [j for j in active if j.steps_done < j.n_steps]
+                planned = prep is not None and prep[0] == cont and prep[1] == admit
                 if eng is not None:
                     for i, j in enumerate(active):
                         j.crd, j.vel = eng.get_state(i)
@@ -153,13 +214,26 @@ class Server:
                 for j in finished:
                     j.t_done = now
                     done.append(j)
-                active = [j for j in active if j.steps_done < j.n_steps] + admit
+                active = cont + admit
                 for j in admit:
                     j.t_admit = now
-                if active:
-                    eng = self._build(active)
+                if planned:
+                    eng = prep[2].result()
+                    for i, j in enumerate(cont):
+                        eng.set_state(i, j.crd, j.vel)
+                    self.n_relayouts += 1
+                    self.n_prepared += 1
                     self.batch_sizes.append(len(active))
+                else:
+                    self._discard(prep)
+                    if active:
+                        eng = self._build(active)
+                        self.batch_sizes.append(len(active))
+                prep = None
                 self.relayout_s += self.clock() - t_re
+            else:
+                self._discard(prep)  # (a window that ended as planned always has a boundary)
+                prep = None
             if not active:
                 if future:
                     wait = future[0].arrival_s - (self.clock() - t0)
@@ -167,11 +241,14 @@ class Server:
                         self.sleep(wait)
                 continue
             w = min(self.window, min(j.n_steps - j.steps_done for j in active))
+            prep = self._prepare(pool, active, queue, w)
             try:
                 eng.step(w)
             except engine.OgError as ex:
                 if ex.status != engine.OG_ERR_SYSTEM_FAULT:
                     raise
+                self._discard(prep)
+                prep = None
                 bad = eng.system_faults()
                 t_re = self.clock()
                 for i, j in enumerate(active):
@@ -200,7 +277,7 @@ class Server:
         return {"n_jobs": len(done), "n_failed": len(failed), "failed": failed, "atom_steps": atom_steps, "span_s": span,
                 "atom_steps_per_s": atom_steps / span if span > 0 else 0.0,
                 "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
-                "relayouts": self.n_relayouts, "relayout_s": self.relayout_s,
+                "relayouts": self.n_relayouts, "prepared_relayouts": self.n_prepared, "relayout_s": self.relayout_s,
                 "mean_batch": float(np.mean(self.batch_sizes)) if self.batch_sizes else 0.0,
                 "jobs": done}
 

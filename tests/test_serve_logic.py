@@ -56,6 +56,12 @@ class FakeEngine:
     def get_state(self, i):
         return self.systems[i]["crd"].copy(), self.systems[i]["vel"].copy()
 
+    def set_state(self, i, crd=None, vel_next=None):
+        if crd is not None:
+            self.systems[i]["crd"] = np.array(crd, float)
+        if vel_next is not None:
+            self.systems[i]["vel"] = np.array(vel_next, float)
+
     def get_energies(self, i):
         return {"step": float(self.systems[i]["crd"][0, 0])}
 
@@ -140,3 +146,24 @@ def test_faulted_job_retired_others_finish():
     assert bad.failed and bad.fault == 4 and bad.steps_done == 20 and np.all(bad.crd == 20)
     for j in (jobs[0], jobs[2]):
         assert not j.failed and np.all(j.crd == 60)
+
+
+@pytest.mark.parametrize("arrive", [0.0, 0.004])
+def test_batches_built_ahead_match_boundary_builds(arrive):
+    """The next batch built during the window (then given the continuing jobs' state) leaves
+    every job where building it at the boundary does: same steps, same coordinates, same
+    batches; with staggered arrivals some boundaries are not predictable and are built there."""
+    out = []
+    for ahead in (False, True):
+        clock = FakeClock()
+        p = {"nsgrid_update_intvl": 10}
+        jobs = [serve.Job(k, _system(100 * (k % 3 + 1)), p, 20 * (k % 4 + 1), arrival_s=arrive * k)
+                for k in range(9)]
+        srv = _server(clock, max_jobs=3, window=20, prepare_ahead=ahead)
+        res = srv.run(jobs)
+        out.append((res, [(j.steps_done, j.crd[0, 0], j.t_admit, j.t_done) for j in jobs], list(FakeEngine.log),
+                    srv.batch_sizes))
+    (r0, j0, log0, b0), (r1, j1, log1, b1) = out
+    assert j0 == j1 and b0 == b1 and r0["n_jobs"] == r1["n_jobs"] == 9
+    assert r0["prepared_relayouts"] == 0 and r1["prepared_relayouts"] > 0
+    assert sorted(map(tuple, log0)) == sorted(map(tuple, log1)) or arrive > 0
