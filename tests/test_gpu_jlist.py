@@ -118,3 +118,31 @@ def test_every_atom_moved_beyond_the_skin(n_waters):
     assert np.max(np.abs(res[10][1] - res[9][1])) < 1e-3
     for k in ("potential", "vdw", "ele"):
         assert abs(res[10][2][k] - res[9][2][k]) <= 1e-6 * abs(res[9][2][k]), k
+
+
+def test_put_state_from_pinned_and_pageable_buffers_agree():
+    """og_put_state from a pinned and from a pageable host buffer: the same state, bit for bit
+    (a scatter kernel reading the pinned buffer over PCIe instead of a staging copy was tried:
+    1.12 ms against 0.53 ms for 24 MB)."""
+    import torch
+    s = systems.water_system(1500, seed=5)
+    p = _params(thermostat="none")
+    out = []
+    for pinned in (False, True):
+        eng = _engine(s, p, 10)
+        eng.step(3)
+        crd, vel = eng.get_state(0)
+        crd = crd + 0.01
+        if pinned:
+            c = torch.from_numpy(np.ascontiguousarray(crd).reshape(-1)).pin_memory()
+            v = torch.from_numpy(np.ascontiguousarray(vel).reshape(-1)).pin_memory()
+            eng.put_state_ptr(0, c.data_ptr(), v.data_ptr())
+        else:
+            c = np.ascontiguousarray(crd).reshape(-1)
+            v = np.ascontiguousarray(vel).reshape(-1)
+            eng.put_state_ptr(0, c.ctypes.data, v.ctypes.data)
+        eng.synchronize()
+        eng.step(2)
+        out.append(eng.get_state(0))
+        eng.close()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
