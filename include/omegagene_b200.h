@@ -265,7 +265,9 @@ og_status og_get_flags(og_engine *e, int32_t *flags);
  * j-major fed by a per-warp queue of the j atoms within the cutoff of the i cell, at 128/80;
  * 9 = the same at 102 registers in blocks of 128 threads; 10 = packed j-major over j lists
  * culled once per list build (cutoff + 0.7 A around the i cell, rebuilt whenever an atom has
- * moved 0.35 A since), at 102 registers (engines with fewer than 2^24 atom slots). */
+ * moved 0.35 A since), at 102 registers (engines with fewer than 2^24 atom slots).  An engine
+ * holding a system with another electrostatics or nonbond model uses the generic forms of
+ * variants 9 and 10 only (a fixed other variant means 9). */
 #define OG_N_PAIR_VARIANTS 11
 /* Autotuner result: the pair-kernel variant in use and the best time of each variant on the
  * first list, in ms (variant_ms[OG_N_PAIR_VARIANTS]); for variant 10 the time is one step's

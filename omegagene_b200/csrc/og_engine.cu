@@ -767,8 +767,8 @@ og_status launch_pair(og_engine *e, bool vir, int variant, bool ene) {
     // 5-6: j-major with packed FP32x2 arithmetic (128/80); 7-9: the same with a j-atom queue
     // (128/80 in blocks of 256, 102 in blocks of 128).  The virial kernel is that of the
     // variant's family.
-    // a system with another electrostatics / nonbond model: the generic j-queue kernel for all
-    if (e->any_gen) {
+    // a system with another electrostatics / nonbond model: the generic j-queue (or j-list) kernel
+    if (e->any_gen && variant != OG_JL_VARIANT) {
         if (vir) k_pair_ljzd_jq<true, true, 2, 256, true><<<nb, 256, 0, st>>>(JQ_ARGS);
         else if (ene) k_pair_ljzd_jq<false, true, 5, 128, true><<<2 * nb, 128, 0, st>>>(JQ_ARGS);
         else k_pair_ljzd_jq<false, false, 5, 128, true><<<2 * nb, 128, 0, st>>>(JQ_ARGS);
@@ -781,9 +781,17 @@ og_status launch_pair(og_engine *e, bool vir, int variant, bool ene) {
                                                  e->d_cp_head, e->d_cp_shift, e->d_cp_mask, e->pair_cap,
                                                  2.0f * e->jl_skin + 1e-3f, e->d_jl, e->d_jl_count, e->d_xq_ref);
         LAUNCH_CHECK();
-        if (vir) k_pair_ljzd_jl<true, true, 2, 128, false><<<2 * nb, 128, 0, st>>>(JL_ARGS);
-        else if (ene) k_pair_ljzd_jl<false, true, 5, 128, false><<<2 * nb, 128, 0, st>>>(JL_ARGS);
-        else k_pair_ljzd_jl<false, false, 5, 128, false><<<2 * nb, 128, 0, st>>>(JL_ARGS);
+        if (e->any_gen) {
+            if (vir) k_pair_ljzd_jl<true, true, 2, 128, true><<<2 * nb, 128, 0, st>>>(JL_ARGS);
+            else if (ene) k_pair_ljzd_jl<false, true, 5, 128, true><<<2 * nb, 128, 0, st>>>(JL_ARGS);
+            else k_pair_ljzd_jl<false, false, 5, 128, true><<<2 * nb, 128, 0, st>>>(JL_ARGS);
+        } else if (vir) {
+            k_pair_ljzd_jl<true, true, 2, 128, false><<<2 * nb, 128, 0, st>>>(JL_ARGS);
+        } else if (ene) {
+            k_pair_ljzd_jl<false, true, 5, 128, false><<<2 * nb, 128, 0, st>>>(JL_ARGS);
+        } else {
+            k_pair_ljzd_jl<false, false, 5, 128, false><<<2 * nb, 128, 0, st>>>(JL_ARGS);
+        }
         LAUNCH_CHECK();
         return OG_OK;
     }
@@ -1395,13 +1403,12 @@ og_status build_list_checked(og_engine *e) {
 // the fastest; OG_PAIR_VARIANT=0/1/2 in the environment fixes the choice.  The trial launches
 // write the force accumulators, which are cleared afterwards.
 og_status autotune_pair(og_engine *e) {
-    if (e->any_gen) {  // one kernel serves the other models
-        e->pair_variant = 9;
-        return OG_OK;
-    }
+    // the other electrostatics / nonbond models have generic instantiations of variants 9 and 10
+    // only; a fixed choice of another variant falls back to 9
     const char *env = getenv("OG_PAIR_VARIANT");
     if (e->fixed_variant >= 0 || (env && *env)) {
         e->pair_variant = e->fixed_variant >= 0 ? e->fixed_variant : atoi(env) % OG_N_PAIR_VARIANTS;
+        if (e->any_gen && e->pair_variant != OG_JL_VARIANT) e->pair_variant = 9;
         return e->pair_variant == OG_JL_VARIANT ? jl_alloc(e) : OG_OK;
     }
     k_cell_bbox<<<blocks(e->cells_cap, 256), 256, 0, e->stream>>>(e->d_counters, e->cells_cap, e->d_xq,
@@ -1414,7 +1421,7 @@ og_status autotune_pair(og_engine *e) {
     }
     double best = 1e30;
     for (int v = 0; v < OG_N_PAIR_VARIANTS; v++) {
-        if (v == OG_JL_VARIANT && !try_jl) {
+        if ((v == OG_JL_VARIANT && !try_jl) || (e->any_gen && v != 9 && v != OG_JL_VARIANT)) {
             e->variant_ms[v] = 0.0;
             continue;
         }

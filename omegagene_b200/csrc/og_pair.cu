@@ -1225,6 +1225,9 @@ template __global__ void k_pair_ljzd_jq<false, false, 5, 128, true>(OG_JQ_ARGS_D
 template __global__ void k_pair_ljzd_jl<true, true, 2, 128, false>(OG_JL_ARGS_DECL);
 template __global__ void k_pair_ljzd_jl<false, true, 5, 128, false>(OG_JL_ARGS_DECL);
 template __global__ void k_pair_ljzd_jl<false, false, 5, 128, false>(OG_JL_ARGS_DECL);
+template __global__ void k_pair_ljzd_jl<true, true, 2, 128, true>(OG_JL_ARGS_DECL);
+template __global__ void k_pair_ljzd_jl<false, true, 5, 128, true>(OG_JL_ARGS_DECL);
+template __global__ void k_pair_ljzd_jl<false, false, 5, 128, true>(OG_JL_ARGS_DECL);
 template __global__ void k_jl_build<256>(int *, const int *, const SysDev *, const float4 *, const float4 *,
                                          const int *, const float4 *, const unsigned long long *, long long, float,
                                          int2 *, int *, float4 *);

@@ -45,15 +45,22 @@ def _rms(a, b):
     return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
 
 
+# the generic instantiations of the j-queue (9) and j-list (10) pair kernels
+VARIANTS = (9, 10)
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("name", sorted(MODELS))
-def test_model_forces_match_fp64_oracle(name):
+def test_model_forces_match_fp64_oracle(name, variant):
     s, p = _system(name), MODELS[name]["params"]
     md = ogo.OracleMD(s, p)
     ref = md.forces()
     w64 = md.work.reshape(-1, 3)
     eng = engine.Engine(0)
+    eng.set_tuning(variant)
     eng.add_system(s, p)
     eng.finalize()
+    assert eng.tuning()["pair_variant"] == variant
     eng.compute_forces()
     work, ene, _ = eng.get_forces(0)
     assert _rms(work, w64) <= 1e-5, (name, _rms(work, w64))
@@ -65,10 +72,12 @@ def test_model_forces_match_fp64_oracle(name):
     eng.close()
 
 
+@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("name", sorted(MODELS))
-def test_model_tracks_reference_log(name):
+def test_model_tracks_reference_log(name, variant):
     s, mdl = _system(name), MODELS[name]
     eng = engine.Engine(0)
+    eng.set_tuning(variant)
     eng.add_system(s, mdl["params"])
     eng.finalize()
     eng.set_trace(3)
@@ -84,11 +93,13 @@ def test_model_tracks_reference_log(name):
     eng.close()
 
 
-def test_mixed_models_in_one_batch():
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_mixed_models_in_one_batch(variant):
     base = _load("make_ala3_golden").load_system()
     p_zd = dict(MODELS["zq_a0"]["params"], electrostatic="zero-dipole")
     p_zo = MODELS["zo_a01"]["params"]
     eng = engine.Engine(0)
+    eng.set_tuning(variant)
     eng.add_system(base, p_zd)
     eng.add_system(base, p_zo)
     eng.finalize()
