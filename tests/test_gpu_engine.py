@@ -197,19 +197,22 @@ def test_batch_invariance_bitwise(variant):
 
 def test_nve_drift_small():
     """Config-0 water: short velocity-rescaled warm-up at 0.5 fs, then NVE at 2 fs; the total
-    energy drift stays within 0.01 kcal/mol/ns per degree of freedom."""
+    energy drift stays within 0.01 kcal/mol/ns per degree of freedom.  The pair variant is fixed
+    (the j-list kernel) so that the trajectory is reproducible, and the slope is fitted over
+    2,900 steps: over 900 steps the estimate scatters by +-0.016 with the FP32 summation order
+    alone (measured over pair variants 6/9/10 and two seeds), over 2,900 by +-0.002."""
     s = systems.water_system(3000, box=44.8, seed=0, lattice_m=15)
     warm = _params(nsgrid_update_intvl=10, time_step=0.5, thermostat="scaling", temperature=300.0)
-    eng = _engine([(s, warm, None)])
+    eng = _engine([(s, warm, None)], variant=10)
     eng.step(2000)
     crd, vel = eng.get_state(0)
     s2 = dict(s)
     s2["crd"], s2["vel"] = crd, vel
     nve = _params(nsgrid_update_intvl=10, time_step=2.0)
-    eng2 = _engine([(s2, nve, None)])
-    eng2.set_trace(1000)
-    eng2.step(1000)
-    tr = eng2.get_trace(1000)[:, 0, :]
+    eng2 = _engine([(s2, nve, None)], variant=10)
+    eng2.set_trace(3000)
+    eng2.step(3000)
+    tr = eng2.get_trace(3000)[:, 0, :]
     tot = tr[:, engine.ENERGY_NAMES.index("total")]
     t_ns = np.arange(len(tot)) * 2.0 * 1e-6
     slope = np.polyfit(t_ns[100:], tot[100:], 1)[0]
