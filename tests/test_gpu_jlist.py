@@ -28,7 +28,8 @@ pytestmark = pytest.mark.gpu
 
 def _params(**kw):
     p = dict(engine.DEFAULT_PARAMS)
-    p.update(nsgrid_update_intvl=10, time_step=2.0, **kw)
+    p.update(nsgrid_update_intvl=10, time_step=2.0)
+    p.update(kw)
     return p
 
 
@@ -146,3 +147,40 @@ def test_put_state_from_pinned_and_pageable_buffers_agree():
         out.append(eng.get_state(0))
         eng.close()
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("age", [3, 6])
+def test_aged_jlists_give_the_fresh_lists_forces(age):
+    """Two identical runs; in one, an atom is moved 0.6 A and back through og_put_state, which
+    marks the j lists stale, so its next step evaluates freshly built j lists while the other
+    evaluates lists built up to `age` steps earlier (the same cell-pair list, the same
+    coordinates).  A pair missing from the aged lists (one at 11.5-12 A moves a hydrogen by
+    ~1e-5 A in a step) would separate the two; summation order alone leaves them within 1e-8 A."""
+    s = systems.water_system(3000, box=44.8, seed=0, lattice_m=15)
+    p = _params(thermostat="none", time_step=0.5)
+    runs = []
+    for fresh in (False, True):
+        eng = _engine(s, p, 10)
+        eng.step(10)  # one list interval, then `age` steps into the next
+        last = 0
+        for k in range(age):
+            b = eng.jlist_builds()
+            eng.step(1)
+            if eng.jlist_builds() > b:
+                last = k + 1
+        if not fresh:
+            assert age - last >= 2, "the lists were rebuilt %d steps ago" % (age - last)
+        if fresh:
+            crd, _ = eng.get_state(0)
+            moved = crd.copy()
+            moved[7, 0] += 0.6
+            b0 = eng.jlist_builds()
+            _put(eng, moved)
+            _put(eng, crd)
+        eng.step(1)
+        if fresh:
+            assert eng.jlist_builds() == b0 + 1
+        runs.append(eng.get_state(0))
+        eng.close()
+    assert np.max(np.abs(runs[0][0] - runs[1][0])) < 1e-8
+    assert np.max(np.abs(runs[0][1] - runs[1][1])) < 1e-5
