@@ -251,6 +251,7 @@ def run_ours(args, world, rank, local, pg):
     rem = (-args.warmup) % INTVL
     if rem:
         eng.step(rem)
+    builds0 = eng.jlist_builds()
     eng.set_timing(True)
     clocks = ClockSampler(local)
     barrier(pg)
@@ -260,6 +261,7 @@ def run_ours(args, world, rank, local, pg):
     torch.cuda.synchronize()
     clk = clocks.stop()
     st = eng.stats()
+    jl_builds = eng.jlist_builds() - builds0
     barrier(pg)
     ms_total = max_over_ranks(pg, st["step_ms"])
     pair_ms = st["pair_kernel_ms"] / args.steps
@@ -341,6 +343,10 @@ def run_ours(args, world, rank, local, pg):
                      "flop_per_pair": FLOP_PER_PAIR, "autotune": tuning,
                      "cell_pairs": n_cell_pairs,
                      "cluster_efficiency": n_int / (64.0 * n_cell_pairs) if n_cell_pairs else None,
+                     "jlist_builds": jl_builds,
+                     "jlist_note": "pair variant 10: j-list builds in the timed steps (at every cell-pair list "
+                                   "build and whenever an atom had moved past the 0.35 A skin); pair_kernel_ms "
+                                   "includes them",
                      "peak_note": "FP32 CUDA-core peak = 148 SMs x 128 lanes x 2 x %.0f MHz (nominal at the "
                                   "measured max SM clock; MEASURED_PEAKS.json has no FP32 figure)" % sm_max},
         "e2e": e2e, "gpu_launches": launches, "clocks": clk, "device_flags": flags,
