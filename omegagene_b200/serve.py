@@ -22,8 +22,9 @@ background thread creates and finalizes that engine, with the continuing jobs' s
 placeholder coordinates; when the window ends as planned, their positions and velocities are
 set with og_set_state (the list is built from them at the first step) and the engine takes over.
 The result is the same engine the boundary would have built.  A window that faults, a job
-arriving that the rules would admit, or a V-McMD job in the batch (its generator state is only
-known at the boundary) falls back to building the batch at the boundary.
+arriving that the rules would admit, a V-McMD job in the batch (its generator state is only
+known at the boundary) or a build that failed (two handles at once may not fit) falls back to
+building the batch at the boundary.
 
 A job whose system faults (a coordinate leaves the box or turns non-finite) is retired as failed
 with its state at the start of the window; og_step undoes the window for every job, and the
@@ -165,7 +166,7 @@ class Server:
         if prep is not None:
             try:
                 prep[2].result().close()
-            except Exception:
+            except Exception:  # a build that failed left nothing to close
                 pass
 
     def run(self, jobs):
@@ -201,7 +202,13 @@ class Server:
             if finished or admit:
                 t_re = self.clock()
                 cont = [j for j in active if j.steps_done < j.n_steps]
-                planned = prep is not None and prep[0] == cont and prep[1] == admit
+                ahead = None  # the engine built during the window, when it is the one needed
+                if prep is not None and prep[0] == cont and prep[1] == admit:
+                    try:
+                        ahead = prep[2].result()
+                    except Exception:  # e.g. no room for two handles: build at the boundary
+                        ahead = None
+                    prep = None
                 if eng is not None:
                     for i, j in enumerate(active):
                         j.crd, j.vel = eng.get_state(i)
@@ -217,8 +224,8 @@ class Server:
                 active = cont + admit
                 for j in admit:
                     j.t_admit = now
-                if planned:
-                    eng = prep[2].result()
+                if ahead is not None:
+                    eng = ahead
                     for i, j in enumerate(cont):
                         eng.set_state(i, j.crd, j.vel)
                     self.n_relayouts += 1

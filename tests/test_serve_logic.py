@@ -167,3 +167,25 @@ def test_batches_built_ahead_match_boundary_builds(arrive):
     assert j0 == j1 and b0 == b1 and r0["n_jobs"] == r1["n_jobs"] == 9
     assert r0["prepared_relayouts"] == 0 and r1["prepared_relayouts"] > 0
     assert sorted(map(tuple, log0)) == sorted(map(tuple, log1)) or arrive > 0
+
+
+def test_failed_ahead_build_falls_back_to_the_boundary():
+    """An engine built ahead that fails (say, two handles do not fit at once) is replaced by one
+    built at the boundary; every job still runs exactly its steps."""
+    import threading
+    clock = FakeClock()
+    p = {"nsgrid_update_intvl": 10}
+    main = threading.current_thread()
+
+    def factory(dev):
+        if threading.current_thread() is not main:
+            raise MemoryError("no room for a second handle")
+        return FakeEngine(clock)
+
+    jobs = [serve.Job(k, _system(100 * (k + 1)), p, 20 * (k % 3 + 1)) for k in range(6)]
+    srv = serve.Server(0, hbm_budget_bytes=10 ** 12, max_jobs=3, window=20, clock=clock, sleep=clock.sleep,
+                       engine_factory=factory)
+    res = srv.run(jobs)
+    assert res["n_jobs"] == 6 and res["prepared_relayouts"] == 0
+    for j in jobs:
+        assert np.all(j.crd == j.n_steps) and j.steps_done == j.n_steps
