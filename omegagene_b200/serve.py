@@ -41,7 +41,10 @@ import numpy as np
 
 from . import engine
 
-BYTES_PER_ATOM = 1400  # device footprint per atom: state, grid, cell pairs, list scratch
+# device footprint per atom: state, grid, cell pairs, list scratch and, for the j-list pair
+# kernel, its entries (measured on a 60-job water batch of 546k atoms: 1,728 bytes per atom with
+# the j-queue kernel, 4,054 with the j-list kernel)
+BYTES_PER_ATOM = 4200
 
 
 class Job:
