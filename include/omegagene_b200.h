@@ -269,6 +269,13 @@ og_status og_get_flags(og_engine *e, int32_t *flags);
  * holding a system with another electrostatics or nonbond model uses the generic forms of
  * variants 9 and 10 only (a fixed other variant means 9). */
 #define OG_N_PAIR_VARIANTS 11
+/* Not a tuned variant: the pair terms in FP64 throughout (positions, charges, C6/C12, every
+ * operation) over the same cell-pair list, accumulated in the same fixed point.  A validation
+ * mode for separating the production kernels' FP32 arithmetic from everything else of a
+ * trajectory; several times slower; zero-dipole alpha = 0 with plain LJ only.  Chosen only with
+ * og_set_tuning, never by the autotuner.  No counterpart in the reference, whose pair term is
+ * FP32 (real_pw, CelesteObject.h:14). */
+#define OG_PAIR_VARIANT_F64 11
 /* Autotuner result: the pair-kernel variant in use and the best time of each variant on the
  * first list, in ms (variant_ms[OG_N_PAIR_VARIANTS]); for variant 10 the time is one step's
  * launch plus its share of the j-list build (build time / nsgrid_update_intvl). */
@@ -277,7 +284,7 @@ og_status og_get_tuning(og_engine *e, int32_t *pair_variant, double *variant_ms)
  * whenever an atom has moved farther than the skin (0.35 A, or OG_JL_SKIN in the environment)
  * since the last.  0 for the other variants. */
 og_status og_get_jlist_builds(og_engine *e, int64_t *n_builds);
-/* Fixes the pair-kernel variant (0..OG_N_PAIR_VARIANTS-1) before og_finalize and skips the autotuner, e.g. when a
+/* Fixes the pair-kernel variant (0..OG_N_PAIR_VARIANTS-1, or OG_PAIR_VARIANT_F64) before og_finalize and skips the autotuner, e.g. when a
  * serving loop re-creates engines for new batches; -1 restores autotuning.  No counterpart in
  * the reference, which has one pair kernel. */
 og_status og_set_tuning(og_engine *e, int32_t pair_variant);
@@ -313,16 +320,22 @@ og_status og_get_graph_info(og_engine *e, int32_t *enabled, int64_t *replays, in
  * length.  The engine's own energy / kinetic-energy reduction (two levels: 4096-item chunks,
  * then chunks in order), so a segment's sum does not depend on the other segments.
  * Stream-ordered on cuda_stream (a cudaStream_t, NULL = default); its scratch is a
- * stream-ordered allocation released before return. */
+ * stream-ordered allocation released before return.  n_seg <= OG_SEGMENT_SUM_MAX_SEGMENTS
+ * (one grid row per segment), else OG_ERR_CAPACITY.  A CUDA error already pending on the calling
+ * thread is reported as OG_ERR_CUDA and left pending; nothing is launched then. */
+#define OG_SEGMENT_SUM_MAX_SEGMENTS 65535
 og_status og_segment_sum(const double *d_values, int32_t stride, const int32_t *d_seg_base, int32_t n_seg,
                          int32_t max_seg_len, double *d_out, void *cuda_stream);
 /* og_segment_sum without any device allocation, for callers that cannot allocate at call time
  * (all free device memory already handed to another allocator's pool, or an allocation call not
  * acceptable on their path).  No counterpart in the reference.  Scratch is a fixed 512 KiB
- * array in device memory (n_seg * ceil(max_seg_len / 4096) <= 65536, else OG_ERR_CAPACITY),
- * held by every GPU that loads the library until the process exits.  The first call on a device
- * (with that device current) looks up the array's device address; make that first call before
- * any stream capture.  All calls share the array: calls that overlap on the GPU race. */
+ * array in device memory (n_seg <= OG_SEGMENT_SUM_MAX_SEGMENTS and
+ * n_seg * ceil(max_seg_len / 4096) <= 65536, else OG_ERR_CAPACITY), held by every GPU that loads
+ * the library until the process exits.  The first call on a device (with that device current)
+ * looks up the array's device address; make that first call before any stream capture.  The
+ * address is that of the device's primary context (the CUDA runtime's): call it from that
+ * context only, and not after a cudaDeviceReset of the device.  All calls share the array:
+ * calls that overlap on the GPU race. */
 og_status og_segment_sum_noalloc(const double *d_values, int32_t stride, const int32_t *d_seg_base, int32_t n_seg,
                                  int32_t max_seg_len, double *d_out, void *cuda_stream);
 /* Number of systems and atoms held. */

@@ -313,11 +313,23 @@ def hps_tables(topol):
     lam = np.zeros((nt, nt), np.float64)
     raw = topol.get("lj_hps_raw", b"")
     n = min(len(raw) // HPS.itemsize, len(topol["lj_pairs"]))
-    for rec in np.frombuffer(raw[:n * HPS.itemsize], HPS):
-        i, j = int(rec["t1"]) - 1, int(rec["t2"]) - 1
-        cut[i, j] = cut[j, i] = rec["cut"]
-        lam[i, j] = lam[j, i] = rec["lam"]
+    rec = np.frombuffer(raw[:n * HPS.itemsize], HPS)
+    i, j, k = _last_per_type_pair(rec["t1"], rec["t2"], nt)
+    cut[i, j] = cut[j, i] = rec["cut"][k]
+    lam[i, j] = lam[j, i] = rec["lam"][k]
     return cut, lam
+
+
+def _last_per_type_pair(t1, t2, nt):
+    """0-based (i, j) and record index of the last record of every unordered type pair among
+    1-based records (t1, t2): the record a sequential fill of both orders leaves in place."""
+    i = np.asarray(t1, np.int64) - 1
+    j = np.asarray(t2, np.int64) - 1
+    key = np.minimum(i, j) * nt + np.maximum(i, j)
+    rev = key[::-1]
+    _, first_in_rev = np.unique(rev, return_index=True)
+    k = len(key) - 1 - first_in_rev
+    return i[k], j[k], k
 
 
 def pack_hps(t1, t2, cut, lam):
@@ -333,10 +345,10 @@ def lj_tables(topol):
     nt = int(topol["n_lj_types"])
     c6 = np.zeros((nt, nt), np.float64)
     c12 = np.zeros((nt, nt), np.float64)
-    for rec in topol["lj_pairs"]:
-        i, j = int(rec["t1"]) - 1, int(rec["t2"]) - 1
-        c6[i, j] = c6[j, i] = rec["p6"]
-        c12[i, j] = c12[j, i] = rec["p12"]
+    rec = topol["lj_pairs"]
+    i, j, k = _last_per_type_pair(rec["t1"], rec["t2"], nt)
+    c6[i, j] = c6[j, i] = rec["p6"][k]
+    c12[i, j] = c12[j, i] = rec["p12"][k]
     return c6, c12
 
 
@@ -344,14 +356,19 @@ def nb15off_table(n_atoms, pairs, max_nb15off=32):
     """Padded exclusion table as MmSystem::set_nb15off builds it (MmSystem.cpp:478-525):
     each listed pair is entered in both rows unless already present; -1 pads."""
     tab = np.full((n_atoms, max_nb15off), -1, np.int32)
-    cnt = np.zeros(n_atoms, np.int64)
-    for a1, a2 in np.asarray(pairs).reshape(-1, 2):
-        for x, y in ((a1, a2), (a2, a1)):
-            row = tab[x, :cnt[x]]
-            if (row == y).any():
-                continue
-            if cnt[x] >= max_nb15off:
-                raise ClsFormatError("more than %d exclusions for atom %d" % (max_nb15off, x))
-            tab[x, cnt[x]] = y
-            cnt[x] += 1
+    p = np.asarray(pairs, np.int64).reshape(-1, 2)
+    # entries in the sequential order (a1 -> a2, then a2 -> a1, record by record); a repeat of an
+    # entry already in its row is skipped, so each row keeps its first occurrences in order
+    x = np.stack([p[:, 0], p[:, 1]], 1).reshape(-1)
+    y = np.stack([p[:, 1], p[:, 0]], 1).reshape(-1)
+    _, first = np.unique(x * max(n_atoms, 1) + y, return_index=True)
+    first.sort()
+    x, y = x[first], y[first]
+    order = np.argsort(x, kind="stable")
+    x, y = x[order], y[order]
+    start = np.searchsorted(x, np.arange(n_atoms))
+    col = np.arange(len(x)) - start[x]
+    if len(col) and col.max() >= max_nb15off:
+        raise ClsFormatError("more than %d exclusions for atom %d" % (max_nb15off, int(x[np.argmax(col)])))
+    tab[x, col] = y
     return tab

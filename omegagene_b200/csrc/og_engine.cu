@@ -60,10 +60,15 @@ __global__ void k_pair_ljzd_jm2(const int *, const int *, const SysDev *, const 
 template <bool VIR, bool ENE, int MINB, int NT, bool GEN>
 __global__ void k_pair_ljzd_jl(int *, const int *, const SysDev *, const float4 *, const int *, const int *,
                                const float4 *, const int2 *, const int2 *, const int *, const float2 *,
-                               unsigned long long *, double *, const EleDev *, const float2 *);
+                               unsigned long long *, double *, const EleDev *, const float2 *, int *, int);
+template <bool VIR>
+__global__ void k_pair_f64(const int *, const int *, const SysDev *, const double *, const int *, const int *,
+                           const double *, const int *, const int2 *, const unsigned long long *, const double2 *,
+                           long long, unsigned long long *, double *);
 template <int NT>
 __global__ void k_jl_build(int *, const int *, const SysDev *, const float4 *, const float4 *, const int *,
-                           const float4 *, const unsigned long long *, long long, float, int2 *, int *, float4 *);
+                           const float4 *, const unsigned long long *, long long, float, int2 *, int *, float4 *,
+                           const int *);
 __global__ void k_cell_bbox(const int *, int, const float4 *, const unsigned char *, float4 *);
 // og_integrate.cu
 __global__ void k_excess(int, const int2 *, const int *, const SysDev *, const EleDev *, const double *,
@@ -113,7 +118,7 @@ __global__ void k_shake_quad(int, const int4 *, const double *, const int *, con
                              double *, const double *, int, double, int *);
 __global__ void k_finish(int, const int *, const SysDev *, int, double *, const double *, const double *, double *,
                          const int *, double *, const double *, float4 *, const float *, double *, int *, int *,
-                         const float4 *, float);
+                         const float4 *, float, int *);
 __global__ void k_slot_refresh(const int *, int, const int *, const double *, const double *, const float *,
                                const int *, float4 *, int *);
 __global__ void k_energies(int, const SysDev *, const double *, const double *, double *, double *, int,
@@ -122,7 +127,7 @@ __global__ void k_trace_advance(long long *, long long *);
 __global__ void k_capture_frames(int, const int *, const int *, const int *, const SysDev *, const long long *,
                                  const double *, const double *, float *, double *);
 __global__ void k_put_state(int, int, const int *, const SysDev *, const double *, const double *, double *, double *,
-                            const int *, double *, const double *, float4 *, const float4 *, float, int *);
+                            const int *, double *, const double *, float4 *, const float4 *, float, int *, int *);
 
 __global__ void k_fill_int(int *p, long long n, int v) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -231,6 +236,7 @@ struct og_engine {
     int2 *d_jl = nullptr;
     int *d_jl_count = nullptr;
     float4 *d_xq_ref = nullptr;
+    int *d_jl_stale = nullptr;   // per system: its j lists must be rebuilt before the next pair launch
     float jl_skin = OG_JL_SKIN;
     unsigned long long *d_frc = nullptr;
     int *d_uni_lo = nullptr, *d_uni_hi = nullptr;
@@ -270,6 +276,7 @@ struct og_engine {
     float *d_grp_mass_inv = nullptr;
     double *d_moment = nullptr;
     float2 *d_lj = nullptr;
+    double2 *d_lj64 = nullptr;  // FP64 C6/C12 of the validation variant OG_PAIR_VARIANT_F64 (else null)
     double *d_sys_acc = nullptr, *d_mcmd = nullptr, *d_energies = nullptr, *d_thermo = nullptr,
            *d_sum_tmp = nullptr;
     int *d_mask_plain = nullptr, *d_mask_thermo = nullptr, *d_active = nullptr, *d_any = nullptr,
@@ -744,7 +751,10 @@ og_status build_list(og_engine *e) {
         e->d_slot_atom, e->d_atom_slot, e->d_excl_start, e->d_excl_list, e->d_cell_excl, e->d_cell_origin,
         e->d_cp_mask, e->d_cp_shift);
     LAUNCH_CHECK();
-    if (e->d_jl) CK(cudaMemsetAsync(e->d_counters + OG_CNT_JL_STALE, 1, sizeof(int), st));  // new list: rebuild
+    if (e->d_jl) {  // new list: every system's j lists are rebuilt
+        CK(cudaMemsetAsync(e->d_jl_stale, 1, sizeof(int) * e->n_sys, st));
+        CK(cudaMemsetAsync(e->d_counters + OG_CNT_JL_STALE, 1, sizeof(int), st));
+    }
     return OG_OK;
 }
 
@@ -756,7 +766,7 @@ og_status build_list(og_engine *e) {
 #define JQ_ARGS PAIR_ARGS, e->d_ele, e->d_hps
 #define JL_ARGS                                                                                                 \
     e->d_counters, e->d_cell_sys, e->d_sys, e->d_xq, e->d_slot_type, e->d_cp_head, e->d_cp_shift, e->d_cp_c2img, \
-        e->d_jl, e->d_jl_count, e->d_lj, e->d_frc, e->d_cell_acc, e->d_ele, e->d_hps
+        e->d_jl, e->d_jl_count, e->d_lj, e->d_frc, e->d_cell_acc, e->d_ele, e->d_hps, e->d_jl_stale, e->n_sys
 
 // Pair kernel variants differ in the register budget per thread (resident blocks per SM).
 // ene = false: the caller does not read this step's energies (only variants 5-6 skip them).
@@ -775,11 +785,26 @@ og_status launch_pair(og_engine *e, bool vir, int variant, bool ene) {
         LAUNCH_CHECK();
         return OG_OK;
     }
+    if (variant == OG_PAIR_VARIANT_F64) {
+        if (!e->d_lj64) return fail(e, OG_ERR_STATE, "FP64 pair variant without its FP64 LJ table");
+        if (vir)
+            k_pair_f64<true><<<nb, 256, 0, st>>>(e->d_counters, e->d_cell_sys, e->d_sys, e->d_slot_crd, e->d_slot_atom,
+                                                 e->d_slot_type, e->d_charge, e->d_cp_head, e->d_cp_c2img,
+                                                 e->d_cp_mask, e->d_lj64, e->pair_cap, e->d_frc, e->d_cell_acc);
+        else
+            k_pair_f64<false><<<nb, 256, 0, st>>>(e->d_counters, e->d_cell_sys, e->d_sys, e->d_slot_crd,
+                                                  e->d_slot_atom, e->d_slot_type, e->d_charge, e->d_cp_head,
+                                                  e->d_cp_c2img, e->d_cp_mask, e->d_lj64, e->pair_cap, e->d_frc,
+                                                  e->d_cell_acc);
+        LAUNCH_CHECK();
+        return OG_OK;
+    }
     if (variant == OG_JL_VARIANT) {
         if (!e->d_jl) return fail(e, OG_ERR_STATE, "pair variant %d without its j lists", OG_JL_VARIANT);
         k_jl_build<256><<<nb, 256, 0, st>>>(e->d_counters, e->d_cell_sys, e->d_sys, e->d_bbox, e->d_xq,
                                                  e->d_cp_head, e->d_cp_shift, e->d_cp_mask, e->pair_cap,
-                                                 2.0f * e->jl_skin + 1e-3f, e->d_jl, e->d_jl_count, e->d_xq_ref);
+                                                 2.0f * e->jl_skin + 1e-3f, e->d_jl, e->d_jl_count, e->d_xq_ref,
+                                                 e->d_jl_stale);
         LAUNCH_CHECK();
         if (e->any_gen) {
             if (vir) k_pair_ljzd_jl<true, true, 2, 128, true><<<2 * nb, 128, 0, st>>>(JL_ARGS);
@@ -1125,7 +1150,7 @@ og_status run_step(og_engine *e, bool ene) {
                                                        e->d_crd_prev, e->d_vel, e->d_vel_next, e->d_atom_slot,
                                                        e->d_slot_crd, e->d_cell_origin, e->d_xq, e->d_mass, e->d_ke,
                                                        e->d_counters, e->d_sys_fault, e->d_xq_ref,
-                                                       e->jl_skin * e->jl_skin);
+                                                       e->jl_skin * e->jl_skin, e->d_jl_stale);
     LAUNCH_CHECK();
     if ((s = seg_sum<1>(e, e->d_ke, 1, 0, e->d_seg_atoms, e->mc_atoms, e->d_sys_acc, OG_ACC_SIZE, OG_ACC_KIN, 0)))
         return s;
@@ -1329,8 +1354,9 @@ og_status jl_alloc(og_engine *e) {
     if (env && *env) e->jl_skin = std::min(2.0f, std::max(0.05f, (float)atof(env)));
     og_status s;
     if ((s = dalloc(e, &e->d_jl, 8 * (size_t)e->pair_cap)) || (s = dalloc(e, &e->d_jl_count, (size_t)e->cells_cap)) ||
-        (s = dalloc(e, &e->d_xq_ref, (size_t)e->slots_cap)))
+        (s = dalloc(e, &e->d_xq_ref, (size_t)e->slots_cap)) || (s = dalloc(e, &e->d_jl_stale, (size_t)e->n_sys)))
         return s;
+    CK(cudaMemsetAsync(e->d_jl_stale, 1, sizeof(int) * e->n_sys, e->stream));
     CK(cudaMemsetAsync(e->d_counters + OG_CNT_JL_STALE, 1, sizeof(int), e->stream));
     return OG_OK;
 }
@@ -1339,9 +1365,11 @@ void jl_free(og_engine *e) {
     dfree(e, e->d_jl);
     dfree(e, e->d_jl_count);
     dfree(e, e->d_xq_ref);
+    dfree(e, e->d_jl_stale);
     e->d_jl = nullptr;
     e->d_jl_count = nullptr;
     e->d_xq_ref = nullptr;
+    e->d_jl_stale = nullptr;
 }
 
 // Captures one list interval -- the rebuild step and the intvl-1 steps after it -- into a graph.
@@ -1406,6 +1434,12 @@ og_status autotune_pair(og_engine *e) {
     // the other electrostatics / nonbond models have generic instantiations of variants 9 and 10
     // only; a fixed choice of another variant falls back to 9
     const char *env = getenv("OG_PAIR_VARIANT");
+    if (e->fixed_variant == OG_PAIR_VARIANT_F64) {
+        if (e->any_gen)
+            return fail(e, OG_ERR_INVALID, "the FP64 pair variant evaluates zero-dipole alpha = 0 with plain LJ only");
+        e->pair_variant = OG_PAIR_VARIANT_F64;
+        return OG_OK;
+    }
     if (e->fixed_variant >= 0 || (env && *env)) {
         e->pair_variant = e->fixed_variant >= 0 ? e->fixed_variant : atoi(env) % OG_N_PAIR_VARIANTS;
         if (e->any_gen && e->pair_variant != OG_JL_VARIANT) e->pair_variant = 9;
@@ -1684,6 +1718,7 @@ og_status og_finalize(og_engine *e) {
     std::vector<double> crd, vel, charge;
     std::vector<float> charge_f, mass, mass_inv;
     std::vector<float2> lj, hps_tab;
+    std::vector<double2> lj64;  // only for the FP64 validation variant
     std::vector<EleDev> ele_tab;
     std::vector<int2> excess, bondv, spair;
     std::vector<int> excess_sys, bond_sys, spair_sys, grp_start(1, 0), grp_atoms, grp_sys;
@@ -1896,6 +1931,8 @@ og_status og_finalize(og_engine *e) {
         for (int i = 0; i < d.n_lj_types; i++)
             for (int j = 0; j < d.n_lj_types; j++)
                 lj.push_back(make_float2((float)h.lj6[i * d.n_lj_types + j], (float)h.lj12[i * d.n_lj_types + j]));
+        if (e->fixed_variant == OG_PAIR_VARIANT_F64)
+            for (int i = 0; i < d.n_lj_types * d.n_lj_types; i++) lj64.push_back(make_double2(h.lj6[i], h.lj12[i]));
         for (int i = 0; i < d.n_lj_types; i++)
             for (int j = 0; j < d.n_lj_types; j++)
                 hps_tab.push_back(h.ele.hps ? make_float2((float)h.hcut[i * d.n_lj_types + j],
@@ -1977,6 +2014,7 @@ og_status og_finalize(og_engine *e) {
         (s = upload(e, &e->d_grp_sys, grp_sys)) || (s = upload(e, &e->d_grp_mass_inv, grp_mass_inv)) ||
         (s = dalloc(e, &e->d_moment, 3 * (size_t)(e->n_groups + 1))) || (s = upload(e, &e->d_lj, lj)) ||
         (s = upload(e, &e->d_hps, hps_tab)) || (s = upload(e, &e->d_ele, ele_tab)) ||
+        (!lj64.empty() && (s = upload(e, &e->d_lj64, lj64))) ||
         (s = dalloc(e, &e->d_sys_acc, OG_ACC_SIZE * (size_t)S)) || (s = dalloc(e, &e->d_mcmd, S)) ||
         (s = dalloc(e, &e->d_energies, OG_N_ENERGY * (size_t)S)) || (s = upload(e, &e->d_thermo, thermo)) ||
         (s = dalloc(e, &e->d_sum_tmp, S)) || (s = upload(e, &e->d_mask_plain, mask_plain)) ||
@@ -2556,7 +2594,8 @@ extern "C" og_status og_put_state(og_engine *e, int32_t sys, const double *crd, 
                                                                 crd ? sc : nullptr, vel_next ? sv : nullptr, e->d_crd,
                                                                 e->d_vel_next, e->d_atom_slot, e->d_slot_crd,
                                                                 e->d_cell_origin, e->d_xq, e->d_xq_ref,
-                                                                e->jl_skin * e->jl_skin, e->d_counters);
+                                                                e->jl_skin * e->jl_skin, e->d_jl_stale,
+                                                                e->d_counters);
     LAUNCH_CHECK();
     return OG_OK;
 }
@@ -2629,8 +2668,10 @@ extern "C" og_status og_get_tuning(og_engine *e, int32_t *pair_variant, double *
 extern "C" og_status og_segment_sum(const double *d_values, int32_t stride, const int32_t *d_seg_base, int32_t n_seg,
                                     int32_t max_seg_len, double *d_out, void *cuda_stream) {
     if (!d_values || !d_seg_base || !d_out || n_seg <= 0 || stride <= 0 || max_seg_len < 0) return OG_ERR_INVALID;
+    if (n_seg > OG_SEGMENT_SUM_MAX_SEGMENTS) return OG_ERR_CAPACITY;  // one grid row per segment
+    if (cudaPeekAtLastError() != cudaSuccess) return OG_ERR_CUDA;     // the caller's error, left pending
     cudaStream_t st = (cudaStream_t)cuda_stream;
-    const int max_chunks = std::max(1, (max_seg_len + 4095) / 4096);
+    const int max_chunks = (int)std::max(1LL, ((long long)max_seg_len + 4095) / 4096);
     double *part = nullptr;
     if (cudaMallocAsync((void **)&part, sizeof(double) * (size_t)n_seg * max_chunks, st) != cudaSuccess)
         return OG_ERR_NOMEM;
@@ -2645,8 +2686,9 @@ extern "C" og_status og_segment_sum(const double *d_values, int32_t stride, cons
 extern "C" og_status og_set_tuning(og_engine *e, int32_t pair_variant) {
     if (!e) return OG_ERR_INVALID;
     if (e->finalized) return fail(e, OG_ERR_STATE, "og_set_tuning after og_finalize");
-    if (pair_variant < -1 || pair_variant >= OG_N_PAIR_VARIANTS)
-        return fail(e, OG_ERR_INVALID, "pair variant must be -1 or 0..%d", OG_N_PAIR_VARIANTS - 1);
+    if (pair_variant < -1 || (pair_variant >= OG_N_PAIR_VARIANTS && pair_variant != OG_PAIR_VARIANT_F64))
+        return fail(e, OG_ERR_INVALID, "pair variant must be -1, 0..%d or %d (FP64)", OG_N_PAIR_VARIANTS - 1,
+                    OG_PAIR_VARIANT_F64);
     e->fixed_variant = pair_variant;
     return OG_OK;
 }

@@ -899,13 +899,19 @@ __global__ void k_thermo_crd(int n_atoms, const int *__restrict__ atom_sys, cons
 }
 
 // The pair kernel's j lists hold while every slot is within skin of the position they were
-// built from (xq_ref; null when the engine does not use them); otherwise they are marked stale.
-__device__ __forceinline__ void og_jl_check(const float4 &p, int sl, const float4 *__restrict__ xq_ref, float skin2,
-                                            int *__restrict__ counters) {
+// built from (xq_ref; null when the engine does not use them); otherwise the lists of the slot's
+// system are marked stale (jl_stale[s]), with the engine-wide "some system is stale" word.  Only
+// that system's lists are rebuilt, so a system's j lists, and with them the order of its FP32
+// i sums, never depend on the other systems of the batch.
+__device__ __forceinline__ void og_jl_check(const float4 &p, int sl, int s, const float4 *__restrict__ xq_ref,
+                                            float skin2, int *__restrict__ jl_stale, int *__restrict__ counters) {
     if (!xq_ref) return;
     const float4 o = xq_ref[sl];
     const float dx = p.x - o.x, dy = p.y - o.y, dz = p.z - o.z;
-    if (!(dx * dx + dy * dy + dz * dz <= skin2)) counters[OG_CNT_JL_STALE] = 1;
+    if (!(dx * dx + dy * dy + dz * dz <= skin2)) {
+        jl_stale[s] = 1;
+        counters[OG_CNT_JL_STALE] = 1;
+    }
 }
 
 // End of step, per atom: velocities from the constrained displacement (SubBox.cpp:1462-1481,
@@ -918,7 +924,8 @@ __global__ void k_finish(int n_atoms, const int *__restrict__ atom_sys, const Sy
                          const int *__restrict__ atom_slot, double *__restrict__ slot_crd,
                          const double *__restrict__ cell_origin, float4 *__restrict__ xq,
                          const float *__restrict__ mass, double *__restrict__ ke, int *__restrict__ counters,
-                         int *__restrict__ sys_fault, const float4 *__restrict__ xq_ref, float jl_skin2) {
+                         int *__restrict__ sys_fault, const float4 *__restrict__ xq_ref, float jl_skin2,
+                         int *__restrict__ jl_stale) {
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= n_atoms) return;
     const SysDev &S = sys[atom_sys[a]];
@@ -945,7 +952,7 @@ __global__ void k_finish(int n_atoms, const int *__restrict__ atom_sys, const Sy
     p.y = r[1];
     p.z = r[2];
     xq[sl] = p;
-    og_jl_check(p, sl, xq_ref, jl_skin2, counters);
+    og_jl_check(p, sl, atom_sys[a], xq_ref, jl_skin2, jl_stale, counters);
     ke[a] = vn * (double)mass[a];
     if (!(disp2 <= S.max_step_disp2)) {  // also catches NaN
         og_set_flag(counters, OG_FLAG_DISPLACEMENT);
@@ -1012,7 +1019,7 @@ __global__ void k_put_state(int n_atoms, int atom0, const int *__restrict__ atom
                             double *__restrict__ vel_next, const int *__restrict__ atom_slot,
                             double *__restrict__ slot_crd, const double *__restrict__ cell_origin,
                             float4 *__restrict__ xq, const float4 *__restrict__ xq_ref, float jl_skin2,
-                            int *__restrict__ counters) {
+                            int *__restrict__ jl_stale, int *__restrict__ counters) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_atoms) return;
     const int a = atom0 + i;
@@ -1037,7 +1044,7 @@ __global__ void k_put_state(int n_atoms, int atom0, const int *__restrict__ atom
         p.y = r[1];
         p.z = r[2];
         xq[sl] = p;
-        og_jl_check(p, sl, xq_ref, jl_skin2, counters);
+        og_jl_check(p, sl, atom_sys[a], xq_ref, jl_skin2, jl_stale, counters);
     }
 }
 

@@ -12,9 +12,18 @@
 // host it is only a stand-in symbol, not a device address.  The device address is obtained
 // once per device with cudaGetSymbolAddress, with that device current, on the first call made
 // while that device is current; that first call should therefore come before any stream
-// capture.  Every used scratch entry is written before it is read in the same call, so nothing
-// needs clearing; all calls share the array, so calls that overlap on the GPU (different
-// streams, or different host threads) race and must be serialised by the caller.
+// capture.  The address belongs to the device's primary context (the one the CUDA runtime
+// uses): call this only from that context, and not after a cudaDeviceReset of the device,
+// which unloads the module and leaves the looked-up address stale.  Every used scratch entry
+// is written before it is read in the same call, so nothing needs clearing; all calls share
+// the array, so calls that overlap on the GPU (different streams, or different host threads)
+// race and must be serialised by the caller.
+//
+// Limits: n_seg <= 65535 (one grid row per segment) and n_seg * ceil(max_seg_len / 4096) <=
+// 65536 (the scratch holds one partial sum per 4096-item chunk of every segment); beyond
+// either the call returns OG_ERR_CAPACITY without launching anything.  A CUDA error already
+// pending on the calling thread when the call starts is reported as OG_ERR_CUDA and left
+// pending for its owner; nothing is launched then either.
 #include <mutex>
 
 #include "../../include/omegagene_b200.h"
@@ -40,7 +49,9 @@ extern "C" og_status og_segment_sum_noalloc(const double *d_values, int32_t stri
                                             int32_t n_seg, int32_t max_seg_len, double *d_out, void *cuda_stream) {
     if (!d_values || !d_seg_base || !d_out || n_seg <= 0 || stride <= 0 || max_seg_len < 0) return OG_ERR_INVALID;
     const long long max_chunks = max_seg_len > 0 ? ((long long)max_seg_len + 4095) / 4096 : 1;
+    if (n_seg > OG_SEGMENT_SUM_MAX_SEGMENTS) return OG_ERR_CAPACITY;
     if ((long long)n_seg * max_chunks > OG_NOALLOC_SCRATCH_DOUBLES) return OG_ERR_CAPACITY;
+    if (cudaPeekAtLastError() != cudaSuccess) return OG_ERR_CUDA;  // the caller's error, left pending
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return OG_ERR_CUDA;
     if (dev < 0 || dev >= 256) return OG_ERR_INVALID;
@@ -58,5 +69,5 @@ extern "C" og_status og_segment_sum_noalloc(const double *d_values, int32_t stri
     dim3 grid((unsigned)max_chunks, (unsigned)n_seg);
     og::k_part<1><<<grid, 256, 0, st>>>(d_values, stride, 0, d_seg_base, (int)max_chunks, part);
     og::k_part_final<1><<<n_seg, 256, 0, st>>>(part, (int)max_chunks, d_out, 1, 0, nullptr, 0);
-    return cudaGetLastError() == cudaSuccess ? OG_OK : OG_ERR_CUDA;
+    return cudaGetLastError() == cudaSuccess ? OG_OK : OG_ERR_CUDA;  // only this call's launches
 }

@@ -1048,7 +1048,9 @@ k_pair_ljzd_jq(const int *__restrict__ counters, const int *__restrict__ cell_sy
 // k_put_state check this every step against xq_ref and set the stale counter otherwise), a
 // dropped entry's pairs are farther apart than cutoff + 1e-3 A, so the step evaluates exactly
 // the pairs the j-queue kernel evaluates.  The build runs at the first step of every list and
-// after any stale mark; otherwise it returns at once.
+// after any stale mark; otherwise it returns at once.  Staleness is per system (jl_stale[s]):
+// only the cells of a stale system are rebuilt, so a system's lists, and the order of its FP32
+// i sums, are the ones it has alone in the engine.
 //
 // Entry: x = j slot | exclusion byte << 24 (slots below 2^24), y = cell-pair index.  Cell1's
 // entries start at 8 * cp_head[c1] (at most 8 per cell pair), with their count in jl_count.
@@ -1057,7 +1059,8 @@ __global__ void __launch_bounds__(NT)
 k_jl_build(int *__restrict__ counters, const int *__restrict__ cell_sys, const SysDev *__restrict__ sys,
            const float4 *__restrict__ bbox, const float4 *__restrict__ xq, const int *__restrict__ cp_head,
            const float4 *__restrict__ cp_shift, const unsigned long long *__restrict__ cp_mask, long long pair_cap,
-           float reach, int2 *__restrict__ jl, int *__restrict__ jl_count, float4 *__restrict__ xq_ref) {
+           float reach, int2 *__restrict__ jl, int *__restrict__ jl_count, float4 *__restrict__ xq_ref,
+           const int *__restrict__ jl_stale) {
     if (counters[OG_CNT_JL_STALE] == 0) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) counters[OG_CNT_JL_BUILDS]++;
     const int lane = threadIdx.x & 31;
@@ -1069,7 +1072,9 @@ k_jl_build(int *__restrict__ counters, const int *__restrict__ cell_sys, const S
     __shared__ int s_k[NT / 32][32];
     const int c1 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (c1 >= n_cells) return;
-    const SysDev &S = sys[cell_sys[c1]];
+    const int s1 = cell_sys[c1];
+    if (!jl_stale[s1]) return;
+    const SysDev &S = sys[s1];
     if (lane < OG_CELL) xq_ref[c1 * OG_CELL + lane] = xq[c1 * OG_CELL + lane];
     const float rb = sqrtf(S.cutoff2) + reach, rb2 = rb * rb;
     const float4 b1l = bbox[2 * c1], b1h = bbox[2 * c1 + 1];
@@ -1138,18 +1143,22 @@ k_jl_build(int *__restrict__ counters, const int *__restrict__ cell_sys, const S
 }
 
 // The step kernel over the j lists (see k_jl_build).  Each round, lane l takes entry r + l.
-// The first thread clears the stale counter: this launch follows the build that consumed it.
+// The first block clears the stale marks: this launch follows the build that consumed them.
 template <bool VIR, bool ENE, int MINB, int NT = 128, bool GEN = false>
 __global__ void __launch_bounds__(NT, MINB)
 k_pair_ljzd_jl(int *__restrict__ counters, const int *__restrict__ cell_sys, const SysDev *__restrict__ sys,
                const float4 *__restrict__ xq, const int *__restrict__ slot_type, const int *__restrict__ cp_head,
                const float4 *__restrict__ cp_shift, const int2 *__restrict__ cp_c2img, const int2 *__restrict__ jl,
                const int *__restrict__ jl_count, const float2 *__restrict__ lj, unsigned long long *__restrict__ frc,
-               double *__restrict__ cell_acc, const EleDev *__restrict__ ele, const float2 *__restrict__ hps) {
+               double *__restrict__ cell_acc, const EleDev *__restrict__ ele, const float2 *__restrict__ hps,
+               int *__restrict__ jl_stale, int n_sys) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    if (blockIdx.x == 0 && threadIdx.x == 0) counters[OG_CNT_JL_STALE] = 0;
+    if (blockIdx.x == 0) {
+        if (threadIdx.x == 0) counters[OG_CNT_JL_STALE] = 0;
+        for (int s = threadIdx.x; s < n_sys; s += NT) jl_stale[s] = 0;
+    }
     const int n_cells = counters[OG_CNT_N_CELLS];
     if (warp >= n_cells) return;
     const int c1 = warp;
@@ -1196,6 +1205,110 @@ k_pair_ljzd_jl(int *__restrict__ counters, const int *__restrict__ cell_sys, con
     og_flush_icell<VIR, ENE>(A, c1, lane, frc, cell_acc);
 }
 
+// ---------------------------------------------------------------------------------------------
+// FP64 evaluation of the cell-pair list (pair variant OG_PAIR_VARIANT_F64): the reference's pair
+// terms (ForceField::calc_pairwise with ZeroMultipoleSum::calc_zero02pole_alpha0,
+// ForceField.cpp:333-418, ZeroMultipoleSum.cpp:309-332) in double precision throughout, on the
+// list's FP64 grid coordinates (MiniCell::crd), FP64 charges and an FP64 C6/C12 table, with the
+// image shift of each cell pair formed from the float box length as PBC holds it.  A validation
+// mode: it separates the FP32 arithmetic of the production kernels from everything else of a
+// trajectory (list, integrator, constraints).  Zero-dipole alpha = 0 with plain LJ only.
+// One warp per cell1: lane l takes i atom l & 7 and j atoms (l >> 3) and (l >> 3) + 4 of every
+// cell pair; j work is reduced over the 8 lanes of a j atom, i work over the lanes of an i atom
+// at the end, both added to the fixed-point accumulators.
+template <bool VIR>
+__global__ void __launch_bounds__(256)
+k_pair_f64(const int *__restrict__ counters, const int *__restrict__ cell_sys, const SysDev *__restrict__ sys,
+           const double *__restrict__ slot_crd, const int *__restrict__ slot_atom, const int *__restrict__ slot_type,
+           const double *__restrict__ charge, const int *__restrict__ cp_head, const int2 *__restrict__ cp_c2img,
+           const unsigned long long *__restrict__ cp_mask, const double2 *__restrict__ lj64, long long pair_cap,
+           unsigned long long *__restrict__ frc, double *__restrict__ cell_acc) {
+    const int c1 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int n_cells = counters[OG_CNT_N_CELLS];
+    if (c1 >= n_cells) return;
+    const SysDev &S = sys[cell_sys[c1]];
+    const int a1 = lane & 7, h = lane >> 3;
+    const int s1 = c1 * OG_CELL + a1;
+    const double x1[3] = {slot_crd[3 * (size_t)s1], slot_crd[3 * (size_t)s1 + 1], slot_crd[3 * (size_t)s1 + 2]};
+    const int at1 = slot_atom[s1];
+    const double q1 = at1 >= 0 ? charge[at1] : 0.0;
+    const int row1 = S.lj_base + slot_type[s1] * S.n_types;
+    const double rc = S.cutoff, rc2 = rc * rc;
+    const double fco = 1.0 / (rc * rc * rc), bco = 0.5 * fco, zco = 1.0 / rc + bco * rc * rc;
+    const double Lb[3] = {(double)S.Lf[0], (double)S.Lf[1], (double)S.Lf[2]};
+    double wi[3] = {0.0, 0.0, 0.0}, ev = 0.0, ee = 0.0, vir[VIR ? 9 : 1] = {};
+    int n_act = 0;
+    const long long k_beg = cp_head[c1], k_end = min((long long)cp_head[c1 + 1], pair_cap);
+    for (long long k = k_beg; k < k_end; k++) {
+        const int2 ci = cp_c2img[k];
+        const unsigned long long m = cp_mask[k];
+        const int img = ci.y;
+        const double sh[3] = {(img & 1) ? -Lb[0] : ((img & 2) ? Lb[0] : 0.0),
+                              (img & 4) ? -Lb[1] : ((img & 8) ? Lb[1] : 0.0),
+                              (img & 16) ? -Lb[2] : ((img & 32) ? Lb[2] : 0.0)};
+#pragma unroll
+        for (int half = 0; half < 2; half++) {
+            const int a2 = h + 4 * half;
+            const int s2 = ci.x * OG_CELL + a2;
+            double w[3] = {0.0, 0.0, 0.0};
+            if (!((m >> (a2 * OG_CELL + a1)) & 1ull)) {
+                double d[3];
+                for (int q = 0; q < 3; q++) d[q] = x1[q] - (slot_crd[3 * (size_t)s2 + q] + sh[q]);
+                const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+                if (r2 < rc2) {
+                    const int at2 = slot_atom[s2];
+                    const double cc = q1 * (at2 >= 0 ? charge[at2] : 0.0) * OG_CHARGE_COEFF;
+                    const double2 c = lj64[row1 + slot_type[s2]];
+                    const double r = sqrt(r2), ri = 1.0 / r, r2i = 1.0 / r2, r6i = r2i * r2i * r2i;
+                    const double t6 = c.x * r6i, t12 = c.y * r6i * r6i;
+                    ev += t12 - t6;
+                    ee += cc * (ri - zco + bco * r2);
+                    const double wc = r2i * (-12.0 * t12 + 6.0 * t6) - cc * (ri * r2i - fco);
+                    for (int q = 0; q < 3; q++) w[q] = wc * d[q];
+                    n_act++;
+                }
+            }
+            for (int q = 0; q < 3; q++) wi[q] += w[q];
+            // j work: the 8 lanes of this j atom
+            double wj[3] = {w[0], w[1], w[2]};
+            for (int q = 0; q < 3; q++)
+                for (int o = 1; o < OG_CELL; o <<= 1) wj[q] += __shfl_xor_sync(0xffffffffu, wj[q], o);
+            if (a1 == 0 && (wj[0] != 0.0 || wj[1] != 0.0 || wj[2] != 0.0)) {
+                unsigned long long *fj = frc + 3 * (size_t)s2;
+                for (int q = 0; q < 3; q++) atomicAdd(fj + q, (unsigned long long)og_to_fix(-wj[q]));
+                if (VIR && img != 0)  // sum over pairs of d (x) f: the shift term takes -(work on j)
+                    for (int a = 0; a < 3; a++)
+                        for (int b = 0; b < 3; b++) vir[a * 3 + b] += sh[a] * wj[b];
+            }
+        }
+    }
+    for (int q = 0; q < 3; q++) {
+        wi[q] += __shfl_xor_sync(0xffffffffu, wi[q], 8);
+        wi[q] += __shfl_xor_sync(0xffffffffu, wi[q], 16);
+    }
+    if (lane < OG_CELL && (wi[0] != 0.0 || wi[1] != 0.0 || wi[2] != 0.0)) {
+        unsigned long long *fa = frc + 3 * (size_t)s1;
+        for (int q = 0; q < 3; q++) atomicAdd(fa + q, (unsigned long long)og_to_fix(wi[q]));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        ev += __shfl_xor_sync(0xffffffffu, ev, o);
+        ee += __shfl_xor_sync(0xffffffffu, ee, o);
+        n_act += __shfl_xor_sync(0xffffffffu, n_act, o);
+        if (VIR)
+            for (int k = 0; k < 9; k++) vir[k] += __shfl_xor_sync(0xffffffffu, vir[k], o);
+    }
+    if (lane == 0) {
+        double *acc = cell_acc + (size_t)c1 * OG_CELL_ACC;
+        acc[0] = ev;
+        acc[1] = ee;
+        if (VIR) {
+            for (int k = 0; k < 9; k++) acc[2 + k] = vir[k];
+            acc[11] = (double)n_act;
+        }
+    }
+}
+
 #define OG_PAIR_ARGS_DECL                                                                                   \
     const int *, const int *, const SysDev *, const float4 *, const float4 *, const int *, const int *,      \
         const float4 *, const int2 *, const unsigned long long *, const float2 *, unsigned long long *, double *, \
@@ -1221,16 +1334,23 @@ template __global__ void k_pair_ljzd_jq<false, true, 5, 128, true>(OG_JQ_ARGS_DE
 template __global__ void k_pair_ljzd_jq<false, false, 5, 128, true>(OG_JQ_ARGS_DECL);
 #define OG_JL_ARGS_DECL                                                                                    \
     int *, const int *, const SysDev *, const float4 *, const int *, const int *, const float4 *, const int2 *, \
-        const int2 *, const int *, const float2 *, unsigned long long *, double *, const EleDev *, const float2 *
+        const int2 *, const int *, const float2 *, unsigned long long *, double *, const EleDev *, const float2 *, \
+        int *, int
 template __global__ void k_pair_ljzd_jl<true, true, 2, 128, false>(OG_JL_ARGS_DECL);
 template __global__ void k_pair_ljzd_jl<false, true, 5, 128, false>(OG_JL_ARGS_DECL);
 template __global__ void k_pair_ljzd_jl<false, false, 5, 128, false>(OG_JL_ARGS_DECL);
 template __global__ void k_pair_ljzd_jl<true, true, 2, 128, true>(OG_JL_ARGS_DECL);
 template __global__ void k_pair_ljzd_jl<false, true, 5, 128, true>(OG_JL_ARGS_DECL);
 template __global__ void k_pair_ljzd_jl<false, false, 5, 128, true>(OG_JL_ARGS_DECL);
+#define OG_F64_ARGS_DECL                                                                                   \
+    const int *, const int *, const SysDev *, const double *, const int *, const int *, const double *,      \
+        const int *, const int2 *, const unsigned long long *, const double2 *, long long, unsigned long long *, \
+        double *
+template __global__ void k_pair_f64<true>(OG_F64_ARGS_DECL);
+template __global__ void k_pair_f64<false>(OG_F64_ARGS_DECL);
 template __global__ void k_jl_build<256>(int *, const int *, const SysDev *, const float4 *, const float4 *,
                                          const int *, const float4 *, const unsigned long long *, long long, float,
-                                         int2 *, int *, float4 *);
+                                         int2 *, int *, float4 *, const int *);
 
 template __global__ void k_pair_ljzd<true, 2>(const int *, const int *, const SysDev *, const float4 *,
                                                 const float4 *, const int *, const int *, const float4 *,

@@ -24,6 +24,7 @@ ENERGY_NAMES = ["vdw", "ele", "bond", "angle", "potential", "kinetic", "temperat
                 "ele_self", "mcmd_factor", "torsion", "improper", "vdw14", "ele14"]
 N_ENERGY = len(ENERGY_NAMES)
 N_PAIR_VARIANTS = 11  # OG_N_PAIR_VARIANTS
+PAIR_VARIANT_F64 = 11  # OG_PAIR_VARIANT_F64: FP64 validation evaluation, chosen only by set_tuning
 
 
 class OgError(RuntimeError):
@@ -560,7 +561,8 @@ class Engine:
         return {"pair_variant": v.value, "variant_ms": ms.tolist()}
 
     def set_tuning(self, variant):
-        """Fixes the pair-kernel variant (0..9) before finalize(); -1 = autotune."""
+        """Fixes the pair-kernel variant (0..N_PAIR_VARIANTS-1, or PAIR_VARIANT_F64 for the FP64
+        validation evaluation) before finalize(); -1 = autotune."""
         self._check(self.L.og_set_tuning(self.h, int(variant)), "og_set_tuning")
 
     def set_graphs(self, on=True):

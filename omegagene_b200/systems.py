@@ -102,16 +102,20 @@ def _water_trios(first_atom, n_waters):
 
 def _lj_records(lj_types, mix="lb"):
     """LJ pair records with Lorentz-Berthelot mixing; types with eps 0 get zero terms."""
-    recs = []
     nt = len(lj_types)
-    for i in range(nt):
-        for j in range(i, nt):
-            si, ei = lj_types[i]
-            sj, ej = lj_types[j]
-            s = 0.5 * (si + sj)
-            e = math.sqrt(ei * ej)
-            recs.append((i + 1, j + 1, 4.0 * e * s ** 6, 4.0 * e * s ** 12))
-    return np.array(recs, dtype=[("t1", "<i4"), ("t2", "<i4"), ("p6", "<f8"), ("p12", "<f8")])
+    sig = np.array([t[0] for t in lj_types], np.float64)
+    eps = np.array([t[1] for t in lj_types], np.float64)
+    i, j = np.triu_indices(nt)
+    s = 0.5 * (sig[i] + sig[j])
+    e = np.sqrt(eps[i] * eps[j])
+    out = np.zeros(len(i), dtype=[("t1", "<i4"), ("t2", "<i4"), ("p6", "<f8"), ("p12", "<f8")])
+    out["t1"], out["t2"] = i + 1, j + 1
+    # powers through the C library's pow, one value at a time (numpy's vectorised pow may
+    # round differently in the last bit)
+    sl = s.tolist()
+    out["p6"] = 4.0 * e * np.array([x ** 6 for x in sl])
+    out["p12"] = 4.0 * e * np.array([x ** 12 for x in sl])
+    return out
 
 
 def _assemble(crd, vel, box, charge, mass, atom_type, lj_types, bonds, angles, excl, pairs, trios,
@@ -157,6 +161,8 @@ def _saw_chain(rng, n_backbone, radius, bond=1.53, angle_deg=111.0, min_dist=3.2
     d0 = rng.normal(size=3)
     d0 /= np.linalg.norm(d0)
     pts.append(pts[0] + bond * d0)
+    buf = np.zeros((n_backbone, 3))  # pts as an array (rows past len(pts) are stale)
+    buf[:2] = pts
     restarts = 0
     while len(pts) < n_backbone:
         ok = False
@@ -174,9 +180,10 @@ def _saw_chain(rng, n_backbone, radius, bond=1.53, angle_deg=111.0, min_dist=3.2
             cand = pts[-1] + bond * d
             if np.linalg.norm(cand) > radius:
                 continue
-            arr = np.asarray(pts[:-2])
+            arr = buf[:len(pts) - 2]
             if len(arr) and np.min(np.linalg.norm(arr - cand, axis=1)) < min_dist:
                 continue
+            buf[len(pts)] = cand
             pts.append(cand)
             ok = True
             break
@@ -192,7 +199,9 @@ def chain_water_system(n_chain=2000, n_waters=30000, seed=1, radius=30.0, box=No
     the preceding backbone atom; backbone bonds 1.53 A / 310, angles 111 deg / 63 (E = k(x-x0)^2,
     ForceField.cpp:108-177).  Charges ~ N(0, 0.25) shifted to zero net; sigma ~ U(2.5, 3.8),
     epsilon ~ U(0.02, 0.2) binned into n_sigma_bins x n_eps_bins LJ types with Lorentz-Berthelot
-    mixing.  Waters within 2.4 A of the solute are removed.  Exclusions: 1-2, 1-3 and 1-4 pairs."""
+    mixing, or, with n_sigma_bins=None, one LJ type per chain atom with its own sigma and
+    epsilon (exact Lorentz-Berthelot mixing over an (n_chain + 2)^2 table).  Waters within 2.4 A
+    of the solute are removed.  Exclusions: 1-2, 1-3 and 1-4 pairs."""
     rng = np.random.default_rng(seed)
     n_h = n_chain // 3
     n_bb = n_chain - n_h
@@ -216,6 +225,8 @@ def chain_water_system(n_chain=2000, n_waters=30000, seed=1, radius=30.0, box=No
     crd_c[bb_index] = bb
     pos_of_bb = {idx: k for k, idx in enumerate(bb_index)}
     placed = list(bb_index)
+    is_placed = np.zeros(n_c, bool)
+    is_placed[bb_index] = True
     for h, p in parent_of_h.items():
         # start on the outer bisector of the parent's backbone angle; keep the direction that
         # leaves the H farthest from every other chain atom
@@ -228,39 +239,53 @@ def chain_water_system(n_chain=2000, n_waters=30000, seed=1, radius=30.0, box=No
         if np.linalg.norm(v0) < 1e-6:
             v0 = rng.normal(size=3)
         best, best_d = None, -1.0
-        others = np.asarray([crd_c[i] for i in placed if i != p])
+        # every candidate lies 1.09 A from the parent, so only placed atoms within 8 A of the
+        # parent can be a candidate's nearest one (the backbone neighbours are ~2.5 A away)
+        near = is_placed.copy()
+        near[p] = False
+        others = crd_c[near]
+        others = others[np.einsum("ij,ij->i", others - crd_c[p], others - crd_c[p]) < 64.0]
         for t in range(64):
             v = v0 / np.linalg.norm(v0) if t == 0 else v0 / np.linalg.norm(v0) + 0.8 * rng.normal(size=3)
             v /= np.linalg.norm(v)
             cand = crd_c[p] + 1.09 * v
-            dmin = np.min(np.linalg.norm(others - cand, axis=1)) if len(others) else 9.0
+            dmin = math.sqrt(np.min(((others - cand) ** 2).sum(1))) if len(others) else 9.0
             if dmin > best_d:
                 best, best_d = cand, dmin
             if dmin >= 2.6:
                 break
         crd_c[h] = best
         placed.append(h)
+        is_placed[h] = True
     sig = rng.uniform(2.5, 3.8, n_c)
     eps = rng.uniform(0.02, 0.2, n_c)
-    sb = np.minimum((sig - 2.5) / 1.3 * n_sigma_bins, n_sigma_bins - 1).astype(int)
-    eb = np.minimum((eps - 0.02) / 0.18 * n_eps_bins, n_eps_bins - 1).astype(int)
     lj_types = [(SIGMA_O, EPS_O), (0.0, 0.0)]
-    for i in range(n_sigma_bins):
-        for j in range(n_eps_bins):
-            lj_types.append((2.5 + (i + 0.5) * 1.3 / n_sigma_bins, 0.02 + (j + 0.5) * 0.18 / n_eps_bins))
-    type_c = 2 + sb * n_eps_bins + eb
+    if n_sigma_bins is None:
+        lj_types += [(float(a), float(b)) for a, b in zip(sig, eps)]
+        type_c = 2 + np.arange(n_c)
+    else:
+        sb = np.minimum((sig - 2.5) / 1.3 * n_sigma_bins, n_sigma_bins - 1).astype(int)
+        eb = np.minimum((eps - 0.02) / 0.18 * n_eps_bins, n_eps_bins - 1).astype(int)
+        for i in range(n_sigma_bins):
+            for j in range(n_eps_bins):
+                lj_types.append((2.5 + (i + 0.5) * 1.3 / n_sigma_bins, 0.02 + (j + 0.5) * 0.18 / n_eps_bins))
+        type_c = 2 + sb * n_eps_bins + eb
     q = rng.normal(0.0, 0.25, n_c)
     q -= q.mean()
     mass_c = np.where(np.isin(np.arange(n_c), list(parent_of_h.keys())), M_H, 12.011)
     box = float(box if box is not None else water_box_side(n_waters + n_chain / 3.0))
     # waters on a lattice filling the box, solute at the centre, then overlap removal
     w = water_positions(rng, n_waters, box, jitter=0.3).reshape(n_waters, 3, 3) - 0.5 * box
-    dmin = np.full(n_waters, np.inf)
-    for start in range(0, n_c, 256):
-        blk = crd_c[start:start + 256]
-        d = np.linalg.norm(w[:, None, :, :] - blk[None, :, None, :], axis=-1).min(axis=(1, 2))
-        dmin = np.minimum(dmin, d)
-    w = w[dmin >= 2.4]
+    # a water goes when one of its atoms lies within 2.4 A of a solute atom; only the atom pairs
+    # a k-d tree finds within 2.5 A can be that close, and those are measured exactly
+    from scipy.spatial import cKDTree
+    wa = w.reshape(-1, 3)
+    hits = cKDTree(crd_c).query_ball_point(wa, 2.5)
+    close = np.zeros(n_waters, bool)
+    for k, js in enumerate(hits):
+        if js and np.sqrt(((crd_c[js] - wa[k]) ** 2).sum(1)).min() < 2.4:
+            close[k // 3] = True
+    w = w[~close]
     nw = len(w)
     crd = np.concatenate([crd_c, w.reshape(-1, 3)]) + 0.5 * box
     n = len(crd)

@@ -21,7 +21,10 @@ import os
 import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_ROOT = os.environ.get("OG_REFERENCE_ROOT", "/root/reference")
+# The reference checkout this recipe compiles from, where it lies (read-only; nothing is written
+# there).  OG_REFERENCE_ROOT, or the ref_root argument of build_ref, names another checkout.
+REF_CHECKOUT = "/root/reference"
+REF_ROOT = os.environ.get("OG_REFERENCE_ROOT") or REF_CHECKOUT
 REF_OUT = os.path.join(HERE, "_ref")
 
 CORE = [
@@ -55,13 +58,14 @@ def build_oracle(force=False):
     return out
 
 
-def reference_available():
-    return os.path.isdir(os.path.join(REF_ROOT, "src", "celeste", "core"))
+def reference_available(ref_root=None):
+    return os.path.isdir(os.path.join(ref_root or REF_ROOT, "src", "celeste", "core"))
 
 
-def build_ref(force=False, jobs=8):
+def build_ref(force=False, jobs=8, ref_root=None):
     """Compile the reference pieces; returns the output directory or None if absent."""
-    if not reference_available():
+    REF_ROOT = ref_root or globals()["REF_ROOT"]
+    if not reference_available(REF_ROOT):
         return None
     core = os.path.join(REF_ROOT, "src", "celeste", "core")
     rnd = os.path.join(REF_ROOT, "src", "celeste", "random", "Random.cpp")

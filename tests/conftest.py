@@ -7,16 +7,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REFERENCE_ROOT = os.environ.get("OG_REFERENCE_ROOT", "/root/reference")
-
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
     config.addinivalue_line("markers", "slow: long-running CPU test")
-
-
-@pytest.fixture(scope="session")
-def reference_root():
-    if not os.path.isdir(os.path.join(REFERENCE_ROOT, "samples")):
-        pytest.skip("reference tree not present")
-    return REFERENCE_ROOT

@@ -29,4 +29,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python %s <reference checkout root>" % os.path.basename(__file__))
+    main(sys.argv[1])

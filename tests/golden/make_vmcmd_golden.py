@@ -136,4 +136,6 @@ def make_ala3_vmcmd(ref_root):
 
 if __name__ == "__main__":
     make_mt_vectors()
-    make_ala3_vmcmd(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python %s <reference checkout root>" % os.path.basename(__file__))
+    make_ala3_vmcmd(sys.argv[1])

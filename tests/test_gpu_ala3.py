@@ -73,3 +73,31 @@ def test_ala3_tracks_reference_log():
                 continue
             got = tr[i, names.index(k)]
             assert abs(got - ref) <= 1e-5 * abs(ref) + 1e-4, (i, k, got, ref)
+
+
+@pytest.mark.parametrize("run", ["shake", "shake_heating", "noshake"])
+def test_ala3_thermostat_tracks_reference_runs(run):
+    """The engine's velocity-scaling thermostat against the reference's own runs of the ala3
+    sample (tests/golden/ala3_thermo.json): with SHAKE (the iterative loop of
+    Thermostat.cpp:86-170, as a device-side loop), with a heating ramp, and without constraints
+    (Thermostat.cpp:57-84).  Over ten steps every printed term within 1e-5 |E| + 1e-4 kcal/mol
+    (the FP32 pair forces start a separation of ~1e-7 per step); the temperature within 1e-6
+    relative of what the reference printed."""
+    s, _ = _golden()
+    gold = json.load(open(os.path.join(HERE, "golden", "ala3_thermo.json")))["runs"][run]
+    n = 10
+    eng = engine.Engine(0)
+    eng.add_system(s, gold["params"])
+    eng.finalize()
+    eng.set_trace(n)
+    eng.step(n)
+    tr = eng.get_trace(n)[:, 0, :]
+    names = engine.ENERGY_NAMES
+    for i, row in enumerate(gold["steps"][:n]):
+        for k, ref in row.items():
+            if k == "step":
+                continue
+            got = tr[i, names.index(k)]
+            tol = 1e-6 * abs(ref) if k == "temperature" else 1e-5 * abs(ref) + 1e-4
+            assert abs(got - ref) <= tol, (run, i, k, got, ref)
+    assert eng.flags() & 16 == 0  # the thermostat loop converged within its limit

@@ -104,6 +104,37 @@ def test_forces_energies_virial_vs_fp64(name, make, variant):
     assert np.linalg.norm(vir - w64) <= 1e-5 * np.linalg.norm(w64), (vir, w64)
 
 
+@pytest.mark.parametrize("name,make", SMALL, ids=[n for n, _ in SMALL])
+def test_fp64_variant_matches_fp64_oracle(name, make):
+    """The FP64 validation variant evaluates what the FP64 oracle evaluates (the same list, the
+    same formulas in double precision): forces within 1e-9 RMS relative (the fixed-point
+    accumulators resolve 2^-32 kcal/mol/A), energies within 1e-9 relative; the virial within
+    1e-7 (its x (x) f part reads positions from the FP32 cell-relative offsets)."""
+    s = make()
+    p = _params()
+    eng = _engine([(s, p, None)], engine.PAIR_VARIANT_F64)
+    assert eng.tuning()["pair_variant"] == engine.PAIR_VARIANT_F64
+    eng.compute_forces()
+    work, ene, vir = eng.get_forces(0)
+    md = ogo.OracleMD(s, p)
+    e64 = md.forces(virial=True)
+    assert _rel_rms(work, md.work.reshape(-1, 3)) <= 1e-9
+    for k in ("vdw", "ele", "bond", "angle", "potential"):
+        assert abs(ene[k] - e64[k]) <= 1e-9 * abs(e64[k]) + 1e-9, (k, ene[k], e64[k])
+    # the virial's x (x) f part takes the positions from the FP32 cell-relative offsets
+    assert np.linalg.norm(vir - e64["virial"]) <= 1e-7 * np.linalg.norm(e64["virial"])
+
+
+def test_fp64_variant_refuses_other_models():
+    s = systems.water_system(700, seed=9)
+    eng = engine.Engine(0)
+    eng.set_tuning(engine.PAIR_VARIANT_F64)
+    eng.add_system(s, _params(electrostatic="zero-quadrupole"))
+    with pytest.raises(engine.OgError) as ex:
+        eng.finalize()
+    assert ex.value.status == engine.OG_ERR_INVALID
+
+
 def test_forces_bitwise_reproducible():
     s = systems.water_system(3000, box=44.8, seed=0, lattice_m=15)
     eng = _engine([(s, _params(), None)])
@@ -175,24 +206,57 @@ def test_mcmd_scaling_matches_oracle():
         assert abs(tr[i, names.index("potential")] - r["potential"]) <= 1e-5 * abs(r["potential"]) + 5e-3
 
 
-@pytest.mark.parametrize("variant", [1, 6, 8])
+@pytest.mark.parametrize("variant", [1, 6, 8, 9, 10])
 def test_batch_invariance_bitwise(variant):
     """A system gives the same trajectory alone and batched with others (fixed-point forces,
     per-system fixed-order reductions), for a given pair-kernel variant (variants of different
-    families add FP32 partial sums in different orders)."""
+    families add FP32 partial sums in different orders).  The mix holds a deliberately hot
+    system (velocities x4, no thermostat): with the j-list kernel (variant 10) its atoms pass
+    the skin far more often than the others', so the engine rebuilds j lists at steps where
+    the system under test alone would not; only the hot system's lists may change then."""
     a = systems.water_system(1500, seed=5)
-    others = [systems.water_system(700, seed=9), systems.chain_water_system(300, 2500, seed=4, radius=12.0)]
+    hot = systems.water_system(700, seed=9)
+    hot = dict(hot, vel=np.asarray(hot["vel"]) * 4.0)
+    chain = systems.chain_water_system(300, 2500, seed=4, radius=12.0)
     p = _params(nsgrid_update_intvl=10, time_step=2.0, thermostat="scaling", temperature=300.0)
+    p_hot = _params(nsgrid_update_intvl=10, time_step=2.0)
     alone = _engine([(a, p, None)], variant)
     alone.set_trace(25)
     alone.step(25)
-    mixed = _engine([(others[0], p, None), (a, p, None), (others[1], p, None)], variant)
+    mixed = _engine([(hot, p_hot, None), (a, p, None), (chain, p, None)], variant)
     mixed.set_trace(25)
     mixed.step(25)
     np.testing.assert_array_equal(alone.get_trace(25)[:, 0, :], mixed.get_trace(25)[:, 1, :])
     c1, v1 = alone.get_state(0)
     c2, v2 = mixed.get_state(1)
     assert np.array_equal(c1, c2) and np.array_equal(v1, v2)
+    if variant == 10:
+        # the hot system forced j-list builds that the system alone did not have
+        assert mixed.jlist_builds() > alone.jlist_builds() >= 3, (mixed.jlist_builds(), alone.jlist_builds())
+
+
+def test_jlist_put_state_of_other_system_keeps_bits():
+    """Variant 10: moving a molecule of another system through og_put_state between steps marks
+    only that system's j lists stale; the system under test keeps its trajectory bit for bit."""
+    a = systems.water_system(1500, seed=5)
+    b = systems.water_system(700, seed=9)
+    p = _params(nsgrid_update_intvl=10, time_step=2.0)
+    alone = _engine([(a, p, None)], 10)
+    mixed = _engine([(a, p, None), (b, p, None)], 10)
+    for k in range(3):
+        alone.step(3)
+        mixed.step(3)
+        crd, _ = mixed.get_state(1)
+        crd = crd.copy()
+        crd[3 * (10 + k):3 * (11 + k)] += np.array([0.8, -0.5, 0.3])  # one water, 1 A
+        mixed.put_state_ptr(1, crd.ctypes.data, None)
+        mixed.synchronize()
+    alone.step(7)
+    mixed.step(7)
+    c1, v1 = alone.get_state(0)
+    c2, v2 = mixed.get_state(0)
+    assert np.array_equal(c1, c2) and np.array_equal(v1, v2)
+    assert mixed.jlist_builds() > alone.jlist_builds()
 
 
 def test_nve_drift_small():

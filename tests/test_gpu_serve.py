@@ -27,12 +27,18 @@ def _jobs():
     return [serve.Job(k, systems.water_system(n, seed=40 + k), p, steps) for k, (n, steps, p) in enumerate(spec)]
 
 
-def test_served_jobs_equal_alone_runs():
+@pytest.mark.parametrize("variant", [6, 10, "auto"])
+def test_served_jobs_equal_alone_runs(variant):
+    """Also with the j-list kernel (variant 10) and the autotuner's pick: a job's j lists are
+    rebuilt when its own atoms pass the skin, never because another job's did."""
     jobs = _jobs()
-    res = serve.Server(0, max_jobs=3, window=20, pair_variant=6).run(jobs)
+    srv = serve.Server(0, max_jobs=3, window=20, pair_variant=variant)
+    res = srv.run(jobs)
     assert res["n_jobs"] == 5 and res["relayouts"] >= 3
+    used = srv.pair_variant  # "auto" resolves to the first engine's autotuned variant
+    assert used != "auto"
     for j in jobs:
-        _, ene, crd, vel = serve.run_alone(serve.Job(j.id, j.system, j.params, j.n_steps), pair_variant=6)
+        _, ene, crd, vel = serve.run_alone(serve.Job(j.id, j.system, j.params, j.n_steps), pair_variant=used)
         assert np.array_equal(j.crd, crd) and np.array_equal(j.vel, vel), j.id
         assert j.energies == ene, j.id
 
@@ -55,13 +61,14 @@ def _engine(batch, variant=6):
     return eng
 
 
-def test_faulted_system_is_isolated():
+@pytest.mark.parametrize("variant", [6, 10])
+def test_faulted_system_is_isolated(variant):
     """A caller-placed coordinate far outside one system's box makes og_step fail with
     OG_ERR_SYSTEM_FAULT naming that system only; every system is back at the call's start, and
     the others, stepped again without it, match their runs alone bit for bit."""
     p = _params(nsgrid_update_intvl=10, time_step=2.0, thermostat="scaling", temperature=300.0)
     sy = [systems.water_system(n, seed=60 + k) for k, n in enumerate((900, 700, 800))]
-    eng = _engine([(s, p) for s in sy])
+    eng = _engine([(s, p) for s in sy], variant)
     start = [eng.get_state(i) for i in range(3)]
     crd, vel = start[1]
     crd = crd.copy()
@@ -75,17 +82,18 @@ def test_faulted_system_is_isolated():
     for i in (0, 2):
         c, v = eng.get_state(i)
         assert np.array_equal(c, start[i][0]) and np.array_equal(v, start[i][1])
-    rest = _engine([(sy[0], p), (sy[2], p)])
+    rest = _engine([(sy[0], p), (sy[2], p)], variant)
     rest.step(20)
     for k, i in enumerate((0, 2)):
-        alone = _engine([(sy[i], p)])
+        alone = _engine([(sy[i], p)], variant)
         alone.step(20)
         c1, v1 = alone.get_state(0)
         c2, v2 = rest.get_state(k)
         assert np.array_equal(c1, c2) and np.array_equal(v1, v2)
 
 
-def test_served_vmcmd_jobs_equal_alone_runs():
+@pytest.mark.parametrize("variant", [6, 10])
+def test_served_vmcmd_jobs_equal_alone_runs(variant):
     """V-McMD jobs handed between engines keep their virtual state and generator: the served
     virtual-state and lambda logs and final states equal the alone runs' bit for bit."""
     rt = 8.31451 / 4.184 * 1e-3 * 300.0
@@ -98,13 +106,13 @@ def test_served_vmcmd_jobs_equal_alone_runs():
         p = _params(nsgrid_update_intvl=10, time_step=2.0, thermostat="scaling", temperature=300.0,
                     random_seed=300 + k, print_intvl_extended_lambda=2)
         jobs.append(serve.Job(k, systems.water_system(n, seed=80 + k), p, steps, mcmd=vm))
-    res = serve.Server(0, max_jobs=2, window=20, pair_variant=6).run(jobs)
+    res = serve.Server(0, max_jobs=2, window=20, pair_variant=variant).run(jobs)
     assert res["n_jobs"] == 3 and res["relayouts"] >= 3
     for j in jobs:
         logs = {}
         fresh = serve.Job(j.id, j.system, j.params, j.n_steps, mcmd={k: v for k, v in j.mcmd.items()
                                                                       if k not in ("cur_vs", "mt_state")})
-        _, ene, crd, vel = serve.run_alone(fresh, pair_variant=6, logs=logs)
+        _, ene, crd, vel = serve.run_alone(fresh, pair_variant=variant, logs=logs)
         assert np.array_equal(j.crd, crd) and np.array_equal(j.vel, vel), j.id
         assert j.vs_log == logs["vs"] and j.lambda_log == logs["lambda"], j.id
         assert len(j.vs_log) == (j.n_steps - 1) // 3 and len({v for _, v in j.vs_log}) > 1  # steps 3, 6 .. < n

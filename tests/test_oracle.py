@@ -23,8 +23,11 @@ def _cell_list_case(s, cutoff=13.0):
 
 @pytest.fixture(scope="module")
 def ref_built():
-    if obuild.build_ref() is None or ogo.ref_lib() is None:
-        pytest.skip("reference sources not available to build oracle/_ref")
+    """The reference's MiniCell built into oracle/_ref (rebuilt first when its sources are
+    present; a prebuilt library is used as it is)."""
+    obuild.build_ref()
+    if ogo.ref_lib() is None:
+        pytest.skip("oracle/_ref was not built (reference sources absent)")
     return True
 
 
@@ -41,11 +44,21 @@ def test_cell_list_matches_reference_minicell(ref_built, n_waters, box, seed):
     np.testing.assert_array_equal(ours.slot_crd, ref["slot_crd"])
 
 
-def test_cell_list_matches_reference_on_ala3(ref_built, reference_root):
+def _ala3_system():
+    """The reference's ala3 launch set (samples/ala3/md.inp.cls), from the committed fixture."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_ala3_golden", os.path.join(HERE, "golden",
+                                                                                 "make_ala3_golden.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.load_system()
+
+
+def test_cell_list_matches_reference_on_ala3(ref_built):
     """ala3's coordinates come from a PDB (0.001 A grid), so atoms of one column can share a
     float z; the reference's quicksort orders such ties arbitrarily.  A seeded 1e-3 A
     perturbation removes the ties; both implementations get the same coordinates."""
-    s = cls_io.read_cls(os.path.join(reference_root, "samples/ala3/md.inp.cls"))
+    s = _ala3_system()
     s["crd"] = s["crd"] + np.random.default_rng(11).uniform(-1e-3, 1e-3, s["crd"].shape)
     nb, pbc, crd, geom = _cell_list_case(s)
     ours = ogo.CellList(pbc, geom, crd, nb)
@@ -64,8 +77,8 @@ def test_reference_capacity_guard():
     assert ours.n_pairs > ogo.ref_pair_capacity(geom, s["n_atoms"])
 
 
-def _ala3_energies(reference_root):
-    s = cls_io.read_cls(os.path.join(reference_root, "samples/ala3/md.inp.cls"))
+def _ala3_energies():
+    s = _ala3_system()
     n, t = s["n_atoms"], s["topol"]
     nb = cls_io.nb15off_table(n, t["nb15off_pairs"])
     pbc = ogo.make_pbc(s["pbc_val"])
@@ -84,9 +97,9 @@ def _ala3_energies(reference_root):
     return ene[0], ene[1] + exc + self_e
 
 
-def test_oracle_reproduces_ala3_known_answer(reference_root):
+def test_oracle_reproduces_ala3_known_answer():
     gold = json.load(open(os.path.join(HERE, "golden", "ala3_step0.json")))["step0"]
-    vdw, ele = _ala3_energies(reference_root)
+    vdw, ele = _ala3_energies()
     assert float("%.10e" % vdw) == gold["VDW"]
     assert float("%.10e" % ele) == gold["Ele"]
 
@@ -142,3 +155,22 @@ def test_oracle_reproduces_ala3_log_trajectory():
             if key == "step":
                 continue
             assert float("%.10e" % got[key]) == ref, (row["step"], key, got[key], ref)
+
+
+def test_oracle_reproduces_reference_thermostat_runs():
+    """The velocity-scaling thermostat against the reference's own runs of its ala3 sample
+    (tests/golden/ala3_thermo.json, made by make_thermo_golden.py with the reference's all-pairs
+    program): the thermostat-with-SHAKE loop at 300 K (Thermostat.cpp:86-170), the same with a
+    heating ramp 200 -> 300 K (SubBox.cpp:1745-1757), and the unconstrained scaling
+    (Thermostat.cpp:57-84).  Every printed energy of the first eight steps, to the printed 11
+    significant digits."""
+    s, _ = _ala3_golden()
+    gold = json.load(open(os.path.join(HERE, "golden", "ala3_thermo.json")))
+    for name, run in gold["runs"].items():
+        md = ogo.OracleMD(s, run["params"], pair_mode="allpairs_f32")
+        for row in run["steps"][:8]:
+            got = md.step()
+            for key, ref in row.items():
+                if key == "step":
+                    continue
+                assert float("%.10e" % got[key]) == ref, (name, row["step"], key, got[key], ref)

@@ -55,10 +55,40 @@ def test_noalloc_matches_allocating_entry_point_twice():
             assert np.array_equal(got, ref)  # same kernels, same chunking: same bits
 
 
+def test_noalloc_exact_fit_uses_the_whole_scratch():
+    """16 segments x 4096 chunks fill the 65,536 scratch entries exactly; the last segment is
+    long enough to write (and read back) the last entry.  Same bits as og_segment_sum, twice."""
+    import torch
+    sum_alloc, sum_noalloc = _fns()
+    rng = np.random.default_rng(11)
+    lens = [5, 0, 4096, 70000] + [3] * 11 + [4095 * 4096 + 17]  # ceil(len / 4096) = 4096 for the last
+    max_len = 4096 * 4096
+    vals = torch.tensor(rng.normal(size=sum(lens)), device="cuda")
+    base = torch.tensor(np.concatenate([[0], np.cumsum(lens)]), dtype=torch.int32, device="cuda")
+    rc_a, ref = _run(sum_alloc, vals, base, max_len)
+    assert rc_a == engine.OG_OK
+    for _ in range(2):
+        rc, got = _run(sum_noalloc, vals, base, max_len)
+        assert rc == engine.OG_OK
+        assert np.array_equal(got, ref)
+    last = vals[int(base[-2]):].cpu().numpy()
+    np.testing.assert_allclose(got[-1], last.sum(), rtol=1e-10, atol=1e-8)
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch():
     import torch
-    _, sum_noalloc = _fns()
+    sum_alloc, sum_noalloc = _fns()
     vals = torch.zeros(16, dtype=torch.float64, device="cuda")
     base = torch.zeros(70001, dtype=torch.int32, device="cuda")
     rc, _ = _run(sum_noalloc, vals, base, 4096)  # 70000 segments x 1 chunk > 65536 entries
     assert rc == engine.OG_ERR_CAPACITY
+    # one more chunk than the scratch holds: 16 segments x 4097 chunks
+    rc, _ = _run(sum_noalloc, vals, torch.zeros(17, dtype=torch.int32, device="cuda"), 4096 * 4096 + 1)
+    assert rc == engine.OG_ERR_CAPACITY
+    # the grid's segment limit: 65,535 segments fit, 65,536 (which the scratch alone would
+    # hold) are refused by both entry points instead of failing at launch
+    for fn in (sum_alloc, sum_noalloc):
+        rc, out = _run(fn, vals, torch.zeros(65536, dtype=torch.int32, device="cuda"), 4096)
+        assert rc == engine.OG_OK and np.array_equal(out, np.zeros(65535))
+        rc, _ = _run(fn, vals, torch.zeros(65537, dtype=torch.int32, device="cuda"), 4096)
+        assert rc == engine.OG_ERR_CAPACITY
