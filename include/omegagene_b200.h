@@ -284,6 +284,21 @@ og_status og_get_tuning(og_engine *e, int32_t *pair_variant, double *variant_ms)
  * whenever an atom has moved farther than the skin (0.35 A, or OG_JL_SKIN in the environment)
  * since the last.  0 for the other variants. */
 og_status og_get_jlist_builds(og_engine *e, int64_t *n_builds);
+/* Cell-pair list schedule, set before og_finalize (engine-wide).  OG_LIST_FIXED (default) is the
+ * reference's: the list is rebuilt every nsgrid_update_intvl steps (DynamicsModePresto::
+ * calc_in_each_step, DynamicsMode.cpp:480), and an atom that moves farther than the margin
+ * (nsgrid_cutoff - cutoff) between rebuilds loses pairs, as in the reference.
+ * OG_LIST_DISPLACEMENT rebuilds it before a step whenever an atom has moved farther than half the
+ * margin since the last build (checked on the device every step; inside a graph replay the
+ * build is a conditional node), so every pair within the cutoff is in the list: the list is
+ * exact (with no margin, nsgrid_cutoff = cutoff, it is rebuilt every step).  In a batch the rebuild is engine-wide: one system's
+ * moving atom rebuilds every system's list, so results are bitwise independent of the batch only
+ * under OG_LIST_FIXED.  No counterpart in the reference. */
+#define OG_LIST_FIXED 0
+#define OG_LIST_DISPLACEMENT 1
+og_status og_set_list_policy(og_engine *e, int32_t policy);
+/* Cell-pair list builds since og_create (both policies; og_compute_forces builds one too). */
+og_status og_get_list_builds(og_engine *e, int64_t *n_builds);
 /* Fixes the pair-kernel variant (0..OG_N_PAIR_VARIANTS-1, or OG_PAIR_VARIANT_F64) before og_finalize and skips the autotuner, e.g. when a
  * serving loop re-creates engines for new batches; -1 restores autotuning.  No counterpart in
  * the reference, which has one pair kernel. */

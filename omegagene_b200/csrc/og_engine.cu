@@ -118,7 +118,7 @@ __global__ void k_shake_quad(int, const int4 *, const double *, const int *, con
                              double *, const double *, int, double, int *);
 __global__ void k_finish(int, const int *, const SysDev *, int, double *, const double *, const double *, double *,
                          const int *, double *, const double *, float4 *, const float *, double *, int *, int *,
-                         const float4 *, float, int *);
+                         const float4 *, float, int *, const float4 *);
 __global__ void k_slot_refresh(const int *, int, const int *, const double *, const double *, const float *,
                                const int *, float4 *, int *);
 __global__ void k_energies(int, const SysDev *, const double *, const double *, double *, double *, int,
@@ -127,7 +127,9 @@ __global__ void k_trace_advance(long long *, long long *);
 __global__ void k_capture_frames(int, const int *, const int *, const int *, const SysDev *, const long long *,
                                  const double *, const double *, float *, double *);
 __global__ void k_put_state(int, int, const int *, const SysDev *, const double *, const double *, double *, double *,
-                            const int *, double *, const double *, float4 *, const float4 *, float, int *, int *);
+                            const int *, double *, const double *, float4 *, const float4 *, float, int *,
+                            const float4 *, int *);
+__global__ void k_list_cond(const int *, cudaGraphConditionalHandle);
 
 __global__ void k_fill_int(int *p, long long n, int v) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -237,6 +239,14 @@ struct og_engine {
     int *d_jl_count = nullptr;
     float4 *d_xq_ref = nullptr;
     int *d_jl_stale = nullptr;   // per system: its j lists must be rebuilt before the next pair launch
+    // cell-pair list schedule: OG_LIST_FIXED (the reference's, every nsgrid_update_intvl steps) or
+    // OG_LIST_DISPLACEMENT (whenever an atom has moved half the list margin since the last build)
+    int list_policy = OG_LIST_FIXED;
+    float4 *d_xq_build = nullptr;  // slot offsets at the last list build (displacement policy only)
+    // launch accounting of the conditional list build inside graph replays: the kernels of one
+    // build (not counted per replay), builds launched kernel by kernel in the current og_step, and
+    // the list-build counter as last read from the device
+    long long cond_build_kernels = 0, host_cond_builds = 0, builds_seen = 0;
     float jl_skin = OG_JL_SKIN;
     unsigned long long *d_frc = nullptr;
     int *d_uni_lo = nullptr, *d_uni_hi = nullptr;
@@ -489,6 +499,8 @@ og_status setup_geometry(og_engine *e, HostSystem &h) {
     // least 1 A) has left every list built for it: the system has blown up.
     const double margin = std::max(d.nsgrid_cutoff - d.cutoff, 1.0);
     S.max_step_disp2 = margin * margin;
+    const double half = 0.5 * (d.nsgrid_cutoff - d.cutoff);
+    S.list_trig2 = (float)(half * half);
     return OG_OK;
 }
 
@@ -695,6 +707,7 @@ og_status scan_exclusive(og_engine *e, const int *in, int *out, long long n, int
 
 og_status build_list(og_engine *e) {
     cudaStream_t st = e->stream;
+    if (e->d_xq_build) CK(cudaMemsetAsync(e->d_counters + OG_CNT_LIST_STALE, 0, sizeof(int), st));
     CK(cudaMemsetAsync(e->d_col_count, 0, sizeof(int) * e->n_cols, st));
     CK(cudaMemsetAsync(e->d_col_fill, 0, sizeof(int) * e->n_cols, st));
     k_assign_columns<<<blocks(e->n_atoms, 256), 256, 0, st>>>(e->d_sys, e->d_atom_sys, e->d_crd, e->n_atoms,
@@ -726,6 +739,8 @@ og_status build_list(og_engine *e) {
                                                                e->d_slot_crd, e->d_cell_origin, e->d_charge_f,
                                                                e->d_atom_type, e->d_xq, e->d_slot_type);
     LAUNCH_CHECK();
+    if (e->d_xq_build)
+        CK(cudaMemcpyAsync(e->d_xq_build, e->d_xq, sizeof(float4) * (size_t)e->slots_cap, cudaMemcpyDeviceToDevice, st));
     k_cell_excl<<<blocks(e->cells_cap, 256), 256, 0, st>>>(e->d_counters, e->cells_cap, e->d_slot_atom,
                                                             e->d_atom_slot, e->d_excl_start, e->d_excl_list,
                                                             e->d_cell_excl);
@@ -1104,13 +1119,66 @@ og_status thermostat_with_shake(og_engine *e) {
     return OG_OK;
 }
 
+// Displacement list policy, kernel by kernel: the host reads the stale mark (one 4-byte copy and
+// a stream synchronisation per step) and builds the list when it is set.
+og_status build_list_if_stale(og_engine *e) {
+    CK(cudaMemcpyAsync(e->h_pinned + 8, e->d_counters + OG_CNT_LIST_STALE, sizeof(int), cudaMemcpyDeviceToHost,
+                       e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    if (!e->h_pinned[8]) return OG_OK;
+    e->host_cond_builds++;
+    return build_list(e);
+}
+
+// Displacement list policy inside a captured graph: a conditional IF node whose body is the list
+// build, its condition set on the device from the stale mark (k_list_cond), so replays rebuild
+// exactly when an atom has moved half the margin.
+og_status build_list_if_stale_captured(og_engine *e) {
+    cudaStream_t st = e->stream;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t n_deps = 0;
+    CK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &n_deps));
+    if (cs != cudaStreamCaptureStatusActive || !g) return fail(e, OG_ERR_STATE, "list build: stream not capturing");
+    cudaGraphConditionalHandle cond;
+    CK(cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault));
+    k_list_cond<<<1, 32, 0, st>>>(e->d_counters, cond);
+    LAUNCH_CHECK();
+    CK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &n_deps));
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = cond;
+    np.conditional.type = cudaGraphCondTypeIf;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, deps, n_deps, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    CK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    CK(cudaStreamBeginCaptureToGraph(e->side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    e->stream = e->side;
+    const long long l0 = e->launches;
+    og_status s = build_list(e);
+    e->cond_build_kernels = e->launches - l0;  // counted per build that runs, not per replay
+    e->launches = l0;
+    e->stream = st;
+    cudaGraph_t captured = nullptr;
+    cudaError_t r = cudaStreamEndCapture(e->side, &captured);
+    if (s) return s;
+    CK(r);
+    return OG_OK;
+}
+
 // ene: evaluate this step's energies.  They are needed on every step when a system is
 // McMD-scaled (the factor depends on the potential) or the energy trace is on, and otherwise
 // only on the last step of a call, whose energies og_get_energies reads.
 og_status run_step(og_engine *e, bool ene) {
     cudaStream_t st = e->stream;
     og_status s;
-    if (e->host_step % e->intvl == 0) {
+    if (e->list_policy == OG_LIST_DISPLACEMENT) {
+        s = e->capturing ? build_list_if_stale_captured(e) : build_list_if_stale(e);
+        if (s) return s;
+    } else if (e->host_step % e->intvl == 0) {
         s = build_list(e);
         if (s) return s;
     }
@@ -1150,7 +1218,7 @@ og_status run_step(og_engine *e, bool ene) {
                                                        e->d_crd_prev, e->d_vel, e->d_vel_next, e->d_atom_slot,
                                                        e->d_slot_crd, e->d_cell_origin, e->d_xq, e->d_mass, e->d_ke,
                                                        e->d_counters, e->d_sys_fault, e->d_xq_ref,
-                                                       e->jl_skin * e->jl_skin, e->d_jl_stale);
+                                                       e->jl_skin * e->jl_skin, e->d_jl_stale, e->d_xq_build);
     LAUNCH_CHECK();
     if ((s = seg_sum<1>(e, e->d_ke, 1, 0, e->d_seg_atoms, e->mc_atoms, e->d_sys_acc, OG_ACC_SIZE, OG_ACC_KIN, 0)))
         return s;
@@ -1297,6 +1365,7 @@ og_status read_counters(og_engine *e, int *out) {
     CK(cudaMemcpyAsync(e->h_pinned, e->d_counters, sizeof(int) * OG_CNT_SIZE, cudaMemcpyDeviceToHost, e->stream));
     CK(cudaStreamSynchronize(e->stream));
     memcpy(out, e->h_pinned, sizeof(int) * OG_CNT_SIZE);
+    e->builds_seen = out[OG_CNT_LIST_BUILDS];
     return OG_OK;
 }
 
@@ -1992,6 +2061,7 @@ og_status og_finalize(og_engine *e) {
         (s = dalloc(e, &e->d_bbox, 2 * (size_t)cells_cap)) ||
         (s = dalloc(e, &e->d_slot_atom, e->slots_cap)) || (s = dalloc(e, &e->d_slot_type, e->slots_cap)) ||
         (s = dalloc(e, &e->d_slot_crd, 3 * (size_t)e->slots_cap)) || (s = dalloc(e, &e->d_xq, e->slots_cap)) ||
+        (e->list_policy == OG_LIST_DISPLACEMENT && (s = dalloc(e, &e->d_xq_build, e->slots_cap))) ||
         (s = dalloc(e, &e->d_frc, 3 * (size_t)e->slots_cap)) || (s = dalloc(e, &e->d_uni_lo, e->n_uni)) ||
         (s = dalloc(e, &e->d_uni_hi, e->n_uni)) || (s = upload(e, &e->d_excl_start, excl_start)) ||
         (s = upload(e, &e->d_excl_list, excl_list)) || (s = upload(e, &e->d_excess, excess)) ||
@@ -2142,6 +2212,7 @@ og_status og_step(og_engine *e, int32_t n_steps) {
     og_status s;
     e->launches = 0;
     e->faults.clear();
+    const long long builds0 = e->builds_seen;
     if (e->timing) {
         e->pair_ms = 0.0;
     }
@@ -2173,6 +2244,7 @@ og_status og_step(og_engine *e, int32_t n_steps) {
                            e->stream));
         if ((s = clear_flags(e))) return s;
         e->pev_used = 0;
+        e->host_cond_builds = 0;
         if (e->timing) CK(cudaEventRecord(e->ev_step0, e->stream));
         for (int i = 0; i < n_steps;) {
             // whole list intervals replay the captured graph (not while per-kernel timing is on)
@@ -2206,6 +2278,9 @@ og_status og_step(og_engine *e, int32_t n_steps) {
         }
         int c[OG_CNT_SIZE];
         if ((s = read_counters(e, c))) return s;
+        // list builds that ran as conditional nodes of graph replays (the displacement policy)
+        if (e->list_policy == OG_LIST_DISPLACEMENT)
+            e->launches += std::max(0LL, c[OG_CNT_LIST_BUILDS] - builds0 - e->host_cond_builds) * e->cond_build_kernels;
         const int f = c[OG_CNT_FLAGS];
         const bool fault = (f & (OG_FLAG_BAD_COORD | OG_FLAG_COLUMN_CAPACITY | OG_FLAG_DISPLACEMENT)) != 0;
         if (!fault && !(f & OG_FLAG_PAIR_CAPACITY)) return check_flags(e);
@@ -2252,7 +2327,7 @@ og_status og_step(og_engine *e, int32_t n_steps) {
         e->host_step = step0;
         logs_update_limit(e);
         // the list must be rebuilt from the restored coordinates before the first step
-        if (step0 % e->intvl != 0) {
+        if (e->list_policy == OG_LIST_DISPLACEMENT || step0 % e->intvl != 0) {
             if ((s = build_list_checked(e))) return s;
         }
         if (fault) {
@@ -2289,6 +2364,8 @@ og_status og_set_state(og_engine *e, int32_t sys, const double *crd, const doubl
     if (vel_next)
         CK(cudaMemcpyAsync(e->d_vel_next + 3 * (size_t)D.atom_base, vel_next, sizeof(double) * 3 * D.n_atoms,
                            cudaMemcpyHostToDevice, e->stream));
+    if (crd && e->list_policy == OG_LIST_DISPLACEMENT)
+        CK(cudaMemsetAsync(e->d_counters + OG_CNT_LIST_STALE, 1, sizeof(int), e->stream));
     CK(cudaStreamSynchronize(e->stream));
     // new coordinates invalidate the grid: rebuild at the next step
     if (crd) e->host_step = ((e->host_step + e->intvl - 1) / e->intvl) * e->intvl;
@@ -2595,7 +2672,7 @@ extern "C" og_status og_put_state(og_engine *e, int32_t sys, const double *crd, 
                                                                 e->d_vel_next, e->d_atom_slot, e->d_slot_crd,
                                                                 e->d_cell_origin, e->d_xq, e->d_xq_ref,
                                                                 e->jl_skin * e->jl_skin, e->d_jl_stale,
-                                                                e->d_counters);
+                                                                e->d_xq_build, e->d_counters);
     LAUNCH_CHECK();
     return OG_OK;
 }
@@ -2613,6 +2690,24 @@ extern "C" og_status og_get_state_async(og_engine *e, int32_t sys, double *crd, 
     if (energies)
         CK(cudaMemcpyAsync(energies, e->d_energies + OG_N_ENERGY * (size_t)sys, sizeof(double) * OG_N_ENERGY,
                            cudaMemcpyDeviceToHost, e->stream));
+    return OG_OK;
+}
+
+extern "C" og_status og_set_list_policy(og_engine *e, int32_t policy) {
+    if (!e) return OG_ERR_INVALID;
+    if (e->finalized) return fail(e, OG_ERR_STATE, "og_set_list_policy after og_finalize");
+    if (policy != OG_LIST_FIXED && policy != OG_LIST_DISPLACEMENT)
+        return fail(e, OG_ERR_INVALID, "list policy must be OG_LIST_FIXED or OG_LIST_DISPLACEMENT");
+    e->list_policy = policy;
+    return OG_OK;
+}
+
+extern "C" og_status og_get_list_builds(og_engine *e, int64_t *n_builds) {
+    if (!e || !e->finalized || !n_builds) return OG_ERR_INVALID;
+    int c[OG_CNT_SIZE];
+    og_status s = read_counters(e, c);
+    if (s) return s;
+    *n_builds = c[OG_CNT_LIST_BUILDS];
     return OG_OK;
 }
 

@@ -94,6 +94,7 @@ __global__ void k_scan_columns(const int *__restrict__ col_count, int n_cols,
         col_atom_start[n_cols] = carry_a;
         col_cell_start[n_cols] = carry_c;
         counters[OG_CNT_N_CELLS] = carry_c;
+        counters[OG_CNT_LIST_BUILDS]++;
     }
     __syncthreads();
     for (int s = threadIdx.x; s <= n_sys; s += blockDim.x)

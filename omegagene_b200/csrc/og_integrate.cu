@@ -914,6 +914,18 @@ __device__ __forceinline__ void og_jl_check(const float4 &p, int sl, int s, cons
     }
 }
 
+// Displacement list policy: the cell-pair list holds every pair within the list cutoff at its
+// build, so it holds every pair within the interaction cutoff while no atom has moved farther
+// than half the margin since (xq_build: the slot offsets at the build, null under the fixed
+// schedule); past that the list is marked stale and rebuilt before the next force evaluation.
+__device__ __forceinline__ void og_list_check(const float4 &p, int sl, const SysDev &S,
+                                              const float4 *__restrict__ xq_build, int *__restrict__ counters) {
+    if (!xq_build) return;
+    const float4 o = xq_build[sl];
+    const float dx = p.x - o.x, dy = p.y - o.y, dz = p.z - o.z;
+    if (!(dx * dx + dy * dy + dz * dz <= S.list_trig2)) counters[OG_CNT_LIST_STALE] = 1;
+}
+
 // End of step, per atom: velocities from the constrained displacement (SubBox.cpp:1462-1481,
 // only when the plain constraint path ran), MiniCell::move_atom (MiniCell.cpp:1312-1325) and the
 // refreshed cell-relative float coordinate, PBC wrap (SubBox.cpp:1482-1502) and the kinetic
@@ -925,7 +937,7 @@ __global__ void k_finish(int n_atoms, const int *__restrict__ atom_sys, const Sy
                          const double *__restrict__ cell_origin, float4 *__restrict__ xq,
                          const float *__restrict__ mass, double *__restrict__ ke, int *__restrict__ counters,
                          int *__restrict__ sys_fault, const float4 *__restrict__ xq_ref, float jl_skin2,
-                         int *__restrict__ jl_stale) {
+                         int *__restrict__ jl_stale, const float4 *__restrict__ xq_build) {
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= n_atoms) return;
     const SysDev &S = sys[atom_sys[a]];
@@ -953,6 +965,7 @@ __global__ void k_finish(int n_atoms, const int *__restrict__ atom_sys, const Sy
     p.z = r[2];
     xq[sl] = p;
     og_jl_check(p, sl, atom_sys[a], xq_ref, jl_skin2, jl_stale, counters);
+    og_list_check(p, sl, S, xq_build, counters);
     ke[a] = vn * (double)mass[a];
     if (!(disp2 <= S.max_step_disp2)) {  // also catches NaN
         og_set_flag(counters, OG_FLAG_DISPLACEMENT);
@@ -1019,7 +1032,8 @@ __global__ void k_put_state(int n_atoms, int atom0, const int *__restrict__ atom
                             double *__restrict__ vel_next, const int *__restrict__ atom_slot,
                             double *__restrict__ slot_crd, const double *__restrict__ cell_origin,
                             float4 *__restrict__ xq, const float4 *__restrict__ xq_ref, float jl_skin2,
-                            int *__restrict__ jl_stale, int *__restrict__ counters) {
+                            int *__restrict__ jl_stale, const float4 *__restrict__ xq_build,
+                            int *__restrict__ counters) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_atoms) return;
     const int a = atom0 + i;
@@ -1045,7 +1059,14 @@ __global__ void k_put_state(int n_atoms, int atom0, const int *__restrict__ atom
         p.z = r[2];
         xq[sl] = p;
         og_jl_check(p, sl, atom_sys[a], xq_ref, jl_skin2, jl_stale, counters);
+        og_list_check(p, sl, S, xq_build, counters);
     }
+}
+
+// Displacement list policy inside a captured graph: the IF node around the list build runs its
+// body when the list is stale.
+__global__ void k_list_cond(const int *__restrict__ counters, cudaGraphConditionalHandle cond) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) cudaGraphSetConditional(cond, counters[OG_CNT_LIST_STALE] ? 1u : 0u);
 }
 
 // Advances the thermostat loop index and clears the "still iterating" count for the next

@@ -42,6 +42,8 @@
 #define OG_CNT_ACTIVE 3
 #define OG_CNT_JL_STALE 4   // nonzero: the j lists must be rebuilt before the next pair launch
 #define OG_CNT_JL_BUILDS 5  // j-list builds so far
+#define OG_CNT_LIST_STALE 6 // displacement list policy: some atom moved half the list margin since the build
+#define OG_CNT_LIST_BUILDS 7 // cell-pair list builds so far
 #define OG_CNT_SIZE 8
 
 // Per-system constants (read-only during a step).
@@ -63,6 +65,7 @@ struct SysDev {
     float zcore, bcoeff, fcoeff; // zero-dipole alpha=0 (ZeroMultipoleSum.cpp:150-202), float
     double cutoff;
     double max_step_disp2;       // squared displacement per step beyond which a system is faulted
+    float list_trig2;            // displacement list policy: squared half margin, (nsgrid_cutoff - cutoff)^2 / 4
     int lj_base, n_types;
     // integrator
     double dt;

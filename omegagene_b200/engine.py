@@ -105,7 +105,8 @@ def load_library():
         "og_step_async": [E, C.c_int32], "og_synchronize": [E],
         "og_get_pair_count": [E, C.c_int32, _p(C.c_int64)],
         "og_get_tuning": [E, _p(C.c_int32), C.c_void_p], "og_set_tuning": [E, C.c_int32],
-        "og_get_jlist_builds": [E, _p(C.c_int64)],
+        "og_get_jlist_builds": [E, _p(C.c_int64)], "og_set_list_policy": [E, C.c_int32],
+        "og_get_list_builds": [E, _p(C.c_int64)],
         "og_set_graphs": [E, C.c_int32], "og_release_pool_memory": [C.c_int32],
         "og_get_system_faults": [E, C.c_void_p],
         "og_get_graph_info": [E, _p(C.c_int32), _p(C.c_int64), _p(C.c_int64), C.c_char_p],
@@ -523,6 +524,18 @@ class Engine:
         k, p, s = C.c_int64(), C.c_double(), C.c_double()
         self._check(self.L.og_get_stats(self.h, C.byref(k), C.byref(p), C.byref(s)), "og_get_stats")
         return {"kernel_launches": k.value, "pair_kernel_ms": p.value, "step_ms": s.value}
+
+    def set_list_policy(self, policy):
+        """Cell-pair list schedule before finalize(): "fixed" (the reference's, every
+        nsgrid_update_intvl steps) or "displacement" (rebuilt whenever an atom has moved half the
+        list margin since the last build; exact lists)."""
+        code = {"fixed": 0, "displacement": 1}[policy]
+        self._check(self.L.og_set_list_policy(self.h, code), "og_set_list_policy")
+
+    def list_builds(self):
+        n = C.c_int64()
+        self._check(self.L.og_get_list_builds(self.h, C.byref(n)), "og_get_list_builds")
+        return n.value
 
     def jlist_builds(self):
         """Pair variant 10: j-list builds since finalize (list builds plus skin rebuilds)."""
