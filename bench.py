@@ -51,13 +51,17 @@ PAIR_KERNELS = {9: "k_pair_ljzd_jq<0,0,5,128,0>",
                 10: "k_pair_ljzd_jl<0,0,5,128,0> (+ k_jl_build at list builds)"}
 BOX = 215.5
 LATTICE = 70
+# pair-list cutoff by list policy: the reference's 13 A with its fixed schedule; 14 A when the
+# list is rebuilt on displacement (a 1 A trigger halves the rebuilds of the 0.5 A one at 13 A:
+# 2.26 against 2.43 ms per step at 1M atoms, the 22% more cell pairs included)
+LIST_CUTOFF = {"fixed": 13.0, "displacement": 14.0}
 PAIR_TIMING_STEPS = 10  # kernel-by-kernel steps whose pair launches are timed for the roofline
-PAIRED_STEPS, PAIRED_GAP = 200, 300  # paired FP32-vs-FP64 drift: segment length, steps between starts
+PAIRED_STEPS, PAIRED_GAP = 150, 150  # paired FP32-vs-FP64 drift: segment length, steps between starts
 CHAIN_STEPS = 1000  # timed thermostatted steps of the solvated chain
 CHAIN_RELAX = 2000  # its relaxation at 0.5 fs
 FLOP_PER_PAIR = 40  # FP32 FLOP per interacting pair (sub 3, r2 5, rsqrt 1, powers 4, LJ 5, ZD 6, force 3, accum 6, energy 7)
 WORKLOAD = ("333334 TIP3P waters (1000002 atoms), 215.5 A cubic box, NVE dt 2 fs, SHAKE-trio rigid water, "
-            "cutoff 12 A, pair-list cutoff 13 A rebuilt whenever an atom has moved 0.5 A, zero-dipole alpha 0; "
+            "cutoff 12 A, pair-list cutoff 14 A rebuilt whenever an atom has moved 1 A, zero-dipole alpha 0; "
             "seeded lattice start relaxed for 2000 untimed steps at 0.5 fs with 300 K velocity rescaling")
 
 
@@ -300,7 +304,7 @@ def nve_drift(eng, system, n_steps, dt_fs=DT_FS, chunk=100):
     return drift, len(tot), note
 
 
-def paired_drift(system, params, device, segments, seg_steps, gap_steps):
+def paired_drift(system, params, device, segments, seg_steps, gap_steps, variant=-1):
     """NVE drift of the engine against the FP64 evaluation along the same trajectory: from shared
     starting states, the production engine and the FP64 pair variant each run seg_steps steps,
     short enough that the two trajectories stay close (the FP32 force error seeds a separation
@@ -317,8 +321,8 @@ def paired_drift(system, params, device, segments, seg_steps, gap_steps):
     note = ""
     for k in range(segments):
         runs = []
-        for variant in (-1, engine.PAIR_VARIANT_F64):
-            eng = _engine(s, params, variant=variant, device=device)
+        for v in (variant, engine.PAIR_VARIANT_F64):
+            eng = _engine(s, params, variant=v, device=device)
             eng.set_trace(seg_steps)
             try:
                 eng.step(seg_steps)
@@ -329,7 +333,7 @@ def paired_drift(system, params, device, segments, seg_steps, gap_steps):
                 eng.close()
                 break
             runs.append(eng.get_trace(seg_steps)[:, 0, names.index("total")])
-            if variant == -1:
+            if v != engine.PAIR_VARIANT_F64:
                 crd, vel = eng.get_state(0)
             eng.close()
         if len(runs) < 2:
@@ -338,7 +342,7 @@ def paired_drift(system, params, device, segments, seg_steps, gap_steps):
         d32.append(float(np.polyfit(t_ns, runs[0] / dof, 1)[0]))
         d64.append(float(np.polyfit(t_ns, runs[1] / dof, 1)[0]))
         if k + 1 < segments:
-            eng = _engine(dict(s, crd=crd, vel=vel), params, device=device)
+            eng = _engine(dict(s, crd=crd, vel=vel), params, variant=variant, device=device)
             try:
                 eng.step(gap_steps)
             except engine.OgError as ex:
@@ -372,7 +376,8 @@ def run_ours(args, world, rank, local, pg, pool):
         per = max(1, (len(seeds) + 7) // 8)
         bg["walkers"] = [pool.submit(w_walkers, seeds[i:i + per]) for i in range(0, len(seeds), per)]
     s = systems.water_system(N_WATERS, box=BOX, seed=20 + rank, lattice_m=LATTICE)
-    p = _params(nsgrid_update_intvl=INTVL, time_step=DT_FS, thermostat="none", com_cancel_groups=["all"])
+    p = _params(nsgrid_update_intvl=INTVL, time_step=DT_FS, thermostat="none", com_cancel_groups=["all"],
+                nsgrid_cutoff=LIST_CUTOFF[args.list_policy])
     # the lattice start melts and heats: relax it (untimed) with velocity rescaling to 300 K at
     # 0.5 fs, so that the NVE run starts from liquid water
     if args.equil_steps > 0:
@@ -446,7 +451,7 @@ def run_ours(args, world, rank, local, pg, pool):
         "e2e": e2e, "gpu_launches": launches, "clocks": clk, "device_flags": flags,
         "lists": {"cell_pair_list_builds": list_builds, "jlist_builds": jl_builds, "steps": args.steps,
                   "note": "builds in the timed steps (displacement policy: whenever an atom had moved half the "
-                          "1 A margin since the last build; j lists also when one passed the 0.35 A skin)"},
+                          "list margin since the last build; j lists also when one passed the 0.35 A skin)"},
     }
     pk = peaks()
     sm_max = (pk or {}).get("sm_max_mhz", 1965.0)
@@ -481,7 +486,7 @@ def run_ours(args, world, rank, local, pg, pool):
         crd, vel = eng.get_state(0)
         eng.close()
         acc.update(paired_drift(dict(s, crd=crd, vel=vel), p, local, args.paired_segments, PAIRED_STEPS,
-                                PAIRED_GAP))
+                                PAIRED_GAP, variant=tuning["pair_variant"]))
         # forces and state of the last configuration, FP64-checked by a background process
         e = _engine(dict(s, crd=crd, vel=vel), p, device=local)
         e.compute_forces()
@@ -899,7 +904,7 @@ def main():
                     help="water1m: cell-pair list rebuilds when an atom has moved half the margin (exact), or every "
                          "%d steps (the reference's schedule)" % INTVL)
     ap.add_argument("--drift-steps", type=int, default=2000)
-    ap.add_argument("--paired-segments", type=int, default=6)
+    ap.add_argument("--paired-segments", type=int, default=16)
     ap.add_argument("--batch-jobs", type=int, default=64)
     ap.add_argument("--batch-job-steps", type=int, default=1000)
     ap.add_argument("--mcmd-steps", type=int, default=1000)
@@ -941,7 +946,8 @@ def main():
         }))
         return
     if args.list_policy == "fixed":
-        WORKLOAD = WORKLOAD.replace("rebuilt whenever an atom has moved 0.5 A", "rebuilt every %d steps" % INTVL)
+        WORKLOAD = WORKLOAD.replace("pair-list cutoff 14 A rebuilt whenever an atom has moved 1 A",
+                                    "pair-list cutoff 13 A rebuilt every %d steps" % INTVL)
     pool = None
     if world == 1 and not args.no_extras:
         # CPU work beside the GPU's: spawned before the first GPU call

@@ -212,6 +212,18 @@ og_status og_step(og_engine *e, int32_t n_steps);
  * forces and energies without advancing time (SubBox::nsgrid_update + SubBox::calc_energy). */
 og_status og_compute_forces(og_engine *e);
 
+/* Forces and energies at the current coordinates over the current cell-pair list, without
+ * rebuilding it and without advancing time: the per-step force call of a caller that runs its own
+ * integrator, as the reference's GPU path does (SubBox::calc_energy_pairwise_cuda ->
+ * cuda_pairwise_ljzd, SubBox.cpp:906-955, cuda_setup.cu:777-801, with the list rebuilt only on
+ * its nsgrid_update steps).  Coordinates come in through og_put_state; j lists that the move
+ * made stale are rebuilt first.  Read the results with og_get_forces. */
+og_status og_compute_forces_current(og_engine *e);
+/* Before og_finalize: evaluate the pair Lennard-Jones + zero-dipole terms alone, without the
+ * excluded-pair ZD term (and a caller gives no bonded terms): the share of the force field that
+ * the reference computes on the GPU, its host computing the rest (SubBox::calc_energy,
+ * SubBox.cpp:906-955).  OG_E_ELE is then the pair sum plus the self energy. */
+og_status og_set_pair_only(og_engine *e, int32_t on);
 /* Replaces a system's coordinates / velocities and marks the cell list for a rebuild at the
  * next step (synchronous). */
 og_status og_set_state(og_engine *e, int32_t sys, const double *crd, const double *vel_next);
@@ -278,7 +290,7 @@ og_status og_get_flags(og_engine *e, int32_t *flags);
 #define OG_PAIR_VARIANT_F64 11
 /* Autotuner result: the pair-kernel variant in use and the best time of each variant on the
  * first list, in ms (variant_ms[OG_N_PAIR_VARIANTS]); for variant 10 the time is one step's
- * launch plus its share of the j-list build (build time / nsgrid_update_intvl). */
+ * launch plus half a j-list build (the rate measured on water at 2 fs: one build per ~2.4 steps). */
 og_status og_get_tuning(og_engine *e, int32_t *pair_variant, double *variant_ms);
 /* Pair variant 10: j-list builds since og_finalize -- one at each cell-pair list build, plus one
  * whenever an atom has moved farther than the skin (0.35 A, or OG_JL_SKIN in the environment)
@@ -353,6 +365,11 @@ og_status og_segment_sum(const double *d_values, int32_t stride, const int32_t *
  * calls that overlap on the GPU race. */
 og_status og_segment_sum_noalloc(const double *d_values, int32_t stride, const int32_t *d_seg_base, int32_t n_seg,
                                  int32_t max_seg_len, double *d_out, void *cuda_stream);
+/* Device memory the engine holds (bytes_held) and the most it has held at once (bytes_peak),
+ * counting every buffer it allocated (the pair-list region grows when a list outgrows it).  A
+ * serving loop sizes admission from these.  Either pointer may be NULL.  No counterpart in the
+ * reference. */
+og_status og_get_footprint(og_engine *e, int64_t *bytes_held, int64_t *bytes_peak);
 /* Number of systems and atoms held. */
 og_status og_get_sizes(og_engine *e, int32_t *n_systems, int64_t *n_atoms_total);
 

@@ -210,6 +210,29 @@ def read_cls(path):
 
 # ------------------------------------------------------------------ writer
 
+def _pack_records(t, key, dtype):
+    """A dihedral section: the parsed records when present, else the raw bytes (count 0 if none)."""
+    if key in t and t[key] is not None:
+        arr = np.asarray(t[key], dtype)
+        return struct.pack("<i", len(arr)) + arr.tobytes()
+    return t.get(key + "_raw", struct.pack("<i", 0))
+
+
+def _pack_nb14(t):
+    """The 1-4 section from the parsed pairs (the reader swapped the record's two factors into
+    coeff_vdw = second, coeff_ele = first; they are written back in record order), else raw."""
+    nb = t.get("nb14")
+    if nb is None:
+        return t.get("nb14_raw", struct.pack("<i", 0))
+    atoms = np.asarray(nb["atoms"], np.int64).reshape(-1, 2)
+    rec = np.zeros(len(atoms), NB14)
+    rec["a1"], rec["a2"] = atoms[:, 0], atoms[:, 1]
+    types = np.asarray(nb["types"], np.int64).reshape(-1, 2) + 1
+    rec["t1"], rec["t2"] = types[:, 0], types[:, 1]
+    rec["f1"], rec["f2"] = nb["coeff_ele"], nb["coeff_vdw"]
+    return struct.pack("<i", len(rec)) + rec.tobytes()
+
+
 def _pack_topol(t, n_atoms):
     parts = [struct.pack("<i", n_atoms),
              np.asarray(t["charge"], "<f8").tobytes(),
@@ -224,8 +247,8 @@ def _pack_topol(t, n_atoms):
         arr = np.asarray(t.get(key, np.zeros(0, dt)), dt)
         body = struct.pack("<i", len(arr)) + arr.tobytes()
         parts += [struct.pack("<i", len(body)), body]
-    for key in ("torsions_raw", "impros_raw", "nb14_raw"):
-        body = t.get(key, struct.pack("<i", 0))
+    for key, body in (("torsions", _pack_records(t, "torsions", DIHED)), ("impros", _pack_records(t, "impros", DIHED)),
+                      ("nb14", _pack_nb14(t))):
         parts += [struct.pack("<i", len(body)), body]
     p15 = np.asarray(t["nb15off_pairs"], "<i4").reshape(-1, 2)
     body = struct.pack("<i", len(p15)) + p15.tobytes()

@@ -146,6 +146,7 @@ using namespace og;
 // The pair variant over j lists, and the default displacement (A) after which its lists are
 // rebuilt (OG_JL_SKIN in the environment overrides it, 0.05-2 A).
 #define OG_JL_VARIANT 10
+#define OG_JL_BUILDS_PER_STEP 0.5  // j-list builds per step charged to variant 10 by the autotuner
 #define OG_JL_SKIN 0.35f
 
 namespace {
@@ -242,6 +243,7 @@ struct og_engine {
     // cell-pair list schedule: OG_LIST_FIXED (the reference's, every nsgrid_update_intvl steps) or
     // OG_LIST_DISPLACEMENT (whenever an atom has moved half the list margin since the last build)
     int list_policy = OG_LIST_FIXED;
+    bool pair_only = false;  // og_set_pair_only: the pair LJ + ZD terms alone (no excluded-pair term)
     float4 *d_xq_build = nullptr;  // slot offsets at the last list build (displacement policy only)
     // launch accounting of the conditional list build inside graph replays: the kernels of one
     // build (not counted per replay), builds launched kernel by kernel in the current og_step, and
@@ -325,6 +327,8 @@ struct og_engine {
     double variant_ms[OG_N_PAIR_VARIANTS] = {};
     int timing = 0;  // 1: step + per-pair-kernel events (kernel by kernel); 2: step events only
     std::vector<void *> allocs;
+    std::vector<size_t> alloc_bytes;          // size of each entry of allocs
+    size_t bytes_held = 0, bytes_peak = 0;    // device bytes held by the engine now / at most
     // V-McMD: state table, per-system current state, per-slot generators and log rings
     VsDev *d_vstates = nullptr;
     int *d_vs_cur = nullptr, *d_vs_log = nullptr, *d_vm_snap_cur = nullptr;
@@ -416,6 +420,9 @@ og_status dalloc(og_engine *e, T **p, size_t n) {
     if (r != cudaSuccess)
         return fail(e, OG_ERR_NOMEM, "device allocation (%zu bytes): %s", n * sizeof(T), cudaGetErrorString(r));
     e->allocs.push_back(q);
+    e->alloc_bytes.push_back(n * sizeof(T));
+    e->bytes_held += n * sizeof(T);
+    e->bytes_peak = std::max(e->bytes_peak, e->bytes_held);
     *p = (T *)q;
     return OG_OK;
 }
@@ -424,7 +431,9 @@ void dfree(og_engine *e, void *p) {
     if (!p) return;
     for (size_t i = 0; i < e->allocs.size(); i++)
         if (e->allocs[i] == p) {
+            e->bytes_held -= e->alloc_bytes[i];
             e->allocs.erase(e->allocs.begin() + i);
+            e->alloc_bytes.erase(e->alloc_bytes.begin() + i);
             break;
         }
     cudaFreeAsync(p, e->stream);
@@ -1119,13 +1128,16 @@ og_status thermostat_with_shake(og_engine *e) {
     return OG_OK;
 }
 
-// Displacement list policy, kernel by kernel: the host reads the stale mark (one 4-byte copy and
-// a stream synchronisation per step) and builds the list when it is set.
+// Displacement list policy, kernel by kernel: the host reads the counters (one copy and a stream
+// synchronisation per step) and builds the list when it is stale and no system has faulted in
+// this call (as k_list_cond decides inside a graph).
 og_status build_list_if_stale(og_engine *e) {
-    CK(cudaMemcpyAsync(e->h_pinned + 8, e->d_counters + OG_CNT_LIST_STALE, sizeof(int), cudaMemcpyDeviceToHost,
+    CK(cudaMemcpyAsync(e->h_pinned + 8, e->d_counters, sizeof(int) * OG_CNT_SIZE, cudaMemcpyDeviceToHost,
                        e->stream));
     CK(cudaStreamSynchronize(e->stream));
-    if (!e->h_pinned[8]) return OG_OK;
+    const int *c = e->h_pinned + 8;
+    const bool fault = (c[OG_CNT_FLAGS] & (OG_FLAG_BAD_COORD | OG_FLAG_COLUMN_CAPACITY | OG_FLAG_DISPLACEMENT)) != 0;
+    if (!c[OG_CNT_LIST_STALE] || fault) return OG_OK;
     e->host_cond_builds++;
     return build_list(e);
 }
@@ -1540,7 +1552,11 @@ og_status autotune_pair(og_engine *e) {
             if (v == OG_JL_VARIANT && rep == 0) first = ms;  // the j lists are built once, here
             else vbest = std::min(vbest, (double)ms);
         }
-        if (v == OG_JL_VARIANT) vbest += std::max(0.0, first - vbest) / e->intvl;
+        // the j lists are rebuilt at every cell-pair list build and whenever an atom passes the
+        // skin: on water at 2 fs about once per 2.4 steps (42 builds per 100 steps at 1M atoms, 8 in
+        // 20 at the start of a run), so the build is charged at one per two steps, not one per
+        // list interval
+        if (v == OG_JL_VARIANT) vbest += std::max(0.0, first - vbest) * OG_JL_BUILDS_PER_STEP;
         e->variant_ms[v] = vbest;
         if (vbest < best) {
             best = vbest;
@@ -1957,7 +1973,7 @@ og_status og_finalize(og_engine *e) {
             for (int p = h.xs[i]; p < h.xs[i + 1]; p++) excl_list.push_back(atom_base + h.xl[p]);
             excl_start.push_back((int)excl_list.size());
         }
-        for (int q = 0; q < h.n_excess; q++) {
+        for (int q = 0; q < (e->pair_only ? 0 : h.n_excess); q++) {
             excess.push_back(make_int2(atom_base + h.excess[2 * q], atom_base + h.excess[2 * q + 1]));
             excess_sys.push_back(k);
         }
@@ -2326,9 +2342,16 @@ og_status og_step(og_engine *e, int32_t n_steps) {
         CK(cudaStreamSynchronize(e->stream));
         e->host_step = step0;
         logs_update_limit(e);
-        // the list must be rebuilt from the restored coordinates before the first step
-        if (e->list_policy == OG_LIST_DISPLACEMENT || step0 % e->intvl != 0) {
-            if ((s = build_list_checked(e))) return s;
+        // the list must be rebuilt from the restored coordinates before the first step: under
+        // the displacement policy it is marked stale (the next step builds it); under the fixed
+        // schedule it is built now unless the step is a rebuild step anyway.  A faulted system's
+        // restored coordinates may not bin (the caller placed them, or they are those the fault
+        // ran from): a failed build then leaves valid indices, and the call reports the fault.
+        if (e->list_policy == OG_LIST_DISPLACEMENT) {
+            CK(cudaMemsetAsync(e->d_counters + OG_CNT_LIST_STALE, 1, sizeof(int), e->stream));
+        } else if (step0 % e->intvl != 0) {
+            s = build_list_checked(e);
+            if (s && !fault) return s;
         }
         if (fault) {
             std::string who;
@@ -2352,6 +2375,24 @@ og_status og_compute_forces(og_engine *e) {
     if ((s = compute_forces(e, true))) return s;
     CK(cudaStreamSynchronize(e->stream));
     return check_flags(e);
+}
+
+og_status og_compute_forces_current(og_engine *e) {
+    if (!e) return OG_ERR_INVALID;
+    if (!e->finalized) return fail(e, OG_ERR_STATE, "og_compute_forces_current before og_finalize");
+    CK(cudaSetDevice(e->device));
+    og_status s = clear_flags(e);
+    if (s) return s;
+    if ((s = compute_forces(e, true))) return s;
+    CK(cudaStreamSynchronize(e->stream));
+    return check_flags(e);
+}
+
+og_status og_set_pair_only(og_engine *e, int32_t on) {
+    if (!e) return OG_ERR_INVALID;
+    if (e->finalized) return fail(e, OG_ERR_STATE, "og_set_pair_only after og_finalize");
+    e->pair_only = on != 0;
+    return OG_OK;
 }
 
 og_status og_set_state(og_engine *e, int32_t sys, const double *crd, const double *vel_next) {
@@ -2690,6 +2731,13 @@ extern "C" og_status og_get_state_async(og_engine *e, int32_t sys, double *crd, 
     if (energies)
         CK(cudaMemcpyAsync(energies, e->d_energies + OG_N_ENERGY * (size_t)sys, sizeof(double) * OG_N_ENERGY,
                            cudaMemcpyDeviceToHost, e->stream));
+    return OG_OK;
+}
+
+extern "C" og_status og_get_footprint(og_engine *e, int64_t *bytes_held, int64_t *bytes_peak) {
+    if (!e) return OG_ERR_INVALID;
+    if (bytes_held) *bytes_held = (int64_t)e->bytes_held;
+    if (bytes_peak) *bytes_peak = (int64_t)e->bytes_peak;
     return OG_OK;
 }
 

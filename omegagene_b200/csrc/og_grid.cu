@@ -125,29 +125,35 @@ __global__ void k_sort_columns(const int *__restrict__ col_count, const int *__r
     const int col = blockIdx.x;
     const int n = col_count[col];
     if (n == 0) return;
-    if (n > OG_MAX_COLUMN_ATOMS) {
+    const unsigned long long *src = col_keys + col_atom_start[col];
+    // A column beyond the sort capacity (a blown-up system piles its atoms into one column) is
+    // flagged, which faults the call and undoes it, and still laid out, unsorted, from the
+    // keys in global memory: every slot, cell and atom index of the build stays valid for the
+    // kernels that run until the call ends.
+    const bool over = n > OG_MAX_COLUMN_ATOMS;
+    const unsigned long long *K = over ? src : keys;
+    if (over) {
         if (threadIdx.x == 0) {
             og_set_flag(counters, OG_FLAG_COLUMN_CAPACITY);
             atomicOr(&sys_fault[col_sys[col]], OG_FLAG_COLUMN_CAPACITY);
         }
-        return;
-    }
-    int np2 = 1;
-    while (np2 < n) np2 <<= 1;
-    const unsigned long long *src = col_keys + col_atom_start[col];
-    for (int i = threadIdx.x; i < np2; i += blockDim.x) keys[i] = i < n ? src[i] : ~0ull;
-    __syncthreads();
-    for (int k = 2; k <= np2; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < np2; i += blockDim.x) {
-                int ixj = i ^ j;
-                if (ixj > i) {
-                    unsigned long long a = keys[i], b = keys[ixj];
-                    bool up = (i & k) == 0;
-                    if ((a > b) == up) { keys[i] = b; keys[ixj] = a; }
+    } else {
+        int np2 = 1;
+        while (np2 < n) np2 <<= 1;
+        for (int i = threadIdx.x; i < np2; i += blockDim.x) keys[i] = i < n ? src[i] : ~0ull;
+        __syncthreads();
+        for (int k = 2; k <= np2; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = threadIdx.x; i < np2; i += blockDim.x) {
+                    int ixj = i ^ j;
+                    if (ixj > i) {
+                        unsigned long long a = keys[i], b = keys[ixj];
+                        bool up = (i & k) == 0;
+                        if ((a > b) == up) { keys[i] = b; keys[ixj] = a; }
+                    }
                 }
+                __syncthreads();
             }
-            __syncthreads();
         }
     }
     const int s = col_sys[col];
@@ -156,7 +162,7 @@ __global__ void k_sort_columns(const int *__restrict__ col_count, const int *__r
     const int ncz = (n + OG_CELL - 1) / OG_CELL;
     for (int k = threadIdx.x; k < ncz * OG_CELL; k += blockDim.x) {
         int use = k < n ? k : n - 1;
-        int atom = atom_base + (int)(keys[use] & 0xffffffffull);
+        int atom = atom_base + (int)(K[use] & 0xffffffffull);
         int slot = head * OG_CELL + k;
         slot_atom[slot] = k < n ? atom : -1;
         for (int d = 0; d < 3; d++) slot_crd[3 * slot + d] = (double)__double2float_rn(crd[3 * atom + d]);
@@ -196,6 +202,10 @@ __global__ void k_cell_info(const int *__restrict__ counters, int cells_cap, con
     cell_valid[c] = (unsigned char)v;
     int umin = __float2int_rz(__fdiv_rn(__fsub_rn(zmin, S.lowerf[2]), S.L_z_uni));
     int umax = __float2int_rz(__fdiv_rn(__fsub_rn(zmax, S.lowerf[2]), S.L_z_uni));
+    // in-box cells give bins 0..n_uni_z; a runaway coordinate (a blown-up system, whose call is
+    // undone) is held a few bins outside so that no later index arithmetic overflows
+    umin = max(-4, min(umin, S.n_uni_z + 4));
+    umax = max(-4, min(umax, S.n_uni_z + 4));
     cell_uni[c] = make_int2(umin, umax);
     const int n_uni = S.n_columns * S.n_uni_z;
     int steps = 0;

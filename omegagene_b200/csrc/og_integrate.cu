@@ -1064,9 +1064,14 @@ __global__ void k_put_state(int n_atoms, int atom0, const int *__restrict__ atom
 }
 
 // Displacement list policy inside a captured graph: the IF node around the list build runs its
-// body when the list is stale.
+// body when the list is stale, unless a system has faulted in this call (the call is undone;
+// no list is built from its non-finite or runaway coordinates).
 __global__ void k_list_cond(const int *__restrict__ counters, cudaGraphConditionalHandle cond) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) cudaGraphSetConditional(cond, counters[OG_CNT_LIST_STALE] ? 1u : 0u);
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        const bool fault = (counters[OG_CNT_FLAGS] & (OG_FLAG_BAD_COORD | OG_FLAG_COLUMN_CAPACITY |
+                                                      OG_FLAG_DISPLACEMENT)) != 0;
+        cudaGraphSetConditional(cond, (counters[OG_CNT_LIST_STALE] && !fault) ? 1u : 0u);
+    }
 }
 
 // Advances the thermostat loop index and clears the "still iterating" count for the next

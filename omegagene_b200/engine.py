@@ -106,7 +106,7 @@ def load_library():
         "og_get_pair_count": [E, C.c_int32, _p(C.c_int64)],
         "og_get_tuning": [E, _p(C.c_int32), C.c_void_p], "og_set_tuning": [E, C.c_int32],
         "og_get_jlist_builds": [E, _p(C.c_int64)], "og_set_list_policy": [E, C.c_int32],
-        "og_get_list_builds": [E, _p(C.c_int64)],
+        "og_get_list_builds": [E, _p(C.c_int64)], "og_get_footprint": [E, _p(C.c_int64), _p(C.c_int64)],
         "og_set_graphs": [E, C.c_int32], "og_release_pool_memory": [C.c_int32],
         "og_get_system_faults": [E, C.c_void_p],
         "og_get_graph_info": [E, _p(C.c_int32), _p(C.c_int64), _p(C.c_int64), C.c_char_p],
@@ -531,6 +531,12 @@ class Engine:
         list margin since the last build; exact lists)."""
         code = {"fixed": 0, "displacement": 1}[policy]
         self._check(self.L.og_set_list_policy(self.h, code), "og_set_list_policy")
+
+    def footprint(self):
+        """(device bytes held now, most held at once) by this engine."""
+        held, peak = C.c_int64(), C.c_int64()
+        self._check(self.L.og_get_footprint(self.h, C.byref(held), C.byref(peak)), "og_get_footprint")
+        return held.value, peak.value
 
     def list_builds(self):
         n = C.c_int64()

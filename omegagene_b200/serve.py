@@ -41,10 +41,13 @@ import numpy as np
 
 from . import engine
 
-# device footprint per atom: state, grid, cell pairs, list scratch and, for the j-list pair
-# kernel, its entries (measured on a 60-job water batch of 546k atoms: 1,728 bytes per atom with
-# the j-queue kernel, 4,054 with the j-list kernel)
+# device footprint per atom assumed until the server has measured an engine: state, grid, cell
+# pairs, list scratch and, for the j-list pair kernel, its entries (a 60-job water batch of 546k
+# atoms holds 1,728 bytes per atom with the j-queue kernel, 4,054 with the j-list kernel).  Every
+# engine the server builds then reports what it holds (og_get_footprint), and admission uses the
+# largest measured bytes per atom so far, with a 10% margin.
 BYTES_PER_ATOM = 4200
+FOOTPRINT_MARGIN = 1.1
 
 
 class Job:
@@ -94,11 +97,14 @@ class Job:
 
 class Server:
     def __init__(self, device=0, hbm_budget_bytes=None, max_jobs=64, window=100, pair_variant="auto",
-                 clock=time.perf_counter, sleep=time.sleep, engine_factory=None, prepare_ahead=True):
+                 clock=time.perf_counter, sleep=time.sleep, engine_factory=None, prepare_ahead=True,
+                 bytes_per_atom=None):
         """pair_variant: a fixed pair-kernel variant, or "auto": the first engine autotunes and
         every later engine reuses its choice, so a job keeps one kernel (and bitwise results)
         across re-formed batches.  prepare_ahead: build the next batch's engine during the
-        current window when the next batch is known (see the module docstring)."""
+        current window when the next batch is known (see the module docstring).  bytes_per_atom:
+        a fixed admission estimate; None measures every engine built (og_get_footprint) and
+        admits by the largest bytes per atom seen, starting from BYTES_PER_ATOM."""
         self.device = device
         if hbm_budget_bytes is None:
             import torch
@@ -116,6 +122,26 @@ class Server:
         self.prepare_ahead = prepare_ahead
         self.batch_sizes = []
         self.engine_factory = engine_factory or engine.Engine
+        self.measure = bytes_per_atom is None
+        self.bytes_per_atom = float(BYTES_PER_ATOM if bytes_per_atom is None else bytes_per_atom)
+        self.measured_bytes_per_atom = 0.0
+        self.batch_footprints = []  # (atoms, peak device bytes) of every engine built
+
+    def job_bytes(self, j):
+        """Device memory a job is expected to take (the admission estimate)."""
+        return j.n_atoms * self.bytes_per_atom
+
+    def _measured(self, eng, members):
+        """Records the engine's footprint and, when measuring, raises the admission estimate to
+        the largest bytes per atom seen (with the margin)."""
+        if not hasattr(eng, "footprint"):
+            return
+        _, peak = eng.footprint()
+        atoms = sum(j.n_atoms for j, *_ in members)
+        self.batch_footprints.append((atoms, peak))
+        if atoms and self.measure:
+            self.measured_bytes_per_atom = max(self.measured_bytes_per_atom, peak / atoms)
+            self.bytes_per_atom = FOOTPRINT_MARGIN * self.measured_bytes_per_atom
 
     def _build(self, active):
         eng = self._engine_for([(j, j.crd, j.vel, j.steps_done) for j in active])
@@ -134,17 +160,19 @@ class Server:
             s["crd"], s["vel"] = crd, vel
             eng.add_system(s, j.params, j.mcmd, first_step=first)
         eng.finalize()
+        self._measured(eng, members)
         return eng
 
     def _admits(self, running, queue):
         """Queued jobs the rules admit next to the running ones, first come first served."""
-        used = sum(j.bytes for j in running)
+        used = sum(self.job_bytes(j) for j in running)
         out = []
         for j in queue:
-            if len(running) + len(out) >= self.max_jobs or used + j.bytes > self.budget:
+            n = len(running) + len(out)
+            if n >= self.max_jobs or (used + self.job_bytes(j) > self.budget and n > 0):
                 break
             out.append(j)
-            used += j.bytes
+            used += self.job_bytes(j)
         return out
 
     def _prepare(self, pool, active, queue, w):
@@ -196,12 +224,14 @@ class Server:
             while future and future[0].arrival_s <= now:
                 queue.append(future.popleft())
             finished = [j for j in active if j.steps_done >= j.n_steps]
-            used = sum(j.bytes for j in active if j.steps_done < j.n_steps)
+            used = sum(self.job_bytes(j) for j in active if j.steps_done < j.n_steps)
             n_run = len(active) - len(finished)
             admit = []
-            while queue and n_run + len(admit) < self.max_jobs and used + queue[0].bytes <= self.budget:
+            while queue and n_run + len(admit) < self.max_jobs and (
+                    used + self.job_bytes(queue[0]) <= self.budget or n_run + len(admit) == 0):
+                # (a job estimated above the whole budget still runs, alone)
                 admit.append(queue.popleft())
-                used += admit[-1].bytes
+                used += self.job_bytes(admit[-1])
             if finished or admit:
                 t_re = self.clock()
                 cont = [j for j in active if j.steps_done < j.n_steps]
@@ -218,6 +248,7 @@ class Server:
                         j.energies = eng.get_energies(i)
                         if j.vmcmd:
                             j.collect_vmcmd(eng, i)
+                    self._measured(eng, [(j,) for j in active])  # the peak includes any list growth
                     eng.close()
                     eng = None
                 now = self.clock() - t0

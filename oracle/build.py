@@ -11,7 +11,10 @@
   - ``omegagene_ns``: the cell-list CPU program.  MiniCell.cpp is compiled with
     ``-DF_CUDA -DF_ECP`` so that it allocates its coordinate buffer (through the malloc
     stubs of ``ref_minicell_shim.cpp``); every other file is the plain CPU build, so the
-    pair list and forces are the reference's CPU code.
+    pair list and forces are the reference's CPU code;
+  - ``omegagene_og``: the reference's GPU program (its CELESTE_GPU build: every file with
+    ``-DF_CUDA``) linked against ``omegagene_b200/libomegagene_celeste.so`` in place of its
+    ``cuda_setup.cu``: the drop-in, the reference's own host code driving this engine.
 
 The reference's own CMake build is not used (it requires a .git directory).  Outputs
 never go anywhere but ``oracle/`` and ``oracle/_ref/``.
@@ -84,7 +87,9 @@ def build_ref(force=False, jobs=8, ref_root=None):
         if f == "MiniCell.cpp":
             jobs_list.append((os.path.join(objdir, stem + ".cudaecp.o"), src, ["-DF_CUDA", "-DF_ECP"]))
         jobs_list.append((os.path.join(objdir, stem + ".ns.o"), src, []))
+        jobs_list.append((os.path.join(objdir, stem + ".cuda.o"), src, ["-DF_CUDA"]))
     jobs_list.append((os.path.join(objdir, "Random.o"), rnd, []))
+    jobs_list.append((os.path.join(objdir, "main.cuda.o"), main, ["-DF_CUDA"]))
     jobs_list.append((os.path.join(objdir, "main.wons.o"), main, ["-DF_WO_NS"]))
     jobs_list.append((os.path.join(objdir, "main.ns.o"), main, []))
     jobs_list.append((os.path.join(objdir, "shim.o"), shim, []))
@@ -103,14 +108,24 @@ def build_ref(force=False, jobs=8, ref_root=None):
     ns_objs = [o(f[:-4] + (".cudaecp.o" if f == "MiniCell.cpp" else ".ns.o")) for f in CORE]
     ns_objs += [o("Random.o"), o("main.ns.o"), o("shim.o")]
     lib_objs = [o("MiniCell.cudaecp.o"), o("PBC.ns.o"), o("CelesteObject.ns.o"), o("shim.o")]
+    og_dir = os.path.join(os.path.dirname(HERE), "omegagene_b200")
+    og_objs = [o(f[:-4] + ".cuda.o") for f in CORE] + [o("Random.o"), o("main.cuda.o")]
     targets = [
         (os.path.join(REF_OUT, "omegagene_wons"), wons_objs, []),
         (os.path.join(REF_OUT, "omegagene_ns"), ns_objs, []),
         (os.path.join(REF_OUT, "libogref_minicell.so"), lib_objs, ["-shared"]),
     ]
+    celeste = os.path.join(og_dir, "libomegagene_celeste.so")
+    if os.path.exists(celeste):
+        # the drop-in: found at run time relative to the program ($ORIGIN/../../omegagene_b200)
+        targets.append((os.path.join(REF_OUT, "omegagene_og"), og_objs,
+                        ["-L" + og_dir, "-l:libomegagene_celeste.so", "-l:libomegagene_b200.so",
+                         "-Wl,-rpath,$ORIGIN/../../omegagene_b200"]))
     for out, objs, extra in targets:
-        if force or not _newer(out, objs):
-            _run(["g++", "-O3", "-fPIC"] + extra + ["-o", out] + objs + ["-lm"])
+        libs = [x for x in extra if x.startswith("-l") or x.startswith("-L") or x.startswith("-Wl")]
+        flags = [x for x in extra if x not in libs]
+        if force or not _newer(out, objs + ([celeste] if out.endswith("omegagene_og") else [])):
+            _run(["g++", "-O3", "-fPIC"] + flags + ["-o", out] + objs + libs + ["-lm"])
     return REF_OUT
 
 

@@ -46,10 +46,29 @@ def test_served_jobs_equal_alone_runs(variant):
 def test_memory_budget_limits_admission():
     jobs = _jobs()
     budget = max(j.bytes for j in jobs) + min(j.bytes for j in jobs)
-    srv = serve.Server(0, hbm_budget_bytes=budget, max_jobs=8, window=20)
+    srv = serve.Server(0, hbm_budget_bytes=budget, max_jobs=8, window=20, bytes_per_atom=serve.BYTES_PER_ATOM)
     res = srv.run(jobs)
     assert res["n_jobs"] == 5
     assert max(srv.batch_sizes) <= 2
+
+
+def test_admission_by_measured_footprint_stays_within_budget():
+    """The server measures every engine it builds (og_get_footprint) and admits by the largest
+    bytes per atom seen: every batch's device footprint stays within the budget, and the
+    estimate is the measurement, not the starting constant."""
+    jobs = _jobs()
+    budget = int(0.6 * sum(j.n_atoms for j in jobs) * 2000)
+    srv = serve.Server(0, hbm_budget_bytes=budget, max_jobs=8, window=20)
+    res = srv.run(jobs)
+    assert res["n_jobs"] == 5
+    assert srv.measured_bytes_per_atom > 0 and srv.bytes_per_atom != serve.BYTES_PER_ATOM
+    assert max(peak for _, peak in srv.batch_footprints[1:]) <= budget, (srv.batch_footprints, budget)
+    eng = engine.Engine(0)
+    eng.add_system(jobs[0].system, jobs[0].params)
+    eng.finalize()
+    held, peak = eng.footprint()
+    assert 0 < held <= peak
+    eng.close()
 
 
 def _engine(batch, variant=6):
@@ -116,3 +135,35 @@ def test_served_vmcmd_jobs_equal_alone_runs(variant):
         assert np.array_equal(j.crd, crd) and np.array_equal(j.vel, vel), j.id
         assert j.vs_log == logs["vs"] and j.lambda_log == logs["lambda"], j.id
         assert len(j.vs_log) == (j.n_steps - 1) // 3 and len({v for _, v in j.vs_log}) > 1  # steps 3, 6 .. < n
+
+
+@pytest.mark.parametrize("policy", ["fixed", "displacement"])
+def test_column_overflow_faults_the_system_only(policy):
+    """A caller piles one system's 5,100 atoms into one MiniCell column (beyond the 4,096 the
+    engine sorts): og_step fails with OG_ERR_SYSTEM_FAULT naming that system with bit 2, every
+    system is back at the call's start, and the list build that met the column left every index
+    valid (the column is laid out unsorted and the call undone)."""
+    p = _params(nsgrid_update_intvl=10, time_step=2.0)
+    a = systems.water_system(900, seed=61)
+    b = systems.water_system(1700, seed=62)
+    eng = engine.Engine(0)
+    eng.set_tuning(10)
+    eng.set_list_policy(policy)
+    for s in (a, b):
+        eng.add_system(s, p)
+    eng.finalize()
+    start = [eng.get_state(i) for i in range(2)]
+    crd, vel = start[1]
+    crd = crd.copy()
+    lo = b["pbc_val"][9:12] - 0.5 * b["pbc_val"][0]
+    crd[:, 0] = lo[0] + 0.5 + 0.001 * (np.arange(len(crd)) % 7)  # one column: x, y within 0.01 A
+    crd[:, 1] = lo[1] + 0.5 + 0.001 * (np.arange(len(crd)) % 5)
+    eng.set_state(1, crd, vel)
+    with pytest.raises(engine.OgError) as ex:
+        eng.step(20)
+    assert ex.value.status == engine.OG_ERR_SYSTEM_FAULT
+    f = eng.system_faults()
+    assert f[0] == 0 and f[1] & 2
+    c0, v0 = eng.get_state(0)
+    assert np.array_equal(c0, start[0][0]) and np.array_equal(v0, start[0][1])
+    eng.close()
