@@ -94,7 +94,7 @@ class ClockSampler:
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
-                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                      "--format=csv,noheader,nounits", "-lms", "50"],
                                      stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
 
     def stop(self):
@@ -105,6 +105,10 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
+        if os.path.getsize(self.path) == 0:  # a timed region shorter than the sampling period
+            with open(self.path, "w") as f:
+                subprocess.run(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                "--format=csv,noheader,nounits"], stdout=f, stderr=subprocess.DEVNULL, timeout=30)
         sm, mx, reasons = [], 0.0, set()
         for line in open(self.path):
             f = [x.strip() for x in line.split(",")]
@@ -401,18 +405,19 @@ def run_ours(args, world, rank, local, pg, pool):
     clocks.start()
     eng.step(args.steps)
     torch.cuda.synchronize()
-    clk = clocks.stop()
     st = eng.stats()
     list_builds, jl_builds = eng.list_builds() - builds0, eng.jlist_builds() - jl0
+    # the pair kernel alone (roofline): CUDA events around each pair launch, kernel by kernel
+    # (the clock samples run on through these steps)
+    eng.set_timing(True)
+    eng.step(PAIR_TIMING_STEPS)
+    pair_ms = eng.stats()["pair_kernel_ms"] / PAIR_TIMING_STEPS
+    clk = clocks.stop()
     barrier(pg)
     ms_total = max_over_ranks(pg, st["step_ms"])
     launches = st["kernel_launches"]
     value = replica_value(args.steps, ms_total, world)
     gi = eng.graph_info()
-    # the pair kernel alone (roofline): CUDA events around each pair launch, kernel by kernel
-    eng.set_timing(True)
-    eng.step(PAIR_TIMING_STEPS)
-    pair_ms = eng.stats()["pair_kernel_ms"] / PAIR_TIMING_STEPS
     # ---- end to end through the C ABI with host state (pinned) copied every step
     eng.set_timing(False)
     crd_h = torch.empty(3 * n_atoms, dtype=torch.float64, pin_memory=True)

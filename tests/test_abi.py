@@ -96,3 +96,17 @@ def test_cls_rejects_bad_magic(tmp_path):
     p.write_bytes(b"\0" * 64)
     with pytest.raises(cls_io.ClsFormatError):
         cls_io.read_cls(str(p))
+
+
+def test_celeste_library_exports_the_reference_entry_points():
+    """libomegagene_celeste.so defines every cuda_* function include/omegagene_celeste.h declares
+    (the reference's CELESTE_GPU entry points), with C linkage."""
+    import __graft_entry__
+    __graft_entry__.build()
+    from omegagene_b200 import build as ogb
+    txt = open(os.path.join(ROOT, "include", "omegagene_celeste.h")).read()
+    names = re.findall(r"^\s*(?:int|void)\s+(cuda\w+)\s*\(", txt, re.M)
+    assert len(names) >= 30
+    lib = ctypes.CDLL(ogb.CELESTE_OUT)
+    for n in names:
+        assert hasattr(lib, n), n
