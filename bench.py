@@ -241,7 +241,7 @@ def replica_value(steps, ms_max, world):
 
 def w_walkers(seeds):
     from omegagene_b200 import systems
-    return [systems.chain_water_system(300, 2500, seed=int(k), radius=12.0, h_angles=True) for k in seeds]
+    return [systems.chain_water_system(300, 2500, seed=int(k), radius=12.0) for k in seeds]
 
 
 def w_chain():
@@ -594,7 +594,8 @@ def run_configs(args, device, pool, bg):
     eng.close()
     c1.update({"nve_drift_kcal_mol_ns_dof": d, "nve_steps": n_d, "nve_note": note})
     c1.update(paired_drift(s1, p1n, device, 6, PAIRED_STEPS, PAIRED_GAP))
-    c1["workload"] = ("2,000-atom chain (per-atom LJ types, SHAKE'd X-H) in 30,000 TIP3P waters less overlaps "
+    c1["workload"] = ("2,000-atom chain (per-atom LJ types, SHAKE'd X-H, 111 deg / 63 angles on every bonded "
+                      "triple) in 30,000 TIP3P waters less overlaps "
                       "(%d atoms, 97.3 A box); %d steps at 0.5 fs, then up to %d timed steps at 2 fs with 300 K "
                       "rescaling; force check at their end; NVE drift with the thermostat off, exact lists" % (
                           s1["n_atoms"], CHAIN_RELAX, CHAIN_STEPS))
@@ -848,7 +849,7 @@ def run_mcmd(args):
     import torch
     from omegagene_b200 import engine, serve, systems
     torch.cuda.set_device(0)
-    walkers = [systems.chain_water_system(300, 2500, seed=args.walker_seed0 + w, radius=12.0, h_angles=True)
+    walkers = [systems.chain_water_system(300, 2500, seed=args.walker_seed0 + w, radius=12.0)
                for w in range(args.walkers)]
     p = dict(engine.DEFAULT_PARAMS)
     p.update(nsgrid_update_intvl=INTVL, time_step=DT_FS, thermostat="scaling", temperature=300.0)

@@ -188,7 +188,10 @@ typedef struct {
 /* std::mt19937 state: 624 words and the next position (624 = twist before the next draw). */
 #define OG_MT_WORDS 625
 
-/* Creates an engine on a CUDA device (cuda_set_device, cuda_setup.cu:1085-1093). */
+/* Creates an engine on a CUDA device (cuda_set_device, cuda_setup.cu:1085-1093).  Debugging:
+ * with OG_DEBUG_POISON=<byte> in the environment at creation, every device buffer the engine
+ * allocates is first filled with that byte, so a kernel that reads memory nothing has written
+ * yields results that depend on the byte (runs with two bytes must agree bit for bit). */
 og_status og_create(int device, og_engine **out);
 og_status og_destroy(og_engine *e);
 /* Last error message of this engine ("" if none); valid until the next call. */

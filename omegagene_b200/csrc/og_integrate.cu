@@ -11,10 +11,18 @@ namespace og {
 // ------------------------------------------------------------- helpers
 
 // Minimum image of PBC::diff_crd_minim_image, double overload (PBC.cpp:70-84): the reference
-// truncates d * (1 / (L/2)) to int twice, with float box lengths.
+// truncates d * (1 / (L/2)) to int twice, with float box lengths.  Where float(2/L) * L rounds
+// above 2 (a 97.26 A box: by 8.8e-8), a difference within L * (L*lhi/2 - 1) of +-L (4.3e-6 A
+// there) cycles +L -> -L through the two truncations and comes back as +-L instead of ~0: two
+// atoms of one molecule on opposite faces with x offsets that agree to a few microangstroms
+// get a bond, angle or constraint vector one box long (the reference's SHAKE then diverges and
+// throws the molecule across the box).  The third pass fires only on that result (|d| > 3L/4;
+// every other result of the two passes is within L/2 of 0), so all others are the reference's
+// bit for bit.
 __device__ __forceinline__ double minim(double d, float L, float lhi) {
     d = d - (double)(L * (float)(int)(d * (double)lhi));
     d = d - (double)(L * (float)(int)(d * (double)lhi));
+    if (fabs(d) > 0.75 * (double)L) d = d > 0.0 ? d - (double)L : d + (double)L;
     return d;
 }
 
@@ -145,12 +153,13 @@ __global__ void k_angles(int n, const int4 *__restrict__ a, const double2 *__res
     const double th = acos(cost);
     const double dif = th - kt[k].y, coef = kt[k].x * dif;
     e_out[k] = coef * dif;
+    const double r12i = 1.0 / r12_2, r32i = 1.0 / r32_2;
     const double st = fmax(1e-10, sin(th));
     const double gc = -(2.0 * coef) / st;
     double w1[3], w2[3];
     for (int q = 0; q < 3; q++) {
-        w1[q] = gc * (d32[q] * rri - d12[q] * cost / r12_2);
-        w2[q] = gc * (d12[q] * rri - d32[q] * cost / r32_2);
+        w1[q] = gc * (d32[q] * rri - d12[q] * cost * r12i);
+        w2[q] = gc * (d12[q] * rri - d32[q] * cost * r32i);
     }
     add_fix(frc + 3 * (size_t)atom_slot[i], w1[0], w1[1], w1[2]);
     add_fix(frc + 3 * (size_t)atom_slot[j], -w1[0] - w2[0], -w1[1] - w2[1], -w1[2] - w2[2]);

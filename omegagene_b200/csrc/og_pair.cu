@@ -776,10 +776,18 @@ __device__ __forceinline__ void og_eval_j(OgIAcc<VIR> &A, bool active, float4 xj
         const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
         const bool act_a = ((skip >> (2 * p)) & 1u) == 0u && r2.x < K.rc2;
         const bool act_b = ((skip >> (2 * p + 1)) & 1u) == 0u && r2.y < K.rc2;
-        const float2 r2s = og_f2(act_a ? r2.x : 1.0f, act_b ? r2.y : 1.0f);
+        // zero-dipole path: a skipped pair takes r2 = +inf, so rsqrt gives 0 and every inverse
+        // power vanishes; with the ZD force constant masked too its work is 0 without a 0/1
+        // multiply.  rsqrtf alone (2 ulp) is the inverse distance of the forces: well inside
+        // their 1e-5 bar, and a central force of r alone, so still conservative.  The generic
+        // path keeps one Newton step and the 0/1 mask.
+        const float2 r2s = GEN ? og_f2(act_a ? r2.x : 1.0f, act_b ? r2.y : 1.0f)
+                               : og_f2(act_a ? r2.x : __int_as_float(0x7f800000), act_b ? r2.y : __int_as_float(0x7f800000));
         float2 y = og_f2(rsqrtf(r2s.x), rsqrtf(r2s.y));
-        const float2 h = __ffma2_rn(__fmul2_rn(__fmul2_rn(r2s, mone), y), y, one);
-        y = __ffma2_rn(__fmul2_rn(half, y), h, y);
+        if (GEN) {
+            const float2 h = __ffma2_rn(__fmul2_rn(__fmul2_rn(r2s, mone), y), y, one);
+            y = __ffma2_rn(__fmul2_rn(half, y), h, y);
+        }
         const float2 r2inv = __fmul2_rn(y, y);
         const float2 r6 = __fmul2_rn(__fmul2_rn(r2inv, r2inv), r2inv);
         const float2 pa = __ldg(&lj[T.x + tj]), pb = __ldg(&lj[T.y + tj]);
@@ -789,14 +797,19 @@ __device__ __forceinline__ void og_eval_j(OgIAcc<VIR> &A, bool active, float4 xj
         const float2 on = og_f2(act_a ? 1.f : 0.f, act_b ? 1.f : 0.f);
         float2 wc;
         if (!GEN) {
-            wc = __ffma2_rn(__fmul2_rn(cc, mone), __ffma2_rn(y, r2inv, K.nfco),
+            const float2 nfco = og_f2(act_a ? K.nfco.x : 0.f, act_b ? K.nfco.y : 0.f);
+            wc = __ffma2_rn(__fmul2_rn(cc, mone), __ffma2_rn(y, r2inv, nfco),
                             __fmul2_rn(r2inv, __ffma2_rn(t12, m12, __fmul2_rn(six, t6))));
-            wc = __fmul2_rn(wc, on);
             if (ENE) {
-                const float2 pv = __fmul2_rn(__ffma2_rn(t6, mone, t12), on);
-                const float2 pe = __fmul2_rn(__fmul2_rn(cc, __ffma2_rn(K.bco, r2s, __fadd2_rn(y, K.nzcore))), on);
+                // the Ele energy is a small net of large pair terms of both signs: its 1/r takes
+                // the Newton step (the forces above do not, so a step's forces are the same
+                // whether or not it reports energies).  The energies of skipped pairs (r2s = +inf,
+                // ye = NaN) are masked explicitly
+                const float2 ye = __ffma2_rn(__fmul2_rn(half, y), __ffma2_rn(__fmul2_rn(__fmul2_rn(r2s, mone), y), y, one), y);
+                const float2 pv = __ffma2_rn(t6, mone, t12);
+                const float2 pe = __fmul2_rn(cc, __ffma2_rn(K.bco, r2s, __fadd2_rn(ye, K.nzcore)));
                 av = __fadd2_rn(av, pv);
-                ae = __fadd2_rn(ae, pe);
+                ae = __fadd2_rn(ae, og_f2(act_a ? pe.x : 0.f, act_b ? pe.y : 0.f));
             }
         } else {
             float w2[2], v2[2], e2[2];

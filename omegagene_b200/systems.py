@@ -194,10 +194,13 @@ def _saw_chain(rng, n_backbone, radius, bond=1.53, angle_deg=111.0, min_dist=3.2
 
 
 def chain_water_system(n_chain=2000, n_waters=30000, seed=1, radius=30.0, box=None, temperature=300.0,
-                       n_sigma_bins=8, n_eps_bins=8, h_angles=False):
+                       n_sigma_bins=8, n_eps_bins=8, h_angles=True):
     """Solvated synthetic chain: every third atom is a hydrogen bonded (SHAKE pair, 1.09 A) to
     the preceding backbone atom; backbone bonds 1.53 A / 310, angles 111 deg / 63 (E = k(x-x0)^2,
-    ForceField.cpp:108-177).  Charges ~ N(0, 0.25) shifted to zero net; sigma ~ U(2.5, 3.8),
+    ForceField.cpp:108-177), on every bonded triple: backbone ones and, with h_angles, both
+    backbone neighbour - parent - H ones.  Without them a hydrogen is a free rotor on its
+    constraint sphere that can swing onto its (LJ-excluded) 1-3 neighbours; at 2 fs such a
+    chain blows up within tens of steps in FP64 as in FP32.  Charges ~ N(0, 0.25) shifted to zero net; sigma ~ U(2.5, 3.8),
     epsilon ~ U(0.02, 0.2) binned into n_sigma_bins x n_eps_bins LJ types with Lorentz-Berthelot
     mixing, or, with n_sigma_bins=None, one LJ type per chain atom with its own sigma and
     epsilon (exact Lorentz-Berthelot mixing over an (n_chain + 2)^2 table).  Waters within 2.4 A
@@ -232,10 +235,17 @@ def chain_water_system(n_chain=2000, n_waters=30000, seed=1, radius=30.0, box=No
         # leaves the H farthest from every other chain atom
         k = pos_of_bb[p]
         v0 = np.zeros(3)
-        for kk in (k - 1, k + 1):
-            if 0 <= kk < n_bb:
-                d = bb[k] - bb[kk]
-                v0 += d / np.linalg.norm(d)
+        nbs = [kk for kk in (k - 1, k + 1) if 0 <= kk < n_bb]
+        for kk in nbs:
+            d = bb[k] - bb[kk]
+            v0 += d / np.linalg.norm(d)
+        if len(nbs) == 1:
+            # a chain end: 111 deg from its one bond (along the bond the angle would be 180 deg,
+            # where the angle force's 1 / sin(theta) turns rounding into force)
+            d = v0 / np.linalg.norm(v0)
+            u = np.cross(d, rng.normal(size=3))
+            u /= np.linalg.norm(u)
+            v0 = math.cos(math.radians(69.0)) * d + math.sin(math.radians(69.0)) * u
         if np.linalg.norm(v0) < 1e-6:
             v0 = rng.normal(size=3)
         best, best_d = None, -1.0
@@ -294,12 +304,12 @@ def chain_water_system(n_chain=2000, n_waters=30000, seed=1, radius=30.0, box=No
     atom_type = np.concatenate([type_c, np.tile([0, 1, 1], nw)])
     bonds = [(bb_index[i], bb_index[i + 1], 310.0, 1.53) for i in range(n_bb - 1)]
     angles = [(bb_index[i], bb_index[i + 1], bb_index[i + 2], 63.0, math.radians(111.0)) for i in range(n_bb - 2)]
-    if h_angles:  # hold each hydrogen's direction: backbone neighbour - parent - H, 109.5 deg, k 35
+    if h_angles:  # hold each hydrogen's direction: backbone neighbour - parent - H
         for h, p in sorted(parent_of_h.items()):
             k = pos_of_bb[p]
             for kk in (k - 1, k + 1):
                 if 0 <= kk < n_bb:
-                    angles.append((bb_index[kk], p, h, 35.0, math.radians(109.5)))
+                    angles.append((bb_index[kk], p, h, 63.0, math.radians(111.0)))
     bonds = np.array(bonds, dtype=[("a1", "<i4"), ("a2", "<i4"), ("k", "<f8"), ("r0", "<f8")])
     angles = np.array(angles, dtype=[("a1", "<i4"), ("a2", "<i4"), ("a3", "<i4"), ("k", "<f8"), ("t0", "<f8")])
     # 1-2, 1-3 and 1-4 pairs are excluded from the pair list (the reference's "nb15off")

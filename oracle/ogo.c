@@ -32,16 +32,29 @@ void ogo_pbc_init(ogo_pbc *p, const double val[12]) {
     }
 }
 
-/* PBC::diff_crd_minim_image, double/double overload (PBC.cpp:70-84). */
+/* PBC::diff_crd_minim_image, double/double overload (PBC.cpp:70-84), plus one guarded pass.
+ * The reference truncates d * L_half_inv to int twice.  Where float(2/L) * L rounds above 2,
+ * a difference within L * (L * L_half_inv / 2 - 1) of +-L cycles +L -> -L through the two
+ * truncations and comes back one box long instead of ~0 (a molecule split across opposite
+ * faces with nearly equal x; the reference's SHAKE then diverges).  The third pass fires only
+ * on such a result (|d| > 3L/4; every other two-pass result lies within L/2 of 0), so every
+ * other output is the reference's bit for bit.  The engine applies the same pass. */
 static void diff_minim_d(const ogo_pbc *p, double d[3], const double a[3], const double b[3]) {
     for (int i = 0; i < 3; i++) {
         d[i] = a[i] - b[i];
         d[i] = d[i] - (double)(p->L[i] * (float)(int)(d[i] * (double)p->L_half_inv[i]));
         d[i] = d[i] - (double)(p->L[i] * (float)(int)(d[i] * (double)p->L_half_inv[i]));
+        if (fabs(d[i]) > 0.75 * (double)p->L[i]) d[i] = d[i] > 0.0 ? d[i] - (double)p->L[i] : d[i] + (double)p->L[i];
     }
 }
 
-/* PBC::diff_crd_minim_image, float/float overload (PBC.cpp:44-51). */
+/* The guarded minimum image above for n differences (tests). */
+void ogo_minim_image_d(const ogo_pbc *p, int n, const double *a, const double *b, double *d) {
+    for (int k = 0; k < n; k++) diff_minim_d(p, d + 3 * k, a + 3 * k, b + 3 * k);
+}
+
+/* PBC::diff_crd_minim_image, float/float overload (PBC.cpp:44-51), as the reference has it (no
+ * guarded pass): it serves the all-pairs FP32 build, whose output the sample's log records. */
 static void diff_minim_f(const ogo_pbc *p, float d[3], const float a[3], const float b[3]) {
     for (int i = 0; i < 3; i++) {
         d[i] = a[i] - b[i];

@@ -71,6 +71,10 @@ typedef struct {
 void ogo_pbc_init(ogo_pbc *p, const double val[12]);
 int  ogo_geom_init(ogo_geom *g, const ogo_pbc *p, int n_atoms, double nsgrid_cutoff);
 
+/* d[k] = minimum image of a[k] - b[k] (k < n, 3 doubles each): PBC::diff_crd_minim_image's two
+ * truncating passes (PBC.cpp:70-84) and the guarded third one of the engine (ogo.c). */
+void ogo_minim_image_d(const ogo_pbc *p, int n, const double *a, const double *b, double *d);
+
 /* Wraps coordinates into the box like MmSystem::revise_crd_inbox (MmSystem.cpp:808-816). */
 void ogo_revise_crd_inbox(const ogo_pbc *p, int n, double *crd);
 

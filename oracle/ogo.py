@@ -90,6 +90,7 @@ def lib():
         path = build.build_oracle()
         L = C.CDLL(path)
         L.ogo_pbc_init.argtypes = [C.POINTER(Pbc), f64p]
+        L.ogo_minim_image_d.argtypes = [C.POINTER(Pbc), C.c_int, f64p, f64p, f64p]
         L.ogo_geom_init.argtypes = [C.POINTER(Geom), C.POINTER(Pbc), C.c_int, C.c_double]
         L.ogo_grid_build.argtypes = [C.POINTER(Geom), C.c_int, f64p, C.POINTER(Grid)]
         L.ogo_grid_free.argtypes = [C.POINTER(Grid)]

@@ -26,7 +26,7 @@ pytestmark = pytest.mark.gpu
 def test_mcmd_walkers_track_oracle_200_steps():
     p = dict(engine.DEFAULT_PARAMS)
     p.update(nsgrid_update_intvl=10, time_step=2.0, thermostat="scaling", temperature=300.0)
-    walkers = [systems.chain_water_system(300, 2500, seed=500 + w, radius=12.0, h_angles=True) for w in range(3)]
+    walkers = [systems.chain_water_system(300, 2500, seed=500 + w, radius=12.0) for w in range(3)]
     warm = engine.Engine(0)
     for w in walkers:
         warm.add_system(w, dict(p, time_step=0.5))
