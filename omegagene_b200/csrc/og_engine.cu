@@ -29,17 +29,19 @@ __global__ void k_sort_columns(const int *, const int *, const int *, const int 
 __global__ void k_cell_info(const int *, int, const int *, const int *, const int *, const SysDev *, const double *,
                             const int *, double *, float2 *, int2 *, unsigned char *, int *, int *);
 __global__ void k_count_pairs(const int *, int, int, const int *, const int *, const SysDev *, const int *,
-                              const int *, const int *, const float2 *, const int2 *, const int *, const int *, int *);
+                              const int *, const int *, const float2 *, const int2 *, const int *, const int *,
+                              const int *, int *);
 __global__ void k_fill_pairs(int *, int, int, long long, const int *, const int *, const SysDev *, const int *,
                              const int *, const int *, const float2 *, const int2 *, const int *, const int *,
-                             const int *, int2 *);
+                             const int *, const long long *, int2 *);
 __global__ void k_pair_records(const int *, long long, const int *, const SysDev *, const int *, const int2 *,
                                const unsigned char *, const int *, const int *, const int *, const int *, const int *,
                                const double *, unsigned long long *, float4 *);
 __global__ void k_cell_excl(const int *, int, const int *, const int *, const int *, const int *, int *);
-__global__ void k_pair_heads(int *, int, int, const int *, int *);
-__global__ void k_scan_block(const int *, int *, long long, int *);
-__global__ void k_scan_add(int *, long long, const int *);
+__global__ void k_pair_heads(int *, int, int, long long, const long long *, int *);
+template <typename TI>
+__global__ void k_scan_block(const TI *, long long *, long long, long long *);
+__global__ void k_scan_add(long long *, long long, const long long *);
 // og_pair.cu
 template <bool VIR, int MINB>
 __global__ void k_pair_ljzd(const int *, const int *, const SysDev *, const float4 *, const float4 *, const int *,
@@ -253,8 +255,9 @@ struct og_engine {
     float jl_skin = OG_JL_SKIN;
     unsigned long long *d_frc = nullptr;
     int *d_uni_lo = nullptr, *d_uni_hi = nullptr;
-    int *d_count = nullptr, *d_offset = nullptr;
-    std::vector<int *> d_scan_tmp;  // per level: sums, scanned sums
+    int *d_count = nullptr;
+    long long *d_offset = nullptr;        // 64-bit exclusive scan of d_count (pair list offsets)
+    std::vector<long long *> d_scan_tmp;  // per level: sums, scanned sums
     std::vector<long long> scan_len;
     int2 *d_cp_c2img = nullptr;
     unsigned long long *d_cp_mask = nullptr;
@@ -702,14 +705,15 @@ og_status build_exclusions(og_engine *e, HostSystem &h) {
 
 // ---------------------------------------------------------- device scan
 
-og_status scan_exclusive(og_engine *e, const int *in, int *out, long long n, int level) {
+template <typename TI>
+og_status scan_exclusive(og_engine *e, const TI *in, long long *out, long long n, int level) {
     const long long nb = (n + 2047) / 2048;
     if (level >= (int)e->d_scan_tmp.size() / 2) return fail(e, OG_ERR_CAPACITY, "scan depth");
-    int *sums = e->d_scan_tmp[2 * level], *sums_out = e->d_scan_tmp[2 * level + 1];
-    k_scan_block<<<(unsigned)nb, 1024, 0, e->stream>>>(in, out, n, nb > 1 ? sums : nullptr);
+    long long *sums = e->d_scan_tmp[2 * level], *sums_out = e->d_scan_tmp[2 * level + 1];
+    k_scan_block<TI><<<(unsigned)nb, 1024, 0, e->stream>>>(in, out, n, nb > 1 ? sums : nullptr);
     LAUNCH_CHECK();
     if (nb > 1) {
-        og_status s = scan_exclusive(e, sums, sums_out, nb, level + 1);
+        og_status s = scan_exclusive<long long>(e, sums, sums_out, nb, level + 1);
         if (s) return s;
         k_scan_add<<<blocks(n, 256), 256, 0, e->stream>>>(out, n, sums_out);
         LAUNCH_CHECK();
@@ -763,17 +767,18 @@ og_status build_list(og_engine *e) {
     k_count_pairs<<<blocks(n_items, 256), 256, 0, st>>>(e->d_counters, e->cells_cap, e->nnc, e->d_cell_sys,
                                                          e->d_sys_cell_base, e->d_sys, e->d_cell_col,
                                                          e->d_col_cell_start, e->d_col_head_cell, e->d_cell_zr,
-                                                         e->d_cell_uni, e->d_uni_lo, e->d_uni_hi, e->d_count);
+                                                         e->d_cell_uni, e->d_uni_lo, e->d_uni_hi, e->d_sys_fault,
+                                                         e->d_count);
     LAUNCH_CHECK();
-    og_status s = scan_exclusive(e, e->d_count, e->d_offset, n_items + 1, 0);
+    og_status s = scan_exclusive<int>(e, e->d_count, e->d_offset, n_items + 1, 0);
     if (s) return s;
-    k_pair_heads<<<blocks(e->cells_cap + 1, 256), 256, 0, st>>>(e->d_counters, e->cells_cap, e->nnc, e->d_offset,
-                                                                 e->d_cp_head);
+    k_pair_heads<<<blocks(e->cells_cap + 1, 256), 256, 0, st>>>(e->d_counters, e->cells_cap, e->nnc, e->pair_cap,
+                                                                 e->d_offset, e->d_cp_head);
     LAUNCH_CHECK();
     k_fill_pairs<<<blocks(n_items, 256), 256, 0, st>>>(
         e->d_counters, e->cells_cap, e->nnc, e->pair_cap, e->d_cell_sys, e->d_sys_cell_base, e->d_sys, e->d_cell_col,
-        e->d_col_cell_start, e->d_col_head_cell, e->d_cell_zr, e->d_cell_uni, e->d_uni_lo, e->d_uni_hi, e->d_offset,
-        e->d_cp_c2img);
+        e->d_col_cell_start, e->d_col_head_cell, e->d_cell_zr, e->d_cell_uni, e->d_uni_lo, e->d_uni_hi,
+        e->d_sys_fault, e->d_offset, e->d_cp_c2img);
     LAUNCH_CHECK();
     k_pair_records<<<blocks((long long)e->cells_cap * 32, 256), 256, 0, st>>>(
         e->d_counters, e->pair_cap, e->d_cell_sys, e->d_sys, e->d_cp_head, e->d_cp_c2img, e->d_cell_valid,
@@ -2047,6 +2052,10 @@ og_status og_finalize(og_engine *e) {
         sd[k] = D;
     }
     sys_col_base[S] = col_base;
+    // the j-queue and j-list kernels read the LJ table pre-scaled for forces, (6 C6, 12 C12),
+    // from a copy after the plain one
+    for (int k = 0; k < S; k++) sd[k].ljf_off = lj_base;
+    for (int i = 0; i < lj_base; i++) lj.push_back(make_float2(6.0f * lj[i].x, 12.0f * lj[i].y));
     e->n_atoms = atom_base;
     e->n_cols = col_base;
     e->n_uni = uni_base;
@@ -2206,7 +2215,7 @@ og_status og_finalize(og_engine *e) {
     if ((s = dalloc(e, &e->d_count, n_items)) || (s = dalloc(e, &e->d_offset, n_items))) return s;
     for (long long len = n_items; len > 1;) {
         long long nb = (len + 2047) / 2048;
-        int *a, *b;
+        long long *a, *b;
         if ((s = dalloc(e, &a, nb)) || (s = dalloc(e, &b, nb))) return s;
         e->d_scan_tmp.push_back(a);
         e->d_scan_tmp.push_back(b);

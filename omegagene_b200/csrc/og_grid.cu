@@ -30,13 +30,23 @@ __global__ void k_assign_columns(const SysDev *__restrict__ sys, const int *__re
     for (int d = 0; d < 2; d++) {
         float x = __double2float_rn(crd[3 * a + d] - (double)S.lowerf[d]);
         if (!(fabsf(x) < 64.0f * S.Lf[d])) { bad = true; x = 0.0f; }
-        for (int it = 0; it < 128 && x < 0.0f; it++) x = __fadd_rn(x, S.Lf[d]);
-        for (int it = 0; it < 128 && x >= S.Lf[d]; it++) x = __fsub_rn(x, S.Lf[d]);
-        int ci = (int)floorf(__fdiv_rn(x, S.L_cell[d]));
         const int nd = d == 0 ? S.nx : S.ny;
-        // MiniCell::get_column_id_from_crd (:1251-1259)
-        if (ci < 0) ci += nd;
-        if (ci >= nd) ci -= nd;
+        int ci;
+        if (x >= 0.0f && x <= S.Lf[d]) {
+            // An in-box coordinate stays in the column that holds it.  Within a few
+            // microangstroms of the upper face x, or x / L_cell, rounds up to the box length or
+            // the column count, which the reference wraps to column 0 (MiniCell.cpp:329-335,
+            // :1251-1259): the atom would sit one box length from the grid coordinate it keeps,
+            // and its pairs within the cutoff would be missed until the next build.
+            ci = min((int)floorf(__fdiv_rn(x, S.L_cell[d])), nd - 1);
+        } else {
+            for (int it = 0; it < 128 && x < 0.0f; it++) x = __fadd_rn(x, S.Lf[d]);
+            for (int it = 0; it < 128 && x >= S.Lf[d]; it++) x = __fsub_rn(x, S.Lf[d]);
+            ci = (int)floorf(__fdiv_rn(x, S.L_cell[d]));
+            // MiniCell::get_column_id_from_crd (:1251-1259)
+            if (ci < 0) ci += nd;
+            if (ci >= nd) ci -= nd;
+        }
         if (ci < 0 || ci >= nd) { bad = true; ci = 0; }
         c[d] = ci;
     }
@@ -332,13 +342,19 @@ __device__ int enumerate_column(int c1, int nb, const SysDev &S, int cell_base,
         int fu = x2 * nuz + y2 * (nuz * nx) + first_u[ii];
         int lu = x2 * nuz + y2 * (nuz * nx) + last_u[ii];
         if (fu < 0 || lu >= n_uni) continue;
-        int stg = 0;
-        for (int u = fu; u <= lu; u++) {
-            const bool filled = uni_lo[S.uni_base + u] != 0x7fffffff;
-            if (stg == 0 && filled) { stg = 1; fu = u; }
-            else if (stg == 1 && !filled) { lu = u - 1; break; }
-        }
-        if (stg == 0) continue;
+        // The window's cells run from its first to its last filled bin.  The reference stops at
+        // the first empty bin after a filled one (MiniCell.cpp:1062-1076), so a z gap in column
+        // 2 of a bin's height or more (7.5 A in a 44.8 A water box) hides every cell beyond it,
+        // pairs within the cutoff included.  Without such a gap both give the same list.
+        int f = -1, l = -1;
+        for (int u = fu; u <= lu; u++)
+            if (uni_lo[S.uni_base + u] != 0x7fffffff) {
+                if (f < 0) f = u;
+                l = u;
+            }
+        if (f < 0) continue;
+        fu = f;
+        lu = l;
         const int lo = uni_lo[S.uni_base + fu], hi = uni_hi[S.uni_base + lu];
         if (lo > hi || head2 < 0) continue;
         // z indices stay inside column 2 (a bin can alias the next column's bin 0 when a
@@ -374,7 +390,8 @@ __global__ void k_count_pairs(const int *__restrict__ counters, int cells_cap, i
                               const SysDev *__restrict__ sys, const int *__restrict__ cell_col,
                               const int *__restrict__ col_cell_start, const int *__restrict__ col_head_cell,
                               const float2 *__restrict__ cell_zr, const int2 *__restrict__ cell_uni,
-                              const int *__restrict__ uni_lo, const int *__restrict__ uni_hi, int *__restrict__ count) {
+                              const int *__restrict__ uni_lo, const int *__restrict__ uni_hi,
+                              const int *__restrict__ sys_fault, int *__restrict__ count) {
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (long long)cells_cap * nnc) return;
     const int c1 = (int)(idx / nnc), nb = (int)(idx % nnc);
@@ -383,7 +400,9 @@ __global__ void k_count_pairs(const int *__restrict__ counters, int cells_cap, i
     if (c1 < n_cells) {
         const int s = cell_sys[c1];
         const SysDev &S = sys[s];
-        if (nb < S.n_nb_cols)
+        // a system already faulted in this call (its coordinates left the box or piled into one
+        // column) gets no pairs: the call is undone, and its list would be all pairs of a column
+        if (nb < S.n_nb_cols && sys_fault[s] == 0)
             n = enumerate_column(c1, nb, S, sys_cell_base[s], cell_col, col_cell_start, col_head_cell, cell_zr,
                                  cell_uni, uni_lo, uni_hi, nullptr, 0);
     }
@@ -396,14 +415,15 @@ __global__ void k_fill_pairs(int *__restrict__ counters, int cells_cap, int nnc,
                              const int *__restrict__ col_cell_start, const int *__restrict__ col_head_cell,
                              const float2 *__restrict__ cell_zr, const int2 *__restrict__ cell_uni,
                              const int *__restrict__ uni_lo, const int *__restrict__ uni_hi,
-                             const int *__restrict__ offset, int2 *__restrict__ cp_c2img) {
+                             const int *__restrict__ sys_fault, const long long *__restrict__ offset,
+                             int2 *__restrict__ cp_c2img) {
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int n_cells = counters[OG_CNT_N_CELLS];
     if (idx >= (long long)n_cells * nnc) return;
     const int c1 = (int)(idx / nnc), nb = (int)(idx % nnc);
     const int s = cell_sys[c1];
     const SysDev &S = sys[s];
-    if (nb >= S.n_nb_cols) return;
+    if (nb >= S.n_nb_cols || sys_fault[s] != 0) return;
     const long long off = offset[idx];
     const int cap = (int)max(0ll, min(pair_cap - off, (long long)1 << 30));
     int n = enumerate_column(c1, nb, S, sys_cell_base[s], cell_col, col_cell_start, col_head_cell, cell_zr, cell_uni,
@@ -443,23 +463,28 @@ __global__ void k_pair_records(const int *__restrict__ counters, long long pair_
 }
 
 // CSR heads from the scanned counts; also publishes the total.
-__global__ void k_pair_heads(int *__restrict__ counters, int cells_cap, int nnc, const int *__restrict__ offset,
-                             int *__restrict__ cp_head) {
+// Heads are held within the buffer (pair_cap): past it the list is incomplete, the fill flags
+// it, and every kernel that walks [cp_head[c], cp_head[c + 1]) stays inside the buffer.
+__global__ void k_pair_heads(int *__restrict__ counters, int cells_cap, int nnc, long long pair_cap,
+                             const long long *__restrict__ offset, int *__restrict__ cp_head) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int n_cells = counters[OG_CNT_N_CELLS];
-    const int total = offset[(long long)cells_cap * nnc];
+    const long long total = offset[(long long)cells_cap * nnc];
     if (c > cells_cap) return;
-    cp_head[c] = c < n_cells ? offset[(long long)c * nnc] : total;
-    if (c == 0) counters[OG_CNT_N_PAIRS] = total;
+    cp_head[c] = (int)min(c < n_cells ? offset[(long long)c * nnc] : total, pair_cap);
+    if (c == 0) counters[OG_CNT_N_PAIRS] = (int)min(total, 2147483647ll);
 }
 
 // ------------------------------------------------------------------ scan
 
 // Exclusive scan of an int array in blocks of 2*blockDim (Blelloch-free Hillis-Steele per
 // block, then block totals are scanned by the same kernel recursively from the host).
-__global__ void k_scan_block(const int *__restrict__ in, int *__restrict__ out, long long n,
-                             int *__restrict__ block_sums) {
-    __shared__ int s[2048];
+// 64-bit sums: the pair counts of a blown-up system (its atoms piled into one column) can total
+// more than 2^31, and a wrapped offset would send the list fill outside its buffer.
+template <typename TI>
+__global__ void k_scan_block(const TI *__restrict__ in, long long *__restrict__ out, long long n,
+                             long long *__restrict__ block_sums) {
+    __shared__ long long s[2048];
     const long long base = (long long)blockIdx.x * 2048;
     for (int k = 0; k < 2; k++) {
         long long i = base + threadIdx.x + k * 1024;
@@ -488,7 +513,7 @@ __global__ void k_scan_block(const int *__restrict__ in, int *__restrict__ out, 
         if (threadIdx.x < d) {
             int ai = off * (2 * threadIdx.x + 1) - 1;
             int bi = off * (2 * threadIdx.x + 2) - 1;
-            int t = s[ai];
+            long long t = s[ai];
             s[ai] = s[bi];
             s[bi] += t;
         }
@@ -499,8 +524,10 @@ __global__ void k_scan_block(const int *__restrict__ in, int *__restrict__ out, 
         if (i < n) out[i] = s[threadIdx.x + k * 1024];
     }
 }
+template __global__ void k_scan_block<int>(const int *, long long *, long long, long long *);
+template __global__ void k_scan_block<long long>(const long long *, long long *, long long, long long *);
 
-__global__ void k_scan_add(int *__restrict__ out, long long n, const int *__restrict__ block_offsets) {
+__global__ void k_scan_add(long long *__restrict__ out, long long n, const long long *__restrict__ block_offsets) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] += block_offsets[i / 2048];
 }

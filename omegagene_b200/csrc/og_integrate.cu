@@ -1058,7 +1058,12 @@ __global__ void k_put_state(int n_atoms, int atom0, const int *__restrict__ atom
             const double g = slot_crd[3 * (size_t)sl + q] + d;
             slot_crd[3 * (size_t)sl + q] = g;
             r[q] = (float)(g - cell_origin[3 * c + q]);
-            crd[3 * a + q] = x;
+            // held in the box as every step end holds it (SubBox.cpp:1482-1502), so that a list
+            // built from it puts the atom in the column of its own grid coordinate
+            double xw = x;
+            if (xw >= (double)S.upperf[q]) xw -= (double)S.Lf[q];
+            else if (xw < (double)S.lowerf[q]) xw += (double)S.Lf[q];
+            crd[3 * a + q] = xw;
         }
         if (new_vel) vel_next[3 * a + q] = new_vel[3 * i + q];
     }

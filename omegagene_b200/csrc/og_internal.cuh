@@ -67,6 +67,7 @@ struct SysDev {
     double max_step_disp2;       // squared displacement per step beyond which a system is faulted
     float list_trig2;            // displacement list policy: squared half margin, (nsgrid_cutoff - cutoff)^2 / 4
     int lj_base, n_types;
+    int ljf_off;                 // the force-scaled copy (6 C6, 12 C12) of the LJ table starts here
     // integrator
     double dt;
     double temperature_coeff_thermo;  // Thermostat.cpp:13-16

@@ -721,14 +721,17 @@ struct OgICell {
     int2 t2[OG_CELL / 2];
 };
 
+// GEN = false: the row offsets point into the force-scaled copy of the LJ table (6 C6, 12 C12).
+template <bool GEN>
 __device__ __forceinline__ void og_load_icell(OgICell &ic, int c1, int lane, const float4 *__restrict__ xq,
                                               const int *__restrict__ slot_type, const SysDev &S) {
     if (lane < OG_CELL / 2) {
         const float4 a = xq[c1 * OG_CELL + 2 * lane], b = xq[c1 * OG_CELL + 2 * lane + 1];
+        const int base = S.lj_base + (GEN ? 0 : S.ljf_off);
         ic.ab[lane][0] = make_float4(a.x, b.x, a.y, b.y);
         ic.ab[lane][1] = make_float4(a.z, b.z, a.w * (float)OG_CHARGE_COEFF, b.w * (float)OG_CHARGE_COEFF);
-        ic.t2[lane] = make_int2(slot_type[c1 * OG_CELL + 2 * lane] * S.n_types + S.lj_base,
-                                slot_type[c1 * OG_CELL + 2 * lane + 1] * S.n_types + S.lj_base);
+        ic.t2[lane] = make_int2(slot_type[c1 * OG_CELL + 2 * lane] * S.n_types + base,
+                                slot_type[c1 * OG_CELL + 2 * lane + 1] * S.n_types + base);
     }
     __syncwarp();
 }
@@ -760,10 +763,10 @@ __device__ __forceinline__ void og_eval_j(OgIAcc<VIR> &A, bool active, float4 xj
                                           int img, const OgICell &ic, const OgZdConst &K, const SysDev &S,
                                           const EleDev &E, const float2 *__restrict__ lj,
                                           const float2 *__restrict__ hps, unsigned long long *__restrict__ frc) {
-    const float2 one = og_f2(1.f, 1.f), half = og_f2(0.5f, 0.5f), six = og_f2(6.f, 6.f);
-    const float2 m12 = og_f2(-12.f, -12.f), mone = og_f2(-1.f, -1.f);
+    const float2 one = og_f2(1.f, 1.f), half = og_f2(0.5f, 0.5f), mone = og_f2(-1.f, -1.f);
     const float2 nrx = og_f2(-xj.x, -xj.x), nry = og_f2(-xj.y, -xj.y), nrz = og_f2(-xj.z, -xj.z);
-    const float2 qj = og_f2(xj.w, xj.w);
+    // GEN: +q_j; zero-dipole path: -q_j, so cc below is -q_i q_j (the sign the work takes)
+    const float2 qj = GEN ? og_f2(xj.w, xj.w) : og_f2(-xj.w, -xj.w);
     float2 av = og_f2(0.f, 0.f), ae = og_f2(0.f, 0.f);
     float2 wjx = og_f2(0.f, 0.f), wjy = og_f2(0.f, 0.f), wjz = og_f2(0.f, 0.f);
 #pragma unroll
@@ -791,25 +794,27 @@ __device__ __forceinline__ void og_eval_j(OgIAcc<VIR> &A, bool active, float4 xj
         const float2 r2inv = __fmul2_rn(y, y);
         const float2 r6 = __fmul2_rn(__fmul2_rn(r2inv, r2inv), r2inv);
         const float2 pa = __ldg(&lj[T.x + tj]), pb = __ldg(&lj[T.y + tj]);
-        const float2 t6 = __fmul2_rn(og_f2(pa.x, pb.x), r6);
-        const float2 t12 = __fmul2_rn(__fmul2_rn(og_f2(pa.y, pb.y), r6), r6);
+        const float2 c6p = og_f2(pa.x, pb.x), c12p = og_f2(pa.y, pb.y);
+        // zero-dipole path: t6 = 6 C6 / r^6 and t12 = 12 C12 / r^12 from the scaled table
+        const float2 t6 = __fmul2_rn(c6p, r6);
+        const float2 t12 = __fmul2_rn(__fmul2_rn(c12p, r6), r6);
         const float2 cc = __fmul2_rn(og_f2(Bp.z, Bp.w), qj);
         const float2 on = og_f2(act_a ? 1.f : 0.f, act_b ? 1.f : 0.f);
         float2 wc;
         if (!GEN) {
+            // work = -q_i q_j (1/r^3 - fco) + (6 C6/r^6 - 12 C12/r^12) / r^2, cc = -q_i q_j
             const float2 nfco = og_f2(act_a ? K.nfco.x : 0.f, act_b ? K.nfco.y : 0.f);
-            wc = __ffma2_rn(__fmul2_rn(cc, mone), __ffma2_rn(y, r2inv, nfco),
-                            __fmul2_rn(r2inv, __ffma2_rn(t12, m12, __fmul2_rn(six, t6))));
+            wc = __ffma2_rn(cc, __ffma2_rn(y, r2inv, nfco), __fmul2_rn(r2inv, __ffma2_rn(t12, mone, t6)));
             if (ENE) {
                 // the Ele energy is a small net of large pair terms of both signs: its 1/r takes
                 // the Newton step (the forces above do not, so a step's forces are the same
                 // whether or not it reports energies).  The energies of skipped pairs (r2s = +inf,
                 // ye = NaN) are masked explicitly
                 const float2 ye = __ffma2_rn(__fmul2_rn(half, y), __ffma2_rn(__fmul2_rn(__fmul2_rn(r2s, mone), y), y, one), y);
-                const float2 pv = __ffma2_rn(t6, mone, t12);
+                const float2 pv = __ffma2_rn(t12, og_f2(1.f / 12.f, 1.f / 12.f), __fmul2_rn(t6, og_f2(-1.f / 6.f, -1.f / 6.f)));
                 const float2 pe = __fmul2_rn(cc, __ffma2_rn(K.bco, r2s, __fadd2_rn(ye, K.nzcore)));
                 av = __fadd2_rn(av, pv);
-                ae = __fadd2_rn(ae, og_f2(act_a ? pe.x : 0.f, act_b ? pe.y : 0.f));
+                ae = __fadd2_rn(ae, og_f2(act_a ? -pe.x : 0.f, act_b ? -pe.y : 0.f));
             }
         } else {
             float w2[2], v2[2], e2[2];
@@ -841,13 +846,12 @@ __device__ __forceinline__ void og_eval_j(OgIAcc<VIR> &A, bool active, float4 xj
             }
         }
         if (VIR) A.n_act += (act_a ? 1 : 0) + (act_b ? 1 : 0);
-        const float2 wx = __fmul2_rn(wc, dx), wy = __fmul2_rn(wc, dy), wz = __fmul2_rn(wc, dz);
-        A.fx[p] = __fadd2_rn(A.fx[p], wx);
-        A.fy[p] = __fadd2_rn(A.fy[p], wy);
-        A.fz[p] = __fadd2_rn(A.fz[p], wz);
-        wjx = __fadd2_rn(wjx, wx);
-        wjy = __fadd2_rn(wjy, wy);
-        wjz = __fadd2_rn(wjz, wz);
+        A.fx[p] = __ffma2_rn(wc, dx, A.fx[p]);
+        A.fy[p] = __ffma2_rn(wc, dy, A.fy[p]);
+        A.fz[p] = __ffma2_rn(wc, dz, A.fz[p]);
+        wjx = __ffma2_rn(wc, dx, wjx);
+        wjy = __ffma2_rn(wc, dy, wjy);
+        wjz = __ffma2_rn(wc, dz, wjz);
     }
     if (ENE) {
         A.dv += (double)av.x + (double)av.y;
@@ -944,7 +948,7 @@ k_pair_ljzd_jq(const int *__restrict__ counters, const int *__restrict__ cell_sy
     __shared__ float4 s_rsp[NT / 32][32];    // surviving records of the current chunk, in order:
     __shared__ uint2 s_rm[NT / 32][32];      //   shift + cell2, exclusion mask,
     __shared__ int s_rimg[NT / 32][VIR ? 32 : 1];  //   image bits (virial only)
-    og_load_icell(s_i[wib], c1, lane, xq, slot_type, S);
+    og_load_icell<GEN>(s_i[wib], c1, lane, xq, slot_type, S);
     const OgZdConst K = og_zd_const(S);
     const float rskip = sqrtf(K.rc2) + 1e-3f, rskip2 = rskip * rskip;
     const float4 b1l = bbox[2 * c1], b1h = bbox[2 * c1 + 1];
@@ -1178,7 +1182,7 @@ k_pair_ljzd_jl(int *__restrict__ counters, const int *__restrict__ cell_sys, con
     const SysDev &S = sys[cell_sys[c1]];
     const EleDev &E = ele[GEN ? cell_sys[c1] : 0];
     __shared__ OgICell s_i[NT / 32];
-    og_load_icell(s_i[wib], c1, lane, xq, slot_type, S);
+    og_load_icell<GEN>(s_i[wib], c1, lane, xq, slot_type, S);
     const OgZdConst K = og_zd_const(S);
     OgIAcc<VIR> A;
     og_iacc_zero(A);

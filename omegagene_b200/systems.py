@@ -66,11 +66,19 @@ def _wrap(crd, lo, box):
     return lo + np.mod(crd - lo, box)
 
 
-def water_system(n_waters, box=None, seed=0, temperature=300.0, lattice_m=None, jitter=0.3):
-    """Rigid TIP3P box: one SHAKE trio per molecule, exclusions within molecules."""
+def water_system(n_waters, box=None, seed=0, temperature=300.0, lattice_m=None, jitter=0.3, void=None):
+    """Rigid TIP3P box: one SHAKE trio per molecule, exclusions within molecules.  void = (lo, hi)
+    corners of a block (box-centred coordinates): molecules with an atom inside it are removed,
+    leaving a cavity."""
     rng = np.random.default_rng(seed)
     box = float(box if box is not None else water_box_side(n_waters))
     crd = water_positions(rng, n_waters, box, lattice_m=lattice_m, jitter=jitter)
+    if void is not None:
+        lo, hi = np.asarray(void[0], float), np.asarray(void[1], float)
+        c = crd.reshape(-1, 3, 3) - 0.5 * box
+        inside = np.all((c >= lo) & (c <= hi), axis=2).any(axis=1)
+        crd = crd.reshape(-1, 3, 3)[~inside].reshape(-1, 3)
+        n_waters = len(crd) // 3
     n = 3 * n_waters
     mass = np.tile([M_O, M_H, M_H], n_waters)
     vel = _maxwell(rng, mass, temperature)

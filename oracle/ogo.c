@@ -121,7 +121,7 @@ static int cmp_zkey(const void *a, const void *b) {
  * into columns, then quicksorts each column on z.  Here each column is ordered by
  * (float z, atom id): identical to the reference wherever no two atoms of a column share
  * a float z, and a fixed tie order otherwise. */
-int ogo_grid_build(const ogo_geom *g, int n_atoms, const double *crd, ogo_grid *out) {
+int ogo_grid_build(const ogo_geom *g, int n_atoms, const double *crd, int reference_wrap, ogo_grid *out) {
     memset(out, 0, sizeof(*out));
     const int nc = g->n_columns;
     int *col_of  = (int *)malloc(sizeof(int) * (size_t)(n_atoms > 0 ? n_atoms : 1));
@@ -131,6 +131,15 @@ int ogo_grid_build(const ogo_geom *g, int n_atoms, const double *crd, ogo_grid *
         int c[2];
         for (int d = 0; d < 2; d++) {
             float x = (float)(crd[i * 3 + d] - (double)g->box_lower[d]);
+            if (!reference_wrap && x >= 0.0f && x <= g->exbox_l[d]) {
+                /* an in-box coordinate stays in the column that holds it: within a few
+                 * microangstroms of the upper face, x or x / L_cell rounds up to the box length or
+                 * the column count, which the reference wraps to column 0 (MiniCell.cpp:329-335,
+                 * :1251-1259), one box length from the coordinate the grid keeps for the atom */
+                int ci = (int)floorf(x / g->L_cell[d]);
+                c[d] = ci < g->n_cells_xy[d] ? ci : g->n_cells_xy[d] - 1;
+                continue;
+            }
             while (x < 0.0f) x += g->exbox_l[d];
             while (x >= g->exbox_l[d]) x -= g->exbox_l[d];
             c[d] = (int)floorf(x / g->L_cell[d]);
@@ -248,7 +257,7 @@ static uint64_t pair_mask(const ogo_grid *gr, int c1, int c2, const int *nb15off
  * add_cell_pair (:1163-1203).  Loop order and float arithmetic are those of the
  * reference, so the list comes out in the reference's order. */
 int ogo_enumerate_cell_pairs(const ogo_geom *g, const ogo_pbc *p, const ogo_grid *gr,
-                             const int *nb15off, int max_nb15off, ogo_cellpairs *out) {
+                             const int *nb15off, int max_nb15off, int reference_gap_stop, ogo_cellpairs *out) {
     memset(out, 0, sizeof(*out));
     const int nx = g->n_cells_xy[0], ny = g->n_cells_xy[1], nuz = g->n_uni_z;
     const int n_uni = g->n_columns * nuz;
@@ -318,12 +327,22 @@ int ogo_enumerate_cell_pairs(const ogo_geom *g, const ogo_pbc *p, const ogo_grid
                     if (first_u[ii] < 0) continue;
                     int fu = x2 * nuz + y2 * (nuz * nx) + first_u[ii];
                     int lu = x2 * nuz + y2 * (nuz * nx) + last_u[ii];
-                    int stg = 0;
+                    /* reference_gap_stop: the reference's scan (MiniCell.cpp:1062-1076), which
+                     * ends at the first empty bin after a filled one and so hides the cells
+                     * beyond a z gap of a bin's height; otherwise the engine's window, from the
+                     * first to the last filled bin (the same list when no bin inside is empty) */
+                    int f = -1, l = -1;
                     for (int u = fu; u <= lu; u++) {
-                        if (stg == 0 && uni_lo[u] >= 0) { stg = 1; fu = u; }
-                        else if (stg == 1 && uni_lo[u] < 0) { lu = u - 1; break; }
+                        if (uni_lo[u] >= 0) {
+                            if (f < 0) f = u;
+                            l = u;
+                        } else if (f >= 0 && reference_gap_stop) {
+                            break;
+                        }
                     }
-                    if (stg == 0) continue;
+                    if (f < 0) continue;
+                    fu = f;
+                    lu = l;
                     int lo = uni_lo[fu], hi = uni_hi[lu];
                     if (lo > hi || head2 < 0) continue;
                     int first_cell = head2 + lo, last_cell = head2 + hi;

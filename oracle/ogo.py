@@ -92,10 +92,10 @@ def lib():
         L.ogo_pbc_init.argtypes = [C.POINTER(Pbc), f64p]
         L.ogo_minim_image_d.argtypes = [C.POINTER(Pbc), C.c_int, f64p, f64p, f64p]
         L.ogo_geom_init.argtypes = [C.POINTER(Geom), C.POINTER(Pbc), C.c_int, C.c_double]
-        L.ogo_grid_build.argtypes = [C.POINTER(Geom), C.c_int, f64p, C.POINTER(Grid)]
+        L.ogo_grid_build.argtypes = [C.POINTER(Geom), C.c_int, f64p, C.c_int, C.POINTER(Grid)]
         L.ogo_grid_free.argtypes = [C.POINTER(Grid)]
         L.ogo_enumerate_cell_pairs.argtypes = [C.POINTER(Geom), C.POINTER(Pbc), C.POINTER(Grid), i32p, C.c_int,
-                                               C.POINTER(CellPairs)]
+                                               C.c_int, C.POINTER(CellPairs)]
         L.ogo_cellpairs_free.argtypes = [C.POINTER(CellPairs)]
         L.ogo_zd_constants.argtypes = [C.c_double, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                        C.POINTER(C.c_float)]
@@ -188,17 +188,23 @@ def wrap_inbox(pbc, crd):
 
 
 class CellList:
-    """Grid assignment + cell-pair list computed by the oracle (copied to numpy)."""
+    """Grid assignment + cell-pair list computed by the oracle (copied to numpy).  reference=True
+    keeps two faults of the reference's: its bin scan hides the cells of a neighbour column
+    beyond a z gap of a uniform bin's height (MiniCell.cpp:1062-1076), and its column arithmetic
+    wraps an in-box coordinate within float rounding of the upper face into column 0
+    (:329-335).  The default is the engine's grid and list, equal to the reference's whenever
+    neither case occurs."""
 
-    def __init__(self, pbc, geom, crd, nb15off):
+    def __init__(self, pbc, geom, crd, nb15off, reference=False):
         L = lib()
         grid = Grid()
         crd = np.ascontiguousarray(crd, np.float64).reshape(-1)
         n = len(crd) // 3
-        L.ogo_grid_build(C.byref(geom), n, crd, C.byref(grid))
+        L.ogo_grid_build(C.byref(geom), n, crd, 1 if reference else 0, C.byref(grid))
         cps = CellPairs()
         L.ogo_enumerate_cell_pairs(C.byref(geom), C.byref(pbc), C.byref(grid),
-                                   np.ascontiguousarray(nb15off, np.int32).reshape(-1), MAX_NB15OFF, C.byref(cps))
+                                   np.ascontiguousarray(nb15off, np.int32).reshape(-1), MAX_NB15OFF,
+                                   1 if reference else 0, C.byref(cps))
         self._grid, self._cps = grid, cps
         self.n_cells = grid.n_cells
         self.n_slots = grid.n_slots

@@ -12,6 +12,8 @@ import pytest
 from omegagene_b200 import engine, systems
 from oracle import ogo
 
+import cases
+
 pytestmark = pytest.mark.gpu
 
 FORCE_RTOL = 1e-5
@@ -51,6 +53,10 @@ SMALL = [
     ("water1500", lambda: systems.water_system(1500, seed=5)),
     ("water700", lambda: systems.water_system(700, seed=9)),
     ("chain300", lambda: systems.chain_water_system(300, 2500, seed=4, radius=12.0)),
+    # where the reference's list build loses pairs (tests/cases.py, test_oracle.py): a cavity
+    # whose z gap its bin scan does not cross, an oxygen at the upper face
+    ("water_void", cases.void_water),
+    ("water_face", cases.face_water),
 ]
 
 

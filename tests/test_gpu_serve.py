@@ -111,6 +111,31 @@ def test_faulted_system_is_isolated(variant):
         assert np.array_equal(c1, c2) and np.array_equal(v1, v2)
 
 
+@pytest.mark.parametrize("graphs", [False, True])
+def test_blown_up_large_system_faults_cleanly(graphs):
+    """A 600,000-atom system whose velocities carry every atom far out of its box in one step:
+    at the next list build (fixed schedule, every step) all its atoms fall into one MiniCell
+    column of ~75,000 cells, whose cell pairs would number more than 2^31.  The system is
+    faulted before the pair enumeration, which gives it no pairs (and the list offsets are
+    64-bit besides), so the call ends in OG_ERR_SYSTEM_FAULT naming that system, with the other
+    system back at the call's start."""
+    p = _params(nsgrid_update_intvl=1, time_step=2.0)
+    big = systems.water_system(200000, seed=70)
+    big = dict(big, vel=np.asarray(big["vel"]) * 1e9)
+    small = systems.water_system(800, seed=71)
+    eng = _engine([(big, p), (small, p)], 10)
+    eng.set_graphs(graphs)
+    start = eng.get_state(1)
+    with pytest.raises(engine.OgError) as ex:
+        eng.step(3)
+    assert ex.value.status == engine.OG_ERR_SYSTEM_FAULT
+    f = eng.system_faults()
+    assert f[0] != 0 and f[1] == 0
+    c, v = eng.get_state(1)
+    assert np.array_equal(c, start[0]) and np.array_equal(v, start[1])
+    eng.close()
+
+
 @pytest.mark.parametrize("variant", [6, 10])
 def test_served_vmcmd_jobs_equal_alone_runs(variant):
     """V-McMD jobs handed between engines keep their virtual state and generator: the served

@@ -10,6 +10,8 @@ from omegagene_b200 import cls_io, systems
 from oracle import build as obuild
 from oracle import ogo
 
+import cases
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -35,7 +37,7 @@ def ref_built():
 def test_cell_list_matches_reference_minicell(ref_built, n_waters, box, seed):
     s = systems.water_system(n_waters, box=box, seed=seed)
     nb, pbc, crd, geom = _cell_list_case(s)
-    ours = ogo.CellList(pbc, geom, crd, nb)
+    ours = ogo.CellList(pbc, geom, crd, nb, reference=True)
     ref = ogo.ref_minicell(s["pbc_val"], crd, nb, 13.0, expected_pairs=ours.n_pairs, geom=geom)
     assert ogo.geom_dict(geom) == pytest.approx(ref["geom"])
     assert ours.n_cells == ref["n_cells"]
@@ -61,7 +63,7 @@ def test_cell_list_matches_reference_on_ala3(ref_built):
     s = _ala3_system()
     s["crd"] = s["crd"] + np.random.default_rng(11).uniform(-1e-3, 1e-3, s["crd"].shape)
     nb, pbc, crd, geom = _cell_list_case(s)
-    ours = ogo.CellList(pbc, geom, crd, nb)
+    ours = ogo.CellList(pbc, geom, crd, nb, reference=True)
     ref = ogo.ref_minicell(s["pbc_val"], crd, nb, 13.0, expected_pairs=ours.n_pairs, geom=geom)
     for k in ("slot_atomid", "idx_head", "cell1", "cell2", "image", "mask"):
         np.testing.assert_array_equal(getattr(ours, k), ref[k], err_msg=k)
@@ -174,3 +176,80 @@ def test_oracle_reproduces_reference_thermostat_runs():
                 if key == "step":
                     continue
                 assert float("%.10e" % got[key]) == ref, (name, row["step"], key, got[key], ref)
+
+
+def test_cell_list_across_a_z_gap():
+    """The reference's bin scan (MiniCell.cpp:1062-1076) stops at the first empty bin after a
+    filled one, so cells of a neighbour column beyond the cavity are never paired and atom pairs
+    within the cutoff are lost.  The engine's list (first to last filled bin) holds every pair
+    within the cutoff, holds every pair of the reference's list, and its FP64 forces equal the
+    all-pairs ones; the reference's list gives forces off by far more than rounding."""
+    s = cases.void_water()
+    nb, pbc, crd, geom = _cell_list_case(s)
+    ref = ogo.CellList(pbc, geom, crd, nb, reference=True)
+    ours = ogo.CellList(pbc, geom, crd, nb)
+    k_ref = ogo.unmasked_pair_keys(ref.slot_atomid, ref.cell1, ref.cell2, ref.image, ref.mask)
+    k_ours = ogo.unmasked_pair_keys(ours.slot_atomid, ours.cell1, ours.cell2, ours.image, ours.mask)
+    assert np.isin(k_ref, k_ours).all() and len(k_ours) > len(k_ref)
+    # every atom pair within 12 A (minimum image, exclusions aside) is in the engine's list;
+    # pair codes (lo << 26 | hi) are the keys without their image bits
+    from scipy.spatial import cKDTree
+    L = float(pbc.L[0])
+    x = np.mod(np.asarray(crd, np.float64).reshape(-1, 3) - np.array(pbc.lower, np.float64), L)
+    close = cKDTree(x, boxsize=L).query_pairs(11.99, output_type="ndarray").astype(np.int64)
+    close = np.sort(close, axis=1)
+    ii = np.repeat(np.arange(s["n_atoms"], dtype=np.int64), nb.shape[1])
+    jj = np.asarray(nb, np.int64).reshape(-1)
+    excl = (ii[jj > ii] << 26) | jj[jj > ii]
+    want = (close[:, 0] << 26) | close[:, 1]
+    want = want[~np.isin(want, excl)]
+    assert np.isin(want, k_ours >> 6).all()
+    assert not np.isin(want, k_ref >> 6).all()
+    # forces: FP64 over each list vs FP64 all pairs, both at the list's grid positions (the
+    # coordinates rounded through float, MiniCell.cpp:413-470)
+    n, t = s["n_atoms"], s["topol"]
+    c6, c12 = cls_io.lj_tables(t)
+    q, ty = t["charge"], t["atom_type"].astype(np.int32)
+    Ld = np.array(pbc.L, np.float32).astype(np.float64)
+    grid_pos = np.ascontiguousarray(ours.slot_crd[ours.atomids_rev].reshape(-1))
+    wa, ea, va = np.zeros(3 * n), np.zeros(2), np.zeros(9)
+    ogo.lib().ogo_pair_allpairs_f64(Ld, n, np.ascontiguousarray(ogo.wrap_inbox(pbc, grid_pos).reshape(-1)), q, ty,
+                                    int(t["n_lj_types"]), c6.reshape(-1), c12.reshape(-1), nb.reshape(-1),
+                                    nb.shape[1], 12.0, wa, ea, va)
+    for cl, close_enough in ((ours, True), (ref, False)):
+        pos = np.ascontiguousarray(cl.slot_crd[cl.atomids_rev].reshape(-1))
+        w, e, v = np.zeros(3 * n), np.zeros(2), np.zeros(9)
+        ogo.lib().ogo_pair_cells_f64(Ld, cl._grid, cl._cps, pos, q, ty, int(t["n_lj_types"]), c6.reshape(-1),
+                                     c12.reshape(-1), 12.0, w, e, v)
+        err = float(np.abs(w - wa).max())
+        assert (err < 1e-6) == close_enough, err
+
+
+def test_atom_at_the_upper_face_stays_in_its_column():
+    """The reference computes x = crd - lower in float and wraps x >= L (MiniCell.cpp:329-335):
+    an in-box oxygen 1e-7 A below the upper face goes into column 0, a box length from the grid
+    coordinate it keeps, and its pairs go missing.  The engine's grid keeps it in the last
+    column: FP64 forces over its list equal the all-pairs ones."""
+    s = cases.face_water()
+    nb, pbc, crdw, geom = _cell_list_case(s)
+    L = float(np.float32(pbc.L[0]))
+    assert np.float32(crdw[0, 0] - np.float64(np.float32(pbc.lower[0]))) == np.float32(L)
+    n, t = s["n_atoms"], s["topol"]
+    c6, c12 = cls_io.lj_tables(t)
+    q, ty = t["charge"], t["atom_type"].astype(np.int32)
+    Ld = np.array(pbc.L, np.float32).astype(np.float64)
+    errs = {}
+    for ref_mode in (True, False):
+        cl = ogo.CellList(pbc, geom, crdw, nb, reference=ref_mode)
+        col0 = int(cl.cell_column[cl.atomids_rev[0] // 8])
+        pos = np.ascontiguousarray(cl.slot_crd[cl.atomids_rev].reshape(-1))
+        wa, ea, va = np.zeros(3 * n), np.zeros(2), np.zeros(9)
+        ogo.lib().ogo_pair_allpairs_f64(Ld, n, np.ascontiguousarray(ogo.wrap_inbox(pbc, pos).reshape(-1)), q, ty,
+                                        int(t["n_lj_types"]), c6.reshape(-1), c12.reshape(-1), nb.reshape(-1),
+                                        nb.shape[1], 12.0, wa, ea, va)
+        wc, ec, vc = np.zeros(3 * n), np.zeros(2), np.zeros(9)
+        ogo.lib().ogo_pair_cells_f64(Ld, cl._grid, cl._cps, pos, q, ty, int(t["n_lj_types"]), c6.reshape(-1),
+                                     c12.reshape(-1), 12.0, wc, ec, vc)
+        errs[ref_mode] = (col0 % geom.n_cells_xy[0], float(np.abs(wc - wa).max()))
+    assert errs[True][0] == 0 and errs[True][1] > 1e-2, errs
+    assert errs[False][0] == geom.n_cells_xy[0] - 1 and errs[False][1] < 1e-6, errs
