@@ -212,10 +212,13 @@ __global__ void k_cell_info(const int *__restrict__ counters, int cells_cap, con
     cell_valid[c] = (unsigned char)v;
     int umin = __float2int_rz(__fdiv_rn(__fsub_rn(zmin, S.lowerf[2]), S.L_z_uni));
     int umax = __float2int_rz(__fdiv_rn(__fsub_rn(zmax, S.lowerf[2]), S.L_z_uni));
-    // in-box cells give bins 0..n_uni_z; a runaway coordinate (a blown-up system, whose call is
-    // undone) is held a few bins outside so that no later index arithmetic overflows
-    umin = max(-4, min(umin, S.n_uni_z + 4));
-    umax = max(-4, min(umax, S.n_uni_z + 4));
+    // Bins of the cell's own column.  A cell whose top lies within float rounding of the upper
+    // face divides out to bin n_uni_z, which the reference registers as the next column's bin 0
+    // (MiniCell.cpp:912-926): no cell of its own column then finds it, and the pairs it should
+    // form with them are lost until the next build.  It belongs to bin n_uni_z - 1.  (The clamp
+    // also holds a runaway coordinate of a blown-up system, whose call is undone, in range.)
+    umin = max(0, min(umin, S.n_uni_z - 1));
+    umax = max(0, min(umax, S.n_uni_z - 1));
     cell_uni[c] = make_int2(umin, umax);
     const int n_uni = S.n_columns * S.n_uni_z;
     int steps = 0;
@@ -357,8 +360,8 @@ __device__ int enumerate_column(int c1, int nb, const SysDev &S, int cell_base,
         lu = l;
         const int lo = uni_lo[S.uni_base + fu], hi = uni_hi[S.uni_base + lu];
         if (lo > hi || head2 < 0) continue;
-        // z indices stay inside column 2 (a bin can alias the next column's bin 0 when a
-        // cell's top z equals the box's upper bound)
+        // z indices stay inside column 2 (a window that runs past the column's last bin, with
+        // few bins per column, reads the next column's bins)
         const int last2 = col_cell_start[gcol2 + 1] - 1;
         const float shz = __fmul_rn((float)iz, S.Lf[2]);
         for (int c2 = head2 + lo; c2 <= head2 + hi && c2 <= last2; c2++) {

@@ -257,7 +257,7 @@ static uint64_t pair_mask(const ogo_grid *gr, int c1, int c2, const int *nb15off
  * add_cell_pair (:1163-1203).  Loop order and float arithmetic are those of the
  * reference, so the list comes out in the reference's order. */
 int ogo_enumerate_cell_pairs(const ogo_geom *g, const ogo_pbc *p, const ogo_grid *gr,
-                             const int *nb15off, int max_nb15off, int reference_gap_stop, ogo_cellpairs *out) {
+                             const int *nb15off, int max_nb15off, int reference_faults, ogo_cellpairs *out) {
     memset(out, 0, sizeof(*out));
     const int nx = g->n_cells_xy[0], ny = g->n_cells_xy[1], nuz = g->n_uni_z;
     const int n_uni = g->n_columns * nuz;
@@ -273,6 +273,13 @@ int ogo_enumerate_cell_pairs(const ogo_geom *g, const ogo_pbc *p, const ogo_grid
         float zmax = (float)gr->slot_crd[(c * OGO_N_ATOM_CELL + OGO_N_ATOM_CELL - 1) * 3 + 2] - p->lower[2];
         int   umin = (int)(zmin / g->L_z_uni);
         int   umax = (int)(zmax / g->L_z_uni);
+        if (!reference_faults) {
+            /* a top within float rounding of the upper face divides out to bin nuz, which the
+             * reference registers in the next column's bin 0 (MiniCell.cpp:912-926): its own
+             * column never finds the cell.  It belongs to bin nuz - 1. */
+            if (umin > nuz - 1) umin = nuz - 1;
+            if (umax > nuz - 1) umax = nuz - 1;
+        }
         cu[c * 2] = umin;
         cu[c * 2 + 1] = umax;
         for (int z = umin; z <= umax; z++) {
@@ -327,7 +334,7 @@ int ogo_enumerate_cell_pairs(const ogo_geom *g, const ogo_pbc *p, const ogo_grid
                     if (first_u[ii] < 0) continue;
                     int fu = x2 * nuz + y2 * (nuz * nx) + first_u[ii];
                     int lu = x2 * nuz + y2 * (nuz * nx) + last_u[ii];
-                    /* reference_gap_stop: the reference's scan (MiniCell.cpp:1062-1076), which
+                    /* reference_faults: the reference's scan (MiniCell.cpp:1062-1076), which
                      * ends at the first empty bin after a filled one and so hides the cells
                      * beyond a z gap of a bin's height; otherwise the engine's window, from the
                      * first to the last filled bin (the same list when no bin inside is empty) */
@@ -336,7 +343,7 @@ int ogo_enumerate_cell_pairs(const ogo_geom *g, const ogo_pbc *p, const ogo_grid
                         if (uni_lo[u] >= 0) {
                             if (f < 0) f = u;
                             l = u;
-                        } else if (f >= 0 && reference_gap_stop) {
+                        } else if (f >= 0 && reference_faults) {
                             break;
                         }
                     }

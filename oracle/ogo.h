@@ -83,10 +83,12 @@ void ogo_revise_crd_inbox(const ogo_pbc *p, int n, double *crd);
  * keeps it in the last column, where its grid coordinate lies. */
 int  ogo_grid_build(const ogo_geom *g, int n_atoms, const double *crd, int reference_wrap, ogo_grid *out);
 void ogo_grid_free(ogo_grid *gr);
-/* reference_gap_stop = 1: the reference's bin scan, which hides the cells of a neighbour column
- * beyond a z gap of a uniform bin's height (MiniCell.cpp:1062-1076); 0: the engine's list. */
+/* reference_faults = 1: the reference's uniform grid and bin scan, which register a cell whose
+ * top lies within float rounding of the upper face in the next column (MiniCell.cpp:912-926) and
+ * hide the cells of a neighbour column beyond a z gap of a bin's height (:1062-1076); 0: the
+ * engine's list, which has neither fault. */
 int  ogo_enumerate_cell_pairs(const ogo_geom *g, const ogo_pbc *p, const ogo_grid *gr,
-                              const int *nb15off, int max_nb15off, int reference_gap_stop, ogo_cellpairs *out);
+                              const int *nb15off, int max_nb15off, int reference_faults, ogo_cellpairs *out);
 void ogo_cellpairs_free(ogo_cellpairs *cp);
 
 /* ZeroMultipoleSum::set_zms_params for alpha = 0 (ZeroMultipoleSum.cpp:150-202). */

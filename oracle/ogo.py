@@ -189,11 +189,12 @@ def wrap_inbox(pbc, crd):
 
 class CellList:
     """Grid assignment + cell-pair list computed by the oracle (copied to numpy).  reference=True
-    keeps two faults of the reference's: its bin scan hides the cells of a neighbour column
-    beyond a z gap of a uniform bin's height (MiniCell.cpp:1062-1076), and its column arithmetic
-    wraps an in-box coordinate within float rounding of the upper face into column 0
-    (:329-335).  The default is the engine's grid and list, equal to the reference's whenever
-    neither case occurs."""
+    keeps three faults of the reference's, which lose pairs within the cutoff: its column
+    arithmetic wraps an in-box coordinate within float rounding of the upper x or y face into
+    column 0 (MiniCell.cpp:329-335); its uniform grid registers a cell whose top lies within
+    float rounding of the upper z face in the next column (:912-926); its bin scan hides the
+    cells of a neighbour column beyond a z gap of a bin's height (:1062-1076).  The default is
+    the engine's grid and list, equal to the reference's whenever none of these occurs."""
 
     def __init__(self, pbc, geom, crd, nb15off, reference=False):
         L = lib()

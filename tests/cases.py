@@ -14,20 +14,21 @@ def void_water():
     return systems.water_system(3000, box=44.8, seed=0, lattice_m=15, void=((-5.0, -5.0, -9.0), (5.0, 5.0, 9.0)))
 
 
-def face_water():
-    """3,000-site water box (44.8 A) with molecule 0 moved so that its oxygen sits 1e-7 A below
-    the upper x face, where float(x - lower) rounds to the box length; molecules within 2.6 A of
-    its new place are removed.  Velocities zero."""
+def moved_water(mol, axis, delta):
+    """3,000-site water box (44.8 A) with molecule `mol` moved so that its oxygen sits `delta` A
+    below the box's upper face along `axis`; molecules within 2.6 A of its new place are
+    removed.  Velocities zero."""
     s = systems.water_system(3000, box=44.8, seed=0, lattice_m=15)
     pbc = ogo.make_pbc(s["pbc_val"])
     crd = np.array(s["crd"], dtype=np.float64)
-    upper = float(np.float32(pbc.upper[0]))
-    crd[0:3, 0] += upper - 1e-7 - crd[0, 0]
-    crd[0:3] = ogo.wrap_inbox(pbc, crd[0:3])
-    d = crd.reshape(-1, 3, 3)[:, 0, :] - crd[0]
+    upper = float(np.float32(pbc.upper[axis]))
+    sl = slice(3 * mol, 3 * mol + 3)
+    crd[sl, axis] += upper - delta - crd[3 * mol, axis]
+    crd[sl] = ogo.wrap_inbox(pbc, crd[sl])
+    d = crd.reshape(-1, 3, 3)[:, 0, :] - crd[3 * mol]
     d -= float(pbc.L[0]) * np.round(d / float(pbc.L[0]))
     keep = np.sqrt((d ** 2).sum(1)) > 2.6
-    keep[0] = True
+    keep[mol] = True
     w = crd.reshape(-1, 3, 3)[keep].reshape(-1, 3)
     nw = len(w) // 3
     mass = np.tile([systems.M_O, systems.M_H, systems.M_H], nw)
@@ -36,3 +37,16 @@ def face_water():
                              atom_type=np.tile([0, 1, 1], nw), lj_types=[(systems.SIGMA_O, systems.EPS_O), (0.0, 0.0)],
                              bonds=None, angles=None, excl=systems._water_exclusions(0, nw), pairs=None,
                              trios=systems._water_trios(0, nw))
+
+
+def face_water():
+    """Molecule 0's oxygen 1e-7 A below the upper x face, where float(x - lower) rounds to the
+    box length."""
+    return moved_water(0, 0, 1e-7)
+
+
+def top_water():
+    """Molecule 9's oxygen 2e-7 A below the upper z face, where its cell's top divides out to
+    the uniform bin n_uni_z (201,810 cell pairs by the reference's grid, 201,962 with the cell
+    kept in its own column)."""
+    return moved_water(9, 2, 2e-7)

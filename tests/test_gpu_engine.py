@@ -54,9 +54,10 @@ SMALL = [
     ("water700", lambda: systems.water_system(700, seed=9)),
     ("chain300", lambda: systems.chain_water_system(300, 2500, seed=4, radius=12.0)),
     # where the reference's list build loses pairs (tests/cases.py, test_oracle.py): a cavity
-    # whose z gap its bin scan does not cross, an oxygen at the upper face
+    # whose z gap its bin scan does not cross, oxygens at the upper x and z faces
     ("water_void", cases.void_water),
     ("water_face", cases.face_water),
+    ("water_top", cases.top_water),
 ]
 
 
