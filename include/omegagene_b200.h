@@ -239,7 +239,11 @@ og_status og_put_state(og_engine *e, int32_t sys, const double *crd, const doubl
 /* Stream-ordered device->host copies of state and energies (NULL pointers are skipped);
  * complete after og_synchronize.  The role of cuda_memcpy_dtoh_work (cuda_setup.cu:803-823). */
 og_status og_get_state_async(og_engine *e, int32_t sys, double *crd, double *vel_next, double *energies);
-/* Steps without the end-of-call synchronisation (see og_step); flags are read with og_get_flags. */
+/* Steps without the end-of-call synchronisation (see og_step); flags are read with og_get_flags.
+ * Under the displacement list policy with graphs on (and no V-McMD system), the call's last step
+ * (the one that computes energies) replays a captured one-step CUDA graph: its list rebuild is a
+ * conditional node decided on the device, so the graph holds at any step.  The results equal
+ * kernel-by-kernel steps bit for bit; the first such call captures the graph. */
 og_status og_step_async(og_engine *e, int32_t n_steps);
 og_status og_synchronize(og_engine *e);
 og_status og_get_state(og_engine *e, int32_t sys, double *crd, double *vel_next);

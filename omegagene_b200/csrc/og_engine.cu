@@ -308,6 +308,11 @@ struct og_engine {
     std::string graph_note;           // why graph capture turned graphs off, if it did
     long long graph_kernels = 0;      // kernel launches one replay stands for
     long long graph_replays = 0;
+    // one step with energies, replayed by og_step_async under the displacement list policy
+    // (whose rebuilds are conditional nodes, so the graph holds at any step)
+    cudaGraphExec_t graph1_exec = nullptr;
+    long long graph1_kernels = 0;
+    bool graph1_failed = false;       // capture failed once: single steps run kernel by kernel
     // segment bases for the two-level reductions and their chunk counts
     int *d_seg_atoms = nullptr, *d_seg_exc = nullptr, *d_seg_bond = nullptr, *d_seg_angle = nullptr;
     int mc_atoms = 1, mc_cells = 1, mc_exc = 1, mc_bond = 1, mc_angle = 1, mc_grp = 1;
@@ -1407,6 +1412,8 @@ og_status check_flags(og_engine *e) {
 void drop_graph(og_engine *e) {
     if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
     e->graph_exec = nullptr;
+    if (e->graph1_exec) cudaGraphExecDestroy(e->graph1_exec);
+    e->graph1_exec = nullptr;
 }
 
 og_status grow_pairs(og_engine *e, long long need) {
@@ -1487,6 +1494,30 @@ og_status capture_interval(og_engine *e) {
         e->graph_exec = nullptr;
         e->use_graphs = false;
         e->graph_note = s != OG_OK ? e->err : std::string(cudaGetErrorString(r));
+    }
+    return OG_OK;
+}
+
+// One step with energies as a graph (og_step_async's single steps under the displacement
+// policy).  A failed capture leaves single steps kernel by kernel; the interval graphs of
+// og_step are not affected.
+og_status capture_one_step(og_engine *e) {
+    const long long step0 = e->host_step, launches0 = e->launches;
+    CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeRelaxed));
+    e->capturing = true;
+    og_status s = run_step(e, true);
+    e->capturing = false;
+    cudaGraph_t g = nullptr;
+    cudaError_t r = cudaStreamEndCapture(e->stream, &g);
+    e->host_step = step0;
+    e->graph1_kernels = e->launches - launches0;
+    e->launches = launches0;
+    if (s == OG_OK && r == cudaSuccess && g) r = cudaGraphInstantiate(&e->graph1_exec, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (s != OG_OK || r != cudaSuccess || !e->graph1_exec) {
+        cudaGetLastError();
+        e->graph1_exec = nullptr;
+        e->graph1_failed = true;
     }
     return OG_OK;
 }
@@ -1629,6 +1660,7 @@ og_status og_destroy(og_engine *e) {
     if (e->ev_step0) cudaEventDestroy(e->ev_step0);
     if (e->ev_step1) cudaEventDestroy(e->ev_step1);
     if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
+    if (e->graph1_exec) cudaGraphExecDestroy(e->graph1_exec);
     if (e->stream) cudaStreamDestroy(e->stream);
     if (e->side) cudaStreamDestroy(e->side);
     delete e;
@@ -2801,6 +2833,20 @@ extern "C" og_status og_step_async(og_engine *e, int32_t n_steps) {
     for (int i = 0; i < n_steps; i++) {
         og_status s = logs_reserve(e, 1);  // synchronises only when a V-McMD log ring is full
         if (s) return s;
+        // the call's last step (the one with energies) replays a one-step graph when nothing of
+        // the step is decided on the host: the displacement policy's rebuilds are conditional
+        // nodes; V-McMD systems keep the kernel-by-kernel path
+        if (i == n_steps - 1 && e->use_graphs && !e->graph1_failed && e->timing != 1 &&
+            e->list_policy == OG_LIST_DISPLACEMENT && e->n_vm == 0) {
+            if (!e->graph1_exec && (s = capture_one_step(e))) return s;
+            if (e->graph1_exec) {
+                CK(cudaGraphLaunch(e->graph1_exec, e->stream));
+                e->launches += e->graph1_kernels;
+                e->graph_replays++;
+                e->host_step++;
+                continue;
+            }
+        }
         s = run_step(e, i == n_steps - 1);
         if (s) return s;
     }

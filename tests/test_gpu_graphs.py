@@ -68,3 +68,43 @@ def test_graph_split_calls_equal_one_call():
     np.testing.assert_array_equal(t1, t2)
     for (c1, v1), (c2, v2) in zip(s1, s2):
         assert np.array_equal(c1, c2) and np.array_equal(v1, v2)
+
+
+def test_single_step_graph_equals_kernel_by_kernel():
+    """og_step_async replays a captured one-step graph (with energies) for the last step of a
+    call under the displacement list policy, whose rebuilds are conditional nodes.  Single-step
+    calls with og_put_state in between, as an end-to-end caller makes them, give the trajectory
+    and per-step energies of kernel-by-kernel steps bit for bit, rebuilds included; a batch with a
+    thermostat-with-SHAKE system and an NVE system covers the WHILE node inside the graph."""
+    thermo = _params(nsgrid_update_intvl=10, time_step=2.0, thermostat="scaling", temperature=300.0)
+    hot = systems.water_system(1500, seed=5)
+    hot = dict(hot, vel=np.asarray(hot["vel"]) * 4.0)  # passes the list margin within a few steps
+    batch = [(hot, _params(nsgrid_update_intvl=10, time_step=2.0)), (systems.water_system(700, seed=9), thermo)]
+    n = 40
+    out = []
+    for graphs in (True, False):
+        eng = engine.Engine(0)
+        eng.set_tuning(10)
+        eng.set_list_policy("displacement")
+        eng.set_graphs(graphs)
+        for s, p in batch:
+            eng.add_system(s, p)
+        eng.finalize()
+        eng.set_trace(n)
+        b0 = eng.list_builds()
+        for k in range(n):
+            if k % 7 == 3:  # a caller's coordinates handed back between steps
+                c = np.ascontiguousarray(eng.get_state(0)[0])
+                eng.put_state_ptr(0, c.ctypes.data, 0)
+            eng.step_async(1)
+        eng.synchronize()
+        assert eng.flags() & (8 | 16) == 0
+        out.append((eng.get_state(0), eng.get_state(1), eng.get_trace(n).copy(), eng.list_builds() - b0,
+                    eng.graph_info()))
+        eng.close()
+    (a0, a1, ta, ba, ga), (b0_, b1, tb, bb, gb) = out
+    assert ba == bb and ba >= 2  # rebuilds happened inside the graph replays too
+    assert ga["replays"] >= n - 1 and gb["replays"] == 0
+    for x, y in ((a0, b0_), (a1, b1)):
+        assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1])
+    np.testing.assert_array_equal(ta, tb)
