@@ -1099,14 +1099,23 @@ k_jl_build(int *__restrict__ counters, const int *__restrict__ cell_sys, const S
     const long long k_end = min((long long)cp_head[c1 + 1], pair_cap);
     int2 *out = jl + 8 * k_beg;
     int count = 0;
+    // each chunk's records are loaded while the previous chunk is processed
+    float4 sp_next = make_float4(0.f, 0.f, 0.f, 0.f);
+    unsigned long long m_next = ~0ull;
+    if (k_beg + lane < k_end) {
+        sp_next = cp_shift[k_beg + lane];
+        m_next = cp_mask[k_beg + lane];
+    }
     for (long long chunk = k_beg; chunk < k_end; chunk += 32) {
         const long long kk = chunk + lane;
-        float4 sp = make_float4(0.f, 0.f, 0.f, 0.f);
-        unsigned long long m = ~0ull;
+        const float4 sp = sp_next;
+        const unsigned long long m = m_next;
+        if (kk + 32 < k_end) {
+            sp_next = cp_shift[kk + 32];
+            m_next = cp_mask[kk + 32];
+        }
         bool keep = false;
         if (kk < k_end) {
-            sp = cp_shift[kk];
-            m = cp_mask[kk];
             const int c2 = __float_as_int(sp.w);
             const float4 l2 = bbox[2 * c2], h2 = bbox[2 * c2 + 1];
             const float gx = fmaxf(0.f, fmaxf(l2.x + sp.x - b1h.x, b1l.x - (h2.x + sp.x)));
@@ -1123,36 +1132,47 @@ k_jl_build(int *__restrict__ counters, const int *__restrict__ cell_sys, const S
             s_k[wib][rank] = (int)kk;
         }
         __syncwarp();
-        for (int r = 0; r < n_keep; r += 4) {
-            const int idx = r + q;
-            const bool active = idx < n_keep;
-            float4 rsp = make_float4(0.f, 0.f, 0.f, 0.f);
-            unsigned long long rm = ~0ull;
-            int rk = 0;
-            if (active) {
-                rsp = s_sp[wib][idx];
-                const uint2 mm = s_m[wib][idx];
-                rm = ((unsigned long long)mm.y << 32) | mm.x;
-                rk = s_k[wib][idx];
+        // the survivors, four at a time (lane: survivor q, j atom jj); two such rounds per pass,
+        // with both rounds' position loads issued before either is tested
+        for (int r = 0; r < n_keep; r += 8) {
+            float4 rsp[2], xj[2];
+            unsigned skip[2];
+            int rk[2];
+            bool live[2];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int idx = r + 4 * h + q;
+                const bool active = idx < n_keep;
+                rsp[h] = make_float4(0.f, 0.f, 0.f, 0.f);
+                unsigned long long rm = ~0ull;
+                rk[h] = 0;
+                if (active) {
+                    rsp[h] = s_sp[wib][idx];
+                    const uint2 mm = s_m[wib][idx];
+                    rm = ((unsigned long long)mm.y << 32) | mm.x;
+                    rk[h] = s_k[wib][idx];
+                }
+                skip[h] = active ? (unsigned)(rm >> (jj * OG_CELL)) & 0xffu : 0xffu;
+                live[h] = active && skip[h] != 0xffu;
+                xj[h] = live[h] ? xq[__float_as_int(rsp[h].w) * OG_CELL + jj] : make_float4(0.f, 0.f, 0.f, 0.f);
             }
-            const int c2 = __float_as_int(rsp.w);
-            const unsigned skip = active ? (unsigned)(rm >> (jj * OG_CELL)) & 0xffu : 0xffu;
-            bool push = false;
-            if (active && skip != 0xffu) {
-                float4 xj = xq[c2 * OG_CELL + jj];
-                xj.x += rsp.x;
-                xj.y += rsp.y;
-                xj.z += rsp.z;
-                const float gx = fmaxf(0.f, fmaxf(xj.x - b1h.x, b1l.x - xj.x));
-                const float gy = fmaxf(0.f, fmaxf(xj.y - b1h.y, b1l.y - xj.y));
-                const float gz = fmaxf(0.f, fmaxf(xj.z - b1h.z, b1l.z - xj.z));
-                push = gx * gx + gy * gy + gz * gz < rb2;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int c2 = __float_as_int(rsp[h].w);
+                bool push = false;
+                if (live[h]) {
+                    const float x = xj[h].x + rsp[h].x, y = xj[h].y + rsp[h].y, z = xj[h].z + rsp[h].z;
+                    const float gx = fmaxf(0.f, fmaxf(x - b1h.x, b1l.x - x));
+                    const float gy = fmaxf(0.f, fmaxf(y - b1h.y, b1l.y - y));
+                    const float gz = fmaxf(0.f, fmaxf(z - b1h.z, b1l.z - z));
+                    push = gx * gx + gy * gy + gz * gz < rb2;
+                }
+                const unsigned pb = __ballot_sync(0xffffffffu, push);
+                if (push)
+                    out[count + __popc(pb & ((1u << lane) - 1u))] =
+                        make_int2((int)((unsigned)(c2 * OG_CELL + jj) | (skip[h] << 24)), rk[h]);
+                count += __popc(pb);
             }
-            const unsigned pb = __ballot_sync(0xffffffffu, push);
-            if (push)
-                out[count + __popc(pb & ((1u << lane) - 1u))] =
-                    make_int2((int)((unsigned)(c2 * OG_CELL + jj) | (skip << 24)), rk);
-            count += __popc(pb);
         }
         __syncwarp();  // the next chunk's survivors overwrite this chunk's
     }
