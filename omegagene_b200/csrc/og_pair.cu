@@ -1208,21 +1208,19 @@ k_pair_ljzd_jl(int *__restrict__ counters, const int *__restrict__ cell_sys, con
     og_iacc_zero(A);
     const int2 *ent = jl + 8LL * cp_head[c1];
     const int n = jl_count[c1];
-    // entries are loaded two rounds ahead and their gathers issued one round ahead, so neither
-    // load of the entry -> position chain is waited on in the round that issues it
-    float4 g_xj = make_float4(0.f, 0.f, 0.f, 0.f);
+    // entries are loaded two rounds ahead and their gathers issued one round ahead; the gathered
+    // values stay as loaded (position and cell-pair shift apart) until the round that uses them,
+    // so neither load of the entry -> position chain is waited on in the round that issues it
+    float4 g_xq = make_float4(0.f, 0.f, 0.f, 0.f), g_sp = make_float4(0.f, 0.f, 0.f, 0.f);
     int g_tj = 0, g_slot = 0, g_img = 0;
     unsigned g_skip = 0xffu;
     auto gather = [&](int2 e, bool ok) {
         if (ok) {
             g_slot = e.x & 0xffffff;
             g_skip = (unsigned)e.x >> 24;
-            const float4 sp = cp_shift[e.y];
-            g_xj = xq[g_slot];
+            g_sp = cp_shift[e.y];
+            g_xq = xq[g_slot];
             g_tj = slot_type[g_slot];
-            g_xj.x += sp.x;
-            g_xj.y += sp.y;
-            g_xj.z += sp.z;
             if (VIR) g_img = cp_c2img[e.y].y;
         }
     };
@@ -1231,7 +1229,7 @@ k_pair_ljzd_jl(int *__restrict__ counters, const int *__restrict__ cell_sys, con
     if (32 + lane < n) e_ahead = ent[32 + lane];
     for (int r = 0; r < n; r += 32) {
         const bool active = r + lane < n;
-        const float4 xj = g_xj;
+        const float4 xj = make_float4(g_xq.x + g_sp.x, g_xq.y + g_sp.y, g_xq.z + g_sp.z, g_xq.w);
         const int tj = g_tj, slot = g_slot, img = g_img;
         const unsigned skip = active ? g_skip : 0xffu;
         const int2 e1 = e_ahead;
