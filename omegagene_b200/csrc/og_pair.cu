@@ -1208,9 +1208,12 @@ k_pair_ljzd_jl(int *__restrict__ counters, const int *__restrict__ cell_sys, con
     og_iacc_zero(A);
     const int2 *ent = jl + 8LL * cp_head[c1];
     const int n = jl_count[c1];
-    // entries are loaded two rounds ahead and their gathers issued one round ahead; the gathered
-    // values stay as loaded (position and cell-pair shift apart) until the round that uses them,
-    // so neither load of the entry -> position chain is waited on in the round that issues it
+    // entries are loaded AHEAD rounds ahead and their gathers issued one round ahead; the
+    // gathered values stay as loaded (position and cell-pair shift apart) until the round that
+    // uses them, so neither load of the entry -> position chain is waited on in the round that
+    // issues it.  Three rounds for the energy-free zero-dipole kernel; two where the energy or
+    // generic terms leave no registers for the third (it spills there)
+    constexpr int AHEAD = (ENE || GEN) ? 2 : 3;
     float4 g_xq = make_float4(0.f, 0.f, 0.f, 0.f), g_sp = make_float4(0.f, 0.f, 0.f, 0.f);
     int g_tj = 0, g_slot = 0, g_img = 0;
     unsigned g_skip = 0xffu;
@@ -1224,16 +1227,22 @@ k_pair_ljzd_jl(int *__restrict__ counters, const int *__restrict__ cell_sys, con
             if (VIR) g_img = cp_c2img[e.y].y;
         }
     };
-    int2 e_ahead = make_int2(0, 0);
+    int2 e_ahead[AHEAD - 1];  // entries of rounds r + 1 .. r + AHEAD - 1
     if (lane < n) gather(ent[lane], true);
-    if (32 + lane < n) e_ahead = ent[32 + lane];
+#pragma unroll
+    for (int a = 0; a < AHEAD - 1; a++) {
+        e_ahead[a] = make_int2(0, 0);
+        if (32 * (a + 1) + lane < n) e_ahead[a] = ent[32 * (a + 1) + lane];
+    }
     for (int r = 0; r < n; r += 32) {
         const bool active = r + lane < n;
         const float4 xj = make_float4(g_xq.x + g_sp.x, g_xq.y + g_sp.y, g_xq.z + g_sp.z, g_xq.w);
         const int tj = g_tj, slot = g_slot, img = g_img;
         const unsigned skip = active ? g_skip : 0xffu;
-        const int2 e1 = e_ahead;
-        if (r + 64 + lane < n) e_ahead = ent[r + 64 + lane];
+        const int2 e1 = e_ahead[0];
+#pragma unroll
+        for (int a = 0; a + 1 < AHEAD - 1; a++) e_ahead[a] = e_ahead[a + 1];
+        if (r + 32 * AHEAD + lane < n) e_ahead[AHEAD - 2] = ent[r + 32 * AHEAD + lane];
         gather(e1, r + 32 + lane < n);
         og_eval_j<VIR, ENE, GEN>(A, active, xj, tj, skip, slot, img, s_i[wib], K, S, E, lj, hps, frc);
     }
